@@ -1,0 +1,86 @@
+/*
+ * sdsb200_analysis.h -- host analysis that produces the Symbolic maps consumed by
+ * the numeric phase (libsdsb200.so).
+ *
+ * The reference keeps its analysis in Julia (the files under src/symbolic/,
+ * symbolic_analysis at src/symbolic/maps.jl:255-268); a Julia caller of the
+ * numeric phase passes its own `Symbolic` maps and never needs this library.
+ * It exists so that C, C++ and Python callers (and the tests and benchmark of
+ * this repository) can build the same maps without Julia: every step restates
+ * the reference's algorithm (pattern, 2x2 pivot pairs, etree, postorder, column
+ * counts, fundamental supernodes, relaxed amalgamation, supernodal row
+ * structure, panel layout, assembly map, extend-add maps) except the ordering,
+ * whose reference implementation is third-party (AMD.jl / METIS through
+ * CliqueTrees.jl) and is replaced by this library's own AMD and nested
+ * dissection.
+ *
+ * All arrays returned by sdsa_get are int64, 1-based where the reference's maps
+ * are 1-based (the values are exactly those a Julia `Symbolic` would hold).
+ */
+#ifndef SDSB200_ANALYSIS_H
+#define SDSB200_ANALYSIS_H
+#include <stdint.h>
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* structures: same codes as the numeric phase (sdsb200.h) */
+#define SDSA_STRUCTURE_G 0
+#define SDSA_STRUCTURE_S 1
+#define SDSA_STRUCTURE_SPD 3
+
+/* reordering algorithms (cuDSS names: "default", "algo3" AMD, "algo4" ND, "algo5" natural) */
+#define SDSA_REORDER_DEFAULT 0 /* AMD and ND evaluated, the lower flops + 1e8 * sdepth wins */
+#define SDSA_REORDER_AMD 1
+#define SDSA_REORDER_ND 2
+#define SDSA_REORDER_NATURAL 3
+
+#define SDSA_PAIRS_NONE 0
+#define SDSA_PAIRS_DEFAULT 1
+#define SDSA_PAIRS_ALL 2
+
+typedef struct sdsa_options {
+    int structure;          /* SDSA_STRUCTURE_* */
+    int view;               /* 'L', 'U' or 'F' */
+    int index_base;         /* 0 or 1: base of rowptr/colval */
+    int reordering;         /* SDSA_REORDER_* (ignored when user_perm != NULL) */
+    const int64_t* user_perm; /* length n, 0- or 1-based, or NULL */
+    int pivot_pairs;        /* SDSA_PAIRS_* (structure "S" only) */
+    double pivot_pair_tolerance; /* 1e-6 */
+    double pivot_threshold;      /* 0.01: partner threshold of the pairs */
+    int use_superpanels;    /* 1: amalgamation on */
+    int amalg_max_width;    /* 32 */
+    double amalg_zero_fraction; /* 0.25 */
+    int amalg_min_width;    /* 8 */
+} sdsa_options;
+
+typedef struct sdsa_result sdsa_result;
+
+/* Fill `o` with the reference defaults (Options() of src/options.jl). */
+void sdsa_default_options(sdsa_options* o, int structure);
+
+/* Analyse the n x n CSR pattern (rowptr: n+1, colval: nnz). nzval (length nnz,
+ * may be NULL) is read only for the 2x2 pivot pairs of structure "S".
+ * Returns 0 or a negative error code; sdsa_last_error() gives the message. */
+int sdsa_analyze(int64_t n, const int64_t* rowptr, const int64_t* colval, const double* nzval,
+                 const sdsa_options* opts, sdsa_result** out);
+
+/* Array accessors by name: length (or -1 for an unknown name), then copy. Names:
+ * perm iperm super_ptr snparent snpost rowptr rowval front_ptr front_nrows front_ncols
+ * child_ptr child_list relind_ptr relind amap amap_ptr amap_src counts
+ * pairs (2*npairs: partner, candidate)
+ * full_rowptr full_colval full_srcptr full_src full_conj  (residual map of the full matrix) */
+int64_t sdsa_len(const sdsa_result* r, const char* name);
+int sdsa_get(const sdsa_result* r, const char* name, int64_t* out);
+
+/* Scalars by name: n nnz ns nnz_stored nnz_L flops factor_len sdepth alg_used
+ * (1 amd, 2 nd, 3 natural, 4 user) npairs pair_rounds */
+double sdsa_stat(const sdsa_result* r, const char* name);
+
+void sdsa_free(sdsa_result* r);
+const char* sdsa_last_error(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

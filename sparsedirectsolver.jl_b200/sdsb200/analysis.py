@@ -1,0 +1,113 @@
+"""Host analysis: CSR pattern -> the reference's ``Symbolic`` maps.
+
+Thin ctypes layer over ``libsdsb200_analysis.so`` (include/sdsb200_analysis.h),
+which restates the reference's ``symbolic_analysis``
+(SparseDirectSolver.jl src/symbolic/maps.jl:255-268).
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+from dataclasses import dataclass, field
+
+import numpy as np
+
+from ._native import analysis_lib
+
+STRUCTURES = {"G": 0, "S": 1, "SPD": 3}
+REORDERING = {"default": 0, "algo1": 1, "algo2": 1, "algo3": 1, "amd": 1, "algo4": 2, "nd": 2, "algo5": 3,
+              "natural": 3}
+PAIRS = {"none": 0, "default": 1, "all": 2}
+
+MAP_NAMES = ("perm", "iperm", "super_ptr", "snparent", "snpost", "rowptr", "rowval", "front_ptr", "front_nrows",
+             "front_ncols", "child_ptr", "child_list", "relind_ptr", "relind", "amap", "amap_ptr", "amap_src",
+             "counts", "pairs", "full_rowptr", "full_colval", "full_srcptr", "full_src", "full_conj")
+
+
+class _Opts(C.Structure):
+    _fields_ = [("structure", C.c_int), ("view", C.c_int), ("index_base", C.c_int), ("reordering", C.c_int),
+                ("user_perm", C.POINTER(C.c_int64)), ("pivot_pairs", C.c_int),
+                ("pivot_pair_tolerance", C.c_double), ("pivot_threshold", C.c_double),
+                ("use_superpanels", C.c_int), ("amalg_max_width", C.c_int), ("amalg_zero_fraction", C.c_double),
+                ("amalg_min_width", C.c_int)]
+
+
+@dataclass
+class Symbolic:
+    """The reference's ``Symbolic`` (src/symbolic/maps.jl:62-95): 1-based int64 maps.
+
+    Field names follow ``DEVICE_MAPS`` (maps.jl:16-18); ``snpost``, ``counts``,
+    ``pairs`` and the ``full_*`` residual map are the host-side extras.
+    """
+
+    n: int
+    nnz: int
+    ns: int
+    structure: str
+    view: str
+    index_base: int
+    nnz_stored: int
+    nnz_L: int
+    flops: float
+    sdepth: int
+    alg_used: int
+    maps: dict = field(default_factory=dict)
+
+    def __getattr__(self, name):
+        maps = self.__dict__.get("maps")
+        if maps is not None and name in maps:
+            return maps[name]
+        raise AttributeError(name)
+
+    @property
+    def factor_len(self) -> int:
+        return int(self.front_ptr[-1] - 1) if self.ns > 0 else 0
+
+
+def analyze(rowptr, colval, n, structure="SPD", nzval=None, view="F", index_base=0, reordering="default",
+            user_perm=None, pivot_pairs="default", pivot_pair_tolerance=1e-6, pivot_threshold=0.01,
+            use_superpanels=1, amalgamation=(32, 0.25, 8)) -> Symbolic:
+    """Analyse the pattern of an ``n x n`` CSR matrix (``index_base`` of its arrays)."""
+    lib = analysis_lib()
+    rp = np.ascontiguousarray(rowptr, dtype=np.int64)
+    cv = np.ascontiguousarray(colval, dtype=np.int64)
+    if rp.size != n + 1:
+        raise ValueError(f"rowptr has {rp.size} entries, expected n + 1 = {n + 1}")
+    nz = None if nzval is None else np.ascontiguousarray(np.asarray(nzval, dtype=np.float64).reshape(-1)[: cv.size])
+    up = None if user_perm is None else np.ascontiguousarray(user_perm, dtype=np.int64)
+    o = _Opts()
+    lib.sdsa_default_options(C.byref(o), STRUCTURES[structure])
+    o.view = ord(view)
+    o.index_base = int(index_base)
+    o.reordering = REORDERING[reordering]
+    o.user_perm = up.ctypes.data_as(C.POINTER(C.c_int64)) if up is not None else None
+    o.pivot_pairs = PAIRS[pivot_pairs]
+    o.pivot_pair_tolerance = pivot_pair_tolerance
+    o.pivot_threshold = pivot_threshold
+    o.use_superpanels = int(use_superpanels)
+    o.amalg_max_width, o.amalg_zero_fraction, o.amalg_min_width = amalgamation
+    res = C.c_void_p()
+    rc = lib.sdsa_analyze(C.c_int64(n), rp.ctypes.data_as(C.c_void_p), cv.ctypes.data_as(C.c_void_p),
+                          nz.ctypes.data_as(C.c_void_p) if nz is not None else None, C.byref(o), C.byref(res))
+    if rc != 0:
+        raise ValueError("analysis failed: " + lib.sdsa_last_error().decode())
+    try:
+        maps = {}
+        for nm in MAP_NAMES:
+            ln = lib.sdsa_len(res, nm.encode())
+            a = np.zeros(max(ln, 0), dtype=np.int64)
+            if ln > 0:
+                lib.sdsa_get(res, nm.encode(), a.ctypes.data_as(C.c_void_p))
+            maps[nm] = a
+        st = lambda k: lib.sdsa_stat(res, k.encode())  # noqa: E731
+        return Symbolic(n=int(n), nnz=int(cv.size), ns=int(st("ns")), structure=structure, view=view,
+                        index_base=int(index_base), nnz_stored=int(st("nnz_stored")), nnz_L=int(st("nnz_L")),
+                        flops=float(st("flops")), sdepth=int(st("sdepth")), alg_used=int(st("alg_used")),
+                        maps=maps)
+    finally:
+        lib.sdsa_free(res)
+
+
+def analyze_csr(A, structure="SPD", **kw) -> Symbolic:
+    """``analyze`` for a scipy CSR matrix (0-based arrays)."""
+    return analyze(A.indptr, A.indices, A.shape[0], structure, nzval=A.data, index_base=0, **kw)
