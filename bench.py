@@ -1,0 +1,388 @@
+"""Benchmark of the numeric phase: factor + solve of the 3-D Laplacian workload.
+
+Workload (one step): factorization of the 7-point Laplacian on a 48 x 48 x 48
+grid (n = 110 592, nested dissection) and the solve of 4 right-hand sides
+U[-1, 1], to a scaled backward error <= 1e-12, in two forms:
+
+* mixed: FP32 factor (assembly and Schur updates in FP32) + FP64 iterative
+  refinement (FP64 residual), the headline form;
+* fp64: every operation in FP64.
+
+value = algorithmic GFLOP/s of one step (factorization flops in the
+reference's convention sum over panel columns of rows^2, plus 4 nnz_stored
+nrhs for the solve), with the values and right-hand sides resident in HBM.
+e2e = the same through the public DirectSolver API with host buffers (H2D of
+values and right-hand sides, D2H of the solution inside the timed region).
+
+`--impl reference` times the CPU oracle (this repository's restatement of the
+reference's CPU factorization and solve; the reference itself is Julia, which
+is not installed) on the same workload.
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes as C
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+PKG = os.path.join(ROOT, "sparsedirectsolver.jl_b200")
+for p in (ROOT, PKG):
+    if p not in sys.path:
+        sys.path.insert(0, p)
+
+import numpy as np  # noqa: E402
+
+METRIC = "factor+solve ms & GFLOP/s at bwd err ≤1e-12: mixed+IR vs FP64, 1 B200"
+GRID = 48
+NRHS = 4
+BERR_TARGET = 1e-12
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--grid", type=int, default=GRID)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    return ap.parse_args()
+
+
+def workload(grid):
+    from sdsb200 import matrices as M
+
+    A = M.lap3d(grid, grid, grid)
+    b = M.rhs(A.shape[0], NRHS, seed=0)
+    return A, b
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons during the timed region."""
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.path = os.path.join(ROOT, "gpurun_out", f"clocks_{os.getpid()}.csv")
+
+    def __enter__(self):
+        os.makedirs(os.path.dirname(self.path), exist_ok=True)
+        try:
+            self.fh = open(self.path, "w")
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.index}",
+                 "--query-gpu=clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+                 "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+                 "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap",
+                 "--format=csv,noheader,nounits", "-lms", "100"], stdout=self.fh, stderr=subprocess.DEVNULL)
+        except OSError:
+            self.proc = None
+        return self
+
+    def __exit__(self, *exc):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+            self.fh.close()
+
+    def summary(self):
+        if self.proc is None or not os.path.exists(self.path):
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in open(self.path):
+            parts = [x.strip() for x in line.split(",")]
+            if len(parts) < 8:
+                continue
+            try:
+                sm.append(float(parts[0]))
+                smax = float(parts[1])
+            except ValueError:
+                continue
+            for nm, v in zip(names, parts[4:8]):
+                if v.lower().startswith("active"):
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": smax, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def measured_gemm_peak(torch, dtype):
+    """Dense GEMM throughput of cuBLAS on this GPU (TFLOP/s), best of a few 8192^3 products."""
+    n = 8192
+    a = torch.randn(n, n, device="cuda", dtype=dtype)
+    bm = torch.randn(n, n, device="cuda", dtype=dtype)
+    prev = torch.backends.cuda.matmul.allow_tf32
+    torch.backends.cuda.matmul.allow_tf32 = False
+    for _ in range(2):
+        torch.matmul(a, bm)
+    best = 0.0
+    for _ in range(4):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        torch.matmul(a, bm)
+        e1.record()
+        torch.cuda.synchronize()
+        best = max(best, 2.0 * n ** 3 / (e0.elapsed_time(e1) / 1e3) / 1e12)
+    torch.backends.cuda.matmul.allow_tf32 = prev
+    del a, bm
+    torch.cuda.empty_cache()
+    return best
+
+
+def measured_peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(path):
+        with open(path) as fh:
+            return json.load(fh), "measured"
+    return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0}, "fallback"
+
+
+def run_reference(args, rank):
+    """CPU oracle timed on the host cores, same workload, same metric."""
+    if rank != 0:
+        return
+    from oracle.oracle import Oracle
+    from sdsb200 import analyze_csr
+    from sdsb200 import matrices as M
+
+    A, b = workload(args.grid)
+    S = analyze_csr(A, "SPD", reordering="nd")
+    O = Oracle(S)
+    flops = S.flops + 4.0 * S.nnz_stored * NRHS
+    times = []
+    for it in range(args.warmup + args.steps):
+        t0 = time.perf_counter()
+        O.factorize(A.data, "SPD")
+        x = O.solve(b)
+        dt = time.perf_counter() - t0
+        if it >= args.warmup:
+            times.append(dt)
+    berr = M.scaled_backward_error(A, x, b)
+    ms = 1e3 * statistics.mean(times)
+    gflops = flops / (ms / 1e3) / 1e9
+    out = {"impl": "reference", "metric": METRIC, "value": round(gflops, 4), "unit": "GFLOP/s", "n_gpus": args.gpus,
+           "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms, 3), "higher_is_better": True,
+           "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+           "config": {"workload": f"lap3d_{args.grid} SPD Cholesky factor+solve, nested dissection, {NRHS} RHS",
+                      "n": int(A.shape[0]), "nrhs": NRHS, "form": "fp64"},
+           "bwd_err": berr,
+           "cpu_baseline": {"value": round(gflops, 4), "unit": "GFLOP/s", "cores": 1, "kind": "port",
+                            "sample": f"full workload, {args.steps} steps (serial C++ restatement of ref_factorize! "
+                                      "+ ref_solve!; the Julia reference cannot run here)"},
+           "e2e": {"value": round(gflops, 4), "unit": "GFLOP/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(out), flush=True)
+
+
+def main():
+    args = parse()
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        run_reference(args, rank)
+        return
+    import torch
+
+    from sdsb200 import capi
+    from sdsb200 import matrices as M
+    from sdsb200._native import numeric_lib
+    from sdsb200.solver import DirectSolver
+
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as tdist
+
+        tdist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+        dist = tdist
+    lib = numeric_lib()
+    A, b = workload(args.grid)
+    n = A.shape[0]
+    forms = {
+        "mixed": dict(factor_precision="fp32", ir_n_steps=20, ir_tol=2e-15),
+        "fp64": dict(factor_precision="fp64", ir_n_steps=0),
+    }
+    solvers = {}
+    for name, kw in forms.items():
+        ds = DirectSolver(A, "SPD", reordering_alg="nd", max_nrhs=NRHS, **kw)
+        ds.execute("analysis")
+        solvers[name] = ds
+    S = solvers["fp64"].symbolic
+    flops = S.flops + 4.0 * S.nnz_stored * NRHS
+    stream = torch.cuda.current_stream()
+    st = C.c_void_p(stream.cuda_stream)
+    Bd = torch.from_numpy(np.ascontiguousarray(b.T)).cuda()        # column-major n x nrhs
+    Xd = torch.empty_like(Bd)
+    info = np.zeros(1, np.int64)
+
+    def step(ds):
+        o = ds._opts()
+        rc = lib.sdsb200_factor(ds._plan, C.c_void_p(ds.nzval.data_ptr()), None, C.byref(o), info.ctypes.data, st)
+        assert rc == 0, lib.sdsb200_last_error()
+        launches = lib.sdsb200_plan_stat(ds._plan, b"launches_done")
+        steps = C.c_int32(0)
+        rc = lib.sdsb200_solve(ds._plan, C.c_void_p(Xd.data_ptr()), n, C.c_void_p(Bd.data_ptr()), n, NRHS,
+                               C.c_void_p(ds.nzval.data_ptr()), C.byref(o), C.byref(steps), st)
+        assert rc == 0, lib.sdsb200_last_error()
+        launches += lib.sdsb200_plan_stat(ds._plan, b"launches_done")
+        return int(steps.value), int(launches)
+
+    results = {}
+    for name, ds in solvers.items():
+        for _ in range(args.warmup):
+            step(ds)
+        torch.cuda.synchronize()
+        if dist:
+            dist.barrier()
+        launches = 0
+        irsteps = []
+        with ClockSampler(local) as clk:
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            torch.cuda.synchronize()
+            e0.record()
+            for _ in range(args.steps):
+                s_, l_ = step(ds)
+                irsteps.append(s_)
+                launches += l_
+            e1.record()
+            torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1) / args.steps
+        if dist:
+            t = torch.tensor([ms], device="cuda")
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            ms = float(t.item())
+        x = Xd.t().cpu().numpy()
+        berr = M.scaled_backward_error(A, x, b)
+        results[name] = dict(ms=ms, gflops=world * flops / (ms / 1e3) / 1e9, berr=berr, ir_steps=irsteps[-1],
+                             launches=launches, clocks=clk.summary(), x=x, info=int(info[0]))
+    # error of the mixed solution against the FP64 one, per right-hand side
+    xf, xm = results["fp64"]["x"], results["mixed"]["x"]
+    err_vs_fp64 = [float(np.abs(xm[:, r] - xf[:, r]).max() / np.abs(xf[:, r]).max()) for r in range(NRHS)]
+
+    # profiling pass (separate from the timed region): per-kind kernel time of one step
+    prof = {}
+    for name, ds in solvers.items():
+        lib.sdsb200_set_profiling(ds._plan, 1)
+        step(ds)
+        torch.cuda.synchronize()
+        kinds = {}
+        for k in ("small", "assemble", "panel", "gemm", "pivot", "scale", "stats", "fwd", "bwd", "diag", "permute",
+                  "residual"):
+            ms_k = lib.sdsb200_plan_stat(ds._plan, f"prof_ms:{k}".encode())
+            if ms_k > 0:
+                kinds[k] = dict(ms=ms_k, flops=lib.sdsb200_plan_stat(ds._plan, f"prof_flops:{k}".encode()),
+                                bytes=lib.sdsb200_plan_stat(ds._plan, f"prof_bytes:{k}".encode()),
+                                launches=int(lib.sdsb200_plan_stat(ds._plan, f"prof_launches:{k}".encode())))
+        lib.sdsb200_set_profiling(ds._plan, 0)
+        prof[name] = kinds
+
+    peaks, peak_kind = measured_peaks()
+    fp64_peak = measured_gemm_peak(torch, torch.float64)
+    fp32_peak = measured_gemm_peak(torch, torch.float32)
+    head = "mixed"
+    kinds = prof[head]
+    dom = max(kinds, key=lambda k: kinds[k]["ms"]) if kinds else None
+    roofline = None
+    if dom is not None:
+        d = kinds[dom]
+        per_launch_ms = d["ms"] / max(d["launches"], 1)
+        if dom in ("gemm", "panel", "pivot"):
+            peak = fp32_peak if head == "mixed" else fp64_peak
+            ach = d["flops"] / (d["ms"] / 1e3) / 1e12
+            roofline = {"kernel": dom, "bound": "fp32" if head == "mixed" else "fp64", "achieved": round(ach, 3),
+                        "peak": round(peak, 3), "unit": "TFLOP/s", "frac": round(ach / peak, 4),
+                        "peak_source": "cuBLAS GEMM of the same precision measured in this run (no tensor cores)",
+                        "traffic": None, "launches": d["launches"], "ms_per_launch": round(per_launch_ms, 4)}
+        else:
+            peak = float(peaks.get("hbm_gbs", 6650.0))
+            ach = d["bytes"] / (d["ms"] / 1e3) / 1e9
+            roofline = {"kernel": dom, "bound": "hbm", "achieved": round(ach, 2), "peak": peak, "unit": "GB/s",
+                        "frac": round(ach / peak, 4), "peak_source": f"MEASURED_PEAKS.json hbm_gbs ({peak_kind})",
+                        "traffic": None, "launches": d["launches"], "ms_per_launch": round(per_launch_ms, 4)}
+
+    # end to end through the public API with host buffers
+    e2e = None
+    if not args.no_e2e:
+        ds = solvers[head]
+        nz_host = torch.from_numpy(np.ascontiguousarray(A.data)).pin_memory()
+        b_host = torch.from_numpy(np.ascontiguousarray(b)).pin_memory()
+        x_host = torch.empty_like(b_host).pin_memory()
+        for _ in range(args.warmup):
+            ds.nzval.copy_(nz_host, non_blocking=True)
+            ds.execute("factorization")
+            x_host.copy_(ds.execute("solve", None, b_host.cuda(non_blocking=True)), non_blocking=True)
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(args.steps):
+            ds.nzval.copy_(nz_host, non_blocking=True)
+            ds.execute("factorization")
+            x_host.copy_(ds.execute("solve", None, b_host.cuda(non_blocking=True)), non_blocking=True)
+        e1.record()
+        torch.cuda.synchronize()
+        ms_e2e = e0.elapsed_time(e1) / args.steps
+        berr_e2e = M.scaled_backward_error(A, x_host.numpy(), b)
+        e2e = {"value": round(world * flops / (ms_e2e / 1e3) / 1e9, 3), "unit": "GFLOP/s",
+               "ms_per_step": round(ms_e2e, 3), "h2d_bytes_per_step": int(8 * (A.nnz + n * NRHS)),
+               "d2h_bytes_per_step": int(8 * n * NRHS), "bwd_err": berr_e2e}
+
+    cpu = None
+    if rank == 0 and not args.no_cpu_baseline:
+        from oracle.oracle import Oracle
+
+        O = Oracle(S)
+        t0 = time.perf_counter()
+        O.factorize(A.data, "SPD")
+        O.solve(b)
+        dt = time.perf_counter() - t0
+        cpu = {"value": round(flops / dt / 1e9, 4), "unit": "GFLOP/s", "cores": 1, "kind": "port",
+               "sample": "one full factor+solve of the same workload by the serial CPU oracle "
+                         f"({dt:.1f} s)"}
+
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank != 0:
+        return
+    r = results[head]
+    out = {
+        "metric": METRIC, "value": round(r["gflops"], 3), "unit": "GFLOP/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": round(r["ms"], 3), "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32 factor + f64 refinement", "data": "synthetic",
+        "config": {"workload": f"lap3d_{args.grid} SPD Cholesky factor+solve to bwd err <= 1e-12, nested dissection, "
+                               f"{NRHS} RHS (form: mixed FP32 factor + FP64 IR)",
+                   "n": int(n), "nnz": int(A.nnz), "nnz_stored": int(S.nnz_stored), "flops_per_step": flops,
+                   "factor_flops": S.flops, "parallelism": f"replicas x{world}",
+                   "l2": "inputs larger than L2 (factor %.0f MB)" % (S.nnz_stored * 4 / 1e6)},
+        "bwd_err": r["berr"], "ir_steps": r["ir_steps"], "err_vs_fp64_per_rhs": err_vs_fp64,
+        "fp64": {"ms_per_step": round(results["fp64"]["ms"], 3), "value": round(results["fp64"]["gflops"], 3),
+                 "bwd_err": results["fp64"]["berr"], "unit": "GFLOP/s",
+                 "speedup_mixed_vs_fp64": round(results["fp64"]["ms"] / r["ms"], 3)},
+        "gpu_launches": int(r["launches"]),
+        "clocks": r["clocks"],
+        "roofline": roofline,
+        "kernel_profile": {k: {kk: {"ms": round(v["ms"], 4), "launches": v["launches"]} for kk, v in prof[k].items()}
+                           for k in prof},
+        "peaks": {"fp64_gemm_tflops_measured": round(fp64_peak, 2), "fp32_gemm_tflops_measured": round(fp32_peak, 2),
+                  "hbm_gbs": peaks.get("hbm_gbs"), "source": peak_kind},
+        "cpu_baseline": cpu,
+        "e2e": e2e,
+    }
+    ok = r["berr"] <= BERR_TARGET and results["fp64"]["berr"] <= BERR_TARGET
+    out["valid"] = bool(ok)
+    print(json.dumps(out), flush=True)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,163 @@
+/*
+ * sdsb200.h -- C ABI of the B200 (sm_100a) numeric phase: factorization,
+ * refactorization and solve of a multifrontal sparse direct solver, as a
+ * drop-in for SparseDirectSolver.jl's numeric and solve phases.
+ *
+ * Replaced reference interfaces (SparseDirectSolver.jl):
+ *   sdsb200_plan_create   allocate_numeric src/numeric/storage.jl:205-256 and
+ *                         allocate_solve src/solve/sweeps.jl:164-173, called from
+ *                         _symbolic! src/solver.jl:641-642
+ *   sdsb200_factor        _numeric_phase_cholesky!/ldlt!/lu! src/solver.jl:728-741,
+ *                         i.e. factorize_cholesky! src/numeric/factorize.jl:327-360,
+ *                         factorize_ldlt! src/numeric/ldlt.jl:1447-1475,
+ *                         factorize_lu! src/numeric/lu.jl:543-555, with the info
+ *                         read of _numeric_info! factorize.jl:383-415
+ *   sdsb200_solve         _solve_phase! src/solver.jl:810-871 (permute_rhs!,
+ *                         forward_sweep!, diagonal_sweep!, backward_sweep!,
+ *                         unpermute_solution!) and _refine_phase! :902-926 (refine!
+ *                         src/solve/refinement.jl:359-397)
+ *   sdsb200_get_*         the data-parameter outputs of getparam src/solver.jl:1090-1141
+ *                         (info, inertia, npivots, pivot_stats, perm_row, diag) and
+ *                         host_numeric src/numeric/extract.jl:13-21
+ *   sdsb200_set_members   set_members! src/numeric/storage.jl:290-306 (ubatch_index)
+ *   sdsb200_set_interrupt user_host_interrupt polling src/logging.jl:60-63
+ *   sdsb200_plan_destroy  release of the Numeric / SolveWorkspace buffers
+ *
+ * Conventions: all Symbolic maps are HOST arrays, 1-based exactly as the
+ * reference's `Symbolic` holds them (src/symbolic/maps.jl:62-95), of int32 or
+ * int64 (`index_width`). Value arrays (nzval, B, X) are DEVICE pointers unless
+ * the name starts with h_. Streams are cudaStream_t passed as void*.
+ * The plan owns every device buffer; nzval/B/X are borrowed for the call.
+ * Every call is asynchronous on `stream` except the documented host reads.
+ */
+#ifndef SDSB200_H
+#define SDSB200_H
+#include <stddef.h>
+#include <stdint.h>
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* return codes (mapped to the reference's errors, src/errors.jl:18-60) */
+#define SDSB200_OK 0
+#define SDSB200_INVALID_VALUE 1   /* InvalidValueError */
+#define SDSB200_NOT_SUPPORTED 2   /* NotSupportedError */
+#define SDSB200_PHASE_ORDER 3     /* FactorizationError (solve before factorization) */
+#define SDSB200_INTERRUPTED 4     /* InterruptedError (user_host_interrupt) */
+#define SDSB200_CUDA_ERROR 5
+#define SDSB200_ALLOC_FAILED 6
+#define SDSB200_TIMEOUT 7         /* a bounded device wait gave up */
+
+/* structures (reference Structure enum): "G", "S", "SPD" */
+#define SDSB200_STRUCTURE_G 0
+#define SDSB200_STRUCTURE_S 1
+#define SDSB200_STRUCTURE_SPD 3
+
+/* factor precision of the plan */
+#define SDSB200_PRECISION_FP64 0  /* the plain form: every operation in FP64 */
+#define SDSB200_PRECISION_FP32 1  /* FP32 factor, assembly and Schur updates; FP64 residual + refinement */
+
+/* The reference's Symbolic maps (DEVICE_MAPS, src/symbolic/maps.jl:16-18) as host arrays.
+ * Arrays are int32_t* when index_width == 4, int64_t* when 8. */
+typedef struct sdsb200_symbolic {
+    int64_t n, nnz, ns;
+    int32_t index_width;      /* 4 or 8 */
+    int32_t structure;        /* SDSB200_STRUCTURE_* */
+    const void* perm;         /* n: column k of the factor is original column perm[k] */
+    const void* super_ptr;    /* ns + 1 */
+    const void* snparent;     /* ns (0 = root) */
+    const void* rowptr;       /* ns + 1: solve gather lists */
+    const void* rowval;
+    const void* front_ptr;    /* ns + 1: panel_ptr of the Layout */
+    const void* child_ptr;    /* ns + 1 */
+    const void* child_list;
+    const void* relind_ptr;   /* ns + 1 */
+    const void* relind;
+    const void* amap;         /* nnz (signed: negative = conjugate / U^T structure, 0 = ignored) */
+    const void* amap_ptr;     /* ns + 1 */
+    const void* amap_src;
+    /* residual map of the full matrix M (FullPatternMap, src/symbolic/pattern.jl:215-290); NULL disables
+     * iterative refinement. full_rowptr: n + 1; full_colval / full_srcptr: nnz(M) (+1); full_src. */
+    const void* full_rowptr;
+    const void* full_colval;
+    const void* full_srcptr;
+    const void* full_src;
+    int64_t full_nnz;         /* entries of M */
+    int64_t full_nsrc;        /* length of full_src */
+} sdsb200_symbolic;
+
+typedef struct sdsb200_plan_options {
+    int32_t nbatch;           /* uniform batch members (ubatch_size); 1 for a single matrix */
+    int32_t precision;        /* SDSB200_PRECISION_* */
+    int32_t max_nrhs;         /* largest nrhs of a solve (workspace) */
+    int32_t reserved;
+} sdsb200_plan_options;
+
+/* The Options fields the numeric and solve phases read (src/options.jl:155-223). */
+typedef struct sdsb200_opts {
+    int32_t pivot_type;        /* PivotType: 0 auto, 1 none, 4 diagonal, 5 local block, 6 Bunch-Kaufman */
+    int32_t pivot_epsilon_alg; /* 0 default/algo2 (static), 1 algo1 (scaled by max|a_ij|) */
+    double pivot_threshold;    /* 0.01 */
+    double pivot_epsilon;      /* < 0: default_pivot_epsilon (1e-13 FP64, 1e-5 FP32) */
+    int32_t ir_n_steps;        /* iterative refinement steps (0: none) */
+    int32_t ir_mode;           /* 0 plain */
+    double ir_tol;             /* > 0: stop when max_k ||r_k|| / ||b_k|| <= ir_tol (one host read per step) */
+    int32_t solve_mode;        /* 0 A, 1 A^T, 2 A^H (= A^T for real) */
+    int32_t deterministic_mode;/* the solve is always deterministic (owner-pull); accepted for parity */
+} sdsb200_opts;
+
+typedef struct sdsb200_plan sdsb200_plan;
+
+void sdsb200_default_opts(sdsb200_opts* o);
+
+/* Build the plan: copy the maps to the device, derive the level schedule and
+ * the extend-add maps, allocate every buffer of the numeric and solve phases
+ * (the only allocations). Synchronous. */
+int sdsb200_plan_create(sdsb200_plan** plan, const sdsb200_symbolic* sym, const sdsb200_plan_options* popts,
+                        void* stream);
+int sdsb200_plan_destroy(sdsb200_plan* plan);
+
+/* Factorize (or refactorize: same call) the values nzval (device, nnz * nbatch, member-major).
+ * h_psign: pivot_sign (n int8 on the host, indexed by original row) or NULL.
+ * h_info (nbatch, may be NULL): original column (1-based) of the first failed pivot per member,
+ * 0 = success; written at the phase's one host synchronization. */
+int sdsb200_factor(sdsb200_plan* plan, const double* nzval, const int8_t* h_psign, const sdsb200_opts* opts,
+                   int64_t* h_info, void* stream);
+
+/* Solve op(A) X = B for nrhs right-hand sides per member (device, column-major, leading dimension
+ * ldb/ldx >= n, members one after the other at stride ld * nrhs). X == B is allowed without refinement.
+ * nzval (device) is needed when opts->ir_n_steps > 0. h_ir_steps (may be NULL): refinement steps run. */
+int sdsb200_solve(sdsb200_plan* plan, double* X, int64_t ldx, const double* B, int64_t ldb, int32_t nrhs,
+                  const double* nzval, const sdsb200_opts* opts, int32_t* h_ir_steps, void* stream);
+
+/* Outputs (synchronous host copies; member = 0-based batch member). */
+int sdsb200_get_stats(sdsb200_plan* plan, int32_t member, int64_t* h_stats /* 6 * ns */,
+                      int64_t* h_totals /* 6 */);
+int sdsb200_get_pivots(sdsb200_plan* plan, int32_t member, int32_t* h_piv /* n, 1-based */,
+                       int8_t* h_kind /* n */, double* h_d /* 2n */);
+/* factor panels of one member as FP64 (factor_len each; h_ufactor: "G" only, may be NULL) */
+int sdsb200_get_factor(sdsb200_plan* plan, int32_t member, double* h_factor, double* h_ufactor);
+
+/* ubatch_index / ubatch_mask: restrict later calls to h_members (0-based), nact of them; nact < 0 = all. */
+int sdsb200_set_members(sdsb200_plan* plan, const int32_t* h_members, int32_t nact);
+
+/* user_host_interrupt: a host flag polled between launch groups (factorization) and refinement steps. */
+int sdsb200_set_interrupt(sdsb200_plan* plan, const volatile int32_t* h_flag);
+
+/* Profiling mode (on != 0): CUDA events around every launch of the following factor and solve
+ * calls, accumulated per kernel kind (resets the totals). Costs one event record per launch. */
+int sdsb200_set_profiling(sdsb200_plan* plan, int32_t on);
+
+/* Plan facts: "ns", "nlevels", "factor_len", "cb_len", "launches_factor", "launches_solve",
+ * "launches_done" (kernel launches of the last factor or solve call), "device_bytes", "flops";
+ * with profiling, "prof_ms:<kind>", "prof_flops:<kind>", "prof_bytes:<kind>", "prof_launches:<kind>"
+ * for kinds small assemble panel gemm pivot scale stats fwd bwd diag permute residual.
+ * Returns -1 for an unknown name. */
+double sdsb200_plan_stat(const sdsb200_plan* plan, const char* name);
+
+const char* sdsb200_last_error(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

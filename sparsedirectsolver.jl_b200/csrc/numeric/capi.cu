@@ -1,0 +1,602 @@
+// C ABI of the numeric phase (include/sdsb200.h): plan creation, the
+// factorization program interpreter, the solve with iterative refinement and
+// the output accessors.
+#include <cuda_runtime.h>
+#include <math.h>
+#include <stdint.h>
+#include <string.h>
+
+#include <algorithm>
+#include <string>
+#include <vector>
+
+#include "common.cuh"
+#include "kernels.cuh"
+#include "plan.h"
+#include "solve.cuh"
+
+using namespace sds;
+
+namespace {
+
+thread_local std::string g_error;
+
+int fail(int code, const std::string& msg) {
+    g_error = msg;
+    return code;
+}
+
+int cuda_fail(cudaError_t e, const char* where) {
+    return fail(SDSB200_CUDA_ERROR, std::string(where) + ": " + cudaGetErrorString(e));
+}
+
+#define CK(expr, where)                              \
+    do {                                             \
+        cudaError_t _e = (expr);                     \
+        if (_e != cudaSuccess) return cuda_fail(_e, where); \
+    } while (0)
+
+double default_eps(const Plan* P) { return P->elsize == 8 ? 1e-13 : 1e-5; }
+
+bool interrupted(const Plan* P) { return P->interrupt && *P->interrupt != 0; }
+
+// profiling mode: an event pair around every launch, resolved at the end of the phase
+void prof_begin(Plan* P, cudaStream_t st) {
+    P->launches_done++;
+    if (!P->profile) return;
+    size_t k = P->prof_next;
+    while (P->events.size() < k + 2) {
+        cudaEvent_t e;
+        cudaEventCreate(&e);
+        P->events.push_back(e);
+    }
+    cudaEventRecord(P->events[k], st);
+}
+
+void prof_end(Plan* P, cudaStream_t st, int kind, double flops, double bytes) {
+    if (!P->profile) return;
+    size_t k = P->prof_next;
+    cudaEventRecord(P->events[k + 1], st);
+    P->pending.push_back({kind, {flops, bytes}});
+    P->prof_next += 2;
+}
+
+void prof_resolve(Plan* P) {
+    if (!P->profile) return;
+    for (size_t q = 0; q < P->pending.size(); ++q) {
+        float ms = 0;
+        cudaEventSynchronize(P->events[2 * q + 1]);
+        cudaEventElapsedTime(&ms, P->events[2 * q], P->events[2 * q + 1]);
+        ProfAcc& a = P->prof[P->pending[q].first];
+        a.ms += ms;
+        a.flops += P->pending[q].second.first;
+        a.bytes += P->pending[q].second.second;
+        a.launches++;
+    }
+    P->pending.clear();
+    P->prof_next = 0;
+}
+
+const char* const PROF_NAMES[PK_COUNT] = {"small", "assemble", "panel", "gemm", "pivot", "scale",
+                                          "stats", "fwd", "bwd", "diag", "permute", "residual"};
+
+int prof_kind_of(LaunchKind k) {
+    switch (k) {
+        case L_SMALL: return PK_SMALL;
+        case L_ASSEMBLE: return PK_ASSEMBLE;
+        case L_CHOL_PANEL: return PK_PANEL;
+        case L_GEMM: return PK_GEMM;
+        case L_PIVOT_FRONT: return PK_PIVOT;
+        case L_SCALE: return PK_SCALE;
+        default: return PK_STATS;
+    }
+}
+
+__global__ void absmax_kernel(const double* x, int64_t len, double* out) {
+    __shared__ double red[256];
+    double m = 0.0;
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < len; i += (int64_t)gridDim.x * blockDim.x)
+        m = fmax(m, fabs(x[i]));
+    red[threadIdx.x] = m;
+    __syncthreads();
+    for (int h = 128; h > 0; h >>= 1) {
+        if (threadIdx.x < h) red[threadIdx.x] = fmax(red[threadIdx.x], red[threadIdx.x + h]);
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+        // max of nonnegative doubles: their bit patterns order the same way
+        atomicMax(reinterpret_cast<unsigned long long*>(out), (unsigned long long)__double_as_longlong(red[0]));
+    }
+}
+
+template <typename T>
+int run_factor(Plan* P, const double* nzval, double eps, double u, int pivot, int lu_pivot, cudaStream_t st) {
+    const int nm = P->nact;
+    const int32_t* members = P->all_members ? nullptr : P->d_members;
+    T* factor = static_cast<T*>(P->d_factor);
+    T* ufactor = static_cast<T*>(P->d_ufactor);
+    T* cb = static_cast<T*>(P->d_cb);
+    T* work = static_cast<T*>(P->d_work);
+    int last_level = -1;
+    for (const ProgLaunch& L : P->prog) {
+        if (L.kind != L_STATS && L.level != last_level) {
+            if (interrupted(P)) return fail(SDSB200_INTERRUPTED, "interrupted by user_host_interrupt");
+            last_level = L.level;
+        }
+        cudaError_t e = cudaSuccess;
+        prof_begin(P, st);
+        switch (L.kind) {
+            case L_SMALL: {
+                SmallArgs<T> a{};
+                a.maps = P->maps;
+                a.list = P->d_lists + L.list;
+                a.members = members;
+                a.nzval = nzval;
+                a.factor = factor; a.ufactor = ufactor; a.cb = cb;
+                a.d = P->d_d; a.piv = P->d_piv; a.kind = P->d_kind; a.stats = P->d_stats; a.finfo = P->d_finfo;
+                a.psign = P->d_psign;
+                a.nnz = P->nnz; a.factor_len = P->factor_len; a.cb_len = P->cb_len; a.n = P->n;
+                a.ns = (int32_t)P->ns; a.pivot = pivot; a.lu_pivot = lu_pivot; a.u = u; a.eps = eps;
+                e = launch_small<T>(P->structure, a, L.count, nm, L.cls, st);
+                break;
+            }
+            case L_ASSEMBLE: {
+                LargeAsmArgs<T> a{};
+                a.maps = P->maps;
+                a.tasks = P->d_coltasks + L.list;
+                a.count = L.count;
+                a.members = members;
+                a.nzval = nzval;
+                a.factor = factor; a.ufactor = ufactor; a.cb = cb;
+                a.nnz = P->nnz; a.factor_len = P->factor_len; a.cb_len = P->cb_len;
+                e = launch_assemble_large<T>(P->structure, a, nm, st);
+                break;
+            }
+            case L_CHOL_PANEL: {
+                CholPanelArgs<T> a{};
+                a.fronts = P->d_fronts;
+                a.tasks = P->d_ptasks + L.list;
+                a.count = L.count;
+                a.members = members;
+                a.factor = factor; a.finfo = P->d_finfo; a.stats = P->d_stats;
+                a.factor_len = P->factor_len; a.ns = (int32_t)P->ns; a.kb = L.cls; a.eps = eps;
+                e = launch_chol_panel<T>(a, L.nb, nm, st);
+                break;
+            }
+            case L_GEMM: {
+                GemmArgs<T> a{};
+                a.tiles = P->d_tiles + L.list;
+                a.count = L.count;
+                a.members = members;
+                auto buf = [&](BufId b, int64_t& stride) -> T* {
+                    switch (b) {
+                        case BUF_FACTOR: stride = P->factor_len; return factor;
+                        case BUF_UFACTOR: stride = P->factor_len; return ufactor;
+                        case BUF_CB: stride = P->cb_len; return cb;
+                        default: stride = P->work_len; return work;
+                    }
+                };
+                a.abuf = buf(L.abuf, a.astride);
+                a.bbuf = buf(L.bbuf, a.bstride);
+                a.cbuf = buf(L.cbuf, a.cstride);
+                a.finfo = P->d_finfo;
+                a.ns = (int32_t)P->ns;
+                e = launch_gemm<T>(a, nm, st);
+                break;
+            }
+            case L_PIVOT_FRONT: {
+                LargePivotArgs<T> a{};
+                a.fronts = P->d_fronts;
+                a.list = P->d_lists + L.list;
+                a.count = L.count;
+                a.members = members;
+                a.factor = factor; a.ufactor = ufactor;
+                a.scratch = P->d_scratch; a.scr_off = P->d_scr_off + L.cls; a.scr_len = P->scr_len;
+                a.d = P->d_d; a.piv = P->d_piv; a.kind = P->d_kind; a.stats = P->d_stats; a.finfo = P->d_finfo;
+                a.psign = P->d_psign; a.perm = P->d_perm0;
+                a.factor_len = P->factor_len; a.n = P->n; a.ns = (int32_t)P->ns;
+                a.pivot = pivot; a.lu_pivot = lu_pivot; a.u = u; a.eps = eps;
+                e = launch_large_pivot<T>(P->structure, a, nm, st);
+                break;
+            }
+            case L_SCALE: {
+                ScaleArgs<T> a{};
+                a.fronts = P->d_fronts;
+                a.list = P->d_lists + L.list;
+                a.count = L.count;
+                a.woff = P->d_woff + L.cls;
+                a.members = members;
+                a.factor = factor; a.d = P->d_d; a.kind = P->d_kind; a.work = work;
+                a.factor_len = P->factor_len; a.n = P->n; a.work_len = P->work_len;
+                e = launch_scale_ld_front<T>(P->structure, a, L.maxw, nm, st);
+                break;
+            }
+            case L_STATS: {
+                StatsArgs a{};
+                a.stats = P->d_stats;
+                a.members = members;
+                a.super_ptr0 = P->d_super0;
+                a.perm0 = P->d_perm0;
+                a.totals = P->d_totals;
+                a.info = P->d_info;
+                a.ns = (int32_t)P->ns;
+                e = launch_stats(a, nm, st);
+                break;
+            }
+        }
+        prof_end(P, st, prof_kind_of(L.kind), L.flops * nm, L.bytes * nm);
+        if (e != cudaSuccess) return cuda_fail(e, "factorization launch");
+    }
+    return SDSB200_OK;
+}
+
+template <typename T>
+int run_sweeps(Plan* P, int nrhs, bool transpose, cudaStream_t st) {
+    const int nm = P->nact;
+    const int32_t* members = P->all_members ? nullptr : P->d_members;
+    const bool gen = P->structure == STRUCT_G, ldl = P->structure == STRUCT_S;
+    const T* factor = static_cast<const T*>(P->d_factor);
+    const T* ufactor = static_cast<const T*>(P->d_ufactor);
+    SweepArgs<T> a{};
+    a.fronts = P->d_fronts;
+    a.members = members;
+    a.Y = P->d_Y;
+    a.U = P->d_U;
+    a.uoff = P->d_uoff;
+    a.child_list = P->maps.child_list;
+    a.relind = P->maps.relind;
+    a.rowval = P->maps.rowval;
+    a.n = P->n; a.factor_len = P->factor_len; a.ulen = P->ulen;
+    a.nrhs = nrhs;
+    a.unit = P->structure != STRUCT_SPD;
+    // forward: L (reordered) or, for A^T of "G", U^T (no reordering)
+    a.fac = (gen && transpose) ? ufactor : factor;
+    a.piv = P->d_piv;
+    a.reorder = ldl || (gen && !transpose);
+    for (int L = 0; L < P->nlevels; ++L) {
+        a.list = P->d_level_lists + P->level_list_off[L];
+        a.count = (int32_t)P->level_fronts[L].size();
+        prof_begin(P, st);
+        cudaError_t e = launch_sweep<T>(true, a, nm, P->level_maxw[L], st);
+        prof_end(P, st, PK_FWD, 2.0 * P->level_panel_entries[L] * nrhs * nm,
+                 (double)sizeof(T) * P->level_panel_entries[L] * nm);
+        if (e != cudaSuccess) return cuda_fail(e, "forward sweep");
+    }
+    if (P->structure != STRUCT_SPD) {
+        DiagArgs d{};
+        d.members = members; d.d = P->d_d; d.kind = P->d_kind; d.Y = P->d_Y; d.n = P->n; d.nrhs = nrhs; d.two = ldl;
+        prof_begin(P, st);
+        cudaError_t e = launch_diag(d, nm, st);
+        prof_end(P, st, PK_DIAG, (double)P->n * nrhs * nm, 24.0 * P->n * nrhs * nm);
+        if (e != cudaSuccess) return cuda_fail(e, "diagonal sweep");
+    }
+    a.fac = (gen && !transpose) ? ufactor : factor;
+    a.reorder = ldl || (gen && transpose);
+    for (int L = P->nlevels - 1; L >= 0; --L) {
+        a.list = P->d_level_lists + P->level_list_off[L];
+        a.count = (int32_t)P->level_fronts[L].size();
+        prof_begin(P, st);
+        cudaError_t e = launch_sweep<T>(false, a, nm, P->level_maxw[L], st);
+        prof_end(P, st, PK_BWD, 2.0 * P->level_panel_entries[L] * nrhs * nm,
+                 (double)sizeof(T) * P->level_panel_entries[L] * nm);
+        if (e != cudaSuccess) return cuda_fail(e, "backward sweep");
+    }
+    return SDSB200_OK;
+}
+
+int sweeps(Plan* P, int nrhs, bool transpose, cudaStream_t st) {
+    return P->elsize == 8 ? run_sweeps<double>(P, nrhs, transpose, st) : run_sweeps<float>(P, nrhs, transpose, st);
+}
+
+int permute(Plan* P, int mode, const double* in, int64_t ldin, double* out, int64_t ldout, int nrhs, cudaStream_t st) {
+    PermArgs a{};
+    a.members = P->all_members ? nullptr : P->d_members;
+    a.perm = P->d_perm0;
+    a.Y = P->d_Y;
+    a.in = in; a.out = out; a.ldin = ldin; a.ldout = ldout;
+    a.n = P->n; a.nrhs = nrhs; a.mode = mode;
+    prof_begin(P, st);
+    cudaError_t e = launch_permute(a, P->nact, st);
+    prof_end(P, st, PK_PERMUTE, 0.0, (mode == 2 ? 32.0 : 20.0) * P->n * nrhs * P->nact);
+    return e == cudaSuccess ? SDSB200_OK : cuda_fail(e, "permute");
+}
+
+}  // namespace
+
+extern "C" {
+
+const char* sdsb200_last_error(void) { return g_error.c_str(); }
+
+void sdsb200_default_opts(sdsb200_opts* o) {
+    memset(o, 0, sizeof(*o));
+    o->pivot_type = PIVOT_AUTO;
+    o->pivot_epsilon_alg = 0;
+    o->pivot_threshold = 0.01;
+    o->pivot_epsilon = -1.0;
+    o->ir_n_steps = 0;
+    o->ir_mode = 0;
+    o->ir_tol = 0.0;
+    o->solve_mode = 0;
+    o->deterministic_mode = 0;
+}
+
+int sdsb200_plan_create(sdsb200_plan** plan, const sdsb200_symbolic* sym, const sdsb200_plan_options* popts,
+                        void* stream) {
+    if (!plan) return fail(SDSB200_INVALID_VALUE, "plan is NULL");
+    *plan = nullptr;
+    try {
+        Plan* P = build_plan(sym, popts, (cudaStream_t)stream);
+        *plan = reinterpret_cast<sdsb200_plan*>(P);
+        return SDSB200_OK;
+    } catch (const PlanError& e) {
+        return fail(e.code, e.msg);
+    } catch (const std::exception& e) {
+        return fail(SDSB200_ALLOC_FAILED, e.what());
+    }
+}
+
+int sdsb200_plan_destroy(sdsb200_plan* plan) {
+    free_plan(reinterpret_cast<Plan*>(plan));
+    return SDSB200_OK;
+}
+
+int sdsb200_factor(sdsb200_plan* plan, const double* nzval, const int8_t* h_psign, const sdsb200_opts* opts,
+                   int64_t* h_info, void* stream) {
+    Plan* P = reinterpret_cast<Plan*>(plan);
+    if (!P) return fail(SDSB200_INVALID_VALUE, "plan is NULL");
+    if (!nzval && P->nnz > 0) return fail(SDSB200_INVALID_VALUE, "nzval is NULL");
+    sdsb200_opts o;
+    if (opts) o = *opts;
+    else sdsb200_default_opts(&o);
+    cudaStream_t st = (cudaStream_t)stream;
+    int pivot = o.pivot_type;
+    int lu_pivot = 1;
+    if (P->structure == STRUCT_S) {
+        if (pivot == PIVOT_AUTO || pivot == PIVOT_LOCAL || pivot == PIVOT_BK) pivot = PIVOT_BK;
+        else if (pivot != PIVOT_NONE && pivot != PIVOT_DIAGONAL)
+            return fail(SDSB200_NOT_SUPPORTED, "pivot_type is not supported by LDLT");
+    } else if (P->structure == STRUCT_G) {
+        if (pivot == PIVOT_NONE || pivot == PIVOT_DIAGONAL) lu_pivot = 0;
+        else if (pivot != PIVOT_AUTO && pivot != PIVOT_LOCAL && pivot != PIVOT_BK)
+            return fail(SDSB200_NOT_SUPPORTED, "pivot_type is not supported by LU");
+    }
+    double eps = o.pivot_epsilon < 0 ? default_eps(P) : o.pivot_epsilon;
+    if (!(o.pivot_threshold >= 0) || !std::isfinite(o.pivot_threshold))
+        return fail(SDSB200_INVALID_VALUE, "pivot_threshold must be finite and nonnegative");
+    if (o.pivot_epsilon_alg == 1 && P->structure != STRUCT_SPD) {
+        // scaled epsilon: eps * max |a_ij| of the first active member (one host read)
+        int m0 = P->all_members ? 0 : -1;
+        std::vector<int32_t> mem(1, 0);
+        if (m0 < 0) CK(cudaMemcpyAsync(mem.data(), P->d_members, sizeof(int32_t), cudaMemcpyDeviceToHost, st), "members");
+        CK(cudaMemsetAsync(P->d_amax, 0, sizeof(double), st), "memset");
+        absmax_kernel<<<256, 256, 0, st>>>(nzval + (int64_t)(m0 < 0 ? mem[0] : 0) * P->nnz, P->nnz, P->d_amax);
+        double amax = 0;
+        CK(cudaMemcpyAsync(&amax, P->d_amax, sizeof(double), cudaMemcpyDeviceToHost, st), "amax");
+        CK(cudaStreamSynchronize(st), "amax sync");
+        if (amax > 0) eps *= amax;
+    }
+    if (h_psign) CK(cudaMemcpyAsync(P->d_psign, h_psign, P->n, cudaMemcpyHostToDevice, st), "psign");
+    else CK(cudaMemsetAsync(P->d_psign, 0, P->n, st), "psign");
+    P->launches_done = 0;
+    CK(cudaMemsetAsync(P->d_finfo, 0, sizeof(int32_t) * P->ns * P->nbatch, st), "memset finfo");
+    CK(cudaMemsetAsync(P->d_stats, 0, sizeof(int64_t) * NSTAT * P->ns * P->nbatch, st), "memset stats");
+    P->factored = false;
+    int rc = P->elsize == 8 ? run_factor<double>(P, nzval, eps, o.pivot_threshold, pivot, lu_pivot, st)
+                            : run_factor<float>(P, nzval, eps, o.pivot_threshold, pivot, lu_pivot, st);
+    if (rc != SDSB200_OK) return rc;
+    // the phase's one host synchronization: the reduced info of the active members
+    CK(cudaMemcpyAsync(P->h_info_pinned, P->d_info, sizeof(int64_t) * P->nact, cudaMemcpyDeviceToHost, st), "info");
+    CK(cudaStreamSynchronize(st), "factorization");
+    prof_resolve(P);
+    if (h_info) {
+        if (P->all_members) {
+            for (int k = 0; k < P->nact; ++k) h_info[k] = P->h_info_pinned[k];
+        } else {
+            std::vector<int32_t> mem(P->nact);
+            CK(cudaMemcpy(mem.data(), P->d_members, sizeof(int32_t) * P->nact, cudaMemcpyDeviceToHost), "members");
+            for (int k = 0; k < P->nact; ++k) h_info[mem[k]] = P->h_info_pinned[k];
+        }
+    }
+    P->factored = true;
+    return SDSB200_OK;
+}
+
+int sdsb200_solve(sdsb200_plan* plan, double* X, int64_t ldx, const double* B, int64_t ldb, int32_t nrhs,
+                  const double* nzval, const sdsb200_opts* opts, int32_t* h_ir_steps, void* stream) {
+    Plan* P = reinterpret_cast<Plan*>(plan);
+    if (!P) return fail(SDSB200_INVALID_VALUE, "plan is NULL");
+    if (!P->factored) return fail(SDSB200_PHASE_ORDER, "solve before a successful factorization");
+    if (nrhs < 1 || nrhs > P->max_nrhs) return fail(SDSB200_INVALID_VALUE, "nrhs outside 1:max_nrhs of the plan");
+    if (ldx < P->n || ldb < P->n) return fail(SDSB200_INVALID_VALUE, "leading dimension smaller than n");
+    if (!X || !B) return fail(SDSB200_INVALID_VALUE, "X or B is NULL");
+    sdsb200_opts o;
+    if (opts) o = *opts;
+    else sdsb200_default_opts(&o);
+    if (o.solve_mode < 0 || o.solve_mode > 2) return fail(SDSB200_INVALID_VALUE, "solve_mode must be 0, 1 or 2");
+    if (o.ir_n_steps < 0) return fail(SDSB200_INVALID_VALUE, "ir_n_steps must be nonnegative");
+    const bool transpose = P->structure == STRUCT_G && o.solve_mode != 0;
+    if (o.ir_n_steps > 0) {
+        if (!P->has_full) return fail(SDSB200_INVALID_VALUE, "refinement needs the residual map of the plan");
+        if (!nzval) return fail(SDSB200_INVALID_VALUE, "refinement needs nzval");
+        if ((const double*)X == B) return fail(SDSB200_INVALID_VALUE, "X and B must differ with refinement");
+    }
+    cudaStream_t st = (cudaStream_t)stream;
+    // max shared memory of a sweep CTA: the widest front times nrhs (chunks of right-hand sides beyond it)
+    int maxw = 1;
+    for (int w : P->level_maxw) maxw = std::max(maxw, w);
+    if ((size_t)maxw * nrhs * sizeof(double) > 200 * 1024)
+        return fail(SDSB200_NOT_SUPPORTED, "front too wide for this many right-hand sides in one solve");
+    P->launches_done = 0;
+    int rc = permute(P, 0, B, ldb, nullptr, 0, nrhs, st);
+    if (rc) return rc;
+    rc = sweeps(P, nrhs, transpose, st);
+    if (rc) return rc;
+    rc = permute(P, 1, nullptr, 0, X, ldx, nrhs, st);
+    if (rc) return rc;
+    int steps = 0;
+    for (int it = 0; it < o.ir_n_steps; ++it) {
+        if (interrupted(P)) {
+            if (h_ir_steps) *h_ir_steps = steps;
+            return fail(SDSB200_INTERRUPTED, "interrupted by user_host_interrupt");
+        }
+        ResidualArgs r{};
+        r.members = P->all_members ? nullptr : P->d_members;
+        if (transpose) {
+            r.rowptr = P->d_fullT_rowptr; r.colval = P->d_fullT_colval; r.srcptr = P->d_fullT_srcptr; r.src = P->d_fullT_src;
+        } else {
+            r.rowptr = P->d_full_rowptr; r.colval = P->d_full_colval; r.srcptr = P->d_full_srcptr; r.src = P->d_full_src;
+        }
+        r.nzval = nzval; r.X = X; r.B = B; r.R = P->d_R;
+        r.n = P->n; r.nnz = P->nnz; r.ldx = ldx; r.ldb = ldb; r.nrhs = nrhs;
+        prof_begin(P, st);
+        cudaError_t re = launch_residual(r, P->nact, st);
+        prof_end(P, st, PK_RESIDUAL, 2.0 * P->full_nnz * nrhs * P->nact,
+                 (16.0 * P->full_nnz + 8.0 * P->full_nsrc + 8.0 * P->full_nsrc) * P->nact + 24.0 * P->n * nrhs * P->nact);
+        CK(re, "residual");
+        if (o.ir_tol > 0) {
+            NormArgs na{};
+            na.members = r.members; na.R = P->d_R; na.B = B; na.out = P->d_norms; na.n = P->n; na.ldb = ldb; na.nrhs = nrhs;
+            int ncols = nrhs * P->nact;
+            CK(launch_norms(na, ncols, st), "norms");
+            CK(cudaMemcpyAsync(P->h_norms, P->d_norms, sizeof(double) * 2 * ncols, cudaMemcpyDeviceToHost, st), "norms");
+            CK(cudaStreamSynchronize(st), "norms sync");
+            double rel = 0;
+            for (int c = 0; c < ncols; ++c) {
+                double rr = sqrt(P->h_norms[2 * c]), bb = sqrt(P->h_norms[2 * c + 1]);
+                rel = std::max(rel, bb > 0 ? rr / bb : rr);
+            }
+            if (rel <= o.ir_tol) break;
+        }
+        rc = permute(P, 0, P->d_R, P->n, nullptr, 0, nrhs, st);
+        if (rc) return rc;
+        rc = sweeps(P, nrhs, transpose, st);
+        if (rc) return rc;
+        rc = permute(P, 2, nullptr, 0, X, ldx, nrhs, st);
+        if (rc) return rc;
+        steps++;
+    }
+    if (h_ir_steps) *h_ir_steps = steps;
+    CK(cudaGetLastError(), "solve");
+    if (P->profile) {
+        CK(cudaStreamSynchronize(st), "solve");
+        prof_resolve(P);
+    }
+    return SDSB200_OK;
+}
+
+int sdsb200_get_stats(sdsb200_plan* plan, int32_t member, int64_t* h_stats, int64_t* h_totals) {
+    Plan* P = reinterpret_cast<Plan*>(plan);
+    if (!P || member < 0 || member >= P->nbatch) return fail(SDSB200_INVALID_VALUE, "bad plan or member");
+    if (h_stats)
+        CK(cudaMemcpy(h_stats, P->d_stats + (int64_t)member * NSTAT * P->ns, sizeof(int64_t) * NSTAT * P->ns,
+                      cudaMemcpyDeviceToHost), "stats");
+    if (h_totals) {
+        // totals are reduced per active slot; recompute from the statistics for any member
+        std::vector<int64_t> st(NSTAT * P->ns);
+        CK(cudaMemcpy(st.data(), P->d_stats + (int64_t)member * NSTAT * P->ns, sizeof(int64_t) * NSTAT * P->ns,
+                      cudaMemcpyDeviceToHost), "stats");
+        for (int q = 0; q < NSTAT; ++q) h_totals[q] = 0;
+        for (int64_t s = 0; s < P->ns; ++s) {
+            for (int q = 0; q < NSTAT - 1; ++q) h_totals[q] += st[s * NSTAT + q];
+            if (st[s * NSTAT + ST_INFO] != 0) h_totals[ST_INFO] += 1;
+        }
+    }
+    return SDSB200_OK;
+}
+
+int sdsb200_get_pivots(sdsb200_plan* plan, int32_t member, int32_t* h_piv, int8_t* h_kind, double* h_d) {
+    Plan* P = reinterpret_cast<Plan*>(plan);
+    if (!P || member < 0 || member >= P->nbatch) return fail(SDSB200_INVALID_VALUE, "bad plan or member");
+    if (h_piv) CK(cudaMemcpy(h_piv, P->d_piv + (int64_t)member * P->n, sizeof(int32_t) * P->n, cudaMemcpyDeviceToHost), "piv");
+    if (h_kind) CK(cudaMemcpy(h_kind, P->d_kind + (int64_t)member * P->n, P->n, cudaMemcpyDeviceToHost), "kind");
+    if (h_d) CK(cudaMemcpy(h_d, P->d_d + (int64_t)member * 2 * P->n, sizeof(double) * 2 * P->n, cudaMemcpyDeviceToHost), "d");
+    return SDSB200_OK;
+}
+
+int sdsb200_get_factor(sdsb200_plan* plan, int32_t member, double* h_factor, double* h_ufactor) {
+    Plan* P = reinterpret_cast<Plan*>(plan);
+    if (!P || member < 0 || member >= P->nbatch) return fail(SDSB200_INVALID_VALUE, "bad plan or member");
+    const int64_t len = P->factor_len;
+    auto get = [&](const void* src, double* dst) -> int {
+        if (!dst) return SDSB200_OK;
+        if (P->elsize == 8) {
+            CK(cudaMemcpy(dst, static_cast<const double*>(src) + member * len, sizeof(double) * len, cudaMemcpyDeviceToHost), "factor");
+        } else {
+            std::vector<float> tmp(len);
+            CK(cudaMemcpy(tmp.data(), static_cast<const float*>(src) + member * len, sizeof(float) * len, cudaMemcpyDeviceToHost), "factor");
+            for (int64_t k = 0; k < len; ++k) dst[k] = tmp[k];
+        }
+        return SDSB200_OK;
+    };
+    int rc = get(P->d_factor, h_factor);
+    if (rc) return rc;
+    if (h_ufactor) {
+        if (!P->d_ufactor) return fail(SDSB200_INVALID_VALUE, "no U^T panels: structure is not G");
+        return get(P->d_ufactor, h_ufactor);
+    }
+    return SDSB200_OK;
+}
+
+int sdsb200_set_members(sdsb200_plan* plan, const int32_t* h_members, int32_t nact) {
+    Plan* P = reinterpret_cast<Plan*>(plan);
+    if (!P) return fail(SDSB200_INVALID_VALUE, "plan is NULL");
+    if (nact < 0 || !h_members) {
+        P->all_members = true;
+        P->nact = P->nbatch;
+        return SDSB200_OK;
+    }
+    if (nact == 0 || nact > P->nbatch) return fail(SDSB200_INVALID_VALUE, "nact outside 1:nbatch");
+    std::vector<char> seen(P->nbatch, 0);
+    for (int k = 0; k < nact; ++k) {
+        if (h_members[k] < 0 || h_members[k] >= P->nbatch || seen[h_members[k]])
+            return fail(SDSB200_INVALID_VALUE, "members must be distinct indices in 0:nbatch-1");
+        seen[h_members[k]] = 1;
+    }
+    CK(cudaMemcpy(P->d_members, h_members, sizeof(int32_t) * nact, cudaMemcpyHostToDevice), "members");
+    P->all_members = false;
+    P->nact = nact;
+    return SDSB200_OK;
+}
+
+int sdsb200_set_profiling(sdsb200_plan* plan, int32_t on) {
+    Plan* P = reinterpret_cast<Plan*>(plan);
+    if (!P) return fail(SDSB200_INVALID_VALUE, "plan is NULL");
+    P->profile = on != 0;
+    for (int k = 0; k < PK_COUNT; ++k) P->prof[k] = ProfAcc();
+    P->pending.clear();
+    P->prof_next = 0;
+    return SDSB200_OK;
+}
+
+int sdsb200_set_interrupt(sdsb200_plan* plan, const volatile int32_t* h_flag) {
+    Plan* P = reinterpret_cast<Plan*>(plan);
+    if (!P) return fail(SDSB200_INVALID_VALUE, "plan is NULL");
+    P->interrupt = h_flag;
+    return SDSB200_OK;
+}
+
+double sdsb200_plan_stat(const sdsb200_plan* plan, const char* name) {
+    const Plan* P = reinterpret_cast<const Plan*>(plan);
+    if (!P || !name) return -1;
+    std::string nm(name);
+    if (nm == "ns") return (double)P->ns;
+    if (nm == "nlevels") return P->nlevels;
+    if (nm == "factor_len") return (double)P->factor_len;
+    if (nm == "cb_len") return (double)P->cb_len;
+    if (nm == "launches_factor") return P->launches_factor;
+    if (nm == "launches_solve") return 2.0 * P->nlevels + 3;
+    if (nm == "device_bytes") return (double)P->device_bytes;
+    if (nm == "flops") return P->flops;
+    if (nm == "elsize") return P->elsize;
+    if (nm == "launches_done") return (double)P->launches_done;
+    for (int k = 0; k < PK_COUNT; ++k) {
+        std::string kn(PROF_NAMES[k]);
+        if (nm == "prof_ms:" + kn) return P->prof[k].ms;
+        if (nm == "prof_flops:" + kn) return P->prof[k].flops;
+        if (nm == "prof_bytes:" + kn) return P->prof[k].bytes;
+        if (nm == "prof_launches:" + kn) return (double)P->prof[k].launches;
+    }
+    return -1;
+}
+
+}  // extern "C"

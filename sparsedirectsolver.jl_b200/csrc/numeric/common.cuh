@@ -1,0 +1,86 @@
+// Shared definitions of the B200 numeric phase (device descriptors, plan layout).
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <string>
+#include <vector>
+
+#include "../../../include/sdsb200.h"
+
+namespace sds {
+
+constexpr int NSTAT = 6;  // per-front statistics: npos, nneg, nzero, nperturbed, n2x2, info
+enum { ST_NPOS = 0, ST_NNEG, ST_NZERO, ST_NPERT, ST_N2X2, ST_INFO };
+enum { KIND_1X1 = 1, KIND_2X2_FIRST = 2, KIND_2X2_SECOND = 3, KIND_PERTURBED = 4 };
+enum { PIVOT_AUTO = 0, PIVOT_NONE = 1, PIVOT_DIAGONAL = 4, PIVOT_LOCAL = 5, PIVOT_BK = 6 };
+enum { STRUCT_G = 0, STRUCT_S = 1, STRUCT_SPD = 3 };
+
+// Device descriptor of one front (supernode). All offsets 0-based, per batch member.
+struct DFront {
+    int64_t panel;     // offset of the f x w panel (column-major, ld f) in the factor buffer
+    int64_t cb;        // offset of the m x m contribution block (column-major, ld m) in the CB arena; -1 none
+    int32_t f, w, c0;  // rows, fully-summed columns, first factor column
+    int32_t parent;    // -1 for a root
+    int32_t ch_begin, ch_end;  // children in child_list
+    int32_t ri_begin;  // this front's relind (its rows w..f-1 among the parent's), length f - w
+    int32_t am_begin, am_end;  // assembly entries (am_src/am_loc)
+    int32_t row_begin;         // rows in rowval (f entries; its own columns first)
+    int32_t amcol_begin;       // per-column start of the assembly entries: amcol[amcol_begin + j], j <= w
+    int32_t eacol_begin;       // column-owner extend-add lists of a large front: eacol[eacol_begin + p], p <= f
+    int32_t level;
+    int32_t pad;
+};
+
+// Column task of the large-front assembly: (front, parent index p); one warp each.
+struct ColTask {
+    int32_t front, p;
+};
+
+// One tile of a grouped GEMM  C -= A * B^T  (all column-major). Offsets point at the
+// tile's first element: A at its first row, B at its first row (= the tile's first
+// column of C), C at (row0, col0). Entry (r, c) of the tile is written only when
+// r + diag >= c (diag = row0 - col0 for the lower triangle; a large value disables the mask).
+struct GemmTile {
+    int64_t a, b, c;
+    int32_t lda, ldb, ldc;
+    int32_t m, n, k;     // valid rows and columns of this tile (<= tile size), inner dimension
+    int32_t diag;
+    int32_t front;       // status check: the tile is skipped when this front failed (-1: none)
+};
+
+// A launch of the factorization program.
+enum LaunchKind : int32_t {
+    L_SMALL = 1,       // fused small fronts (one CTA per front, front in shared memory)
+    L_ASSEMBLE,        // column-task assembly of large fronts
+    L_CHOL_PANEL,      // large Cholesky: diagonal block + trsm of one column block
+    L_GEMM,            // grouped GEMM tiles
+    L_PIVOT_FRONT,     // large LDLT / LU: cooperative pivoting over the panel
+    L_STATS,           // statistics reduction
+    L_SCALE,           // W = L21 D of large LDLT / LU fronts
+};
+
+struct Launch {
+    LaunchKind kind;
+    int32_t level;
+    int32_t count;       // fronts / tasks / tiles
+    int32_t cls;         // small-front class (max rows), or column-block start (panel)
+    int64_t list;        // offset of the front/task/tile list in its device array
+    int32_t nb;          // panel block width
+    int32_t smem;        // dynamic shared memory bytes
+};
+
+struct DeviceMaps {
+    const DFront* fronts;
+    const int32_t* child_list;
+    const int32_t* relind;
+    const int32_t* am_src;
+    const int32_t* am_loc;   // (loc + 1) for L entries, -(loc + 1) for U^T entries; loc within the panel
+    const int32_t* amcol;    // per-column starts of the assembly entries
+    const int32_t* ea;       // extend-add pairs (child, t) packed as 2 int32
+    const int32_t* eacol;    // per parent index starts into ea
+    const int32_t* rowval;   // 0-based
+    const int32_t* perm;     // 0-based
+};
+
+}  // namespace sds

@@ -1,0 +1,299 @@
+// Dense kernels of the large fronts (the reference's regime C: cuSOLVER potrf,
+// cuBLAS trsm/syrk/gemm through src/dense/interface.jl and the KA fallbacks of
+// src/dense/fallback/, replaced here by hand-written kernels).
+//
+// * chol_panel_kernel: one column block of a large Cholesky front, in two
+//   launches: the diagonal mode factors the nb x nb diagonal block in shared
+//   memory and writes it back; the trsm mode solves one tile of rows below
+//   with it (trsm R, L, T). The static pivot clamp and the failure rule are
+//   the ones of the fused kernels.
+// * gemm_nt_kernel: grouped C -= A B^T over a list of tiles (Schur updates of
+//   the fully-summed columns and of the contribution block; "lower" tiles write
+//   only on or below the diagonal).
+// * large_pivot_kernel: LDLT / LU fronts beyond shared memory: one CTA runs the
+//   reference's in-front steps (front_factor.cuh) on the global panels.
+// * scale_ld_kernel: W = L21 D for the contribution-block update of those fronts.
+#include <cuda_runtime.h>
+#include <math.h>
+#include <stdint.h>
+
+#include "common.cuh"
+#include "front_factor.cuh"
+#include "kernels.cuh"
+
+namespace sds {
+
+template <typename T, int NB>
+__global__ void __launch_bounds__(PANEL_ROWS) chol_panel_kernel(CholPanelArgs<T> A) {
+    __shared__ T L[NB][NB + 1];
+    __shared__ int s_status;
+    const PanelTask task = A.tasks[blockIdx.x];
+    const int member = A.members ? A.members[blockIdx.y] : blockIdx.y;
+    const int s = task.front;
+    const DFront fd = A.fronts[s];
+    int32_t* finfo = A.finfo + (int64_t)member * A.ns;
+    if (finfo[s] != 0) return;
+    const int f = fd.f, w = fd.w, kb = A.kb;
+    if (kb >= w) return;
+    const int nbb = min(NB, w - kb);
+    T* P = A.factor + (int64_t)member * A.factor_len + fd.panel;
+    const int tid = threadIdx.x;
+    for (int q = tid; q < NB * NB; q += blockDim.x) {
+        int i = q % NB, j = q / NB;
+        L[i][j] = (i < nbb && j < nbb && i >= j) ? P[(kb + i) + (int64_t)(kb + j) * f] : T(0);
+    }
+    if (tid == 0) s_status = 0;
+    __syncthreads();
+    if (task.row0 < 0) {
+        // diagonal mode: factor the block, write it back, record the status and the statistics
+        const double eps = A.eps;
+        for (int j = 0; j < nbb; ++j) {
+            double ajj = (double)L[j][j];
+            bool ok = ajj > eps || (eps > 0 && ajj >= 0);
+            if (!ok) {
+                if (tid == 0) s_status = j + 1;
+                break;
+            }
+            double djj = sqrt(fmax(ajj, eps));
+            T inv = T(1.0 / djj);
+            __syncthreads();
+            for (int i = j + 1 + tid; i < nbb; i += blockDim.x) L[i][j] *= inv;
+            if (tid == 0) L[j][j] = T(djj);
+            __syncthreads();
+            const int r = nbb - j - 1;
+            for (int q = tid; q < r * r; q += blockDim.x) {
+                int i = j + 1 + q % r, l = j + 1 + q / r;
+                if (i >= l) L[i][l] -= L[i][j] * L[l][j];
+            }
+            __syncthreads();
+        }
+        __syncthreads();
+        const int status = s_status;
+        for (int q = tid; q < nbb * nbb; q += blockDim.x) {
+            int i = q % nbb, j = q / nbb;
+            P[(kb + i) + (int64_t)(kb + j) * f] = i >= j ? L[i][j] : T(0);
+        }
+        if (tid == 0) {
+            int64_t* S = A.stats + ((int64_t)member * A.ns + s) * NSTAT;
+            if (status) {
+                finfo[s] = kb + status;
+                S[ST_NPOS] = kb + status - 1;
+                S[ST_INFO] = kb + status;
+            } else if (kb + nbb == w) {
+                S[ST_NPOS] = w;
+                S[ST_INFO] = 0;
+            }
+        }
+        return;
+    }
+    // trsm mode: the block was factored by the previous launch; solve X L11^T = B for this row tile
+    const int r = task.row0 + tid;
+    if (r >= f) return;
+    T x[NB];
+#pragma unroll
+    for (int j = 0; j < NB; ++j) x[j] = j < nbb ? P[r + (int64_t)(kb + j) * f] : T(0);
+#pragma unroll
+    for (int j = 0; j < NB; ++j) {
+        if (j < nbb) {
+            T acc = x[j];
+#pragma unroll
+            for (int l = 0; l < j; ++l) acc -= x[l] * L[j][l];
+            x[j] = acc / L[j][j];
+        }
+    }
+#pragma unroll
+    for (int j = 0; j < NB; ++j)
+        if (j < nbb) P[r + (int64_t)(kb + j) * f] = x[j];
+}
+
+template <typename T>
+cudaError_t launch_chol_panel(const CholPanelArgs<T>& a, int nb, int nmembers, cudaStream_t st) {
+    dim3 grid(a.count, nmembers);
+    if (nb == 32) chol_panel_kernel<T, 32><<<grid, PANEL_ROWS, 0, st>>>(a);
+    else chol_panel_kernel<T, 64><<<grid, PANEL_ROWS, 0, st>>>(a);
+    return cudaGetLastError();
+}
+
+template cudaError_t launch_chol_panel<double>(const CholPanelArgs<double>&, int, int, cudaStream_t);
+template cudaError_t launch_chol_panel<float>(const CholPanelArgs<float>&, int, int, cudaStream_t);
+
+// ---------------------------------------------------------------------------
+// Grouped C -= A B^T, 64 x 64 tiles, 256 threads, 4 x 4 outputs per thread.
+template <typename T>
+__global__ void __launch_bounds__(256) gemm_nt_kernel(GemmArgs<T> A) {
+    constexpr int BM = GEMM_BM, BN = GEMM_BN, BK = 16;
+    __shared__ T As[BK][BM + 1];
+    __shared__ T Bs[BK][BN + 1];
+    const GemmTile t = A.tiles[blockIdx.x];
+    const int member = A.members ? A.members[blockIdx.y] : blockIdx.y;
+    if (A.finfo && t.front >= 0 && A.finfo[(int64_t)member * A.ns + t.front] != 0) return;
+    const T* Ab = A.abuf + (int64_t)member * A.astride + t.a;
+    const T* Bb = A.bbuf + (int64_t)member * A.bstride + t.b;
+    T* Cb = A.cbuf + (int64_t)member * A.cstride + t.c;
+    const int tid = threadIdx.x, tx = tid & 15, ty = tid >> 4;
+    T acc[4][4];
+#pragma unroll
+    for (int i = 0; i < 4; ++i)
+#pragma unroll
+        for (int j = 0; j < 4; ++j) acc[i][j] = T(0);
+    const int M = t.m, N = t.n, K = t.k;
+    for (int k0 = 0; k0 < K; k0 += BK) {
+#pragma unroll
+        for (int q = 0; q < (BM * BK) / 256; ++q) {
+            int e = tid + 256 * q, r = e % BM, kk = e / BM;
+            As[kk][r] = (r < M && k0 + kk < K) ? Ab[r + (int64_t)(k0 + kk) * t.lda] : T(0);
+        }
+#pragma unroll
+        for (int q = 0; q < (BN * BK) / 256; ++q) {
+            int e = tid + 256 * q, r = e % BN, kk = e / BN;
+            Bs[kk][r] = (r < N && k0 + kk < K) ? Bb[r + (int64_t)(k0 + kk) * t.ldb] : T(0);
+        }
+        __syncthreads();
+#pragma unroll
+        for (int kk = 0; kk < BK; ++kk) {
+            T a[4], b[4];
+#pragma unroll
+            for (int i = 0; i < 4; ++i) a[i] = As[kk][tx + 16 * i];
+#pragma unroll
+            for (int j = 0; j < 4; ++j) b[j] = Bs[kk][ty + 16 * j];
+#pragma unroll
+            for (int i = 0; i < 4; ++i)
+#pragma unroll
+                for (int j = 0; j < 4; ++j) acc[i][j] += a[i] * b[j];
+        }
+        __syncthreads();
+    }
+#pragma unroll
+    for (int i = 0; i < 4; ++i)
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+            int r = tx + 16 * i, c = ty + 16 * j;
+            if (r < M && c < N && r + t.diag >= c) Cb[r + (int64_t)c * t.ldc] -= acc[i][j];
+        }
+}
+
+template <typename T>
+cudaError_t launch_gemm(const GemmArgs<T>& a, int nmembers, cudaStream_t st) {
+    if (a.count == 0) return cudaSuccess;
+    dim3 grid(a.count, nmembers);
+    gemm_nt_kernel<T><<<grid, 256, 0, st>>>(a);
+    return cudaGetLastError();
+}
+
+template cudaError_t launch_gemm<double>(const GemmArgs<double>&, int, cudaStream_t);
+template cudaError_t launch_gemm<float>(const GemmArgs<float>&, int, cudaStream_t);
+
+// ---------------------------------------------------------------------------
+template <typename T, int STRUCT>
+__global__ void __launch_bounds__(1024) large_pivot_kernel(LargePivotArgs<T> A) {
+    const int s = A.list[blockIdx.x];
+    const int member = A.members ? A.members[blockIdx.y] : blockIdx.y;
+    const DFront fd = A.fronts[s];
+    const int f = fd.f, w = fd.w;
+    constexpr bool GEN = STRUCT == STRUCT_G;
+    T* P = A.factor + (int64_t)member * A.factor_len + fd.panel;
+    T* U = GEN ? A.ufactor + (int64_t)member * A.factor_len + fd.panel : nullptr;
+    double* scr = A.scratch + (int64_t)member * A.scr_len + A.scr_off[blockIdx.x];
+    FrontScratch sc;
+    sc.lvec = scr;
+    sc.dd = scr + 2 * f;
+    sc.ee = sc.dd + w;
+    sc.lp = reinterpret_cast<int*>(sc.ee + w);
+    sc.ctl = sc.lp + w;
+    sc.kd = reinterpret_cast<signed char*>(sc.ctl + 16);
+    const int tid = threadIdx.x, nt = blockDim.x;
+    if (STRUCT == STRUCT_S) {
+        for (int q = tid; q < w * w; q += nt) {
+            int i = q % w, j = q / w;
+            if (i > j) P[j + (int64_t)i * f] = P[i + (int64_t)j * f];
+        }
+        __syncthreads();
+    }
+    int64_t st[NSTAT] = {0, 0, 0, 0, 0, 0};
+    GlobalStore<T, GEN> store{P, U, f, w};
+    if (STRUCT == STRUCT_S)
+        ldlt_front_steps<T>(store, sc, f, w, A.pivot, A.u, A.eps, A.psign, A.perm, fd.c0, st);
+    else
+        lu_front_steps<T>(store, sc, f, w, A.lu_pivot != 0, A.u, A.eps, st);
+    __syncthreads();
+    // unit diagonals, zero strict upper part of the diagonal block (LDLT used it as workspace)
+    for (int q = tid; q < w * w; q += nt) {
+        int i = q % w, j = q / w;
+        if (i == j) {
+            P[i + (int64_t)j * f] = T(1);
+            if (GEN) U[i + (int64_t)j * f] = T(1);
+        } else if (i < j && !GEN) {
+            P[i + (int64_t)j * f] = T(0);
+        }
+    }
+    const int64_t n = A.n;
+    for (int q = tid; q < w; q += nt) {
+        const int64_t g = fd.c0 + q;
+        A.piv[member * n + g] = fd.c0 + sc.lp[q] + 1;
+        A.kind[member * n + g] = sc.kd[q];
+        A.d[member * 2 * n + g] = sc.dd[q];
+        A.d[member * 2 * n + n + g] = STRUCT == STRUCT_S ? sc.ee[q] : 0.0;
+    }
+    if (tid == 0) {
+        int64_t* S = A.stats + ((int64_t)member * A.ns + s) * NSTAT;
+        for (int q = 0; q < NSTAT; ++q) S[q] = st[q];
+        A.finfo[(int64_t)member * A.ns + s] = (int32_t)st[ST_INFO];
+    }
+}
+
+template <typename T>
+cudaError_t launch_large_pivot(int structure, const LargePivotArgs<T>& a, int nmembers, cudaStream_t st) {
+    if (a.count == 0) return cudaSuccess;
+    dim3 grid(a.count, nmembers);
+    if (structure == STRUCT_S) large_pivot_kernel<T, STRUCT_S><<<grid, 1024, 0, st>>>(a);
+    else large_pivot_kernel<T, STRUCT_G><<<grid, 1024, 0, st>>>(a);
+    return cudaGetLastError();
+}
+
+template cudaError_t launch_large_pivot<double>(int, const LargePivotArgs<double>&, int, cudaStream_t);
+template cudaError_t launch_large_pivot<float>(int, const LargePivotArgs<float>&, int, cudaStream_t);
+
+// W = L21 D (1x1 and 2x2 blocks of D), rows w..f-1 of the panel, into work (m x w, ld m)
+template <typename T, int STRUCT>
+__global__ void scale_ld_kernel(ScaleArgs<T> A) {
+    const int s = A.list[blockIdx.x];
+    const int member = A.members ? A.members[blockIdx.z] : blockIdx.z;
+    const DFront fd = A.fronts[s];
+    const int f = fd.f, w = fd.w, m = f - w;
+    const int q = blockIdx.y;  // column
+    if (q >= w) return;
+    const T* P = A.factor + (int64_t)member * A.factor_len + fd.panel;
+    const double* d = A.d + (int64_t)member * 2 * A.n;
+    const int8_t* kd = A.kind + (int64_t)member * A.n;
+    T* W = A.work + (int64_t)member * A.work_len + A.woff[blockIdx.x];
+    const int g = fd.c0 + q;
+    const int kq = kd[g];
+    for (int i = threadIdx.x; i < m; i += blockDim.x) {
+        double v;
+        double x = (double)P[w + i + (int64_t)q * f];
+        if (STRUCT == STRUCT_S && kq == KIND_2X2_FIRST) {
+            double x2 = (double)P[w + i + (int64_t)(q + 1) * f];
+            v = x * d[g] + x2 * d[A.n + g];
+        } else if (STRUCT == STRUCT_S && kq == KIND_2X2_SECOND) {
+            double x1 = (double)P[w + i + (int64_t)(q - 1) * f];
+            v = x1 * d[A.n + g - 1] + x * d[g];
+        } else {
+            v = x * d[g];
+        }
+        W[i + (int64_t)q * m] = T(v);
+    }
+}
+
+template <typename T>
+cudaError_t launch_scale_ld_front(int structure, const ScaleArgs<T>& a, int maxw, int nmembers, cudaStream_t st) {
+    if (a.count == 0) return cudaSuccess;
+    dim3 grid(a.count, maxw, nmembers);
+    if (structure == STRUCT_S) scale_ld_kernel<T, STRUCT_S><<<grid, 128, 0, st>>>(a);
+    else scale_ld_kernel<T, STRUCT_G><<<grid, 128, 0, st>>>(a);
+    return cudaGetLastError();
+}
+
+template cudaError_t launch_scale_ld_front<double>(int, const ScaleArgs<double>&, int, int, cudaStream_t);
+template cudaError_t launch_scale_ld_front<float>(int, const ScaleArgs<float>&, int, int, cudaStream_t);
+
+}  // namespace sds

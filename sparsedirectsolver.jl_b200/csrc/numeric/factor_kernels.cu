@@ -1,0 +1,357 @@
+// Fused per-front kernels of the numeric phase.
+//
+// small_front_kernel: one CTA per front of one level, the whole f x f front in
+// shared memory: zero, assemble A, extend-add the children's contribution
+// blocks (children in child_list order, so every sum has a fixed order and the
+// result is bitwise reproducible), the dense partial factorization of the w
+// fully-summed columns (Cholesky; Bunch-Kaufman LDLT; threshold-pivoting LU),
+// the Schur update of the contribution block, and the write-out of the panel,
+// D, pivots, statistics and contribution block. It replaces the reference's
+// regime A/B kernels (subtree_cholesky_kernel! src/numeric/subtree.jl:274-316,
+// front_cholesky_kernel! src/numeric/front.jl:154-206, front_ldlt_kernel!
+// src/numeric/ldlt.jl:992-1111, subtree_ldlt_kernel! :1133-1228,
+// front_lu_kernel! src/numeric/lu.jl:264-330, subtree_lu_kernel! :424-493) with
+// one level-batched design; the in-front arithmetic follows the CPU reference
+// (src/reference/*.jl) step by step.
+//
+// assemble_large_kernel: column-owner assembly of the fronts too large for
+// shared memory: one warp per (front, parent index p) zeroes the storage it
+// owns, adds the entries of A of that column and pulls every child's
+// contribution in child order. No atomics.
+#include <cuda_runtime.h>
+#include <math.h>
+#include <stdint.h>
+
+#include "common.cuh"
+#include "kernels.cuh"
+#include "front_factor.cuh"
+#include "pivot.cuh"
+
+namespace sds {
+
+template <typename T, int STRUCT>
+__global__ void __launch_bounds__(256) small_front_kernel(SmallArgs<T> A) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const int s = A.list[blockIdx.x];
+    const int member = A.members ? A.members[blockIdx.y] : blockIdx.y;
+    const DFront fd = A.maps.fronts[s];
+    const int f = fd.f, w = fd.w, m = f - w;
+    const int ld = f | 1;
+    T* F = reinterpret_cast<T*>(smem_raw);
+    size_t off = ((size_t)ld * f * sizeof(T) + 15) & ~size_t(15);
+    double* dd = reinterpret_cast<double*>(smem_raw + off);  // w
+    double* ee = dd + w;                                     // w
+    double* lvec = ee + w;                                   // 2 f (multipliers)
+    int* lp = reinterpret_cast<int*>(lvec + 2 * f);          // w
+    int* ri = lp + w;                                        // relind of the current child (<= f)
+    int* ctl = ri + f;                                       // control words
+    signed char* kd = reinterpret_cast<signed char*>(ctl + 16);
+
+    const int tid = threadIdx.x, nt = blockDim.x, lane = tid & 31, warp = tid >> 5, nwarps = nt >> 5;
+    const double* nz = A.nzval + (int64_t)member * A.nnz;
+    T* factor = A.factor + (int64_t)member * A.factor_len;
+    T* cbar = A.cb + (int64_t)member * A.cb_len;
+
+    for (int q = tid; q < ld * f; q += nt) F[q] = T(0);
+    if (tid < 16) ctl[tid] = 0;
+    __syncthreads();
+    // assembly of A: each run of equal destinations is summed by one thread, in entry order
+    for (int k = fd.am_begin + tid; k < fd.am_end; k += nt) {
+        int code = A.maps.am_loc[k];
+        if (k > fd.am_begin && A.maps.am_loc[k - 1] == code) continue;
+        T acc = T(0);
+        for (int q = k; q < fd.am_end && A.maps.am_loc[q] == code; ++q) acc += T(nz[A.maps.am_src[q]]);
+        int loc = (code > 0 ? code : -code) - 1;
+        int i = loc % f, j = loc / f;
+        if (code > 0) F[i + j * ld] += acc;
+        else F[j + i * ld] += acc;
+    }
+    __syncthreads();
+    // extend-add, children in order
+    for (int q = fd.ch_begin; q < fd.ch_end; ++q) {
+        const int c = A.maps.child_list[q];
+        const DFront cd = A.maps.fronts[c];
+        const int mc = cd.f - cd.w;
+        if (mc <= 0 || cd.cb < 0) continue;
+        for (int t = tid; t < mc; t += nt) ri[t] = A.maps.relind[cd.ri_begin + t];
+        __syncthreads();
+        const T* C = cbar + cd.cb;
+        for (int jj = warp; jj < mc; jj += nwarps) {
+            const int pj = ri[jj];
+            for (int ii = (STRUCT == STRUCT_G ? 0 : jj) + lane; ii < mc; ii += 32)
+                F[ri[ii] + pj * ld] += C[ii + (int64_t)jj * mc];
+        }
+        __syncthreads();
+    }
+    if (STRUCT == STRUCT_S) {  // the pivoting reads both triangles of the fully-summed block
+        for (int q = tid; q < w * w; q += nt) {
+            int i = q % w, j = q / w;
+            if (i > j) F[j + i * ld] = F[i + j * ld];
+        }
+        __syncthreads();
+    }
+    int64_t st[NSTAT] = {0, 0, 0, 0, 0, 0};
+    int status = 0;
+    const double eps = A.eps;
+
+    if (STRUCT == STRUCT_SPD) {
+        for (int j = 0; j < w; ++j) {
+            double ajj = (double)F[j + j * ld];
+            bool ok = ajj > eps || (eps > 0 && ajj >= 0);
+            if (!ok) { status = j + 1; break; }
+            double djj = sqrt(fmax(ajj, eps));
+            T inv = T(1.0 / djj);
+            __syncthreads();
+            for (int i = j + 1 + tid; i < f; i += nt) F[i + j * ld] *= inv;
+            if (tid == 0) F[j + j * ld] = T(djj);
+            __syncthreads();
+            for (int l = j + 1 + warp; l < f; l += nwarps) {
+                const T flj = F[l + j * ld];
+                for (int i = l + lane; i < f; i += 32) F[i + l * ld] -= F[i + j * ld] * flj;
+            }
+            __syncthreads();
+        }
+        st[ST_NPOS] = status ? status - 1 : w;
+        st[ST_INFO] = status;
+    } else if (STRUCT == STRUCT_S) {
+        SmemStore<T> store{F, ld, f, w};
+        FrontScratch sc{lvec, dd, ee, lp, kd, ctl};
+        ldlt_front_steps<T>(store, sc, f, w, A.pivot, A.u, eps, A.psign, A.maps.perm, fd.c0, st);
+        // F22 -= (L21 D) L21^T, lower triangle, kk in order (ldlt.jl:184-191)
+        for (int jj = warp; jj < m; jj += nwarps)
+            for (int ii = jj + lane; ii < m; ii += 32) {
+                T acc = F[w + ii + (w + jj) * ld];
+                int q = 0;
+                while (q < w) {
+                    if (kd[q] == KIND_2X2_FIRST) {
+                        double x1 = (double)F[w + ii + q * ld], x2 = (double)F[w + ii + (q + 1) * ld];
+                        T w1 = T(x1 * dd[q] + x2 * ee[q]), w2 = T(x1 * ee[q] + x2 * dd[q + 1]);
+                        acc -= w1 * F[w + jj + q * ld];
+                        acc -= w2 * F[w + jj + (q + 1) * ld];
+                        q += 2;
+                    } else {
+                        acc -= T((double)F[w + ii + q * ld] * dd[q]) * F[w + jj + q * ld];
+                        q += 1;
+                    }
+                }
+                F[w + ii + (w + jj) * ld] = acc;
+            }
+        __syncthreads();
+    } else {  // STRUCT_G: LU with row interchanges inside the fully-summed rows
+        SmemStore<T> store{F, ld, f, w};
+        FrontScratch sc{lvec, dd, ee, lp, kd, ctl};
+        lu_front_steps<T>(store, sc, f, w, A.lu_pivot != 0, A.u, eps, st);
+        // F22 -= (L21 D) U12, summed over k in order (lu.jl:142-150)
+        for (int jj = warp; jj < m; jj += nwarps)
+            for (int ii = lane; ii < m; ii += 32) {
+                T acc = T(0);
+                for (int q = 0; q < w; ++q) acc += F[w + ii + q * ld] * T(dd[q]) * F[q + (w + jj) * ld];
+                F[w + ii + (w + jj) * ld] -= acc;
+            }
+        __syncthreads();
+    }
+
+    // write-out: panel (and U^T panel), D / pivots, statistics, contribution block
+    T* P = factor + fd.panel;
+    const bool unit = STRUCT != STRUCT_SPD;
+    for (int j = warp; j < w; j += nwarps)
+        for (int i = lane; i < f; i += 32) {
+            T v = i < j ? T(0) : (i == j && unit ? T(1) : F[i + j * ld]);
+            P[i + (int64_t)j * f] = v;
+        }
+    if (STRUCT == STRUCT_G) {
+        T* U = A.ufactor + (int64_t)member * A.factor_len + fd.panel;
+        for (int j = warp; j < w; j += nwarps)
+            for (int i = lane; i < f; i += 32) U[i + (int64_t)j * f] = i < j ? T(0) : (i == j ? T(1) : F[j + i * ld]);
+    }
+    if (STRUCT != STRUCT_SPD) {
+        const int64_t n = A.n;
+        for (int q = tid; q < w; q += nt) {
+            const int64_t g = fd.c0 + q;
+            A.piv[member * n + g] = fd.c0 + lp[q] + 1;
+            A.kind[member * n + g] = kd[q];
+            A.d[member * 2 * n + g] = dd[q];
+            A.d[member * 2 * n + n + g] = STRUCT == STRUCT_S ? ee[q] : 0.0;
+        }
+    }
+    if (tid == 0) {
+        int64_t* S = A.stats + ((int64_t)member * A.ns + s) * NSTAT;
+        for (int q = 0; q < NSTAT; ++q) S[q] = st[q];
+        A.finfo[(int64_t)member * A.ns + s] = (int32_t)st[ST_INFO];
+    }
+    if (fd.cb >= 0 && m > 0 && status == 0) {
+        T* C = cbar + fd.cb;
+        for (int jj = warp; jj < m; jj += nwarps)
+            for (int ii = (STRUCT == STRUCT_G ? 0 : jj) + lane; ii < m; ii += 32)
+                C[ii + (int64_t)jj * m] = F[w + ii + (w + jj) * ld];
+    }
+}
+
+size_t small_front_smem(int fmax, int elsize) {
+    size_t ld = fmax | 1;
+    size_t b = (ld * fmax * elsize + 15) & ~size_t(15);
+    b += sizeof(double) * (2 * fmax + 2 * fmax);  // dd, ee (w <= f), lvec (2 f)
+    b += sizeof(int) * (fmax + fmax + 16);        // lp, ri, ctl
+    b += fmax + 16;                               // kind
+    return (b + 15) & ~size_t(15);
+}
+
+template <typename T>
+cudaError_t launch_small(int structure, const SmallArgs<T>& a, int count, int nmembers, int fmax, cudaStream_t st) {
+    size_t smem = small_front_smem(fmax, sizeof(T));
+    int threads = fmax <= 48 ? 128 : 256;
+    dim3 grid(count, nmembers);
+    cudaError_t e = cudaSuccess;
+    switch (structure) {
+        case STRUCT_SPD:
+            e = cudaFuncSetAttribute(small_front_kernel<T, STRUCT_SPD>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+            if (e == cudaSuccess) small_front_kernel<T, STRUCT_SPD><<<grid, threads, smem, st>>>(a);
+            break;
+        case STRUCT_S:
+            e = cudaFuncSetAttribute(small_front_kernel<T, STRUCT_S>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+            if (e == cudaSuccess) small_front_kernel<T, STRUCT_S><<<grid, threads, smem, st>>>(a);
+            break;
+        default:
+            e = cudaFuncSetAttribute(small_front_kernel<T, STRUCT_G>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+            if (e == cudaSuccess) small_front_kernel<T, STRUCT_G><<<grid, threads, smem, st>>>(a);
+    }
+    if (e != cudaSuccess) return e;
+    return cudaGetLastError();
+}
+
+template cudaError_t launch_small<double>(int, const SmallArgs<double>&, int, int, int, cudaStream_t);
+template cudaError_t launch_small<float>(int, const SmallArgs<float>&, int, int, int, cudaStream_t);
+
+// ---------------------------------------------------------------------------
+// Column-owner assembly of large fronts (one warp per task).
+// Storage of a large front: the panel (f x w, ld f) holds F[:, 0:w] -- for "S"
+// both triangles of the fully-summed block -- ; "G" keeps F[j, i] (i > j, j < w)
+// in the U^T panel at ufactor[panel + i + j f]; the contribution block
+// F[w:f, w:f] lives at cb (ld m).
+template <typename T, int STRUCT>
+__global__ void assemble_large_kernel(LargeAsmArgs<T> A) {
+    const int task = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+    const int lane = threadIdx.x & 31;
+    if (task >= A.count) return;
+    const int member = A.members ? A.members[blockIdx.y] : blockIdx.y;
+    const ColTask ct = A.tasks[task];
+    const DFront fd = A.maps.fronts[ct.front];
+    const int f = fd.f, w = fd.w, m = f - w, p = ct.p;
+    const double* nz = A.nzval + (int64_t)member * A.nnz;
+    T* factor = A.factor + (int64_t)member * A.factor_len;
+    T* ufac = STRUCT == STRUCT_G ? A.ufactor + (int64_t)member * A.factor_len : nullptr;
+    const T* cbar = A.cb + (int64_t)member * A.cb_len;
+    T* cbown = A.cb + (int64_t)member * A.cb_len + fd.cb;
+    if (p < w) {
+        T* col = factor + fd.panel + (int64_t)p * f;
+        for (int i = lane; i < f; i += 32) col[i] = T(0);
+        if (STRUCT == STRUCT_G) {
+            T* ucol = ufac + fd.panel + (int64_t)p * f;
+            for (int i = lane; i < f; i += 32) ucol[i] = T(0);
+        }
+        __syncwarp();
+        const int a0 = A.maps.amcol[fd.amcol_begin + p], a1 = A.maps.amcol[fd.amcol_begin + p + 1];
+        for (int k = a0 + lane; k < a1; k += 32) {
+            int code = A.maps.am_loc[k];
+            if (k > a0 && A.maps.am_loc[k - 1] == code) continue;
+            T acc = T(0);
+            for (int q = k; q < a1 && A.maps.am_loc[q] == code; ++q) acc += T(nz[A.maps.am_src[q]]);
+            int loc = (code > 0 ? code : -code) - 1;
+            if (code > 0) factor[fd.panel + loc] += acc;
+            else ufac[fd.panel + loc] += acc;
+        }
+    } else {
+        if (fd.cb < 0) return;
+        T* col = cbown + (int64_t)(p - w) * m;
+        for (int i = (STRUCT == STRUCT_G ? 0 : p - w) + lane; i < m; i += 32) col[i] = T(0);
+    }
+    __syncwarp();
+    const int e0 = A.maps.eacol[fd.eacol_begin + p], e1 = A.maps.eacol[fd.eacol_begin + p + 1];
+    for (int e = e0; e < e1; ++e) {
+        const int c = A.maps.ea[2 * e], t = A.maps.ea[2 * e + 1];
+        const DFront cd = A.maps.fronts[c];
+        const int mc = cd.f - cd.w;
+        const T* C = cbar + cd.cb;
+        const int* ri = A.maps.relind + cd.ri_begin;
+        // lower part: C[ii, t], ii >= t  ->  F[ri[ii], p]
+        for (int ii = t + lane; ii < mc; ii += 32) {
+            const int pi = ri[ii];
+            const T v = C[ii + (int64_t)t * mc];
+            if (p < w) factor[fd.panel + pi + (int64_t)p * f] += v;
+            else if (pi >= w) cbown[(pi - w) + (int64_t)(p - w) * m] += v;
+        }
+        if (STRUCT == STRUCT_G) {
+            if (p < w) {
+                // upper part of row p: C[t, jj], jj > t  ->  F[p, ri[jj]] = U^T panel (ri[jj], p)
+                for (int jj = t + 1 + lane; jj < mc; jj += 32)
+                    ufac[fd.panel + ri[jj] + (int64_t)p * f] += C[t + (int64_t)jj * mc];
+            } else {
+                // rows of the contribution block above its diagonal: C[ii, t] with w <= ri[ii] < p
+                for (int ii = lane; ii < t; ii += 32) {
+                    const int pi = ri[ii];
+                    if (pi >= w) cbown[(pi - w) + (int64_t)(p - w) * m] += C[ii + (int64_t)t * mc];
+                }
+            }
+        }
+    }
+    if (STRUCT == STRUCT_S && p < w) {
+        // mirror of the fully-summed block happens after all columns are assembled (panel kernel)
+    }
+}
+
+template <typename T>
+cudaError_t launch_assemble_large(int structure, const LargeAsmArgs<T>& a, int nmembers, cudaStream_t st) {
+    const int warps = 8;
+    dim3 grid((a.count + warps - 1) / warps, nmembers);
+    switch (structure) {
+        case STRUCT_SPD: assemble_large_kernel<T, STRUCT_SPD><<<grid, warps * 32, 0, st>>>(a); break;
+        case STRUCT_S: assemble_large_kernel<T, STRUCT_S><<<grid, warps * 32, 0, st>>>(a); break;
+        default: assemble_large_kernel<T, STRUCT_G><<<grid, warps * 32, 0, st>>>(a);
+    }
+    return cudaGetLastError();
+}
+
+template cudaError_t launch_assemble_large<double>(int, const LargeAsmArgs<double>&, int, cudaStream_t);
+template cudaError_t launch_assemble_large<float>(int, const LargeAsmArgs<float>&, int, cudaStream_t);
+
+// ---------------------------------------------------------------------------
+// Totals of the per-front statistics and the smallest failed factor column
+// (reduce_stats! src/numeric/ldlt.jl:1276-1340, _cholesky_stats_kernel!
+// src/numeric/factorize.jl:13-45): one CTA per member, no atomics.
+__global__ void stats_kernel(StatsArgs A) {
+    const int member = A.members ? A.members[blockIdx.x] : blockIdx.x;
+    __shared__ int64_t red[NSTAT + 1][256];
+    int64_t acc[NSTAT] = {0, 0, 0, 0, 0, 0};
+    int64_t best = INT64_MAX;
+    const int64_t* S = A.stats + (int64_t)member * A.ns * NSTAT;
+    for (int s = threadIdx.x; s < A.ns; s += blockDim.x) {
+        for (int q = 0; q < NSTAT - 1; ++q) acc[q] += S[(int64_t)s * NSTAT + q];
+        int64_t fi = S[(int64_t)s * NSTAT + ST_INFO];
+        if (fi != 0) {
+            acc[ST_INFO] += 1;
+            best = min(best, (int64_t)A.super_ptr0[s] + fi - 1);
+        }
+    }
+    for (int q = 0; q < NSTAT; ++q) red[q][threadIdx.x] = acc[q];
+    red[NSTAT][threadIdx.x] = best;
+    __syncthreads();
+    for (int h = blockDim.x / 2; h > 0; h >>= 1) {
+        if (threadIdx.x < h) {
+            for (int q = 0; q < NSTAT; ++q) red[q][threadIdx.x] += red[q][threadIdx.x + h];
+            red[NSTAT][threadIdx.x] = min(red[NSTAT][threadIdx.x], red[NSTAT][threadIdx.x + h]);
+        }
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+        for (int q = 0; q < NSTAT; ++q) A.totals[(int64_t)member * NSTAT + q] = red[q][0];
+        int64_t b = red[NSTAT][0];
+        A.info[member] = b == INT64_MAX ? 0 : (int64_t)A.perm0[b] + 1;  // original column, 1-based
+    }
+}
+
+cudaError_t launch_stats(const StatsArgs& a, int nmembers, cudaStream_t st) {
+    stats_kernel<<<nmembers, 256, 0, st>>>(a);
+    return cudaGetLastError();
+}
+
+}  // namespace sds

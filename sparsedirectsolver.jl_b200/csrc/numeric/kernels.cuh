@@ -1,0 +1,147 @@
+// Kernel argument blocks and launch functions of the numeric phase.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "common.cuh"
+
+namespace sds {
+
+template <typename T>
+struct SmallArgs {
+    DeviceMaps maps;
+    const int32_t* list;     // fronts of this launch
+    const int32_t* members;  // active batch members (NULL: 0..nmembers-1)
+    const double* nzval;
+    T* factor;
+    T* ufactor;
+    T* cb;
+    double* d;
+    int32_t* piv;
+    int8_t* kind;
+    int64_t* stats;
+    int32_t* finfo;
+    const int8_t* psign;
+    int64_t nnz, factor_len, cb_len, n;
+    int32_t ns;
+    int32_t pivot;
+    int32_t lu_pivot;
+    double u, eps;
+};
+
+template <typename T>
+struct LargeAsmArgs {
+    DeviceMaps maps;
+    const ColTask* tasks;
+    int32_t count;
+    const int32_t* members;
+    const double* nzval;
+    T* factor;
+    T* ufactor;
+    T* cb;
+    int64_t nnz, factor_len, cb_len;
+};
+
+struct StatsArgs {
+    const int64_t* stats;
+    const int32_t* members;
+    const int32_t* super_ptr0;  // 0-based first column of each front
+    const int32_t* perm0;       // 0-based original column of each factor column
+    int64_t* totals;            // 6 per member
+    int64_t* info;              // 1 per member (original column, 1-based; 0 = success)
+    int32_t ns;
+};
+
+// Large Cholesky column-block panel: diagonal block + trsm of the rows below.
+struct PanelTask {
+    int32_t front;
+    int32_t row0;   // first row of this CTA's row tile (>= kb + nb), or -1: the diagonal-block writer
+};
+
+template <typename T>
+struct CholPanelArgs {
+    const DFront* fronts;
+    const PanelTask* tasks;
+    int32_t count;
+    const int32_t* members;
+    T* factor;
+    int32_t* finfo;
+    int64_t* stats;
+    int64_t factor_len;
+    int32_t ns;
+    int32_t kb;     // first column of the block
+    double eps;
+};
+
+template <typename T>
+struct GemmArgs {
+    const GemmTile* tiles;
+    int32_t count;
+    const int32_t* members;
+    const T* abuf;     // buffer of A (factor or workspace)
+    const T* bbuf;     // buffer of B (factor or U^T panels)
+    T* cbuf;           // buffer of C (factor or CB arena)
+    int64_t astride, bstride, cstride;  // per-member strides of the three buffers
+    const int32_t* finfo;
+    int32_t ns;
+};
+
+// Large LDLT / LU fronts: one CTA per front, the in-front steps on the global panels.
+template <typename T>
+struct LargePivotArgs {
+    const DFront* fronts;
+    const int32_t* list;
+    int32_t count;
+    const int32_t* members;
+    T* factor;
+    T* ufactor;
+    double* scratch;         // per-front scratch (offsets in scr_off), per member stride scr_len
+    const int64_t* scr_off;  // per listed front
+    int64_t scr_len;
+    double* d;
+    int32_t* piv;
+    int8_t* kind;
+    int64_t* stats;
+    int32_t* finfo;
+    const int8_t* psign;
+    const int32_t* perm;
+    int64_t factor_len, n;
+    int32_t ns;
+    int32_t pivot, lu_pivot;
+    double u, eps;
+};
+
+// W = L21 D of large LDLT / LU fronts into a workspace (m x w per front, ld m).
+template <typename T>
+struct ScaleArgs {
+    const DFront* fronts;
+    const int32_t* list;
+    int32_t count;
+    const int64_t* woff;     // workspace offset per listed front
+    const int32_t* members;
+    const T* factor;
+    const double* d;
+    const int8_t* kind;
+    T* work;
+    int64_t factor_len, n, work_len;
+};
+
+template <typename T>
+cudaError_t launch_small(int structure, const SmallArgs<T>& a, int count, int nmembers, int fmax, cudaStream_t st);
+size_t small_front_smem(int fmax, int elsize);
+template <typename T>
+cudaError_t launch_assemble_large(int structure, const LargeAsmArgs<T>& a, int nmembers, cudaStream_t st);
+cudaError_t launch_stats(const StatsArgs& a, int nmembers, cudaStream_t st);
+template <typename T>
+cudaError_t launch_chol_panel(const CholPanelArgs<T>& a, int nb, int nmembers, cudaStream_t st);
+template <typename T>
+cudaError_t launch_gemm(const GemmArgs<T>& a, int nmembers, cudaStream_t st);
+template <typename T>
+cudaError_t launch_large_pivot(int structure, const LargePivotArgs<T>& a, int nmembers, cudaStream_t st);
+template <typename T>
+cudaError_t launch_scale_ld_front(int structure, const ScaleArgs<T>& a, int maxw, int nmembers, cudaStream_t st);
+
+constexpr int PANEL_ROWS = 128;  // rows of the trsm tile of a Cholesky panel CTA
+constexpr int GEMM_BM = 64, GEMM_BN = 64;
+
+}  // namespace sds

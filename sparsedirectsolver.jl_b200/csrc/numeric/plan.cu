@@ -1,0 +1,569 @@
+// Plan construction (host): validates the reference's Symbolic maps, derives the
+// level schedule, classifies fronts (shared-memory fused kernel vs. large-front
+// dense path), places the contribution blocks in one arena by lifetime, builds
+// the launch program of the factorization and allocates every device buffer.
+// Replaces allocate_numeric (src/numeric/storage.jl:205-256), NumericPlan
+// (:36-104) and allocate_solve (src/solve/sweeps.jl:164-173) of the reference;
+// the schedule is this library's own (levels of the supernodal tree, fronts
+// binned by size), not the reference's regime A/B/C schedule.
+#include <cuda_runtime.h>
+#include <stdint.h>
+#include <string.h>
+
+#include <algorithm>
+#include <map>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "plan.h"
+
+namespace sds {
+
+namespace {
+
+struct BuildError : std::runtime_error {
+    int code;
+    BuildError(int c, const std::string& m) : std::runtime_error(m), code(c) {}
+};
+
+std::vector<int64_t> read_map(const void* p, int64_t len, int width, const char* name) {
+    if (len < 0) throw BuildError(SDSB200_INVALID_VALUE, std::string("negative length of ") + name);
+    std::vector<int64_t> out(len);
+    if (len == 0) return out;
+    if (!p) throw BuildError(SDSB200_INVALID_VALUE, std::string("map ") + name + " is NULL");
+    if (width == 4) {
+        const int32_t* q = static_cast<const int32_t*>(p);
+        for (int64_t k = 0; k < len; ++k) out[k] = q[k];
+    } else {
+        const int64_t* q = static_cast<const int64_t*>(p);
+        for (int64_t k = 0; k < len; ++k) out[k] = q[k];
+    }
+    return out;
+}
+
+template <class X>
+X* dalloc(Plan* P, size_t count) {
+    if (count == 0) count = 1;
+    void* ptr = nullptr;
+    cudaError_t e = cudaMalloc(&ptr, count * sizeof(X));
+    if (e != cudaSuccess) throw BuildError(SDSB200_ALLOC_FAILED, std::string("cudaMalloc: ") + cudaGetErrorString(e));
+    P->allocations.push_back(ptr);
+    P->device_bytes += (int64_t)(count * sizeof(X));
+    return static_cast<X*>(ptr);
+}
+
+template <class X>
+X* upload(Plan* P, const std::vector<X>& v, cudaStream_t st) {
+    X* d = dalloc<X>(P, v.size());
+    if (!v.empty()) {
+        cudaError_t e = cudaMemcpyAsync(d, v.data(), v.size() * sizeof(X), cudaMemcpyHostToDevice, st);
+        if (e != cudaSuccess) throw BuildError(SDSB200_CUDA_ERROR, cudaGetErrorString(e));
+    }
+    return d;
+}
+
+int32_t to_i32(int64_t v, const char* what) {
+    if (v < INT32_MIN || v > INT32_MAX) throw BuildError(SDSB200_INVALID_VALUE, std::string(what) + " overflows int32");
+    return (int32_t)v;
+}
+
+// first-fit placement of intervals [start, end] of `len` elements on one arena
+struct Arena {
+    struct Block { int64_t off, len; int end; };
+    std::vector<Block> live;
+    int64_t top = 0;
+    int64_t place(int64_t len, int start, int end) {
+        // release the blocks whose lifetime ended before `start`
+        live.erase(std::remove_if(live.begin(), live.end(), [&](const Block& b) { return b.end < start; }), live.end());
+        std::sort(live.begin(), live.end(), [](const Block& a, const Block& b) { return a.off < b.off; });
+        int64_t cur = 0;
+        for (const Block& b : live) {
+            int64_t aligned = (cur + 31) & ~int64_t(31);
+            if (b.off >= aligned + len) break;
+            cur = std::max(cur, b.off + b.len);
+        }
+        cur = (cur + 31) & ~int64_t(31);
+        live.push_back({cur, len, end});
+        top = std::max(top, cur + len);
+        return cur;
+    }
+};
+
+}  // namespace
+
+Plan* build_plan(const sdsb200_symbolic* sym, const sdsb200_plan_options* popts, cudaStream_t st) {
+    Plan* P = new Plan();
+    try {
+        if (!sym) throw BuildError(SDSB200_INVALID_VALUE, "symbolic is NULL");
+        const int width = sym->index_width;
+        if (width != 4 && width != 8) throw BuildError(SDSB200_INVALID_VALUE, "index_width must be 4 or 8");
+        if (sym->structure != STRUCT_G && sym->structure != STRUCT_S && sym->structure != STRUCT_SPD)
+            throw BuildError(SDSB200_NOT_SUPPORTED, "structure must be G, S or SPD");
+        P->n = sym->n;
+        P->nnz = sym->nnz;
+        P->ns = sym->ns;
+        P->structure = sym->structure;
+        P->nbatch = popts ? std::max(1, popts->nbatch) : 1;
+        P->precision = popts ? popts->precision : SDSB200_PRECISION_FP64;
+        if (P->precision != SDSB200_PRECISION_FP64 && P->precision != SDSB200_PRECISION_FP32)
+            throw BuildError(SDSB200_NOT_SUPPORTED, "precision must be FP64 or FP32");
+        P->elsize = P->precision == SDSB200_PRECISION_FP64 ? 8 : 4;
+        P->max_nrhs = popts ? std::max(1, popts->max_nrhs) : 1;
+        P->nact = P->nbatch;
+        const int64_t n = P->n, ns = P->ns, nnz = P->nnz;
+        if (n < 0 || ns < 0 || nnz < 0) throw BuildError(SDSB200_INVALID_VALUE, "negative size");
+
+        std::vector<int64_t> perm = read_map(sym->perm, n, width, "perm");
+        std::vector<int64_t> super_ptr = read_map(sym->super_ptr, ns + 1, width, "super_ptr");
+        std::vector<int64_t> snparent = read_map(sym->snparent, ns, width, "snparent");
+        std::vector<int64_t> rowptr = read_map(sym->rowptr, ns + 1, width, "rowptr");
+        std::vector<int64_t> front_ptr = read_map(sym->front_ptr, ns + 1, width, "front_ptr");
+        std::vector<int64_t> child_ptr = read_map(sym->child_ptr, ns + 1, width, "child_ptr");
+        std::vector<int64_t> relind_ptr = read_map(sym->relind_ptr, ns + 1, width, "relind_ptr");
+        std::vector<int64_t> amap_ptr = read_map(sym->amap_ptr, ns + 1, width, "amap_ptr");
+        if (ns > 0 && (super_ptr[0] != 1 || super_ptr[ns] != n + 1))
+            throw BuildError(SDSB200_INVALID_VALUE, "super_ptr does not cover 1:n");
+        std::vector<int64_t> rowval = read_map(sym->rowval, ns ? rowptr[ns] - 1 : 0, width, "rowval");
+        std::vector<int64_t> child_list = read_map(sym->child_list, ns ? child_ptr[ns] - 1 : 0, width, "child_list");
+        std::vector<int64_t> relind = read_map(sym->relind, ns ? relind_ptr[ns] - 1 : 0, width, "relind");
+        std::vector<int64_t> amap = read_map(sym->amap, nnz, width, "amap");
+        std::vector<int64_t> amap_src = read_map(sym->amap_src, ns ? amap_ptr[ns] - 1 : 0, width, "amap_src");
+        P->factor_len = ns ? front_ptr[ns] - 1 : 0;
+        const bool gen = P->structure == STRUCT_G;
+
+        // fronts
+        P->fronts.resize(ns);
+        for (int64_t s = 0; s < ns; ++s) {
+            DFront& F = P->fronts[s];
+            int64_t f = rowptr[s + 1] - rowptr[s], w = super_ptr[s + 1] - super_ptr[s];
+            if (w < 1 || f < w) throw BuildError(SDSB200_INVALID_VALUE, "front with w < 1 or f < w");
+            if (front_ptr[s + 1] - front_ptr[s] != f * w)
+                throw BuildError(SDSB200_INVALID_VALUE, "front_ptr does not match the panel sizes");
+            F.panel = front_ptr[s] - 1;
+            F.cb = -1;
+            F.f = to_i32(f, "front rows");
+            F.w = to_i32(w, "front width");
+            F.c0 = to_i32(super_ptr[s] - 1, "column");
+            F.parent = to_i32(snparent[s] - 1, "snparent");
+            if (F.parent >= 0 && F.parent <= s)
+                throw BuildError(SDSB200_INVALID_VALUE, "supernodes must be numbered children before parents");
+            F.ch_begin = to_i32(child_ptr[s] - 1, "child_ptr");
+            F.ch_end = to_i32(child_ptr[s + 1] - 1, "child_ptr");
+            F.ri_begin = to_i32(relind_ptr[s] - 1, "relind_ptr");
+            int64_t nri = relind_ptr[s + 1] - relind_ptr[s];
+            if (nri != (F.parent >= 0 ? f - w : 0))
+                throw BuildError(SDSB200_INVALID_VALUE, "relind length does not match the front");
+            F.am_begin = to_i32(amap_ptr[s] - 1, "amap_ptr");
+            F.am_end = to_i32(amap_ptr[s + 1] - 1, "amap_ptr");
+            F.row_begin = to_i32(rowptr[s] - 1, "rowptr");
+            F.level = 0;
+        }
+        // levels: height above the leaves (children are numbered first)
+        for (int64_t s = 0; s < ns; ++s) {
+            int p = P->fronts[s].parent;
+            if (p >= 0) P->fronts[p].level = std::max(P->fronts[p].level, P->fronts[s].level + 1);
+        }
+        P->nlevels = 0;
+        for (auto& F : P->fronts) P->nlevels = std::max(P->nlevels, F.level + 1);
+        P->level_fronts.assign(P->nlevels, {});
+        for (int64_t s = 0; s < ns; ++s) P->level_fronts[P->fronts[s].level].push_back((int)s);
+        for (auto& F : P->fronts) {
+            double f = F.f;
+            for (int k = 0; k < F.w; ++k) P->flops += (f - k) * (f - k);
+        }
+
+        // assembly entries: 0-based source, signed local position, per-column starts
+        std::vector<int32_t> am_src(amap_src.size()), am_loc(amap_src.size());
+        std::vector<int32_t> amcol;
+        for (int64_t s = 0; s < ns; ++s) {
+            DFront& F = P->fronts[s];
+            F.amcol_begin = (int32_t)amcol.size();
+            int64_t f = F.f;
+            int j = 0;
+            for (int64_t k = F.am_begin; k < F.am_end; ++k) {
+                int64_t p = amap_src[k] - 1;
+                if (p < 0 || p >= nnz) throw BuildError(SDSB200_INVALID_VALUE, "amap_src out of range");
+                int64_t off = amap[p];
+                int64_t loc = (off < 0 ? -off : off) - front_ptr[s];
+                if (loc < 0 || loc >= f * F.w) throw BuildError(SDSB200_INVALID_VALUE, "amap offset outside its panel");
+                am_src[k] = (int32_t)p;
+                am_loc[k] = (gen && off < 0) ? -(int32_t)(loc + 1) : (int32_t)(loc + 1);
+                while (j <= loc / f) { amcol.push_back((int32_t)k); ++j; }
+            }
+            while (j <= F.w) { amcol.push_back(F.am_end); ++j; }
+        }
+
+        // small / large classification
+        const std::vector<int> classes = P->elsize == 8 ? std::vector<int>{32, 64, 96, 128, 160}
+                                                        : std::vector<int>{32, 64, 96, 128, 160, 224};
+        P->fsmall_max = classes.back();
+        auto class_of = [&](int f) {
+            for (int c : classes)
+                if (f <= c) return c;
+            return 0;
+        };
+
+        // contribution blocks on one arena, by lifetime [level, parent level]
+        {
+            Arena arena;
+            std::vector<int> order;
+            for (int L = 0; L < P->nlevels; ++L)
+                for (int s : P->level_fronts[L]) order.push_back(s);
+            for (int s : order) {
+                DFront& F = P->fronts[s];
+                int64_t m = F.f - F.w;
+                if (F.parent < 0 || m == 0) continue;
+                F.cb = arena.place(m * m, F.level, P->fronts[F.parent].level);
+            }
+            P->cb_len = ((arena.top + 31) & ~int64_t(31));
+        }
+
+        // column-owner extend-add lists of the large fronts
+        std::vector<int32_t> ea, eacol;
+        for (int64_t s = 0; s < ns; ++s) {
+            DFront& F = P->fronts[s];
+            F.eacol_begin = (int32_t)eacol.size();
+            if (class_of(F.f) != 0) continue;
+            std::vector<std::vector<std::pair<int, int>>> per(F.f);
+            for (int q = F.ch_begin; q < F.ch_end; ++q) {
+                int c = (int)child_list[q] - 1;
+                if (c < 0 || c >= ns || P->fronts[c].parent != s)
+                    throw BuildError(SDSB200_INVALID_VALUE, "child_list is inconsistent with snparent");
+                const DFront& C = P->fronts[c];
+                int mc = C.f - C.w;
+                if (mc <= 0 || C.cb < 0) continue;
+                for (int t = 0; t < mc; ++t) {
+                    int p = (int)relind[C.ri_begin + t] - 1;
+                    if (p < 0 || p >= F.f) throw BuildError(SDSB200_INVALID_VALUE, "relind out of range");
+                    per[p].push_back({c, t});
+                }
+            }
+            for (int p = 0; p < F.f; ++p) {
+                eacol.push_back((int32_t)(ea.size() / 2));
+                for (auto& ct : per[p]) { ea.push_back(ct.first); ea.push_back(ct.second); }
+            }
+            eacol.push_back((int32_t)(ea.size() / 2));
+        }
+
+        // launch program of the factorization
+        std::vector<int32_t> lists;
+        std::vector<ColTask> coltasks;
+        std::vector<PanelTask> ptasks;
+        std::vector<GemmTile> tiles;
+        std::vector<int64_t> scr_off, woff;
+        const int NB = 32;
+        auto add_gemm_tiles = [&](int64_t a, int lda, int64_t b, int ldb, int64_t c, int ldc, int M, int N, int K,
+                                  bool lower, int front) -> double {
+            // algorithmic flops: 2 K per entry of C that is written (the lower trapezoid for SYRK-like updates)
+            double entries = 0;
+            for (int j = 0; j < N; ++j) entries += lower ? std::max(0, M - j) : M;
+            for (int ti = 0; ti < M; ti += GEMM_BM)
+                for (int tj = 0; tj < N; tj += GEMM_BN) {
+                    int mm = std::min(GEMM_BM, M - ti), nn = std::min(GEMM_BN, N - tj);
+                    if (lower && ti + mm - 1 < tj) continue;
+                    GemmTile t;
+                    t.a = a + ti;
+                    t.b = b + tj;
+                    t.c = c + ti + (int64_t)tj * ldc;
+                    t.lda = lda; t.ldb = ldb; t.ldc = ldc;
+                    t.m = mm; t.n = nn; t.k = K;
+                    t.diag = lower ? ti - tj : (1 << 29);
+                    t.front = front;
+                    tiles.push_back(t);
+                }
+            return 2.0 * K * entries;
+        };
+        for (int L = 0; L < P->nlevels; ++L) {
+            std::map<int, std::vector<int>> small;
+            std::vector<int> large;
+            for (int s : P->level_fronts[L]) {
+                int c = class_of(P->fronts[s].f);
+                if (c) small[c].push_back(s);
+                else large.push_back(s);
+            }
+            for (auto& kv : small) {
+                ProgLaunch pl{};
+                pl.kind = L_SMALL; pl.level = L; pl.count = (int)kv.second.size(); pl.cls = kv.first;
+                pl.list = (int64_t)lists.size();
+                lists.insert(lists.end(), kv.second.begin(), kv.second.end());
+                for (int s : kv.second) {
+                    const DFront& F = P->fronts[s];
+                    double f = F.f, w = F.w, m = F.f - F.w;
+                    for (int k = 0; k < F.w; ++k) pl.flops += (f - k) * (f - k);
+                    double tri = (P->structure == STRUCT_G) ? 1.0 : 0.5;
+                    pl.bytes += P->elsize * (f * w * (gen ? 2 : 1) + (F.cb >= 0 ? tri * m * m : 0.0));
+                    pl.bytes += 12.0 * (F.am_end - F.am_begin);
+                    for (int q = F.ch_begin; q < F.ch_end; ++q) {
+                        const DFront& C = P->fronts[child_list[q] - 1];
+                        double mc = C.f - C.w;
+                        pl.bytes += P->elsize * tri * mc * mc + 4.0 * mc;
+                    }
+                }
+                P->prog.push_back(pl);
+            }
+            if (large.empty()) continue;
+            {
+                ProgLaunch pl{};
+                pl.kind = L_ASSEMBLE; pl.level = L; pl.list = (int64_t)coltasks.size();
+                for (int s : large) {
+                    const DFront& F = P->fronts[s];
+                    for (int p = 0; p < F.f; ++p)
+                        if (p < F.w || F.cb >= 0) coltasks.push_back({s, p});
+                }
+                pl.count = (int)(coltasks.size() - pl.list);
+                P->prog.push_back(pl);
+            }
+            if (P->structure == STRUCT_SPD) {
+                int maxw = 0;
+                for (int s : large) maxw = std::max(maxw, P->fronts[s].w);
+                for (int kb = 0; kb < maxw; kb += NB) {
+                    ProgLaunch dl{};
+                    dl.kind = L_CHOL_PANEL; dl.level = L; dl.cls = kb; dl.nb = NB; dl.list = (int64_t)ptasks.size();
+                    for (int s : large)
+                        if (P->fronts[s].w > kb) ptasks.push_back({s, -1});
+                    dl.count = (int)(ptasks.size() - dl.list);
+                    P->prog.push_back(dl);
+                    ProgLaunch tl = dl;
+                    tl.list = (int64_t)ptasks.size();
+                    for (int s : large) {
+                        const DFront& F = P->fronts[s];
+                        if (F.w <= kb) continue;
+                        int nbb = std::min(NB, F.w - kb);
+                        for (int r0 = kb + nbb; r0 < F.f; r0 += PANEL_ROWS) ptasks.push_back({s, r0});
+                    }
+                    tl.count = (int)(ptasks.size() - tl.list);
+                    if (tl.count) P->prog.push_back(tl);
+                    ProgLaunch gl{};
+                    gl.kind = L_GEMM; gl.level = L; gl.list = (int64_t)tiles.size();
+                    gl.abuf = gl.bbuf = gl.cbuf = BUF_FACTOR;
+                    for (int s : large) {
+                        const DFront& F = P->fronts[s];
+                        if (F.w <= kb + NB) continue;
+                        int k1 = kb + NB;
+                        int64_t f = F.f;
+                        gl.flops += add_gemm_tiles(F.panel + k1 + (int64_t)kb * f, F.f, F.panel + k1 + (int64_t)kb * f,
+                                                   F.f, F.panel + k1 + (int64_t)k1 * f, F.f, F.f - k1, F.w - k1, NB,
+                                                   true, s);
+                    }
+                    gl.count = (int)(tiles.size() - gl.list);
+                    if (gl.count) P->prog.push_back(gl);
+                }
+                ProgLaunch cl{};
+                cl.kind = L_GEMM; cl.level = L; cl.list = (int64_t)tiles.size();
+                cl.abuf = cl.bbuf = BUF_FACTOR; cl.cbuf = BUF_CB;
+                for (int s : large) {
+                    const DFront& F = P->fronts[s];
+                    int m = F.f - F.w;
+                    if (F.cb < 0 || m == 0) continue;
+                    cl.flops += add_gemm_tiles(F.panel + F.w, F.f, F.panel + F.w, F.f, F.cb, m, m, m, F.w, true, s);
+                }
+                cl.count = (int)(tiles.size() - cl.list);
+                if (cl.count) P->prog.push_back(cl);
+            } else {
+                ProgLaunch pl{};
+                pl.kind = L_PIVOT_FRONT; pl.level = L; pl.list = (int64_t)lists.size(); pl.count = (int)large.size();
+                pl.cls = (int)scr_off.size();
+                int64_t so = 0;
+                for (int s : large) {
+                    const DFront& F = P->fronts[s];
+                    lists.push_back(s);
+                    scr_off.push_back(so);
+                    so += 2 * (int64_t)F.f + 2 * (int64_t)F.w + (F.w + 16 + 1) / 2 + (F.w + 7) / 8 + 8;
+                }
+                P->scr_len = std::max(P->scr_len, so);
+                P->prog.push_back(pl);
+                std::vector<int> withcb;
+                for (int s : large)
+                    if (P->fronts[s].cb >= 0) withcb.push_back(s);
+                if (!withcb.empty()) {
+                    ProgLaunch sl{};
+                    sl.kind = L_SCALE;
+                    sl.level = L; sl.list = (int64_t)lists.size(); sl.count = (int)withcb.size();
+                    sl.cls = (int)woff.size();
+                    int64_t wo = 0;
+                    int maxw = 0;
+                    ProgLaunch gl{};
+                    gl.kind = L_GEMM; gl.level = L;
+                    gl.abuf = BUF_WORK; gl.bbuf = gen ? BUF_UFACTOR : BUF_FACTOR; gl.cbuf = BUF_CB;
+                    gl.list = (int64_t)tiles.size();
+                    for (int s : withcb) {
+                        const DFront& F = P->fronts[s];
+                        int m = F.f - F.w;
+                        lists.push_back(s);
+                        woff.push_back(wo);
+                        gl.flops += add_gemm_tiles(wo, m, F.panel + F.w, F.f, F.cb, m, m, m, F.w, !gen, s);
+                        wo += ((int64_t)m * F.w + 31) & ~int64_t(31);
+                        maxw = std::max(maxw, F.w);
+                    }
+                    sl.maxw = maxw;
+                    P->work_len = std::max(P->work_len, wo);
+                    P->prog.push_back(sl);
+                    gl.count = (int)(tiles.size() - gl.list);
+                    P->prog.push_back(gl);
+                }
+            }
+        }
+        {
+            ProgLaunch pl{};
+            pl.kind = L_STATS;
+            P->prog.push_back(pl);
+        }
+        P->launches_factor = (int)P->prog.size();
+
+        // solve: update vectors, per-level lists
+        std::vector<int64_t> uoff(ns, -1);
+        int64_t uo = 0;
+        for (int64_t s = 0; s < ns; ++s) {
+            int64_t m = P->fronts[s].f - P->fronts[s].w;
+            if (m > 0) {
+                uoff[s] = uo;
+                uo += (m * P->max_nrhs + 3) & ~int64_t(3);
+            }
+        }
+        P->ulen = std::max<int64_t>(uo, 1);
+        std::vector<int32_t> level_lists;
+        P->level_maxw.assign(P->nlevels, 0);
+        P->level_panel_entries.assign(P->nlevels, 0.0);
+        for (int L = 0; L < P->nlevels; ++L) {
+            P->level_list_off.push_back((int64_t)level_lists.size());
+            for (int s : P->level_fronts[L]) {
+                level_lists.push_back(s);
+                const DFront& F = P->fronts[s];
+                P->level_maxw[L] = std::max(P->level_maxw[L], F.w);
+                P->level_panel_entries[L] += (double)F.f * F.w - 0.5 * (double)F.w * (F.w - 1);
+            }
+        }
+
+        // host maps kept for the outputs
+        P->h_perm0.resize(n);
+        for (int64_t k = 0; k < n; ++k) {
+            if (perm[k] < 1 || perm[k] > n) throw BuildError(SDSB200_INVALID_VALUE, "perm out of range");
+            P->h_perm0[k] = (int32_t)(perm[k] - 1);
+        }
+        P->h_super0.resize(ns);
+        for (int64_t s = 0; s < ns; ++s) P->h_super0[s] = (int32_t)(super_ptr[s] - 1);
+        std::vector<int32_t> rv0(rowval.size()), cl0(child_list.size()), ri0(relind.size());
+        for (size_t k = 0; k < rowval.size(); ++k) rv0[k] = (int32_t)(rowval[k] - 1);
+        for (size_t k = 0; k < child_list.size(); ++k) cl0[k] = (int32_t)(child_list[k] - 1);
+        for (size_t k = 0; k < relind.size(); ++k) ri0[k] = (int32_t)(relind[k] - 1);
+
+        // residual map (and its transpose for op(A) = A^T of "G")
+        if (sym->full_rowptr && sym->full_colval && sym->full_srcptr && sym->full_src) {
+            P->has_full = true;
+            P->full_nnz = sym->full_nnz;
+            P->full_nsrc = sym->full_nsrc;
+            std::vector<int64_t> frp = read_map(sym->full_rowptr, n + 1, width, "full_rowptr");
+            std::vector<int64_t> fcv = read_map(sym->full_colval, P->full_nnz, width, "full_colval");
+            std::vector<int64_t> fsp = read_map(sym->full_srcptr, P->full_nnz + 1, width, "full_srcptr");
+            std::vector<int64_t> fsr = read_map(sym->full_src, P->full_nsrc, width, "full_src");
+            for (auto& v : frp) v -= 1;
+            for (auto& v : fcv) v -= 1;
+            for (auto& v : fsp) v -= 1;
+            for (auto& v : fsr) v -= 1;
+            P->d_full_rowptr = upload(P, frp, st);
+            P->d_full_colval = upload(P, fcv, st);
+            P->d_full_srcptr = upload(P, fsp, st);
+            P->d_full_src = upload(P, fsr, st);
+            if (gen) {
+                // transpose: entries regrouped by column, each keeping its source list
+                std::vector<int64_t> cnt(n + 1, 0);
+                for (int64_t e = 0; e < P->full_nnz; ++e) cnt[fcv[e] + 1]++;
+                std::vector<int64_t> trp(n + 1, 0);
+                for (int64_t i = 0; i < n; ++i) trp[i + 1] = trp[i] + cnt[i + 1];
+                std::vector<int64_t> tcv(P->full_nnz), tsp(P->full_nnz + 1), tsr;
+                std::vector<int64_t> next(trp.begin(), trp.end() - 1);
+                std::vector<int64_t> epos(P->full_nnz);
+                for (int64_t r = 0; r < n; ++r)
+                    for (int64_t e = frp[r]; e < frp[r + 1]; ++e) {
+                        int64_t q = next[fcv[e]]++;
+                        tcv[q] = r;
+                        epos[q] = e;
+                    }
+                tsp[0] = 0;
+                for (int64_t q = 0; q < P->full_nnz; ++q) {
+                    int64_t e = epos[q];
+                    for (int64_t k = fsp[e]; k < fsp[e + 1]; ++k) tsr.push_back(fsr[k]);
+                    tsp[q + 1] = (int64_t)tsr.size();
+                }
+                P->d_fullT_rowptr = upload(P, trp, st);
+                P->d_fullT_colval = upload(P, tcv, st);
+                P->d_fullT_srcptr = upload(P, tsp, st);
+                P->d_fullT_src = upload(P, tsr, st);
+            }
+        }
+
+        // device copies
+        P->d_fronts = upload(P, P->fronts, st);
+        P->maps.fronts = P->d_fronts;
+        P->maps.child_list = upload(P, cl0, st);
+        P->maps.relind = upload(P, ri0, st);
+        P->maps.am_src = upload(P, am_src, st);
+        P->maps.am_loc = upload(P, am_loc, st);
+        P->maps.amcol = upload(P, amcol, st);
+        P->maps.ea = upload(P, ea, st);
+        P->maps.eacol = upload(P, eacol, st);
+        P->maps.rowval = upload(P, rv0, st);
+        P->d_perm0 = upload(P, P->h_perm0, st);
+        P->maps.perm = P->d_perm0;
+        P->d_super0 = upload(P, P->h_super0, st);
+        P->d_lists = upload(P, lists, st);
+        P->d_coltasks = upload(P, coltasks, st);
+        P->d_ptasks = upload(P, ptasks, st);
+        P->d_tiles = upload(P, tiles, st);
+        P->d_scr_off = upload(P, scr_off, st);
+        P->d_woff = upload(P, woff, st);
+        P->d_uoff = upload(P, uoff, st);
+        P->d_level_lists = upload(P, level_lists, st);
+
+        const int64_t nb = P->nbatch;
+        const size_t es = P->elsize;
+        auto alloc_bytes = [&](size_t bytes) -> void* {
+            return (void*)dalloc<unsigned char>(P, bytes);
+        };
+        P->d_factor = alloc_bytes(es * std::max<int64_t>(P->factor_len, 1) * nb);
+        if (gen) P->d_ufactor = alloc_bytes(es * std::max<int64_t>(P->factor_len, 1) * nb);
+        P->d_cb = alloc_bytes(es * std::max<int64_t>(P->cb_len, 1) * nb);
+        P->d_d = dalloc<double>(P, 2 * n * nb);
+        P->d_piv = dalloc<int32_t>(P, n * nb);
+        P->d_kind = dalloc<int8_t>(P, n * nb);
+        P->d_stats = dalloc<int64_t>(P, NSTAT * ns * nb);
+        P->d_finfo = dalloc<int32_t>(P, ns * nb);
+        P->d_totals = dalloc<int64_t>(P, NSTAT * nb);
+        P->d_info = dalloc<int64_t>(P, nb);
+        P->d_psign = dalloc<int8_t>(P, n);
+        P->d_members = dalloc<int32_t>(P, nb);
+        P->d_amax = dalloc<double>(P, 1);
+        if (P->scr_len) P->d_scratch = dalloc<double>(P, P->scr_len * nb);
+        if (P->work_len) P->d_work = alloc_bytes(es * P->work_len * nb);
+        P->d_Y = dalloc<double>(P, n * P->max_nrhs * nb);
+        P->d_U = dalloc<double>(P, P->ulen * nb);
+        P->d_R = dalloc<double>(P, n * P->max_nrhs * nb);
+        P->d_norms = dalloc<double>(P, 2 * P->max_nrhs * nb);
+        if (cudaMallocHost(&P->h_norms, sizeof(double) * 2 * P->max_nrhs * nb) != cudaSuccess)
+            throw BuildError(SDSB200_ALLOC_FAILED, "cudaMallocHost");
+        if (cudaMallocHost(&P->h_info_pinned, sizeof(int64_t) * nb) != cudaSuccess)
+            throw BuildError(SDSB200_ALLOC_FAILED, "cudaMallocHost");
+        cudaMemsetAsync(P->d_psign, 0, n, st);
+        cudaMemsetAsync(P->d_kind, 0, n * nb, st);
+        cudaMemsetAsync(P->d_d, 0, sizeof(double) * 2 * n * nb, st);
+        cudaMemsetAsync(P->d_piv, 0, sizeof(int32_t) * n * nb, st);
+        cudaError_t e = cudaStreamSynchronize(st);
+        if (e != cudaSuccess) throw BuildError(SDSB200_CUDA_ERROR, cudaGetErrorString(e));
+        return P;
+    } catch (const BuildError& be) {
+        free_plan(P);
+        throw PlanError{be.code, be.what()};
+    }
+}
+
+void free_plan(Plan* P) {
+    if (!P) return;
+    for (void* p : P->allocations) cudaFree(p);
+    for (cudaEvent_t e : P->events) cudaEventDestroy(e);
+    if (P->h_norms) cudaFreeHost(P->h_norms);
+    if (P->h_info_pinned) cudaFreeHost(P->h_info_pinned);
+    delete P;
+}
+
+}  // namespace sds

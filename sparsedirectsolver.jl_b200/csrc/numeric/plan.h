@@ -1,0 +1,121 @@
+// The plan of the numeric phase: device copies of the Symbolic maps, the level
+// schedule, the launch program of the factorization and every buffer of the
+// numeric and solve phases (the only allocations; the phases allocate nothing).
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <string>
+#include <vector>
+
+#include "common.cuh"
+#include "kernels.cuh"
+
+namespace sds {
+
+enum BufId : int32_t { BUF_FACTOR = 0, BUF_UFACTOR, BUF_CB, BUF_WORK };
+
+struct ProgLaunch {
+    LaunchKind kind;
+    int32_t level;
+    int32_t count;
+    int32_t cls;       // small: max rows of the class; panel: kb; pivot: -; gemm: -
+    int64_t list;      // offset into the list array of the kind
+    int32_t nb;        // panel block width
+    int32_t maxw;      // scale: widest front
+    BufId abuf, bbuf, cbuf;
+    double flops;      // algorithmic flops of the launch (reference convention for the fronts)
+    double bytes;      // algorithmic device-memory bytes of the launch
+};
+
+// per-kind accounting of the profiling mode (CUDA events around every launch)
+enum ProfKind { PK_SMALL = 0, PK_ASSEMBLE, PK_PANEL, PK_GEMM, PK_PIVOT, PK_SCALE, PK_STATS, PK_FWD, PK_BWD, PK_DIAG,
+                PK_PERMUTE, PK_RESIDUAL, PK_COUNT };
+
+struct ProfAcc {
+    double ms = 0, flops = 0, bytes = 0;
+    int64_t launches = 0;
+};
+
+struct Plan {
+    int64_t n = 0, nnz = 0, ns = 0;
+    int structure = 0, nbatch = 1, precision = 0, elsize = 8, max_nrhs = 1;
+    int64_t factor_len = 0, cb_len = 0, ulen = 0, scr_len = 0, work_len = 0;
+    int nlevels = 0;
+    int fsmall_max = 0;
+    std::vector<DFront> fronts;
+    std::vector<std::vector<int>> level_fronts;
+    std::vector<int> level_maxw;
+    std::vector<double> level_panel_entries;   // stored lower-trapezoid entries of the panels of each level
+    std::vector<int32_t> h_perm0, h_super0;
+    double flops = 0;
+
+    DeviceMaps maps{};
+    DFront* d_fronts = nullptr;
+    int32_t* d_super0 = nullptr;
+    int32_t* d_perm0 = nullptr;
+
+    void* d_factor = nullptr;
+    void* d_ufactor = nullptr;
+    void* d_cb = nullptr;
+    double* d_d = nullptr;
+    int32_t* d_piv = nullptr;
+    int8_t* d_kind = nullptr;
+    int64_t* d_stats = nullptr;
+    int32_t* d_finfo = nullptr;
+    int64_t* d_totals = nullptr;
+    int64_t* d_info = nullptr;
+    int8_t* d_psign = nullptr;
+    int32_t* d_members = nullptr;
+    double* d_scratch = nullptr;
+    void* d_work = nullptr;
+    double* d_amax = nullptr;
+
+    std::vector<ProgLaunch> prog;
+    int32_t* d_lists = nullptr;
+    ColTask* d_coltasks = nullptr;
+    PanelTask* d_ptasks = nullptr;
+    GemmTile* d_tiles = nullptr;
+    int64_t* d_scr_off = nullptr;
+    int64_t* d_woff = nullptr;
+    int64_t* d_uoff = nullptr;
+    int32_t* d_level_lists = nullptr;   // all fronts of each level (solve sweeps)
+    std::vector<int64_t> level_list_off;
+
+    double* d_Y = nullptr;
+    double* d_U = nullptr;
+    double* d_R = nullptr;
+    double* d_norms = nullptr;
+    double* h_norms = nullptr;
+    int64_t* h_info_pinned = nullptr;
+    bool has_full = false;
+    int64_t full_nnz = 0, full_nsrc = 0;
+    int64_t *d_full_rowptr = nullptr, *d_full_colval = nullptr, *d_full_srcptr = nullptr, *d_full_src = nullptr;
+    int64_t *d_fullT_rowptr = nullptr, *d_fullT_colval = nullptr, *d_fullT_srcptr = nullptr, *d_fullT_src = nullptr;
+
+    bool factored = false;
+    int nact = 1;
+    bool all_members = true;
+    const volatile int32_t* interrupt = nullptr;
+    std::vector<void*> allocations;
+    int64_t device_bytes = 0;
+    int launches_factor = 0;
+    int launches_solve = 0;
+    int64_t launches_done = 0;   // kernel launches issued by the last factor / solve calls
+
+    bool profile = false;
+    ProfAcc prof[PK_COUNT];
+    std::vector<cudaEvent_t> events;
+    size_t prof_next = 0;
+    std::vector<std::pair<int, std::pair<double, double>>> pending;  // kind, (flops, bytes) per event pair
+};
+
+struct PlanError {
+    int code;
+    std::string msg;
+};
+
+Plan* build_plan(const sdsb200_symbolic* sym, const sdsb200_plan_options* popts, cudaStream_t stream);
+void free_plan(Plan* p);
+
+}  // namespace sds

@@ -1,0 +1,352 @@
+// Solve phase: permutation of the right-hand sides, level-batched forward,
+// diagonal and backward sweeps over the supernodal factor, and the FP64
+// residual / correction of iterative refinement.
+//
+// Replaces permute_rhs! / unpermute_solution! (src/solve/permute.jl:117-148),
+// forward_sweep! / solve_fwd_kernel! (src/solve/sweeps.jl:438-482, 908-942),
+// diagonal_sweep! / _sv_diag_kernel! (:549-569, 955-969), backward_sweep! /
+// solve_bwd_kernel! (:495-529, 984-1004) and residual! / add_correction!
+// (src/solve/refinement.jl:136-153, 190-209, 229-333).
+//
+// The forward sweep is the deterministic owner-pull variant of the reference
+// (sweeps.jl:250-285): every front writes L21 x into its own update vector and
+// the parent pulls its children's vectors through relind in child order, so
+// the solve is bitwise reproducible without atomics. Right-hand-side vectors
+// are FP64 whatever the factor precision (the FP32 factor is read and widened).
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "common.cuh"
+#include "solve.cuh"
+
+namespace sds {
+
+constexpr int SOLVE_THREADS = 256;
+
+template <typename T>
+__global__ void __launch_bounds__(SOLVE_THREADS) forward_kernel(SweepArgs<T> A) {
+    extern __shared__ double xs[];  // w x nrhs
+    const int s = A.list[blockIdx.x];
+    const int member = A.members ? A.members[blockIdx.y] : blockIdx.y;
+    const DFront fd = A.fronts[s];
+    const int f = fd.f, w = fd.w, m = f - w, nrhs = A.nrhs;
+    const int64_t n = A.n;
+    const T* L = A.fac + (int64_t)member * A.factor_len + fd.panel;
+    double* Y = A.Y + (int64_t)member * n * nrhs;
+    double* U = A.U + (int64_t)member * A.ulen;
+    double* u = m > 0 ? U + A.uoff[s] : nullptr;
+    const int32_t* piv = A.piv ? A.piv + (int64_t)member * n : nullptr;
+    const int tid = threadIdx.x, nt = blockDim.x, lane = tid & 31, warp = tid >> 5, nwarps = nt >> 5;
+    for (int q = tid; q < w * nrhs; q += nt) {
+        int k = q % w, r = q / w;
+        int src = A.reorder ? piv[fd.c0 + k] - 1 : fd.c0 + k;
+        xs[q] = Y[src + (int64_t)r * n];
+    }
+    for (int q = tid; q < m * nrhs; q += nt) u[q] = 0.0;
+    __syncthreads();
+    for (int cq = fd.ch_begin; cq < fd.ch_end; ++cq) {
+        const int c = A.child_list[cq];
+        const DFront cd = A.fronts[c];
+        const int mc = cd.f - cd.w;
+        if (mc <= 0) continue;
+        const double* uc = U + A.uoff[c];
+        const int32_t* ri = A.relind + cd.ri_begin;
+        for (int q = tid; q < mc * nrhs; q += nt) {
+            int i = q % mc, r = q / mc;
+            int p = ri[i];
+            double v = uc[q];
+            if (p < w) xs[p + r * w] -= v;
+            else u[(p - w) + r * m] += v;
+        }
+        __syncthreads();
+    }
+    // L11 solve in blocks of 32 columns: warp 0 solves the block, the CTA updates the rows below it
+    for (int jb = 0; jb < w; jb += 32) {
+        const int bw = min(32, w - jb);
+        if (warp == 0) {
+            for (int r = 0; r < nrhs; ++r) {
+                double val = lane < bw ? xs[jb + lane + r * w] : 0.0;
+                for (int j = 0; j < bw; ++j) {
+                    if (!A.unit && lane == j) val /= (double)L[(jb + j) + (int64_t)(jb + j) * f];
+                    double xj = __shfl_sync(0xffffffffu, val, j);
+                    if (lane > j && lane < bw) val -= (double)L[(jb + lane) + (int64_t)(jb + j) * f] * xj;
+                }
+                if (lane < bw) xs[jb + lane + r * w] = val;
+            }
+        }
+        __syncthreads();
+        for (int q = jb + bw + tid; q < w; q += nt) {
+            double acc[8];
+            for (int r0 = 0; r0 < nrhs; r0 += 8) {
+                const int rc = min(8, nrhs - r0);
+#pragma unroll
+                for (int r = 0; r < 8; ++r) acc[r] = 0.0;
+                for (int j = 0; j < bw; ++j) {
+                    const double l = (double)L[q + (int64_t)(jb + j) * f];
+#pragma unroll
+                    for (int r = 0; r < 8; ++r)
+                        if (r < rc) acc[r] += l * xs[jb + j + (r0 + r) * w];
+                }
+                for (int r = 0; r < rc; ++r) xs[q + (r0 + r) * w] -= acc[r];
+            }
+        }
+        __syncthreads();
+    }
+    // u += L21 x
+    for (int i = tid; i < m; i += nt) {
+        double acc[8];
+        for (int r0 = 0; r0 < nrhs; r0 += 8) {
+            const int rc = min(8, nrhs - r0);
+#pragma unroll
+            for (int r = 0; r < 8; ++r) acc[r] = 0.0;
+            for (int j = 0; j < w; ++j) {
+                const double l = (double)L[w + i + (int64_t)j * f];
+#pragma unroll
+                for (int r = 0; r < 8; ++r)
+                    if (r < rc) acc[r] += l * xs[j + (r0 + r) * w];
+            }
+            for (int r = 0; r < rc; ++r) u[i + (r0 + r) * m] += acc[r];
+        }
+    }
+    for (int q = tid; q < w * nrhs; q += nt) {
+        int k = q % w, r = q / w;
+        Y[fd.c0 + k + (int64_t)r * n] = xs[q];
+    }
+    (void)lane; (void)nwarps;
+}
+
+template <typename T>
+__global__ void __launch_bounds__(SOLVE_THREADS) backward_kernel(SweepArgs<T> A) {
+    extern __shared__ double xs[];  // w x nrhs
+    const int s = A.list[blockIdx.x];
+    const int member = A.members ? A.members[blockIdx.y] : blockIdx.y;
+    const DFront fd = A.fronts[s];
+    const int f = fd.f, w = fd.w, m = f - w, nrhs = A.nrhs;
+    const int64_t n = A.n;
+    const T* L = A.fac + (int64_t)member * A.factor_len + fd.panel;
+    double* Y = A.Y + (int64_t)member * n * nrhs;
+    double* xb = m > 0 ? A.U + (int64_t)member * A.ulen + A.uoff[s] : nullptr;
+    const int32_t* piv = A.piv ? A.piv + (int64_t)member * n : nullptr;
+    const int32_t* rows = A.rowval + fd.row_begin;
+    const int tid = threadIdx.x, nt = blockDim.x, lane = tid & 31, warp = tid >> 5, nwarps = nt >> 5;
+    for (int q = tid; q < w * nrhs; q += nt) {
+        int k = q % w, r = q / w;
+        xs[q] = Y[fd.c0 + k + (int64_t)r * n];
+    }
+    for (int q = tid; q < m * nrhs; q += nt) {
+        int i = q % m, r = q / m;
+        xb[q] = Y[rows[w + i] + (int64_t)r * n];
+    }
+    __syncthreads();
+    // x1 -= L21^T x2: one warp per column
+    for (int j = warp; j < w; j += nwarps) {
+        double acc[8];
+        for (int r0 = 0; r0 < nrhs; r0 += 8) {
+            const int rc = min(8, nrhs - r0);
+#pragma unroll
+            for (int r = 0; r < 8; ++r) acc[r] = 0.0;
+            for (int i = lane; i < m; i += 32) {
+                const double l = (double)L[w + i + (int64_t)j * f];
+#pragma unroll
+                for (int r = 0; r < 8; ++r)
+                    if (r < rc) acc[r] += l * xb[i + (r0 + r) * m];
+            }
+#pragma unroll
+            for (int r = 0; r < 8; ++r) {
+                double v = acc[r];
+                for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+                if (lane == 0 && r < rc) xs[j + (r0 + r) * w] -= v;
+            }
+        }
+    }
+    __syncthreads();
+    // L11^T solve, blocks of 32 from the last
+    const int nblk = (w + 31) / 32;
+    for (int bq = nblk - 1; bq >= 0; --bq) {
+        const int jb = bq * 32, bw = min(32, w - jb);
+        if (warp == 0) {
+            for (int r = 0; r < nrhs; ++r) {
+                double val = lane < bw ? xs[jb + lane + r * w] : 0.0;
+                for (int j = bw - 1; j >= 0; --j) {
+                    if (!A.unit && lane == j) val /= (double)L[(jb + j) + (int64_t)(jb + j) * f];
+                    double xj = __shfl_sync(0xffffffffu, val, j);
+                    if (lane < j) val -= (double)L[(jb + j) + (int64_t)(jb + lane) * f] * xj;
+                }
+                if (lane < bw) xs[jb + lane + r * w] = val;
+            }
+        }
+        __syncthreads();
+        for (int i = warp; i < jb; i += nwarps) {
+            const double l = lane < bw ? (double)L[(jb + lane) + (int64_t)i * f] : 0.0;
+            for (int r = 0; r < nrhs; ++r) {
+                double v = lane < bw ? l * xs[jb + lane + r * w] : 0.0;
+                for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+                if (lane == 0) xs[i + r * w] -= v;
+            }
+        }
+        __syncthreads();
+    }
+    for (int q = tid; q < w * nrhs; q += nt) {
+        int k = q % w, r = q / w;
+        int dst = A.reorder ? piv[fd.c0 + k] - 1 : fd.c0 + k;
+        Y[dst + (int64_t)r * n] = xs[q];
+    }
+}
+
+template <typename T>
+cudaError_t launch_sweep(bool forward, const SweepArgs<T>& a, int nmembers, int maxw, cudaStream_t st) {
+    if (a.count == 0) return cudaSuccess;
+    size_t smem = (size_t)maxw * a.nrhs * sizeof(double);
+    dim3 grid(a.count, nmembers);
+    cudaError_t e;
+    if (forward) {
+        e = cudaFuncSetAttribute(forward_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        if (e != cudaSuccess) return e;
+        forward_kernel<T><<<grid, SOLVE_THREADS, smem, st>>>(a);
+    } else {
+        e = cudaFuncSetAttribute(backward_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        if (e != cudaSuccess) return e;
+        backward_kernel<T><<<grid, SOLVE_THREADS, smem, st>>>(a);
+    }
+    return cudaGetLastError();
+}
+
+template cudaError_t launch_sweep<double>(bool, const SweepArgs<double>&, int, int, cudaStream_t);
+template cudaError_t launch_sweep<float>(bool, const SweepArgs<float>&, int, int, cudaStream_t);
+
+// D^{-1} (1x1 and 2x2 blocks, d[k], d[n + k], d[k + 1]) -- _sv_diag_kernel! sweeps.jl:549-569
+__global__ void diag_kernel(DiagArgs A) {
+    const int member = A.members ? A.members[blockIdx.y] : blockIdx.y;
+    const int64_t n = A.n;
+    const double* d = A.d + (int64_t)member * 2 * n;
+    const int8_t* kind = A.kind + (int64_t)member * n;
+    double* Y = A.Y + (int64_t)member * n * A.nrhs;
+    for (int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; q < n * A.nrhs; q += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t k = q % n, r = q / n;
+        const int kk = kind[k];
+        if (A.two && kk == KIND_2X2_SECOND) continue;
+        if (A.two && kk == KIND_2X2_FIRST) {
+            double a = d[k], b = d[n + k], c = d[k + 1];
+            double det = a * c - b * b;
+            double y1 = Y[k + r * n], y2 = Y[k + 1 + r * n];
+            Y[k + r * n] = (c * y1 - b * y2) / det;
+            Y[k + 1 + r * n] = (a * y2 - b * y1) / det;
+        } else {
+            Y[k + r * n] /= d[k];
+        }
+    }
+}
+
+cudaError_t launch_diag(const DiagArgs& a, int nmembers, cudaStream_t st) {
+    int64_t work = a.n * a.nrhs;
+    int blocks = (int)std::min<int64_t>((work + 255) / 256, 4096);
+    dim3 grid(blocks > 0 ? blocks : 1, nmembers);
+    diag_kernel<<<grid, 256, 0, st>>>(a);
+    return cudaGetLastError();
+}
+
+// Y[k, r] = B[perm[k], r] (mode 0); X[perm[k], r] = Y[k, r] (mode 1); X[perm[k], r] += Y[k, r] (mode 2)
+__global__ void permute_kernel(PermArgs A) {
+    const int member = A.members ? A.members[blockIdx.y] : blockIdx.y;
+    const int64_t n = A.n;
+    double* Y = A.Y + (int64_t)member * n * A.nrhs;
+    for (int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; q < n * A.nrhs; q += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t k = q % n, r = q / n;
+        const int64_t g = A.perm[k];
+        if (A.mode == 0) {
+            Y[q] = A.in[member * A.ldin * A.nrhs + g + r * A.ldin];
+        } else if (A.mode == 1) {
+            A.out[member * A.ldout * A.nrhs + g + r * A.ldout] = Y[q];
+        } else {
+            A.out[member * A.ldout * A.nrhs + g + r * A.ldout] += Y[q];
+        }
+    }
+}
+
+cudaError_t launch_permute(const PermArgs& a, int nmembers, cudaStream_t st) {
+    int64_t work = a.n * a.nrhs;
+    int blocks = (int)std::min<int64_t>((work + 255) / 256, 4096);
+    dim3 grid(blocks > 0 ? blocks : 1, nmembers);
+    permute_kernel<<<grid, 256, 0, st>>>(a);
+    return cudaGetLastError();
+}
+
+// R = B - op(A) X over the full-pattern map (duplicates summed in source order); one warp per row
+__global__ void residual_kernel(ResidualArgs A) {
+    const int member = A.members ? A.members[blockIdx.y] : blockIdx.y;
+    const int64_t n = A.n;
+    const double* nz = A.nzval + (int64_t)member * A.nnz;
+    const double* X = A.X + (int64_t)member * A.ldx * A.nrhs;
+    const double* B = A.B + (int64_t)member * A.ldb * A.nrhs;
+    double* R = A.R + (int64_t)member * n * A.nrhs;
+    const int lane = threadIdx.x & 31;
+    const int64_t warp = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
+    const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
+    for (int64_t i = warp; i < n; i += nw) {
+        for (int r0 = 0; r0 < A.nrhs; r0 += 8) {
+            const int rc = min(8, A.nrhs - r0);
+            double acc[8];
+#pragma unroll
+            for (int r = 0; r < 8; ++r) acc[r] = 0.0;
+            for (int64_t e = A.rowptr[i] + lane; e < A.rowptr[i + 1]; e += 32) {
+                double v = 0.0;
+                for (int64_t q = A.srcptr[e]; q < A.srcptr[e + 1]; ++q) v += nz[A.src[q]];
+                const int64_t c = A.colval[e];
+#pragma unroll
+                for (int r = 0; r < 8; ++r)
+                    if (r < rc) acc[r] += v * X[c + (int64_t)(r0 + r) * A.ldx];
+            }
+#pragma unroll
+            for (int r = 0; r < 8; ++r) {
+                double v = acc[r];
+                for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+                if (lane == 0 && r < rc) R[i + (int64_t)(r0 + r) * n] = B[i + (int64_t)(r0 + r) * A.ldb] - v;
+            }
+        }
+    }
+}
+
+cudaError_t launch_residual(const ResidualArgs& a, int nmembers, cudaStream_t st) {
+    int64_t warps = a.n;
+    int blocks = (int)std::min<int64_t>((warps * 32 + 255) / 256, 8192);
+    dim3 grid(blocks > 0 ? blocks : 1, nmembers);
+    residual_kernel<<<grid, 256, 0, st>>>(a);
+    return cudaGetLastError();
+}
+
+// ||R_k||^2 and ||B_k||^2 per (member, rhs): one CTA each
+__global__ void norms_kernel(NormArgs A) {
+    const int col = blockIdx.x;  // member-major: col = j * nrhs + r over the active members
+    const int j = col / A.nrhs, r = col % A.nrhs;
+    const int member = A.members ? A.members[j] : j;
+    const int64_t n = A.n;
+    const double* R = A.R + (int64_t)member * n * A.nrhs + (int64_t)r * n;
+    const double* B = A.B + (int64_t)member * A.ldb * A.nrhs + (int64_t)r * A.ldb;
+    __shared__ double sr[256], sb[256];
+    double ar = 0.0, ab = 0.0;
+    for (int64_t i = threadIdx.x; i < n; i += blockDim.x) {
+        ar += R[i] * R[i];
+        ab += B[i] * B[i];
+    }
+    sr[threadIdx.x] = ar;
+    sb[threadIdx.x] = ab;
+    __syncthreads();
+    for (int h = 128; h > 0; h >>= 1) {
+        if (threadIdx.x < h) {
+            sr[threadIdx.x] += sr[threadIdx.x + h];
+            sb[threadIdx.x] += sb[threadIdx.x + h];
+        }
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+        A.out[2 * col] = sr[0];
+        A.out[2 * col + 1] = sb[0];
+    }
+}
+
+cudaError_t launch_norms(const NormArgs& a, int ncols, cudaStream_t st) {
+    norms_kernel<<<ncols, 256, 0, st>>>(a);
+    return cudaGetLastError();
+}
+
+}  // namespace sds

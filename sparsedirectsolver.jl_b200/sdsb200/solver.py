@@ -1,0 +1,392 @@
+"""DirectSolver: the reference's handle API over the B200 numeric phase.
+
+Mirrors SparseDirectSolver.jl's ``DirectSolver`` / ``execute!`` / ``setparam!``
+/ ``getparam`` (src/solver.jl:187-259, 444-460, 1013-1194): the same phase
+strings ("analysis", "factorization", "refactorization", "solve",
+"solve_refinement"), structures ("SPD", "S", "G"), parameter names and
+error classes (src/errors.jl). Analysis runs on the host
+(libsdsb200_analysis.so); factorization and solve run on the GPU through the C
+ABI of libsdsb200.so, with torch used only to hold device memory. There is no
+CPU fallback: without the CUDA library or a device every phase raises.
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+
+from . import capi
+from ._native import numeric_lib
+from .analysis import analyze
+
+
+class SparseDirectSolverError(Exception):
+    pass
+
+
+class InvalidValueError(SparseDirectSolverError):
+    pass
+
+
+class NotSupportedError(SparseDirectSolverError):
+    pass
+
+
+class FactorizationError(SparseDirectSolverError):
+    pass
+
+
+class InterruptedError_(SparseDirectSolverError):
+    pass
+
+
+_ERRORS = {capi.INVALID_VALUE: InvalidValueError, capi.NOT_SUPPORTED: NotSupportedError,
+           capi.PHASE_ORDER: FactorizationError, capi.INTERRUPTED: InterruptedError_}
+
+_DEFAULTS = {
+    "reordering_alg": "default", "factorization_alg": "default", "solve_alg": "default", "matching_alg": "default",
+    "solve_mode": 0, "ir_n_steps": 0, "ir_tol": 0.0, "pivot_type": "A", "pivot_threshold": 0.01,
+    "pivot_epsilon": None, "pivot_epsilon_alg": "default", "deterministic_mode": 0, "ubatch_size": 0,
+    "ubatch_index": -1, "use_superpanels": 1, "ir_mode": "plain", "factor_precision": None,
+    "amalgamation": (32, 0.25, 8), "pivot_pairs": "default", "pivot_pair_tolerance": 1e-6, "user_perm": None,
+    "pivot_sign": None, "user_host_interrupt": None, "max_nrhs": 8,
+}
+
+
+def _check(rc, lib):
+    if rc != capi.OK:
+        msg = lib.sdsb200_last_error().decode()
+        raise _ERRORS.get(rc, RuntimeError)(msg)
+
+
+def _i32(a):
+    return np.ascontiguousarray(a, dtype=np.int32)
+
+
+class DirectSolver:
+    """``DirectSolver(A, structure, view)`` for a square CSR matrix.
+
+    ``A`` is a scipy CSR matrix (0-based) or a tuple ``(rowptr, colval, nzval, n)``
+    with ``index_base`` 0 or 1. ``nzval`` may hold ``nnz * nbatch`` values
+    (a uniform batch, member-major), as a numpy array or a CUDA torch tensor.
+    """
+
+    def __init__(self, A, structure="SPD", view="F", index_base=0, device="cuda:0", **params):
+        import torch  # device memory only
+
+        self._torch = torch
+        if structure not in ("SPD", "S", "G"):
+            raise InvalidValueError(f'structure must be "G", "S" or "SPD", got {structure!r}')
+        if view not in ("L", "U", "F"):
+            raise InvalidValueError(f"view must be 'L', 'U' or 'F', got {view!r}")
+        if isinstance(A, tuple):
+            rowptr, colval, nzval, n = A
+        else:
+            A = A.tocsr()
+            if A.shape[0] != A.shape[1]:
+                raise InvalidValueError(f"the matrix must be square, got {A.shape}")
+            rowptr, colval, nzval, n = A.indptr, A.indices, A.data, A.shape[0]
+            index_base = 0
+        self.n = int(n)
+        self.rowptr = np.asarray(rowptr, dtype=np.int64)
+        self.colval = np.asarray(colval, dtype=np.int64)
+        self.nnz = int(self.colval.size)
+        self.structure = structure
+        self.view = view
+        self.index_base = int(index_base)
+        self.device = torch.device(device)
+        self.params = dict(_DEFAULTS)
+        for k, v in params.items():
+            self.setparam(k, v)
+        self._set_values(nzval)
+        self.symbolic = None
+        self._plan = None
+        self._stage = 0           # 0 created, 1 analyzed, 2 factorized
+        self._info = np.zeros(self.nbatch, dtype=np.int64)
+        self._ir_steps = -1
+        self._keep = []
+
+    # -- values ------------------------------------------------------------------------------------------------
+    def _set_values(self, nzval):
+        torch = self._torch
+        if isinstance(nzval, torch.Tensor):
+            t = nzval.to(self.device, torch.float64).reshape(-1).contiguous()
+        else:
+            t = torch.from_numpy(np.ascontiguousarray(nzval, dtype=np.float64).reshape(-1)).to(self.device)
+        if self.nnz == 0 or t.numel() % self.nnz != 0:
+            if not (self.nnz == 0 and t.numel() == 0):
+                raise InvalidValueError(f"nzval has {t.numel()} entries, not a multiple of nnz = {self.nnz}")
+        self.nbatch = max(1, t.numel() // max(self.nnz, 1))
+        self.nzval = t
+
+    def update(self, nzval):
+        """``update!``: new values with the same pattern (src/solver.jl:309-330)."""
+        old = self.nbatch
+        self._set_values(nzval)
+        if self._plan is not None and self.nbatch != old:
+            raise InvalidValueError("the number of batch members changed; run the analysis again")
+
+    # -- parameters -------------------------------------------------------------------------------------------
+    def setparam(self, name, value):
+        if name not in _DEFAULTS:
+            raise InvalidValueError(f"unknown parameter {name!r}")
+        if name == "pivot_type" and value not in capi.PIVOT_TYPE:
+            raise InvalidValueError(f"pivot_type must be one of {sorted(capi.PIVOT_TYPE)}")
+        if name == "pivot_type" and value in ("C", "R"):
+            raise NotSupportedError("global pivoting ('C', 'R') is not supported")
+        if name == "pivot_threshold" and not (np.isfinite(value) and value >= 0):
+            raise InvalidValueError("pivot_threshold must be finite and nonnegative")
+        if name == "ir_n_steps" and int(value) < 0:
+            raise InvalidValueError("ir_n_steps must be nonnegative")
+        if name == "solve_mode" and int(value) not in (0, 1, 2):
+            raise InvalidValueError("solve_mode must be 0, 1 or 2")
+        if name == "ir_mode" and value not in ("plain",):
+            raise NotSupportedError(f"ir_mode {value!r} is not supported (plain iterative refinement only)")
+        if name == "factor_precision" and value not in (None, "fp64", "fp32", "float64", "float32"):
+            raise InvalidValueError("factor_precision must be fp64 or fp32")
+        if name == "pivot_sign" and value is not None:
+            value = np.asarray(value, dtype=np.int8)
+            if value.size != self.n if hasattr(self, "n") else False:
+                raise InvalidValueError(f"pivot_sign has {value.size} entries, the matrix has {self.n} rows")
+        if name == "ubatch_index" and self._plan_exists():
+            self._apply_members(int(value))
+        self.params[name] = value
+
+    def _plan_exists(self):
+        return getattr(self, "_plan", None) is not None
+
+    def getparam(self, name):
+        lib = numeric_lib()
+        if name == "info":
+            return int(self._info[0]) if self.nbatch == 1 else self._info.copy()
+        if name == "ir_n_steps" and self._ir_steps >= 0:
+            return self._ir_steps
+        if name in ("perm_reorder_row", "perm_reorder_col", "perm_col"):
+            self._need(1, name)
+            return self.symbolic.perm.copy()
+        if name == "perm_row":
+            self._need(1, name)
+            if self.structure == "G" and self._stage >= 2:
+                piv = np.zeros(self.n, np.int32)
+                _check(lib.sdsb200_get_pivots(self._plan, 0, piv.ctypes.data, None, None), lib)
+                return self.symbolic.perm[piv - 1]
+            return self.symbolic.perm.copy()
+        if name in ("lu_nnz", "flops", "nsuperpanels"):
+            self._need(1, name)
+            return {"lu_nnz": self.symbolic.nnz_L, "flops": self.symbolic.flops, "nsuperpanels": self.symbolic.ns}[name]
+        if name in ("inertia", "npivots", "pivot_stats"):
+            self._need(2, name)
+            out = []
+            for k in range(self.nbatch):
+                tot = np.zeros(6, np.int64)
+                _check(lib.sdsb200_get_stats(self._plan, k, None, tot.ctypes.data), lib)
+                st = dict(npos=int(tot[0]), nneg=int(tot[1]), nzero=int(tot[2]), nperturbed=int(tot[3]),
+                          n2x2=int(tot[4]))
+                out.append(st["nperturbed"] if name == "npivots" else
+                           (st["npos"], st["nneg"]) if name == "inertia" else st)
+            return out[0] if self.nbatch == 1 else out
+        if name == "diag":
+            self._need(2, name)
+            return self.factor_diag()
+        if name in self.params:
+            return self.params[name]
+        raise InvalidValueError(f"unknown parameter {name!r}")
+
+    def _need(self, stage, name):
+        if self._stage < stage:
+            raise FactorizationError(f"{name!r} is not available before the "
+                                     f"{'analysis' if stage == 1 else 'factorization'}")
+
+    # -- phases -----------------------------------------------------------------------------------------------
+    def execute(self, phase, X=None, B=None):
+        """``execute!(phase, solver, X, B)``."""
+        if phase in ("reordering", "symbolic_factorization", "analysis"):
+            return self._analysis()
+        if phase in ("factorization", "refactorization"):
+            return self._factorize(refactor=phase == "refactorization")
+        if phase in ("solve", "solve_refinement", "solve_fwd_perm", "solve_fwd", "solve_diag", "solve_bwd",
+                     "solve_bwd_perm"):
+            if phase not in ("solve", "solve_refinement"):
+                raise NotSupportedError(f"phase {phase!r}: only the complete solve is exposed")
+            return self._solve(X, B)
+        raise InvalidValueError(f"unknown phase {phase!r}")
+
+    def _opts(self):
+        o = capi.Opts()
+        lib = numeric_lib()
+        lib.sdsb200_default_opts(C.byref(o))
+        p = self.params
+        o.pivot_type = capi.PIVOT_TYPE[p["pivot_type"]]
+        o.pivot_threshold = float(p["pivot_threshold"])
+        o.pivot_epsilon = -1.0 if p["pivot_epsilon"] is None else float(p["pivot_epsilon"])
+        o.pivot_epsilon_alg = 1 if p["pivot_epsilon_alg"] == "algo1" else 0
+        o.ir_n_steps = int(p["ir_n_steps"])
+        o.ir_tol = float(p["ir_tol"])
+        o.solve_mode = int(p["solve_mode"])
+        o.deterministic_mode = int(p["deterministic_mode"])
+        return o
+
+    def _precision(self):
+        fp = self.params["factor_precision"]
+        return 1 if fp in ("fp32", "float32") else 0
+
+    def _analysis(self):
+        p = self.params
+        nz_host = self.nzval[: self.nnz].cpu().numpy() if self.structure == "S" else None
+        self.symbolic = analyze(self.rowptr, self.colval, self.n, self.structure, nzval=nz_host, view=self.view,
+                                index_base=self.index_base, reordering=p["reordering_alg"],
+                                user_perm=p["user_perm"], pivot_pairs=p["pivot_pairs"],
+                                pivot_pair_tolerance=p["pivot_pair_tolerance"],
+                                pivot_threshold=p["pivot_threshold"], use_superpanels=p["use_superpanels"],
+                                amalgamation=tuple(p["amalgamation"]))
+        self._create_plan()
+        self._stage = 1
+
+    def _create_plan(self):
+        lib = numeric_lib()
+        if self._plan is not None:
+            lib.sdsb200_plan_destroy(self._plan)
+            self._plan = None
+        S = self.symbolic
+        keep = {}
+        sym = capi.Symbolic()
+        sym.n, sym.nnz, sym.ns = S.n, S.nnz, S.ns
+        sym.index_width = 8
+        sym.structure = capi.STRUCTURE[self.structure]
+        for nm in ("perm", "super_ptr", "snparent", "rowptr", "rowval", "front_ptr", "child_ptr", "child_list",
+                   "relind_ptr", "relind", "amap", "amap_ptr", "amap_src", "full_rowptr", "full_colval",
+                   "full_srcptr", "full_src"):
+            a = np.ascontiguousarray(getattr(S, nm), dtype=np.int64)
+            if a.size == 0:
+                a = np.zeros(1, np.int64)
+            keep[nm] = a
+            setattr(sym, nm, a.ctypes.data)
+        sym.full_nnz = int(S.full_colval.size)
+        sym.full_nsrc = int(S.full_src.size)
+        po = capi.PlanOptions(nbatch=self.nbatch, precision=self._precision(), max_nrhs=int(self.params["max_nrhs"]))
+        plan = C.c_void_p()
+        stream = self._torch.cuda.current_stream(self.device).cuda_stream
+        _check(lib.sdsb200_plan_create(C.byref(plan), C.byref(sym), C.byref(po), C.c_void_p(stream)), lib)
+        self._plan = plan
+        if int(self.params["ubatch_index"]) >= 0:
+            self._apply_members(int(self.params["ubatch_index"]))
+        if self.params["user_host_interrupt"] is not None:
+            flag = self.params["user_host_interrupt"]
+            lib.sdsb200_set_interrupt(self._plan, C.addressof(flag))
+
+    def _apply_members(self, index):
+        lib = numeric_lib()
+        if index < 0:
+            _check(lib.sdsb200_set_members(self._plan, None, -1), lib)
+        else:
+            if index >= self.nbatch:
+                raise InvalidValueError(f"ubatch_index {index} outside 0:{self.nbatch - 1}")
+            m = np.array([index], np.int32)
+            _check(lib.sdsb200_set_members(self._plan, m.ctypes.data, 1), lib)
+
+    def _factorize(self, refactor=False):
+        if self._stage < 1:
+            raise FactorizationError("factorization before analysis")
+        lib = numeric_lib()
+        ps = self.params["pivot_sign"]
+        ps_arr = None if ps is None else np.ascontiguousarray(ps, dtype=np.int8)
+        info = np.zeros(self.nbatch, np.int64)
+        stream = self._torch.cuda.current_stream(self.device).cuda_stream
+        o = self._opts()
+        rc = lib.sdsb200_factor(self._plan, C.c_void_p(self.nzval.data_ptr()),
+                                ps_arr.ctypes.data if ps_arr is not None else None, C.byref(o), info.ctypes.data,
+                                C.c_void_p(stream))
+        if rc == capi.INTERRUPTED:
+            self._stage = 1
+        _check(rc, lib)
+        self._info = info
+        self._stage = 2
+        return int(info[0]) if self.nbatch == 1 else info
+
+    def _solve(self, X, B):
+        torch = self._torch
+        if self._stage < 2:
+            raise FactorizationError("solve before factorization")
+        lib = numeric_lib()
+        n = self.n
+        vec = B.dim() == 1 if isinstance(B, torch.Tensor) else np.asarray(B).ndim == 1
+        Bt = B if isinstance(B, torch.Tensor) else torch.from_numpy(np.asarray(B, dtype=np.float64))
+        Bt = Bt.to(self.device, torch.float64)
+        Bm = Bt.reshape(n, -1) if vec or self.nbatch == 1 else Bt.reshape(self.nbatch, n, -1)
+        # column-major storage: (members, nrhs, n) contiguous
+        if Bm.dim() == 2:
+            Bcm = Bm.t().contiguous()
+            nrhs = Bm.shape[1]
+        else:
+            Bcm = Bm.transpose(1, 2).contiguous()
+            nrhs = Bm.shape[2]
+        Xcm = torch.empty_like(Bcm)
+        o = self._opts()
+        steps = C.c_int32(0)
+        stream = torch.cuda.current_stream(self.device).cuda_stream
+        _check(lib.sdsb200_solve(self._plan, C.c_void_p(Xcm.data_ptr()), n, C.c_void_p(Bcm.data_ptr()), n, nrhs,
+                                 C.c_void_p(self.nzval.data_ptr()), C.byref(o), C.byref(steps),
+                                 C.c_void_p(stream)), lib)
+        self._ir_steps = int(steps.value) if o.ir_n_steps > 0 else -1
+        out = Xcm.t() if Xcm.dim() == 2 else Xcm.transpose(1, 2)
+        out = out.reshape(Bt.shape)
+        if X is not None:
+            if isinstance(X, torch.Tensor):
+                X.copy_(out)
+                return X
+            np.copyto(X, out.cpu().numpy())
+            return X
+        return out
+
+    # -- outputs for tests -------------------------------------------------------------------------------------
+    def factor_host(self, member=0):
+        """Panels as host FP64 arrays (factor, ufactor or None), the reference's ``host_numeric``."""
+        lib = numeric_lib()
+        flen = self.symbolic.factor_len
+        fac = np.zeros(max(flen, 1))
+        ufac = np.zeros(max(flen, 1)) if self.structure == "G" else None
+        _check(lib.sdsb200_get_factor(self._plan, member, fac.ctypes.data,
+                                      ufac.ctypes.data if ufac is not None else None), lib)
+        return fac, ufac
+
+    def pivots_host(self, member=0):
+        lib = numeric_lib()
+        piv = np.zeros(max(self.n, 1), np.int32)
+        kind = np.zeros(max(self.n, 1), np.int8)
+        d = np.zeros(max(2 * self.n, 1))
+        _check(lib.sdsb200_get_pivots(self._plan, member, piv.ctypes.data, kind.ctypes.data, d.ctypes.data), lib)
+        return piv, kind, d
+
+    def stats_host(self, member=0):
+        lib = numeric_lib()
+        st = np.zeros(max(6 * self.symbolic.ns, 1), np.int64)
+        _check(lib.sdsb200_get_stats(self._plan, member, st.ctypes.data, None), lib)
+        return st[: 6 * self.symbolic.ns].reshape(-1, 6)
+
+    def factor_diag(self, member=0):
+        """``getparam("diag")``: diagonal of L (Cholesky) or of D (LDLT, LU) in factor order."""
+        fac, _ = self.factor_host(member)
+        if self.structure == "SPD":
+            S = self.symbolic
+            out = np.zeros(self.n)
+            for s in range(S.ns):
+                f, w, base, c0 = (int(S.front_nrows[s]), int(S.front_ncols[s]), int(S.front_ptr[s]) - 1,
+                                  int(S.super_ptr[s]) - 1)
+                for j in range(w):
+                    out[c0 + j] = fac[base + j * f + j]
+            return out
+        return self.pivots_host(member)[2][: self.n].copy()
+
+    def plan_stat(self, name):
+        return numeric_lib().sdsb200_plan_stat(self._plan, name.encode())
+
+    def close(self):
+        if self._plan is not None:
+            numeric_lib().sdsb200_plan_destroy(self._plan)
+            self._plan = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

@@ -1,0 +1,230 @@
+"""Parity of the B200 numeric phase with the CPU oracle (GPU).
+
+Pattern of the reference's own device tests (test/utils.jl:357-369, 620-630,
+797-808): analyse once, factor with the CPU oracle and on the device from the
+same Symbolic, then compare exactly what must be exact (pivot order, pivot
+kinds, per-front statistics, inertia, info) and the values within a growth
+tolerance; solves must reach a scaled backward error <= 1e-12.
+"""
+import numpy as np
+import pytest
+import scipy.sparse as sp
+
+from helpers import dense_panels, eigen_inertia, oracle_for, rel_max_diff, small_kkt
+from sdsb200 import matrices as M
+
+pytestmark = pytest.mark.gpu
+
+FP64_TOL = 1e-10   # panels / D relative to max(1, max|entry|)
+BERR = 1e-12       # scaled backward error of every FP64 solve
+
+
+@pytest.fixture(scope="module")
+def torch_cuda():
+    torch = pytest.importorskip("torch")
+    if not torch.cuda.is_available():
+        pytest.fail("CUDA device required for -m gpu tests")
+    return torch
+
+
+def _solver(A, structure, **params):
+    from sdsb200.solver import DirectSolver
+
+    return DirectSolver(A, structure, **params)
+
+
+def _check_factor(A, structure, torch_cuda, okw=None, **params):
+    okw = okw or {}
+    S, O, info = oracle_for(A, structure, reordering=params.get("reordering_alg", "default"), **okw)
+    ds = _solver(A, structure, **params)
+    ds.execute("analysis")
+    assert np.array_equal(ds.symbolic.perm, S.perm)
+    dinfo = ds.execute("factorization")
+    assert dinfo == info
+    fac, ufac = ds.factor_host()
+    assert rel_max_diff(dense_panels(S, fac), dense_panels(S, O.factor)) <= FP64_TOL
+    if structure == "G":
+        assert rel_max_diff(dense_panels(S, ufac), dense_panels(S, O.ufactor)) <= FP64_TOL
+    if structure != "SPD":
+        piv, kind, d = ds.pivots_host()
+        assert np.array_equal(piv[: S.n], O.piv[: S.n])
+        assert np.array_equal(kind[: S.n], O.kind[: S.n])
+        assert rel_max_diff(d[: 2 * S.n], O.d[: 2 * S.n]) <= FP64_TOL
+    st = ds.stats_host()
+    assert np.array_equal(st, O.stats_matrix())
+    return ds, S, O
+
+
+def _check_solve(ds, A, nrhs=1, transpose=False):
+    b = M.rhs(A.shape[0], nrhs, seed=1)
+    if transpose:
+        ds.setparam("solve_mode", 1)
+    x = ds.execute("solve", None, b if nrhs > 1 else b[:, 0]).cpu().numpy()
+    AA = A.T.tocsr() if transpose else A
+    err = M.scaled_backward_error(AA, x.reshape(A.shape[0], -1), b)
+    if transpose:
+        ds.setparam("solve_mode", 0)
+    return err
+
+
+@pytest.mark.parametrize("reordering", ["amd", "nd"])
+def test_cholesky_lap2d_64(torch_cuda, reordering):
+    A = M.lap2d_shifted(64, 64, seed=0)
+    ds, S, O = _check_factor(A, "SPD", torch_cuda, reordering_alg=reordering)
+    assert _check_solve(ds, A, 1) <= BERR
+    assert _check_solve(ds, A, 3) <= BERR
+
+
+def test_cholesky_large_fronts(torch_cuda):
+    # 3-D grid: the top separators exceed the shared-memory fronts (large-front dense path)
+    A = M.lap3d(18, 18, 18, shift=0.05, seed=3)
+    ds, S, O = _check_factor(A, "SPD", torch_cuda, reordering_alg="nd")
+    assert int(S.front_nrows.max()) > 160
+    assert _check_solve(ds, A, 4) <= BERR
+
+
+def test_cholesky_refactorization_bitwise(torch_cuda):
+    A = M.lap3d(14, 14, 14, seed=1)
+    ds = _solver(A, "SPD", reordering_alg="nd")
+    ds.execute("analysis")
+    ds.execute("factorization")
+    f1, _ = ds.factor_host()
+    ds.execute("refactorization")
+    f2, _ = ds.factor_host()
+    assert np.array_equal(f1, f2)
+    b = M.rhs(A.shape[0], 2, seed=4)
+    x1 = ds.execute("solve", None, b).cpu().numpy()
+    x2 = ds.execute("solve", None, b).cpu().numpy()
+    assert np.array_equal(x1, x2)
+
+
+def test_cholesky_failure_info(torch_cuda):
+    A = M.lap2d_shifted(20, 20, seed=0).tolil()
+    A[57, 57] = -5.0
+    A = A.tocsr()
+    S, O, info = oracle_for(A, "SPD", pivot_epsilon=0.0)
+    assert info > 0
+    ds = _solver(A, "SPD", pivot_epsilon=0.0)
+    ds.execute("analysis")
+    assert ds.execute("factorization") == info
+
+
+@pytest.mark.parametrize("nx,nj", [(20, 150), (30, 400)])
+def test_ldlt_kkt(torch_cuda, nx, nj):
+    A = small_kkt(nx, nx, nj, seed=2)
+    ds, S, O = _check_factor(A, "S", torch_cuda)
+    inertia = ds.getparam("inertia")
+    assert inertia == (nx * nx, nj)
+    if A.shape[0] <= 2000:
+        assert inertia == eigen_inertia(A)
+    assert _check_solve(ds, A, 1) <= BERR
+
+
+def test_ldlt_large_fronts_and_2x2(torch_cuda):
+    # one dense front: BK with 2x2 pivots on the global-memory path
+    A = small_kkt(14, 14, 90, seed=5)
+    big = dict(amalgamation=(10_000, 100.0, 10_000))
+    S, O, info = oracle_for(A, "S", amalgamation=big["amalgamation"])
+    ds = _solver(A, "S", **big)
+    ds.execute("analysis")
+    assert ds.execute("factorization") == info
+    piv, kind, d = ds.pivots_host()
+    assert np.array_equal(piv[: S.n], O.piv[: S.n])
+    assert np.array_equal(kind[: S.n], O.kind[: S.n])
+    assert np.array_equal(ds.stats_host(), O.stats_matrix())
+    fac, _ = ds.factor_host()
+    assert rel_max_diff(dense_panels(S, fac), dense_panels(S, O.factor)) <= FP64_TOL
+    assert ds.getparam("inertia") == eigen_inertia(A)
+    assert _check_solve(ds, A, 2) <= BERR
+
+
+def test_ldlt_pivot_sign_and_zero_pivot(torch_cuda):
+    # a structurally singular diagonal block with epsilon = 0: info of the failed pivot
+    A = sp.csr_matrix(np.array([[4.0, 1, 0, 0], [1, 3, 0, 0], [0, 0, 0, 0], [0, 0, 0, 2]]))
+    A = A + sp.csr_matrix((np.zeros(1), ([2], [2])), shape=(4, 4))
+    A.sort_indices()
+    S, O, info = oracle_for(A, "S", pivot_epsilon=0.0, pivot_pairs="none")
+    ds = _solver(A, "S", pivot_epsilon=0.0, pivot_pairs="none")
+    ds.execute("analysis")
+    assert ds.execute("factorization") == info != 0
+    # with epsilon > 0 and a requested sign the pivot is perturbed to -eps
+    psign = np.zeros(4, np.int8)
+    psign[2] = -1
+    S2, O2, info2 = oracle_for(A, "S", pivot_epsilon=1e-8, pivot_sign=psign, pivot_pairs="none")
+    ds2 = _solver(A, "S", pivot_epsilon=1e-8, pivot_sign=psign, pivot_pairs="none")
+    ds2.execute("analysis")
+    assert ds2.execute("factorization") == info2 == 0
+    assert ds2.getparam("npivots") == 1
+    piv, kind, d = ds2.pivots_host()
+    assert np.array_equal(kind[:4], O2.kind[:4])
+    assert np.allclose(d[:8], O2.d[:8])
+
+
+@pytest.mark.parametrize("g", [10, 16])
+def test_lu_convection_diffusion(torch_cuda, g):
+    A = M.convection_diffusion3d(g, g, g, seed=g)
+    ds, S, O = _check_factor(A, "G", torch_cuda, okw=dict(pivot_threshold=0.1), pivot_threshold=0.1,
+                             reordering_alg="nd")
+    perm_row = ds.getparam("perm_row")
+    assert np.array_equal(perm_row, S.perm[O.piv[: S.n] - 1])
+    assert np.array_equal(ds.getparam("perm_col"), S.perm)
+    assert _check_solve(ds, A, 2) <= BERR
+    assert _check_solve(ds, A, 2, transpose=True) <= BERR
+
+
+def test_lu_row_swaps(torch_cuda):
+    # weak diagonal: threshold pivoting must swap rows inside the fully-summed block
+    rng = np.random.default_rng(7)
+    A = M.convection_diffusion3d(8, 8, 8, seed=7).tolil()
+    for i in range(0, A.shape[0], 5):
+        A[i, i] = 0.05 * rng.uniform()
+    A = A.tocsr()
+    A.sort_indices()
+    ds, S, O = _check_factor(A, "G", torch_cuda, okw=dict(pivot_threshold=0.5), pivot_threshold=0.5)
+    piv = O.piv[: S.n]
+    assert (piv != np.arange(1, S.n + 1)).any()
+    assert _check_solve(ds, A, 1) <= BERR
+
+
+def test_refinement_fp32_factor(torch_cuda):
+    A = M.lap3d(16, 16, 16, seed=2)
+    ds = _solver(A, "SPD", reordering_alg="nd", factor_precision="fp32", ir_n_steps=10, ir_tol=1e-14)
+    ds.execute("analysis")
+    assert ds.execute("factorization") == 0
+    b = M.rhs(A.shape[0], 4, seed=3)
+    x = ds.execute("solve", None, b).cpu().numpy()
+    assert M.scaled_backward_error(A, x, b) <= BERR
+    assert 1 <= ds.getparam("ir_n_steps") <= 10
+
+
+def test_uniform_batch(torch_cuda):
+    A = M.lap2d_shifted(24, 24, seed=0)
+    nb = 6
+    vals = M.batch_members(A, nb, spread=0.1, seed=1)
+    ds = _solver((A.indptr, A.indices, vals.reshape(-1), A.shape[0]), "SPD")
+    ds.execute("analysis")
+    info = ds.execute("factorization")
+    assert list(info) == [0] * nb
+    b = M.rhs(A.shape[0] * nb, 1, seed=2).reshape(nb, A.shape[0], 1)
+    x = ds.execute("solve", None, b).cpu().numpy().reshape(nb, A.shape[0], 1)
+    for k in range(nb):
+        Ak = sp.csr_matrix((vals[k], A.indices, A.indptr), shape=A.shape)
+        assert M.scaled_backward_error(Ak, x[k], b[k]) <= BERR
+    # ubatch_index: refactor one member only
+    ds.setparam("ubatch_index", 3)
+    ds.execute("refactorization")
+    ds.setparam("ubatch_index", -1)
+
+
+def test_phase_order_errors(torch_cuda):
+    from sdsb200.solver import FactorizationError, InvalidValueError
+
+    A = M.lap2d_shifted(8, 8)
+    ds = _solver(A, "SPD")
+    with pytest.raises(FactorizationError):
+        ds.execute("factorization")
+    ds.execute("analysis")
+    with pytest.raises(FactorizationError):
+        ds.execute("solve", None, np.ones(64))
+    with pytest.raises(InvalidValueError):
+        ds.setparam("pivot_threshold", -1.0)
