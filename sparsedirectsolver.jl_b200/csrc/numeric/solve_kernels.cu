@@ -37,10 +37,10 @@ __global__ void __launch_bounds__(SOLVE_THREADS) forward_kernel(SweepArgs<T> A) 
     double* u = m > 0 ? U + A.uoff[s] : nullptr;
     const int32_t* piv = A.piv ? A.piv + (int64_t)member * n : nullptr;
     const int tid = threadIdx.x, nt = blockDim.x, lane = tid & 31, warp = tid >> 5, nwarps = nt >> 5;
+    // gather this front's slice in the numbering before pivoting: the children's updates use it
     for (int q = tid; q < w * nrhs; q += nt) {
         int k = q % w, r = q / w;
-        int src = A.reorder ? piv[fd.c0 + k] - 1 : fd.c0 + k;
-        xs[q] = Y[src + (int64_t)r * n];
+        xs[q] = Y[fd.c0 + k + (int64_t)r * n];
     }
     for (int q = tid; q < m * nrhs; q += nt) u[q] = 0.0;
     __syncthreads();
@@ -57,6 +57,19 @@ __global__ void __launch_bounds__(SOLVE_THREADS) forward_kernel(SweepArgs<T> A) 
             double v = uc[q];
             if (p < w) xs[p + r * w] -= v;
             else u[(p - w) + r * m] += v;
+        }
+        __syncthreads();
+    }
+    if (A.reorder) {
+        // apply the local pivot order (the rows of this front's own columns only)
+        for (int q = tid; q < w * nrhs; q += nt) {
+            int k = q % w, r = q / w;
+            Y[fd.c0 + k + (int64_t)r * n] = xs[q];
+        }
+        __syncthreads();
+        for (int q = tid; q < w * nrhs; q += nt) {
+            int k = q % w, r = q / w;
+            xs[q] = Y[piv[fd.c0 + k] - 1 + (int64_t)r * n];
         }
         __syncthreads();
     }
