@@ -144,6 +144,11 @@ int sdsb200_set_members(sdsb200_plan* plan, const int32_t* h_members, int32_t na
 /* user_host_interrupt: a host flag polled between launch groups (factorization) and refinement steps. */
 int sdsb200_set_interrupt(sdsb200_plan* plan, const volatile int32_t* h_flag);
 
+/* CUDA graphs (on by default): the launch program of sdsb200_factor and of the solve / refinement
+ * steps is captured once per set of buffers and options and replayed. The user_host_interrupt flag is
+ * then polled before a factorization and before each refinement step, not between launch groups. */
+int sdsb200_set_graphs(sdsb200_plan* plan, int32_t on);
+
 /* Profiling mode (on != 0): CUDA events around every launch of the following factor and solve
  * calls, accumulated per kernel kind (resets the totals). Costs one event record per launch. */
 int sdsb200_set_profiling(sdsb200_plan* plan, int32_t on);

@@ -85,11 +85,54 @@ int prof_kind_of(LaunchKind k) {
         case L_SMALL: return PK_SMALL;
         case L_ASSEMBLE: return PK_ASSEMBLE;
         case L_CHOL_PANEL: return PK_PANEL;
+        case L_CHOL_DIAG: return PK_PANEL;
         case L_GEMM: return PK_GEMM;
         case L_PIVOT_FRONT: return PK_PIVOT;
         case L_SCALE: return PK_SCALE;
         default: return PK_STATS;
     }
+}
+
+// Run `body` (launches only, no host synchronization) captured as a CUDA graph on the plan's own
+// stream, replayed while `key` is unchanged. Without graphs (or when profiling) it runs eagerly.
+template <class F>
+int run_graph(Plan* P, Plan::CachedGraph& g, const std::vector<uint64_t>& key, cudaStream_t st, F body) {
+    if (!P->use_graphs || P->profile) return body(st);
+    CK(cudaEventRecord(P->join_in, st), "join");
+    CK(cudaStreamWaitEvent(P->own, P->join_in, 0), "join");
+    if (!g.exec || g.key != key) {
+        if (g.exec) {
+            cudaGraphExecDestroy(g.exec);
+            g.exec = nullptr;
+        }
+        cudaGraph_t graph = nullptr;
+        CK(cudaStreamBeginCapture(P->own, cudaStreamCaptureModeThreadLocal), "begin capture");
+        const int64_t before = P->launches_done;
+        int rc = body(P->own);
+        cudaError_t e = cudaStreamEndCapture(P->own, &graph);
+        if (rc != SDSB200_OK) {
+            if (e == cudaSuccess && graph) cudaGraphDestroy(graph);
+            return rc;
+        }
+        CK(e, "end capture");
+        g.launches = P->launches_done - before;
+        P->launches_done = before;
+        e = cudaGraphInstantiate(&g.exec, graph, 0);
+        cudaGraphDestroy(graph);
+        CK(e, "graph instantiate");
+        g.key = key;
+    }
+    CK(cudaGraphLaunch(g.exec, P->own), "graph launch");
+    P->launches_done += g.launches;
+    CK(cudaEventRecord(P->join_out, P->own), "join");
+    CK(cudaStreamWaitEvent(st, P->join_out, 0), "join");
+    return SDSB200_OK;
+}
+
+uint64_t bits(double x) {
+    uint64_t u;
+    memcpy(&u, &x, sizeof(u));
+    return u;
 }
 
 __global__ void absmax_kernel(const double* x, int64_t len, double* out) {
@@ -173,6 +216,7 @@ int run_factor(Plan* P, const double* nzval, double eps, double u, int pivot, in
                         case BUF_FACTOR: stride = P->factor_len; return factor;
                         case BUF_UFACTOR: stride = P->factor_len; return ufactor;
                         case BUF_CB: stride = P->cb_len; return cb;
+                        case BUF_INV: stride = P->inv_len; return static_cast<T*>(P->d_inv);
                         default: stride = P->work_len; return work;
                     }
                 };
@@ -182,6 +226,21 @@ int run_factor(Plan* P, const double* nzval, double eps, double u, int pivot, in
                 a.finfo = P->d_finfo;
                 a.ns = (int32_t)P->ns;
                 e = launch_gemm<T>(a, nm, st);
+                break;
+            }
+            case L_CHOL_DIAG: {
+                CholDiagArgs<T> a{};
+                a.fronts = P->d_fronts;
+                a.list = P->d_lists + L.list;
+                a.inv_off = P->d_inv_off + L.maxw;
+                a.count = L.count;
+                a.members = members;
+                a.factor = factor;
+                a.inv = static_cast<T*>(P->d_inv);
+                a.inv_len = P->inv_len;
+                a.finfo = P->d_finfo; a.stats = P->d_stats;
+                a.factor_len = P->factor_len; a.ns = (int32_t)P->ns; a.kb = L.cls; a.eps = eps;
+                e = launch_chol_diag<T>(a, nm, st);
                 break;
             }
             case L_PIVOT_FRONT: {
@@ -253,14 +312,47 @@ int run_sweeps(Plan* P, int nrhs, bool transpose, cudaStream_t st) {
     a.fac = (gen && transpose) ? ufactor : factor;
     a.piv = P->d_piv;
     a.reorder = ldl || (gen && !transpose);
+    a.tiles = P->d_rect_tiles;
+    auto level_sweep = [&](bool fwd, int L) -> int {
+        const int64_t off = P->level_list_off[L];
+        const int ns_ = P->level_nsmall[L], nl_ = P->level_nlarge[L];
+        double ent = P->level_panel_entries[L];   // booked on the first launch of the level
+        const int pk = fwd ? PK_FWD : PK_BWD;
+        if (!fwd && P->level_nbtile[L]) {
+            SweepArgs<T> t = a;
+            t.tiles = P->d_rect_tiles + 2 * P->level_btile_off[L];
+            prof_begin(P, st);
+            cudaError_t e = launch_sweep_rect<T>(false, t, P->level_nbtile[L], nm, P->level_maxw_large[L], st);
+            prof_end(P, st, pk, 2.0 * ent * nrhs * nm, (double)sizeof(T) * ent * nm);
+            ent = 0;
+            if (e != cudaSuccess) return cuda_fail(e, "backward sweep (rectangular)");
+        }
+        for (int part = 0; part < 2; ++part) {
+            const int cnt = part == 0 ? ns_ : nl_;
+            if (!cnt) continue;
+            SweepArgs<T> t = a;
+            t.list = P->d_level_lists + off + (part == 0 ? 0 : ns_);
+            t.count = cnt;
+            t.rect = part == 0;
+            prof_begin(P, st);
+            cudaError_t e = launch_sweep<T>(fwd, t, nm, part == 0 ? P->level_maxw_small[L] : P->level_maxw_large[L], st);
+            prof_end(P, st, pk, 2.0 * ent * nrhs * nm, (double)sizeof(T) * ent * nm);
+            ent = 0;
+            if (e != cudaSuccess) return cuda_fail(e, fwd ? "forward sweep" : "backward sweep");
+        }
+        if (fwd && P->level_nftile[L]) {
+            SweepArgs<T> t = a;
+            t.tiles = P->d_rect_tiles + 2 * P->level_ftile_off[L];
+            prof_begin(P, st);
+            cudaError_t e = launch_sweep_rect<T>(true, t, P->level_nftile[L], nm, P->level_maxw_large[L], st);
+            prof_end(P, st, pk, 0.0, 0.0);
+            if (e != cudaSuccess) return cuda_fail(e, "forward sweep (rectangular)");
+        }
+        return SDSB200_OK;
+    };
     for (int L = 0; L < P->nlevels; ++L) {
-        a.list = P->d_level_lists + P->level_list_off[L];
-        a.count = (int32_t)P->level_fronts[L].size();
-        prof_begin(P, st);
-        cudaError_t e = launch_sweep<T>(true, a, nm, P->level_maxw[L], st);
-        prof_end(P, st, PK_FWD, 2.0 * P->level_panel_entries[L] * nrhs * nm,
-                 (double)sizeof(T) * P->level_panel_entries[L] * nm);
-        if (e != cudaSuccess) return cuda_fail(e, "forward sweep");
+        int rc = level_sweep(true, L);
+        if (rc) return rc;
     }
     if (P->structure != STRUCT_SPD) {
         DiagArgs d{};
@@ -273,13 +365,8 @@ int run_sweeps(Plan* P, int nrhs, bool transpose, cudaStream_t st) {
     a.fac = (gen && !transpose) ? ufactor : factor;
     a.reorder = ldl || (gen && transpose);
     for (int L = P->nlevels - 1; L >= 0; --L) {
-        a.list = P->d_level_lists + P->level_list_off[L];
-        a.count = (int32_t)P->level_fronts[L].size();
-        prof_begin(P, st);
-        cudaError_t e = launch_sweep<T>(false, a, nm, P->level_maxw[L], st);
-        prof_end(P, st, PK_BWD, 2.0 * P->level_panel_entries[L] * nrhs * nm,
-                 (double)sizeof(T) * P->level_panel_entries[L] * nm);
-        if (e != cudaSuccess) return cuda_fail(e, "backward sweep");
+        int rc = level_sweep(false, L);
+        if (rc) return rc;
     }
     return SDSB200_OK;
 }
@@ -378,11 +465,16 @@ int sdsb200_factor(sdsb200_plan* plan, const double* nzval, const int8_t* h_psig
     if (h_psign) CK(cudaMemcpyAsync(P->d_psign, h_psign, P->n, cudaMemcpyHostToDevice, st), "psign");
     else CK(cudaMemsetAsync(P->d_psign, 0, P->n, st), "psign");
     P->launches_done = 0;
-    CK(cudaMemsetAsync(P->d_finfo, 0, sizeof(int32_t) * P->ns * P->nbatch, st), "memset finfo");
-    CK(cudaMemsetAsync(P->d_stats, 0, sizeof(int64_t) * NSTAT * P->ns * P->nbatch, st), "memset stats");
     P->factored = false;
-    int rc = P->elsize == 8 ? run_factor<double>(P, nzval, eps, o.pivot_threshold, pivot, lu_pivot, st)
-                            : run_factor<float>(P, nzval, eps, o.pivot_threshold, pivot, lu_pivot, st);
+    if (interrupted(P)) return fail(SDSB200_INTERRUPTED, "interrupted by user_host_interrupt");
+    std::vector<uint64_t> key = {(uint64_t)(uintptr_t)nzval, bits(eps), bits(o.pivot_threshold), (uint64_t)pivot,
+                                 (uint64_t)lu_pivot, (uint64_t)P->nact, (uint64_t)P->all_members};
+    int rc = run_graph(P, P->g_factor, key, st, [&](cudaStream_t s) -> int {
+        CK(cudaMemsetAsync(P->d_finfo, 0, sizeof(int32_t) * P->ns * P->nbatch, s), "memset finfo");
+        CK(cudaMemsetAsync(P->d_stats, 0, sizeof(int64_t) * NSTAT * P->ns * P->nbatch, s), "memset stats");
+        return P->elsize == 8 ? run_factor<double>(P, nzval, eps, o.pivot_threshold, pivot, lu_pivot, s)
+                              : run_factor<float>(P, nzval, eps, o.pivot_threshold, pivot, lu_pivot, s);
+    });
     if (rc != SDSB200_OK) return rc;
     // the phase's one host synchronization: the reduced info of the active members
     CK(cudaMemcpyAsync(P->h_info_pinned, P->d_info, sizeof(int64_t) * P->nact, cudaMemcpyDeviceToHost, st), "info");
@@ -427,38 +519,59 @@ int sdsb200_solve(sdsb200_plan* plan, double* X, int64_t ldx, const double* B, i
     if ((size_t)maxw * nrhs * sizeof(double) > 200 * 1024)
         return fail(SDSB200_NOT_SUPPORTED, "front too wide for this many right-hand sides in one solve");
     P->launches_done = 0;
-    int rc = permute(P, 0, B, ldb, nullptr, 0, nrhs, st);
-    if (rc) return rc;
-    rc = sweeps(P, nrhs, transpose, st);
-    if (rc) return rc;
-    rc = permute(P, 1, nullptr, 0, X, ldx, nrhs, st);
+    const uint64_t common = ((uint64_t)nrhs << 32) | ((uint64_t)transpose << 8) | ((uint64_t)P->all_members << 4);
+    std::vector<uint64_t> key = {(uint64_t)(uintptr_t)X, (uint64_t)ldx, (uint64_t)(uintptr_t)B, (uint64_t)ldb, common,
+                                 (uint64_t)P->nact};
+    int rc = run_graph(P, P->g_solve, key, st, [&](cudaStream_t s) -> int {
+        int r = permute(P, 0, B, ldb, nullptr, 0, nrhs, s);
+        if (r) return r;
+        r = sweeps(P, nrhs, transpose, s);
+        if (r) return r;
+        return permute(P, 1, nullptr, 0, X, ldx, nrhs, s);
+    });
     if (rc) return rc;
     int steps = 0;
+    const bool check = o.ir_tol > 0;
+    const int ncols = nrhs * P->nact;
     for (int it = 0; it < o.ir_n_steps; ++it) {
         if (interrupted(P)) {
             if (h_ir_steps) *h_ir_steps = steps;
             return fail(SDSB200_INTERRUPTED, "interrupted by user_host_interrupt");
         }
-        ResidualArgs r{};
-        r.members = P->all_members ? nullptr : P->d_members;
-        if (transpose) {
-            r.rowptr = P->d_fullT_rowptr; r.colval = P->d_fullT_colval; r.srcptr = P->d_fullT_srcptr; r.src = P->d_fullT_src;
-        } else {
-            r.rowptr = P->d_full_rowptr; r.colval = P->d_full_colval; r.srcptr = P->d_full_srcptr; r.src = P->d_full_src;
-        }
-        r.nzval = nzval; r.X = X; r.B = B; r.R = P->d_R;
-        r.n = P->n; r.nnz = P->nnz; r.ldx = ldx; r.ldb = ldb; r.nrhs = nrhs;
-        prof_begin(P, st);
-        cudaError_t re = launch_residual(r, P->nact, st);
-        prof_end(P, st, PK_RESIDUAL, 2.0 * P->full_nnz * nrhs * P->nact,
-                 (16.0 * P->full_nnz + 8.0 * P->full_nsrc + 8.0 * P->full_nsrc) * P->nact + 24.0 * P->n * nrhs * P->nact);
-        CK(re, "residual");
-        if (o.ir_tol > 0) {
-            NormArgs na{};
-            na.members = r.members; na.R = P->d_R; na.B = B; na.out = P->d_norms; na.n = P->n; na.ldb = ldb; na.nrhs = nrhs;
-            int ncols = nrhs * P->nact;
-            CK(launch_norms(na, ncols, st), "norms");
-            CK(cudaMemcpyAsync(P->h_norms, P->d_norms, sizeof(double) * 2 * ncols, cudaMemcpyDeviceToHost, st), "norms");
+        std::vector<uint64_t> rkey = key;
+        rkey.push_back((uint64_t)(uintptr_t)nzval);
+        rkey.push_back(check);
+        rc = run_graph(P, P->g_resid, rkey, st, [&](cudaStream_t s) -> int {
+            ResidualArgs r{};
+            r.members = P->all_members ? nullptr : P->d_members;
+            if (transpose) {
+                r.rowptr = P->d_fullT_rowptr; r.colval = P->d_fullT_colval; r.srcptr = P->d_fullT_srcptr;
+                r.src = P->d_fullT_src;
+            } else {
+                r.rowptr = P->d_full_rowptr; r.colval = P->d_full_colval; r.srcptr = P->d_full_srcptr;
+                r.src = P->d_full_src;
+            }
+            r.nzval = nzval; r.X = X; r.B = B; r.R = P->d_R;
+            r.n = P->n; r.nnz = P->nnz; r.ldx = ldx; r.ldb = ldb; r.nrhs = nrhs;
+            prof_begin(P, s);
+            cudaError_t re = launch_residual(r, P->nact, s);
+            prof_end(P, s, PK_RESIDUAL, 2.0 * P->full_nnz * nrhs * P->nact,
+                     (16.0 * P->full_nnz + 16.0 * P->full_nsrc) * P->nact + 24.0 * P->n * nrhs * P->nact);
+            CK(re, "residual");
+            if (check) {
+                NormArgs na{};
+                na.members = r.members; na.R = P->d_R; na.B = B; na.out = P->d_norms; na.n = P->n; na.ldb = ldb;
+                na.nrhs = nrhs;
+                prof_begin(P, s);
+                CK(launch_norms(na, ncols, s), "norms");
+                prof_end(P, s, PK_RESIDUAL, 0.0, 16.0 * P->n * ncols);
+                CK(cudaMemcpyAsync(P->h_norms, P->d_norms, sizeof(double) * 2 * ncols, cudaMemcpyDeviceToHost, s),
+                   "norms");
+            }
+            return SDSB200_OK;
+        });
+        if (rc) return rc;
+        if (check) {
             CK(cudaStreamSynchronize(st), "norms sync");
             double rel = 0;
             for (int c = 0; c < ncols; ++c) {
@@ -467,11 +580,14 @@ int sdsb200_solve(sdsb200_plan* plan, double* X, int64_t ldx, const double* B, i
             }
             if (rel <= o.ir_tol) break;
         }
-        rc = permute(P, 0, P->d_R, P->n, nullptr, 0, nrhs, st);
-        if (rc) return rc;
-        rc = sweeps(P, nrhs, transpose, st);
-        if (rc) return rc;
-        rc = permute(P, 2, nullptr, 0, X, ldx, nrhs, st);
+        std::vector<uint64_t> ckey = key;
+        rc = run_graph(P, P->g_corr, ckey, st, [&](cudaStream_t s) -> int {
+            int r = permute(P, 0, P->d_R, P->n, nullptr, 0, nrhs, s);
+            if (r) return r;
+            r = sweeps(P, nrhs, transpose, s);
+            if (r) return r;
+            return permute(P, 2, nullptr, 0, X, ldx, nrhs, s);
+        });
         if (rc) return rc;
         steps++;
     }
@@ -555,6 +671,13 @@ int sdsb200_set_members(sdsb200_plan* plan, const int32_t* h_members, int32_t na
     CK(cudaMemcpy(P->d_members, h_members, sizeof(int32_t) * nact, cudaMemcpyHostToDevice), "members");
     P->all_members = false;
     P->nact = nact;
+    return SDSB200_OK;
+}
+
+int sdsb200_set_graphs(sdsb200_plan* plan, int32_t on) {
+    Plan* P = reinterpret_cast<Plan*>(plan);
+    if (!P) return fail(SDSB200_INVALID_VALUE, "plan is NULL");
+    P->use_graphs = on != 0;
     return SDSB200_OK;
 }
 

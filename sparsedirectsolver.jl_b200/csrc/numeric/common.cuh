@@ -47,13 +47,16 @@ struct GemmTile {
     int32_t m, n, k;     // valid rows and columns of this tile (<= tile size), inner dimension
     int32_t diag;
     int32_t front;       // status check: the tile is skipped when this front failed (-1: none)
+    int32_t mode;        // 0: C -= A B^T; 1: C = A B^T (in place over A's rows: trsm by an inverse)
+    int32_t pad;
 };
 
 // A launch of the factorization program.
 enum LaunchKind : int32_t {
     L_SMALL = 1,       // fused small fronts (one CTA per front, front in shared memory)
     L_ASSEMBLE,        // column-task assembly of large fronts
-    L_CHOL_PANEL,      // large Cholesky: diagonal block + trsm of one column block
+    L_CHOL_PANEL,      // large Cholesky: diagonal block + trsm of one column block (row-tile form)
+    L_CHOL_DIAG,       // large Cholesky: factor + invert the diagonal block of one column block
     L_GEMM,            // grouped GEMM tiles
     L_PIVOT_FRONT,     // large LDLT / LU: cooperative pivoting over the panel
     L_STATS,           // statistics reduction

@@ -168,17 +168,214 @@ __global__ void __launch_bounds__(256) gemm_nt_kernel(GemmArgs<T> A) {
 #pragma unroll
         for (int j = 0; j < 4; ++j) {
             int r = tx + 16 * i, c = ty + 16 * j;
-            if (r < M && c < N && r + t.diag >= c) Cb[r + (int64_t)c * t.ldc] -= acc[i][j];
+            if (r < M && c < N && r + t.diag >= c) {
+                if (t.mode) Cb[r + (int64_t)c * t.ldc] = acc[i][j];
+                else Cb[r + (int64_t)c * t.ldc] -= acc[i][j];
+            }
         }
+}
+
+// FP64 on the tensor cores: mma.sync m8n8k4 (DMMA). 64 x 64 CTA tile, 4 warps of 32 x 32,
+// K in steps of 16 staged by cp.async into two shared-memory buffers.
+__device__ __forceinline__ void cp_async8(void* smem, const void* gmem, bool valid) {
+    unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+    int sz = valid ? 8 : 0;
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(s), "l"(gmem), "r"(sz));
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N)); }
+
+__global__ void __launch_bounds__(128) gemm_nt_dmma_kernel(GemmArgs<double> A) {
+    constexpr int BM = 64, BN = 64, BK = 16, LDS = 72;
+    __shared__ __align__(16) double As[2][BK][LDS];
+    __shared__ __align__(16) double Bs[2][BK][LDS];
+    const GemmTile t = A.tiles[blockIdx.x];
+    const int member = A.members ? A.members[blockIdx.y] : blockIdx.y;
+    if (A.finfo && t.front >= 0 && A.finfo[(int64_t)member * A.ns + t.front] != 0) return;
+    const double* Ab = A.abuf + (int64_t)member * A.astride + t.a;
+    const double* Bb = A.bbuf + (int64_t)member * A.bstride + t.b;
+    double* Cb = A.cbuf + (int64_t)member * A.cstride + t.c;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int wm = warp & 1, wn = warp >> 1;
+    const int M = t.m, N = t.n, K = t.k;
+    double acc[4][4][2];
+#pragma unroll
+    for (int i = 0; i < 4; ++i)
+#pragma unroll
+        for (int j = 0; j < 4; ++j) acc[i][j][0] = acc[i][j][1] = 0.0;
+    auto load = [&](int buf, int k0) {
+#pragma unroll
+        for (int q = 0; q < (BM * BK) / 128; ++q) {
+            int e = tid + 128 * q, r = e % BM, kk = e / BM;
+            bool va = r < M && k0 + kk < K;
+            cp_async8(&As[buf][kk][r], va ? Ab + r + (int64_t)(k0 + kk) * t.lda : Ab, va);
+            bool vb = r < N && k0 + kk < K;
+            cp_async8(&Bs[buf][kk][r], vb ? Bb + r + (int64_t)(k0 + kk) * t.ldb : Bb, vb);
+        }
+        cp_async_commit();
+    };
+    const int nk = (K + BK - 1) / BK;
+    load(0, 0);
+    for (int it = 0; it < nk; ++it) {
+        const int buf = it & 1;
+        if (it + 1 < nk) {
+            load(buf ^ 1, (it + 1) * BK);
+            cp_async_wait<1>();
+        } else {
+            cp_async_wait<0>();
+        }
+        __syncthreads();
+#pragma unroll
+        for (int kk = 0; kk < BK; kk += 4) {
+            double a[4], b[4];
+#pragma unroll
+            for (int i = 0; i < 4; ++i) a[i] = As[buf][kk + (lane & 3)][wm * 32 + i * 8 + (lane >> 2)];
+#pragma unroll
+            for (int j = 0; j < 4; ++j) b[j] = Bs[buf][kk + (lane & 3)][wn * 32 + j * 8 + (lane >> 2)];
+#pragma unroll
+            for (int i = 0; i < 4; ++i)
+#pragma unroll
+                for (int j = 0; j < 4; ++j)
+                    asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};\n"
+                                 : "+d"(acc[i][j][0]), "+d"(acc[i][j][1])
+                                 : "d"(a[i]), "d"(b[j]));
+        }
+        __syncthreads();
+    }
+#pragma unroll
+    for (int i = 0; i < 4; ++i)
+#pragma unroll
+        for (int j = 0; j < 4; ++j)
+#pragma unroll
+            for (int e = 0; e < 2; ++e) {
+                const int r = wm * 32 + i * 8 + (lane >> 2);
+                const int c = wn * 32 + j * 8 + (lane & 3) * 2 + e;
+                if (r < M && c < N && r + t.diag >= c) {
+                    double* p = Cb + r + (int64_t)c * t.ldc;
+                    if (t.mode) *p = acc[i][j][e];
+                    else *p -= acc[i][j][e];
+                }
+            }
 }
 
 template <typename T>
 cudaError_t launch_gemm(const GemmArgs<T>& a, int nmembers, cudaStream_t st) {
     if (a.count == 0) return cudaSuccess;
     dim3 grid(a.count, nmembers);
-    gemm_nt_kernel<T><<<grid, 256, 0, st>>>(a);
+    if constexpr (sizeof(T) == 8) {
+        gemm_nt_dmma_kernel<<<grid, 128, 0, st>>>(a);
+    } else {
+        gemm_nt_kernel<T><<<grid, 256, 0, st>>>(a);
+    }
     return cudaGetLastError();
 }
+
+// ---------------------------------------------------------------------------
+// Diagonal block of a large Cholesky front (64 x 64 at column kb): factor in shared memory with the
+// static clamp and failure rule of the fused kernels, write L11 back, write inv(L11) (ld 64) to
+// scratch for the trsm of the rows below as a GEMM (X = B inv(L11)^T).
+template <typename T>
+__global__ void __launch_bounds__(256) chol_diag_kernel(CholDiagArgs<T> A) {
+    constexpr int NB = CHOL_NB;
+    extern __shared__ __align__(16) unsigned char diag_smem[];
+    double(*L)[NB + 1] = reinterpret_cast<double(*)[NB + 1]>(diag_smem);
+    double(*X)[NB + 1] = reinterpret_cast<double(*)[NB + 1]>(diag_smem + sizeof(double) * NB * (NB + 1));
+    __shared__ int s_status;
+    const int s = A.list[blockIdx.x];
+    const int member = A.members ? A.members[blockIdx.y] : blockIdx.y;
+    const DFront fd = A.fronts[s];
+    int32_t* finfo = A.finfo + (int64_t)member * A.ns;
+    if (finfo[s] != 0) return;
+    const int f = fd.f, w = fd.w, kb = A.kb;
+    if (kb >= w) return;
+    const int nbb = min(NB, w - kb);
+    T* P = A.factor + (int64_t)member * A.factor_len + fd.panel;
+    const int tid = threadIdx.x, nt = blockDim.x;
+    for (int q = tid; q < NB * NB; q += nt) {
+        int i = q % NB, j = q / NB;
+        L[i][j] = (i < nbb && j < nbb && i >= j) ? (double)P[(kb + i) + (int64_t)(kb + j) * f] : 0.0;
+    }
+    if (tid == 0) s_status = 0;
+    __syncthreads();
+    const double eps = A.eps;
+    for (int j = 0; j < nbb; ++j) {
+        double ajj = L[j][j];
+        bool ok = ajj > eps || (eps > 0 && ajj >= 0);
+        if (!ok) {
+            if (tid == 0) s_status = j + 1;
+            break;
+        }
+        double djj = sqrt(fmax(ajj, eps));
+        double inv = 1.0 / djj;
+        __syncthreads();
+        for (int i = j + 1 + tid; i < nbb; i += nt) L[i][j] = (double)T(L[i][j] * inv);
+        if (tid == 0) L[j][j] = (double)T(djj);
+        __syncthreads();
+        const int r = nbb - j - 1;
+        for (int q = tid; q < r * r; q += nt) {
+            int i = j + 1 + q % r, l = j + 1 + q / r;
+            if (i >= l) L[i][l] = (double)T(L[i][l] - L[i][j] * L[l][j]);
+        }
+        __syncthreads();
+    }
+    __syncthreads();
+    const int status = s_status;
+    for (int q = tid; q < nbb * nbb; q += nt) {
+        int i = q % nbb, j = q / nbb;
+        P[(kb + i) + (int64_t)(kb + j) * f] = i >= j ? T(L[i][j]) : T(0);
+    }
+    if (status) {
+        if (tid == 0) {
+            int64_t* S = A.stats + ((int64_t)member * A.ns + s) * NSTAT;
+            finfo[s] = kb + status;
+            S[ST_NPOS] = kb + status - 1;
+            S[ST_INFO] = kb + status;
+        }
+        return;
+    }
+    if (tid == 0 && kb + nbb == w) {
+        int64_t* S = A.stats + ((int64_t)member * A.ns + s) * NSTAT;
+        S[ST_NPOS] = w;
+        S[ST_INFO] = 0;
+    }
+    if (kb + nbb >= f) return;  // no rows below: no trsm
+    // inverse of the lower-triangular block, one column per thread (forward substitution)
+    for (int j = tid; j < nbb; j += nt) {
+        for (int i = 0; i < nbb; ++i) {
+            double acc = i == j ? 1.0 : 0.0;
+            for (int l = j; l < i; ++l) acc -= L[i][l] * X[l][j];
+            X[i][j] = i < j ? 0.0 : acc / L[i][i];
+        }
+    }
+    __syncthreads();
+    T* inv = A.inv + (int64_t)member * A.inv_len + A.inv_off[blockIdx.x];
+    for (int q = tid; q < NB * NB; q += nt) {
+        int i = q % NB, j = q / NB;
+        inv[i + (int64_t)j * NB] = (i < nbb && j < nbb) ? T(X[i][j]) : T(0);
+    }
+}
+
+template <typename T>
+cudaError_t launch_chol_diag(const CholDiagArgs<T>& a, int nmembers, cudaStream_t st) {
+    if (a.count == 0) return cudaSuccess;
+    dim3 grid(a.count, nmembers);
+    const int smem = 2 * sizeof(double) * CHOL_NB * (CHOL_NB + 1);
+    chol_diag_kernel<T><<<grid, 256, smem, st>>>(a);
+    return cudaGetLastError();
+}
+
+cudaError_t prepare_dense_kernels(int max_smem) {
+    cudaError_t e = cudaFuncSetAttribute((const void*)chol_diag_kernel<double>,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize, max_smem);
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute((const void*)chol_diag_kernel<float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 max_smem);
+    return e;
+}
+
+template cudaError_t launch_chol_diag<double>(const CholDiagArgs<double>&, int, cudaStream_t);
+template cudaError_t launch_chol_diag<float>(const CholDiagArgs<float>&, int, cudaStream_t);
 
 template cudaError_t launch_gemm<double>(const GemmArgs<double>&, int, cudaStream_t);
 template cudaError_t launch_gemm<float>(const GemmArgs<float>&, int, cudaStream_t);

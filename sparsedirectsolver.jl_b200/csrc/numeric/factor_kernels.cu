@@ -201,22 +201,28 @@ cudaError_t launch_small(int structure, const SmallArgs<T>& a, int count, int nm
     size_t smem = small_front_smem(fmax, sizeof(T));
     int threads = fmax <= 48 ? 128 : 256;
     dim3 grid(count, nmembers);
-    cudaError_t e = cudaSuccess;
     switch (structure) {
-        case STRUCT_SPD:
-            e = cudaFuncSetAttribute(small_front_kernel<T, STRUCT_SPD>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-            if (e == cudaSuccess) small_front_kernel<T, STRUCT_SPD><<<grid, threads, smem, st>>>(a);
-            break;
-        case STRUCT_S:
-            e = cudaFuncSetAttribute(small_front_kernel<T, STRUCT_S>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-            if (e == cudaSuccess) small_front_kernel<T, STRUCT_S><<<grid, threads, smem, st>>>(a);
-            break;
-        default:
-            e = cudaFuncSetAttribute(small_front_kernel<T, STRUCT_G>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-            if (e == cudaSuccess) small_front_kernel<T, STRUCT_G><<<grid, threads, smem, st>>>(a);
+        case STRUCT_SPD: small_front_kernel<T, STRUCT_SPD><<<grid, threads, smem, st>>>(a); break;
+        case STRUCT_S: small_front_kernel<T, STRUCT_S><<<grid, threads, smem, st>>>(a); break;
+        default: small_front_kernel<T, STRUCT_G><<<grid, threads, smem, st>>>(a);
     }
-    if (e != cudaSuccess) return e;
     return cudaGetLastError();
+}
+
+// the opt-in shared-memory limit of every kernel with a dynamic allocation, set once at plan creation
+// (outside any stream capture)
+cudaError_t prepare_factor_kernels(int max_smem) {
+    cudaError_t e = cudaSuccess;
+    auto set = [&](const void* k) {
+        if (e == cudaSuccess) e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, max_smem);
+    };
+    set((const void*)small_front_kernel<double, STRUCT_SPD>);
+    set((const void*)small_front_kernel<double, STRUCT_S>);
+    set((const void*)small_front_kernel<double, STRUCT_G>);
+    set((const void*)small_front_kernel<float, STRUCT_SPD>);
+    set((const void*)small_front_kernel<float, STRUCT_S>);
+    set((const void*)small_front_kernel<float, STRUCT_G>);
+    return e;
 }
 
 template cudaError_t launch_small<double>(int, const SmallArgs<double>&, int, int, int, cudaStream_t);

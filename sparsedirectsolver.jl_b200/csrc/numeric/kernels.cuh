@@ -73,6 +73,25 @@ struct CholPanelArgs {
     double eps;
 };
 
+// Diagonal block of a large Cholesky front: factor in place and write its inverse (ld 64) to scratch.
+template <typename T>
+struct CholDiagArgs {
+    const DFront* fronts;
+    const int32_t* list;
+    const int64_t* inv_off;   // per listed front: offset of its 64 x 64 inverse in the scratch buffer
+    int32_t count;
+    const int32_t* members;
+    T* factor;
+    T* inv;                   // scratch, per member stride inv_len
+    int64_t inv_len;
+    int32_t* finfo;
+    int64_t* stats;
+    int64_t factor_len;
+    int32_t ns;
+    int32_t kb;
+    double eps;
+};
+
 template <typename T>
 struct GemmArgs {
     const GemmTile* tiles;
@@ -136,6 +155,12 @@ template <typename T>
 cudaError_t launch_chol_panel(const CholPanelArgs<T>& a, int nb, int nmembers, cudaStream_t st);
 template <typename T>
 cudaError_t launch_gemm(const GemmArgs<T>& a, int nmembers, cudaStream_t st);
+template <typename T>
+cudaError_t launch_chol_diag(const CholDiagArgs<T>& a, int nmembers, cudaStream_t st);
+constexpr int CHOL_NB = 64;
+cudaError_t prepare_factor_kernels(int max_smem);
+cudaError_t prepare_dense_kernels(int max_smem);
+cudaError_t prepare_solve_kernels(int max_smem);   // column block of the large-front Cholesky
 template <typename T>
 cudaError_t launch_large_pivot(int structure, const LargePivotArgs<T>& a, int nmembers, cudaStream_t st);
 template <typename T>

@@ -17,6 +17,11 @@
 #include <vector>
 
 #include "plan.h"
+#include "solve.cuh"
+
+namespace sds {
+constexpr int RECT_ROWS_PLAN = RECT_ROWS, RECT_COLS_PLAN = RECT_COLS;
+}
 
 namespace sds {
 
@@ -251,7 +256,7 @@ Plan* build_plan(const sdsb200_symbolic* sym, const sdsb200_plan_options* popts,
         std::vector<ColTask> coltasks;
         std::vector<PanelTask> ptasks;
         std::vector<GemmTile> tiles;
-        std::vector<int64_t> scr_off, woff;
+        std::vector<int64_t> scr_off, woff, inv_off;
         const int NB = 32;
         auto add_gemm_tiles = [&](int64_t a, int lda, int64_t b, int ldb, int64_t c, int ldc, int M, int N, int K,
                                   bool lower, int front) -> double {
@@ -270,6 +275,8 @@ Plan* build_plan(const sdsb200_symbolic* sym, const sdsb200_plan_options* popts,
                     t.m = mm; t.n = nn; t.k = K;
                     t.diag = lower ? ti - tj : (1 << 29);
                     t.front = front;
+                    t.mode = 0;
+                    t.pad = 0;
                     tiles.push_back(t);
                 }
             return 2.0 * K * entries;
@@ -315,24 +322,48 @@ Plan* build_plan(const sdsb200_symbolic* sym, const sdsb200_plan_options* popts,
                 P->prog.push_back(pl);
             }
             if (P->structure == STRUCT_SPD) {
+                const int NB = CHOL_NB;
                 int maxw = 0;
                 for (int s : large) maxw = std::max(maxw, P->fronts[s].w);
                 for (int kb = 0; kb < maxw; kb += NB) {
                     ProgLaunch dl{};
-                    dl.kind = L_CHOL_PANEL; dl.level = L; dl.cls = kb; dl.nb = NB; dl.list = (int64_t)ptasks.size();
+                    dl.kind = L_CHOL_DIAG; dl.level = L; dl.cls = kb; dl.nb = NB; dl.list = (int64_t)lists.size();
+                    dl.maxw = (int)inv_off.size();
+                    int64_t io = 0;
                     for (int s : large)
-                        if (P->fronts[s].w > kb) ptasks.push_back({s, -1});
-                    dl.count = (int)(ptasks.size() - dl.list);
+                        if (P->fronts[s].w > kb) {
+                            lists.push_back(s);
+                            inv_off.push_back(io);
+                            io += (int64_t)NB * NB;
+                        }
+                    P->inv_len = std::max(P->inv_len, io);
+                    dl.count = (int)(lists.size() - dl.list);
+                    dl.flops = 0;
+                    for (int s : large)
+                        if (P->fronts[s].w > kb) {
+                            double nbb = std::min(NB, P->fronts[s].w - kb);
+                            dl.flops += nbb * nbb * nbb / 3.0 * 2.0;
+                        }
                     P->prog.push_back(dl);
-                    ProgLaunch tl = dl;
-                    tl.list = (int64_t)ptasks.size();
+                    ProgLaunch tl{};
+                    tl.kind = L_GEMM; tl.level = L; tl.list = (int64_t)tiles.size();
+                    tl.abuf = BUF_FACTOR; tl.bbuf = BUF_INV; tl.cbuf = BUF_FACTOR;
+                    int64_t io2 = 0;
                     for (int s : large) {
                         const DFront& F = P->fronts[s];
                         if (F.w <= kb) continue;
                         int nbb = std::min(NB, F.w - kb);
-                        for (int r0 = kb + nbb; r0 < F.f; r0 += PANEL_ROWS) ptasks.push_back({s, r0});
+                        int r1 = kb + nbb;
+                        if (r1 < F.f) {
+                            size_t t0 = tiles.size();
+                            tl.flops += add_gemm_tiles(F.panel + r1 + (int64_t)kb * F.f, F.f, io2, NB,
+                                                       F.panel + r1 + (int64_t)kb * F.f, F.f, F.f - r1, nbb, nbb,
+                                                       false, s);
+                            for (size_t q = t0; q < tiles.size(); ++q) tiles[q].mode = 1;
+                        }
+                        io2 += (int64_t)NB * NB;
                     }
-                    tl.count = (int)(ptasks.size() - tl.list);
+                    tl.count = (int)(tiles.size() - tl.list);
                     if (tl.count) P->prog.push_back(tl);
                     ProgLaunch gl{};
                     gl.kind = L_GEMM; gl.level = L; gl.list = (int64_t)tiles.size();
@@ -422,16 +453,52 @@ Plan* build_plan(const sdsb200_symbolic* sym, const sdsb200_plan_options* popts,
             }
         }
         P->ulen = std::max<int64_t>(uo, 1);
-        std::vector<int32_t> level_lists;
+        std::vector<int32_t> level_lists, rect_tiles;
         P->level_maxw.assign(P->nlevels, 0);
         P->level_panel_entries.assign(P->nlevels, 0.0);
+        P->level_nsmall.assign(P->nlevels, 0);
+        P->level_nlarge.assign(P->nlevels, 0);
+        P->level_maxw_small.assign(P->nlevels, 1);
+        P->level_maxw_large.assign(P->nlevels, 1);
+        P->level_nftile.assign(P->nlevels, 0);
+        P->level_nbtile.assign(P->nlevels, 0);
+        auto solve_large = [&](const DFront& F) { return (int64_t)(F.f - F.w) * F.w >= 16384; };
         for (int L = 0; L < P->nlevels; ++L) {
             P->level_list_off.push_back((int64_t)level_lists.size());
+            for (int pass = 0; pass < 2; ++pass)
+                for (int s : P->level_fronts[L]) {
+                    const DFront& F = P->fronts[s];
+                    if (solve_large(F) != (pass == 1)) continue;
+                    level_lists.push_back(s);
+                    if (pass == 0) {
+                        P->level_nsmall[L]++;
+                        P->level_maxw_small[L] = std::max(P->level_maxw_small[L], F.w);
+                    } else {
+                        P->level_nlarge[L]++;
+                        P->level_maxw_large[L] = std::max(P->level_maxw_large[L], F.w);
+                    }
+                    P->level_maxw[L] = std::max(P->level_maxw[L], F.w);
+                    P->level_panel_entries[L] += (double)F.f * F.w - 0.5 * (double)F.w * (F.w - 1);
+                }
+            P->level_ftile_off.push_back((int64_t)rect_tiles.size() / 2);
             for (int s : P->level_fronts[L]) {
-                level_lists.push_back(s);
                 const DFront& F = P->fronts[s];
-                P->level_maxw[L] = std::max(P->level_maxw[L], F.w);
-                P->level_panel_entries[L] += (double)F.f * F.w - 0.5 * (double)F.w * (F.w - 1);
+                if (!solve_large(F)) continue;
+                for (int r0 = 0; r0 < F.f - F.w; r0 += RECT_ROWS_PLAN) {
+                    rect_tiles.push_back(s);
+                    rect_tiles.push_back(r0);
+                    P->level_nftile[L]++;
+                }
+            }
+            P->level_btile_off.push_back((int64_t)rect_tiles.size() / 2);
+            for (int s : P->level_fronts[L]) {
+                const DFront& F = P->fronts[s];
+                if (!solve_large(F)) continue;
+                for (int c0 = 0; c0 < F.w; c0 += RECT_COLS_PLAN) {
+                    rect_tiles.push_back(s);
+                    rect_tiles.push_back(c0);
+                    P->level_nbtile[L]++;
+                }
             }
         }
 
@@ -513,8 +580,10 @@ Plan* build_plan(const sdsb200_symbolic* sym, const sdsb200_plan_options* popts,
         P->d_tiles = upload(P, tiles, st);
         P->d_scr_off = upload(P, scr_off, st);
         P->d_woff = upload(P, woff, st);
+        P->d_inv_off = upload(P, inv_off, st);
         P->d_uoff = upload(P, uoff, st);
         P->d_level_lists = upload(P, level_lists, st);
+        P->d_rect_tiles = upload(P, rect_tiles, st);
 
         const int64_t nb = P->nbatch;
         const size_t es = P->elsize;
@@ -536,6 +605,7 @@ Plan* build_plan(const sdsb200_symbolic* sym, const sdsb200_plan_options* popts,
         P->d_amax = dalloc<double>(P, 1);
         if (P->scr_len) P->d_scratch = dalloc<double>(P, P->scr_len * nb);
         if (P->work_len) P->d_work = alloc_bytes(es * P->work_len * nb);
+        if (P->inv_len) P->d_inv = alloc_bytes(es * P->inv_len * nb);
         P->d_Y = dalloc<double>(P, n * P->max_nrhs * nb);
         P->d_U = dalloc<double>(P, P->ulen * nb);
         P->d_R = dalloc<double>(P, n * P->max_nrhs * nb);
@@ -544,6 +614,20 @@ Plan* build_plan(const sdsb200_symbolic* sym, const sdsb200_plan_options* popts,
             throw BuildError(SDSB200_ALLOC_FAILED, "cudaMallocHost");
         if (cudaMallocHost(&P->h_info_pinned, sizeof(int64_t) * nb) != cudaSuccess)
             throw BuildError(SDSB200_ALLOC_FAILED, "cudaMallocHost");
+        {
+            int dev = 0, optin = 0;
+            cudaGetDevice(&dev);
+            cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+            if (prepare_factor_kernels(optin) != cudaSuccess || prepare_dense_kernels(optin) != cudaSuccess ||
+                prepare_solve_kernels(optin) != cudaSuccess)
+                throw BuildError(SDSB200_CUDA_ERROR, "kernel attribute setup failed");
+            if ((int64_t)small_front_smem(P->fsmall_max, P->elsize) > optin)
+                throw BuildError(SDSB200_NOT_SUPPORTED, "shared memory per block too small for the front classes");
+        }
+        if (cudaStreamCreateWithFlags(&P->own, cudaStreamNonBlocking) != cudaSuccess ||
+            cudaEventCreateWithFlags(&P->join_in, cudaEventDisableTiming) != cudaSuccess ||
+            cudaEventCreateWithFlags(&P->join_out, cudaEventDisableTiming) != cudaSuccess)
+            throw BuildError(SDSB200_CUDA_ERROR, "stream or event creation failed");
         cudaMemsetAsync(P->d_psign, 0, n, st);
         cudaMemsetAsync(P->d_kind, 0, n * nb, st);
         cudaMemsetAsync(P->d_d, 0, sizeof(double) * 2 * n * nb, st);
@@ -561,6 +645,11 @@ void free_plan(Plan* P) {
     if (!P) return;
     for (void* p : P->allocations) cudaFree(p);
     for (cudaEvent_t e : P->events) cudaEventDestroy(e);
+    for (Plan::CachedGraph* g : {&P->g_factor, &P->g_solve, &P->g_resid, &P->g_corr})
+        if (g->exec) cudaGraphExecDestroy(g->exec);
+    if (P->join_in) cudaEventDestroy(P->join_in);
+    if (P->join_out) cudaEventDestroy(P->join_out);
+    if (P->own) cudaStreamDestroy(P->own);
     if (P->h_norms) cudaFreeHost(P->h_norms);
     if (P->h_info_pinned) cudaFreeHost(P->h_info_pinned);
     delete P;

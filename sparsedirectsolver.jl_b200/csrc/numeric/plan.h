@@ -13,7 +13,7 @@
 
 namespace sds {
 
-enum BufId : int32_t { BUF_FACTOR = 0, BUF_UFACTOR, BUF_CB, BUF_WORK };
+enum BufId : int32_t { BUF_FACTOR = 0, BUF_UFACTOR, BUF_CB, BUF_WORK, BUF_INV };
 
 struct ProgLaunch {
     LaunchKind kind;
@@ -40,7 +40,7 @@ struct ProfAcc {
 struct Plan {
     int64_t n = 0, nnz = 0, ns = 0;
     int structure = 0, nbatch = 1, precision = 0, elsize = 8, max_nrhs = 1;
-    int64_t factor_len = 0, cb_len = 0, ulen = 0, scr_len = 0, work_len = 0;
+    int64_t factor_len = 0, cb_len = 0, ulen = 0, scr_len = 0, work_len = 0, inv_len = 0;
     int nlevels = 0;
     int fsmall_max = 0;
     std::vector<DFront> fronts;
@@ -69,6 +69,8 @@ struct Plan {
     int32_t* d_members = nullptr;
     double* d_scratch = nullptr;
     void* d_work = nullptr;
+    void* d_inv = nullptr;          // inverses of the diagonal blocks of large Cholesky fronts
+    int64_t* d_inv_off = nullptr;
     double* d_amax = nullptr;
 
     std::vector<ProgLaunch> prog;
@@ -79,8 +81,12 @@ struct Plan {
     int64_t* d_scr_off = nullptr;
     int64_t* d_woff = nullptr;
     int64_t* d_uoff = nullptr;
-    int32_t* d_level_lists = nullptr;   // all fronts of each level (solve sweeps)
+    int32_t* d_level_lists = nullptr;   // fronts of each level for the solve sweeps: small first, then large
     std::vector<int64_t> level_list_off;
+    std::vector<int> level_nsmall, level_nlarge, level_maxw_small, level_maxw_large;
+    int32_t* d_rect_tiles = nullptr;    // (front, start) pairs: forward row tiles, backward column tiles
+    std::vector<int64_t> level_ftile_off, level_btile_off;
+    std::vector<int> level_nftile, level_nbtile;
 
     double* d_Y = nullptr;
     double* d_U = nullptr;
@@ -102,6 +108,17 @@ struct Plan {
     int launches_factor = 0;
     int launches_solve = 0;
     int64_t launches_done = 0;   // kernel launches issued by the last factor / solve calls
+
+    // CUDA graphs: the static launch program captured once per key (buffers, options) and replayed
+    struct CachedGraph {
+        std::vector<uint64_t> key;
+        cudaGraphExec_t exec = nullptr;
+        int64_t launches = 0;
+    };
+    bool use_graphs = true;
+    cudaStream_t own = nullptr;          // capture / replay stream, joined to the caller's by events
+    cudaEvent_t join_in = nullptr, join_out = nullptr;
+    CachedGraph g_factor, g_solve, g_resid, g_corr;
 
     bool profile = false;
     ProfAcc prof[PK_COUNT];

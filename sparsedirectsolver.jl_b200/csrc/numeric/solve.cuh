@@ -25,6 +25,8 @@ struct SweepArgs {
     int32_t nrhs;
     int32_t unit;              // unit diagonal (LDLT, LU)
     int32_t reorder;           // apply (forward) / undo (backward) the local pivot order
+    int32_t rect;              // 1: this CTA also does the rectangular part (L21 x / L21^T x)
+    const int32_t* tiles;      // split rectangular part of large fronts: (front, first row / column) pairs
 };
 
 struct DiagArgs {
@@ -73,6 +75,11 @@ struct NormArgs {
 
 template <typename T>
 cudaError_t launch_sweep(bool forward, const SweepArgs<T>& a, int nmembers, int maxw, cudaStream_t st);
+// rectangular part of large fronts: forward u += L21 x (row tiles), backward x1 -= L21^T x2 (column tiles)
+template <typename T>
+cudaError_t launch_sweep_rect(bool forward, const SweepArgs<T>& a, int ntiles, int nmembers, int maxw, cudaStream_t st);
+constexpr int RECT_ROWS = 256;   // rows of a forward tile
+constexpr int RECT_COLS = 16;    // columns of a backward tile (one warp each, 16 warps)
 cudaError_t launch_diag(const DiagArgs& a, int nmembers, cudaStream_t st);
 cudaError_t launch_permute(const PermArgs& a, int nmembers, cudaStream_t st);
 cudaError_t launch_residual(const ResidualArgs& a, int nmembers, cudaStream_t st);

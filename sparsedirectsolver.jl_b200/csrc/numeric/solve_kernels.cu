@@ -73,16 +73,23 @@ __global__ void __launch_bounds__(SOLVE_THREADS) forward_kernel(SweepArgs<T> A) 
         }
         __syncthreads();
     }
-    // L11 solve in blocks of 32 columns: warp 0 solves the block, the CTA updates the rows below it
+    // L11 solve in blocks of 32 columns: the CTA stages the diagonal block in shared memory, warp 0
+    // solves it, the CTA updates the rows of L11 below it
+    __shared__ double Ld[32][33];
     for (int jb = 0; jb < w; jb += 32) {
         const int bw = min(32, w - jb);
+        for (int q = tid; q < 32 * 32; q += nt) {
+            int i = q & 31, j = q >> 5;
+            Ld[i][j] = (i < bw && j < bw && i >= j) ? (double)L[(jb + i) + (int64_t)(jb + j) * f] : 0.0;
+        }
+        __syncthreads();
         if (warp == 0) {
             for (int r = 0; r < nrhs; ++r) {
                 double val = lane < bw ? xs[jb + lane + r * w] : 0.0;
                 for (int j = 0; j < bw; ++j) {
-                    if (!A.unit && lane == j) val /= (double)L[(jb + j) + (int64_t)(jb + j) * f];
+                    if (!A.unit && lane == j) val /= Ld[j][j];
                     double xj = __shfl_sync(0xffffffffu, val, j);
-                    if (lane > j && lane < bw) val -= (double)L[(jb + lane) + (int64_t)(jb + j) * f] * xj;
+                    if (lane > j) val -= Ld[lane][j] * xj;
                 }
                 if (lane < bw) xs[jb + lane + r * w] = val;
             }
@@ -105,20 +112,22 @@ __global__ void __launch_bounds__(SOLVE_THREADS) forward_kernel(SweepArgs<T> A) 
         }
         __syncthreads();
     }
-    // u += L21 x
-    for (int i = tid; i < m; i += nt) {
-        double acc[8];
-        for (int r0 = 0; r0 < nrhs; r0 += 8) {
-            const int rc = min(8, nrhs - r0);
+    // u += L21 x (large fronts: the row tiles of forward_rect_kernel)
+    if (A.rect) {
+        for (int i = tid; i < m; i += nt) {
+            double acc[8];
+            for (int r0 = 0; r0 < nrhs; r0 += 8) {
+                const int rc = min(8, nrhs - r0);
 #pragma unroll
-            for (int r = 0; r < 8; ++r) acc[r] = 0.0;
-            for (int j = 0; j < w; ++j) {
-                const double l = (double)L[w + i + (int64_t)j * f];
+                for (int r = 0; r < 8; ++r) acc[r] = 0.0;
+                for (int j = 0; j < w; ++j) {
+                    const double l = (double)L[w + i + (int64_t)j * f];
 #pragma unroll
-                for (int r = 0; r < 8; ++r)
-                    if (r < rc) acc[r] += l * xs[j + (r0 + r) * w];
+                    for (int r = 0; r < 8; ++r)
+                        if (r < rc) acc[r] += l * xs[j + (r0 + r) * w];
+                }
+                for (int r = 0; r < rc; ++r) u[i + (r0 + r) * m] += acc[r];
             }
-            for (int r = 0; r < rc; ++r) u[i + (r0 + r) * m] += acc[r];
         }
     }
     for (int q = tid; q < w * nrhs; q += nt) {
@@ -146,44 +155,54 @@ __global__ void __launch_bounds__(SOLVE_THREADS) backward_kernel(SweepArgs<T> A)
         int k = q % w, r = q / w;
         xs[q] = Y[fd.c0 + k + (int64_t)r * n];
     }
-    for (int q = tid; q < m * nrhs; q += nt) {
-        int i = q % m, r = q / m;
-        xb[q] = Y[rows[w + i] + (int64_t)r * n];
-    }
-    __syncthreads();
-    // x1 -= L21^T x2: one warp per column
-    for (int j = warp; j < w; j += nwarps) {
-        double acc[8];
-        for (int r0 = 0; r0 < nrhs; r0 += 8) {
-            const int rc = min(8, nrhs - r0);
-#pragma unroll
-            for (int r = 0; r < 8; ++r) acc[r] = 0.0;
-            for (int i = lane; i < m; i += 32) {
-                const double l = (double)L[w + i + (int64_t)j * f];
-#pragma unroll
-                for (int r = 0; r < 8; ++r)
-                    if (r < rc) acc[r] += l * xb[i + (r0 + r) * m];
-            }
-#pragma unroll
-            for (int r = 0; r < 8; ++r) {
-                double v = acc[r];
-                for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
-                if (lane == 0 && r < rc) xs[j + (r0 + r) * w] -= v;
-            }
+    if (A.rect) {
+        for (int q = tid; q < m * nrhs; q += nt) {
+            int i = q % m, r = q / m;
+            xb[q] = Y[rows[w + i] + (int64_t)r * n];
         }
     }
     __syncthreads();
-    // L11^T solve, blocks of 32 from the last
+    // x1 -= L21^T x2: one warp per column (large fronts: the column tiles of backward_rect_kernel)
+    if (A.rect) {
+        for (int j = warp; j < w; j += nwarps) {
+            double acc[8];
+            for (int r0 = 0; r0 < nrhs; r0 += 8) {
+                const int rc = min(8, nrhs - r0);
+#pragma unroll
+                for (int r = 0; r < 8; ++r) acc[r] = 0.0;
+                for (int i = lane; i < m; i += 32) {
+                    const double l = (double)L[w + i + (int64_t)j * f];
+#pragma unroll
+                    for (int r = 0; r < 8; ++r)
+                        if (r < rc) acc[r] += l * xb[i + (r0 + r) * m];
+                }
+#pragma unroll
+                for (int r = 0; r < 8; ++r) {
+                    double v = acc[r];
+                    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+                    if (lane == 0 && r < rc) xs[j + (r0 + r) * w] -= v;
+                }
+            }
+        }
+        __syncthreads();
+    }
+    // L11^T solve, blocks of 32 from the last, the diagonal block staged in shared memory
+    __shared__ double Ld[32][33];
     const int nblk = (w + 31) / 32;
     for (int bq = nblk - 1; bq >= 0; --bq) {
         const int jb = bq * 32, bw = min(32, w - jb);
+        for (int q = tid; q < 32 * 32; q += nt) {
+            int i = q & 31, j = q >> 5;
+            Ld[i][j] = (i < bw && j < bw && i >= j) ? (double)L[(jb + i) + (int64_t)(jb + j) * f] : 0.0;
+        }
+        __syncthreads();
         if (warp == 0) {
             for (int r = 0; r < nrhs; ++r) {
                 double val = lane < bw ? xs[jb + lane + r * w] : 0.0;
                 for (int j = bw - 1; j >= 0; --j) {
-                    if (!A.unit && lane == j) val /= (double)L[(jb + j) + (int64_t)(jb + j) * f];
+                    if (!A.unit && lane == j) val /= Ld[j][j];
                     double xj = __shfl_sync(0xffffffffu, val, j);
-                    if (lane < j) val -= (double)L[(jb + j) + (int64_t)(jb + lane) * f] * xj;
+                    if (lane < j) val -= Ld[j][lane] * xj;
                 }
                 if (lane < bw) xs[jb + lane + r * w] = val;
             }
@@ -206,22 +225,114 @@ __global__ void __launch_bounds__(SOLVE_THREADS) backward_kernel(SweepArgs<T> A)
     }
 }
 
+// u[rows of the tile] += L21[rows, :] x1 for one row tile of a large front (x1 from Y, pivoted order)
+template <typename T>
+__global__ void __launch_bounds__(RECT_ROWS) forward_rect_kernel(SweepArgs<T> A) {
+    extern __shared__ double xs[];  // w x nrhs
+    const int s = A.tiles[2 * blockIdx.x], row0 = A.tiles[2 * blockIdx.x + 1];
+    const int member = A.members ? A.members[blockIdx.y] : blockIdx.y;
+    const DFront fd = A.fronts[s];
+    const int f = fd.f, w = fd.w, m = f - w, nrhs = A.nrhs;
+    const int64_t n = A.n;
+    const T* L = A.fac + (int64_t)member * A.factor_len + fd.panel;
+    const double* Y = A.Y + (int64_t)member * n * nrhs;
+    double* u = A.U + (int64_t)member * A.ulen + A.uoff[s];
+    for (int q = threadIdx.x; q < w * nrhs; q += blockDim.x) {
+        int k = q % w, r = q / w;
+        xs[q] = Y[fd.c0 + k + (int64_t)r * n];
+    }
+    __syncthreads();
+    const int i = row0 + threadIdx.x;
+    if (i >= m) return;
+    for (int r0 = 0; r0 < nrhs; r0 += 8) {
+        const int rc = min(8, nrhs - r0);
+        double acc[8];
+#pragma unroll
+        for (int r = 0; r < 8; ++r) acc[r] = 0.0;
+        for (int j = 0; j < w; ++j) {
+            const double l = (double)L[w + i + (int64_t)j * f];
+#pragma unroll
+            for (int r = 0; r < 8; ++r)
+                if (r < rc) acc[r] += l * xs[j + (r0 + r) * w];
+        }
+        for (int r = 0; r < rc; ++r) u[i + (r0 + r) * m] += acc[r];
+    }
+}
+
+// Y[c0 + j] -= (L21^T x2)[j] for one tile of RECT_COLS columns of a large front, one warp per column;
+// x2 gathered from the finished ancestor rows
+template <typename T>
+__global__ void __launch_bounds__(RECT_COLS * 32) backward_rect_kernel(SweepArgs<T> A) {
+    const int s = A.tiles[2 * blockIdx.x], col0 = A.tiles[2 * blockIdx.x + 1];
+    const int member = A.members ? A.members[blockIdx.y] : blockIdx.y;
+    const DFront fd = A.fronts[s];
+    const int f = fd.f, w = fd.w, m = f - w, nrhs = A.nrhs;
+    const int64_t n = A.n;
+    const T* L = A.fac + (int64_t)member * A.factor_len + fd.panel;
+    double* Y = A.Y + (int64_t)member * n * nrhs;
+    const int32_t* rows = A.rowval + fd.row_begin + w;
+    const int lane = threadIdx.x & 31;
+    const int j = col0 + (threadIdx.x >> 5);
+    if (j >= w) return;
+    for (int r0 = 0; r0 < nrhs; r0 += 8) {
+        const int rc = min(8, nrhs - r0);
+        double acc[8];
+#pragma unroll
+        for (int r = 0; r < 8; ++r) acc[r] = 0.0;
+        for (int i = lane; i < m; i += 32) {
+            const double l = (double)L[w + i + (int64_t)j * f];
+            const int64_t g = rows[i];
+#pragma unroll
+            for (int r = 0; r < 8; ++r)
+                if (r < rc) acc[r] += l * Y[g + (int64_t)(r0 + r) * n];
+        }
+#pragma unroll
+        for (int r = 0; r < 8; ++r) {
+            double v = acc[r];
+            for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+            if (lane == 0 && r < rc) Y[fd.c0 + j + (int64_t)(r0 + r) * n] -= v;
+        }
+    }
+}
+
+template <typename T>
+cudaError_t launch_sweep_rect(bool forward, const SweepArgs<T>& a, int ntiles, int nmembers, int maxw, cudaStream_t st) {
+    if (ntiles == 0) return cudaSuccess;
+    dim3 grid(ntiles, nmembers);
+    if (forward) {
+        size_t smem = (size_t)maxw * a.nrhs * sizeof(double);
+        forward_rect_kernel<T><<<grid, RECT_ROWS, smem, st>>>(a);
+    } else {
+        backward_rect_kernel<T><<<grid, RECT_COLS * 32, 0, st>>>(a);
+    }
+    return cudaGetLastError();
+}
+
+template cudaError_t launch_sweep_rect<double>(bool, const SweepArgs<double>&, int, int, int, cudaStream_t);
+template cudaError_t launch_sweep_rect<float>(bool, const SweepArgs<float>&, int, int, int, cudaStream_t);
+
 template <typename T>
 cudaError_t launch_sweep(bool forward, const SweepArgs<T>& a, int nmembers, int maxw, cudaStream_t st) {
     if (a.count == 0) return cudaSuccess;
     size_t smem = (size_t)maxw * a.nrhs * sizeof(double);
     dim3 grid(a.count, nmembers);
-    cudaError_t e;
-    if (forward) {
-        e = cudaFuncSetAttribute(forward_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        if (e != cudaSuccess) return e;
-        forward_kernel<T><<<grid, SOLVE_THREADS, smem, st>>>(a);
-    } else {
-        e = cudaFuncSetAttribute(backward_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        if (e != cudaSuccess) return e;
-        backward_kernel<T><<<grid, SOLVE_THREADS, smem, st>>>(a);
-    }
+    if (forward) forward_kernel<T><<<grid, SOLVE_THREADS, smem, st>>>(a);
+    else backward_kernel<T><<<grid, SOLVE_THREADS, smem, st>>>(a);
     return cudaGetLastError();
+}
+
+cudaError_t prepare_solve_kernels(int max_smem) {
+    cudaError_t e = cudaSuccess;
+    auto set = [&](const void* k) {
+        if (e == cudaSuccess) e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, max_smem);
+    };
+    set((const void*)forward_kernel<double>);
+    set((const void*)forward_kernel<float>);
+    set((const void*)backward_kernel<double>);
+    set((const void*)backward_kernel<float>);
+    set((const void*)forward_rect_kernel<double>);
+    set((const void*)forward_rect_kernel<float>);
+    return e;
 }
 
 template cudaError_t launch_sweep<double>(bool, const SweepArgs<double>&, int, int, cudaStream_t);

@@ -228,3 +228,25 @@ def test_phase_order_errors(torch_cuda):
         ds.execute("solve", None, np.ones(64))
     with pytest.raises(InvalidValueError):
         ds.setparam("pivot_threshold", -1.0)
+
+
+@pytest.mark.parametrize("structure", ["SPD", "S", "G"])
+def test_graph_replay_matches_eager(torch_cuda, structure):
+    from sdsb200._native import numeric_lib
+
+    A = {"SPD": lambda: M.lap3d(16, 16, 16, seed=4), "S": lambda: small_kkt(16, 16, 100, seed=4),
+         "G": lambda: M.convection_diffusion3d(12, 12, 12, seed=4)}[structure]()
+    b = M.rhs(A.shape[0], 2, seed=5)
+    out = []
+    for graphs in (0, 1):
+        ds = _solver(A, structure, reordering_alg="nd", ir_n_steps=2)
+        ds.execute("analysis")
+        numeric_lib().sdsb200_set_graphs(ds._plan, graphs)
+        for _ in range(2):  # second call replays the captured graph
+            ds.execute("factorization")
+            x = ds.execute("solve", None, b).cpu().numpy()
+        out.append((ds.factor_host()[0], x, ds.stats_host()))
+        assert M.scaled_backward_error(A, x, b) <= BERR
+    assert np.array_equal(out[0][0], out[1][0])
+    assert np.array_equal(out[0][1], out[1][1])
+    assert np.array_equal(out[0][2], out[1][2])
