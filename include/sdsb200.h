@@ -149,12 +149,17 @@ int sdsb200_set_interrupt(sdsb200_plan* plan, const volatile int32_t* h_flag);
  * then polled before a factorization and before each refinement step, not between launch groups. */
 int sdsb200_set_graphs(sdsb200_plan* plan, int32_t on);
 
+/* Solve engine (on by default): one cooperative persistent launch per solve when a single batch member
+ * is active (off: one launch per level and sweep, the engine of uniform batches). */
+int sdsb200_set_persistent(sdsb200_plan* plan, int32_t on);
+
 /* Profiling mode (on != 0): CUDA events around every launch of the following factor and solve
  * calls, accumulated per kernel kind (resets the totals). Costs one event record per launch. */
 int sdsb200_set_profiling(sdsb200_plan* plan, int32_t on);
 
 /* Plan facts: "ns", "nlevels", "factor_len", "cb_len", "launches_factor", "launches_solve",
- * "launches_done" (kernel launches of the last factor or solve call), "device_bytes", "flops";
+ * "launches_done" (kernel launches of the last factor or solve call), "device_bytes", "flops",
+ * "solve_status" (synchronizes; nonzero when a bounded wait of the persistent solve gave up);
  * with profiling, "prof_ms:<kind>", "prof_flops:<kind>", "prof_bytes:<kind>", "prof_launches:<kind>"
  * for kinds small assemble panel gemm pivot scale stats fwd bwd diag permute residual.
  * Returns -1 for an unknown name. */

@@ -4,6 +4,7 @@
 #include <cuda_runtime.h>
 #include <math.h>
 #include <stdint.h>
+#include <stdlib.h>
 #include <string.h>
 
 #include <algorithm>
@@ -58,6 +59,7 @@ void prof_end(Plan* P, cudaStream_t st, int kind, double flops, double bytes) {
     size_t k = P->prof_next;
     cudaEventRecord(P->events[k + 1], st);
     P->pending.push_back({kind, {flops, bytes}});
+    P->pending_level.push_back(P->cur_level);
     P->prof_next += 2;
 }
 
@@ -68,12 +70,14 @@ void prof_resolve(Plan* P) {
         cudaEventSynchronize(P->events[2 * q + 1]);
         cudaEventElapsedTime(&ms, P->events[2 * q], P->events[2 * q + 1]);
         ProfAcc& a = P->prof[P->pending[q].first];
+        P->records.push_back({P->pending[q].first, P->pending_level[q], (double)ms});
         a.ms += ms;
         a.flops += P->pending[q].second.first;
         a.bytes += P->pending[q].second.second;
         a.launches++;
     }
     P->pending.clear();
+    P->pending_level.clear();
     P->prof_next = 0;
 }
 
@@ -89,6 +93,7 @@ int prof_kind_of(LaunchKind k) {
         case L_GEMM: return PK_GEMM;
         case L_PIVOT_FRONT: return PK_PIVOT;
         case L_SCALE: return PK_SCALE;
+        case L_BLOCKINV: return PK_PANEL;
         default: return PK_STATS;
     }
 }
@@ -167,6 +172,7 @@ int run_factor(Plan* P, const double* nzval, double eps, double u, int pivot, in
             last_level = L.level;
         }
         cudaError_t e = cudaSuccess;
+        P->cur_level = L.level;
         prof_begin(P, st);
         switch (L.kind) {
             case L_SMALL: {
@@ -270,6 +276,27 @@ int run_factor(Plan* P, const double* nzval, double eps, double u, int pivot, in
                 e = launch_scale_ld_front<T>(P->structure, a, L.maxw, nm, st);
                 break;
             }
+            case L_BLOCKINV: {
+                BlockInvArgs<T> a{};
+                a.fronts = P->d_fronts;
+                a.tasks = P->d_binv_tasks;
+                a.count = P->n_binv_tasks;
+                a.dinv_off = P->d_dinv_off;
+                a.members = members;
+                a.panels = factor;
+                a.dinv = static_cast<T*>(P->d_dinv_L);
+                a.factor_len = P->factor_len;
+                a.dinv_len = P->dinv_len;
+                a.finfo = P->d_finfo;
+                a.ns = (int32_t)P->ns;
+                e = launch_block_inv<T>(a, nm, st);
+                if (e == cudaSuccess && P->structure == STRUCT_G) {
+                    a.panels = ufactor;
+                    a.dinv = static_cast<T*>(P->d_dinv_U);
+                    e = launch_block_inv<T>(a, nm, st);
+                }
+                break;
+            }
             case L_STATS: {
                 StatsArgs a{};
                 a.stats = P->d_stats;
@@ -314,6 +341,7 @@ int run_sweeps(Plan* P, int nrhs, bool transpose, cudaStream_t st) {
     a.reorder = ldl || (gen && !transpose);
     a.tiles = P->d_rect_tiles;
     auto level_sweep = [&](bool fwd, int L) -> int {
+        P->cur_level = L;
         const int64_t off = P->level_list_off[L];
         const int ns_ = P->level_nsmall[L], nl_ = P->level_nlarge[L];
         double ent = P->level_panel_entries[L];   // booked on the first launch of the level
@@ -370,6 +398,66 @@ int run_sweeps(Plan* P, int nrhs, bool transpose, cudaStream_t st) {
     }
     return SDSB200_OK;
 }
+
+// the whole solve in one cooperative launch (one active batch member)
+template <typename T>
+int run_persistent(Plan* P, int nrhs, bool transpose, const double* in, int64_t ldin, double* out, int64_t ldout,
+                   int mode, cudaStream_t st) {
+    const bool gen = P->structure == STRUCT_G, ldl = P->structure == STRUCT_S;
+    const int32_t member = 0;
+    (void)member;
+    PersistArgs<T> a{};
+    SweepArgs<T> base{};
+    base.fronts = P->d_fronts;
+    base.members = nullptr;
+    base.Y = P->d_Y;
+    base.U = P->d_U;
+    base.uoff = P->d_uoff;
+    base.child_list = P->maps.child_list;
+    base.relind = P->maps.relind;
+    base.rowval = P->maps.rowval;
+    base.piv = P->d_piv;
+    base.n = P->n; base.factor_len = P->factor_len; base.ulen = P->ulen;
+    base.nrhs = nrhs;
+    base.unit = P->structure != STRUCT_SPD;
+    base.rect = 1;
+    const T* factor = static_cast<const T*>(P->d_factor);
+    const T* ufactor = static_cast<const T*>(P->d_ufactor);
+    const T* dL = static_cast<const T*>(P->d_dinv_L);
+    const T* dU = static_cast<const T*>(P->d_dinv_U);
+    a.fw = base;
+    a.fw.fac = (gen && transpose) ? ufactor : factor;
+    a.fw.reorder = ldl || (gen && !transpose);
+    a.bw = base;
+    a.bw.fac = (gen && !transpose) ? ufactor : factor;
+    a.bw.reorder = ldl || (gen && transpose);
+    a.dinv_fw = (gen && transpose) ? dU : dL;
+    a.dinv_bw = (gen && !transpose) ? dU : dL;
+    a.dinv_off = P->d_dinv_off;
+    a.lev_small = P->d_p_lev_small;
+    a.lev_large = P->d_p_lev_large;
+    a.lev_maxblk = P->d_p_lev_maxblk;
+    a.list = P->d_p_list;
+    a.nlevels = P->nlevels;
+    a.d = P->d_d;
+    a.kind = P->d_kind;
+    a.diag_mode = P->structure == STRUCT_SPD ? 0 : (ldl ? 2 : 1);
+    a.perm = P->d_perm0;
+    a.in = in; a.ldin = ldin; a.out = out; a.ldout = ldout; a.mode = mode;
+    a.xtmp = P->d_xtmp;
+    a.barrier = P->d_barrier;
+    a.status = P->d_solve_status;
+    const size_t smem = sizeof(double) * std::max<size_t>((size_t)P->p_maxw_small * nrhs, 2 * SOLVE_BLK * (size_t)nrhs);
+    const int grid = persistent_solve_grid<T>(smem);
+    if (grid <= 0) return fail(SDSB200_CUDA_ERROR, "no co-resident grid for the persistent solve");
+    CK(cudaMemsetAsync(P->d_barrier, 0, sizeof(unsigned int), st), "barrier reset");
+    prof_begin(P, st);
+    cudaError_t e = launch_persistent_solve<T>(a, grid, smem, st);
+    prof_end(P, st, PK_FWD, 0.0, 0.0);
+    return e == cudaSuccess ? SDSB200_OK : cuda_fail(e, "persistent solve");
+}
+
+bool use_persistent(const Plan* P) { return P->nact == 1 && P->all_members && P->persistent; }
 
 int sweeps(Plan* P, int nrhs, bool transpose, cudaStream_t st) {
     return P->elsize == 8 ? run_sweeps<double>(P, nrhs, transpose, st) : run_sweeps<float>(P, nrhs, transpose, st);
@@ -523,6 +611,9 @@ int sdsb200_solve(sdsb200_plan* plan, double* X, int64_t ldx, const double* B, i
     std::vector<uint64_t> key = {(uint64_t)(uintptr_t)X, (uint64_t)ldx, (uint64_t)(uintptr_t)B, (uint64_t)ldb, common,
                                  (uint64_t)P->nact};
     int rc = run_graph(P, P->g_solve, key, st, [&](cudaStream_t s) -> int {
+        if (use_persistent(P))
+            return P->elsize == 8 ? run_persistent<double>(P, nrhs, transpose, B, ldb, X, ldx, 0, s)
+                                  : run_persistent<float>(P, nrhs, transpose, B, ldb, X, ldx, 0, s);
         int r = permute(P, 0, B, ldb, nullptr, 0, nrhs, s);
         if (r) return r;
         r = sweeps(P, nrhs, transpose, s);
@@ -582,6 +673,9 @@ int sdsb200_solve(sdsb200_plan* plan, double* X, int64_t ldx, const double* B, i
         }
         std::vector<uint64_t> ckey = key;
         rc = run_graph(P, P->g_corr, ckey, st, [&](cudaStream_t s) -> int {
+            if (use_persistent(P))
+                return P->elsize == 8 ? run_persistent<double>(P, nrhs, transpose, P->d_R, P->n, X, ldx, 2, s)
+                                      : run_persistent<float>(P, nrhs, transpose, P->d_R, P->n, X, ldx, 2, s);
             int r = permute(P, 0, P->d_R, P->n, nullptr, 0, nrhs, s);
             if (r) return r;
             r = sweeps(P, nrhs, transpose, s);
@@ -674,6 +768,15 @@ int sdsb200_set_members(sdsb200_plan* plan, const int32_t* h_members, int32_t na
     return SDSB200_OK;
 }
 
+int sdsb200_set_persistent(sdsb200_plan* plan, int32_t on) {
+    Plan* P = reinterpret_cast<Plan*>(plan);
+    if (!P) return fail(SDSB200_INVALID_VALUE, "plan is NULL");
+    P->persistent = on != 0;
+    for (Plan::CachedGraph* g : {&P->g_solve, &P->g_corr})
+        g->key.clear();
+    return SDSB200_OK;
+}
+
 int sdsb200_set_graphs(sdsb200_plan* plan, int32_t on) {
     Plan* P = reinterpret_cast<Plan*>(plan);
     if (!P) return fail(SDSB200_INVALID_VALUE, "plan is NULL");
@@ -685,6 +788,7 @@ int sdsb200_set_profiling(sdsb200_plan* plan, int32_t on) {
     Plan* P = reinterpret_cast<Plan*>(plan);
     if (!P) return fail(SDSB200_INVALID_VALUE, "plan is NULL");
     P->profile = on != 0;
+    P->records.clear();
     for (int k = 0; k < PK_COUNT; ++k) P->prof[k] = ProfAcc();
     P->pending.clear();
     P->prof_next = 0;
@@ -712,6 +816,25 @@ double sdsb200_plan_stat(const sdsb200_plan* plan, const char* name) {
     if (nm == "flops") return P->flops;
     if (nm == "elsize") return P->elsize;
     if (nm == "launches_done") return (double)P->launches_done;
+    if (nm == "solve_status") {
+        int32_t v = 0;
+        cudaDeviceSynchronize();
+        cudaMemcpy(&v, P->d_solve_status, sizeof(v), cudaMemcpyDeviceToHost);
+        return v;
+    }
+    if (nm == "prof_records") return (double)P->records.size();
+    if (nm.rfind("prof_record:", 0) == 0) {
+        // "prof_record:<i>:kind|level|ms"
+        size_t a = nm.find(':', 12);
+        if (a == std::string::npos) return -1;
+        size_t i = (size_t)atol(nm.substr(12, a - 12).c_str());
+        if (i >= P->records.size()) return -1;
+        std::string f = nm.substr(a + 1);
+        if (f == "kind") return P->records[i].kind;
+        if (f == "level") return P->records[i].level;
+        if (f == "ms") return P->records[i].ms;
+        return -1;
+    }
     for (int k = 0; k < PK_COUNT; ++k) {
         std::string kn(PROF_NAMES[k]);
         if (nm == "prof_ms:" + kn) return P->prof[k].ms;

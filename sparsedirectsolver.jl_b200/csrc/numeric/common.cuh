@@ -61,6 +61,7 @@ enum LaunchKind : int32_t {
     L_PIVOT_FRONT,     // large LDLT / LU: cooperative pivoting over the panel
     L_STATS,           // statistics reduction
     L_SCALE,           // W = L21 D of large LDLT / LU fronts
+    L_BLOCKINV,        // inverses of the diagonal blocks of the wide fronts (solve)
 };
 
 struct Launch {

@@ -272,15 +272,19 @@ cudaError_t launch_gemm(const GemmArgs<T>& a, int nmembers, cudaStream_t st) {
 }
 
 // ---------------------------------------------------------------------------
-// Diagonal block of a large Cholesky front (64 x 64 at column kb): factor in shared memory with the
-// static clamp and failure rule of the fused kernels, write L11 back, write inv(L11) (ld 64) to
-// scratch for the trsm of the rows below as a GEMM (X = B inv(L11)^T).
+// Diagonal block of a large Cholesky front (64 x 64 at column kb): factor with the static clamp and
+// failure rule of the fused kernels, write L11 back, write inv(L11) (ld 64) to scratch for the trsm
+// of the rows below as a GEMM (X = B inv(L11)^T).
+// Each thread owns fixed entries of the lower triangle and keeps them in registers; a step publishes
+// one column (or row) through a double-buffered shared vector, so each pivot costs one barrier.
+// Factorization: right-looking on the unscaled columns (a_il -= a_ij a_lj / d_j with d_j the clamped
+// pivot), scaled by sqrt(d_j) at the end. Inverse: right-looking substitution on the identity.
 template <typename T>
 __global__ void __launch_bounds__(256) chol_diag_kernel(CholDiagArgs<T> A) {
-    constexpr int NB = CHOL_NB;
-    extern __shared__ __align__(16) unsigned char diag_smem[];
-    double(*L)[NB + 1] = reinterpret_cast<double(*)[NB + 1]>(diag_smem);
-    double(*X)[NB + 1] = reinterpret_cast<double(*)[NB + 1]>(diag_smem + sizeof(double) * NB * (NB + 1));
+    constexpr int NB = CHOL_NB, NE = NB * (NB + 1) / 2, SLOTS = (NE + 255) / 256;
+    __shared__ double colv[2][NB];
+    __shared__ double rowv[2][NB];
+    __shared__ double dpiv[NB];
     __shared__ int s_status;
     const int s = A.list[blockIdx.x];
     const int member = A.members ? A.members[blockIdx.y] : blockIdx.y;
@@ -291,40 +295,49 @@ __global__ void __launch_bounds__(256) chol_diag_kernel(CholDiagArgs<T> A) {
     if (kb >= w) return;
     const int nbb = min(NB, w - kb);
     T* P = A.factor + (int64_t)member * A.factor_len + fd.panel;
-    const int tid = threadIdx.x, nt = blockDim.x;
-    for (int q = tid; q < NB * NB; q += nt) {
-        int i = q % NB, j = q / NB;
-        L[i][j] = (i < nbb && j < nbb && i >= j) ? (double)P[(kb + i) + (int64_t)(kb + j) * f] : 0.0;
+    const int tid = threadIdx.x;
+    // owned entries: e = tid + 256 k of the column-major lower triangle
+    int ri[SLOTS], ci[SLOTS];
+    double a[SLOTS], x[SLOTS];
+#pragma unroll
+    for (int k = 0; k < SLOTS; ++k) {
+        int e = tid + 256 * k, col = 0;
+        if (e < NE) {
+            int rem = e;
+            while (rem >= NB - col) { rem -= NB - col; ++col; }
+            ri[k] = col + rem;
+            ci[k] = col;
+        } else {
+            ri[k] = -1;
+            ci[k] = NB;
+        }
+        const bool in = ri[k] >= 0 && ri[k] < nbb && ci[k] < nbb;
+        a[k] = in ? (double)P[(kb + ri[k]) + (int64_t)(kb + ci[k]) * f] : 0.0;
+        x[k] = (in && ri[k] == ci[k]) ? 1.0 : 0.0;
     }
     if (tid == 0) s_status = 0;
-    __syncthreads();
     const double eps = A.eps;
+    int status = 0;
     for (int j = 0; j < nbb; ++j) {
-        double ajj = L[j][j];
-        bool ok = ajj > eps || (eps > 0 && ajj >= 0);
+        double* cv = colv[j & 1];
+#pragma unroll
+        for (int k = 0; k < SLOTS; ++k)
+            if (ci[k] == j) cv[ri[k]] = a[k];
+        __syncthreads();
+        const double ajj = cv[j];
+        const bool ok = ajj > eps || (eps > 0 && ajj >= 0);
         if (!ok) {
-            if (tid == 0) s_status = j + 1;
+            status = j + 1;
             break;
         }
-        double djj = sqrt(fmax(ajj, eps));
-        double inv = 1.0 / djj;
-        __syncthreads();
-        for (int i = j + 1 + tid; i < nbb; i += nt) L[i][j] = (double)T(L[i][j] * inv);
-        if (tid == 0) L[j][j] = (double)T(djj);
-        __syncthreads();
-        const int r = nbb - j - 1;
-        for (int q = tid; q < r * r; q += nt) {
-            int i = j + 1 + q % r, l = j + 1 + q / r;
-            if (i >= l) L[i][l] = (double)T(L[i][l] - L[i][j] * L[l][j]);
-        }
-        __syncthreads();
+        const double dj = fmax(ajj, eps);
+        const double invd = 1.0 / dj;
+        if (tid == 0) dpiv[j] = dj;
+#pragma unroll
+        for (int k = 0; k < SLOTS; ++k)
+            if (ci[k] > j && ri[k] < nbb) a[k] -= cv[ri[k]] * (cv[ci[k]] * invd);
     }
     __syncthreads();
-    const int status = s_status;
-    for (int q = tid; q < nbb * nbb; q += nt) {
-        int i = q % nbb, j = q / nbb;
-        P[(kb + i) + (int64_t)(kb + j) * f] = i >= j ? T(L[i][j]) : T(0);
-    }
     if (status) {
         if (tid == 0) {
             int64_t* S = A.stats + ((int64_t)member * A.ns + s) * NSTAT;
@@ -334,43 +347,148 @@ __global__ void __launch_bounds__(256) chol_diag_kernel(CholDiagArgs<T> A) {
         }
         return;
     }
+    // scale: L_il = a_il / sqrt(d_l), L_ll = sqrt(d_l); rounded to the factor precision
+#pragma unroll
+    for (int k = 0; k < SLOTS; ++k) {
+        if (ri[k] < 0 || ri[k] >= nbb || ci[k] >= nbb) continue;
+        const double sd = sqrt(dpiv[ci[k]]);
+        a[k] = (double)T(ri[k] == ci[k] ? sd : a[k] / sd);
+        P[(kb + ri[k]) + (int64_t)(kb + ci[k]) * f] = T(a[k]);
+    }
+    // the strict upper triangle of the diagonal block is stored as zeros
+    for (int q = tid; q < nbb * nbb; q += 256) {
+        int i = q % nbb, j = q / nbb;
+        if (i < j) P[(kb + i) + (int64_t)(kb + j) * f] = T(0);
+    }
     if (tid == 0 && kb + nbb == w) {
         int64_t* S = A.stats + ((int64_t)member * A.ns + s) * NSTAT;
         S[ST_NPOS] = w;
         S[ST_INFO] = 0;
     }
     if (kb + nbb >= f) return;  // no rows below: no trsm
-    // inverse of the lower-triangular block, one column per thread (forward substitution)
-    for (int j = tid; j < nbb; j += nt) {
-        for (int i = 0; i < nbb; ++i) {
-            double acc = i == j ? 1.0 : 0.0;
-            for (int l = j; l < i; ++l) acc -= L[i][l] * X[l][j];
-            X[i][j] = i < j ? 0.0 : acc / L[i][i];
+    // inverse: X = L^{-1}; step l divides row l by L_ll and subtracts L_il X_l. from the rows below
+    for (int l = 0; l < nbb; ++l) {
+        double* cv = colv[l & 1];
+        double* rv = rowv[l & 1];
+#pragma unroll
+        for (int k = 0; k < SLOTS; ++k) {
+            if (ci[k] == l) cv[ri[k]] = a[k];
         }
+        __syncthreads();
+        const double rl = 1.0 / cv[l];
+#pragma unroll
+        for (int k = 0; k < SLOTS; ++k)
+            if (ri[k] == l) {
+                x[k] *= rl;
+                rv[ci[k]] = x[k];
+            }
+        __syncthreads();
+#pragma unroll
+        for (int k = 0; k < SLOTS; ++k)
+            if (ri[k] > l && ri[k] < nbb && ci[k] <= l) x[k] -= cv[ri[k]] * rv[ci[k]];
+    }
+    T* inv = A.inv + (int64_t)member * A.inv_len + A.inv_off[blockIdx.x];
+    for (int q = tid; q < NB * NB; q += 256) {
+        int i = q % NB, j = q / NB;
+        if (i < j || i >= nbb) inv[i + (int64_t)j * NB] = T(0);
     }
     __syncthreads();
-    T* inv = A.inv + (int64_t)member * A.inv_len + A.inv_off[blockIdx.x];
-    for (int q = tid; q < NB * NB; q += nt) {
-        int i = q % NB, j = q / NB;
-        inv[i + (int64_t)j * NB] = (i < nbb && j < nbb) ? T(X[i][j]) : T(0);
-    }
+#pragma unroll
+    for (int k = 0; k < SLOTS; ++k)
+        if (ri[k] >= 0 && ri[k] < nbb && ci[k] < nbb) inv[ri[k] + (int64_t)ci[k] * NB] = T(x[k]);
 }
+
+// inverse of one 64 x 64 diagonal block of a panel (lower triangle as stored; unit or not), with the
+// register-owned right-looking substitution of chol_diag_kernel
+template <typename T>
+__global__ void __launch_bounds__(256) block_inv_kernel(BlockInvArgs<T> A) {
+    constexpr int NB = CHOL_NB, NE = NB * (NB + 1) / 2, SLOTS = (NE + 255) / 256;
+    __shared__ double colv[2][NB];
+    __shared__ double rowv[2][NB];
+    const int s = A.tasks[2 * blockIdx.x], b = A.tasks[2 * blockIdx.x + 1];
+    const int member = A.members ? A.members[blockIdx.y] : blockIdx.y;
+    if (A.finfo && A.finfo[(int64_t)member * A.ns + s] != 0) return;
+    const DFront fd = A.fronts[s];
+    const int f = fd.f, jb = b * NB, nbb = min(NB, fd.w - jb);
+    const T* P = A.panels + (int64_t)member * A.factor_len + fd.panel;
+    T* inv = A.dinv + (int64_t)member * A.dinv_len + A.dinv_off[s] + (int64_t)b * NB * NB;
+    const int tid = threadIdx.x;
+    int ri[SLOTS], ci[SLOTS];
+    double a[SLOTS], x[SLOTS];
+#pragma unroll
+    for (int k = 0; k < SLOTS; ++k) {
+        int e = tid + 256 * k, col = 0;
+        if (e < NE) {
+            int rem = e;
+            while (rem >= NB - col) { rem -= NB - col; ++col; }
+            ri[k] = col + rem;
+            ci[k] = col;
+        } else {
+            ri[k] = -1;
+            ci[k] = NB;
+        }
+        const bool in = ri[k] >= 0 && ri[k] < nbb && ci[k] < nbb;
+        a[k] = in ? (double)P[(jb + ri[k]) + (int64_t)(jb + ci[k]) * f] : 0.0;
+        x[k] = (in && ri[k] == ci[k]) ? 1.0 : 0.0;
+    }
+    for (int l = 0; l < nbb; ++l) {
+        double* cv = colv[l & 1];
+        double* rv = rowv[l & 1];
+#pragma unroll
+        for (int k = 0; k < SLOTS; ++k)
+            if (ci[k] == l) cv[ri[k]] = a[k];
+        __syncthreads();
+        const double rl = 1.0 / cv[l];
+#pragma unroll
+        for (int k = 0; k < SLOTS; ++k)
+            if (ri[k] == l) {
+                x[k] *= rl;
+                rv[ci[k]] = x[k];
+            }
+        __syncthreads();
+#pragma unroll
+        for (int k = 0; k < SLOTS; ++k)
+            if (ri[k] > l && ri[k] < nbb && ci[k] <= l) x[k] -= cv[ri[k]] * rv[ci[k]];
+    }
+    for (int q = tid; q < NB * NB; q += 256) {
+        int i = q % NB, j = q / NB;
+        if (i < j || i >= nbb) inv[i + (int64_t)j * NB] = T(0);
+    }
+    __syncthreads();
+#pragma unroll
+    for (int k = 0; k < SLOTS; ++k)
+        if (ri[k] >= 0 && ri[k] < nbb && ci[k] < nbb) inv[ri[k] + (int64_t)ci[k] * NB] = T(x[k]);
+}
+
+template <typename T>
+cudaError_t launch_block_inv(const BlockInvArgs<T>& a, int nmembers, cudaStream_t st) {
+    if (a.count == 0) return cudaSuccess;
+    dim3 grid(a.count, nmembers);
+    block_inv_kernel<T><<<grid, 256, 0, st>>>(a);
+    return cudaGetLastError();
+}
+
+template cudaError_t launch_block_inv<double>(const BlockInvArgs<double>&, int, cudaStream_t);
+template cudaError_t launch_block_inv<float>(const BlockInvArgs<float>&, int, cudaStream_t);
 
 template <typename T>
 cudaError_t launch_chol_diag(const CholDiagArgs<T>& a, int nmembers, cudaStream_t st) {
     if (a.count == 0) return cudaSuccess;
     dim3 grid(a.count, nmembers);
-    const int smem = 2 * sizeof(double) * CHOL_NB * (CHOL_NB + 1);
-    chol_diag_kernel<T><<<grid, 256, smem, st>>>(a);
+    chol_diag_kernel<T><<<grid, 256, 0, st>>>(a);
     return cudaGetLastError();
 }
 
 cudaError_t prepare_dense_kernels(int max_smem) {
-    cudaError_t e = cudaFuncSetAttribute((const void*)chol_diag_kernel<double>,
-                                         cudaFuncAttributeMaxDynamicSharedMemorySize, max_smem);
-    if (e == cudaSuccess)
-        e = cudaFuncSetAttribute((const void*)chol_diag_kernel<float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 max_smem);
+    cudaError_t e = cudaSuccess;
+    auto set = [&](const void* k) {
+        if (e != cudaSuccess) return;
+        cudaFuncAttributes fa;
+        e = cudaFuncGetAttributes(&fa, k);
+        if (e == cudaSuccess)
+            e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, max_smem - (int)fa.sharedSizeBytes);
+    };
+    (void)set;
     return e;
 }
 

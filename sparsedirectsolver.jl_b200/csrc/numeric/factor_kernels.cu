@@ -214,7 +214,11 @@ cudaError_t launch_small(int structure, const SmallArgs<T>& a, int count, int nm
 cudaError_t prepare_factor_kernels(int max_smem) {
     cudaError_t e = cudaSuccess;
     auto set = [&](const void* k) {
-        if (e == cudaSuccess) e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, max_smem);
+        if (e != cudaSuccess) return;
+        cudaFuncAttributes fa;
+        e = cudaFuncGetAttributes(&fa, k);
+        if (e == cudaSuccess)
+            e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, max_smem - (int)fa.sharedSizeBytes);
     };
     set((const void*)small_front_kernel<double, STRUCT_SPD>);
     set((const void*)small_front_kernel<double, STRUCT_S>);

@@ -157,6 +157,23 @@ template <typename T>
 cudaError_t launch_gemm(const GemmArgs<T>& a, int nmembers, cudaStream_t st);
 template <typename T>
 cudaError_t launch_chol_diag(const CholDiagArgs<T>& a, int nmembers, cudaStream_t st);
+// Inverses of the 64 x 64 diagonal blocks of the L11 panels of the wide fronts (for the solve)
+template <typename T>
+struct BlockInvArgs {
+    const DFront* fronts;
+    const int32_t* tasks;      // (front, block) pairs
+    int32_t count;
+    const int64_t* dinv_off;   // per front
+    const int32_t* members;
+    const T* panels;           // factor or U^T panels
+    T* dinv;
+    int64_t factor_len, dinv_len;
+    const int32_t* finfo;
+    int32_t ns;
+};
+template <typename T>
+cudaError_t launch_block_inv(const BlockInvArgs<T>& a, int nmembers, cudaStream_t st);
+
 constexpr int CHOL_NB = 64;
 cudaError_t prepare_factor_kernels(int max_smem);
 cudaError_t prepare_dense_kernels(int max_smem);

@@ -435,11 +435,60 @@ Plan* build_plan(const sdsb200_symbolic* sym, const sdsb200_plan_options* popts,
                 }
             }
         }
+        // solve-wide fronts: inverses of their 64 x 64 diagonal blocks, computed after the factorization
+        std::vector<int64_t> dinv_off(ns, -1);
+        std::vector<int32_t> binv_tasks;
+        auto solve_wide = [&](const DFront& F) { return F.w >= 96 || (int64_t)(F.f - F.w) * F.w >= 32768; };
+        for (int64_t s = 0; s < ns; ++s) {
+            const DFront& F = P->fronts[s];
+            if (!solve_wide(F)) continue;
+            dinv_off[s] = P->dinv_len;
+            int nblk = (F.w + SOLVE_BLK - 1) / SOLVE_BLK;
+            for (int b = 0; b < nblk; ++b) {
+                binv_tasks.push_back((int32_t)s);
+                binv_tasks.push_back(b);
+            }
+            P->dinv_len += (int64_t)nblk * SOLVE_BLK * SOLVE_BLK;
+        }
+        P->n_binv_tasks = (int)(binv_tasks.size() / 2);
+        if (P->n_binv_tasks) {
+            ProgLaunch bl{};
+            bl.kind = L_BLOCKINV;
+            bl.level = P->nlevels;
+            bl.count = P->n_binv_tasks;
+            P->prog.push_back(bl);
+        }
         {
             ProgLaunch pl{};
             pl.kind = L_STATS;
             P->prog.push_back(pl);
         }
+        // persistent solve lists
+        {
+            std::vector<int32_t> plist, psmall(2 * P->nlevels), plarge(2 * P->nlevels), pmaxblk(P->nlevels, 0);
+            for (int L = 0; L < P->nlevels; ++L) {
+                psmall[2 * L] = (int32_t)plist.size();
+                for (int s : P->level_fronts[L])
+                    if (!solve_wide(P->fronts[s])) {
+                        plist.push_back(s);
+                        P->p_maxw_small = std::max(P->p_maxw_small, P->fronts[s].w);
+                    }
+                psmall[2 * L + 1] = (int32_t)plist.size() - psmall[2 * L];
+                plarge[2 * L] = (int32_t)plist.size();
+                for (int s : P->level_fronts[L])
+                    if (solve_wide(P->fronts[s])) {
+                        plist.push_back(s);
+                        pmaxblk[L] = std::max(pmaxblk[L], (P->fronts[s].w + SOLVE_BLK - 1) / SOLVE_BLK);
+                    }
+                plarge[2 * L + 1] = (int32_t)plist.size() - plarge[2 * L];
+            }
+            P->d_p_list = upload(P, plist, st);
+            P->d_p_lev_small = upload(P, psmall, st);
+            P->d_p_lev_large = upload(P, plarge, st);
+            P->d_p_lev_maxblk = upload(P, pmaxblk, st);
+        }
+        P->d_dinv_off = upload(P, dinv_off, st);
+        P->d_binv_tasks = upload(P, binv_tasks, st);
         P->launches_factor = (int)P->prog.size();
 
         // solve: update vectors, per-level lists
@@ -606,6 +655,14 @@ Plan* build_plan(const sdsb200_symbolic* sym, const sdsb200_plan_options* popts,
         if (P->scr_len) P->d_scratch = dalloc<double>(P, P->scr_len * nb);
         if (P->work_len) P->d_work = alloc_bytes(es * P->work_len * nb);
         if (P->inv_len) P->d_inv = alloc_bytes(es * P->inv_len * nb);
+        if (P->dinv_len) {
+            P->d_dinv_L = alloc_bytes(es * P->dinv_len * nb);
+            if (gen) P->d_dinv_U = alloc_bytes(es * P->dinv_len * nb);
+        }
+        P->d_xtmp = dalloc<double>(P, n * P->max_nrhs);
+        P->d_barrier = dalloc<unsigned int>(P, 1);
+        P->d_solve_status = dalloc<int32_t>(P, 1);
+        cudaMemsetAsync(P->d_solve_status, 0, sizeof(int32_t), st);
         P->d_Y = dalloc<double>(P, n * P->max_nrhs * nb);
         P->d_U = dalloc<double>(P, P->ulen * nb);
         P->d_R = dalloc<double>(P, n * P->max_nrhs * nb);
@@ -618,9 +675,11 @@ Plan* build_plan(const sdsb200_symbolic* sym, const sdsb200_plan_options* popts,
             int dev = 0, optin = 0;
             cudaGetDevice(&dev);
             cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
-            if (prepare_factor_kernels(optin) != cudaSuccess || prepare_dense_kernels(optin) != cudaSuccess ||
-                prepare_solve_kernels(optin) != cudaSuccess)
-                throw BuildError(SDSB200_CUDA_ERROR, "kernel attribute setup failed");
+            cudaError_t ke = prepare_factor_kernels(optin);
+            if (ke == cudaSuccess) ke = prepare_dense_kernels(optin);
+            if (ke == cudaSuccess) ke = prepare_solve_kernels(optin);
+            if (ke != cudaSuccess)
+                throw BuildError(SDSB200_CUDA_ERROR, std::string("kernel attribute setup failed: ") + cudaGetErrorString(ke));
             if ((int64_t)small_front_smem(P->fsmall_max, P->elsize) > optin)
                 throw BuildError(SDSB200_NOT_SUPPORTED, "shared memory per block too small for the front classes");
         }

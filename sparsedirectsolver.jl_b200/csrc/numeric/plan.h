@@ -84,6 +84,21 @@ struct Plan {
     int32_t* d_level_lists = nullptr;   // fronts of each level for the solve sweeps: small first, then large
     std::vector<int64_t> level_list_off;
     std::vector<int> level_nsmall, level_nlarge, level_maxw_small, level_maxw_large;
+    // persistent solve: fronts by level (small, then wide), the diagonal-block inverses of the wide fronts
+    int32_t* d_p_list = nullptr;
+    int32_t* d_p_lev_small = nullptr;
+    int32_t* d_p_lev_large = nullptr;
+    int32_t* d_p_lev_maxblk = nullptr;
+    int p_maxw_small = 1;
+    int64_t dinv_len = 0;
+    int64_t* d_dinv_off = nullptr;
+    void* d_dinv_L = nullptr;
+    void* d_dinv_U = nullptr;
+    int32_t* d_binv_tasks = nullptr;
+    int n_binv_tasks = 0;
+    double* d_xtmp = nullptr;
+    unsigned int* d_barrier = nullptr;
+    int32_t* d_solve_status = nullptr;
     int32_t* d_rect_tiles = nullptr;    // (front, start) pairs: forward row tiles, backward column tiles
     std::vector<int64_t> level_ftile_off, level_btile_off;
     std::vector<int> level_nftile, level_nbtile;
@@ -116,6 +131,7 @@ struct Plan {
         int64_t launches = 0;
     };
     bool use_graphs = true;
+    bool persistent = true;        // the one-launch cooperative solve for a single active member
     cudaStream_t own = nullptr;          // capture / replay stream, joined to the caller's by events
     cudaEvent_t join_in = nullptr, join_out = nullptr;
     CachedGraph g_factor, g_solve, g_resid, g_corr;
@@ -125,6 +141,10 @@ struct Plan {
     std::vector<cudaEvent_t> events;
     size_t prof_next = 0;
     std::vector<std::pair<int, std::pair<double, double>>> pending;  // kind, (flops, bytes) per event pair
+    std::vector<int> pending_level;
+    struct LaunchRecord { int kind, level; double ms; };
+    std::vector<LaunchRecord> records;   // every profiled launch of the last calls
+    int cur_level = -1;
 };
 
 struct PlanError {

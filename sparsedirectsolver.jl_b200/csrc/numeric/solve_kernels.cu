@@ -16,6 +16,8 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <algorithm>
+
 #include "common.cuh"
 #include "solve.cuh"
 
@@ -23,11 +25,55 @@ namespace sds {
 
 constexpr int SOLVE_THREADS = 256;
 
+// acc[r] += sum_{j < W} Lrow[j * ld] * x[j + r * ldx] for r < rc (<= 8): eight independent loads are
+// issued before their FMAs, so that a thread keeps several factor loads in flight
 template <typename T>
-__global__ void __launch_bounds__(SOLVE_THREADS) forward_kernel(SweepArgs<T> A) {
-    extern __shared__ double xs[];  // w x nrhs
-    const int s = A.list[blockIdx.x];
-    const int member = A.members ? A.members[blockIdx.y] : blockIdx.y;
+__device__ __forceinline__ void row_dot(const T* __restrict__ Lrow, int64_t ld, int W, const double* x, int ldx,
+                                        int rc, double* acc) {
+    int j = 0;
+    for (; j + 8 <= W; j += 8) {
+        double lv[8];
+#pragma unroll
+        for (int u = 0; u < 8; ++u) lv[u] = (double)Lrow[(int64_t)(j + u) * ld];
+#pragma unroll
+        for (int u = 0; u < 8; ++u)
+#pragma unroll
+            for (int r = 0; r < 8; ++r)
+                if (r < rc) acc[r] += lv[u] * x[j + u + r * ldx];
+    }
+    for (; j < W; ++j) {
+        const double l = (double)Lrow[(int64_t)j * ld];
+#pragma unroll
+        for (int r = 0; r < 8; ++r)
+            if (r < rc) acc[r] += l * x[j + r * ldx];
+    }
+}
+
+// acc[r] += sum_{i = lane, lane + 32, ... < M} Lcol[i] * xval(i, r): a warp-strided dot with four loads in flight
+template <typename T, class XF>
+__device__ __forceinline__ void col_dot(const T* __restrict__ Lcol, int M, int lane, int rc, XF xval, double* acc) {
+    int i = lane;
+    for (; i + 96 < M; i += 128) {
+        double lv[4];
+#pragma unroll
+        for (int u = 0; u < 4; ++u) lv[u] = (double)Lcol[i + 32 * u];
+#pragma unroll
+        for (int u = 0; u < 4; ++u)
+#pragma unroll
+            for (int r = 0; r < 8; ++r)
+                if (r < rc) acc[r] += lv[u] * xval(i + 32 * u, r);
+    }
+    for (; i < M; i += 32) {
+        const double l = (double)Lcol[i];
+#pragma unroll
+        for (int r = 0; r < 8; ++r)
+            if (r < rc) acc[r] += l * xval(i, r);
+    }
+}
+
+// forward step of one front by one CTA (xs: w x nrhs shared doubles)
+template <typename T>
+__device__ void forward_front(const SweepArgs<T>& A, int s, int member, double* xs) {
     const DFront fd = A.fronts[s];
     const int f = fd.f, w = fd.w, m = f - w, nrhs = A.nrhs;
     const int64_t n = A.n;
@@ -83,16 +129,14 @@ __global__ void __launch_bounds__(SOLVE_THREADS) forward_kernel(SweepArgs<T> A) 
             Ld[i][j] = (i < bw && j < bw && i >= j) ? (double)L[(jb + i) + (int64_t)(jb + j) * f] : 0.0;
         }
         __syncthreads();
-        if (warp == 0) {
-            for (int r = 0; r < nrhs; ++r) {
-                double val = lane < bw ? xs[jb + lane + r * w] : 0.0;
-                for (int j = 0; j < bw; ++j) {
-                    if (!A.unit && lane == j) val /= Ld[j][j];
-                    double xj = __shfl_sync(0xffffffffu, val, j);
-                    if (lane > j) val -= Ld[lane][j] * xj;
-                }
-                if (lane < bw) xs[jb + lane + r * w] = val;
+        for (int r = warp; r < nrhs; r += nwarps) {  // one warp per right-hand side
+            double val = lane < bw ? xs[jb + lane + r * w] : 0.0;
+            for (int j = 0; j < bw; ++j) {
+                if (!A.unit && lane == j) val /= Ld[j][j];
+                double xj = __shfl_sync(0xffffffffu, val, j);
+                if (lane > j) val -= Ld[lane][j] * xj;
             }
+            if (lane < bw) xs[jb + lane + r * w] = val;
         }
         __syncthreads();
         for (int q = jb + bw + tid; q < w; q += nt) {
@@ -101,12 +145,7 @@ __global__ void __launch_bounds__(SOLVE_THREADS) forward_kernel(SweepArgs<T> A) 
                 const int rc = min(8, nrhs - r0);
 #pragma unroll
                 for (int r = 0; r < 8; ++r) acc[r] = 0.0;
-                for (int j = 0; j < bw; ++j) {
-                    const double l = (double)L[q + (int64_t)(jb + j) * f];
-#pragma unroll
-                    for (int r = 0; r < 8; ++r)
-                        if (r < rc) acc[r] += l * xs[jb + j + (r0 + r) * w];
-                }
+                row_dot(L + q + (int64_t)jb * f, f, bw, xs + jb + r0 * w, w, rc, acc);
                 for (int r = 0; r < rc; ++r) xs[q + (r0 + r) * w] -= acc[r];
             }
         }
@@ -120,12 +159,7 @@ __global__ void __launch_bounds__(SOLVE_THREADS) forward_kernel(SweepArgs<T> A) 
                 const int rc = min(8, nrhs - r0);
 #pragma unroll
                 for (int r = 0; r < 8; ++r) acc[r] = 0.0;
-                for (int j = 0; j < w; ++j) {
-                    const double l = (double)L[w + i + (int64_t)j * f];
-#pragma unroll
-                    for (int r = 0; r < 8; ++r)
-                        if (r < rc) acc[r] += l * xs[j + (r0 + r) * w];
-                }
+                row_dot(L + w + i, f, w, xs + r0 * w, w, rc, acc);
                 for (int r = 0; r < rc; ++r) u[i + (r0 + r) * m] += acc[r];
             }
         }
@@ -135,13 +169,18 @@ __global__ void __launch_bounds__(SOLVE_THREADS) forward_kernel(SweepArgs<T> A) 
         Y[fd.c0 + k + (int64_t)r * n] = xs[q];
     }
     (void)lane; (void)nwarps;
+    __syncthreads();
 }
 
 template <typename T>
-__global__ void __launch_bounds__(SOLVE_THREADS) backward_kernel(SweepArgs<T> A) {
+__global__ void __launch_bounds__(SOLVE_THREADS) forward_kernel(SweepArgs<T> A) {
     extern __shared__ double xs[];  // w x nrhs
-    const int s = A.list[blockIdx.x];
-    const int member = A.members ? A.members[blockIdx.y] : blockIdx.y;
+    forward_front(A, A.list[blockIdx.x], A.members ? A.members[blockIdx.y] : blockIdx.y, xs);
+}
+
+// backward step of one front by one CTA
+template <typename T>
+__device__ void backward_front(const SweepArgs<T>& A, int s, int member, double* xs) {
     const DFront fd = A.fronts[s];
     const int f = fd.f, w = fd.w, m = f - w, nrhs = A.nrhs;
     const int64_t n = A.n;
@@ -170,12 +209,8 @@ __global__ void __launch_bounds__(SOLVE_THREADS) backward_kernel(SweepArgs<T> A)
                 const int rc = min(8, nrhs - r0);
 #pragma unroll
                 for (int r = 0; r < 8; ++r) acc[r] = 0.0;
-                for (int i = lane; i < m; i += 32) {
-                    const double l = (double)L[w + i + (int64_t)j * f];
-#pragma unroll
-                    for (int r = 0; r < 8; ++r)
-                        if (r < rc) acc[r] += l * xb[i + (r0 + r) * m];
-                }
+                col_dot(L + w + (int64_t)j * f, m, lane, rc,
+                        [&](int i, int r) { return xb[i + (r0 + r) * m]; }, acc);
 #pragma unroll
                 for (int r = 0; r < 8; ++r) {
                     double v = acc[r];
@@ -196,16 +231,14 @@ __global__ void __launch_bounds__(SOLVE_THREADS) backward_kernel(SweepArgs<T> A)
             Ld[i][j] = (i < bw && j < bw && i >= j) ? (double)L[(jb + i) + (int64_t)(jb + j) * f] : 0.0;
         }
         __syncthreads();
-        if (warp == 0) {
-            for (int r = 0; r < nrhs; ++r) {
-                double val = lane < bw ? xs[jb + lane + r * w] : 0.0;
-                for (int j = bw - 1; j >= 0; --j) {
-                    if (!A.unit && lane == j) val /= Ld[j][j];
-                    double xj = __shfl_sync(0xffffffffu, val, j);
-                    if (lane < j) val -= Ld[j][lane] * xj;
-                }
-                if (lane < bw) xs[jb + lane + r * w] = val;
+        for (int r = warp; r < nrhs; r += nwarps) {
+            double val = lane < bw ? xs[jb + lane + r * w] : 0.0;
+            for (int j = bw - 1; j >= 0; --j) {
+                if (!A.unit && lane == j) val /= Ld[j][j];
+                double xj = __shfl_sync(0xffffffffu, val, j);
+                if (lane < j) val -= Ld[j][lane] * xj;
             }
+            if (lane < bw) xs[jb + lane + r * w] = val;
         }
         __syncthreads();
         for (int i = warp; i < jb; i += nwarps) {
@@ -223,6 +256,13 @@ __global__ void __launch_bounds__(SOLVE_THREADS) backward_kernel(SweepArgs<T> A)
         int dst = A.reorder ? piv[fd.c0 + k] - 1 : fd.c0 + k;
         Y[dst + (int64_t)r * n] = xs[q];
     }
+    __syncthreads();
+}
+
+template <typename T>
+__global__ void __launch_bounds__(SOLVE_THREADS) backward_kernel(SweepArgs<T> A) {
+    extern __shared__ double xs[];  // w x nrhs
+    backward_front(A, A.list[blockIdx.x], A.members ? A.members[blockIdx.y] : blockIdx.y, xs);
 }
 
 // u[rows of the tile] += L21[rows, :] x1 for one row tile of a large front (x1 from Y, pivoted order)
@@ -249,12 +289,7 @@ __global__ void __launch_bounds__(RECT_ROWS) forward_rect_kernel(SweepArgs<T> A)
         double acc[8];
 #pragma unroll
         for (int r = 0; r < 8; ++r) acc[r] = 0.0;
-        for (int j = 0; j < w; ++j) {
-            const double l = (double)L[w + i + (int64_t)j * f];
-#pragma unroll
-            for (int r = 0; r < 8; ++r)
-                if (r < rc) acc[r] += l * xs[j + (r0 + r) * w];
-        }
+        row_dot(L + w + i, f, w, xs + r0 * w, w, rc, acc);
         for (int r = 0; r < rc; ++r) u[i + (r0 + r) * m] += acc[r];
     }
 }
@@ -279,13 +314,8 @@ __global__ void __launch_bounds__(RECT_COLS * 32) backward_rect_kernel(SweepArgs
         double acc[8];
 #pragma unroll
         for (int r = 0; r < 8; ++r) acc[r] = 0.0;
-        for (int i = lane; i < m; i += 32) {
-            const double l = (double)L[w + i + (int64_t)j * f];
-            const int64_t g = rows[i];
-#pragma unroll
-            for (int r = 0; r < 8; ++r)
-                if (r < rc) acc[r] += l * Y[g + (int64_t)(r0 + r) * n];
-        }
+        col_dot(L + w + (int64_t)j * f, m, lane, rc,
+                [&](int i, int r) { return Y[rows[i] + (int64_t)(r0 + r) * n]; }, acc);
 #pragma unroll
         for (int r = 0; r < 8; ++r) {
             double v = acc[r];
@@ -321,22 +351,333 @@ cudaError_t launch_sweep(bool forward, const SweepArgs<T>& a, int nmembers, int 
     return cudaGetLastError();
 }
 
-cudaError_t prepare_solve_kernels(int max_smem) {
-    cudaError_t e = cudaSuccess;
-    auto set = [&](const void* k) {
-        if (e == cudaSuccess) e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, max_smem);
-    };
-    set((const void*)forward_kernel<double>);
-    set((const void*)forward_kernel<float>);
-    set((const void*)backward_kernel<double>);
-    set((const void*)backward_kernel<float>);
-    set((const void*)forward_rect_kernel<double>);
-    set((const void*)forward_rect_kernel<float>);
-    return e;
-}
 
 template cudaError_t launch_sweep<double>(bool, const SweepArgs<double>&, int, int, cudaStream_t);
 template cudaError_t launch_sweep<float>(bool, const SweepArgs<float>&, int, int, cudaStream_t);
+
+// ---------------------------------------------------------------------------
+// Persistent solve. Grid barrier: one arrival per CTA on a monotonic counter; the wait is bounded
+// (about two seconds of spinning), after which the CTA records the failure and goes on, so a lost
+// CTA never hangs the device (the results are then garbage and the status word says so).
+__device__ __forceinline__ void grid_barrier(unsigned int* bar, unsigned int& epoch, int32_t* status) {
+    __syncthreads();
+    epoch += gridDim.x;
+    if (threadIdx.x == 0) {
+        __threadfence();
+        atomicAdd(bar, 1u);
+        unsigned int v;
+        long spins = 0;
+        while (true) {
+            asm volatile("ld.acquire.gpu.u32 %0, [%1];" : "=r"(v) : "l"(bar));
+            if ((int)(v - epoch) >= 0) break;
+            if (++spins > (1L << 26)) {
+                atomicExch(status, 1);
+                break;
+            }
+            __nanosleep(32);
+        }
+        __threadfence();
+    }
+    __syncthreads();
+}
+
+// forward, wide front s, block step b, row tile t: x_b = inv(L_bb) y_b; rows below get -L x_b
+template <typename T>
+__device__ void wide_forward_tile(const PersistArgs<T>& P, int s, int b, int t, double* sm) {
+    const SweepArgs<T>& A = P.fw;
+    const DFront fd = A.fronts[s];
+    const int f = fd.f, w = fd.w, m = f - w, nrhs = A.nrhs;
+    const int64_t n = A.n;
+    const int jb = b * SOLVE_BLK, bw = min(SOLVE_BLK, w - jb);
+    const T* L = A.fac + fd.panel;
+    const T* inv = P.dinv_fw + P.dinv_off[s] + (int64_t)b * SOLVE_BLK * SOLVE_BLK;
+    double* Y = A.Y;
+    double* u = m > 0 ? A.U + A.uoff[s] : nullptr;
+    double* yb = sm;                     // SOLVE_BLK x nrhs
+    double* xb = sm + SOLVE_BLK * nrhs;  // SOLVE_BLK x nrhs
+    const int tid = threadIdx.x, nt = blockDim.x;
+    for (int q = tid; q < SOLVE_BLK * nrhs; q += nt) {
+        int k = q % SOLVE_BLK, r = q / SOLVE_BLK;
+        yb[q] = k < bw ? Y[fd.c0 + jb + k + (int64_t)r * n] : 0.0;
+    }
+    __syncthreads();
+    for (int q = tid; q < SOLVE_BLK * nrhs; q += nt) {
+        int i = q % SOLVE_BLK, r = q / SOLVE_BLK;
+        double acc = 0.0;
+        if (i < bw)
+            for (int j = 0; j <= i; ++j) acc += (double)inv[i + j * SOLVE_BLK] * yb[j + r * SOLVE_BLK];
+        xb[q] = acc;
+    }
+    __syncthreads();
+    const int r0 = t * SOLVE_BLK;
+    for (int q = tid; q < SOLVE_BLK; q += nt) {
+        const int row = r0 + q;
+        if (row >= f || row < jb) continue;
+        if (row < jb + bw) {  // the block's own rows: to the scratch, copied to Y after the level
+            for (int r = 0; r < nrhs; ++r) P.xtmp[fd.c0 + row + (int64_t)r * n] = xb[row - jb + r * SOLVE_BLK];
+            continue;
+        }
+        for (int r0_ = 0; r0_ < nrhs; r0_ += 8) {
+            const int rc = min(8, nrhs - r0_);
+            double acc[8];
+#pragma unroll
+            for (int r = 0; r < 8; ++r) acc[r] = 0.0;
+            row_dot(L + row + (int64_t)jb * f, f, bw, xb + r0_ * SOLVE_BLK, SOLVE_BLK, rc, acc);
+            for (int r = 0; r < rc; ++r) {
+                if (row < w) Y[fd.c0 + row + (int64_t)(r0_ + r) * n] -= acc[r];
+                else u[row - w + (r0_ + r) * m] += acc[r];
+            }
+        }
+    }
+    __syncthreads();
+}
+
+// backward, wide front s, block step b, column tile t: x_b = inv(L_bb)^T y_b; columns before the
+// block get -L_b.^T x_b
+template <typename T>
+__device__ void wide_backward_tile(const PersistArgs<T>& P, int s, int b, int t, double* sm) {
+    const SweepArgs<T>& A = P.bw;
+    const DFront fd = A.fronts[s];
+    const int f = fd.f, w = fd.w, nrhs = A.nrhs;
+    const int64_t n = A.n;
+    const int jb = b * SOLVE_BLK, bw = min(SOLVE_BLK, w - jb);
+    const T* L = A.fac + fd.panel;
+    const T* inv = P.dinv_bw + P.dinv_off[s] + (int64_t)b * SOLVE_BLK * SOLVE_BLK;
+    double* Y = A.Y;
+    double* yb = sm;
+    double* xb = sm + SOLVE_BLK * nrhs;
+    const int tid = threadIdx.x, nt = blockDim.x, lane = tid & 31, warp = tid >> 5, nwarps = nt >> 5;
+    for (int q = tid; q < SOLVE_BLK * nrhs; q += nt) {
+        int k = q % SOLVE_BLK, r = q / SOLVE_BLK;
+        yb[q] = k < bw ? Y[fd.c0 + jb + k + (int64_t)r * n] : 0.0;
+    }
+    __syncthreads();
+    for (int q = tid; q < SOLVE_BLK * nrhs; q += nt) {
+        int i = q % SOLVE_BLK, r = q / SOLVE_BLK;
+        double acc = 0.0;
+        if (i < bw)
+            for (int j = i; j < bw; ++j) acc += (double)inv[j + i * SOLVE_BLK] * yb[j + r * SOLVE_BLK];
+        xb[q] = acc;
+    }
+    __syncthreads();
+    const int c0 = t * SOLVE_BLK;
+    if (t == b) {  // the block's solution: to the scratch, scattered into Y after the level
+        for (int q = tid; q < bw * nrhs; q += nt) {
+            int k = q % bw, r = q / bw;
+            P.xtmp[fd.c0 + jb + k + (int64_t)r * n] = xb[k + r * SOLVE_BLK];
+        }
+    } else {
+        for (int a = c0 + warp; a < min(c0 + SOLVE_BLK, jb); a += nwarps) {
+            const double l = lane < bw ? (double)L[(jb + lane) + (int64_t)a * f] : 0.0;
+            const double l2 = lane + 32 < bw ? (double)L[(jb + lane + 32) + (int64_t)a * f] : 0.0;
+            for (int r = 0; r < nrhs; ++r) {
+                double v = l * xb[lane + r * SOLVE_BLK] + l2 * xb[lane + 32 + r * SOLVE_BLK];
+                for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+                if (lane == 0) Y[fd.c0 + a + (int64_t)r * n] -= v;
+            }
+        }
+    }
+    (void)f;
+    __syncthreads();
+}
+
+template <typename T>
+__global__ void __launch_bounds__(SOLVE_THREADS) persistent_solve_kernel(PersistArgs<T> P) {
+    extern __shared__ double psm[];
+    unsigned int epoch = 0;
+    const int G = gridDim.x;
+    const int64_t n = P.fw.n;
+    const int nrhs = P.fw.nrhs;
+    const int64_t gtid = blockIdx.x * (int64_t)blockDim.x + threadIdx.x, gstride = (int64_t)G * blockDim.x;
+    // Y = in[perm]
+    for (int64_t q = gtid; q < n * nrhs; q += gstride) {
+        int64_t k = q % n, r = q / n;
+        P.fw.Y[q] = P.in[P.perm[k] + r * P.ldin];
+    }
+    grid_barrier(P.barrier, epoch, P.status);
+    // forward levels
+    for (int L = 0; L < P.nlevels; ++L) {
+        const int so = P.lev_small[2 * L], sc = P.lev_small[2 * L + 1];
+        const int lo = P.lev_large[2 * L], lc = P.lev_large[2 * L + 1];
+        for (int i = blockIdx.x; i < sc; i += G) forward_front(P.fw, P.list[so + i], 0, psm);
+        // wide fronts: pull the children and apply the local pivot order (one CTA each, from the end)
+        for (int i = G - 1 - blockIdx.x; i < lc; i += G) {
+            const int s = P.list[lo + i];
+            const DFront fd = P.fw.fronts[s];
+            const int w = fd.w, m = fd.f - fd.w;
+            double* Y = P.fw.Y;
+            double* xt = P.xtmp;
+            double* u = m > 0 ? P.fw.U + P.fw.uoff[s] : nullptr;
+            for (int q = threadIdx.x; q < w * nrhs; q += blockDim.x) {
+                int k = q % w, r = q / w;
+                xt[fd.c0 + k + (int64_t)r * n] = Y[fd.c0 + k + (int64_t)r * n];
+            }
+            for (int q = threadIdx.x; q < m * nrhs; q += blockDim.x) u[q] = 0.0;
+            __syncthreads();
+            for (int cq = fd.ch_begin; cq < fd.ch_end; ++cq) {
+                const int c = P.fw.child_list[cq];
+                const DFront cd = P.fw.fronts[c];
+                const int mc = cd.f - cd.w;
+                if (mc <= 0) continue;
+                const double* uc = P.fw.U + P.fw.uoff[c];
+                const int32_t* ri = P.fw.relind + cd.ri_begin;
+                for (int q = threadIdx.x; q < mc * nrhs; q += blockDim.x) {
+                    int i2 = q % mc, r = q / mc;
+                    int p = ri[i2];
+                    if (p < w) xt[fd.c0 + p + (int64_t)r * n] -= uc[q];
+                    else u[(p - w) + r * m] += uc[q];
+                }
+                __syncthreads();
+            }
+            for (int q = threadIdx.x; q < w * nrhs; q += blockDim.x) {
+                int k = q % w, r = q / w;
+                int src = P.fw.reorder ? P.fw.piv[fd.c0 + k] - 1 : fd.c0 + k;
+                Y[fd.c0 + k + (int64_t)r * n] = xt[src + (int64_t)r * n];
+            }
+            __syncthreads();
+        }
+        grid_barrier(P.barrier, epoch, P.status);
+        const int nb = P.lev_maxblk[L];
+        for (int b = 0; b < nb; ++b) {
+            // (front, row tile) pairs of this step, spread over the grid
+            int task = 0;
+            for (int i = 0; i < lc; ++i) {
+                const int s = P.list[lo + i];
+                const DFront fd = P.fw.fronts[s];
+                const int nblk = (fd.w + SOLVE_BLK - 1) / SOLVE_BLK;
+                if (b >= nblk) continue;
+                const int ntile = (fd.f + SOLVE_BLK - 1) / SOLVE_BLK;
+                for (int t = b; t < ntile; ++t, ++task)
+                    if (task % G == blockIdx.x) wide_forward_tile(P, s, b, t, psm);
+            }
+            grid_barrier(P.barrier, epoch, P.status);
+        }
+        // the wide fronts' solutions into Y (read again only after later barriers)
+        for (int i = 0; i < lc; ++i) {
+            const DFront fd = P.fw.fronts[P.list[lo + i]];
+            for (int64_t q = gtid; q < (int64_t)fd.w * nrhs; q += gstride) {
+                const int64_t k = q % fd.w, r = q / fd.w;
+                P.fw.Y[fd.c0 + k + r * n] = P.xtmp[fd.c0 + k + r * n];
+            }
+        }
+    }
+    // diagonal: D^{-1} with 1x1 and 2x2 blocks
+    if (P.diag_mode) {
+        for (int64_t q = gtid; q < n * nrhs; q += gstride) {
+            const int64_t k = q % n, r = q / n;
+            const int kk = P.kind[k];
+            double* Y = P.fw.Y;
+            if (P.diag_mode == 2 && kk == KIND_2X2_SECOND) continue;
+            if (P.diag_mode == 2 && kk == KIND_2X2_FIRST) {
+                double a = P.d[k], b = P.d[n + k], c = P.d[k + 1];
+                double det = a * c - b * b;
+                double y1 = Y[k + r * n], y2 = Y[k + 1 + r * n];
+                Y[k + r * n] = (c * y1 - b * y2) / det;
+                Y[k + 1 + r * n] = (a * y2 - b * y1) / det;
+            } else {
+                Y[k + r * n] /= P.d[k];
+            }
+        }
+        grid_barrier(P.barrier, epoch, P.status);
+    }
+    // backward levels
+    for (int L = P.nlevels - 1; L >= 0; --L) {
+        const int so = P.lev_small[2 * L], sc = P.lev_small[2 * L + 1];
+        const int lo = P.lev_large[2 * L], lc = P.lev_large[2 * L + 1];
+        if (lc) {
+            // x1 -= L21^T x2 for the wide fronts: one warp per column, columns spread over the grid
+            const int warps = blockDim.x >> 5, lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+            int col = 0;
+            for (int i = 0; i < lc; ++i) {
+                const int s = P.list[lo + i];
+                const DFront fd = P.bw.fronts[s];
+                const int f = fd.f, w = fd.w, m = f - w;
+                const T* Lp = P.bw.fac + fd.panel;
+                const int32_t* rows = P.bw.rowval + fd.row_begin + w;
+                for (int j = 0; j < w; ++j, ++col) {
+                    if (col % (G * warps) != blockIdx.x * warps + warp || m == 0) continue;
+                    for (int r0 = 0; r0 < nrhs; r0 += 8) {
+                        const int rc = min(8, nrhs - r0);
+                        double acc[8];
+#pragma unroll
+                        for (int r = 0; r < 8; ++r) acc[r] = 0.0;
+                        col_dot(Lp + w + (int64_t)j * f, m, lane, rc,
+                                [&](int i2, int r) { return P.bw.Y[rows[i2] + (int64_t)(r0 + r) * n]; }, acc);
+#pragma unroll
+                        for (int r = 0; r < 8; ++r) {
+                            double v = acc[r];
+                            for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+                            if (lane == 0 && r < rc) P.bw.Y[fd.c0 + j + (int64_t)(r0 + r) * n] -= v;
+                        }
+                    }
+                }
+            }
+            grid_barrier(P.barrier, epoch, P.status);
+            const int nb = P.lev_maxblk[L];
+            for (int b = nb - 1; b >= 0; --b) {
+                int task = 0;
+                for (int i = 0; i < lc; ++i) {
+                    const int s = P.list[lo + i];
+                    const DFront fd = P.bw.fronts[s];
+                    const int nblk = (fd.w + SOLVE_BLK - 1) / SOLVE_BLK;
+                    if (b >= nblk) continue;
+                    for (int t = 0; t <= b; ++t, ++task)
+                        if (task % G == blockIdx.x) wide_backward_tile(P, s, b, t, psm);
+                }
+                grid_barrier(P.barrier, epoch, P.status);
+            }
+            // the wide fronts' solutions into Y, undoing their local pivot order
+            for (int i = 0; i < lc; ++i) {
+                const DFront fd = P.bw.fronts[P.list[lo + i]];
+                for (int64_t q = gtid; q < (int64_t)fd.w * nrhs; q += gstride) {
+                    const int64_t k = q % fd.w, r = q / fd.w;
+                    const int64_t dst = P.bw.reorder ? P.bw.piv[fd.c0 + k] - 1 : fd.c0 + k;
+                    P.bw.Y[dst + r * n] = P.xtmp[fd.c0 + k + r * n];
+                }
+            }
+        }
+        for (int i = blockIdx.x; i < sc; i += G) backward_front(P.bw, P.list[so + i], 0, psm);
+        grid_barrier(P.barrier, epoch, P.status);
+    }
+    // out[perm] = Y (or +=)
+    for (int64_t q = gtid; q < n * nrhs; q += gstride) {
+        int64_t k = q % n, r = q / n;
+        double* o = P.out + P.perm[k] + r * P.ldout;
+        if (P.mode == 2) *o += P.fw.Y[q];
+        else *o = P.fw.Y[q];
+    }
+}
+
+template <typename T>
+int persistent_solve_grid(size_t smem) {
+    int dev = 0, sms = 0, per = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, persistent_solve_kernel<T>, SOLVE_THREADS, smem) !=
+        cudaSuccess)
+        return 0;
+    return sms * std::min(per, 2);
+}
+
+template <typename T>
+cudaError_t launch_persistent_solve(const PersistArgs<T>& a, int grid, size_t smem, cudaStream_t st) {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(grid);
+    cfg.blockDim = dim3(SOLVE_THREADS);
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = st;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeCooperative;
+    attr[0].val.cooperative = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    return cudaLaunchKernelEx(&cfg, persistent_solve_kernel<T>, a);
+}
+
+template cudaError_t launch_persistent_solve<double>(const PersistArgs<double>&, int, size_t, cudaStream_t);
+template cudaError_t launch_persistent_solve<float>(const PersistArgs<float>&, int, size_t, cudaStream_t);
+template int persistent_solve_grid<double>(size_t);
+template int persistent_solve_grid<float>(size_t);
 
 // D^{-1} (1x1 and 2x2 blocks, d[k], d[n + k], d[k + 1]) -- _sv_diag_kernel! sweeps.jl:549-569
 __global__ void diag_kernel(DiagArgs A) {
@@ -471,6 +812,26 @@ __global__ void norms_kernel(NormArgs A) {
 cudaError_t launch_norms(const NormArgs& a, int ncols, cudaStream_t st) {
     norms_kernel<<<ncols, 256, 0, st>>>(a);
     return cudaGetLastError();
+}
+
+cudaError_t prepare_solve_kernels(int max_smem) {
+    cudaError_t e = cudaSuccess;
+    auto set = [&](const void* k) {
+        if (e != cudaSuccess) return;
+        cudaFuncAttributes fa;
+        e = cudaFuncGetAttributes(&fa, k);
+        if (e == cudaSuccess)
+            e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, max_smem - (int)fa.sharedSizeBytes);
+    };
+    set((const void*)forward_kernel<double>);
+    set((const void*)forward_kernel<float>);
+    set((const void*)backward_kernel<double>);
+    set((const void*)backward_kernel<float>);
+    set((const void*)forward_rect_kernel<double>);
+    set((const void*)forward_rect_kernel<float>);
+    set((const void*)persistent_solve_kernel<double>);
+    set((const void*)persistent_solve_kernel<float>);
+    return e;
 }
 
 }  // namespace sds

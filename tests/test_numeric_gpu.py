@@ -250,3 +250,29 @@ def test_graph_replay_matches_eager(torch_cuda, structure):
     assert np.array_equal(out[0][0], out[1][0])
     assert np.array_equal(out[0][1], out[1][1])
     assert np.array_equal(out[0][2], out[1][2])
+
+
+@pytest.mark.parametrize("structure", ["SPD", "S", "G"])
+def test_persistent_solve_matches_level_launches(torch_cuda, structure):
+    from sdsb200._native import numeric_lib
+
+    lib = numeric_lib()
+    A = {"SPD": lambda: M.lap3d(20, 20, 20, seed=6), "S": lambda: small_kkt(22, 22, 200, seed=6),
+         "G": lambda: M.convection_diffusion3d(14, 14, 14, seed=6)}[structure]()
+    ds = _solver(A, structure, reordering_alg="nd", max_nrhs=4)
+    ds.execute("analysis")
+    ds.execute("factorization")
+    b = M.rhs(A.shape[0], 3, seed=7)
+    xs = []
+    for mode in (1, 0):
+        lib.sdsb200_set_persistent(ds._plan, mode)
+        for tr in ((False, True) if structure == "G" else (False,)):
+            ds.setparam("solve_mode", int(tr))
+            x = ds.execute("solve", None, b).cpu().numpy()
+            AA = A.T.tocsr() if tr else A
+            assert M.scaled_backward_error(AA, x, b) <= BERR
+            xs.append(x)
+    assert lib.sdsb200_plan_stat(ds._plan, b"solve_status") == 0
+    k = len(xs) // 2
+    for x1, x0 in zip(xs[:k], xs[k:]):
+        assert np.abs(x1 - x0).max() <= 1e-10 * np.abs(x0).max()
