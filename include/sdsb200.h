@@ -157,6 +157,10 @@ int sdsb200_set_persistent(sdsb200_plan* plan, int32_t on);
  * calls, accumulated per kernel kind (resets the totals). Costs one event record per launch. */
 int sdsb200_set_profiling(sdsb200_plan* plan, int32_t on);
 
+/* Profiling: copy up to cap (tag, nanoseconds) pairs of the persistent solve's phase stamps (written
+ * when profiling is on; tag = kind << 40 | level << 16 | step). Returns the pairs copied or -1. */
+int64_t sdsb200_get_trace(sdsb200_plan* plan, int64_t* h_out, int64_t cap);
+
 /* Plan facts: "ns", "nlevels", "factor_len", "cb_len", "launches_factor", "launches_solve",
  * "launches_done" (kernel launches of the last factor or solve call), "device_bytes", "flops",
  * "solve_status" (synchronizes; nonzero when a bounded wait of the persistent solve gave up);

@@ -399,6 +399,8 @@ int run_sweeps(Plan* P, int nrhs, bool transpose, cudaStream_t st) {
     return SDSB200_OK;
 }
 
+constexpr int SOLVE_THREADS_HOST = 256;   // threads of the persistent solve kernel
+
 // the whole solve in one cooperative launch (one active batch member)
 template <typename T>
 int run_persistent(Plan* P, int nrhs, bool transpose, const double* in, int64_t ldin, double* out, int64_t ldout,
@@ -447,7 +449,15 @@ int run_persistent(Plan* P, int nrhs, bool transpose, const double* in, int64_t 
     a.xtmp = P->d_xtmp;
     a.barrier = P->d_barrier;
     a.status = P->d_solve_status;
-    const size_t smem = sizeof(double) * std::max<size_t>((size_t)P->p_maxw_small * nrhs, 2 * SOLVE_BLK * (size_t)nrhs);
+    a.trace = P->profile ? P->d_trace : nullptr;
+    a.trace_cap = Plan::TRACE_CAP;
+    // wide tiles: the inverse block, y_b, x_b and 4 partial sums per rhs (at most 8 per pass)
+    const size_t wide = (size_t)SOLVE_BLK * (SOLVE_BLK + 1) + 2 * SOLVE_BLK * (size_t)nrhs +
+                        4 * SOLVE_BLK * (size_t)std::min(nrhs, 8);
+    // small fronts: one warp each, xs (w x nrhs) and the staged diagonal block (32 x 33) per warp
+    a.warp_xs = (int32_t)(((size_t)P->p_maxw_small * nrhs + 1) & ~size_t(1));
+    a.warp_smem = a.warp_xs + 32 * 33;
+    const size_t smem = sizeof(double) * std::max<size_t>((size_t)a.warp_smem * (SOLVE_THREADS_HOST / 32), wide);
     const int grid = persistent_solve_grid<T>(smem);
     if (grid <= 0) return fail(SDSB200_CUDA_ERROR, "no co-resident grid for the persistent solve");
     CK(cudaMemsetAsync(P->d_barrier, 0, sizeof(unsigned int), st), "barrier reset");
@@ -768,6 +778,14 @@ int sdsb200_set_members(sdsb200_plan* plan, const int32_t* h_members, int32_t na
     return SDSB200_OK;
 }
 
+int64_t sdsb200_get_trace(sdsb200_plan* plan, int64_t* h_out, int64_t cap) {
+    Plan* P = reinterpret_cast<Plan*>(plan);
+    if (!P || !h_out) return -1;
+    int64_t n = std::min<int64_t>(cap, Plan::TRACE_CAP);
+    if (cudaMemcpy(h_out, P->d_trace, sizeof(int64_t) * 2 * n, cudaMemcpyDeviceToHost) != cudaSuccess) return -1;
+    return n;
+}
+
 int sdsb200_set_persistent(sdsb200_plan* plan, int32_t on) {
     Plan* P = reinterpret_cast<Plan*>(plan);
     if (!P) return fail(SDSB200_INVALID_VALUE, "plan is NULL");
@@ -789,6 +807,7 @@ int sdsb200_set_profiling(sdsb200_plan* plan, int32_t on) {
     if (!P) return fail(SDSB200_INVALID_VALUE, "plan is NULL");
     P->profile = on != 0;
     P->records.clear();
+    cudaMemset(P->d_trace, 0, sizeof(int64_t) * 2 * Plan::TRACE_CAP);
     for (int k = 0; k < PK_COUNT; ++k) P->prof[k] = ProfAcc();
     P->pending.clear();
     P->prof_next = 0;

@@ -87,4 +87,24 @@ struct DeviceMaps {
     const int32_t* perm;     // 0-based
 };
 
+// Strided copy loops with many loads in flight: for q = t0, t0 + step, ... < N, first load U values into
+// registers, then store them. The explicit batch keeps loads independent of the stores even when the
+// compiler cannot tell the shared- and global-memory pointers apart.
+template <int U, class LD, class ST>
+__device__ __forceinline__ void batched_copy(int t0, int step, int N, LD load, ST store) {
+    for (int q0 = t0; q0 < N; q0 += U * step) {
+        double v[U];
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+            const int q = q0 + u * step;
+            v[u] = q < N ? load(q) : 0.0;
+        }
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+            const int q = q0 + u * step;
+            if (q < N) store(q, v[u]);
+        }
+    }
+}
+
 }  // namespace sds

@@ -272,20 +272,17 @@ cudaError_t launch_gemm(const GemmArgs<T>& a, int nmembers, cudaStream_t st) {
 }
 
 // ---------------------------------------------------------------------------
-// Diagonal block of a large Cholesky front (64 x 64 at column kb): factor with the static clamp and
-// failure rule of the fused kernels, write L11 back, write inv(L11) (ld 64) to scratch for the trsm
-// of the rows below as a GEMM (X = B inv(L11)^T).
-// Each thread owns fixed entries of the lower triangle and keeps them in registers; a step publishes
-// one column (or row) through a double-buffered shared vector, so each pivot costs one barrier.
-// Factorization: right-looking on the unscaled columns (a_il -= a_ij a_lj / d_j with d_j the clamped
-// pivot), scaled by sqrt(d_j) at the end. Inverse: right-looking substitution on the identity.
+// Diagonal block of a large Cholesky front (32 x 32 at column kb): factor with the static clamp and
+// failure rule of the fused kernels, write L11 back, write inv(L11) (ld 32) to scratch for the trsm
+// of the rows below as a GEMM (X = B inv(L11)^T). One warp, lane i holding row i of the block in
+// registers; the pivot columns and the rows of the inverse move by shuffles (loops fully unrolled, so
+// every register index is a constant).
 template <typename T>
-__global__ void __launch_bounds__(256) chol_diag_kernel(CholDiagArgs<T> A) {
-    constexpr int NB = CHOL_NB, NE = NB * (NB + 1) / 2, SLOTS = (NE + 255) / 256;
-    __shared__ double colv[2][NB];
-    __shared__ double rowv[2][NB];
-    __shared__ double dpiv[NB];
-    __shared__ int s_status;
+__global__ void __launch_bounds__(32) chol_diag_kernel(CholDiagArgs<T> A) {
+    constexpr int NB = CHOL_NB, LD = NB + 1;
+    static_assert(NB == 32, "one lane per row of the diagonal block");
+    __shared__ double L[NB * LD];
+    __shared__ double X[NB * LD];
     const int s = A.list[blockIdx.x];
     const int member = A.members ? A.members[blockIdx.y] : blockIdx.y;
     const DFront fd = A.fronts[s];
@@ -295,51 +292,35 @@ __global__ void __launch_bounds__(256) chol_diag_kernel(CholDiagArgs<T> A) {
     if (kb >= w) return;
     const int nbb = min(NB, w - kb);
     T* P = A.factor + (int64_t)member * A.factor_len + fd.panel;
-    const int tid = threadIdx.x;
-    // owned entries: e = tid + 256 k of the column-major lower triangle
-    int ri[SLOTS], ci[SLOTS];
-    double a[SLOTS], x[SLOTS];
-#pragma unroll
-    for (int k = 0; k < SLOTS; ++k) {
-        int e = tid + 256 * k, col = 0;
-        if (e < NE) {
-            int rem = e;
-            while (rem >= NB - col) { rem -= NB - col; ++col; }
-            ri[k] = col + rem;
-            ci[k] = col;
-        } else {
-            ri[k] = -1;
-            ci[k] = NB;
-        }
-        const bool in = ri[k] >= 0 && ri[k] < nbb && ci[k] < nbb;
-        a[k] = in ? (double)P[(kb + ri[k]) + (int64_t)(kb + ci[k]) * f] : 0.0;
-        x[k] = (in && ri[k] == ci[k]) ? 1.0 : 0.0;
-    }
-    if (tid == 0) s_status = 0;
+    const int i = threadIdx.x;
+    batched_copy<8>(0, 1, NB,
+                    [&](int j) { return (i < nbb && j < nbb && j <= i) ? (double)P[(kb + i) + (int64_t)(kb + j) * f] : 0.0; },
+                    [&](int j, double v) { L[i * LD + j] = v; });
+    __syncwarp();
     const double eps = A.eps;
     int status = 0;
     for (int j = 0; j < nbb; ++j) {
-        double* cv = colv[j & 1];
-#pragma unroll
-        for (int k = 0; k < SLOTS; ++k)
-            if (ci[k] == j) cv[ri[k]] = a[k];
-        __syncthreads();
-        const double ajj = cv[j];
-        const bool ok = ajj > eps || (eps > 0 && ajj >= 0);
-        if (!ok) {
+        const double ajj = L[j * LD + j];
+        if (!(ajj > eps || (eps > 0 && ajj >= 0))) {
             status = j + 1;
             break;
         }
-        const double dj = fmax(ajj, eps);
-        const double invd = 1.0 / dj;
-        if (tid == 0) dpiv[j] = dj;
-#pragma unroll
-        for (int k = 0; k < SLOTS; ++k)
-            if (ci[k] > j && ri[k] < nbb) a[k] -= cv[ri[k]] * (cv[ci[k]] * invd);
+        const double sd = sqrt(fmax(ajj, eps));
+        double lij = 0.0;
+        if (i > j && i < nbb) {
+            lij = (double)T(L[i * LD + j] / sd);
+            L[i * LD + j] = lij;
+        }
+        __syncwarp();
+        if (i == j) L[j * LD + j] = (double)T(sd);
+        if (i > j && i < nbb)
+            for (int l = j + 1; l <= i; ++l) L[i * LD + l] = (double)T(L[i * LD + l] - lij * L[l * LD + j]);
+        __syncwarp();
     }
-    __syncthreads();
+    if (i < nbb)
+        for (int j = 0; j < nbb; ++j) P[(kb + i) + (int64_t)(kb + j) * f] = j <= i ? T(L[i * LD + j]) : T(0);
     if (status) {
-        if (tid == 0) {
+        if (i == 0) {
             int64_t* S = A.stats + ((int64_t)member * A.ns + s) * NSTAT;
             finfo[s] = kb + status;
             S[ST_NPOS] = kb + status - 1;
@@ -347,62 +328,36 @@ __global__ void __launch_bounds__(256) chol_diag_kernel(CholDiagArgs<T> A) {
         }
         return;
     }
-    // scale: L_il = a_il / sqrt(d_l), L_ll = sqrt(d_l); rounded to the factor precision
-#pragma unroll
-    for (int k = 0; k < SLOTS; ++k) {
-        if (ri[k] < 0 || ri[k] >= nbb || ci[k] >= nbb) continue;
-        const double sd = sqrt(dpiv[ci[k]]);
-        a[k] = (double)T(ri[k] == ci[k] ? sd : a[k] / sd);
-        P[(kb + ri[k]) + (int64_t)(kb + ci[k]) * f] = T(a[k]);
-    }
-    // the strict upper triangle of the diagonal block is stored as zeros
-    for (int q = tid; q < nbb * nbb; q += 256) {
-        int i = q % nbb, j = q / nbb;
-        if (i < j) P[(kb + i) + (int64_t)(kb + j) * f] = T(0);
-    }
-    if (tid == 0 && kb + nbb == w) {
+    if (i == 0 && kb + nbb == w) {
         int64_t* S = A.stats + ((int64_t)member * A.ns + s) * NSTAT;
         S[ST_NPOS] = w;
         S[ST_INFO] = 0;
     }
     if (kb + nbb >= f) return;  // no rows below: no trsm
-    // inverse: X = L^{-1}; step l divides row l by L_ll and subtracts L_il X_l. from the rows below
-    for (int l = 0; l < nbb; ++l) {
-        double* cv = colv[l & 1];
-        double* rv = rowv[l & 1];
-#pragma unroll
-        for (int k = 0; k < SLOTS; ++k) {
-            if (ci[k] == l) cv[ri[k]] = a[k];
+    // inverse, right-looking: step k finalizes row k of X and subtracts it from the rows below
+    for (int j = 0; j < NB; ++j) X[i * LD + j] = (i == j) ? 1.0 : 0.0;
+    __syncwarp();
+    for (int k = 0; k < nbb; ++k) {
+        if (i == k) {
+            const double r = 1.0 / L[k * LD + k];
+            for (int j = 0; j <= k; ++j) X[k * LD + j] *= r;
         }
-        __syncthreads();
-        const double rl = 1.0 / cv[l];
-#pragma unroll
-        for (int k = 0; k < SLOTS; ++k)
-            if (ri[k] == l) {
-                x[k] *= rl;
-                rv[ci[k]] = x[k];
-            }
-        __syncthreads();
-#pragma unroll
-        for (int k = 0; k < SLOTS; ++k)
-            if (ri[k] > l && ri[k] < nbb && ci[k] <= l) x[k] -= cv[ri[k]] * rv[ci[k]];
+        __syncwarp();
+        if (i > k && i < nbb) {
+            const double lik = L[i * LD + k];
+            for (int j = 0; j <= k; ++j) X[i * LD + j] -= lik * X[k * LD + j];
+        }
+        __syncwarp();
     }
     T* inv = A.inv + (int64_t)member * A.inv_len + A.inv_off[blockIdx.x];
-    for (int q = tid; q < NB * NB; q += 256) {
-        int i = q % NB, j = q / NB;
-        if (i < j || i >= nbb) inv[i + (int64_t)j * NB] = T(0);
-    }
-    __syncthreads();
-#pragma unroll
-    for (int k = 0; k < SLOTS; ++k)
-        if (ri[k] >= 0 && ri[k] < nbb && ci[k] < nbb) inv[ri[k] + (int64_t)ci[k] * NB] = T(x[k]);
+    for (int j = 0; j < NB; ++j) inv[i + (int64_t)j * NB] = (i < nbb && j < nbb && j <= i) ? T(X[i * LD + j]) : T(0);
 }
 
 // inverse of one 64 x 64 diagonal block of a panel (lower triangle as stored; unit or not), with the
 // register-owned right-looking substitution of chol_diag_kernel
 template <typename T>
 __global__ void __launch_bounds__(256) block_inv_kernel(BlockInvArgs<T> A) {
-    constexpr int NB = CHOL_NB, NE = NB * (NB + 1) / 2, SLOTS = (NE + 255) / 256;
+    constexpr int NB = 64, NE = NB * (NB + 1) / 2, SLOTS = (NE + 255) / 256;
     __shared__ double colv[2][NB];
     __shared__ double rowv[2][NB];
     const int s = A.tasks[2 * blockIdx.x], b = A.tasks[2 * blockIdx.x + 1];
@@ -475,7 +430,7 @@ template <typename T>
 cudaError_t launch_chol_diag(const CholDiagArgs<T>& a, int nmembers, cudaStream_t st) {
     if (a.count == 0) return cudaSuccess;
     dim3 grid(a.count, nmembers);
-    chol_diag_kernel<T><<<grid, 256, 0, st>>>(a);
+    chol_diag_kernel<T><<<grid, 32, 0, st>>>(a);
     return cudaGetLastError();
 }
 

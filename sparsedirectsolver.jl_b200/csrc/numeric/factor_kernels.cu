@@ -78,8 +78,9 @@ __global__ void __launch_bounds__(256) small_front_kernel(SmallArgs<T> A) {
         const T* C = cbar + cd.cb;
         for (int jj = warp; jj < mc; jj += nwarps) {
             const int pj = ri[jj];
-            for (int ii = (STRUCT == STRUCT_G ? 0 : jj) + lane; ii < mc; ii += 32)
-                F[ri[ii] + pj * ld] += C[ii + (int64_t)jj * mc];
+            const int i0 = STRUCT == STRUCT_G ? 0 : jj;
+            batched_copy<4>(i0 + lane, 32, mc, [&](int ii) { return (double)C[ii + (int64_t)jj * mc]; },
+                            [&](int ii, double v) { F[ri[ii] + pj * ld] += T(v); });
         }
         __syncthreads();
     }
@@ -284,12 +285,12 @@ __global__ void assemble_large_kernel(LargeAsmArgs<T> A) {
         const T* C = cbar + cd.cb;
         const int* ri = A.maps.relind + cd.ri_begin;
         // lower part: C[ii, t], ii >= t  ->  F[ri[ii], p]
-        for (int ii = t + lane; ii < mc; ii += 32) {
-            const int pi = ri[ii];
-            const T v = C[ii + (int64_t)t * mc];
-            if (p < w) factor[fd.panel + pi + (int64_t)p * f] += v;
-            else if (pi >= w) cbown[(pi - w) + (int64_t)(p - w) * m] += v;
-        }
+        batched_copy<4>(t + lane, 32, mc, [&](int ii) { return (double)C[ii + (int64_t)t * mc]; },
+                        [&](int ii, double v) {
+                            const int pi = ri[ii];
+                            if (p < w) factor[fd.panel + pi + (int64_t)p * f] += T(v);
+                            else if (pi >= w) cbown[(pi - w) + (int64_t)(p - w) * m] += T(v);
+                        });
         if (STRUCT == STRUCT_G) {
             if (p < w) {
                 // upper part of row p: C[t, jj], jj > t  ->  F[p, ri[jj]] = U^T panel (ri[jj], p)

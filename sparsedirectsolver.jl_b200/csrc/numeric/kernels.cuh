@@ -174,7 +174,7 @@ struct BlockInvArgs {
 template <typename T>
 cudaError_t launch_block_inv(const BlockInvArgs<T>& a, int nmembers, cudaStream_t st);
 
-constexpr int CHOL_NB = 64;
+constexpr int CHOL_NB = 32;   // column block of the large-front Cholesky (one warp per diagonal block)
 cudaError_t prepare_factor_kernels(int max_smem);
 cudaError_t prepare_dense_kernels(int max_smem);
 cudaError_t prepare_solve_kernels(int max_smem);   // column block of the large-front Cholesky

@@ -662,6 +662,7 @@ Plan* build_plan(const sdsb200_symbolic* sym, const sdsb200_plan_options* popts,
         P->d_xtmp = dalloc<double>(P, n * P->max_nrhs);
         P->d_barrier = dalloc<unsigned int>(P, 1);
         P->d_solve_status = dalloc<int32_t>(P, 1);
+        P->d_trace = dalloc<int64_t>(P, 2 * Plan::TRACE_CAP);
         cudaMemsetAsync(P->d_solve_status, 0, sizeof(int32_t), st);
         P->d_Y = dalloc<double>(P, n * P->max_nrhs * nb);
         P->d_U = dalloc<double>(P, P->ulen * nb);

@@ -99,6 +99,8 @@ struct Plan {
     double* d_xtmp = nullptr;
     unsigned int* d_barrier = nullptr;
     int32_t* d_solve_status = nullptr;
+    int64_t* d_trace = nullptr;   // persistent-solve phase stamps (profiling)
+    static constexpr int TRACE_CAP = 16384;
     int32_t* d_rect_tiles = nullptr;    // (front, start) pairs: forward row tiles, backward column tiles
     std::vector<int64_t> level_ftile_off, level_btile_off;
     std::vector<int> level_nftile, level_nbtile;

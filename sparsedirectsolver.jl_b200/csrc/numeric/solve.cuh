@@ -54,6 +54,10 @@ struct PersistArgs {
     double* xtmp;              // n x nrhs scratch
     unsigned int* barrier;     // grid barrier counter (zeroed before the launch)
     int32_t* status;           // nonzero: a barrier wait gave up
+    int64_t* trace;            // profiling: (tag, %globaltimer ns) pairs written by CTA 0, or NULL
+    int32_t trace_cap;
+    int32_t warp_smem;         // doubles of shared memory per warp for the small fronts (xs + Ld)
+    int32_t warp_xs;           // doubles of xs within it
 };
 
 struct DiagArgs {

@@ -53,12 +53,12 @@ __device__ __forceinline__ void row_dot(const T* __restrict__ Lrow, int64_t ld, 
 template <typename T, class XF>
 __device__ __forceinline__ void col_dot(const T* __restrict__ Lcol, int M, int lane, int rc, XF xval, double* acc) {
     int i = lane;
-    for (; i + 96 < M; i += 128) {
-        double lv[4];
+    for (; i + 224 < M; i += 256) {
+        double lv[8];
 #pragma unroll
-        for (int u = 0; u < 4; ++u) lv[u] = (double)Lcol[i + 32 * u];
+        for (int u = 0; u < 8; ++u) lv[u] = (double)Lcol[i + 32 * u];
 #pragma unroll
-        for (int u = 0; u < 4; ++u)
+        for (int u = 0; u < 8; ++u)
 #pragma unroll
             for (int r = 0; r < 8; ++r)
                 if (r < rc) acc[r] += lv[u] * xval(i + 32 * u, r);
@@ -84,10 +84,8 @@ __device__ void forward_front(const SweepArgs<T>& A, int s, int member, double* 
     const int32_t* piv = A.piv ? A.piv + (int64_t)member * n : nullptr;
     const int tid = threadIdx.x, nt = blockDim.x, lane = tid & 31, warp = tid >> 5, nwarps = nt >> 5;
     // gather this front's slice in the numbering before pivoting: the children's updates use it
-    for (int q = tid; q < w * nrhs; q += nt) {
-        int k = q % w, r = q / w;
-        xs[q] = Y[fd.c0 + k + (int64_t)r * n];
-    }
+    batched_copy<4>(tid, nt, w * nrhs, [&](int q) { return Y[fd.c0 + q % w + (int64_t)(q / w) * n]; },
+                    [&](int q, double v) { xs[q] = v; });
     for (int q = tid; q < m * nrhs; q += nt) u[q] = 0.0;
     __syncthreads();
     for (int cq = fd.ch_begin; cq < fd.ch_end; ++cq) {
@@ -97,12 +95,23 @@ __device__ void forward_front(const SweepArgs<T>& A, int s, int member, double* 
         if (mc <= 0) continue;
         const double* uc = U + A.uoff[c];
         const int32_t* ri = A.relind + cd.ri_begin;
-        for (int q = tid; q < mc * nrhs; q += nt) {
-            int i = q % mc, r = q / mc;
-            int p = ri[i];
-            double v = uc[q];
-            if (p < w) xs[p + r * w] -= v;
-            else u[(p - w) + r * m] += v;
+        for (int q0 = tid; q0 < mc * nrhs; q0 += 4 * nt) {
+            int pp[4];
+            double vv[4];
+#pragma unroll
+            for (int k = 0; k < 4; ++k) {
+                const int q = q0 + k * nt;
+                pp[k] = q < mc * nrhs ? ri[q % mc] : -1;
+                vv[k] = q < mc * nrhs ? uc[q] : 0.0;
+            }
+#pragma unroll
+            for (int k = 0; k < 4; ++k) {
+                const int q = q0 + k * nt;
+                if (q >= mc * nrhs) continue;
+                const int r = q / mc, p = pp[k];
+                if (p < w) xs[p + r * w] -= vv[k];
+                else u[(p - w) + r * m] += vv[k];
+            }
         }
         __syncthreads();
     }
@@ -113,10 +122,8 @@ __device__ void forward_front(const SweepArgs<T>& A, int s, int member, double* 
             Y[fd.c0 + k + (int64_t)r * n] = xs[q];
         }
         __syncthreads();
-        for (int q = tid; q < w * nrhs; q += nt) {
-            int k = q % w, r = q / w;
-            xs[q] = Y[piv[fd.c0 + k] - 1 + (int64_t)r * n];
-        }
+        batched_copy<4>(tid, nt, w * nrhs, [&](int q) { return Y[piv[fd.c0 + q % w] - 1 + (int64_t)(q / w) * n]; },
+                        [&](int q, double v) { xs[q] = v; });
         __syncthreads();
     }
     // L11 solve in blocks of 32 columns: the CTA stages the diagonal block in shared memory, warp 0
@@ -124,10 +131,12 @@ __device__ void forward_front(const SweepArgs<T>& A, int s, int member, double* 
     __shared__ double Ld[32][33];
     for (int jb = 0; jb < w; jb += 32) {
         const int bw = min(32, w - jb);
-        for (int q = tid; q < 32 * 32; q += nt) {
-            int i = q & 31, j = q >> 5;
-            Ld[i][j] = (i < bw && j < bw && i >= j) ? (double)L[(jb + i) + (int64_t)(jb + j) * f] : 0.0;
-        }
+        batched_copy<4>(tid, nt, 32 * 32,
+                        [&](int q) {
+                            const int i = q & 31, j = q >> 5;
+                            return (i < bw && j < bw && i >= j) ? (double)L[(jb + i) + (int64_t)(jb + j) * f] : 0.0;
+                        },
+                        [&](int q, double v) { Ld[q & 31][q >> 5] = v; });
         __syncthreads();
         for (int r = warp; r < nrhs; r += nwarps) {  // one warp per right-hand side
             double val = lane < bw ? xs[jb + lane + r * w] : 0.0;
@@ -190,16 +199,11 @@ __device__ void backward_front(const SweepArgs<T>& A, int s, int member, double*
     const int32_t* piv = A.piv ? A.piv + (int64_t)member * n : nullptr;
     const int32_t* rows = A.rowval + fd.row_begin;
     const int tid = threadIdx.x, nt = blockDim.x, lane = tid & 31, warp = tid >> 5, nwarps = nt >> 5;
-    for (int q = tid; q < w * nrhs; q += nt) {
-        int k = q % w, r = q / w;
-        xs[q] = Y[fd.c0 + k + (int64_t)r * n];
-    }
-    if (A.rect) {
-        for (int q = tid; q < m * nrhs; q += nt) {
-            int i = q % m, r = q / m;
-            xb[q] = Y[rows[w + i] + (int64_t)r * n];
-        }
-    }
+    batched_copy<4>(tid, nt, w * nrhs, [&](int q) { return Y[fd.c0 + q % w + (int64_t)(q / w) * n]; },
+                    [&](int q, double v) { xs[q] = v; });
+    if (A.rect)
+        batched_copy<8>(tid, nt, m * nrhs, [&](int q) { return Y[rows[w + q % m] + (int64_t)(q / m) * n]; },
+                        [&](int q, double v) { xb[q] = v; });
     __syncthreads();
     // x1 -= L21^T x2: one warp per column (large fronts: the column tiles of backward_rect_kernel)
     if (A.rect) {
@@ -226,10 +230,12 @@ __device__ void backward_front(const SweepArgs<T>& A, int s, int member, double*
     const int nblk = (w + 31) / 32;
     for (int bq = nblk - 1; bq >= 0; --bq) {
         const int jb = bq * 32, bw = min(32, w - jb);
-        for (int q = tid; q < 32 * 32; q += nt) {
-            int i = q & 31, j = q >> 5;
-            Ld[i][j] = (i < bw && j < bw && i >= j) ? (double)L[(jb + i) + (int64_t)(jb + j) * f] : 0.0;
-        }
+        batched_copy<4>(tid, nt, 32 * 32,
+                        [&](int q) {
+                            const int i = q & 31, j = q >> 5;
+                            return (i < bw && j < bw && i >= j) ? (double)L[(jb + i) + (int64_t)(jb + j) * f] : 0.0;
+                        },
+                        [&](int q, double v) { Ld[q & 31][q >> 5] = v; });
         __syncthreads();
         for (int r = warp; r < nrhs; r += nwarps) {
             double val = lane < bw ? xs[jb + lane + r * w] : 0.0;
@@ -355,6 +361,184 @@ cudaError_t launch_sweep(bool forward, const SweepArgs<T>& a, int nmembers, int 
 template cudaError_t launch_sweep<double>(bool, const SweepArgs<double>&, int, int, cudaStream_t);
 template cudaError_t launch_sweep<float>(bool, const SweepArgs<float>&, int, int, cudaStream_t);
 
+
+// ---------------------------------------------------------------------------
+// Warp-per-front sweeps of the small fronts in the persistent solve (w < 96): eight fronts in flight per
+// CTA. xs: w x nrhs, Ld: 32 x 33 (both per warp, shared memory).
+template <typename T>
+__device__ void warp_forward_front(const SweepArgs<T>& A, int s, double* xs, double* Ld) {
+    const DFront fd = A.fronts[s];
+    const int f = fd.f, w = fd.w, m = f - w, nrhs = A.nrhs, lane = threadIdx.x & 31;
+    const int64_t n = A.n;
+    const T* L = A.fac + fd.panel;
+    double* Y = A.Y;
+    double* U = A.U;
+    double* u = m > 0 ? U + A.uoff[s] : nullptr;
+    batched_copy<8>(lane, 32, w * nrhs, [&](int q) { return Y[fd.c0 + q % w + (int64_t)(q / w) * n]; },
+                    [&](int q, double v) { xs[q] = v; });
+    for (int q = lane; q < m * nrhs; q += 32) u[q] = 0.0;
+    __syncwarp();
+    for (int cq = fd.ch_begin; cq < fd.ch_end; ++cq) {
+        const int c = A.child_list[cq];
+        const DFront cd = A.fronts[c];
+        const int mc = cd.f - cd.w;
+        if (mc <= 0) continue;
+        const double* uc = U + A.uoff[c];
+        const int32_t* ri = A.relind + cd.ri_begin;
+        for (int q0 = lane; q0 < mc * nrhs; q0 += 128) {
+            int pp[4];
+            double vv[4];
+#pragma unroll
+            for (int k = 0; k < 4; ++k) {
+                const int q = q0 + 32 * k;
+                pp[k] = q < mc * nrhs ? ri[q % mc] : -1;
+                vv[k] = q < mc * nrhs ? uc[q] : 0.0;
+            }
+#pragma unroll
+            for (int k = 0; k < 4; ++k) {
+                const int q = q0 + 32 * k;
+                if (q >= mc * nrhs) continue;
+                const int r = q / mc, p = pp[k];
+                if (p < w) xs[p + r * w] -= vv[k];
+                else u[(p - w) + r * m] += vv[k];
+            }
+        }
+        __syncwarp();
+    }
+    if (A.reorder) {
+        for (int q = lane; q < w * nrhs; q += 32) Y[fd.c0 + q % w + (int64_t)(q / w) * n] = xs[q];
+        __syncwarp();
+        batched_copy<8>(lane, 32, w * nrhs, [&](int q) { return Y[A.piv[fd.c0 + q % w] - 1 + (int64_t)(q / w) * n]; },
+                        [&](int q, double v) { xs[q] = v; });
+        __syncwarp();
+    }
+    for (int jb = 0; jb < w; jb += 32) {
+        const int bw = min(32, w - jb);
+        batched_copy<8>(0, 1, bw,
+                        [&](int j) { return (lane < bw && lane >= j) ? (double)L[(jb + lane) + (int64_t)(jb + j) * f] : 0.0; },
+                        [&](int j, double v) { Ld[lane * 33 + j] = v; });
+        __syncwarp();
+        for (int r = 0; r < nrhs; ++r) {
+            double val = lane < bw ? xs[jb + lane + r * w] : 0.0;
+            for (int j = 0; j < bw; ++j) {
+                if (!A.unit && lane == j) val /= Ld[j * 33 + j];
+                const double xj = __shfl_sync(0xffffffffu, val, j);
+                if (lane > j) val -= Ld[lane * 33 + j] * xj;
+            }
+            if (lane < bw) xs[jb + lane + r * w] = val;
+        }
+        __syncwarp();
+        for (int q = jb + bw + lane; q < w; q += 32) {
+            for (int r0 = 0; r0 < nrhs; r0 += 8) {
+                const int rc = min(8, nrhs - r0);
+                double acc[8];
+#pragma unroll
+                for (int r = 0; r < 8; ++r) acc[r] = 0.0;
+                row_dot(L + q + (int64_t)jb * f, f, bw, xs + jb + r0 * w, w, rc, acc);
+                for (int r = 0; r < rc; ++r) xs[q + (r0 + r) * w] -= acc[r];
+            }
+        }
+        __syncwarp();
+    }
+    for (int i = lane; i < m; i += 32) {
+        for (int r0 = 0; r0 < nrhs; r0 += 8) {
+            const int rc = min(8, nrhs - r0);
+            double acc[8];
+#pragma unroll
+            for (int r = 0; r < 8; ++r) acc[r] = 0.0;
+            row_dot(L + w + i, f, w, xs + r0 * w, w, rc, acc);
+            for (int r = 0; r < rc; ++r) u[i + (r0 + r) * m] += acc[r];
+        }
+    }
+    for (int q = lane; q < w * nrhs; q += 32) Y[fd.c0 + q % w + (int64_t)(q / w) * n] = xs[q];
+    __syncwarp();
+}
+
+template <typename T>
+__device__ void warp_backward_front(const SweepArgs<T>& A, int s, double* xs, double* Ld) {
+    const DFront fd = A.fronts[s];
+    const int f = fd.f, w = fd.w, m = f - w, nrhs = A.nrhs, lane = threadIdx.x & 31;
+    const int64_t n = A.n;
+    const T* L = A.fac + fd.panel;
+    double* Y = A.Y;
+    const int32_t* rows = A.rowval + fd.row_begin + w;
+    batched_copy<8>(lane, 32, w * nrhs, [&](int q) { return Y[fd.c0 + q % w + (int64_t)(q / w) * n]; },
+                    [&](int q, double v) { xs[q] = v; });
+    __syncwarp();
+    // x1 -= L21^T x2: x2 = Y[rows below] gathered in chunks into Ld, lanes over the columns
+    const int CH = max(1, (32 * 33) / nrhs);
+    for (int i0 = 0; i0 < m; i0 += CH) {
+        const int ch = min(CH, m - i0);
+        batched_copy<8>(lane, 32, ch * nrhs, [&](int q) { return Y[rows[i0 + q % ch] + (int64_t)(q / ch) * n]; },
+                        [&](int q, double v) { Ld[q] = v; });
+        __syncwarp();
+        for (int j = lane; j < w; j += 32) {
+            const T* Lc = L + w + i0 + (int64_t)j * f;
+            for (int r0 = 0; r0 < nrhs; r0 += 8) {
+                const int rc = min(8, nrhs - r0);
+                double acc[8];
+#pragma unroll
+                for (int r = 0; r < 8; ++r) acc[r] = 0.0;
+                int i = 0;
+                for (; i + 8 <= ch; i += 8) {
+                    double lv[8];
+#pragma unroll
+                    for (int u = 0; u < 8; ++u) lv[u] = (double)Lc[i + u];
+#pragma unroll
+                    for (int u = 0; u < 8; ++u)
+#pragma unroll
+                        for (int r = 0; r < 8; ++r)
+                            if (r < rc) acc[r] += lv[u] * Ld[i + u + (r0 + r) * ch];
+                }
+                for (; i < ch; ++i) {
+                    const double l = (double)Lc[i];
+#pragma unroll
+                    for (int r = 0; r < 8; ++r)
+                        if (r < rc) acc[r] += l * Ld[i + (r0 + r) * ch];
+                }
+                for (int r = 0; r < rc; ++r) xs[j + (r0 + r) * w] -= acc[r];
+            }
+        }
+        __syncwarp();
+    }
+    const int nblk = (w + 31) / 32;
+    for (int bq = nblk - 1; bq >= 0; --bq) {
+        const int jb = bq * 32, bw = min(32, w - jb);
+        batched_copy<8>(0, 1, bw,
+                        [&](int j) { return (lane < bw && lane >= j) ? (double)L[(jb + lane) + (int64_t)(jb + j) * f] : 0.0; },
+                        [&](int j, double v) { Ld[lane * 33 + j] = v; });
+        __syncwarp();
+        for (int r = 0; r < nrhs; ++r) {
+            double val = lane < bw ? xs[jb + lane + r * w] : 0.0;
+            for (int j = bw - 1; j >= 0; --j) {
+                if (!A.unit && lane == j) val /= Ld[j * 33 + j];
+                const double xj = __shfl_sync(0xffffffffu, val, j);
+                if (lane < j) val -= Ld[j * 33 + lane] * xj;
+            }
+            if (lane < bw) xs[jb + lane + r * w] = val;
+        }
+        __syncwarp();
+        for (int i = lane; i < jb; i += 32) {
+            const T* Lr = L + jb + (int64_t)i * f;   // L[jb + k, i], contiguous in k
+            for (int r0 = 0; r0 < nrhs; r0 += 8) {
+                const int rc = min(8, nrhs - r0);
+                double acc[8];
+#pragma unroll
+                for (int r = 0; r < 8; ++r) acc[r] = 0.0;
+                row_dot(Lr, 1, bw, xs + jb + r0 * w, w, rc, acc);
+                for (int r = 0; r < rc; ++r) xs[i + (r0 + r) * w] -= acc[r];
+            }
+        }
+        __syncwarp();
+    }
+    for (int q = lane; q < w * nrhs; q += 32) {
+        const int k = q % w;
+        const int dst = A.reorder ? A.piv[fd.c0 + k] - 1 : fd.c0 + k;
+        Y[dst + (int64_t)(q / w) * n] = xs[q];
+    }
+    __syncwarp();
+}
+
 // ---------------------------------------------------------------------------
 // Persistent solve. Grid barrier: one arrival per CTA on a monotonic counter; the wait is bounded
 // (about two seconds of spinning), after which the CTA records the failure and goes on, so a lost
@@ -381,6 +565,9 @@ __device__ __forceinline__ void grid_barrier(unsigned int* bar, unsigned int& ep
     __syncthreads();
 }
 
+// Shared memory of a wide-front tile: the 64 x 64 inverse block, y_b, x_b and partial sums.
+constexpr int WT_SMEM_DOUBLES_FIXED = SOLVE_BLK * (SOLVE_BLK + 1);
+
 // forward, wide front s, block step b, row tile t: x_b = inv(L_bb) y_b; rows below get -L x_b
 template <typename T>
 __device__ void wide_forward_tile(const PersistArgs<T>& P, int s, int b, int t, double* sm) {
@@ -393,42 +580,58 @@ __device__ void wide_forward_tile(const PersistArgs<T>& P, int s, int b, int t, 
     const T* inv = P.dinv_fw + P.dinv_off[s] + (int64_t)b * SOLVE_BLK * SOLVE_BLK;
     double* Y = A.Y;
     double* u = m > 0 ? A.U + A.uoff[s] : nullptr;
-    double* yb = sm;                     // SOLVE_BLK x nrhs
-    double* xb = sm + SOLVE_BLK * nrhs;  // SOLVE_BLK x nrhs
+    double* Iv = sm;                                  // SOLVE_BLK x (SOLVE_BLK + 1)
+    double* yb = sm + WT_SMEM_DOUBLES_FIXED;          // SOLVE_BLK x nrhs
+    double* xb = yb + SOLVE_BLK * nrhs;               // SOLVE_BLK x nrhs
+    double* part = xb + SOLVE_BLK * nrhs;             // 4 x SOLVE_BLK x nrhs partial sums
     const int tid = threadIdx.x, nt = blockDim.x;
-    for (int q = tid; q < SOLVE_BLK * nrhs; q += nt) {
-        int k = q % SOLVE_BLK, r = q / SOLVE_BLK;
-        yb[q] = k < bw ? Y[fd.c0 + jb + k + (int64_t)r * n] : 0.0;
-    }
+    batched_copy<8>(tid, nt, SOLVE_BLK * SOLVE_BLK,
+                    [&](int q) { return (q % SOLVE_BLK < bw && q / SOLVE_BLK < bw) ? (double)inv[q] : 0.0; },
+                    [&](int q, double v) { Iv[q % SOLVE_BLK + (q / SOLVE_BLK) * (SOLVE_BLK + 1)] = v; });
+    batched_copy<4>(tid, nt, SOLVE_BLK * nrhs,
+                    [&](int q) { return q % SOLVE_BLK < bw ? Y[fd.c0 + jb + q % SOLVE_BLK + (int64_t)(q / SOLVE_BLK) * n] : 0.0; },
+                    [&](int q, double v) { yb[q] = v; });
     __syncthreads();
     for (int q = tid; q < SOLVE_BLK * nrhs; q += nt) {
         int i = q % SOLVE_BLK, r = q / SOLVE_BLK;
         double acc = 0.0;
-        if (i < bw)
-            for (int j = 0; j <= i; ++j) acc += (double)inv[i + j * SOLVE_BLK] * yb[j + r * SOLVE_BLK];
+#pragma unroll 8
+        for (int j = 0; j < SOLVE_BLK; ++j) acc += Iv[i + j * (SOLVE_BLK + 1)] * yb[j + r * SOLVE_BLK];
         xb[q] = acc;
     }
     __syncthreads();
     const int r0 = t * SOLVE_BLK;
-    for (int q = tid; q < SOLVE_BLK; q += nt) {
-        const int row = r0 + q;
-        if (row >= f || row < jb) continue;
-        if (row < jb + bw) {  // the block's own rows: to the scratch, copied to Y after the level
-            for (int r = 0; r < nrhs; ++r) P.xtmp[fd.c0 + row + (int64_t)r * n] = xb[row - jb + r * SOLVE_BLK];
-            continue;
-        }
-        for (int r0_ = 0; r0_ < nrhs; r0_ += 8) {
-            const int rc = min(8, nrhs - r0_);
-            double acc[8];
+    // rows of the tile below the block: 4 threads per row, 16 block columns each
+    const int row = r0 + (tid & (SOLVE_BLK - 1)), quarter = tid / SOLVE_BLK;
+    const bool upd = tid < 4 * SOLVE_BLK && row < f && row >= jb + bw;
+    for (int r0_ = 0; r0_ < nrhs; r0_ += 8) {
+        const int rc = min(8, nrhs - r0_);
+        double acc[8];
 #pragma unroll
-            for (int r = 0; r < 8; ++r) acc[r] = 0.0;
-            row_dot(L + row + (int64_t)jb * f, f, bw, xb + r0_ * SOLVE_BLK, SOLVE_BLK, rc, acc);
+        for (int r = 0; r < 8; ++r) acc[r] = 0.0;
+        if (upd) {
+            const int c0 = quarter * (SOLVE_BLK / 4), cw = max(0, min(SOLVE_BLK / 4, bw - c0));
+            row_dot(L + row + (int64_t)(jb + c0) * f, f, cw, xb + c0 + r0_ * SOLVE_BLK, SOLVE_BLK, rc, acc);
+        }
+        if (tid < 4 * SOLVE_BLK)
+            for (int r = 0; r < rc; ++r) part[(tid & (SOLVE_BLK - 1)) + SOLVE_BLK * (quarter + 4 * r)] = acc[r];
+        __syncthreads();
+        if (tid < SOLVE_BLK && row < f && row >= jb + bw) {
             for (int r = 0; r < rc; ++r) {
-                if (row < w) Y[fd.c0 + row + (int64_t)(r0_ + r) * n] -= acc[r];
-                else u[row - w + (r0_ + r) * m] += acc[r];
+                const double v = part[tid + SOLVE_BLK * (4 * r)] + part[tid + SOLVE_BLK * (1 + 4 * r)] +
+                                 part[tid + SOLVE_BLK * (2 + 4 * r)] + part[tid + SOLVE_BLK * (3 + 4 * r)];
+                if (row < w) Y[fd.c0 + row + (int64_t)(r0_ + r) * n] -= v;
+                else u[row - w + (r0_ + r) * m] += v;
             }
         }
+        __syncthreads();
     }
+    // the block's own rows: to the scratch, copied to Y after the level
+    if (t == b)
+        for (int q = tid; q < bw * nrhs; q += nt) {
+            int k = q % bw, r = q / bw;
+            P.xtmp[fd.c0 + jb + k + (int64_t)r * n] = xb[k + r * SOLVE_BLK];
+        }
     __syncthreads();
 }
 
@@ -444,19 +647,22 @@ __device__ void wide_backward_tile(const PersistArgs<T>& P, int s, int b, int t,
     const T* L = A.fac + fd.panel;
     const T* inv = P.dinv_bw + P.dinv_off[s] + (int64_t)b * SOLVE_BLK * SOLVE_BLK;
     double* Y = A.Y;
-    double* yb = sm;
-    double* xb = sm + SOLVE_BLK * nrhs;
+    double* Iv = sm;
+    double* yb = sm + WT_SMEM_DOUBLES_FIXED;
+    double* xb = yb + SOLVE_BLK * nrhs;
     const int tid = threadIdx.x, nt = blockDim.x, lane = tid & 31, warp = tid >> 5, nwarps = nt >> 5;
-    for (int q = tid; q < SOLVE_BLK * nrhs; q += nt) {
-        int k = q % SOLVE_BLK, r = q / SOLVE_BLK;
-        yb[q] = k < bw ? Y[fd.c0 + jb + k + (int64_t)r * n] : 0.0;
-    }
+    batched_copy<8>(tid, nt, SOLVE_BLK * SOLVE_BLK,
+                    [&](int q) { return (q % SOLVE_BLK < bw && q / SOLVE_BLK < bw) ? (double)inv[q] : 0.0; },
+                    [&](int q, double v) { Iv[q % SOLVE_BLK + (q / SOLVE_BLK) * (SOLVE_BLK + 1)] = v; });
+    batched_copy<4>(tid, nt, SOLVE_BLK * nrhs,
+                    [&](int q) { return q % SOLVE_BLK < bw ? Y[fd.c0 + jb + q % SOLVE_BLK + (int64_t)(q / SOLVE_BLK) * n] : 0.0; },
+                    [&](int q, double v) { yb[q] = v; });
     __syncthreads();
     for (int q = tid; q < SOLVE_BLK * nrhs; q += nt) {
         int i = q % SOLVE_BLK, r = q / SOLVE_BLK;
         double acc = 0.0;
-        if (i < bw)
-            for (int j = i; j < bw; ++j) acc += (double)inv[j + i * SOLVE_BLK] * yb[j + r * SOLVE_BLK];
+#pragma unroll 8
+        for (int j = 0; j < SOLVE_BLK; ++j) acc += Iv[j + i * (SOLVE_BLK + 1)] * yb[j + r * SOLVE_BLK];
         xb[q] = acc;
     }
     __syncthreads();
@@ -467,24 +673,49 @@ __device__ void wide_backward_tile(const PersistArgs<T>& P, int s, int b, int t,
             P.xtmp[fd.c0 + jb + k + (int64_t)r * n] = xb[k + r * SOLVE_BLK];
         }
     } else {
-        for (int a = c0 + warp; a < min(c0 + SOLVE_BLK, jb); a += nwarps) {
-            const double l = lane < bw ? (double)L[(jb + lane) + (int64_t)a * f] : 0.0;
-            const double l2 = lane + 32 < bw ? (double)L[(jb + lane + 32) + (int64_t)a * f] : 0.0;
-            for (int r = 0; r < nrhs; ++r) {
-                double v = l * xb[lane + r * SOLVE_BLK] + l2 * xb[lane + 32 + r * SOLVE_BLK];
+        // columns of the tile: 8 per warp, all their loads issued before the reductions
+        const int a0 = c0 + warp * (SOLVE_BLK / 8);
+        double l1[SOLVE_BLK / 8], l2[SOLVE_BLK / 8];
+#pragma unroll
+        for (int c = 0; c < SOLVE_BLK / 8; ++c) {
+            const int a = a0 + c;
+            const bool ok = a < jb;
+            l1[c] = ok && lane < bw ? (double)L[(jb + lane) + (int64_t)a * f] : 0.0;
+            l2[c] = ok && lane + 32 < bw ? (double)L[(jb + lane + 32) + (int64_t)a * f] : 0.0;
+        }
+        for (int r = 0; r < nrhs; ++r) {
+            const double x1 = xb[lane + r * SOLVE_BLK], x2 = xb[lane + 32 + r * SOLVE_BLK];
+#pragma unroll
+            for (int c = 0; c < SOLVE_BLK / 8; ++c) {
+                double v = l1[c] * x1 + l2[c] * x2;
                 for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
-                if (lane == 0) Y[fd.c0 + a + (int64_t)r * n] -= v;
+                if (lane == 0 && a0 + c < jb) Y[fd.c0 + a0 + c + (int64_t)r * n] -= v;
             }
         }
     }
-    (void)f;
+    (void)f; (void)nwarps;
     __syncthreads();
+}
+
+__device__ __forceinline__ void trace_mark(int64_t* trace, int cap, int& n, int64_t tag) {
+    if (trace && blockIdx.x == 0 && threadIdx.x == 0 && n < cap) {
+        uint64_t t;
+        asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+        trace[2 * n] = tag;
+        trace[2 * n + 1] = (int64_t)t;
+        ++n;
+    }
 }
 
 template <typename T>
 __global__ void __launch_bounds__(SOLVE_THREADS) persistent_solve_kernel(PersistArgs<T> P) {
     extern __shared__ double psm[];
     unsigned int epoch = 0;
+    int ntr = 0;
+    // phase tags: 1 perm, 2 fwd level A, 3 fwd block step, 4 diag, 5 bwd L21^T, 6 bwd block step,
+    // 7 bwd level end (small fronts), 8 final; tag = kind << 40 | level << 16 | step
+#define TRACE(kind, lev, stp) trace_mark(P.trace, P.trace_cap, ntr, ((int64_t)(kind) << 40) | ((int64_t)(lev) << 16) | (stp))
+    TRACE(0, 0, 0);
     const int G = gridDim.x;
     const int64_t n = P.fw.n;
     const int nrhs = P.fw.nrhs;
@@ -495,11 +726,21 @@ __global__ void __launch_bounds__(SOLVE_THREADS) persistent_solve_kernel(Persist
         P.fw.Y[q] = P.in[P.perm[k] + r * P.ldin];
     }
     grid_barrier(P.barrier, epoch, P.status);
+    TRACE(1, 0, 0);
     // forward levels
     for (int L = 0; L < P.nlevels; ++L) {
         const int so = P.lev_small[2 * L], sc = P.lev_small[2 * L + 1];
         const int lo = P.lev_large[2 * L], lc = P.lev_large[2 * L + 1];
-        for (int i = blockIdx.x; i < sc; i += G) forward_front(P.fw, P.list[so + i], 0, psm);
+        if (sc >= G * (blockDim.x >> 5) / 2) {
+            // many small fronts: one warp each
+            const int wpc = blockDim.x >> 5, warp = threadIdx.x >> 5;
+            double* xs = psm + warp * P.warp_smem;
+            for (int i = blockIdx.x * wpc + warp; i < sc; i += G * wpc)
+                warp_forward_front(P.fw, P.list[so + i], xs, xs + P.warp_xs);
+        } else {
+            // few: one CTA each
+            for (int i = blockIdx.x; i < sc; i += G) forward_front(P.fw, P.list[so + i], 0, psm);
+        }
         // wide fronts: pull the children and apply the local pivot order (one CTA each, from the end)
         for (int i = G - 1 - blockIdx.x; i < lc; i += G) {
             const int s = P.list[lo + i];
@@ -537,20 +778,31 @@ __global__ void __launch_bounds__(SOLVE_THREADS) persistent_solve_kernel(Persist
             __syncthreads();
         }
         grid_barrier(P.barrier, epoch, P.status);
+        TRACE(2, L, 0);
         const int nb = P.lev_maxblk[L];
         for (int b = 0; b < nb; ++b) {
-            // (front, row tile) pairs of this step, spread over the grid
-            int task = 0;
+            // (front, row tile) pairs of this step, spread over the grid: task k -> front by running counts
+            int total = 0;
             for (int i = 0; i < lc; ++i) {
-                const int s = P.list[lo + i];
-                const DFront fd = P.fw.fronts[s];
-                const int nblk = (fd.w + SOLVE_BLK - 1) / SOLVE_BLK;
-                if (b >= nblk) continue;
-                const int ntile = (fd.f + SOLVE_BLK - 1) / SOLVE_BLK;
-                for (int t = b; t < ntile; ++t, ++task)
-                    if (task % G == blockIdx.x) wide_forward_tile(P, s, b, t, psm);
+                const DFront fd = P.fw.fronts[P.list[lo + i]];
+                if (b < (fd.w + SOLVE_BLK - 1) / SOLVE_BLK) total += (fd.f + SOLVE_BLK - 1) / SOLVE_BLK - b;
+            }
+            for (int k = blockIdx.x; k < total; k += G) {
+                int kk = k;
+                for (int i = 0; i < lc; ++i) {
+                    const int s = P.list[lo + i];
+                    const DFront fd = P.fw.fronts[s];
+                    if (b >= (fd.w + SOLVE_BLK - 1) / SOLVE_BLK) continue;
+                    const int cnt = (fd.f + SOLVE_BLK - 1) / SOLVE_BLK - b;
+                    if (kk < cnt) {
+                        wide_forward_tile(P, s, b, b + kk, psm);
+                        break;
+                    }
+                    kk -= cnt;
+                }
             }
             grid_barrier(P.barrier, epoch, P.status);
+            TRACE(3, L, b);
         }
         // the wide fronts' solutions into Y (read again only after later barriers)
         for (int i = 0; i < lc; ++i) {
@@ -561,6 +813,8 @@ __global__ void __launch_bounds__(SOLVE_THREADS) persistent_solve_kernel(Persist
             }
         }
     }
+    // the copies of the last level's wide fronts must land before Y is read again
+    grid_barrier(P.barrier, epoch, P.status);
     // diagonal: D^{-1} with 1x1 and 2x2 blocks
     if (P.diag_mode) {
         for (int64_t q = gtid; q < n * nrhs; q += gstride) {
@@ -579,52 +833,83 @@ __global__ void __launch_bounds__(SOLVE_THREADS) persistent_solve_kernel(Persist
             }
         }
         grid_barrier(P.barrier, epoch, P.status);
+        TRACE(4, 0, 0);
     }
     // backward levels
     for (int L = P.nlevels - 1; L >= 0; --L) {
         const int so = P.lev_small[2 * L], sc = P.lev_small[2 * L + 1];
         const int lo = P.lev_large[2 * L], lc = P.lev_large[2 * L + 1];
         if (lc) {
-            // x1 -= L21^T x2 for the wide fronts: one warp per column, columns spread over the grid
-            const int warps = blockDim.x >> 5, lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-            int col = 0;
+            // stage x2 = Y[rows below] of the wide fronts in their update vectors (free in this sweep)
             for (int i = 0; i < lc; ++i) {
                 const int s = P.list[lo + i];
                 const DFront fd = P.bw.fronts[s];
-                const int f = fd.f, w = fd.w, m = f - w;
-                const T* Lp = P.bw.fac + fd.panel;
+                const int w = fd.w, m = fd.f - fd.w;
+                if (m == 0) continue;
+                double* xb = P.bw.U + P.bw.uoff[s];
                 const int32_t* rows = P.bw.rowval + fd.row_begin + w;
-                for (int j = 0; j < w; ++j, ++col) {
-                    if (col % (G * warps) != blockIdx.x * warps + warp || m == 0) continue;
-                    for (int r0 = 0; r0 < nrhs; r0 += 8) {
-                        const int rc = min(8, nrhs - r0);
-                        double acc[8];
+                for (int64_t q = gtid; q < (int64_t)m * nrhs; q += gstride) {
+                    const int i2 = (int)(q % m), r = (int)(q / m);
+                    xb[q] = P.bw.Y[rows[i2] + (int64_t)r * n];
+                }
+            }
+            grid_barrier(P.barrier, epoch, P.status);
+            // x1 -= L21^T x2 for the wide fronts: one warp per column, columns spread over the grid
+            const int warps = blockDim.x >> 5, lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+            int totc = 0;
+            for (int i = 0; i < lc; ++i) totc += P.bw.fronts[P.list[lo + i]].w;
+            for (int col = blockIdx.x * warps + warp; col < totc; col += G * warps) {
+                int j = col, i = 0, s = 0;
+                for (; i < lc; ++i) {
+                    s = P.list[lo + i];
+                    const int wi = P.bw.fronts[s].w;
+                    if (j < wi) break;
+                    j -= wi;
+                }
+                const DFront fd = P.bw.fronts[s];
+                const int f = fd.f, w = fd.w, m = f - w;
+                if (m == 0) continue;
+                const T* Lp = P.bw.fac + fd.panel;
+                const double* xb = P.bw.U + P.bw.uoff[s];
+                for (int r0 = 0; r0 < nrhs; r0 += 8) {
+                    const int rc = min(8, nrhs - r0);
+                    double acc[8];
 #pragma unroll
-                        for (int r = 0; r < 8; ++r) acc[r] = 0.0;
-                        col_dot(Lp + w + (int64_t)j * f, m, lane, rc,
-                                [&](int i2, int r) { return P.bw.Y[rows[i2] + (int64_t)(r0 + r) * n]; }, acc);
+                    for (int r = 0; r < 8; ++r) acc[r] = 0.0;
+                    col_dot(Lp + w + (int64_t)j * f, m, lane, rc,
+                            [&](int i2, int r) { return xb[i2 + (r0 + r) * m]; }, acc);
 #pragma unroll
-                        for (int r = 0; r < 8; ++r) {
-                            double v = acc[r];
-                            for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
-                            if (lane == 0 && r < rc) P.bw.Y[fd.c0 + j + (int64_t)(r0 + r) * n] -= v;
-                        }
+                    for (int r = 0; r < 8; ++r) {
+                        double v = acc[r];
+                        for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+                        if (lane == 0 && r < rc) P.bw.Y[fd.c0 + j + (int64_t)(r0 + r) * n] -= v;
                     }
                 }
             }
             grid_barrier(P.barrier, epoch, P.status);
+            TRACE(5, L, 0);
             const int nb = P.lev_maxblk[L];
             for (int b = nb - 1; b >= 0; --b) {
-                int task = 0;
+                int total = 0;
                 for (int i = 0; i < lc; ++i) {
-                    const int s = P.list[lo + i];
-                    const DFront fd = P.bw.fronts[s];
-                    const int nblk = (fd.w + SOLVE_BLK - 1) / SOLVE_BLK;
-                    if (b >= nblk) continue;
-                    for (int t = 0; t <= b; ++t, ++task)
-                        if (task % G == blockIdx.x) wide_backward_tile(P, s, b, t, psm);
+                    const DFront fd = P.bw.fronts[P.list[lo + i]];
+                    if (b < (fd.w + SOLVE_BLK - 1) / SOLVE_BLK) total += b + 1;
+                }
+                for (int k = blockIdx.x; k < total; k += G) {
+                    int kk = k;
+                    for (int i = 0; i < lc; ++i) {
+                        const int s = P.list[lo + i];
+                        const DFront fd = P.bw.fronts[s];
+                        if (b >= (fd.w + SOLVE_BLK - 1) / SOLVE_BLK) continue;
+                        if (kk <= b) {
+                            wide_backward_tile(P, s, b, kk, psm);
+                            break;
+                        }
+                        kk -= b + 1;
+                    }
                 }
                 grid_barrier(P.barrier, epoch, P.status);
+                TRACE(6, L, b);
             }
             // the wide fronts' solutions into Y, undoing their local pivot order
             for (int i = 0; i < lc; ++i) {
@@ -636,8 +921,16 @@ __global__ void __launch_bounds__(SOLVE_THREADS) persistent_solve_kernel(Persist
                 }
             }
         }
-        for (int i = blockIdx.x; i < sc; i += G) backward_front(P.bw, P.list[so + i], 0, psm);
+        if (sc >= G * (blockDim.x >> 5) / 2) {
+            const int wpc = blockDim.x >> 5, warp = threadIdx.x >> 5;
+            double* xs = psm + warp * P.warp_smem;
+            for (int i = blockIdx.x * wpc + warp; i < sc; i += G * wpc)
+                warp_backward_front(P.bw, P.list[so + i], xs, xs + P.warp_xs);
+        } else {
+            for (int i = blockIdx.x; i < sc; i += G) backward_front(P.bw, P.list[so + i], 0, psm);
+        }
         grid_barrier(P.barrier, epoch, P.status);
+        TRACE(7, L, 0);
     }
     // out[perm] = Y (or +=)
     for (int64_t q = gtid; q < n * nrhs; q += gstride) {
@@ -646,6 +939,8 @@ __global__ void __launch_bounds__(SOLVE_THREADS) persistent_solve_kernel(Persist
         if (P.mode == 2) *o += P.fw.Y[q];
         else *o = P.fw.Y[q];
     }
+    TRACE(8, 0, 0);
+#undef TRACE
 }
 
 template <typename T>
