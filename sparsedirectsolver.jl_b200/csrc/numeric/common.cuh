@@ -107,4 +107,26 @@ __device__ __forceinline__ void batched_copy(int t0, int step, int N, LD load, S
     }
 }
 
+// Scattered accumulation *dst(q) += val(q) for q = t0, t0 + step, ... < N, where no two q of one call
+// share a target (dst returns nullptr to skip q). U values and U current targets are loaded before
+// the U stores, so the read-modify-writes of a batch overlap instead of running one after another.
+template <int U, class T, class VAL, class DST>
+__device__ __forceinline__ void batched_add(int t0, int step, int N, VAL val, DST dst) {
+    for (int q0 = t0; q0 < N; q0 += U * step) {
+        T* p[U];
+        double v[U], c[U];
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+            const int q = q0 + u * step;
+            p[u] = q < N ? dst(q) : nullptr;
+            v[u] = p[u] ? val(q) : 0.0;
+        }
+#pragma unroll
+        for (int u = 0; u < U; ++u) c[u] = p[u] ? (double)*p[u] : 0.0;
+#pragma unroll
+        for (int u = 0; u < U; ++u)
+            if (p[u]) *p[u] = T(c[u] + v[u]);
+    }
+}
+
 }  // namespace sds

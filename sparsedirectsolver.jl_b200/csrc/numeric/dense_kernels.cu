@@ -138,15 +138,23 @@ __global__ void __launch_bounds__(256) gemm_nt_kernel(GemmArgs<T> A) {
         for (int j = 0; j < 4; ++j) acc[i][j] = T(0);
     const int M = t.m, N = t.n, K = t.k;
     for (int k0 = 0; k0 < K; k0 += BK) {
+        {
+            constexpr int QA = (BM * BK) / 256, QB = (BN * BK) / 256;
+            T va[QA], vb[QB];
 #pragma unroll
-        for (int q = 0; q < (BM * BK) / 256; ++q) {
-            int e = tid + 256 * q, r = e % BM, kk = e / BM;
-            As[kk][r] = (r < M && k0 + kk < K) ? Ab[r + (int64_t)(k0 + kk) * t.lda] : T(0);
-        }
+            for (int q = 0; q < QA; ++q) {
+                int e = tid + 256 * q, r = e % BM, kk = e / BM;
+                va[q] = (r < M && k0 + kk < K) ? Ab[r + (int64_t)(k0 + kk) * t.lda] : T(0);
+            }
 #pragma unroll
-        for (int q = 0; q < (BN * BK) / 256; ++q) {
-            int e = tid + 256 * q, r = e % BN, kk = e / BN;
-            Bs[kk][r] = (r < N && k0 + kk < K) ? Bb[r + (int64_t)(k0 + kk) * t.ldb] : T(0);
+            for (int q = 0; q < QB; ++q) {
+                int e = tid + 256 * q, r = e % BN, kk = e / BN;
+                vb[q] = (r < N && k0 + kk < K) ? Bb[r + (int64_t)(k0 + kk) * t.ldb] : T(0);
+            }
+#pragma unroll
+            for (int q = 0; q < QA; ++q) As[(tid + 256 * q) / BM][(tid + 256 * q) % BM] = va[q];
+#pragma unroll
+            for (int q = 0; q < QB; ++q) Bs[(tid + 256 * q) / BN][(tid + 256 * q) % BN] = vb[q];
         }
         __syncthreads();
 #pragma unroll
@@ -163,15 +171,26 @@ __global__ void __launch_bounds__(256) gemm_nt_kernel(GemmArgs<T> A) {
         }
         __syncthreads();
     }
+    if (!t.mode) {
+        T cv[4][4];
+#pragma unroll
+        for (int i = 0; i < 4; ++i)
+#pragma unroll
+            for (int j = 0; j < 4; ++j) {
+                int r = tx + 16 * i, c = ty + 16 * j;
+                cv[i][j] = (r < M && c < N && r + t.diag >= c) ? Cb[r + (int64_t)c * t.ldc] : T(0);
+            }
+#pragma unroll
+        for (int i = 0; i < 4; ++i)
+#pragma unroll
+            for (int j = 0; j < 4; ++j) acc[i][j] = cv[i][j] - acc[i][j];
+    }
 #pragma unroll
     for (int i = 0; i < 4; ++i)
 #pragma unroll
         for (int j = 0; j < 4; ++j) {
             int r = tx + 16 * i, c = ty + 16 * j;
-            if (r < M && c < N && r + t.diag >= c) {
-                if (t.mode) Cb[r + (int64_t)c * t.ldc] = acc[i][j];
-                else Cb[r + (int64_t)c * t.ldc] -= acc[i][j];
-            }
+            if (r < M && c < N && r + t.diag >= c) Cb[r + (int64_t)c * t.ldc] = acc[i][j];
         }
 }
 
@@ -243,6 +262,27 @@ __global__ void __launch_bounds__(128) gemm_nt_dmma_kernel(GemmArgs<double> A) {
         }
         __syncthreads();
     }
+    // epilogue: every C load is issued before the first store (the stores cannot be proven not to
+    // alias the loads, so an interleaved read-modify-write would serialise 32 memory round trips)
+    if (!t.mode) {
+        double cv[4][4][2];
+#pragma unroll
+        for (int i = 0; i < 4; ++i)
+#pragma unroll
+            for (int j = 0; j < 4; ++j)
+#pragma unroll
+                for (int e = 0; e < 2; ++e) {
+                    const int r = wm * 32 + i * 8 + (lane >> 2);
+                    const int c = wn * 32 + j * 8 + (lane & 3) * 2 + e;
+                    cv[i][j][e] = (r < M && c < N && r + t.diag >= c) ? Cb[r + (int64_t)c * t.ldc] : 0.0;
+                }
+#pragma unroll
+        for (int i = 0; i < 4; ++i)
+#pragma unroll
+            for (int j = 0; j < 4; ++j)
+#pragma unroll
+                for (int e = 0; e < 2; ++e) acc[i][j][e] = cv[i][j][e] - acc[i][j][e];
+    }
 #pragma unroll
     for (int i = 0; i < 4; ++i)
 #pragma unroll
@@ -251,11 +291,7 @@ __global__ void __launch_bounds__(128) gemm_nt_dmma_kernel(GemmArgs<double> A) {
             for (int e = 0; e < 2; ++e) {
                 const int r = wm * 32 + i * 8 + (lane >> 2);
                 const int c = wn * 32 + j * 8 + (lane & 3) * 2 + e;
-                if (r < M && c < N && r + t.diag >= c) {
-                    double* p = Cb + r + (int64_t)c * t.ldc;
-                    if (t.mode) *p = acc[i][j][e];
-                    else *p -= acc[i][j][e];
-                }
+                if (r < M && c < N && r + t.diag >= c) Cb[r + (int64_t)c * t.ldc] = acc[i][j][e];
             }
 }
 
@@ -274,15 +310,16 @@ cudaError_t launch_gemm(const GemmArgs<T>& a, int nmembers, cudaStream_t st) {
 // ---------------------------------------------------------------------------
 // Diagonal block of a large Cholesky front (32 x 32 at column kb): factor with the static clamp and
 // failure rule of the fused kernels, write L11 back, write inv(L11) (ld 32) to scratch for the trsm
-// of the rows below as a GEMM (X = B inv(L11)^T). One warp, lane i holding row i of the block in
-// registers; the pivot columns and the rows of the inverse move by shuffles (loops fully unrolled, so
-// every register index is a constant).
+// of the rows below as a GEMM (X = B inv(L11)^T). One warp over a shared-memory copy of the block:
+// the factor is left-looking (lane i owns row i), the inverse is a forward substitution per column
+// (lane c owns column c). Each step is a short dot product with independent partial sums, so the
+// warp's dependent chain is one dot product plus one square root (or one multiply) per column.
 template <typename T>
 __global__ void __launch_bounds__(32) chol_diag_kernel(CholDiagArgs<T> A) {
     constexpr int NB = CHOL_NB, LD = NB + 1;
     static_assert(NB == 32, "one lane per row of the diagonal block");
     __shared__ double L[NB * LD];
-    __shared__ double X[NB * LD];
+    __shared__ double X[(NB + 1) * LD];   // the inverse, and its reciprocal diagonal in the last row
     const int s = A.list[blockIdx.x];
     const int member = A.members ? A.members[blockIdx.y] : blockIdx.y;
     const DFront fd = A.fronts[s];
@@ -299,22 +336,27 @@ __global__ void __launch_bounds__(32) chol_diag_kernel(CholDiagArgs<T> A) {
     __syncwarp();
     const double eps = A.eps;
     int status = 0;
+    // left-looking by columns: lane i forms s_i = a_ij - sum_{l<j} L_il L_jl (row i against the
+    // broadcast row j, four independent partial sums), then L_ij = s_i / sqrt(s_j)
     for (int j = 0; j < nbb; ++j) {
-        const double ajj = L[j * LD + j];
+        double a0 = 0.0, a1 = 0.0, a2 = 0.0, a3 = 0.0;
+        int l = 0;
+        for (; l + 4 <= j; l += 4) {
+            a0 += L[i * LD + l] * L[j * LD + l];
+            a1 += L[i * LD + l + 1] * L[j * LD + l + 1];
+            a2 += L[i * LD + l + 2] * L[j * LD + l + 2];
+            a3 += L[i * LD + l + 3] * L[j * LD + l + 3];
+        }
+        for (; l < j; ++l) a0 += L[i * LD + l] * L[j * LD + l];
+        const double sv = L[i * LD + j] - ((a0 + a1) + (a2 + a3));
+        const double ajj = __shfl_sync(0xffffffffu, sv, j);
         if (!(ajj > eps || (eps > 0 && ajj >= 0))) {
             status = j + 1;
             break;
         }
         const double sd = sqrt(fmax(ajj, eps));
-        double lij = 0.0;
-        if (i > j && i < nbb) {
-            lij = (double)T(L[i * LD + j] / sd);
-            L[i * LD + j] = lij;
-        }
-        __syncwarp();
-        if (i == j) L[j * LD + j] = (double)T(sd);
-        if (i > j && i < nbb)
-            for (int l = j + 1; l <= i; ++l) L[i * LD + l] = (double)T(L[i * LD + l] - lij * L[l * LD + j]);
+        if (i == j) L[i * LD + j] = (double)T(sd);
+        else if (i > j && i < nbb) L[i * LD + j] = (double)T(sv / sd);
         __syncwarp();
     }
     if (i < nbb)
@@ -334,19 +376,22 @@ __global__ void __launch_bounds__(32) chol_diag_kernel(CholDiagArgs<T> A) {
         S[ST_INFO] = 0;
     }
     if (kb + nbb >= f) return;  // no rows below: no trsm
-    // inverse, right-looking: step k finalizes row k of X and subtracts it from the rows below
-    for (int j = 0; j < NB; ++j) X[i * LD + j] = (i == j) ? 1.0 : 0.0;
+    // inverse: lane c solves L x = e_c by forward substitution, x_r kept in X[r][c]; the reciprocal
+    // diagonal is formed once, and rows above c contribute zeros, so every lane runs the same loop
+    X[32 * LD + i] = i < nbb ? 1.0 / L[i * LD + i] : 0.0;
     __syncwarp();
-    for (int k = 0; k < nbb; ++k) {
-        if (i == k) {
-            const double r = 1.0 / L[k * LD + k];
-            for (int j = 0; j <= k; ++j) X[k * LD + j] *= r;
+    for (int r = 0; r < nbb; ++r) {
+        double a0 = 0.0, a1 = 0.0, a2 = 0.0, a3 = 0.0;
+        int l = 0;
+        for (; l + 4 <= r; l += 4) {
+            a0 += L[r * LD + l] * X[l * LD + i];
+            a1 += L[r * LD + l + 1] * X[(l + 1) * LD + i];
+            a2 += L[r * LD + l + 2] * X[(l + 2) * LD + i];
+            a3 += L[r * LD + l + 3] * X[(l + 3) * LD + i];
         }
-        __syncwarp();
-        if (i > k && i < nbb) {
-            const double lik = L[i * LD + k];
-            for (int j = 0; j <= k; ++j) X[i * LD + j] -= lik * X[k * LD + j];
-        }
+        for (; l < r; ++l) a0 += L[r * LD + l] * X[l * LD + i];
+        const double rhs = (r == i ? 1.0 : 0.0) - ((a0 + a1) + (a2 + a3));
+        X[r * LD + i] = r >= i ? rhs * X[32 * LD + r] : 0.0;
         __syncwarp();
     }
     T* inv = A.inv + (int64_t)member * A.inv_len + A.inv_off[blockIdx.x];

@@ -79,8 +79,8 @@ __global__ void __launch_bounds__(256) small_front_kernel(SmallArgs<T> A) {
         for (int jj = warp; jj < mc; jj += nwarps) {
             const int pj = ri[jj];
             const int i0 = STRUCT == STRUCT_G ? 0 : jj;
-            batched_copy<4>(i0 + lane, 32, mc, [&](int ii) { return (double)C[ii + (int64_t)jj * mc]; },
-                            [&](int ii, double v) { F[ri[ii] + pj * ld] += T(v); });
+            batched_add<8, T>(i0 + lane, 32, mc, [&](int ii) { return (double)C[ii + (int64_t)jj * mc]; },
+                              [&](int ii) -> T* { return F + ri[ii] + pj * ld; });
         }
         __syncthreads();
     }
@@ -285,23 +285,24 @@ __global__ void assemble_large_kernel(LargeAsmArgs<T> A) {
         const T* C = cbar + cd.cb;
         const int* ri = A.maps.relind + cd.ri_begin;
         // lower part: C[ii, t], ii >= t  ->  F[ri[ii], p]
-        batched_copy<4>(t + lane, 32, mc, [&](int ii) { return (double)C[ii + (int64_t)t * mc]; },
-                        [&](int ii, double v) {
-                            const int pi = ri[ii];
-                            if (p < w) factor[fd.panel + pi + (int64_t)p * f] += T(v);
-                            else if (pi >= w) cbown[(pi - w) + (int64_t)(p - w) * m] += T(v);
-                        });
+        batched_add<8, T>(t + lane, 32, mc, [&](int ii) { return (double)C[ii + (int64_t)t * mc]; },
+                          [&](int ii) -> T* {
+                              const int pi = ri[ii];
+                              if (p < w) return factor + fd.panel + pi + (int64_t)p * f;
+                              return pi >= w ? cbown + (pi - w) + (int64_t)(p - w) * m : nullptr;
+                          });
         if (STRUCT == STRUCT_G) {
             if (p < w) {
                 // upper part of row p: C[t, jj], jj > t  ->  F[p, ri[jj]] = U^T panel (ri[jj], p)
-                for (int jj = t + 1 + lane; jj < mc; jj += 32)
-                    ufac[fd.panel + ri[jj] + (int64_t)p * f] += C[t + (int64_t)jj * mc];
+                batched_add<8, T>(t + 1 + lane, 32, mc, [&](int jj) { return (double)C[t + (int64_t)jj * mc]; },
+                                  [&](int jj) -> T* { return ufac + fd.panel + ri[jj] + (int64_t)p * f; });
             } else {
                 // rows of the contribution block above its diagonal: C[ii, t] with w <= ri[ii] < p
-                for (int ii = lane; ii < t; ii += 32) {
-                    const int pi = ri[ii];
-                    if (pi >= w) cbown[(pi - w) + (int64_t)(p - w) * m] += C[ii + (int64_t)t * mc];
-                }
+                batched_add<8, T>(lane, 32, t, [&](int ii) { return (double)C[ii + (int64_t)t * mc]; },
+                                  [&](int ii) -> T* {
+                                      const int pi = ri[ii];
+                                      return pi >= w ? cbown + (pi - w) + (int64_t)(p - w) * m : nullptr;
+                                  });
             }
         }
     }

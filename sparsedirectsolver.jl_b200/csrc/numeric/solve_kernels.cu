@@ -71,6 +71,35 @@ __device__ __forceinline__ void col_dot(const T* __restrict__ Lcol, int M, int l
     }
 }
 
+// Pull one child's update vectors (mc x nrhs at uc) into a front: row p = ri[i] of the front takes
+// x[p + r * ldx] -= uc (p < w, the front's own solution entries) or u[(p - w) + r * m] += uc (its
+// update rows). The child's rows map to distinct rows of the front, so one batch of eight never
+// touches a target twice and all of its loads go out before its stores.
+__device__ __forceinline__ void pull_child(int t0, int step, int N, int mc, const int32_t* ri, const double* uc,
+                                           int w, int m, double* x, int64_t ldx, double* u) {
+    for (int q0 = t0; q0 < N; q0 += 8 * step) {
+        double* dst[8];
+        double val[8];
+#pragma unroll
+        for (int k = 0; k < 8; ++k) {
+            const int q = q0 + k * step;
+            dst[k] = nullptr;
+            val[k] = 0.0;
+            if (q < N) {
+                const int p = ri[q % mc], r = q / mc;
+                dst[k] = p < w ? x + p + (int64_t)r * ldx : u + (p - w) + (int64_t)r * m;
+                val[k] = p < w ? -uc[q] : uc[q];
+            }
+        }
+        double cur[8];
+#pragma unroll
+        for (int k = 0; k < 8; ++k) cur[k] = dst[k] ? *dst[k] : 0.0;
+#pragma unroll
+        for (int k = 0; k < 8; ++k)
+            if (dst[k]) *dst[k] = cur[k] + val[k];
+    }
+}
+
 // forward step of one front by one CTA (xs: w x nrhs shared doubles)
 template <typename T>
 __device__ void forward_front(const SweepArgs<T>& A, int s, int member, double* xs) {
@@ -95,24 +124,7 @@ __device__ void forward_front(const SweepArgs<T>& A, int s, int member, double* 
         if (mc <= 0) continue;
         const double* uc = U + A.uoff[c];
         const int32_t* ri = A.relind + cd.ri_begin;
-        for (int q0 = tid; q0 < mc * nrhs; q0 += 4 * nt) {
-            int pp[4];
-            double vv[4];
-#pragma unroll
-            for (int k = 0; k < 4; ++k) {
-                const int q = q0 + k * nt;
-                pp[k] = q < mc * nrhs ? ri[q % mc] : -1;
-                vv[k] = q < mc * nrhs ? uc[q] : 0.0;
-            }
-#pragma unroll
-            for (int k = 0; k < 4; ++k) {
-                const int q = q0 + k * nt;
-                if (q >= mc * nrhs) continue;
-                const int r = q / mc, p = pp[k];
-                if (p < w) xs[p + r * w] -= vv[k];
-                else u[(p - w) + r * m] += vv[k];
-            }
-        }
+        pull_child(tid, nt, mc * nrhs, mc, ri, uc, w, m, xs, w, u);
         __syncthreads();
     }
     if (A.reorder) {
@@ -385,24 +397,7 @@ __device__ void warp_forward_front(const SweepArgs<T>& A, int s, double* xs, dou
         if (mc <= 0) continue;
         const double* uc = U + A.uoff[c];
         const int32_t* ri = A.relind + cd.ri_begin;
-        for (int q0 = lane; q0 < mc * nrhs; q0 += 128) {
-            int pp[4];
-            double vv[4];
-#pragma unroll
-            for (int k = 0; k < 4; ++k) {
-                const int q = q0 + 32 * k;
-                pp[k] = q < mc * nrhs ? ri[q % mc] : -1;
-                vv[k] = q < mc * nrhs ? uc[q] : 0.0;
-            }
-#pragma unroll
-            for (int k = 0; k < 4; ++k) {
-                const int q = q0 + 32 * k;
-                if (q >= mc * nrhs) continue;
-                const int r = q / mc, p = pp[k];
-                if (p < w) xs[p + r * w] -= vv[k];
-                else u[(p - w) + r * m] += vv[k];
-            }
-        }
+        pull_child(lane, 32, mc * nrhs, mc, ri, uc, w, m, xs, w, u);
         __syncwarp();
     }
     if (A.reorder) {
@@ -749,10 +744,9 @@ __global__ void __launch_bounds__(SOLVE_THREADS) persistent_solve_kernel(Persist
             double* Y = P.fw.Y;
             double* xt = P.xtmp;
             double* u = m > 0 ? P.fw.U + P.fw.uoff[s] : nullptr;
-            for (int q = threadIdx.x; q < w * nrhs; q += blockDim.x) {
-                int k = q % w, r = q / w;
-                xt[fd.c0 + k + (int64_t)r * n] = Y[fd.c0 + k + (int64_t)r * n];
-            }
+            batched_copy<8>(threadIdx.x, blockDim.x, w * nrhs,
+                            [&](int q) { return Y[fd.c0 + q % w + (int64_t)(q / w) * n]; },
+                            [&](int q, double v) { xt[fd.c0 + q % w + (int64_t)(q / w) * n] = v; });
             for (int q = threadIdx.x; q < m * nrhs; q += blockDim.x) u[q] = 0.0;
             __syncthreads();
             for (int cq = fd.ch_begin; cq < fd.ch_end; ++cq) {
@@ -762,19 +756,16 @@ __global__ void __launch_bounds__(SOLVE_THREADS) persistent_solve_kernel(Persist
                 if (mc <= 0) continue;
                 const double* uc = P.fw.U + P.fw.uoff[c];
                 const int32_t* ri = P.fw.relind + cd.ri_begin;
-                for (int q = threadIdx.x; q < mc * nrhs; q += blockDim.x) {
-                    int i2 = q % mc, r = q / mc;
-                    int p = ri[i2];
-                    if (p < w) xt[fd.c0 + p + (int64_t)r * n] -= uc[q];
-                    else u[(p - w) + r * m] += uc[q];
-                }
+                pull_child(threadIdx.x, blockDim.x, mc * nrhs, mc, ri, uc, w, m, xt + fd.c0, n, u);
                 __syncthreads();
             }
-            for (int q = threadIdx.x; q < w * nrhs; q += blockDim.x) {
-                int k = q % w, r = q / w;
-                int src = P.fw.reorder ? P.fw.piv[fd.c0 + k] - 1 : fd.c0 + k;
-                Y[fd.c0 + k + (int64_t)r * n] = xt[src + (int64_t)r * n];
-            }
+            batched_copy<8>(threadIdx.x, blockDim.x, w * nrhs,
+                            [&](int q) {
+                                const int k = q % w;
+                                const int src = P.fw.reorder ? P.fw.piv[fd.c0 + k] - 1 : fd.c0 + k;
+                                return xt[src + (int64_t)(q / w) * n];
+                            },
+                            [&](int q, double v) { Y[fd.c0 + q % w + (int64_t)(q / w) * n] = v; });
             __syncthreads();
         }
         grid_barrier(P.barrier, epoch, P.status);
