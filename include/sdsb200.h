@@ -169,6 +169,27 @@ int64_t sdsb200_get_trace(sdsb200_plan* plan, int64_t* h_out, int64_t cap);
  * Returns -1 for an unknown name. */
 double sdsb200_plan_stat(const sdsb200_plan* plan, const char* name);
 
+/* Solve without allocating (no counterpart in the reference): op(A) X = B for one active batch member,
+ * no refinement, as one cooperative kernel launch plus two small memsets. sdsb200_solve keeps its
+ * working vectors in the plan and records its launches into a CUDA graph per set of buffers, and
+ * building that graph makes the driver allocate device memory on the first call with new buffers.
+ * Callers that may not allocate once set-up is over (a framework whose pool allocator owns all device
+ * memory, a real-time loop that forbids allocation after start-up) call this entry point instead:
+ * the working vectors Y and xtmp (n * nrhs doubles each) and the update vectors (the plan's ulen
+ * doubles) live in one static device array of SDSB200_NOALLOC_SCRATCH_BYTES (32 MiB), which every
+ * GPU that loads the library holds until the process exits. Sizes beyond it are rejected with
+ * SDSB200_INVALID_VALUE: 512 + 8 * (2 * n * nrhs + ulen) bytes must fit, ulen being the plan's
+ * update-vector length (the sum over fronts of the rows below the pivot block, times max_nrhs); the
+ * error message gives the bytes needed. The first call on a device looks up the array's device address (which may also load the
+ * library's device code), so make one call during set-up, before any stream capture. The array is
+ * shared by every call on that device and keeps the last call's contents; calls that overlap on the
+ * GPU (other streams, other plans, other threads) race on it and must be serialised by the caller.
+ * solve_mode as sdsb200_opts (1, 2: A^T for "G"). status (device int32, may be NULL): set to 0, then
+ * nonzero if a bounded grid-barrier wait of the launch gave up. */
+#define SDSB200_NOALLOC_SCRATCH_BYTES (32ull << 20)
+int sdsb200_solve_noalloc(sdsb200_plan* plan, double* X, int64_t ldx, const double* B, int64_t ldb, int32_t nrhs,
+                          int32_t solve_mode, int32_t* status, void* stream);
+
 const char* sdsb200_last_error(void);
 
 #ifdef __cplusplus

@@ -865,3 +865,96 @@ double sdsb200_plan_stat(const sdsb200_plan* plan, const char* name) {
 }
 
 }  // extern "C"
+
+// ---------------------------------------------------------------------------
+// sdsb200_solve_noalloc: the persistent solve with its working vectors in a static device array, for
+// callers that may not allocate device memory after set-up. In host code the array's name is only a
+// host-side stand-in: its device address comes from cudaGetSymbolAddress, once per device.
+static __device__ __align__(256) unsigned char g_noalloc_scratch[SDSB200_NOALLOC_SCRATCH_BYTES];
+
+#include <mutex>
+
+namespace {
+
+constexpr int NOALLOC_MAX_DEVICES = 64;
+constexpr size_t NOALLOC_HEADER = 512;   // barrier counter at 0, fallback status word at 256
+std::mutex g_noalloc_mu;
+void* g_noalloc_base[NOALLOC_MAX_DEVICES] = {};
+
+// device address of the static array on the current device (looked up on the first call there)
+int noalloc_base(void** out) {
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return cuda_fail(e, "sdsb200_solve_noalloc: cudaGetDevice");
+    if (dev < 0 || dev >= NOALLOC_MAX_DEVICES) return fail(SDSB200_NOT_SUPPORTED, "sdsb200_solve_noalloc: device index above 63");
+    std::lock_guard<std::mutex> lock(g_noalloc_mu);
+    if (!g_noalloc_base[dev]) {
+        void* p = nullptr;
+        e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+        if (e != cudaSuccess) return cuda_fail(e, "sdsb200_solve_noalloc: cudaGetSymbolAddress of the static scratch");
+        g_noalloc_base[dev] = p;
+    }
+    *out = g_noalloc_base[dev];
+    return SDSB200_OK;
+}
+
+// Points the plan's solve working vectors at the static array for the duration of one launch and
+// puts the plan's own pointers back afterwards (the launch code reads them when it builds its
+// arguments, on the host, before this returns).
+struct ScratchSwap {
+    Plan* P;
+    double* Y; double* U; double* xtmp; unsigned int* barrier; int32_t* status;
+    ScratchSwap(Plan* p, double* y, double* u, double* xt, unsigned int* bar, int32_t* st)
+        : P(p), Y(p->d_Y), U(p->d_U), xtmp(p->d_xtmp), barrier(p->d_barrier), status(p->d_solve_status) {
+        P->d_Y = y; P->d_U = u; P->d_xtmp = xt; P->d_barrier = bar; P->d_solve_status = st;
+    }
+    ~ScratchSwap() { P->d_Y = Y; P->d_U = U; P->d_xtmp = xtmp; P->d_barrier = barrier; P->d_solve_status = status; }
+};
+
+}  // namespace
+
+extern "C" {
+
+int sdsb200_solve_noalloc(sdsb200_plan* plan, double* X, int64_t ldx, const double* B, int64_t ldb, int32_t nrhs,
+                          int32_t solve_mode, int32_t* status, void* stream) {
+    Plan* P = reinterpret_cast<Plan*>(plan);
+    if (!P) return fail(SDSB200_INVALID_VALUE, "plan is NULL");
+    if (!P->factored) return fail(SDSB200_PHASE_ORDER, "solve before a successful factorization");
+    if (nrhs < 1 || nrhs > P->max_nrhs) return fail(SDSB200_INVALID_VALUE, "nrhs outside 1:max_nrhs of the plan");
+    if (ldx < P->n || ldb < P->n) return fail(SDSB200_INVALID_VALUE, "leading dimension smaller than n");
+    if (!X || !B) return fail(SDSB200_INVALID_VALUE, "X or B is NULL");
+    if (solve_mode < 0 || solve_mode > 2) return fail(SDSB200_INVALID_VALUE, "solve_mode must be 0, 1 or 2");
+    if (!(P->nact == 1 && P->all_members))
+        return fail(SDSB200_NOT_SUPPORTED, "sdsb200_solve_noalloc solves a plan with exactly one batch member");
+    int maxw = 1;
+    for (int w : P->level_maxw) maxw = std::max(maxw, w);
+    if ((size_t)maxw * nrhs * sizeof(double) > 200 * 1024)
+        return fail(SDSB200_NOT_SUPPORTED, "front too wide for this many right-hand sides in one solve");
+    const size_t vec = (size_t)P->n * (size_t)nrhs;
+    const size_t need = NOALLOC_HEADER + sizeof(double) * (2 * vec + (size_t)P->ulen);
+    if (need > SDSB200_NOALLOC_SCRATCH_BYTES)
+        return fail(SDSB200_INVALID_VALUE,
+                    "sdsb200_solve_noalloc: the working vectors need " + std::to_string(need) +
+                        " bytes (512 + 8 * (2 * n * nrhs + ulen)), above the static scratch of " +
+                        std::to_string((unsigned long long)SDSB200_NOALLOC_SCRATCH_BYTES) + " bytes");
+    void* base = nullptr;
+    int rc = noalloc_base(&base);
+    if (rc) return rc;
+    unsigned char* b = static_cast<unsigned char*>(base);
+    unsigned int* bar = reinterpret_cast<unsigned int*>(b);
+    int32_t* st_word = status ? status : reinterpret_cast<int32_t*>(b + 256);
+    double* Y = reinterpret_cast<double*>(b + NOALLOC_HEADER);
+    double* xt = Y + vec;
+    double* U = xt + vec;
+    cudaStream_t st = (cudaStream_t)stream;
+    // only the status word and the barrier counter must start at zero (the launch zeroes the barrier);
+    // Y, xtmp and the update vectors are written before they are read in every solve
+    CK(cudaMemsetAsync(st_word, 0, sizeof(int32_t), st), "sdsb200_solve_noalloc: status reset");
+    const bool transpose = P->structure == STRUCT_G && solve_mode != 0;
+    ScratchSwap swap(P, Y, U, xt, bar, st_word);
+    P->launches_done = 0;
+    return P->elsize == 8 ? run_persistent<double>(P, nrhs, transpose, B, ldb, X, ldx, 0, st)
+                          : run_persistent<float>(P, nrhs, transpose, B, ldb, X, ldx, 0, st);
+}
+
+}  // extern "C"
