@@ -463,7 +463,11 @@ int run_persistent(Plan* P, int nrhs, bool transpose, const double* in, int64_t 
     CK(cudaMemsetAsync(P->d_barrier, 0, sizeof(unsigned int), st), "barrier reset");
     prof_begin(P, st);
     cudaError_t e = launch_persistent_solve<T>(a, grid, smem, st);
-    prof_end(P, st, PK_FWD, 0.0, 0.0);
+    // algorithmic work: every stored panel entry read once per sweep (2 flops per entry and rhs each
+    // way), Y and the right-hand side read, the solution written
+    double ent = 0.0;
+    for (double v : P->level_panel_entries) ent += v;
+    prof_end(P, st, PK_FWD, 4.0 * ent * nrhs, 2.0 * sizeof(T) * ent + 24.0 * P->n * nrhs);
     return e == cudaSuccess ? SDSB200_OK : cuda_fail(e, "persistent solve");
 }
 
