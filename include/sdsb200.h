@@ -169,6 +169,22 @@ int64_t sdsb200_get_trace(sdsb200_plan* plan, int64_t* h_out, int64_t cap);
  * Returns -1 for an unknown name. */
 double sdsb200_plan_stat(const sdsb200_plan* plan, const char* name);
 
+/* Adjoint of x = op(A)^{-1} B with respect to the values (no counterpart in the reference, which has no
+ * automatic differentiation): the sampled outer product over the CSR pattern,
+ *   out[k] = alpha * sum_r U[i, r] V[j, r]                     structure "G" (0), every entry k = (i, j);
+ *   out[k] = alpha * sum_r (U[i, r] V[j, r] + U[j, r] V[i, r])   "S" (1) / "SPD" (3), i != j, kept entry;
+ *   out[k] = alpha * sum_r U[i, r] V[i, r]                     "S" / "SPD", kept diagonal entry;
+ *   out[k] = 0                                                 "S" / "SPD", an entry the view drops.
+ * Kept entries are those the factorization reads: the lower triangle for view 'F' and 'L', the upper
+ * for 'U'. With U = A^{-T} X_bar (a transposed solve, solve_mode 1) and V = X, alpha = -1 gives
+ * dLoss/d nzval. rowptr (n + 1) and colval (nnz) are DEVICE arrays of int32 (index_width 4) or int64
+ * (8) with index_base 0 or 1; U, V (ld >= n, ncols columns) and out (nnz) are device arrays, nbatch
+ * members one after the other (strides ldu * ncols, ldv * ncols, nnz). */
+int sdsb200_sampled_outer(int64_t n, int64_t nnz, const void* rowptr, const void* colval, int32_t index_width,
+                          int32_t index_base, int32_t structure, int32_t view, const double* U, int64_t ldu,
+                          const double* V, int64_t ldv, int32_t ncols, int32_t nbatch, double alpha, double* out,
+                          void* stream);
+
 /* Solve without allocating (no counterpart in the reference): op(A) X = B for one active batch member,
  * no refinement, as one cooperative kernel launch plus two small memsets. sdsb200_solve keeps its
  * working vectors in the plan and records its launches into a CUDA graph per set of buffers, and

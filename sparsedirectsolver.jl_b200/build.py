@@ -25,6 +25,7 @@ NUMERIC_SOURCES = [
     "numeric/factor_kernels.cu",
     "numeric/dense_kernels.cu",
     "numeric/solve_kernels.cu",
+    "numeric/adjoint_kernels.cu",
     "numeric/capi.cu",
 ]
 

@@ -870,6 +870,33 @@ double sdsb200_plan_stat(const sdsb200_plan* plan, const char* name) {
 
 }  // extern "C"
 
+extern "C" int sdsb200_sampled_outer(int64_t n, int64_t nnz, const void* rowptr, const void* colval,
+                                     int32_t index_width, int32_t index_base, int32_t structure, int32_t view,
+                                     const double* U, int64_t ldu, const double* V, int64_t ldv, int32_t ncols,
+                                     int32_t nbatch, double alpha, double* out, void* stream) {
+    if (n < 0 || nnz < 0 || ncols < 1 || nbatch < 1) return fail(SDSB200_INVALID_VALUE, "sampled_outer: bad sizes");
+    if (index_width != 4 && index_width != 8) return fail(SDSB200_INVALID_VALUE, "index_width must be 4 or 8");
+    if (index_base != 0 && index_base != 1) return fail(SDSB200_INVALID_VALUE, "index_base must be 0 or 1");
+    if (structure != STRUCT_G && structure != STRUCT_S && structure != STRUCT_SPD)
+        return fail(SDSB200_INVALID_VALUE, "structure must be 0 (G), 1 (S) or 3 (SPD)");
+    if (view != 'F' && view != 'L' && view != 'U') return fail(SDSB200_INVALID_VALUE, "view must be 'F', 'L' or 'U'");
+    if (ldu < n || ldv < n) return fail(SDSB200_INVALID_VALUE, "leading dimension smaller than n");
+    if (n > 0 && (!rowptr || !U || !V || (nnz > 0 && (!colval || !out))))
+        return fail(SDSB200_INVALID_VALUE, "NULL array");
+    cudaStream_t st = (cudaStream_t)stream;
+    cudaError_t e;
+    if (index_width == 4) {
+        OuterArgs<int32_t> a{static_cast<const int32_t*>(rowptr), static_cast<const int32_t*>(colval), index_base, n,
+                             nnz, structure, view, U, V, ldu, ldv, ncols, alpha, out};
+        e = launch_sampled_outer(a, nbatch, st);
+    } else {
+        OuterArgs<int64_t> a{static_cast<const int64_t*>(rowptr), static_cast<const int64_t*>(colval), index_base, n,
+                             nnz, structure, view, U, V, ldu, ldv, ncols, alpha, out};
+        e = launch_sampled_outer(a, nbatch, st);
+    }
+    return e == cudaSuccess ? SDSB200_OK : cuda_fail(e, "sampled outer product");
+}
+
 // ---------------------------------------------------------------------------
 // sdsb200_solve_noalloc: the persistent solve with its working vectors in a static device array, for
 // callers that may not allocate device memory after set-up. In host code the array's name is only a

@@ -183,6 +183,24 @@ cudaError_t launch_large_pivot(int structure, const LargePivotArgs<T>& a, int nm
 template <typename T>
 cudaError_t launch_scale_ld_front(int structure, const ScaleArgs<T>& a, int maxw, int nmembers, cudaStream_t st);
 
+// sampled outer product over a CSR pattern (the adjoint of a solve with respect to the values)
+template <typename I>
+struct OuterArgs {
+    const I* rowptr;           // n + 1, base `base`
+    const I* colval;           // nnz
+    int64_t base, n, nnz;
+    int32_t structure;         // STRUCT_G, STRUCT_S or STRUCT_SPD
+    int32_t view;              // 'F', 'L' or 'U' (symmetric structures keep one triangle)
+    const double* U;           // n x ncols per member (ld ldu, member stride ldu * ncols)
+    const double* V;
+    int64_t ldu, ldv;
+    int32_t ncols;
+    double alpha;
+    double* out;               // nnz per member
+};
+template <typename I>
+cudaError_t launch_sampled_outer(const OuterArgs<I>& a, int nmembers, cudaStream_t st);
+
 constexpr int PANEL_ROWS = 128;  // rows of the trsm tile of a Cholesky panel CTA
 constexpr int GEMM_BM = 64, GEMM_BN = 64;
 
