@@ -90,8 +90,15 @@ typedef struct sdsb200_plan_options {
     int32_t nbatch;           /* uniform batch members (ubatch_size); 1 for a single matrix */
     int32_t precision;        /* SDSB200_PRECISION_* */
     int32_t max_nrhs;         /* largest nrhs of a solve (workspace) */
-    int32_t reserved;
+    int32_t tuning;           /* front tile shapes, 0 = defaults; SDSB200_TUNING(fsmall, wide) */
 } sdsb200_plan_options;
+
+/* Plan tuning (the shapes an autotuner chooses; no counterpart in the reference):
+ * fsmall = the largest front order handled by the shared-memory small-front kernel (one of 32, 64,
+ * 96, 128, 160, and 224 for FP32; 0 = the largest class); wide = the front width from which the
+ * solve treats a front as wide, splitting it into 64-column block steps over the grid (16..1024,
+ * 0 = 96; fronts with (f - w) * w >= 32768 are always wide). */
+#define SDSB200_TUNING(fsmall, wide) ((int32_t)(fsmall) | ((int32_t)(wide) << 16))
 
 /* The Options fields the numeric and solve phases read (src/options.jl:155-223). */
 typedef struct sdsb200_opts {

@@ -1,0 +1,73 @@
+"""Autotuner of the plan's front tile shapes (``tuning``): no counterpart in the reference.
+
+Two shapes decide how the fronts of a plan map onto the kernels:
+* ``fsmall``: the largest front order factored in shared memory by the small-front kernel. Larger
+  fronts take the column-owner assembly, diagonal-block and DMMA GEMM path.
+* ``wide``: the front width from which the solve splits a front into 64-column block steps over
+  the whole grid instead of one CTA or warp.
+
+The autotuner times factorization + solve for each candidate on the solver's own matrix and
+right-hand side (CUDA events, after a warm-up), keeps the fastest, and leaves the solver planned
+and factored with it. Results are cached in-process per (n, nnz, structure, precision, nbatch).
+"""
+from __future__ import annotations
+
+from .capi import tuning as make_tuning
+
+CANDIDATES = (
+    (0, 0), (128, 0), (96, 0), (64, 0),
+    (0, 64), (0, 128), (128, 64), (96, 128),
+)
+
+_cache: dict = {}
+
+
+def _key(solver):
+    return (solver.n, solver.nnz, solver.structure, solver.params["factor_precision"], solver.nbatch)
+
+
+def autotune(solver, B, candidates=CANDIDATES, reps=3, use_cache=True):
+    """Pick the tuning with the smallest factorization + solve time. Returns {tuning: ms}."""
+    import torch
+
+    if solver.symbolic is None:
+        solver.execute("analysis")
+    key = _key(solver)
+    if use_cache and key in _cache:
+        best, times = _cache[key]
+        solver.setparam("tuning", best)
+        solver.replan()
+        solver.execute("factorization")
+        return dict(times)
+    times = {}
+    for fs, wd in candidates:
+        t = make_tuning(fs, wd)
+        solver.setparam("tuning", t)
+        try:
+            solver.replan()
+        except Exception:            # a shape the plan rejects (for example an FP64 class of 224)
+            continue
+        solver.execute("factorization")
+        solver.execute("solve", None, B)
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(reps):
+            solver.execute("factorization")
+            solver.execute("solve", None, B)
+        e1.record()
+        torch.cuda.synchronize()
+        times[t] = e0.elapsed_time(e1) / reps
+    best = min(times, key=times.get)
+    _cache[key] = (best, dict(times))
+    solver.setparam("tuning", best)
+    solver.replan()
+    solver.execute("factorization")
+    return times
+
+
+def describe(t):
+    return {"fsmall": int(t) & 0xFFFF, "wide": (int(t) >> 16) & 0xFFFF}
+
+
+__all__ = ["autotune", "describe", "CANDIDATES"]

@@ -49,7 +49,7 @@ _DEFAULTS = {
     "pivot_epsilon": None, "pivot_epsilon_alg": "default", "deterministic_mode": 0, "ubatch_size": 0,
     "ubatch_index": -1, "use_superpanels": 1, "ir_mode": "plain", "factor_precision": None,
     "amalgamation": (32, 0.25, 8), "pivot_pairs": "default", "pivot_pair_tolerance": 1e-6, "user_perm": None,
-    "pivot_sign": None, "user_host_interrupt": None, "max_nrhs": 8,
+    "pivot_sign": None, "user_host_interrupt": None, "max_nrhs": 8, "tuning": 0,
 }
 
 
@@ -151,6 +151,14 @@ class DirectSolver:
         if name == "ubatch_index" and self._plan_exists():
             self._apply_members(int(value))
         self.params[name] = value
+
+    def replan(self):
+        """Build the device plan again from the current analysis (after a change of a plan-level
+        parameter: ``tuning``, ``max_nrhs``, ``factor_precision``). The factorization must be rerun."""
+        if self._stage < 1:
+            raise FactorizationError("replan before analysis")
+        self._create_plan()
+        self._stage = 1
 
     def _plan_exists(self):
         return getattr(self, "_plan", None) is not None
@@ -263,7 +271,8 @@ class DirectSolver:
             setattr(sym, nm, a.ctypes.data)
         sym.full_nnz = int(S.full_colval.size)
         sym.full_nsrc = int(S.full_src.size)
-        po = capi.PlanOptions(nbatch=self.nbatch, precision=self._precision(), max_nrhs=int(self.params["max_nrhs"]))
+        po = capi.PlanOptions(nbatch=self.nbatch, precision=self._precision(), max_nrhs=int(self.params["max_nrhs"]),
+                              tuning=int(self.params["tuning"]))
         plan = C.c_void_p()
         stream = self._torch.cuda.current_stream(self.device).cuda_stream
         _check(lib.sdsb200_plan_create(C.byref(plan), C.byref(sym), C.byref(po), C.c_void_p(stream)), lib)
