@@ -261,7 +261,13 @@ int run_factor(Plan* P, const double* nzval, double eps, double u, int pivot, in
                 a.psign = P->d_psign; a.perm = P->d_perm0;
                 a.factor_len = P->factor_len; a.n = P->n; a.ns = (int32_t)P->ns;
                 a.pivot = pivot; a.lu_pivot = lu_pivot; a.u = u; a.eps = eps;
-                e = launch_large_pivot<T>(P->structure, a, nm, st);
+                if (L.coop >= 0 && nm == 1 && !members) {
+                    e = cudaMemsetAsync(P->d_coop_bar, 0, sizeof(unsigned int) * L.count, st);
+                    CoopGroups g{P->d_coop_first + L.coop, P->d_coop_bar, P->d_solve_status};
+                    if (e == cudaSuccess) e = launch_large_pivot_coop<T>(P->structure, a, g, L.coop_grid, st);
+                } else {
+                    e = launch_large_pivot<T>(P->structure, a, nm, st);
+                }
                 break;
             }
             case L_SCALE: {

@@ -568,6 +568,270 @@ cudaError_t launch_large_pivot(int structure, const LargePivotArgs<T>& a, int nm
 template cudaError_t launch_large_pivot<double>(int, const LargePivotArgs<double>&, int, cudaStream_t);
 template cudaError_t launch_large_pivot<float>(int, const LargePivotArgs<float>&, int, cudaStream_t);
 
+// ---------------------------------------------------------------------------
+// Cooperative variant of large_pivot_kernel for wide fronts of a single-member plan: each listed
+// front gets a group of co-resident CTAs (cta_first: prefix of the group sizes), and every pivot step
+// of ldlt_front_steps / lu_front_steps runs as phases separated by group barriers:
+// decision (one warp) | column / row interchanges | multipliers | rank-1 or rank-2 update.
+// Each entry receives the same floating-point operations in the same order as in the one-CTA
+// kernel, so pivots, D and the panels are identical; only the update is spread over the group.
+// A group barrier waits at most ~2 s, then records a nonzero status and goes on (no hang).
+__device__ __forceinline__ void group_barrier(unsigned int* bar, unsigned int& epoch, int gs, int32_t* status) {
+    __syncthreads();
+    epoch += gs;
+    if (threadIdx.x == 0) {
+        __threadfence();
+        atomicAdd(bar, 1u);
+        unsigned int v;
+        long spins = 0;
+        while (true) {
+            asm volatile("ld.acquire.gpu.u32 %0, [%1];" : "=r"(v) : "l"(bar));
+            if ((int)(v - epoch) >= 0) break;
+            if (++spins > (1L << 26)) {
+                atomicExch(status, 1);
+                break;
+            }
+            __nanosleep(32);
+        }
+        __threadfence();
+    }
+    __syncthreads();
+}
+
+constexpr int COOP_ROWS = 256;   // rows of one update item (a column chunk, one warp)
+
+template <typename T, int STRUCT>
+__global__ void __launch_bounds__(COOP_THREADS) large_pivot_coop_kernel(LargePivotArgs<T> A, CoopGroups G) {
+    int lo = 0, hi = A.count - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (G.cta_first[mid] <= (int)blockIdx.x) lo = mid;
+        else hi = mid - 1;
+    }
+    const int fi = lo, rank = (int)blockIdx.x - G.cta_first[fi], gs = G.cta_first[fi + 1] - G.cta_first[fi];
+    const int s = A.list[fi];
+    const DFront fd = A.fronts[s];
+    const int f = fd.f, w = fd.w;
+    constexpr bool GEN = STRUCT == STRUCT_G;
+    T* P = A.factor + fd.panel;
+    T* U = GEN ? A.ufactor + fd.panel : nullptr;
+    double* scr = A.scratch + A.scr_off[fi];
+    FrontScratch sc;
+    sc.lvec = scr;
+    sc.dd = scr + 2 * f;
+    sc.ee = sc.dd + w;
+    sc.lp = reinterpret_cast<int*>(sc.ee + w);
+    sc.ctl = sc.lp + w;
+    sc.kd = reinterpret_cast<signed char*>(sc.ctl + 16);
+    unsigned int* bar = G.bar + fi;
+    unsigned int epoch = 0;
+    const int tid = threadIdx.x, nt = blockDim.x, lane = tid & 31, warp = tid >> 5;
+    const int gt = rank * nt + tid, GT = gs * nt, gw = gt >> 5, GW = GT >> 5;
+    const bool lead = rank == 0 && tid == 0;
+    GlobalStore<T, GEN> F{P, U, f, w};
+    if (STRUCT == STRUCT_S) {
+        for (int q = gt; q < w * w; q += GT) {
+            const int i = q % w, j = q / w;
+            if (i > j) P[j + (int64_t)i * f] = P[i + (int64_t)j * f];
+        }
+    }
+    for (int q = gt; q < w; q += GT) sc.lp[q] = q;
+    group_barrier(bar, epoch, gs, G.status);
+    int64_t st[NSTAT] = {0, 0, 0, 0, 0, 0};
+    if (STRUCT == STRUCT_S) {
+        int k = 0;
+        while (k < w) {
+            if (rank == 0 && warp == 0) {
+                int c, r;
+                choose_pivot_w(F, k, w, A.pivot, A.u, A.eps, lane, c, r);
+                if (lane == 0) { sc.ctl[0] = c; sc.ctl[1] = r; }
+            }
+            group_barrier(bar, epoch, gs, G.status);
+            const int c = sc.ctl[0], r = sc.ctl[1];
+            const int p = r < 0 ? k : k + 1, qsw = r < 0 ? c : r;
+            if (p != qsw) {
+                for (int i = gt; i < f; i += GT) {
+                    T t = F.at(i, p); F.at(i, p) = F.at(i, qsw); F.at(i, qsw) = t;
+                }
+                group_barrier(bar, epoch, gs, G.status);
+                for (int j = gt; j < w; j += GT) {
+                    T t = F.at(p, j); F.at(p, j) = F.at(qsw, j); F.at(qsw, j) = t;
+                }
+                if (lead) { int t = sc.lp[p]; sc.lp[p] = sc.lp[qsw]; sc.lp[qsw] = t; }
+                group_barrier(bar, epoch, gs, G.status);
+            }
+            const int nch = (f - k - 1 + COOP_ROWS - 1) / COOP_ROWS;
+            if (r < 0) {
+                double dk = F.get(k, k);
+                signed char kk = KIND_1X1;
+                if (!(fabs(dk) >= A.eps) || dk == 0.0) {
+                    if (dk == 0.0) st[ST_NZERO]++;
+                    int req = A.psign ? (int)A.psign[A.perm[fd.c0 + sc.lp[k]]] : 0;
+                    dk = perturb_sign_of(dk, req) * A.eps;
+                    kk = KIND_PERTURBED;
+                    st[ST_NPERT]++;
+                    if (dk == 0.0 && st[ST_INFO] == 0) st[ST_INFO] = sc.lp[k] + 1;
+                }
+                if (dk > 0) st[ST_NPOS]++;
+                else if (dk < 0) st[ST_NNEG]++;
+                for (int i = k + 1 + gt; i < f; i += GT) sc.lvec[i] = F.get(i, k) / dk;
+                group_barrier(bar, epoch, gs, G.status);
+                if (lead) { F.at(k, k) = T(dk); sc.dd[k] = dk; sc.ee[k] = 0.0; sc.kd[k] = kk; }
+                const int nj = w - k - 1;
+                for (int item = gw; item < nj * nch; item += GW) {
+                    const int j = k + 1 + item % nj, ch = item / nj;
+                    const T fkj = F.at(k, j);
+                    const int i1 = min(f, k + 1 + (ch + 1) * COOP_ROWS);
+                    for (int i = k + 1 + ch * COOP_ROWS + lane; i < i1; i += 32) F.at(i, j) -= T(sc.lvec[i]) * fkj;
+                }
+                for (int i = k + 1 + gt; i < f; i += GT) F.at(i, k) = T(sc.lvec[i]);
+                group_barrier(bar, epoch, gs, G.status);
+                k += 1;
+            } else {
+                const double a = F.get(k, k), b = F.get(k + 1, k), c2 = F.get(k + 1, k + 1);
+                const double det = a * c2 - b * b;
+                const double e11 = c2 / det, e12 = -b / det, e21 = -b / det, e22 = a / det;
+                st[ST_N2X2]++;
+                if (det < 0) { st[ST_NPOS]++; st[ST_NNEG]++; }
+                else if (a > 0) st[ST_NPOS] += 2;
+                else st[ST_NNEG] += 2;
+                for (int i = k + 2 + gt; i < f; i += GT) {
+                    const double x1 = F.get(i, k), x2 = F.get(i, k + 1);
+                    sc.lvec[i] = x1 * e11 + x2 * e21;
+                    sc.lvec[f + i] = x1 * e12 + x2 * e22;
+                }
+                group_barrier(bar, epoch, gs, G.status);
+                if (lead) {
+                    F.at(k, k + 1) = T(b);
+                    sc.dd[k] = a; sc.dd[k + 1] = c2; sc.ee[k] = b; sc.ee[k + 1] = 0.0;
+                    sc.kd[k] = KIND_2X2_FIRST; sc.kd[k + 1] = KIND_2X2_SECOND;
+                }
+                const int nj = w - k - 2;
+                const int nch2 = (f - k - 2 + COOP_ROWS - 1) / COOP_ROWS;
+                for (int item = gw; nj > 0 && item < nj * nch2; item += GW) {
+                    const int j = k + 2 + item % nj, ch = item / nj;
+                    const T fkj = F.at(k, j), fk1j = F.at(k + 1, j);
+                    const int i1 = min(f, k + 2 + (ch + 1) * COOP_ROWS);
+                    for (int i = k + 2 + ch * COOP_ROWS + lane; i < i1; i += 32)
+                        F.at(i, j) -= T(sc.lvec[i]) * fkj + T(sc.lvec[f + i]) * fk1j;
+                }
+                for (int i = k + 2 + gt; i < f; i += GT) {
+                    F.at(i, k) = T(sc.lvec[i]);
+                    F.at(i, k + 1) = T(sc.lvec[f + i]);
+                }
+                if (lead) F.at(k + 1, k) = T(0);
+                group_barrier(bar, epoch, gs, G.status);
+                k += 2;
+            }
+        }
+    } else {
+        const bool pivoting = A.lu_pivot != 0;
+        for (int k = 0; k < w; ++k) {
+            if (rank == 0 && warp == 0) {
+                int r = pivoting ? lu_choose_row_w(F, k, w, A.u, lane) : k;
+                if (lane == 0) sc.ctl[0] = r;
+            }
+            group_barrier(bar, epoch, gs, G.status);
+            const int r = sc.ctl[0];
+            if (r != k) {
+                for (int j = gt; j < f; j += GT) {
+                    T t = F.at(k, j); F.at(k, j) = F.at(r, j); F.at(r, j) = t;
+                }
+                if (lead) { int t = sc.lp[k]; sc.lp[k] = sc.lp[r]; sc.lp[r] = t; }
+                group_barrier(bar, epoch, gs, G.status);
+            }
+            double dk = F.get(k, k);
+            signed char kk = KIND_1X1;
+            if (!(fabs(dk) >= A.eps) || dk == 0.0) {
+                if (dk == 0.0) st[ST_NZERO]++;
+                dk = perturb_sign_of(dk, 0) * A.eps;
+                kk = KIND_PERTURBED;
+                st[ST_NPERT]++;
+                if (dk == 0.0 && st[ST_INFO] == 0) st[ST_INFO] = k + 1;
+            }
+            group_barrier(bar, epoch, gs, G.status);   // every CTA has read F[k, k]
+            if (lead) { F.at(k, k) = T(dk); sc.dd[k] = dk; sc.kd[k] = kk; }
+            const T tdk = T(dk);
+            const int nj = f - k - 1;
+            const int nch = (f - k - 1 + COOP_ROWS - 1) / COOP_ROWS;
+            for (int item = gw; item < nj * nch; item += GW) {
+                const int j = k + 1 + item % nj, ch = item / nj;
+                const int iend = j < w ? f : w;
+                const int i0 = k + 1 + ch * COOP_ROWS;
+                if (i0 >= iend) continue;
+                const T fkj = F.at(k, j);
+                const int i1 = min(iend, i0 + COOP_ROWS);
+                for (int i = i0 + lane; i < i1; i += 32) F.at(i, j) -= F.at(i, k) / tdk * fkj;
+            }
+            group_barrier(bar, epoch, gs, G.status);
+            for (int i = k + 1 + gt; i < f; i += GT) F.at(i, k) /= tdk;
+            for (int j = k + 1 + gt; j < f; j += GT) F.at(k, j) /= tdk;
+            group_barrier(bar, epoch, gs, G.status);
+        }
+    }
+    for (int q = gt; q < w * w; q += GT) {
+        const int i = q % w, j = q / w;
+        if (i == j) {
+            P[i + (int64_t)j * f] = T(1);
+            if (GEN) U[i + (int64_t)j * f] = T(1);
+        } else if (i < j && !GEN) {
+            P[i + (int64_t)j * f] = T(0);
+        }
+    }
+    const int64_t n = A.n;
+    for (int q = gt; q < w; q += GT) {
+        const int64_t g = fd.c0 + q;
+        A.piv[g] = fd.c0 + sc.lp[q] + 1;
+        A.kind[g] = sc.kd[q];
+        A.d[g] = sc.dd[q];
+        A.d[n + g] = STRUCT == STRUCT_S ? sc.ee[q] : 0.0;
+    }
+    if (lead) {
+        int64_t* S = A.stats + (int64_t)s * NSTAT;
+        for (int q = 0; q < NSTAT; ++q) S[q] = st[q];
+        A.finfo[s] = (int32_t)st[ST_INFO];
+    }
+}
+
+template <typename T>
+cudaError_t launch_large_pivot_coop(int structure, const LargePivotArgs<T>& a, const CoopGroups& g, int grid,
+                                    cudaStream_t st) {
+    if (a.count == 0 || grid == 0) return cudaSuccess;
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(grid);
+    cfg.blockDim = dim3(COOP_THREADS);
+    cfg.dynamicSmemBytes = 0;
+    cfg.stream = st;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeCooperative;
+    attr[0].val.cooperative = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    if (structure == STRUCT_S) return cudaLaunchKernelEx(&cfg, large_pivot_coop_kernel<T, STRUCT_S>, a, g);
+    return cudaLaunchKernelEx(&cfg, large_pivot_coop_kernel<T, STRUCT_G>, a, g);
+}
+
+template <typename T>
+int large_pivot_coop_capacity(int structure) {
+    int dev = 0, sms = 0, per = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    cudaError_t e = structure == STRUCT_S
+                        ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, large_pivot_coop_kernel<T, STRUCT_S>,
+                                                                        COOP_THREADS, 0)
+                        : cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, large_pivot_coop_kernel<T, STRUCT_G>,
+                                                                        COOP_THREADS, 0);
+    if (e != cudaSuccess) return 0;
+    return sms * per;
+}
+
+template cudaError_t launch_large_pivot_coop<double>(int, const LargePivotArgs<double>&, const CoopGroups&, int,
+                                                     cudaStream_t);
+template cudaError_t launch_large_pivot_coop<float>(int, const LargePivotArgs<float>&, const CoopGroups&, int,
+                                                    cudaStream_t);
+template int large_pivot_coop_capacity<double>(int);
+template int large_pivot_coop_capacity<float>(int);
+
 // W = L21 D (1x1 and 2x2 blocks of D), rows w..f-1 of the panel, into work (m x w, ld m)
 template <typename T, int STRUCT>
 __global__ void scale_ld_kernel(ScaleArgs<T> A) {

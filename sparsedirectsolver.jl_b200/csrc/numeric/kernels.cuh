@@ -183,6 +183,19 @@ cudaError_t launch_large_pivot(int structure, const LargePivotArgs<T>& a, int nm
 template <typename T>
 cudaError_t launch_scale_ld_front(int structure, const ScaleArgs<T>& a, int maxw, int nmembers, cudaStream_t st);
 
+// groups of co-resident CTAs for the cooperative large-front pivot kernel (single-member plans)
+struct CoopGroups {
+    const int32_t* cta_first;  // per listed front: first CTA of its group (count + 1 entries)
+    unsigned int* bar;         // per listed front: group barrier counter, zeroed before the launch
+    int32_t* status;           // nonzero: a group barrier wait gave up
+};
+constexpr int COOP_THREADS = 256;
+template <typename T>
+cudaError_t launch_large_pivot_coop(int structure, const LargePivotArgs<T>& a, const CoopGroups& g, int grid,
+                                    cudaStream_t st);
+template <typename T>
+int large_pivot_coop_capacity(int structure);   // co-resident CTAs of the cooperative kernel on this device
+
 // sampled outer product over a CSR pattern (the adjoint of a solve with respect to the values)
 template <typename I>
 struct OuterArgs {

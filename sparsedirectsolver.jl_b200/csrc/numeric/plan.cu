@@ -11,9 +11,12 @@
 #include <string.h>
 
 #include <algorithm>
+#include <functional>
 #include <map>
+#include <queue>
 #include <stdexcept>
 #include <string>
+#include <tuple>
 #include <vector>
 
 #include "plan.h"
@@ -74,24 +77,64 @@ int32_t to_i32(int64_t v, const char* what) {
 }
 
 // first-fit placement of intervals [start, end] of `len` elements on one arena
+// Contribution-block arena: blocks live over an interval of levels [start, end] and are placed in
+// order of start. Released space is kept as free segments (by offset, coalesced with neighbours, and
+// by length for a best-fit search), so a placement costs O(log blocks) even with hundreds of
+// thousands of blocks alive at once (uneven batches).
 struct Arena {
-    struct Block { int64_t off, len; int end; };
-    std::vector<Block> live;
+    std::map<int64_t, int64_t> by_off;             // free segment offset -> length
+    std::multimap<int64_t, int64_t> by_len;        // free segment length -> offset
+    std::priority_queue<std::tuple<int, int64_t, int64_t>, std::vector<std::tuple<int, int64_t, int64_t>>,
+                        std::greater<std::tuple<int, int64_t, int64_t>>> live;   // (end, offset, length)
     int64_t top = 0;
-    int64_t place(int64_t len, int start, int end) {
-        // release the blocks whose lifetime ended before `start`
-        live.erase(std::remove_if(live.begin(), live.end(), [&](const Block& b) { return b.end < start; }), live.end());
-        std::sort(live.begin(), live.end(), [](const Block& a, const Block& b) { return a.off < b.off; });
-        int64_t cur = 0;
-        for (const Block& b : live) {
-            int64_t aligned = (cur + 31) & ~int64_t(31);
-            if (b.off >= aligned + len) break;
-            cur = std::max(cur, b.off + b.len);
+    void erase_len(int64_t len, int64_t off) {
+        auto r = by_len.equal_range(len);
+        for (auto it = r.first; it != r.second; ++it)
+            if (it->second == off) { by_len.erase(it); return; }
+    }
+    void add_free(int64_t off, int64_t len) {
+        auto next = by_off.lower_bound(off);
+        if (next != by_off.begin()) {
+            auto prev = std::prev(next);
+            if (prev->first + prev->second == off) {
+                off = prev->first;
+                len += prev->second;
+                erase_len(prev->second, prev->first);
+                by_off.erase(prev);
+            }
         }
-        cur = (cur + 31) & ~int64_t(31);
-        live.push_back({cur, len, end});
-        top = std::max(top, cur + len);
-        return cur;
+        next = by_off.lower_bound(off);
+        if (next != by_off.end() && off + len == next->first) {
+            len += next->second;
+            erase_len(next->second, next->first);
+            by_off.erase(next);
+        }
+        by_off[off] = len;
+        by_len.emplace(len, off);
+    }
+    int64_t place(int64_t len, int start, int end) {
+        while (!live.empty() && std::get<0>(live.top()) < start) {
+            add_free(std::get<1>(live.top()), std::get<2>(live.top()));
+            live.pop();
+        }
+        int64_t at = -1;
+        for (auto it = by_len.lower_bound(len); it != by_len.end(); ++it) {
+            const int64_t off = it->second, seg = it->first;
+            const int64_t a = (off + 31) & ~int64_t(31);
+            if (a + len > off + seg) continue;
+            by_len.erase(it);
+            by_off.erase(off);
+            if (a > off) add_free(off, a - off);
+            if (a + len < off + seg) add_free(a + len, off + seg - (a + len));
+            at = a;
+            break;
+        }
+        if (at < 0) {
+            at = (top + 31) & ~int64_t(31);
+            top = at + len;
+        }
+        live.emplace(end, at, len);
+        return at;
     }
 };
 
@@ -627,6 +670,36 @@ Plan* build_plan(const sdsb200_symbolic* sym, const sdsb200_plan_options* popts,
         P->maps.am_src = upload(P, am_src, st);
         P->maps.am_loc = upload(P, am_loc, st);
         P->maps.amcol = upload(P, amcol, st);
+        // cooperative pivot launches (single-member plans): a group of co-resident CTAs per wide front,
+        // sized by the front's update work f w^2 (at least one CTA, at most f w / 2048)
+        std::vector<int32_t> coop_first;
+        if (P->nbatch == 1) {
+            const int cap = P->elsize == 8 ? large_pivot_coop_capacity<double>(P->structure)
+                                           : large_pivot_coop_capacity<float>(P->structure);
+            for (ProgLaunch& L : P->prog) {
+                if (L.kind != L_PIVOT_FRONT || L.count <= 0 || 2 * L.count > cap) continue;
+                double total = 0;
+                for (int i = 0; i < L.count; ++i) {
+                    const DFront& F = P->fronts[lists[L.list + i]];
+                    total += (double)F.f * F.w * F.w;
+                }
+                L.coop = (int32_t)coop_first.size();
+                int first = 0;
+                for (int i = 0; i < L.count; ++i) {
+                    const DFront& F = P->fronts[lists[L.list + i]];
+                    const double share = total > 0 ? (double)cap * ((double)F.f * F.w * F.w) / total : 1.0;
+                    const int64_t most = std::max<int64_t>(1, (int64_t)F.f * F.w / 2048);
+                    const int g = (int)std::max<int64_t>(1, std::min<int64_t>((int64_t)share, most));
+                    coop_first.push_back(first);
+                    first += g;
+                }
+                coop_first.push_back(first);
+                L.coop_grid = first;
+                P->coop_bar_len = std::max(P->coop_bar_len, L.count);
+            }
+        }
+        P->d_coop_first = upload(P, coop_first, st);
+        if (P->coop_bar_len) P->d_coop_bar = dalloc<unsigned int>(P, P->coop_bar_len);
         P->maps.ea = upload(P, ea, st);
         P->maps.eacol = upload(P, eacol, st);
         P->maps.rowval = upload(P, rv0, st);

@@ -26,6 +26,8 @@ struct ProgLaunch {
     BufId abuf, bbuf, cbuf;
     double flops;      // algorithmic flops of the launch (reference convention for the fronts)
     double bytes;      // algorithmic device-memory bytes of the launch
+    int32_t coop = -1;      // pivot: offset of the group prefix in coop_first (-1: one CTA per front)
+    int32_t coop_grid = 0;  // pivot: CTAs of the cooperative launch
 };
 
 // per-kind accounting of the profiling mode (CUDA events around every launch)
@@ -79,6 +81,9 @@ struct Plan {
     PanelTask* d_ptasks = nullptr;
     GemmTile* d_tiles = nullptr;
     int64_t* d_scr_off = nullptr;
+    int32_t* d_coop_first = nullptr;   // group prefixes of the cooperative pivot launches
+    unsigned int* d_coop_bar = nullptr; // their group barrier counters
+    int32_t coop_bar_len = 0;
     int64_t* d_woff = nullptr;
     int64_t* d_uoff = nullptr;
     int32_t* d_level_lists = nullptr;   // fronts of each level for the solve sweeps: small first, then large
