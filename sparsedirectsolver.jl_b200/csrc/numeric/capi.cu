@@ -231,6 +231,7 @@ int run_factor(Plan* P, const double* nzval, double eps, double u, int pivot, in
                 a.cbuf = buf(L.cbuf, a.cstride);
                 a.finfo = P->d_finfo;
                 a.ns = (int32_t)P->ns;
+                a.status = P->d_solve_status;
                 e = launch_gemm<T>(a, nm, st);
                 break;
             }

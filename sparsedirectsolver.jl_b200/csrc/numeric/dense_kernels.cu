@@ -302,7 +302,7 @@ cudaError_t launch_gemm(const GemmArgs<T>& a, int nmembers, cudaStream_t st) {
     if constexpr (sizeof(T) == 8) {
         gemm_nt_dmma_kernel<<<grid, 128, 0, st>>>(a);
     } else {
-        gemm_nt_kernel<T><<<grid, 256, 0, st>>>(a);
+        return launch_gemm_tc32(a, nmembers, st);   // 3xTF32 on tcgen05
     }
     return cudaGetLastError();
 }

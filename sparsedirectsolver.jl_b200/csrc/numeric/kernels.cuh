@@ -103,7 +103,12 @@ struct GemmArgs {
     int64_t astride, bstride, cstride;  // per-member strides of the three buffers
     const int32_t* finfo;
     int32_t ns;
+    int32_t* status;   // tensor-core GEMM: nonzero when a bounded wait for the MMAs gave up
 };
+
+// FP32 grouped GEMM on the tensor cores (tcgen05, 3xTF32); tc_kernels.cu
+cudaError_t launch_gemm_tc32(const GemmArgs<float>& a, int nmembers, cudaStream_t st);
+cudaError_t prepare_tc_kernels();
 
 // Large LDLT / LU fronts: one CTA per front, the in-front steps on the global panels.
 template <typename T>

@@ -762,6 +762,7 @@ Plan* build_plan(const sdsb200_symbolic* sym, const sdsb200_plan_options* popts,
             cudaError_t ke = prepare_factor_kernels(optin);
             if (ke == cudaSuccess) ke = prepare_dense_kernels(optin);
             if (ke == cudaSuccess) ke = prepare_solve_kernels(optin);
+            if (ke == cudaSuccess) ke = prepare_tc_kernels();
             if (ke != cudaSuccess)
                 throw BuildError(SDSB200_CUDA_ERROR, std::string("kernel attribute setup failed: ") + cudaGetErrorString(ke));
             if ((int64_t)small_front_smem(P->fsmall_max, P->elsize) > optin)
