@@ -95,10 +95,11 @@ typedef struct sdsb200_plan_options {
 
 /* Plan tuning (the shapes an autotuner chooses; no counterpart in the reference):
  * fsmall = the largest front order handled by the shared-memory small-front kernel (one of 32, 64,
- * 96, 128, 160, and 224 for FP32; 0 = the largest class); wide = the front width from which the
- * solve treats a front as wide, splitting it into 64-column block steps over the grid (16..1024,
- * 0 = 96; fronts with (f - w) * w >= 32768 are always wide). */
-#define SDSB200_TUNING(fsmall, wide) ((int32_t)(fsmall) | ((int32_t)(wide) << 16))
+ * 96, 128, 160, and 224 for FP32; 0 = the largest class); wide, area = a front is "wide" in the
+ * solve, its columns split into 64-column block steps over the whole grid, when its width is at
+ * least `wide` (16..2047, 0 = 96) or (f - w) * w is at least 1024 * area (area 1..2047, 0 = 8). */
+#define SDSB200_TUNING(fsmall, wide, area) \
+    ((int32_t)(fsmall) | ((int32_t)(wide) << 9) | ((int32_t)(area) << 20))
 
 /* The Options fields the numeric and solve phases read (src/options.jl:155-223). */
 typedef struct sdsb200_opts {

@@ -245,15 +245,15 @@ Plan* build_plan(const sdsb200_symbolic* sym, const sdsb200_plan_options* popts,
         // small / large classification
         std::vector<int> classes = P->elsize == 8 ? std::vector<int>{32, 64, 96, 128, 160}
                                                   : std::vector<int>{32, 64, 96, 128, 160, 224};
-        const int tune_fsmall = popts ? (popts->tuning & 0xFFFF) : 0;
-        const int tune_wide = popts ? ((popts->tuning >> 16) & 0xFFFF) : 0;
+        const int tune_fsmall = popts ? (popts->tuning & 0x1FF) : 0;
+        const int tune_wide = popts ? ((popts->tuning >> 9) & 0x7FF) : 0;
+        const int tune_area = popts ? ((popts->tuning >> 20) & 0x7FF) : 0;
         if (tune_fsmall) {
             if (std::find(classes.begin(), classes.end(), tune_fsmall) == classes.end())
                 throw BuildError(SDSB200_INVALID_VALUE, "tuning: fsmall must be one of the front classes");
             while (classes.back() > tune_fsmall) classes.pop_back();
         }
-        if (tune_wide && (tune_wide < 16 || tune_wide > 1024))
-            throw BuildError(SDSB200_INVALID_VALUE, "tuning: wide must lie in 16..1024");
+        if (tune_wide && tune_wide < 16) throw BuildError(SDSB200_INVALID_VALUE, "tuning: wide must lie in 16..2047");
         P->fsmall_max = classes.back();
         auto class_of = [&](int f) {
             for (int c : classes)
@@ -491,7 +491,8 @@ Plan* build_plan(const sdsb200_symbolic* sym, const sdsb200_plan_options* popts,
         std::vector<int64_t> dinv_off(ns, -1);
         std::vector<int32_t> binv_tasks;
         const int wide_w = tune_wide ? tune_wide : 96;
-        auto solve_wide = [&](const DFront& F) { return F.w >= wide_w || (int64_t)(F.f - F.w) * F.w >= 32768; };
+        const int64_t wide_area = 1024 * (int64_t)(tune_area ? tune_area : 8);
+        auto solve_wide = [&](const DFront& F) { return F.w >= wide_w || (int64_t)(F.f - F.w) * F.w >= wide_area; };
         for (int64_t s = 0; s < ns; ++s) {
             const DFront& F = P->fronts[s];
             if (!solve_wide(F)) continue;

@@ -3,8 +3,9 @@
 Two shapes decide how the fronts of a plan map onto the kernels:
 * ``fsmall``: the largest front order factored in shared memory by the small-front kernel. Larger
   fronts take the column-owner assembly, diagonal-block and DMMA GEMM path.
-* ``wide``: the front width from which the solve splits a front into 64-column block steps over
-  the whole grid instead of one CTA or warp.
+* ``wide``, ``area``: a front whose width reaches ``wide`` or whose rectangular part (f - w) w
+  reaches 1024 ``area`` is "wide" in the solve: its columns go in 64-column block steps over the
+  whole grid instead of one CTA or warp.
 
 The autotuner times factorization + solve for each candidate on the solver's own matrix and
 right-hand side (CUDA events, after a warm-up), keeps the fastest, and leaves the solver planned
@@ -15,8 +16,9 @@ from __future__ import annotations
 from .capi import tuning as make_tuning
 
 CANDIDATES = (
-    (0, 0), (128, 0), (96, 0), (64, 0),
-    (0, 64), (0, 128), (128, 64), (96, 128),
+    (0, 0, 0), (128, 0, 0), (96, 0, 0),
+    (0, 64, 0), (0, 128, 0),
+    (0, 0, 16), (0, 0, 8), (0, 0, 4), (0, 64, 8), (0, 64, 4),
 )
 
 _cache: dict = {}
@@ -40,8 +42,8 @@ def autotune(solver, B, candidates=CANDIDATES, reps=3, use_cache=True):
         solver.execute("factorization")
         return dict(times)
     times = {}
-    for fs, wd in candidates:
-        t = make_tuning(fs, wd)
+    for cand in candidates:
+        t = make_tuning(*cand)
         solver.setparam("tuning", t)
         try:
             solver.replan()
@@ -67,7 +69,7 @@ def autotune(solver, B, candidates=CANDIDATES, reps=3, use_cache=True):
 
 
 def describe(t):
-    return {"fsmall": int(t) & 0xFFFF, "wide": (int(t) >> 16) & 0xFFFF}
+    return {"fsmall": int(t) & 0x1FF, "wide": (int(t) >> 9) & 0x7FF, "area": (int(t) >> 20) & 0x7FF}
 
 
 __all__ = ["autotune", "describe", "CANDIDATES"]

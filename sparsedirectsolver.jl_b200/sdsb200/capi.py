@@ -35,9 +35,9 @@ class PlanOptions(C.Structure):
     _fields_ = [("nbatch", C.c_int32), ("precision", C.c_int32), ("max_nrhs", C.c_int32), ("tuning", C.c_int32)]
 
 
-def tuning(fsmall=0, wide=0):
-    """SDSB200_TUNING(fsmall, wide): the plan's front tile shapes (0 = defaults)."""
-    return int(fsmall) | (int(wide) << 16)
+def tuning(fsmall=0, wide=0, area=0):
+    """SDSB200_TUNING(fsmall, wide, area): the plan's front tile shapes (0 = defaults)."""
+    return int(fsmall) | (int(wide) << 9) | (int(area) << 20)
 
 
 class Opts(C.Structure):
