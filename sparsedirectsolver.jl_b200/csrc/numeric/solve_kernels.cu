@@ -25,18 +25,28 @@ namespace sds {
 
 constexpr int SOLVE_THREADS = 256;
 
-// acc[r] += sum_{j < W} Lrow[j * ld] * x[j + r * ldx] for r < rc (<= 8): eight independent loads are
-// issued before their FMAs, so that a thread keeps several factor loads in flight
+// acc[r] += sum_{j < W} Lrow[j * ld] * x[j + r * ldx] for r < rc (<= 8): sixteen independent loads
+// are issued before their FMAs, so that a thread keeps many factor loads in flight
 template <typename T>
 __device__ __forceinline__ void row_dot(const T* __restrict__ Lrow, int64_t ld, int W, const double* x, int ldx,
                                         int rc, double* acc) {
     int j = 0;
-    for (; j + 8 <= W; j += 8) {
-        double lv[8];
+    for (; j + 16 <= W; j += 16) {
+        double lv[16];
 #pragma unroll
-        for (int u = 0; u < 8; ++u) lv[u] = (double)Lrow[(int64_t)(j + u) * ld];
+        for (int u = 0; u < 16; ++u) lv[u] = (double)Lrow[(int64_t)(j + u) * ld];
 #pragma unroll
-        for (int u = 0; u < 8; ++u)
+        for (int u = 0; u < 16; ++u)
+#pragma unroll
+            for (int r = 0; r < 8; ++r)
+                if (r < rc) acc[r] += lv[u] * x[j + u + r * ldx];
+    }
+    for (; j + 4 <= W; j += 4) {
+        double lv[4];
+#pragma unroll
+        for (int u = 0; u < 4; ++u) lv[u] = (double)Lrow[(int64_t)(j + u) * ld];
+#pragma unroll
+        for (int u = 0; u < 4; ++u)
 #pragma unroll
             for (int r = 0; r < 8; ++r)
                 if (r < rc) acc[r] += lv[u] * x[j + u + r * ldx];
@@ -49,16 +59,27 @@ __device__ __forceinline__ void row_dot(const T* __restrict__ Lrow, int64_t ld, 
     }
 }
 
-// acc[r] += sum_{i = lane, lane + 32, ... < M} Lcol[i] * xval(i, r): a warp-strided dot with four loads in flight
+// acc[r] += sum_{i = lane, lane + 32, ... < M} Lcol[i] * xval(i, r): a warp-strided dot with sixteen
+// loads in flight per lane
 template <typename T, class XF>
 __device__ __forceinline__ void col_dot(const T* __restrict__ Lcol, int M, int lane, int rc, XF xval, double* acc) {
     int i = lane;
-    for (; i + 224 < M; i += 256) {
-        double lv[8];
+    for (; i + 480 < M; i += 512) {
+        double lv[16];
 #pragma unroll
-        for (int u = 0; u < 8; ++u) lv[u] = (double)Lcol[i + 32 * u];
+        for (int u = 0; u < 16; ++u) lv[u] = (double)Lcol[i + 32 * u];
 #pragma unroll
-        for (int u = 0; u < 8; ++u)
+        for (int u = 0; u < 16; ++u)
+#pragma unroll
+            for (int r = 0; r < 8; ++r)
+                if (r < rc) acc[r] += lv[u] * xval(i + 32 * u, r);
+    }
+    for (; i + 96 < M; i += 128) {
+        double lv[4];
+#pragma unroll
+        for (int u = 0; u < 4; ++u) lv[u] = (double)Lcol[i + 32 * u];
+#pragma unroll
+        for (int u = 0; u < 4; ++u)
 #pragma unroll
             for (int r = 0; r < 8; ++r)
                 if (r < rc) acc[r] += lv[u] * xval(i + 32 * u, r);
