@@ -90,6 +90,7 @@ int prof_kind_of(LaunchKind k) {
         case L_ASSEMBLE: return PK_ASSEMBLE;
         case L_CHOL_PANEL: return PK_PANEL;
         case L_CHOL_DIAG: return PK_PANEL;
+        case L_CHOL_STEP: return PK_PANEL;
         case L_GEMM: return PK_GEMM;
         case L_PIVOT_FRONT: return PK_PIVOT;
         case L_SCALE: return PK_SCALE;
@@ -232,7 +233,23 @@ int run_factor(Plan* P, const double* nzval, double eps, double u, int pivot, in
                 a.finfo = P->d_finfo;
                 a.ns = (int32_t)P->ns;
                 a.status = P->d_solve_status;
+                a.copy_src = static_cast<const T*>(P->d_inv);
+                a.copy_stride = P->inv_len;
                 e = launch_gemm<T>(a, nm, st);
+                break;
+            }
+            case L_CHOL_STEP: {
+                CholStepArgs<T> a{};
+                a.fronts = P->d_fronts;
+                a.tasks = P->d_steptasks + L.list;
+                a.count = L.count;
+                a.members = members;
+                a.factor = factor;
+                a.scratch = static_cast<T*>(P->d_inv);
+                a.scr_len = P->inv_len;
+                a.finfo = P->d_finfo; a.stats = P->d_stats;
+                a.factor_len = P->factor_len; a.ns = (int32_t)P->ns; a.kb = L.cls; a.eps = eps;
+                e = launch_chol_step<T>(a, nm, st);
                 break;
             }
             case L_CHOL_DIAG: {

@@ -47,7 +47,8 @@ struct GemmTile {
     int32_t m, n, k;     // valid rows and columns of this tile (<= tile size), inner dimension
     int32_t diag;
     int32_t front;       // status check: the tile is skipped when this front failed (-1: none)
-    int32_t mode;        // 0: C -= A B^T; 1: C = A B^T (in place over A's rows: trsm by an inverse)
+    int32_t mode;        // 0: C -= A B^T; 1: C = A B^T (in place over A's rows: trsm by an inverse);
+                         // 2: C = copy_src block at a (a deferred diagonal-block write)
     int32_t pad;
 };
 
@@ -62,6 +63,7 @@ enum LaunchKind : int32_t {
     L_STATS,           // statistics reduction
     L_SCALE,           // W = L21 D of large LDLT / LU fronts
     L_BLOCKINV,        // inverses of the diagonal blocks of the wide fronts (solve)
+    L_CHOL_STEP,       // large Cholesky: one 32-column step (diagonal block + trsm of the rows below)
 };
 
 struct Launch {

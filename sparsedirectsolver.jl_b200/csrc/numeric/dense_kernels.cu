@@ -127,6 +127,12 @@ __global__ void __launch_bounds__(256) gemm_nt_kernel(GemmArgs<T> A) {
     const GemmTile t = A.tiles[blockIdx.x];
     const int member = A.members ? A.members[blockIdx.y] : blockIdx.y;
     if (A.finfo && t.front >= 0 && A.finfo[(int64_t)member * A.ns + t.front] != 0) return;
+    if (t.mode == 2) {   // deferred diagonal-block write
+        const T* src = A.copy_src + (int64_t)member * A.copy_stride + t.a;
+        T* dst = A.cbuf + (int64_t)member * A.cstride + t.c;
+        for (int q = threadIdx.x; q < t.m * t.n; q += blockDim.x) dst[q % t.m + (int64_t)(q / t.m) * t.ldc] = src[q % t.m + (int64_t)(q / t.m) * t.lda];
+        return;
+    }
     const T* Ab = A.abuf + (int64_t)member * A.astride + t.a;
     const T* Bb = A.bbuf + (int64_t)member * A.bstride + t.b;
     T* Cb = A.cbuf + (int64_t)member * A.cstride + t.c;
@@ -212,6 +218,12 @@ __global__ void __launch_bounds__(128) gemm_nt_dmma_kernel(GemmArgs<double> A) {
     const GemmTile t = A.tiles[blockIdx.x];
     const int member = A.members ? A.members[blockIdx.y] : blockIdx.y;
     if (A.finfo && t.front >= 0 && A.finfo[(int64_t)member * A.ns + t.front] != 0) return;
+    if (t.mode == 2) {   // deferred diagonal-block write
+        const double* src = A.copy_src + (int64_t)member * A.copy_stride + t.a;
+        double* dst = A.cbuf + (int64_t)member * A.cstride + t.c;
+        for (int q = threadIdx.x; q < t.m * t.n; q += blockDim.x) dst[q % t.m + (int64_t)(q / t.m) * t.ldc] = src[q % t.m + (int64_t)(q / t.m) * t.lda];
+        return;
+    }
     const double* Ab = A.abuf + (int64_t)member * A.astride + t.a;
     const double* Bb = A.bbuf + (int64_t)member * A.bstride + t.b;
     double* Cb = A.cbuf + (int64_t)member * A.cstride + t.c;
@@ -397,6 +409,144 @@ __global__ void __launch_bounds__(32) chol_diag_kernel(CholDiagArgs<T> A) {
     T* inv = A.inv + (int64_t)member * A.inv_len + A.inv_off[blockIdx.x];
     for (int j = 0; j < NB; ++j) inv[i + (int64_t)j * NB] = (i < nbb && j < nbb && j <= i) ? T(X[i * LD + j]) : T(0);
 }
+
+// One 32-column step of a large Cholesky front, diagonal block and trsm fused: every CTA factors the
+// 32 x 32 diagonal block and inverts it (warp 0, the arithmetic of chol_diag_kernel) while warps 1..3
+// stage its own 64-row tile of the rows below; the CTA then replaces the tile by X = B L11^{-T}.
+// The diagonal block itself is read by every CTA of the step, so no CTA overwrites it: the head task
+// puts L11 in the scratch buffer and a copy tile of the next GEMM launch of the level writes it
+// into the panel (a diagonal block with no rows below is written directly by its only task).
+template <typename T>
+__global__ void __launch_bounds__(128) chol_step_kernel(CholStepArgs<T> A) {
+    constexpr int NB = CHOL_NB, LD = NB + 1, TR = 64;
+    __shared__ double L[NB * LD];
+    __shared__ double X[(NB + 1) * LD];
+    __shared__ double Bt[TR * LD];
+    __shared__ int s_status;
+    const CholStepTask task = A.tasks[blockIdx.x];
+    const int member = A.members ? A.members[blockIdx.y] : blockIdx.y;
+    const int s = task.front;
+    const DFront fd = A.fronts[s];
+    int32_t* finfo = A.finfo + (int64_t)member * A.ns;
+    if (finfo[s] != 0) return;
+    const int f = fd.f, w = fd.w, kb = A.kb;
+    const int nbb = min(NB, w - kb), r1 = kb + nbb;
+    T* P = A.factor + (int64_t)member * A.factor_len + fd.panel;
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int row0 = r1 + max(task.tile, 0) * TR;
+    const int rows = task.tile >= 0 ? min(TR, f - row0) : 0;
+    if (warp == 0) {
+        const int i = lane;
+        batched_copy<8>(0, 1, NB,
+                        [&](int j) { return (i < nbb && j < nbb && j <= i) ? (double)P[(kb + i) + (int64_t)(kb + j) * f] : 0.0; },
+                        [&](int j, double v) { L[i * LD + j] = v; });
+        __syncwarp();
+        const double eps = A.eps;
+        int status = 0;
+        for (int j = 0; j < nbb; ++j) {
+            double a0 = 0.0, a1 = 0.0, a2 = 0.0, a3 = 0.0;
+            int l = 0;
+            for (; l + 4 <= j; l += 4) {
+                a0 += L[i * LD + l] * L[j * LD + l];
+                a1 += L[i * LD + l + 1] * L[j * LD + l + 1];
+                a2 += L[i * LD + l + 2] * L[j * LD + l + 2];
+                a3 += L[i * LD + l + 3] * L[j * LD + l + 3];
+            }
+            for (; l < j; ++l) a0 += L[i * LD + l] * L[j * LD + l];
+            const double sv = L[i * LD + j] - ((a0 + a1) + (a2 + a3));
+            const double ajj = __shfl_sync(0xffffffffu, sv, j);
+            if (!(ajj > eps || (eps > 0 && ajj >= 0))) {
+                status = j + 1;
+                break;
+            }
+            const double sd = sqrt(fmax(ajj, eps));
+            if (i == j) L[i * LD + j] = (double)T(sd);
+            else if (i > j && i < nbb) L[i * LD + j] = (double)T(sv / sd);
+            __syncwarp();
+        }
+        if (!status && rows > 0) {
+            X[32 * LD + i] = i < nbb ? 1.0 / L[i * LD + i] : 0.0;
+            __syncwarp();
+            for (int r = 0; r < nbb; ++r) {
+                double a0 = 0.0, a1 = 0.0, a2 = 0.0, a3 = 0.0;
+                int l = 0;
+                for (; l + 4 <= r; l += 4) {
+                    a0 += L[r * LD + l] * X[l * LD + i];
+                    a1 += L[r * LD + l + 1] * X[(l + 1) * LD + i];
+                    a2 += L[r * LD + l + 2] * X[(l + 2) * LD + i];
+                    a3 += L[r * LD + l + 3] * X[(l + 3) * LD + i];
+                }
+                for (; l < r; ++l) a0 += L[r * LD + l] * X[l * LD + i];
+                const double rhs = (r == i ? 1.0 : 0.0) - ((a0 + a1) + (a2 + a3));
+                X[r * LD + i] = r >= i ? rhs * X[32 * LD + r] : 0.0;
+            }
+        }
+        if (lane == 0) s_status = status;
+    } else {
+        batched_copy<8>(tid - 32, 96, TR * NB,
+                        [&](int q) {
+                            const int r = q % TR, c = q / TR;
+                            return (r < rows && c < nbb) ? (double)P[(row0 + r) + (int64_t)(kb + c) * f] : 0.0;
+                        },
+                        [&](int q, double v) { Bt[(q % TR) * LD + q / TR] = v; });
+    }
+    __syncthreads();
+    const int status = s_status;
+    const bool head = task.tile <= 0;
+    if (head && tid == 0) {
+        int64_t* S = A.stats + ((int64_t)member * A.ns + s) * NSTAT;
+        if (status) {
+            finfo[s] = kb + status;
+            S[ST_NPOS] = kb + status - 1;
+            S[ST_INFO] = kb + status;
+        } else if (kb + nbb == w) {
+            S[ST_NPOS] = w;
+            S[ST_INFO] = 0;
+        }
+    }
+    if (head) {
+        // L11 with zeros above the diagonal: the scratch (copied by the next GEMM launch), or the panel
+        // when the block has no rows below it
+        T* dst = task.tile < 0 ? P + kb + (int64_t)kb * f : A.scratch + (int64_t)member * A.scr_len + task.scr;
+        const int64_t ld = task.tile < 0 ? f : NB;
+        for (int q = tid; q < nbb * nbb; q += blockDim.x) {
+            const int i = q % nbb, j = q / nbb;
+            dst[i + j * ld] = j <= i ? T(L[i * LD + j]) : T(0);
+        }
+    }
+    if (status || rows <= 0) return;
+    // X = B inv(L11)^T: X[r][j] = sum_{l <= j} B[r][l] inv[j][l]; thread: row tid % 64, 16 columns
+    const int r = tid & 63, half = tid >> 6;
+    if (r < rows) {
+        double acc[16];
+#pragma unroll
+        for (int jj = 0; jj < 16; ++jj) acc[jj] = 0.0;
+        for (int l = 0; l < nbb; ++l) {
+            const double b = Bt[r * LD + l];
+#pragma unroll
+            for (int jj = 0; jj < 16; ++jj) {
+                const int j = half * 16 + jj;
+                if (l <= j) acc[jj] += b * X[j * LD + l];
+            }
+        }
+#pragma unroll
+        for (int jj = 0; jj < 16; ++jj) {
+            const int j = half * 16 + jj;
+            if (j < nbb) P[(row0 + r) + (int64_t)(kb + j) * f] = T(acc[jj]);
+        }
+    }
+}
+
+template <typename T>
+cudaError_t launch_chol_step(const CholStepArgs<T>& a, int nmembers, cudaStream_t st) {
+    if (a.count == 0) return cudaSuccess;
+    dim3 grid(a.count, nmembers);
+    chol_step_kernel<T><<<grid, 128, 0, st>>>(a);
+    return cudaGetLastError();
+}
+
+template cudaError_t launch_chol_step<double>(const CholStepArgs<double>&, int, cudaStream_t);
+template cudaError_t launch_chol_step<float>(const CholStepArgs<float>&, int, cudaStream_t);
 
 // inverse of one 64 x 64 diagonal block of a panel (lower triangle as stored; unit or not), with the
 // register-owned right-looking substitution of chol_diag_kernel

@@ -92,6 +92,35 @@ struct CholDiagArgs {
     double eps;
 };
 
+// One task of a large-Cholesky step: a 64-row tile of the rows below the diagonal block of front
+// `front` (tile >= 0), or the diagonal block alone when no rows are below it (tile = -1). The task
+// with tile <= 0 is the step's head: it records the statistics and puts L11 at `scr` of the scratch
+// buffer (or, for a diagonal block with nothing below, directly into the panel).
+struct CholStepTask {
+    int32_t front;
+    int32_t tile;
+    int64_t scr;
+};
+
+template <typename T>
+struct CholStepArgs {
+    const DFront* fronts;
+    const CholStepTask* tasks;
+    int32_t count;
+    const int32_t* members;
+    T* factor;
+    T* scratch;               // L11 of the step heads, per member stride scr_len
+    int64_t scr_len;
+    int32_t* finfo;
+    int64_t* stats;
+    int64_t factor_len;
+    int32_t ns;
+    int32_t kb;
+    double eps;
+};
+template <typename T>
+cudaError_t launch_chol_step(const CholStepArgs<T>& a, int nmembers, cudaStream_t st);
+
 template <typename T>
 struct GemmArgs {
     const GemmTile* tiles;
@@ -104,6 +133,8 @@ struct GemmArgs {
     const int32_t* finfo;
     int32_t ns;
     int32_t* status;   // tensor-core GEMM: nonzero when a bounded wait for the MMAs gave up
+    const T* copy_src; // mode-2 tiles: C = copy_src[a ...] (ld lda), m x n
+    int64_t copy_stride;   // per-member stride of copy_src
 };
 
 // FP32 grouped GEMM on the tensor cores (tcgen05, 3xTF32); tc_kernels.cu

@@ -305,6 +305,7 @@ Plan* build_plan(const sdsb200_symbolic* sym, const sdsb200_plan_options* popts,
 
         // launch program of the factorization
         std::vector<int32_t> lists;
+        std::vector<CholStepTask> steptasks;
         std::vector<ColTask> coltasks;
         std::vector<PanelTask> ptasks;
         std::vector<GemmTile> tiles;
@@ -377,46 +378,47 @@ Plan* build_plan(const sdsb200_symbolic* sym, const sdsb200_plan_options* popts,
                 const int NB = CHOL_NB;
                 int maxw = 0;
                 for (int s : large) maxw = std::max(maxw, P->fronts[s].w);
+                // L11 of every (front, step) of the level gets its own scratch slot; it reaches the
+                // panel through a copy tile of the step's update GEMM, or of the contribution-block
+                // GEMM for a front's last step
+                int64_t scr = 0;
+                std::vector<std::pair<int, int64_t>> last_copy;
+                auto copy_tile = [&](int s, int64_t slot, int kb) {
+                    const DFront& F = P->fronts[s];
+                    const int nbb = std::min(NB, F.w - kb);
+                    GemmTile t{};
+                    t.a = slot; t.lda = NB;
+                    t.b = 0; t.ldb = 1;
+                    t.c = F.panel + kb + (int64_t)kb * F.f; t.ldc = F.f;
+                    t.m = nbb; t.n = nbb; t.k = 0;
+                    t.diag = 1 << 29;
+                    t.front = -1;
+                    t.mode = 2;
+                    tiles.push_back(t);
+                };
                 for (int kb = 0; kb < maxw; kb += NB) {
-                    ProgLaunch dl{};
-                    dl.kind = L_CHOL_DIAG; dl.level = L; dl.cls = kb; dl.nb = NB; dl.list = (int64_t)lists.size();
-                    dl.maxw = (int)inv_off.size();
-                    int64_t io = 0;
-                    for (int s : large)
-                        if (P->fronts[s].w > kb) {
-                            lists.push_back(s);
-                            inv_off.push_back(io);
-                            io += (int64_t)NB * NB;
-                        }
-                    P->inv_len = std::max(P->inv_len, io);
-                    dl.count = (int)(lists.size() - dl.list);
-                    dl.flops = 0;
-                    for (int s : large)
-                        if (P->fronts[s].w > kb) {
-                            double nbb = std::min(NB, P->fronts[s].w - kb);
-                            dl.flops += nbb * nbb * nbb / 3.0 * 2.0;
-                        }
-                    P->prog.push_back(dl);
-                    ProgLaunch tl{};
-                    tl.kind = L_GEMM; tl.level = L; tl.list = (int64_t)tiles.size();
-                    tl.abuf = BUF_FACTOR; tl.bbuf = BUF_INV; tl.cbuf = BUF_FACTOR;
-                    int64_t io2 = 0;
+                    ProgLaunch sl{};
+                    sl.kind = L_CHOL_STEP; sl.level = L; sl.cls = kb; sl.nb = NB;
+                    sl.list = (int64_t)steptasks.size();
+                    std::vector<std::pair<int, int64_t>> step_copy;
                     for (int s : large) {
                         const DFront& F = P->fronts[s];
                         if (F.w <= kb) continue;
-                        int nbb = std::min(NB, F.w - kb);
-                        int r1 = kb + nbb;
-                        if (r1 < F.f) {
-                            size_t t0 = tiles.size();
-                            tl.flops += add_gemm_tiles(F.panel + r1 + (int64_t)kb * F.f, F.f, io2, NB,
-                                                       F.panel + r1 + (int64_t)kb * F.f, F.f, F.f - r1, nbb, nbb,
-                                                       false, s);
-                            for (size_t q = t0; q < tiles.size(); ++q) tiles[q].mode = 1;
+                        const int nbb = std::min(NB, F.w - kb), r1 = kb + nbb, rows = F.f - r1;
+                        if (rows <= 0) {
+                            steptasks.push_back({s, -1, 0});
+                        } else {
+                            const int64_t slot = scr;
+                            scr += (int64_t)NB * NB;
+                            for (int t = 0; t * 64 < rows; ++t) steptasks.push_back({s, t, slot});
+                            if (F.w > kb + NB) step_copy.push_back({s, slot});
+                            else last_copy.push_back({s, slot});
                         }
-                        io2 += (int64_t)NB * NB;
+                        sl.flops += 2.0 * nbb * nbb * nbb / 3.0 + 2.0 * (double)std::max(rows, 0) * nbb * nbb;
+                        sl.bytes += P->elsize * (2.0 * nbb * nbb + 2.0 * std::max(rows, 0) * (double)nbb);
                     }
-                    tl.count = (int)(tiles.size() - tl.list);
-                    if (tl.count) P->prog.push_back(tl);
+                    sl.count = (int)(steptasks.size() - sl.list);
+                    P->prog.push_back(sl);
                     ProgLaunch gl{};
                     gl.kind = L_GEMM; gl.level = L; gl.list = (int64_t)tiles.size();
                     gl.abuf = gl.bbuf = gl.cbuf = BUF_FACTOR;
@@ -429,9 +431,11 @@ Plan* build_plan(const sdsb200_symbolic* sym, const sdsb200_plan_options* popts,
                                                    F.f, F.panel + k1 + (int64_t)k1 * f, F.f, F.f - k1, F.w - k1, NB,
                                                    true, s);
                     }
+                    for (auto& sc2 : step_copy) copy_tile(sc2.first, sc2.second, kb);
                     gl.count = (int)(tiles.size() - gl.list);
                     if (gl.count) P->prog.push_back(gl);
                 }
+                P->inv_len = std::max(P->inv_len, scr);
                 ProgLaunch cl{};
                 cl.kind = L_GEMM; cl.level = L; cl.list = (int64_t)tiles.size();
                 cl.abuf = cl.bbuf = BUF_FACTOR; cl.cbuf = BUF_CB;
@@ -443,6 +447,18 @@ Plan* build_plan(const sdsb200_symbolic* sym, const sdsb200_plan_options* popts,
                 }
                 cl.count = (int)(tiles.size() - cl.list);
                 if (cl.count) P->prog.push_back(cl);
+                if (!last_copy.empty()) {
+                    // the last diagonal blocks go to the panel (factor buffer), not to the CB arena
+                    ProgLaunch ql{};
+                    ql.kind = L_GEMM; ql.level = L; ql.list = (int64_t)tiles.size();
+                    ql.abuf = ql.bbuf = ql.cbuf = BUF_FACTOR;
+                    for (auto& lc2 : last_copy) {
+                        const DFront& F = P->fronts[lc2.first];
+                        copy_tile(lc2.first, lc2.second, ((F.w - 1) / NB) * NB);
+                    }
+                    ql.count = (int)(tiles.size() - ql.list);
+                    P->prog.push_back(ql);
+                }
             } else {
                 ProgLaunch pl{};
                 pl.kind = L_PIVOT_FRONT; pl.level = L; pl.list = (int64_t)lists.size(); pl.count = (int)large.size();
@@ -710,6 +726,7 @@ Plan* build_plan(const sdsb200_symbolic* sym, const sdsb200_plan_options* popts,
         P->d_lists = upload(P, lists, st);
         P->d_coltasks = upload(P, coltasks, st);
         P->d_ptasks = upload(P, ptasks, st);
+        P->d_steptasks = upload(P, steptasks, st);
         P->d_tiles = upload(P, tiles, st);
         P->d_scr_off = upload(P, scr_off, st);
         P->d_woff = upload(P, woff, st);

@@ -81,6 +81,7 @@ struct Plan {
     PanelTask* d_ptasks = nullptr;
     GemmTile* d_tiles = nullptr;
     int64_t* d_scr_off = nullptr;
+    CholStepTask* d_steptasks = nullptr; // tasks of the large-Cholesky step launches
     int32_t* d_coop_first = nullptr;   // group prefixes of the cooperative pivot launches
     unsigned int* d_coop_bar = nullptr; // their group barrier counters
     int32_t coop_bar_len = 0;

@@ -108,6 +108,12 @@ __global__ void __launch_bounds__(128) gemm_nt_tc32_kernel(GemmArgs<float> A) {
     const GemmTile t = A.tiles[blockIdx.x];
     const int member = A.members ? A.members[blockIdx.y] : blockIdx.y;
     if (A.finfo && t.front >= 0 && A.finfo[(int64_t)member * A.ns + t.front] != 0) return;
+    if (t.mode == 2) {   // deferred diagonal-block write
+        const float* src = A.copy_src + (int64_t)member * A.copy_stride + t.a;
+        float* dst = A.cbuf + (int64_t)member * A.cstride + t.c;
+        for (int q = threadIdx.x; q < t.m * t.n; q += blockDim.x) dst[q % t.m + (int64_t)(q / t.m) * t.ldc] = src[q % t.m + (int64_t)(q / t.m) * t.lda];
+        return;
+    }
     const float* Ab = A.abuf + (int64_t)member * A.astride + t.a;
     const float* Bb = A.bbuf + (int64_t)member * A.bstride + t.b;
     float* Cb = A.cbuf + (int64_t)member * A.cstride + t.c;
