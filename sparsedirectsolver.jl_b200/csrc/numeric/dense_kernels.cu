@@ -426,20 +426,18 @@ __global__ void __launch_bounds__(128) chol_step_kernel(CholStepArgs<T> A) {
     const CholStepTask task = A.tasks[blockIdx.x];
     const int member = A.members ? A.members[blockIdx.y] : blockIdx.y;
     const int s = task.front;
-    const DFront fd = A.fronts[s];
     int32_t* finfo = A.finfo + (int64_t)member * A.ns;
-    if (finfo[s] != 0) return;
-    const int f = fd.f, w = fd.w, kb = A.kb;
+    const int f = task.f, w = task.w, kb = A.kb;
     const int nbb = min(NB, w - kb), r1 = kb + nbb;
-    T* P = A.factor + (int64_t)member * A.factor_len + fd.panel;
+    T* P = A.factor + (int64_t)member * A.factor_len + task.panel;
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const int row0 = r1 + max(task.tile, 0) * TR;
     const int rows = task.tile >= 0 ? min(TR, f - row0) : 0;
     if (warp == 0) {
         const int i = lane;
-        batched_copy<8>(0, 1, NB,
-                        [&](int j) { return (i < nbb && j < nbb && j <= i) ? (double)P[(kb + i) + (int64_t)(kb + j) * f] : 0.0; },
-                        [&](int j, double v) { L[i * LD + j] = v; });
+        batched_copy<32>(0, 1, NB,
+                         [&](int j) { return (i < nbb && j < nbb && j <= i) ? (double)P[(kb + i) + (int64_t)(kb + j) * f] : 0.0; },
+                         [&](int j, double v) { L[i * LD + j] = v; });
         __syncwarp();
         const double eps = A.eps;
         int status = 0;
@@ -459,13 +457,19 @@ __global__ void __launch_bounds__(128) chol_step_kernel(CholStepArgs<T> A) {
                 status = j + 1;
                 break;
             }
-            const double sd = sqrt(fmax(ajj, eps));
-            if (i == j) L[i * LD + j] = (double)T(sd);
-            else if (i > j && i < nbb) L[i * LD + j] = (double)T(sv / sd);
+            // one reciprocal square root per column: L_jj = a_jj r, L_ij = s_i r, and r is the
+            // inverse's diagonal entry
+            const double r = rsqrt(fmax(ajj, eps));
+            if (i == j) {
+                L[i * LD + j] = (double)T(fmax(ajj, eps) * r);
+                X[32 * LD + j] = r;
+            } else if (i > j && i < nbb) {
+                L[i * LD + j] = (double)T(sv * r);
+            }
             __syncwarp();
         }
         if (!status && rows > 0) {
-            X[32 * LD + i] = i < nbb ? 1.0 / L[i * LD + i] : 0.0;
+            if (i >= nbb) X[32 * LD + i] = 0.0;
             __syncwarp();
             for (int r = 0; r < nbb; ++r) {
                 double a0 = 0.0, a1 = 0.0, a2 = 0.0, a3 = 0.0;
@@ -491,6 +495,7 @@ __global__ void __launch_bounds__(128) chol_step_kernel(CholStepArgs<T> A) {
                         [&](int q, double v) { Bt[(q % TR) * LD + q / TR] = v; });
     }
     __syncthreads();
+    if (finfo[s] != 0) return;   // an earlier step of this front failed
     const int status = s_status;
     const bool head = task.tile <= 0;
     if (head && tid == 0) {

@@ -100,6 +100,8 @@ struct CholStepTask {
     int32_t front;
     int32_t tile;
     int64_t scr;
+    int64_t panel;     // the front's panel offset, order and width (no dependent load of the front
+    int32_t f, w;      // record before the block loads)
 };
 
 template <typename T>

@@ -406,11 +406,11 @@ Plan* build_plan(const sdsb200_symbolic* sym, const sdsb200_plan_options* popts,
                         if (F.w <= kb) continue;
                         const int nbb = std::min(NB, F.w - kb), r1 = kb + nbb, rows = F.f - r1;
                         if (rows <= 0) {
-                            steptasks.push_back({s, -1, 0});
+                            steptasks.push_back({s, -1, 0, F.panel, F.f, F.w});
                         } else {
                             const int64_t slot = scr;
                             scr += (int64_t)NB * NB;
-                            for (int t = 0; t * 64 < rows; ++t) steptasks.push_back({s, t, slot});
+                            for (int t = 0; t * 64 < rows; ++t) steptasks.push_back({s, t, slot, F.panel, F.f, F.w});
                             if (F.w > kb + NB) step_copy.push_back({s, slot});
                             else last_copy.push_back({s, slot});
                         }
