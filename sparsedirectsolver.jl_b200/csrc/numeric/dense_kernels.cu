@@ -420,7 +420,7 @@ template <typename T>
 __global__ void __launch_bounds__(128) chol_step_kernel(CholStepArgs<T> A) {
     constexpr int NB = CHOL_NB, LD = NB + 1, TR = 64;
     __shared__ double L[NB * LD];
-    __shared__ double X[(NB + 1) * LD];
+    __shared__ double rdiag[NB];          // reciprocal diagonal of L11 (zero past the block)
     __shared__ double Bt[TR * LD];
     __shared__ int s_status;
     const CholStepTask task = A.tasks[blockIdx.x];
@@ -462,29 +462,13 @@ __global__ void __launch_bounds__(128) chol_step_kernel(CholStepArgs<T> A) {
             const double r = rsqrt(fmax(ajj, eps));
             if (i == j) {
                 L[i * LD + j] = (double)T(fmax(ajj, eps) * r);
-                X[32 * LD + j] = r;
+                rdiag[j] = r;
             } else if (i > j && i < nbb) {
                 L[i * LD + j] = (double)T(sv * r);
             }
             __syncwarp();
         }
-        if (!status && rows > 0) {
-            if (i >= nbb) X[32 * LD + i] = 0.0;
-            __syncwarp();
-            for (int r = 0; r < nbb; ++r) {
-                double a0 = 0.0, a1 = 0.0, a2 = 0.0, a3 = 0.0;
-                int l = 0;
-                for (; l + 4 <= r; l += 4) {
-                    a0 += L[r * LD + l] * X[l * LD + i];
-                    a1 += L[r * LD + l + 1] * X[(l + 1) * LD + i];
-                    a2 += L[r * LD + l + 2] * X[(l + 2) * LD + i];
-                    a3 += L[r * LD + l + 3] * X[(l + 3) * LD + i];
-                }
-                for (; l < r; ++l) a0 += L[r * LD + l] * X[l * LD + i];
-                const double rhs = (r == i ? 1.0 : 0.0) - ((a0 + a1) + (a2 + a3));
-                X[r * LD + i] = r >= i ? rhs * X[32 * LD + r] : 0.0;
-            }
-        }
+        if (i >= nbb) rdiag[i] = 0.0;   // reciprocal diagonal beyond the block: zero
         if (lane == 0) s_status = status;
     } else {
         batched_copy<8>(tid - 32, 96, TR * NB,
@@ -520,25 +504,28 @@ __global__ void __launch_bounds__(128) chol_step_kernel(CholStepArgs<T> A) {
         }
     }
     if (status || rows <= 0) return;
-    // X = B inv(L11)^T: X[r][j] = sum_{l <= j} B[r][l] inv[j][l]; thread: row tid % 64, 16 columns
-    const int r = tid & 63, half = tid >> 6;
+    // X = B L11^{-T}: each of the first 64 threads solves its row, x L11^T = b, by forward
+    // substitution with x in registers (fully unrolled; four partial sums per entry); columns past
+    // the block have a zero reciprocal diagonal and come out zero
+    const int r = tid;
     if (r < rows) {
-        double acc[16];
+        double x[NB];
 #pragma unroll
-        for (int jj = 0; jj < 16; ++jj) acc[jj] = 0.0;
-        for (int l = 0; l < nbb; ++l) {
-            const double b = Bt[r * LD + l];
+        for (int j = 0; j < NB; ++j) {
+            double a0 = Bt[r * LD + j], a1 = 0.0, a2 = 0.0, a3 = 0.0;
 #pragma unroll
-            for (int jj = 0; jj < 16; ++jj) {
-                const int j = half * 16 + jj;
-                if (l <= j) acc[jj] += b * X[j * LD + l];
+            for (int l = 0; l < j; ++l) {
+                const double t = x[l] * L[j * LD + l];
+                if ((l & 3) == 0) a0 -= t;
+                else if ((l & 3) == 1) a1 -= t;
+                else if ((l & 3) == 2) a2 -= t;
+                else a3 -= t;
             }
+            x[j] = ((a0 + a1) + (a2 + a3)) * rdiag[j];
         }
 #pragma unroll
-        for (int jj = 0; jj < 16; ++jj) {
-            const int j = half * 16 + jj;
-            if (j < nbb) P[(row0 + r) + (int64_t)(kb + j) * f] = T(acc[jj]);
-        }
+        for (int j = 0; j < NB; ++j)
+            if (j < nbb) P[(row0 + r) + (int64_t)(kb + j) * f] = T(x[j]);
     }
 }
 
