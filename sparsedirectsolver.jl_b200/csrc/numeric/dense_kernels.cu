@@ -434,40 +434,44 @@ __global__ void __launch_bounds__(128) chol_step_kernel(CholStepArgs<T> A) {
     const int row0 = r1 + max(task.tile, 0) * TR;
     const int rows = task.tile >= 0 ? min(TR, f - row0) : 0;
     if (warp == 0) {
+        // lane i holds row i of the block in registers; L[j][l] comes from lane j by shuffle, so the
+        // dependent path of a column is one shuffle, a short reduction and one reciprocal square root
         const int i = lane;
-        batched_copy<32>(0, 1, NB,
-                         [&](int j) { return (i < nbb && j < nbb && j <= i) ? (double)P[(kb + i) + (int64_t)(kb + j) * f] : 0.0; },
-                         [&](int j, double v) { L[i * LD + j] = v; });
-        __syncwarp();
+        double x[NB];
+#pragma unroll
+        for (int j = 0; j < NB; ++j)
+            x[j] = (i < nbb && j < nbb && j <= i) ? (double)P[(kb + i) + (int64_t)(kb + j) * f] : 0.0;
         const double eps = A.eps;
         int status = 0;
-        for (int j = 0; j < nbb; ++j) {
-            double a0 = 0.0, a1 = 0.0, a2 = 0.0, a3 = 0.0;
-            int l = 0;
-            for (; l + 4 <= j; l += 4) {
-                a0 += L[i * LD + l] * L[j * LD + l];
-                a1 += L[i * LD + l + 1] * L[j * LD + l + 1];
-                a2 += L[i * LD + l + 2] * L[j * LD + l + 2];
-                a3 += L[i * LD + l + 3] * L[j * LD + l + 3];
+#pragma unroll
+        for (int j = 0; j < NB; ++j) {
+            if (j < nbb && status == 0) {
+                double a0 = 0.0, a1 = 0.0, a2 = 0.0, a3 = 0.0;
+#pragma unroll
+                for (int l = 0; l < j; ++l) {
+                    const double t = x[l] * __shfl_sync(0xffffffffu, x[l], j);
+                    if ((l & 3) == 0) a0 += t;
+                    else if ((l & 3) == 1) a1 += t;
+                    else if ((l & 3) == 2) a2 += t;
+                    else a3 += t;
+                }
+                const double sv = x[j] - ((a0 + a1) + (a2 + a3));
+                const double ajj = __shfl_sync(0xffffffffu, sv, j);
+                if (!(ajj > eps || (eps > 0 && ajj >= 0))) {
+                    status = j + 1;
+                } else {
+                    const double r = rsqrt(fmax(ajj, eps));
+                    if (i == j) {
+                        x[j] = (double)T(fmax(ajj, eps) * r);
+                        rdiag[j] = r;
+                    } else if (i > j && i < nbb) {
+                        x[j] = (double)T(sv * r);
+                    }
+                }
             }
-            for (; l < j; ++l) a0 += L[i * LD + l] * L[j * LD + l];
-            const double sv = L[i * LD + j] - ((a0 + a1) + (a2 + a3));
-            const double ajj = __shfl_sync(0xffffffffu, sv, j);
-            if (!(ajj > eps || (eps > 0 && ajj >= 0))) {
-                status = j + 1;
-                break;
-            }
-            // one reciprocal square root per column: L_jj = a_jj r, L_ij = s_i r, and r is the
-            // inverse's diagonal entry
-            const double r = rsqrt(fmax(ajj, eps));
-            if (i == j) {
-                L[i * LD + j] = (double)T(fmax(ajj, eps) * r);
-                rdiag[j] = r;
-            } else if (i > j && i < nbb) {
-                L[i * LD + j] = (double)T(sv * r);
-            }
-            __syncwarp();
         }
+#pragma unroll
+        for (int j = 0; j < NB; ++j) L[i * LD + j] = x[j];
         if (i >= nbb) rdiag[i] = 0.0;   // reciprocal diagonal beyond the block: zero
         if (lane == 0) s_status = status;
     } else {
