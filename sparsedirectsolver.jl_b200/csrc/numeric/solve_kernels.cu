@@ -171,10 +171,12 @@ __device__ void forward_front(const SweepArgs<T>& A, int s, int member, double* 
                         },
                         [&](int q, double v) { Ld[q & 31][q >> 5] = v; });
         __syncthreads();
-        for (int r = warp; r < nrhs; r += nwarps) {  // one warp per right-hand side
+        // one warp per right-hand side; each lane applies its own reciprocal diagonal entry
+        const double rdl = (!A.unit && lane < bw) ? 1.0 / Ld[lane][lane] : 1.0;
+        for (int r = warp; r < nrhs; r += nwarps) {
             double val = lane < bw ? xs[jb + lane + r * w] : 0.0;
             for (int j = 0; j < bw; ++j) {
-                if (!A.unit && lane == j) val /= Ld[j][j];
+                if (lane == j) val *= rdl;
                 double xj = __shfl_sync(0xffffffffu, val, j);
                 if (lane > j) val -= Ld[lane][j] * xj;
             }
@@ -270,10 +272,11 @@ __device__ void backward_front(const SweepArgs<T>& A, int s, int member, double*
                         },
                         [&](int q, double v) { Ld[q & 31][q >> 5] = v; });
         __syncthreads();
+        const double rdl = (!A.unit && lane < bw) ? 1.0 / Ld[lane][lane] : 1.0;
         for (int r = warp; r < nrhs; r += nwarps) {
             double val = lane < bw ? xs[jb + lane + r * w] : 0.0;
             for (int j = bw - 1; j >= 0; --j) {
-                if (!A.unit && lane == j) val /= Ld[j][j];
+                if (lane == j) val *= rdl;
                 double xj = __shfl_sync(0xffffffffu, val, j);
                 if (lane < j) val -= Ld[j][lane] * xj;
             }
@@ -434,14 +437,25 @@ __device__ void warp_forward_front(const SweepArgs<T>& A, int s, double* xs, dou
                         [&](int j) { return (lane < bw && lane >= j) ? (double)L[(jb + lane) + (int64_t)(jb + j) * f] : 0.0; },
                         [&](int j, double v) { Ld[lane * 33 + j] = v; });
         __syncwarp();
-        for (int r = 0; r < nrhs; ++r) {
-            double val = lane < bw ? xs[jb + lane + r * w] : 0.0;
+        // all right-hand sides (chunks of 8) in one shuffle chain; reciprocal diagonal per lane
+        const double rdl = (!A.unit && lane < bw) ? 1.0 / Ld[lane * 33 + lane] : 1.0;
+        for (int r0 = 0; r0 < nrhs; r0 += 8) {
+            const int rc = min(8, nrhs - r0);
+            double val[8];
+#pragma unroll
+            for (int r = 0; r < 8; ++r) val[r] = (lane < bw && r < rc) ? xs[jb + lane + (r0 + r) * w] : 0.0;
             for (int j = 0; j < bw; ++j) {
-                if (!A.unit && lane == j) val /= Ld[j * 33 + j];
-                const double xj = __shfl_sync(0xffffffffu, val, j);
-                if (lane > j) val -= Ld[lane * 33 + j] * xj;
+                const double lj = Ld[lane * 33 + j];
+#pragma unroll
+                for (int r = 0; r < 8; ++r) {
+                    if (lane == j) val[r] *= rdl;
+                    const double xj = __shfl_sync(0xffffffffu, val[r], j);
+                    if (lane > j) val[r] -= lj * xj;
+                }
             }
-            if (lane < bw) xs[jb + lane + r * w] = val;
+#pragma unroll
+            for (int r = 0; r < 8; ++r)
+                if (lane < bw && r < rc) xs[jb + lane + (r0 + r) * w] = val[r];
         }
         __syncwarp();
         for (int q = jb + bw + lane; q < w; q += 32) {
@@ -524,14 +538,24 @@ __device__ void warp_backward_front(const SweepArgs<T>& A, int s, double* xs, do
                         [&](int j) { return (lane < bw && lane >= j) ? (double)L[(jb + lane) + (int64_t)(jb + j) * f] : 0.0; },
                         [&](int j, double v) { Ld[lane * 33 + j] = v; });
         __syncwarp();
-        for (int r = 0; r < nrhs; ++r) {
-            double val = lane < bw ? xs[jb + lane + r * w] : 0.0;
+        const double rdl = (!A.unit && lane < bw) ? 1.0 / Ld[lane * 33 + lane] : 1.0;
+        for (int r0 = 0; r0 < nrhs; r0 += 8) {
+            const int rc = min(8, nrhs - r0);
+            double val[8];
+#pragma unroll
+            for (int r = 0; r < 8; ++r) val[r] = (lane < bw && r < rc) ? xs[jb + lane + (r0 + r) * w] : 0.0;
             for (int j = bw - 1; j >= 0; --j) {
-                if (!A.unit && lane == j) val /= Ld[j * 33 + j];
-                const double xj = __shfl_sync(0xffffffffu, val, j);
-                if (lane < j) val -= Ld[j * 33 + lane] * xj;
+                const double lj = Ld[j * 33 + lane];
+#pragma unroll
+                for (int r = 0; r < 8; ++r) {
+                    if (lane == j) val[r] *= rdl;
+                    const double xj = __shfl_sync(0xffffffffu, val[r], j);
+                    if (lane < j) val[r] -= lj * xj;
+                }
             }
-            if (lane < bw) xs[jb + lane + r * w] = val;
+#pragma unroll
+            for (int r = 0; r < 8; ++r)
+                if (lane < bw && r < rc) xs[jb + lane + (r0 + r) * w] = val[r];
         }
         __syncwarp();
         for (int i = lane; i < jb; i += 32) {
