@@ -138,6 +138,13 @@ int sdsb200_factor(sdsb200_plan* plan, const double* nzval, const int8_t* h_psig
 int sdsb200_solve(sdsb200_plan* plan, double* X, int64_t ldx, const double* B, int64_t ldb, int32_t nrhs,
                   const double* nzval, const sdsb200_opts* opts, int32_t* h_ir_steps, void* stream);
 
+/* residual! (src/solve/refinement.jl:229-248): R = B - op(A) X over the full pattern with the values
+ * nzval, for the active members (R: n x nrhs per member, ld n, members at stride n * nrhs; X, B as in
+ * sdsb200_solve). solve_mode 1 or 2 with "G": op(A) = A^T. Used by FGMRES-IR for its residual and
+ * its matrix-vector products (B = 0 gives R = -op(A) X). */
+int sdsb200_residual(sdsb200_plan* plan, double* R, const double* X, int64_t ldx, const double* B, int64_t ldb,
+                     int32_t nrhs, const double* nzval, int32_t solve_mode, void* stream);
+
 /* Outputs (synchronous host copies; member = 0-based batch member). */
 int sdsb200_get_stats(sdsb200_plan* plan, int32_t member, int64_t* h_stats /* 6 * ns */,
                       int64_t* h_totals /* 6 */);

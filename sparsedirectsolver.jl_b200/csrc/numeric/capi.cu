@@ -894,6 +894,29 @@ double sdsb200_plan_stat(const sdsb200_plan* plan, const char* name) {
 
 }  // extern "C"
 
+extern "C" int sdsb200_residual(sdsb200_plan* plan, double* R, const double* X, int64_t ldx, const double* B,
+                                int64_t ldb, int32_t nrhs, const double* nzval, int32_t solve_mode, void* stream) {
+    Plan* P = reinterpret_cast<Plan*>(plan);
+    if (!P) return fail(SDSB200_INVALID_VALUE, "plan is NULL");
+    if (!P->has_full) return fail(SDSB200_INVALID_VALUE, "the residual needs the full-pattern map of the plan");
+    if (nrhs < 1) return fail(SDSB200_INVALID_VALUE, "nrhs must be positive");
+    if (ldx < P->n || ldb < P->n) return fail(SDSB200_INVALID_VALUE, "leading dimension smaller than n");
+    if (!R || !X || !B || !nzval) return fail(SDSB200_INVALID_VALUE, "NULL array");
+    if (solve_mode < 0 || solve_mode > 2) return fail(SDSB200_INVALID_VALUE, "solve_mode must be 0, 1 or 2");
+    const bool transpose = P->structure == STRUCT_G && solve_mode != 0;
+    ResidualArgs r{};
+    r.members = P->all_members ? nullptr : P->d_members;
+    if (transpose) {
+        r.rowptr = P->d_fullT_rowptr; r.colval = P->d_fullT_colval; r.srcptr = P->d_fullT_srcptr; r.src = P->d_fullT_src;
+    } else {
+        r.rowptr = P->d_full_rowptr; r.colval = P->d_full_colval; r.srcptr = P->d_full_srcptr; r.src = P->d_full_src;
+    }
+    r.nzval = nzval; r.X = X; r.B = B; r.R = R;
+    r.n = P->n; r.nnz = P->nnz; r.ldx = ldx; r.ldb = ldb; r.nrhs = nrhs;
+    cudaError_t e = launch_residual(r, P->nact, (cudaStream_t)stream);
+    return e == cudaSuccess ? SDSB200_OK : cuda_fail(e, "residual");
+}
+
 extern "C" int sdsb200_sampled_outer(int64_t n, int64_t nnz, const void* rowptr, const void* colval,
                                      int32_t index_width, int32_t index_base, int32_t structure, int32_t view,
                                      const double* U, int64_t ldu, const double* V, int64_t ldv, int32_t ncols,

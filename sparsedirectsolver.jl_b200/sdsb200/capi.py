@@ -19,7 +19,7 @@ PIVOT_TYPE = {"A": 0, "N": 1, "C": 2, "R": 3, "D": 4, "L": 5, "B": 6}
 EXPORTS = ("sdsb200_default_opts", "sdsb200_plan_create", "sdsb200_plan_destroy", "sdsb200_factor", "sdsb200_solve",
            "sdsb200_get_stats", "sdsb200_get_pivots", "sdsb200_get_factor", "sdsb200_set_members",
            "sdsb200_set_interrupt", "sdsb200_set_graphs", "sdsb200_set_persistent", "sdsb200_set_profiling", "sdsb200_get_trace", "sdsb200_plan_stat", "sdsb200_last_error",
-           "sdsb200_solve_noalloc", "sdsb200_sampled_outer")
+           "sdsb200_solve_noalloc", "sdsb200_sampled_outer", "sdsb200_residual")
 
 
 class Symbolic(C.Structure):
@@ -66,6 +66,7 @@ def bind(lib):
         "sdsb200_get_trace": (C.c_int64, [P, P, C.c_int64]),
         "sdsb200_last_error": (C.c_char_p, []),
         "sdsb200_solve_noalloc": (C.c_int, [P, P, C.c_int64, P, C.c_int64, C.c_int32, C.c_int32, P, P]),
+        "sdsb200_residual": (C.c_int, [P, P, P, C.c_int64, P, C.c_int64, C.c_int32, P, C.c_int32, P]),
         "sdsb200_sampled_outer": (C.c_int, [C.c_int64, C.c_int64, P, P, C.c_int32, C.c_int32, C.c_int32, C.c_int32,
                                             P, C.c_int64, P, C.c_int64, C.c_int32, C.c_int32, C.c_double, P, P]),
     }

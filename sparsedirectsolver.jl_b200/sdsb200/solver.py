@@ -140,8 +140,8 @@ class DirectSolver:
             raise InvalidValueError("ir_n_steps must be nonnegative")
         if name == "solve_mode" and int(value) not in (0, 1, 2):
             raise InvalidValueError("solve_mode must be 0, 1 or 2")
-        if name == "ir_mode" and value not in ("plain",):
-            raise NotSupportedError(f"ir_mode {value!r} is not supported (plain iterative refinement only)")
+        if name == "ir_mode" and value not in ("plain", "ir", "fgmres"):
+            raise InvalidValueError(f"ir_mode must be \"ir\" or \"fgmres\", got {value!r}")
         if name == "factor_precision" and value not in (None, "fp64", "fp32", "float64", "float32"):
             raise InvalidValueError("factor_precision must be fp64 or fp32")
         if name == "pivot_sign" and value is not None:
@@ -331,12 +331,24 @@ class DirectSolver:
             nrhs = Bm.shape[2]
         Xcm = torch.empty_like(Bcm)
         o = self._opts()
+        fgmres = self.params["ir_mode"] == "fgmres" and o.ir_n_steps > 0
+        if fgmres:
+            # FGMRES-IR (fgmres_refine!, src/solve/refinement.jl:577-614): a plain solve, then the
+            # Krylov refinement on the host above the C ABI
+            if int(self.params["ubatch_index"]) >= 0:
+                raise NotSupportedError("ir_mode \"fgmres\" refines all batch members together")
+            fg_steps, fg_tol = int(o.ir_n_steps), float(o.ir_tol)
+            o.ir_n_steps = 0
         steps = C.c_int32(0)
         stream = torch.cuda.current_stream(self.device).cuda_stream
         _check(lib.sdsb200_solve(self._plan, C.c_void_p(Xcm.data_ptr()), n, C.c_void_p(Bcm.data_ptr()), n, nrhs,
                                  C.c_void_p(self.nzval.data_ptr()), C.byref(o), C.byref(steps),
                                  C.c_void_p(stream)), lib)
         self._ir_steps = int(steps.value) if o.ir_n_steps > 0 else -1
+        if fgmres:
+            from .refinement import fgmres_refine
+
+            self._ir_steps = fgmres_refine(self, Xcm, Bcm, nrhs, int(o.solve_mode), fg_steps, fg_tol)
         out = Xcm.t() if Xcm.dim() == 2 else Xcm.transpose(1, 2)
         out = out.reshape(Bt.shape)
         if X is not None:

@@ -276,3 +276,29 @@ def test_persistent_solve_matches_level_launches(torch_cuda, structure):
     k = len(xs) // 2
     for x1, x0 in zip(xs[:k], xs[k:]):
         assert np.abs(x1 - x0).max() <= 1e-10 * np.abs(x0).max()
+
+
+@pytest.mark.parametrize("case", ["SPD", "G", "G_T", "S"])
+def test_fgmres_refinement(torch_cuda, case):
+    # FGMRES-IR with the FP32 factor as right preconditioner reaches the FP64 accuracy target, and
+    # needs no more iterations than plain refinement
+    if case == "SPD":
+        A, st, kw = M.lap3d(16, 16, 16, seed=2), "SPD", dict(reordering_alg="nd")
+    elif case.startswith("G"):
+        A, st, kw = M.convection_diffusion3d(10, 10, 10, seed=2), "G", dict(pivot_threshold=0.1)
+    else:
+        A, st, kw = small_kkt(20, 20, 150, seed=2), "S", {}
+    transpose = case == "G_T"
+    b = M.rhs(A.shape[0], 2, seed=3)
+    its = {}
+    for mode in ("ir", "fgmres"):
+        ds = _solver(A, st, factor_precision="fp32", ir_mode=mode, ir_n_steps=10, ir_tol=1e-13, **kw)
+        ds.execute("analysis")
+        ds.execute("factorization")
+        if transpose:
+            ds.setparam("solve_mode", 1)
+        x = ds.execute("solve", None, b).cpu().numpy()
+        AA = A.T.tocsr() if transpose else A
+        assert M.scaled_backward_error(AA, x, b) <= BERR
+        its[mode] = ds.getparam("ir_n_steps")
+    assert 1 <= its["fgmres"] <= its["ir"]
