@@ -15,11 +15,7 @@ from __future__ import annotations
 
 from .capi import tuning as make_tuning
 
-CANDIDATES = (
-    (0, 0, 0), (128, 0, 0), (96, 0, 0),
-    (0, 64, 0), (0, 128, 0),
-    (0, 0, 16), (0, 0, 8), (0, 0, 4), (0, 64, 8), (0, 64, 4),
-)
+CANDIDATES = tuple((fs, wd, ar) for fs in (0, 128, 96) for wd in (0, 64) for ar in (0, 16))
 
 _cache: dict = {}
 
