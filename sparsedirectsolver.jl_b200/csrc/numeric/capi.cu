@@ -88,8 +88,6 @@ int prof_kind_of(LaunchKind k) {
     switch (k) {
         case L_SMALL: return PK_SMALL;
         case L_ASSEMBLE: return PK_ASSEMBLE;
-        case L_CHOL_PANEL: return PK_PANEL;
-        case L_CHOL_DIAG: return PK_PANEL;
         case L_CHOL_STEP: return PK_PANEL;
         case L_GEMM: return PK_GEMM;
         case L_PIVOT_FRONT: return PK_PIVOT;
@@ -202,17 +200,6 @@ int run_factor(Plan* P, const double* nzval, double eps, double u, int pivot, in
                 e = launch_assemble_large<T>(P->structure, a, nm, st);
                 break;
             }
-            case L_CHOL_PANEL: {
-                CholPanelArgs<T> a{};
-                a.fronts = P->d_fronts;
-                a.tasks = P->d_ptasks + L.list;
-                a.count = L.count;
-                a.members = members;
-                a.factor = factor; a.finfo = P->d_finfo; a.stats = P->d_stats;
-                a.factor_len = P->factor_len; a.ns = (int32_t)P->ns; a.kb = L.cls; a.eps = eps;
-                e = launch_chol_panel<T>(a, L.nb, nm, st);
-                break;
-            }
             case L_GEMM: {
                 GemmArgs<T> a{};
                 a.tiles = P->d_tiles + L.list;
@@ -250,21 +237,6 @@ int run_factor(Plan* P, const double* nzval, double eps, double u, int pivot, in
                 a.finfo = P->d_finfo; a.stats = P->d_stats;
                 a.factor_len = P->factor_len; a.ns = (int32_t)P->ns; a.kb = L.cls; a.eps = eps;
                 e = launch_chol_step<T>(a, nm, st);
-                break;
-            }
-            case L_CHOL_DIAG: {
-                CholDiagArgs<T> a{};
-                a.fronts = P->d_fronts;
-                a.list = P->d_lists + L.list;
-                a.inv_off = P->d_inv_off + L.maxw;
-                a.count = L.count;
-                a.members = members;
-                a.factor = factor;
-                a.inv = static_cast<T*>(P->d_inv);
-                a.inv_len = P->inv_len;
-                a.finfo = P->d_finfo; a.stats = P->d_stats;
-                a.factor_len = P->factor_len; a.ns = (int32_t)P->ns; a.kb = L.cls; a.eps = eps;
-                e = launch_chol_diag<T>(a, nm, st);
                 break;
             }
             case L_PIVOT_FRONT: {

@@ -56,8 +56,6 @@ struct GemmTile {
 enum LaunchKind : int32_t {
     L_SMALL = 1,       // fused small fronts (one CTA per front, front in shared memory)
     L_ASSEMBLE,        // column-task assembly of large fronts
-    L_CHOL_PANEL,      // large Cholesky: diagonal block + trsm of one column block (row-tile form)
-    L_CHOL_DIAG,       // large Cholesky: factor + invert the diagonal block of one column block
     L_GEMM,            // grouped GEMM tiles
     L_PIVOT_FRONT,     // large LDLT / LU: cooperative pivoting over the panel
     L_STATS,           // statistics reduction

@@ -2,16 +2,15 @@
 // cuBLAS trsm/syrk/gemm through src/dense/interface.jl and the KA fallbacks of
 // src/dense/fallback/, replaced here by hand-written kernels).
 //
-// * chol_panel_kernel: one column block of a large Cholesky front, in two
-//   launches: the diagonal mode factors the nb x nb diagonal block in shared
-//   memory and writes it back; the trsm mode solves one tile of rows below
-//   with it (trsm R, L, T). The static pivot clamp and the failure rule are
-//   the ones of the fused kernels.
-// * gemm_nt_kernel: grouped C -= A B^T over a list of tiles (Schur updates of
-//   the fully-summed columns and of the contribution block; "lower" tiles write
-//   only on or below the diagonal).
-// * large_pivot_kernel: LDLT / LU fronts beyond shared memory: one CTA runs the
-//   reference's in-front steps (front_factor.cuh) on the global panels.
+// * gemm_nt_dmma_kernel: grouped FP64 C -= A B^T over a list of 64 x 64 tiles on the DMMA tensor
+//   path (Schur updates of the fully-summed columns and of the contribution block; "lower" tiles
+//   write only on or below the diagonal; mode 2 tiles copy a deferred diagonal block). The FP32
+//   form uses the tcgen05 kernel of tc_kernels.cu.
+// * chol_step_kernel: one 32-column step of a large Cholesky front (diagonal block + trsm).
+// * block_inv_kernel: inverses of the 64 x 64 diagonal blocks of the solve's wide fronts.
+// * large_pivot_kernel / large_pivot_coop_kernel: LDLT / LU fronts beyond shared memory, the
+//   reference's in-front steps (front_factor.cuh) on the global panels, by one CTA or by a group of
+//   co-resident CTAs.
 // * scale_ld_kernel: W = L21 D for the contribution-block update of those fronts.
 #include <cuda_runtime.h>
 #include <math.h>
@@ -22,183 +21,6 @@
 #include "kernels.cuh"
 
 namespace sds {
-
-template <typename T, int NB>
-__global__ void __launch_bounds__(PANEL_ROWS) chol_panel_kernel(CholPanelArgs<T> A) {
-    __shared__ T L[NB][NB + 1];
-    __shared__ int s_status;
-    const PanelTask task = A.tasks[blockIdx.x];
-    const int member = A.members ? A.members[blockIdx.y] : blockIdx.y;
-    const int s = task.front;
-    const DFront fd = A.fronts[s];
-    int32_t* finfo = A.finfo + (int64_t)member * A.ns;
-    if (finfo[s] != 0) return;
-    const int f = fd.f, w = fd.w, kb = A.kb;
-    if (kb >= w) return;
-    const int nbb = min(NB, w - kb);
-    T* P = A.factor + (int64_t)member * A.factor_len + fd.panel;
-    const int tid = threadIdx.x;
-    for (int q = tid; q < NB * NB; q += blockDim.x) {
-        int i = q % NB, j = q / NB;
-        L[i][j] = (i < nbb && j < nbb && i >= j) ? P[(kb + i) + (int64_t)(kb + j) * f] : T(0);
-    }
-    if (tid == 0) s_status = 0;
-    __syncthreads();
-    if (task.row0 < 0) {
-        // diagonal mode: factor the block, write it back, record the status and the statistics
-        const double eps = A.eps;
-        for (int j = 0; j < nbb; ++j) {
-            double ajj = (double)L[j][j];
-            bool ok = ajj > eps || (eps > 0 && ajj >= 0);
-            if (!ok) {
-                if (tid == 0) s_status = j + 1;
-                break;
-            }
-            double djj = sqrt(fmax(ajj, eps));
-            T inv = T(1.0 / djj);
-            __syncthreads();
-            for (int i = j + 1 + tid; i < nbb; i += blockDim.x) L[i][j] *= inv;
-            if (tid == 0) L[j][j] = T(djj);
-            __syncthreads();
-            const int r = nbb - j - 1;
-            for (int q = tid; q < r * r; q += blockDim.x) {
-                int i = j + 1 + q % r, l = j + 1 + q / r;
-                if (i >= l) L[i][l] -= L[i][j] * L[l][j];
-            }
-            __syncthreads();
-        }
-        __syncthreads();
-        const int status = s_status;
-        for (int q = tid; q < nbb * nbb; q += blockDim.x) {
-            int i = q % nbb, j = q / nbb;
-            P[(kb + i) + (int64_t)(kb + j) * f] = i >= j ? L[i][j] : T(0);
-        }
-        if (tid == 0) {
-            int64_t* S = A.stats + ((int64_t)member * A.ns + s) * NSTAT;
-            if (status) {
-                finfo[s] = kb + status;
-                S[ST_NPOS] = kb + status - 1;
-                S[ST_INFO] = kb + status;
-            } else if (kb + nbb == w) {
-                S[ST_NPOS] = w;
-                S[ST_INFO] = 0;
-            }
-        }
-        return;
-    }
-    // trsm mode: the block was factored by the previous launch; solve X L11^T = B for this row tile
-    const int r = task.row0 + tid;
-    if (r >= f) return;
-    T x[NB];
-#pragma unroll
-    for (int j = 0; j < NB; ++j) x[j] = j < nbb ? P[r + (int64_t)(kb + j) * f] : T(0);
-#pragma unroll
-    for (int j = 0; j < NB; ++j) {
-        if (j < nbb) {
-            T acc = x[j];
-#pragma unroll
-            for (int l = 0; l < j; ++l) acc -= x[l] * L[j][l];
-            x[j] = acc / L[j][j];
-        }
-    }
-#pragma unroll
-    for (int j = 0; j < NB; ++j)
-        if (j < nbb) P[r + (int64_t)(kb + j) * f] = x[j];
-}
-
-template <typename T>
-cudaError_t launch_chol_panel(const CholPanelArgs<T>& a, int nb, int nmembers, cudaStream_t st) {
-    dim3 grid(a.count, nmembers);
-    if (nb == 32) chol_panel_kernel<T, 32><<<grid, PANEL_ROWS, 0, st>>>(a);
-    else chol_panel_kernel<T, 64><<<grid, PANEL_ROWS, 0, st>>>(a);
-    return cudaGetLastError();
-}
-
-template cudaError_t launch_chol_panel<double>(const CholPanelArgs<double>&, int, int, cudaStream_t);
-template cudaError_t launch_chol_panel<float>(const CholPanelArgs<float>&, int, int, cudaStream_t);
-
-// ---------------------------------------------------------------------------
-// Grouped C -= A B^T, 64 x 64 tiles, 256 threads, 4 x 4 outputs per thread.
-template <typename T>
-__global__ void __launch_bounds__(256) gemm_nt_kernel(GemmArgs<T> A) {
-    constexpr int BM = GEMM_BM, BN = GEMM_BN, BK = 16;
-    __shared__ T As[BK][BM + 1];
-    __shared__ T Bs[BK][BN + 1];
-    const GemmTile t = A.tiles[blockIdx.x];
-    const int member = A.members ? A.members[blockIdx.y] : blockIdx.y;
-    if (A.finfo && t.front >= 0 && A.finfo[(int64_t)member * A.ns + t.front] != 0) return;
-    if (t.mode == 2) {   // deferred diagonal-block write
-        const T* src = A.copy_src + (int64_t)member * A.copy_stride + t.a;
-        T* dst = A.cbuf + (int64_t)member * A.cstride + t.c;
-        for (int q = threadIdx.x; q < t.m * t.n; q += blockDim.x) dst[q % t.m + (int64_t)(q / t.m) * t.ldc] = src[q % t.m + (int64_t)(q / t.m) * t.lda];
-        return;
-    }
-    const T* Ab = A.abuf + (int64_t)member * A.astride + t.a;
-    const T* Bb = A.bbuf + (int64_t)member * A.bstride + t.b;
-    T* Cb = A.cbuf + (int64_t)member * A.cstride + t.c;
-    const int tid = threadIdx.x, tx = tid & 15, ty = tid >> 4;
-    T acc[4][4];
-#pragma unroll
-    for (int i = 0; i < 4; ++i)
-#pragma unroll
-        for (int j = 0; j < 4; ++j) acc[i][j] = T(0);
-    const int M = t.m, N = t.n, K = t.k;
-    for (int k0 = 0; k0 < K; k0 += BK) {
-        {
-            constexpr int QA = (BM * BK) / 256, QB = (BN * BK) / 256;
-            T va[QA], vb[QB];
-#pragma unroll
-            for (int q = 0; q < QA; ++q) {
-                int e = tid + 256 * q, r = e % BM, kk = e / BM;
-                va[q] = (r < M && k0 + kk < K) ? Ab[r + (int64_t)(k0 + kk) * t.lda] : T(0);
-            }
-#pragma unroll
-            for (int q = 0; q < QB; ++q) {
-                int e = tid + 256 * q, r = e % BN, kk = e / BN;
-                vb[q] = (r < N && k0 + kk < K) ? Bb[r + (int64_t)(k0 + kk) * t.ldb] : T(0);
-            }
-#pragma unroll
-            for (int q = 0; q < QA; ++q) As[(tid + 256 * q) / BM][(tid + 256 * q) % BM] = va[q];
-#pragma unroll
-            for (int q = 0; q < QB; ++q) Bs[(tid + 256 * q) / BN][(tid + 256 * q) % BN] = vb[q];
-        }
-        __syncthreads();
-#pragma unroll
-        for (int kk = 0; kk < BK; ++kk) {
-            T a[4], b[4];
-#pragma unroll
-            for (int i = 0; i < 4; ++i) a[i] = As[kk][tx + 16 * i];
-#pragma unroll
-            for (int j = 0; j < 4; ++j) b[j] = Bs[kk][ty + 16 * j];
-#pragma unroll
-            for (int i = 0; i < 4; ++i)
-#pragma unroll
-                for (int j = 0; j < 4; ++j) acc[i][j] += a[i] * b[j];
-        }
-        __syncthreads();
-    }
-    if (!t.mode) {
-        T cv[4][4];
-#pragma unroll
-        for (int i = 0; i < 4; ++i)
-#pragma unroll
-            for (int j = 0; j < 4; ++j) {
-                int r = tx + 16 * i, c = ty + 16 * j;
-                cv[i][j] = (r < M && c < N && r + t.diag >= c) ? Cb[r + (int64_t)c * t.ldc] : T(0);
-            }
-#pragma unroll
-        for (int i = 0; i < 4; ++i)
-#pragma unroll
-            for (int j = 0; j < 4; ++j) acc[i][j] = cv[i][j] - acc[i][j];
-    }
-#pragma unroll
-    for (int i = 0; i < 4; ++i)
-#pragma unroll
-        for (int j = 0; j < 4; ++j) {
-            int r = tx + 16 * i, c = ty + 16 * j;
-            if (r < M && c < N && r + t.diag >= c) Cb[r + (int64_t)c * t.ldc] = acc[i][j];
-        }
-}
 
 // FP64 on the tensor cores: mma.sync m8n8k4 (DMMA). 64 x 64 CTA tile, 4 warps of 32 x 32,
 // K in steps of 16 staged by cp.async into two shared-memory buffers.
@@ -212,7 +34,7 @@ template <int N>
 __device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N)); }
 
 __global__ void __launch_bounds__(128) gemm_nt_dmma_kernel(GemmArgs<double> A) {
-    constexpr int BM = 64, BN = 64, BK = 16, LDS = 72;
+    constexpr int BM = 64, BK = 16, LDS = 72;   // 64 x 64 tile
     __shared__ __align__(16) double As[2][BK][LDS];
     __shared__ __align__(16) double Bs[2][BK][LDS];
     const GemmTile t = A.tiles[blockIdx.x];
@@ -319,100 +141,9 @@ cudaError_t launch_gemm(const GemmArgs<T>& a, int nmembers, cudaStream_t st) {
     return cudaGetLastError();
 }
 
-// ---------------------------------------------------------------------------
-// Diagonal block of a large Cholesky front (32 x 32 at column kb): factor with the static clamp and
-// failure rule of the fused kernels, write L11 back, write inv(L11) (ld 32) to scratch for the trsm
-// of the rows below as a GEMM (X = B inv(L11)^T). One warp over a shared-memory copy of the block:
-// the factor is left-looking (lane i owns row i), the inverse is a forward substitution per column
-// (lane c owns column c). Each step is a short dot product with independent partial sums, so the
-// warp's dependent chain is one dot product plus one square root (or one multiply) per column.
-template <typename T>
-__global__ void __launch_bounds__(32) chol_diag_kernel(CholDiagArgs<T> A) {
-    constexpr int NB = CHOL_NB, LD = NB + 1;
-    static_assert(NB == 32, "one lane per row of the diagonal block");
-    __shared__ double L[NB * LD];
-    __shared__ double X[(NB + 1) * LD];   // the inverse, and its reciprocal diagonal in the last row
-    const int s = A.list[blockIdx.x];
-    const int member = A.members ? A.members[blockIdx.y] : blockIdx.y;
-    const DFront fd = A.fronts[s];
-    int32_t* finfo = A.finfo + (int64_t)member * A.ns;
-    if (finfo[s] != 0) return;
-    const int f = fd.f, w = fd.w, kb = A.kb;
-    if (kb >= w) return;
-    const int nbb = min(NB, w - kb);
-    T* P = A.factor + (int64_t)member * A.factor_len + fd.panel;
-    const int i = threadIdx.x;
-    batched_copy<8>(0, 1, NB,
-                    [&](int j) { return (i < nbb && j < nbb && j <= i) ? (double)P[(kb + i) + (int64_t)(kb + j) * f] : 0.0; },
-                    [&](int j, double v) { L[i * LD + j] = v; });
-    __syncwarp();
-    const double eps = A.eps;
-    int status = 0;
-    // left-looking by columns: lane i forms s_i = a_ij - sum_{l<j} L_il L_jl (row i against the
-    // broadcast row j, four independent partial sums), then L_ij = s_i / sqrt(s_j)
-    for (int j = 0; j < nbb; ++j) {
-        double a0 = 0.0, a1 = 0.0, a2 = 0.0, a3 = 0.0;
-        int l = 0;
-        for (; l + 4 <= j; l += 4) {
-            a0 += L[i * LD + l] * L[j * LD + l];
-            a1 += L[i * LD + l + 1] * L[j * LD + l + 1];
-            a2 += L[i * LD + l + 2] * L[j * LD + l + 2];
-            a3 += L[i * LD + l + 3] * L[j * LD + l + 3];
-        }
-        for (; l < j; ++l) a0 += L[i * LD + l] * L[j * LD + l];
-        const double sv = L[i * LD + j] - ((a0 + a1) + (a2 + a3));
-        const double ajj = __shfl_sync(0xffffffffu, sv, j);
-        if (!(ajj > eps || (eps > 0 && ajj >= 0))) {
-            status = j + 1;
-            break;
-        }
-        const double sd = sqrt(fmax(ajj, eps));
-        if (i == j) L[i * LD + j] = (double)T(sd);
-        else if (i > j && i < nbb) L[i * LD + j] = (double)T(sv / sd);
-        __syncwarp();
-    }
-    if (i < nbb)
-        for (int j = 0; j < nbb; ++j) P[(kb + i) + (int64_t)(kb + j) * f] = j <= i ? T(L[i * LD + j]) : T(0);
-    if (status) {
-        if (i == 0) {
-            int64_t* S = A.stats + ((int64_t)member * A.ns + s) * NSTAT;
-            finfo[s] = kb + status;
-            S[ST_NPOS] = kb + status - 1;
-            S[ST_INFO] = kb + status;
-        }
-        return;
-    }
-    if (i == 0 && kb + nbb == w) {
-        int64_t* S = A.stats + ((int64_t)member * A.ns + s) * NSTAT;
-        S[ST_NPOS] = w;
-        S[ST_INFO] = 0;
-    }
-    if (kb + nbb >= f) return;  // no rows below: no trsm
-    // inverse: lane c solves L x = e_c by forward substitution, x_r kept in X[r][c]; the reciprocal
-    // diagonal is formed once, and rows above c contribute zeros, so every lane runs the same loop
-    X[32 * LD + i] = i < nbb ? 1.0 / L[i * LD + i] : 0.0;
-    __syncwarp();
-    for (int r = 0; r < nbb; ++r) {
-        double a0 = 0.0, a1 = 0.0, a2 = 0.0, a3 = 0.0;
-        int l = 0;
-        for (; l + 4 <= r; l += 4) {
-            a0 += L[r * LD + l] * X[l * LD + i];
-            a1 += L[r * LD + l + 1] * X[(l + 1) * LD + i];
-            a2 += L[r * LD + l + 2] * X[(l + 2) * LD + i];
-            a3 += L[r * LD + l + 3] * X[(l + 3) * LD + i];
-        }
-        for (; l < r; ++l) a0 += L[r * LD + l] * X[l * LD + i];
-        const double rhs = (r == i ? 1.0 : 0.0) - ((a0 + a1) + (a2 + a3));
-        X[r * LD + i] = r >= i ? rhs * X[32 * LD + r] : 0.0;
-        __syncwarp();
-    }
-    T* inv = A.inv + (int64_t)member * A.inv_len + A.inv_off[blockIdx.x];
-    for (int j = 0; j < NB; ++j) inv[i + (int64_t)j * NB] = (i < nbb && j < nbb && j <= i) ? T(X[i * LD + j]) : T(0);
-}
-
 // One 32-column step of a large Cholesky front, diagonal block and trsm fused: every CTA factors the
-// 32 x 32 diagonal block and inverts it (warp 0, the arithmetic of chol_diag_kernel) while warps 1..3
-// stage its own 64-row tile of the rows below; the CTA then replaces the tile by X = B L11^{-T}.
+// 32 x 32 diagonal block (warp 0) while warps 1..3 stage its own 64-row tile of the rows below; the
+// CTA then replaces the tile by X = B L11^{-T}.
 // The diagonal block itself is read by every CTA of the step, so no CTA overwrites it: the head task
 // puts L11 in the scratch buffer and a copy tile of the next GEMM launch of the level writes it
 // into the panel (a diagonal block with no rows below is written directly by its only task).
@@ -545,7 +276,7 @@ template cudaError_t launch_chol_step<double>(const CholStepArgs<double>&, int, 
 template cudaError_t launch_chol_step<float>(const CholStepArgs<float>&, int, cudaStream_t);
 
 // inverse of one 64 x 64 diagonal block of a panel (lower triangle as stored; unit or not), with the
-// register-owned right-looking substitution of chol_diag_kernel
+// register-owned right-looking substitution
 template <typename T>
 __global__ void __launch_bounds__(256) block_inv_kernel(BlockInvArgs<T> A) {
     constexpr int NB = 64, NE = NB * (NB + 1) / 2, SLOTS = (NE + 255) / 256;
@@ -617,29 +348,10 @@ cudaError_t launch_block_inv(const BlockInvArgs<T>& a, int nmembers, cudaStream_
 template cudaError_t launch_block_inv<double>(const BlockInvArgs<double>&, int, cudaStream_t);
 template cudaError_t launch_block_inv<float>(const BlockInvArgs<float>&, int, cudaStream_t);
 
-template <typename T>
-cudaError_t launch_chol_diag(const CholDiagArgs<T>& a, int nmembers, cudaStream_t st) {
-    if (a.count == 0) return cudaSuccess;
-    dim3 grid(a.count, nmembers);
-    chol_diag_kernel<T><<<grid, 32, 0, st>>>(a);
-    return cudaGetLastError();
-}
-
 cudaError_t prepare_dense_kernels(int max_smem) {
-    cudaError_t e = cudaSuccess;
-    auto set = [&](const void* k) {
-        if (e != cudaSuccess) return;
-        cudaFuncAttributes fa;
-        e = cudaFuncGetAttributes(&fa, k);
-        if (e == cudaSuccess)
-            e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, max_smem - (int)fa.sharedSizeBytes);
-    };
-    (void)set;
-    return e;
+    (void)max_smem;   // the dense kernels use static shared memory only
+    return cudaSuccess;
 }
-
-template cudaError_t launch_chol_diag<double>(const CholDiagArgs<double>&, int, cudaStream_t);
-template cudaError_t launch_chol_diag<float>(const CholDiagArgs<float>&, int, cudaStream_t);
 
 template cudaError_t launch_gemm<double>(const GemmArgs<double>&, int, cudaStream_t);
 template cudaError_t launch_gemm<float>(const GemmArgs<float>&, int, cudaStream_t);

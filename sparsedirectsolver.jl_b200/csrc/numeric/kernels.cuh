@@ -53,44 +53,9 @@ struct StatsArgs {
 };
 
 // Large Cholesky column-block panel: diagonal block + trsm of the rows below.
-struct PanelTask {
-    int32_t front;
-    int32_t row0;   // first row of this CTA's row tile (>= kb + nb), or -1: the diagonal-block writer
-};
 
-template <typename T>
-struct CholPanelArgs {
-    const DFront* fronts;
-    const PanelTask* tasks;
-    int32_t count;
-    const int32_t* members;
-    T* factor;
-    int32_t* finfo;
-    int64_t* stats;
-    int64_t factor_len;
-    int32_t ns;
-    int32_t kb;     // first column of the block
-    double eps;
-};
 
 // Diagonal block of a large Cholesky front: factor in place and write its inverse (ld 64) to scratch.
-template <typename T>
-struct CholDiagArgs {
-    const DFront* fronts;
-    const int32_t* list;
-    const int64_t* inv_off;   // per listed front: offset of its 64 x 64 inverse in the scratch buffer
-    int32_t count;
-    const int32_t* members;
-    T* factor;
-    T* inv;                   // scratch, per member stride inv_len
-    int64_t inv_len;
-    int32_t* finfo;
-    int64_t* stats;
-    int64_t factor_len;
-    int32_t ns;
-    int32_t kb;
-    double eps;
-};
 
 // One task of a large-Cholesky step: a 64-row tile of the rows below the diagonal block of front
 // `front` (tile >= 0), or the diagonal block alone when no rows are below it (tile = -1). The task
@@ -190,11 +155,7 @@ template <typename T>
 cudaError_t launch_assemble_large(int structure, const LargeAsmArgs<T>& a, int nmembers, cudaStream_t st);
 cudaError_t launch_stats(const StatsArgs& a, int nmembers, cudaStream_t st);
 template <typename T>
-cudaError_t launch_chol_panel(const CholPanelArgs<T>& a, int nb, int nmembers, cudaStream_t st);
-template <typename T>
 cudaError_t launch_gemm(const GemmArgs<T>& a, int nmembers, cudaStream_t st);
-template <typename T>
-cudaError_t launch_chol_diag(const CholDiagArgs<T>& a, int nmembers, cudaStream_t st);
 // Inverses of the 64 x 64 diagonal blocks of the L11 panels of the wide fronts (for the solve)
 template <typename T>
 struct BlockInvArgs {
@@ -252,7 +213,6 @@ struct OuterArgs {
 template <typename I>
 cudaError_t launch_sampled_outer(const OuterArgs<I>& a, int nmembers, cudaStream_t st);
 
-constexpr int PANEL_ROWS = 128;  // rows of the trsm tile of a Cholesky panel CTA
 constexpr int GEMM_BM = 64, GEMM_BN = 64;
 
 }  // namespace sds

@@ -307,10 +307,8 @@ Plan* build_plan(const sdsb200_symbolic* sym, const sdsb200_plan_options* popts,
         std::vector<int32_t> lists;
         std::vector<CholStepTask> steptasks;
         std::vector<ColTask> coltasks;
-        std::vector<PanelTask> ptasks;
         std::vector<GemmTile> tiles;
-        std::vector<int64_t> scr_off, woff, inv_off;
-        const int NB = 32;
+        std::vector<int64_t> scr_off, woff;
         auto add_gemm_tiles = [&](int64_t a, int lda, int64_t b, int ldb, int64_t c, int ldc, int M, int N, int K,
                                   bool lower, int front) -> double {
             // algorithmic flops: 2 K per entry of C that is written (the lower trapezoid for SYRK-like updates)
@@ -725,12 +723,10 @@ Plan* build_plan(const sdsb200_symbolic* sym, const sdsb200_plan_options* popts,
         P->d_super0 = upload(P, P->h_super0, st);
         P->d_lists = upload(P, lists, st);
         P->d_coltasks = upload(P, coltasks, st);
-        P->d_ptasks = upload(P, ptasks, st);
         P->d_steptasks = upload(P, steptasks, st);
         P->d_tiles = upload(P, tiles, st);
         P->d_scr_off = upload(P, scr_off, st);
         P->d_woff = upload(P, woff, st);
-        P->d_inv_off = upload(P, inv_off, st);
         P->d_uoff = upload(P, uoff, st);
         P->d_level_lists = upload(P, level_lists, st);
         P->d_rect_tiles = upload(P, rect_tiles, st);

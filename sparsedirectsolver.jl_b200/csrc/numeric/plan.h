@@ -72,13 +72,11 @@ struct Plan {
     double* d_scratch = nullptr;
     void* d_work = nullptr;
     void* d_inv = nullptr;          // inverses of the diagonal blocks of large Cholesky fronts
-    int64_t* d_inv_off = nullptr;
     double* d_amax = nullptr;
 
     std::vector<ProgLaunch> prog;
     int32_t* d_lists = nullptr;
     ColTask* d_coltasks = nullptr;
-    PanelTask* d_ptasks = nullptr;
     GemmTile* d_tiles = nullptr;
     int64_t* d_scr_off = nullptr;
     CholStepTask* d_steptasks = nullptr; // tasks of the large-Cholesky step launches

@@ -302,3 +302,28 @@ def test_fgmres_refinement(torch_cuda, case):
         assert M.scaled_backward_error(AA, x, b) <= BERR
         its[mode] = ds.getparam("ir_n_steps")
     assert 1 <= its["fgmres"] <= its["ir"]
+
+
+def test_user_host_interrupt(torch_cuda):
+    # user_host_interrupt (src/logging.jl:60-63): a set host flag stops a factorization and a
+    # refinement loop with InterruptedError; cleared, the same plan factors and solves normally
+    import ctypes as C
+
+    from sdsb200.solver import InterruptedError_
+
+    flag = C.c_int32(0)
+    A = M.lap3d(12, 12, 12, seed=1)
+    ds = _solver(A, "SPD", user_host_interrupt=flag, ir_n_steps=3, ir_tol=0.0)
+    ds.execute("analysis")
+    flag.value = 1
+    with pytest.raises(InterruptedError_):
+        ds.execute("factorization")
+    flag.value = 0
+    assert ds.execute("factorization") == 0
+    b = M.rhs(A.shape[0], 1, seed=2)[:, 0]
+    flag.value = 1
+    with pytest.raises(InterruptedError_):
+        ds.execute("solve", None, b)
+    flag.value = 0
+    x = ds.execute("solve", None, b).cpu().numpy()
+    assert M.scaled_backward_error(A, x, b) <= BERR
