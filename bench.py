@@ -56,6 +56,8 @@ def parse():
                     help="c2 (default): lap3d_48 SPD, the headline line. The others print one line each for the "
                          "other workloads: c1 lap2d_64 SPD AMD, c3 KKT LDL^T (n = 55 000), c4 1024 uneven "
                          "systems, c4u uniform batch 96x96 x 256, c5 LU convection-diffusion 40^3 with A and A^T")
+    ap.add_argument("--tuning", default=None,
+                    help="fsmall,wide,area: fixed front tile shapes instead of the autotuner's search (for profilers)")
     ap.add_argument("--once", choices=["fp64", "mixed"], default=None,
                     help="one analysis + factorization + solve of the workload in one form, untimed (for profilers)")
     return ap.parse_args()
@@ -70,6 +72,10 @@ def run_once(args):
 
     A, b = workload(args.grid)
     kw = dict(factor_precision="fp32", ir_n_steps=20, ir_tol=BERR_TARGET) if args.once == "mixed" else {}
+    if args.tuning:
+        from sdsb200.capi import tuning as make_tuning
+
+        kw["tuning"] = make_tuning(*[int(v) for v in args.tuning.split(",")])
     ds = DirectSolver(A, "SPD", reordering_alg="nd", max_nrhs=NRHS, **kw)
     ds.execute("analysis")
     ds.execute("factorization")
@@ -444,8 +450,15 @@ def main():
         else:
             ds.execute("analysis")
         # front tile shapes picked by the autotuner (outside the timed region, like the analysis)
-        times = autotune(ds, Bt, reps=2, use_cache=False)
-        tuned[name] = describe(min(times, key=times.get))
+        if args.tuning:
+            from sdsb200.capi import tuning as make_tuning
+
+            ds.setparam("tuning", make_tuning(*[int(v) for v in args.tuning.split(",")]))
+            ds.replan()
+            tuned[name] = describe(ds.params["tuning"])
+        else:
+            times = autotune(ds, Bt, reps=2, use_cache=False)
+            tuned[name] = describe(min(times, key=times.get))
         solvers[name] = ds
     S = solvers["fp64"].symbolic
     flops = S.flops + 4.0 * S.nnz_stored * NRHS
