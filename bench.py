@@ -99,6 +99,16 @@ def _time(torch, fn, steps, warmup):
     return e0.elapsed_time(e1) / steps
 
 
+def max_over_ranks(value, dist, device):
+    """The largest value over the ranks of the process group (each replica's step time; the job's
+    time is the slowest replica's)."""
+    import torch
+
+    t = torch.tensor([float(value)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
 def run_config(args):
     """One JSON line for a workload other than the headline one (FP64 and mixed forms side by side)."""
     import torch
@@ -501,9 +511,7 @@ def main():
             torch.cuda.synchronize()
         ms = e0.elapsed_time(e1) / args.steps
         if dist:
-            t = torch.tensor([ms], device="cuda")
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            ms = float(t.item())
+            ms = max_over_ranks(ms, dist, "cuda")
         x = Xd.t().cpu().numpy()
         berr = M.scaled_backward_error(A, x, b)
         results[name] = dict(ms=ms, gflops=world * flops / (ms / 1e3) / 1e9, berr=berr, ir_steps=irsteps[-1],
@@ -578,6 +586,8 @@ def main():
         e1.record()
         torch.cuda.synchronize()
         ms_e2e = e0.elapsed_time(e1) / args.steps
+        if dist:
+            ms_e2e = max_over_ranks(ms_e2e, dist, "cuda")
         berr_e2e = M.scaled_backward_error(A, x_host.numpy(), b)
         e2e = {"value": round(world * flops / (ms_e2e / 1e3) / 1e9, 3), "unit": "GFLOP/s",
                "ms_per_step": round(ms_e2e, 3), "h2d_bytes_per_step": int(8 * (A.nnz + n * NRHS)),
