@@ -483,10 +483,13 @@ __global__ void __launch_bounds__(COOP_THREADS) large_pivot_coop_kernel(LargePiv
     sc.kd = reinterpret_cast<signed char*>(sc.ctl + 16);
     unsigned int* bar = G.bar + fi;
     unsigned int epoch = 0;
-    const int tid = threadIdx.x, nt = blockDim.x, lane = tid & 31, warp = tid >> 5;
+    const int tid = threadIdx.x, nt = blockDim.x, lane = tid & 31;
     const int gt = rank * nt + tid, GT = gs * nt, gw = gt >> 5, GW = GT >> 5;
     const bool lead = rank == 0 && tid == 0;
     GlobalStore<T, GEN> F{P, U, f, w};
+    __shared__ double team_red[COOP_THREADS / 32];
+    __shared__ int team_redi[COOP_THREADS / 32];
+    const CtaTeam team{tid, nt, team_red, team_redi};
     if (STRUCT == STRUCT_S) {
         for (int q = gt; q < w * w; q += GT) {
             const int i = q % w, j = q / w;
@@ -499,10 +502,10 @@ __global__ void __launch_bounds__(COOP_THREADS) large_pivot_coop_kernel(LargePiv
     if (STRUCT == STRUCT_S) {
         int k = 0;
         while (k < w) {
-            if (rank == 0 && warp == 0) {
+            if (rank == 0) {   // the whole first CTA takes the decision (row scans split over its threads)
                 int c, r;
-                choose_pivot_w(F, k, w, A.pivot, A.u, A.eps, lane, c, r);
-                if (lane == 0) { sc.ctl[0] = c; sc.ctl[1] = r; }
+                choose_pivot(F, k, w, A.pivot, A.u, A.eps, team, c, r);
+                if (tid == 0) { sc.ctl[0] = c; sc.ctl[1] = r; }
             }
             group_barrier(bar, epoch, gs, G.status);
             const int c = sc.ctl[0], r = sc.ctl[1];
@@ -585,9 +588,9 @@ __global__ void __launch_bounds__(COOP_THREADS) large_pivot_coop_kernel(LargePiv
     } else {
         const bool pivoting = A.lu_pivot != 0;
         for (int k = 0; k < w; ++k) {
-            if (rank == 0 && warp == 0) {
-                int r = pivoting ? lu_choose_row_w(F, k, w, A.u, lane) : k;
-                if (lane == 0) sc.ctl[0] = r;
+            if (rank == 0) {
+                int r = pivoting ? lu_choose_row(F, k, w, A.u, team) : k;
+                if (tid == 0) sc.ctl[0] = r;
             }
             group_barrier(bar, epoch, gs, G.status);
             const int r = sc.ctl[0];

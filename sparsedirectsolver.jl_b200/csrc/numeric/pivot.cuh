@@ -1,5 +1,5 @@
 // Pivot decisions of the in-front LDLT (Bunch-Kaufman) and LU (threshold partial
-// pivoting), run by one warp over a front accessor. They restate the reference's
+// pivoting), run by one warp or one CTA over a front accessor. They restate the reference's
 // decision sequence exactly (SparseDirectSolver.jl src/reference/ldlt.jl:254-355,
 // src/reference/lu.jl:216-231), including its NaN semantics: Julia's max
 // propagates NaN, so a NaN in a scanned column fails the threshold tests, and a
@@ -30,33 +30,82 @@ __device__ __forceinline__ void warp_argmax(double& v, int& idx) {
     }
 }
 
+// Teams: the threads that take a pivot decision together. Every thread of a team runs the same
+// decision sequence on the same values; only the scans over rows are split among them and reduced.
+// Max and first-index arg-max are exact in any order (jmax propagates NaN whatever the order), so a
+// warp team and a CTA team take identical decisions.
+struct WarpTeam {
+    int rank;                      // lane
+    static constexpr int size = 32;
+    __device__ double reduce_jmax(double v) const { return warp_jmax(v); }
+    __device__ void reduce_argmax(double& v, int& idx) const { warp_argmax(v, idx); }
+};
+
+// all threads of a CTA (every thread must take part in every reduction); red, redi: shared scratch
+// of blockDim.x / 32 entries
+struct CtaTeam {
+    int rank, size;
+    double* red;
+    int* redi;
+    __device__ double reduce_jmax(double v) const {
+        v = warp_jmax(v);
+        __syncthreads();
+        if ((rank & 31) == 0) red[rank >> 5] = v;
+        __syncthreads();
+        double r = red[0];
+        for (int w = 1; w < (size >> 5); ++w) r = jmax(r, red[w]);
+        return r;
+    }
+    __device__ void reduce_argmax(double& v, int& idx) const {
+        warp_argmax(v, idx);
+        __syncthreads();
+        if ((rank & 31) == 0) {
+            red[rank >> 5] = v;
+            redi[rank >> 5] = idx;
+        }
+        __syncthreads();
+        double bv = red[0];
+        int bi = redi[0];
+        for (int w = 1; w < (size >> 5); ++w) {
+            const double ov = red[w];
+            const int oi = redi[w];
+            if ((ov > bv) || (ov == bv && oi >= 0 && (bi < 0 || oi < bi))) {
+                bv = ov;
+                bi = oi;
+            }
+        }
+        v = bv;
+        idx = bi;
+    }
+};
+
 // Front accessor interface: F(i, j) returns the current value (double) of entry (i, j).
 // Acc must provide: double get(int i, int j) const; int f; int w.
 
 // max |F[i, c]| over rows k..f-1, skipping c and skip (Julia max semantics)
-template <class Acc>
-__device__ double colmax_w(const Acc& F, int c, int k, int skip, int lane) {
+template <class Acc, class Team>
+__device__ double colmax(const Acc& F, int c, int k, int skip, const Team& tm) {
     double m = 0.0;
-    for (int i = k + lane; i < F.f; i += 32) {
+    for (int i = k + tm.rank; i < F.f; i += tm.size) {
         if (i == c || i == skip) continue;
         m = jmax(m, fabs(F.get(i, c)));
     }
-    return warp_jmax(m);
+    return tm.reduce_jmax(m);
 }
 
 // d >= u * max_{i != c, i >= k} |F[i, c]| with the reference's early-exit semantics
 // (equivalent to: no NaN in the column and the test on the maximum)
-template <class Acc>
-__device__ bool threshold_ok_w(const Acc& F, int c, int k, double u, double d, int lane) {
-    double m = colmax_w(F, c, k, -1, lane);
+template <class Acc, class Team>
+__device__ bool threshold_ok(const Acc& F, int c, int k, double u, double d, const Team& tm) {
+    double m = colmax(F, c, k, -1, tm);
     return d >= u * m;
 }
 
-template <class Acc>
-__device__ bool accept_1x1_w(const Acc& F, int c, int k, double u, double eps, int lane) {
+template <class Acc, class Team>
+__device__ bool accept_1x1(const Acc& F, int c, int k, double u, double eps, const Team& tm) {
     double d = fabs(F.get(c, c));
     if (!(d >= eps)) return false;
-    return threshold_ok_w(F, c, k, u, d, lane);
+    return threshold_ok(F, c, k, u, d, tm);
 }
 
 template <class Acc>
@@ -67,41 +116,41 @@ __device__ bool nonsingular_2x2_w(const Acc& F, int k, int r, double eps) {
     return det != 0.0 && isfinite(det) && mx >= eps;
 }
 
-template <class Acc>
-__device__ bool accept_2x2_w(const Acc& F, int k, int r, double u, double eps, int lane) {
+template <class Acc, class Team>
+__device__ bool accept_2x2(const Acc& F, int k, int r, double u, double eps, const Team& tm) {
     if (!nonsingular_2x2_w(F, k, r, eps)) return false;
     double akk = F.get(k, k), arr = F.get(r, r), akr = F.get(k, r), ark = F.get(r, k);
     double det = akk * arr - akr * ark;
     double e11 = fabs(arr / det), e12 = fabs(akr / det), e21 = fabs(ark / det), e22 = fabs(akk / det);
-    double m1 = colmax_w(F, k, k, r, lane), m2 = colmax_w(F, r, k, k, lane);
+    double m1 = colmax(F, k, k, r, tm), m2 = colmax(F, r, k, k, tm);
     return u * (e11 * m1 + e21 * m2) <= 1.0 && u * (e12 * m1 + e22 * m2) <= 1.0;
 }
 
 // acceptable 1x1 pivot of the block k..w-1 with the largest |a_jj|, first on ties; -1 if none
-template <class Acc>
-__device__ int best_1x1_w(const Acc& F, int k, int w, double u, double eps, int lane) {
+template <class Acc, class Team>
+__device__ int best_1x1(const Acc& F, int k, int w, double u, double eps, const Team& tm) {
     int best = -1;
     double bv = 0.0;
     for (int j = k; j < w; ++j) {
         double a = fabs(F.get(j, j));
         if (!(a >= eps)) continue;
         if (best >= 0 && !(a > bv)) continue;
-        if (!threshold_ok_w(F, j, k, u, a, lane)) continue;
+        if (!threshold_ok(F, j, k, u, a, tm)) continue;
         best = j;
         bv = a;
     }
     return best;
 }
 
-// Pivot choice at column k: sets c (1x1 at c, r = -1) or the 2x2 on (k, r). Warp-uniform result.
-template <class Acc>
-__device__ void choose_pivot_w(const Acc& F, int k, int w, int pivot, double u, double eps, int lane, int& c_out,
-                               int& r_out) {
+// Pivot choice at column k: sets c (1x1 at c, r = -1) or the 2x2 on (k, r). Team-uniform result.
+template <class Acc, class Team>
+__device__ void choose_pivot(const Acc& F, int k, int w, int pivot, double u, double eps, const Team& tm,
+                             int& c_out, int& r_out) {
     r_out = -1;
     if (pivot == PIVOT_NONE) { c_out = k; return; }
     if (pivot == PIVOT_DIAGONAL) {
-        if (accept_1x1_w(F, k, k, u, eps, lane)) { c_out = k; return; }
-        int best = best_1x1_w(F, k, w, u, eps, lane);
+        if (accept_1x1(F, k, k, u, eps, tm)) { c_out = k; return; }
+        int best = best_1x1(F, k, w, u, eps, tm);
         if (best >= 0) { c_out = best; return; }
         int big = k;
         for (int j = k + 1; j < w; ++j)
@@ -112,27 +161,27 @@ __device__ void choose_pivot_w(const Acc& F, int k, int w, int pivot, double u, 
     const double alpha = (1.0 + sqrt(17.0)) / 8.0;
     double lambda = 0.0;
     int r = -1;
-    for (int i = k + 1 + lane; i < w; i += 32) {
+    for (int i = k + 1 + tm.rank; i < w; i += tm.size) {
         double a = fabs(F.get(i, k));
         if (a > lambda) { lambda = a; r = i; }
     }
-    warp_argmax(lambda, r);
+    tm.reduce_argmax(lambda, r);
     double akk = fabs(F.get(k, k));
     int bc = k, br = -1;
     if (r < 0 || akk >= alpha * lambda) {
         bc = k;
     } else {
         double sigma = 0.0;
-        for (int i = k + lane; i < w; i += 32)
+        for (int i = k + tm.rank; i < w; i += tm.size)
             if (i != r) sigma = jmax(sigma, fabs(F.get(i, r)));
-        sigma = warp_jmax(sigma);
+        sigma = tm.reduce_jmax(sigma);
         if (akk * sigma >= alpha * lambda * lambda) bc = k;
         else if (fabs(F.get(r, r)) >= alpha * sigma) bc = r;
         else { bc = k; br = r; }
     }
-    bool acc = br < 0 ? accept_1x1_w(F, bc, k, u, eps, lane) : accept_2x2_w(F, k, br, u, eps, lane);
+    bool acc = br < 0 ? accept_1x1(F, bc, k, u, eps, tm) : accept_2x2(F, k, br, u, eps, tm);
     if (acc) { c_out = bc; r_out = br; return; }
-    int best = best_1x1_w(F, k, w, u, eps, lane);
+    int best = best_1x1(F, k, w, u, eps, tm);
     if (best >= 0) { c_out = best; return; }
     if (br >= 0 && nonsingular_2x2_w(F, k, br, eps)) { c_out = bc; r_out = br; return; }
     c_out = bc;
@@ -140,23 +189,35 @@ __device__ void choose_pivot_w(const Acc& F, int k, int w, int pivot, double u, 
 
 // LU row choice (lu.jl:216-231): the diagonal if |F[k,k]| >= u max_{i>=k} |F[i,k]|,
 // else the first fully-summed row with the largest |F[r,k]|.
-template <class Acc>
-__device__ int lu_choose_row_w(const Acc& F, int k, int w, double u, int lane) {
+template <class Acc, class Team>
+__device__ int lu_choose_row(const Acc& F, int k, int w, double u, const Team& tm) {
     double g = 0.0;
-    for (int i = k + lane; i < F.f; i += 32) g = jmax(g, fabs(F.get(i, k)));
-    g = warp_jmax(g);
+    for (int i = k + tm.rank; i < F.f; i += tm.size) g = jmax(g, fabs(F.get(i, k)));
+    g = tm.reduce_jmax(g);
     double akk = fabs(F.get(k, k));
     if (akk >= u * g) return k;
     double best = -1.0;
     int r = -1;
-    for (int i = k + 1 + lane; i < w; i += 32) {
+    for (int i = k + 1 + tm.rank; i < w; i += tm.size) {
         double a = fabs(F.get(i, k));
         if (a > best) { best = a; r = i; }
     }
-    warp_argmax(best, r);
+    tm.reduce_argmax(best, r);
     // the reference starts from (k, akk) and takes a row only when strictly larger
     if (r >= 0 && best > akk) return r;
     return k;
+}
+
+// one-warp entry points (lane = the calling thread's lane)
+template <class Acc>
+__device__ void choose_pivot_w(const Acc& F, int k, int w, int pivot, double u, double eps, int lane, int& c_out,
+                               int& r_out) {
+    choose_pivot(F, k, w, pivot, u, eps, WarpTeam{lane}, c_out, r_out);
+}
+
+template <class Acc>
+__device__ int lu_choose_row_w(const Acc& F, int k, int w, double u, int lane) {
+    return lu_choose_row(F, k, w, u, WarpTeam{lane});
 }
 
 }  // namespace sds
