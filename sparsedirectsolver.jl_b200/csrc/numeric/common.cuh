@@ -29,8 +29,11 @@ struct DFront {
     int32_t amcol_begin;       // per-column start of the assembly entries: amcol[amcol_begin + j], j <= w
     int32_t eacol_begin;       // column-owner extend-add lists of a large front: eacol[eacol_begin + p], p <= f
     int32_t level;
-    int32_t pad;
+    int32_t rc_begin;  // this front's row-chunk starts among its parent's rows: rchunk[rc_begin + k], k <= K
 };
+
+// Rows of a front column that the large-front assembly builds at a time in shared memory (per warp)
+constexpr int ASM_ROWS = 256;
 
 // Column task of the large-front assembly: (front, parent index p); one warp each.
 struct ColTask {
@@ -83,6 +86,8 @@ struct DeviceMaps {
     const int32_t* amcol;    // per-column starts of the assembly entries
     const int32_t* ea;       // extend-add pairs (child, t) packed as 2 int32
     const int32_t* eacol;    // per parent index starts into ea
+    const int32_t* rchunk;   // per child of a large front: the first of its relind rows at or beyond each
+                             // multiple of ASM_ROWS of the parent's rows (K + 1 entries, K = ceil(f / ASM_ROWS))
     const int32_t* rowval;   // 0-based
     const int32_t* perm;     // 0-based
 };

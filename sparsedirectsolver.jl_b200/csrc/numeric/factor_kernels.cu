@@ -15,9 +15,9 @@
 // (src/reference/*.jl) step by step.
 //
 // assemble_large_kernel: column-owner assembly of the fronts too large for
-// shared memory: one warp per (front, parent index p) zeroes the storage it
-// owns, adds the entries of A of that column and pulls every child's
-// contribution in child order. No atomics.
+// shared memory: one warp per (front, parent index p) builds the column it
+// owns in row chunks from the entries of A of that column and every child's
+// contribution, in child order. No atomics.
 #include <cuda_runtime.h>
 #include <math.h>
 #include <stdint.h>
@@ -239,86 +239,142 @@ template cudaError_t launch_small<float>(int, const SmallArgs<float>&, int, int,
 // both triangles of the fully-summed block -- ; "G" keeps F[j, i] (i > j, j < w)
 // in the U^T panel at ufactor[panel + i + j f]; the contribution block
 // F[w:f, w:f] lives at cb (ld m).
+//
+// A warp builds its column ASM_ROWS rows at a time in shared memory: the chunk
+// starts at zero, takes the column's entries of A, then the rows of every
+// child's contribution that land in it (the child's row-chunk table gives their
+// range, relind being increasing) in the order of the column's extend-add list,
+// and is written once. Every entry receives the same additions in the same
+// order as a zero fill followed by accumulation in place, at one write of the
+// entry instead of a write, a read and a write.
+constexpr int ASM_WARPS = 8;
+constexpr int ASM_KIDS = 8;   // child descriptors a warp keeps in shared memory per column
+
+template <typename T>
+struct AsmChild {
+    const T* col;      // column t of the child's contribution block
+    const int* ri;     // the child's relind
+    const int* rc;     // the child's row-chunk starts
+    int t, mc;
+};
+
+// buf[ri[q] - r0] += val(q) for q in [q0, q1) (lanes strided; the targets of one call are distinct);
+// eight loads in flight per lane before the shared-memory updates
+template <class T, class VAL>
+__device__ __forceinline__ void chunk_add(T* buf, int r0, int q0, int q1, const int* ri, int lane, VAL val) {
+    constexpr int U = ASM_ROWS / 32;
+    for (int qb = q0 + lane; qb < q1; qb += 32 * U) {
+        int pos[U];
+        double v[U];
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+            const int q = qb + 32 * u;
+            pos[u] = q < q1 ? ri[q] - r0 : -1;
+            v[u] = q < q1 ? val(q) : 0.0;
+        }
+#pragma unroll
+        for (int u = 0; u < U; ++u)
+            if (pos[u] >= 0) buf[pos[u]] = T((double)buf[pos[u]] + v[u]);
+    }
+}
+
 template <typename T, int STRUCT>
-__global__ void assemble_large_kernel(LargeAsmArgs<T> A) {
-    const int task = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+__global__ void __launch_bounds__(ASM_WARPS * 32) assemble_large_kernel(LargeAsmArgs<T> A) {
+    constexpr bool GEN = STRUCT == STRUCT_G;
+    __shared__ T lbuf[ASM_WARPS][ASM_ROWS];
+    __shared__ T ubuf[GEN ? ASM_WARPS : 1][GEN ? ASM_ROWS : 1];
+    __shared__ AsmChild<T> kids[ASM_WARPS][ASM_KIDS];
+    const int wid = threadIdx.x >> 5;
+    const int task = blockIdx.x * ASM_WARPS + wid;
     const int lane = threadIdx.x & 31;
     if (task >= A.count) return;
     const int member = A.members ? A.members[blockIdx.y] : blockIdx.y;
     const ColTask ct = A.tasks[task];
     const DFront fd = A.maps.fronts[ct.front];
     const int f = fd.f, w = fd.w, m = f - w, p = ct.p;
+    const bool panel = p < w;
+    if (!panel && fd.cb < 0) return;
     const double* nz = A.nzval + (int64_t)member * A.nnz;
-    T* factor = A.factor + (int64_t)member * A.factor_len;
-    T* ufac = STRUCT == STRUCT_G ? A.ufactor + (int64_t)member * A.factor_len : nullptr;
     const T* cbar = A.cb + (int64_t)member * A.cb_len;
-    T* cbown = A.cb + (int64_t)member * A.cb_len + fd.cb;
-    if (p < w) {
-        T* col = factor + fd.panel + (int64_t)p * f;
-        for (int i = lane; i < f; i += 32) col[i] = T(0);
-        if (STRUCT == STRUCT_G) {
-            T* ucol = ufac + fd.panel + (int64_t)p * f;
-            for (int i = lane; i < f; i += 32) ucol[i] = T(0);
+    // the column indexed by front row: panel rows 0..f-1; contribution-block rows w..f-1 (from p for
+    // the lower triangle of "SPD" and "S")
+    T* lcol = panel ? A.factor + (int64_t)member * A.factor_len + fd.panel + (int64_t)p * f
+                    : A.cb + (int64_t)member * A.cb_len + fd.cb + (int64_t)(p - w) * m - w;
+    T* ucol = GEN && panel ? A.ufactor + (int64_t)member * A.factor_len + fd.panel + (int64_t)p * f : nullptr;
+    const int rfirst = panel ? 0 : (GEN ? w : p);
+    const int a0 = panel ? A.maps.amcol[fd.amcol_begin + p] : 0;
+    const int a1 = panel ? A.maps.amcol[fd.amcol_begin + p + 1] : 0;
+    const int e0 = A.maps.eacol[fd.eacol_begin + p], e1 = A.maps.eacol[fd.eacol_begin + p + 1];
+    AsmChild<T>* kd = kids[wid];
+    auto child = [&](int e) {
+        AsmChild<T> k;
+        const int c = A.maps.ea[2 * e];
+        k.t = A.maps.ea[2 * e + 1];
+        const DFront cd = A.maps.fronts[c];
+        k.mc = cd.f - cd.w;
+        k.col = cbar + cd.cb + (int64_t)k.t * k.mc;
+        k.ri = A.maps.relind + cd.ri_begin;
+        k.rc = A.maps.rchunk + cd.rc_begin;
+        return k;
+    };
+    if (lane < ASM_KIDS && e0 + lane < e1) kd[lane] = child(e0 + lane);
+    T* lb = lbuf[wid];
+    T* ub = GEN ? ubuf[wid] : nullptr;
+    __syncwarp();
+    for (int r0 = rfirst; r0 < f;) {
+        const int k = r0 / ASM_ROWS;
+        const int r1 = min(f, (k + 1) * ASM_ROWS);
+        const int len = r1 - r0;
+        for (int i = lane; i < len; i += 32) {
+            lb[i] = T(0);
+            if (GEN && panel) ub[i] = T(0);
         }
         __syncwarp();
-        const int a0 = A.maps.amcol[fd.amcol_begin + p], a1 = A.maps.amcol[fd.amcol_begin + p + 1];
-        for (int k = a0 + lane; k < a1; k += 32) {
-            int code = A.maps.am_loc[k];
-            if (k > a0 && A.maps.am_loc[k - 1] == code) continue;
+        // entries of A (runs of one location summed first, as the reference's assembly map lists them)
+        for (int q = a0 + lane; q < a1; q += 32) {
+            const int code = A.maps.am_loc[q];
+            if (q > a0 && A.maps.am_loc[q - 1] == code) continue;
+            const int row = (code > 0 ? code : -code) - 1 - p * f;
+            if (row < r0 || row >= r1) continue;
             T acc = T(0);
-            for (int q = k; q < a1 && A.maps.am_loc[q] == code; ++q) acc += T(nz[A.maps.am_src[q]]);
-            int loc = (code > 0 ? code : -code) - 1;
-            if (code > 0) factor[fd.panel + loc] += acc;
-            else ufac[fd.panel + loc] += acc;
+            for (int z = q; z < a1 && A.maps.am_loc[z] == code; ++z) acc += T(nz[A.maps.am_src[z]]);
+            if (code > 0) lb[row - r0] += acc;
+            else ub[row - r0] += acc;
         }
-    } else {
-        if (fd.cb < 0) return;
-        T* col = cbown + (int64_t)(p - w) * m;
-        for (int i = (STRUCT == STRUCT_G ? 0 : p - w) + lane; i < m; i += 32) col[i] = T(0);
-    }
-    __syncwarp();
-    const int e0 = A.maps.eacol[fd.eacol_begin + p], e1 = A.maps.eacol[fd.eacol_begin + p + 1];
-    for (int e = e0; e < e1; ++e) {
-        const int c = A.maps.ea[2 * e], t = A.maps.ea[2 * e + 1];
-        const DFront cd = A.maps.fronts[c];
-        const int mc = cd.f - cd.w;
-        const T* C = cbar + cd.cb;
-        const int* ri = A.maps.relind + cd.ri_begin;
-        // lower part: C[ii, t], ii >= t  ->  F[ri[ii], p]
-        batched_add<8, T>(t + lane, 32, mc, [&](int ii) { return (double)C[ii + (int64_t)t * mc]; },
-                          [&](int ii) -> T* {
-                              const int pi = ri[ii];
-                              if (p < w) return factor + fd.panel + pi + (int64_t)p * f;
-                              return pi >= w ? cbown + (pi - w) + (int64_t)(p - w) * m : nullptr;
-                          });
-        if (STRUCT == STRUCT_G) {
-            if (p < w) {
-                // upper part of row p: C[t, jj], jj > t  ->  F[p, ri[jj]] = U^T panel (ri[jj], p)
-                batched_add<8, T>(t + 1 + lane, 32, mc, [&](int jj) { return (double)C[t + (int64_t)jj * mc]; },
-                                  [&](int jj) -> T* { return ufac + fd.panel + ri[jj] + (int64_t)p * f; });
-            } else {
-                // rows of the contribution block above its diagonal: C[ii, t] with w <= ri[ii] < p
-                batched_add<8, T>(lane, 32, t, [&](int ii) { return (double)C[ii + (int64_t)t * mc]; },
-                                  [&](int ii) -> T* {
-                                      const int pi = ri[ii];
-                                      return pi >= w ? cbown + (pi - w) + (int64_t)(p - w) * m : nullptr;
-                                  });
+        __syncwarp();
+        for (int e = e0; e < e1; ++e) {
+            const AsmChild<T> c = e - e0 < ASM_KIDS ? kd[e - e0] : child(e);
+            const int lo = c.rc[k], hi = c.rc[k + 1];
+            // column t of the child: its rows from the diagonal down land in column p; "G" contribution
+            // block columns also take the rows above the diagonal (those below front row w are skipped by
+            // the chunk bounds: they belong to the U^T panel)
+            const int qb = (GEN && !panel) ? lo : max(lo, c.t);
+            const T* col = c.col;
+            chunk_add(lb, r0, qb, hi, c.ri, lane, [&](int q) { return (double)col[q]; });
+            if (GEN && panel) {
+                // row t of the child right of its diagonal: F[p, ri[jj]], the U^T panel column p
+                const T* row = col - (int64_t)c.t * c.mc + c.t;
+                const int64_t mcl = c.mc;
+                chunk_add(ub, r0, max(lo, c.t + 1), hi, c.ri, lane, [&](int q) { return (double)row[q * mcl]; });
             }
+            __syncwarp();
         }
-    }
-    if (STRUCT == STRUCT_S && p < w) {
-        // mirror of the fully-summed block happens after all columns are assembled (panel kernel)
+        for (int i = lane; i < len; i += 32) {
+            lcol[r0 + i] = lb[i];
+            if (GEN && panel) ucol[r0 + i] = ub[i];
+        }
+        __syncwarp();
+        r0 = r1;
     }
 }
 
 template <typename T>
 cudaError_t launch_assemble_large(int structure, const LargeAsmArgs<T>& a, int nmembers, cudaStream_t st) {
-    const int warps = 8;
-    dim3 grid((a.count + warps - 1) / warps, nmembers);
+    dim3 grid((a.count + ASM_WARPS - 1) / ASM_WARPS, nmembers);
     switch (structure) {
-        case STRUCT_SPD: assemble_large_kernel<T, STRUCT_SPD><<<grid, warps * 32, 0, st>>>(a); break;
-        case STRUCT_S: assemble_large_kernel<T, STRUCT_S><<<grid, warps * 32, 0, st>>>(a); break;
-        default: assemble_large_kernel<T, STRUCT_G><<<grid, warps * 32, 0, st>>>(a);
+        case STRUCT_SPD: assemble_large_kernel<T, STRUCT_SPD><<<grid, ASM_WARPS * 32, 0, st>>>(a); break;
+        case STRUCT_S: assemble_large_kernel<T, STRUCT_S><<<grid, ASM_WARPS * 32, 0, st>>>(a); break;
+        default: assemble_large_kernel<T, STRUCT_G><<<grid, ASM_WARPS * 32, 0, st>>>(a);
     }
     return cudaGetLastError();
 }

@@ -206,6 +206,7 @@ Plan* build_plan(const sdsb200_symbolic* sym, const sdsb200_plan_options* popts,
             F.am_end = to_i32(amap_ptr[s + 1] - 1, "amap_ptr");
             F.row_begin = to_i32(rowptr[s] - 1, "rowptr");
             F.level = 0;
+            F.rc_begin = -1;
         }
         // levels: height above the leaves (children are numbered first)
         for (int64_t s = 0; s < ns; ++s) {
@@ -277,24 +278,36 @@ Plan* build_plan(const sdsb200_symbolic* sym, const sdsb200_plan_options* popts,
         }
 
         // column-owner extend-add lists of the large fronts
-        std::vector<int32_t> ea, eacol;
+        // and each child's row-chunk starts: the parent's rows are built ASM_ROWS at a time, and the
+        // child's contribution rows that land in chunk k are ii in [rchunk[k], rchunk[k + 1])
+        std::vector<int32_t> ea, eacol, rchunk;
         for (int64_t s = 0; s < ns; ++s) {
             DFront& F = P->fronts[s];
             F.eacol_begin = (int32_t)eacol.size();
             if (class_of(F.f) != 0) continue;
             std::vector<std::vector<std::pair<int, int>>> per(F.f);
+            const int nchunk = (F.f + ASM_ROWS - 1) / ASM_ROWS;
             for (int q = F.ch_begin; q < F.ch_end; ++q) {
                 int c = (int)child_list[q] - 1;
                 if (c < 0 || c >= ns || P->fronts[c].parent != s)
                     throw BuildError(SDSB200_INVALID_VALUE, "child_list is inconsistent with snparent");
-                const DFront& C = P->fronts[c];
+                DFront& C = P->fronts[c];
                 int mc = C.f - C.w;
                 if (mc <= 0 || C.cb < 0) continue;
+                C.rc_begin = (int32_t)rchunk.size();
+                int prev = -1;
                 for (int t = 0; t < mc; ++t) {
                     int p = (int)relind[C.ri_begin + t] - 1;
                     if (p < 0 || p >= F.f) throw BuildError(SDSB200_INVALID_VALUE, "relind out of range");
+                    if (p <= prev) throw BuildError(SDSB200_INVALID_VALUE, "relind of a front is not increasing");
+                    for (int k = prev < 0 ? 0 : prev / ASM_ROWS + 1; k <= p / ASM_ROWS; ++k)
+                        rchunk.push_back(t);
+                    prev = p;
                     per[p].push_back({c, t});
                 }
+                for (int k = prev / ASM_ROWS + 1; k <= nchunk; ++k) rchunk.push_back(mc);
+                if ((int64_t)rchunk.size() - C.rc_begin != nchunk + 1)
+                    throw BuildError(SDSB200_INVALID_VALUE, "row-chunk table of a front has the wrong length");
             }
             for (int p = 0; p < F.f; ++p) {
                 eacol.push_back((int32_t)(ea.size() / 2));
@@ -717,6 +730,7 @@ Plan* build_plan(const sdsb200_symbolic* sym, const sdsb200_plan_options* popts,
         if (P->coop_bar_len) P->d_coop_bar = dalloc<unsigned int>(P, P->coop_bar_len);
         P->maps.ea = upload(P, ea, st);
         P->maps.eacol = upload(P, eacol, st);
+        P->maps.rchunk = upload(P, rchunk, st);
         P->maps.rowval = upload(P, rv0, st);
         P->d_perm0 = upload(P, P->h_perm0, st);
         P->maps.perm = P->d_perm0;
