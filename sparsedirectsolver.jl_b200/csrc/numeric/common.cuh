@@ -35,6 +35,19 @@ struct DFront {
 // Rows of a front column that the large-front assembly builds at a time in shared memory (per warp)
 constexpr int ASM_ROWS = 256;
 
+// Row chunk and column group of one update item of the cooperative LDLT / LU kernel
+constexpr int COOP_ROWS = 256;
+constexpr int COOP_COLS = 32;
+
+// Scratch (in doubles) of a wide LDLT / LU front: multipliers (2 f), D (2 w), local order and
+// control (w + 16 ints), kinds (w bytes); then the cooperative kernel's per-chunk column maxima
+__host__ __device__ inline int64_t pivot_scratch_base(int f, int w) {
+    return 2 * (int64_t)f + 2 * (int64_t)w + (w + 16 + 1) / 2 + (w + 7) / 8 + 8;
+}
+__host__ __device__ inline int64_t pivot_scratch_len(int f, int w) {
+    return pivot_scratch_base(f, w) + (int64_t)w * ((f + COOP_ROWS - 1) / COOP_ROWS);
+}
+
 // Column task of the large-front assembly: (front, parent index p); one warp each.
 struct ColTask {
     int32_t front, p;

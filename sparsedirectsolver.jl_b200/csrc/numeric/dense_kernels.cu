@@ -456,8 +456,135 @@ __device__ __forceinline__ void group_barrier(unsigned int* bar, unsigned int& e
     __syncthreads();
 }
 
-constexpr int COOP_ROWS = 256;   // rows of one update item (a column chunk, one warp)
+static_assert(COOP_ROWS == COOP_THREADS, "an update item holds one row per thread");
 
+// Multipliers of one elimination step of the cooperative kernel
+struct CoopStep {
+    double dk;                    // LDLT 1x1 pivot
+    double e11, e12, e21, e22;    // LDLT 2x2: the inverse of the pivot block
+    double b;                     // LDLT 2x2: its subdiagonal entry
+};
+
+// Eight values per lane (columns u = 0..7 of the lane's row) -> the warp's maximum of column
+// (lane >> 2) & 7 in every lane: a butterfly that halves the columns a lane keeps (7 exchanges), then
+// two plain ones. jmax is exact in any order.
+__device__ __forceinline__ double transpose_jmax8(double (&v)[8], int lane) {
+#pragma unroll
+    for (int s = 0; s < 3; ++s) {
+        const int o = 16 >> s, n = 4 >> s;
+        const bool hi = (lane & o) != 0;
+#pragma unroll
+        for (int u = 0; u < n; ++u) {
+            const double keep = hi ? v[u + n] : v[u];
+            const double send = hi ? v[u] : v[u + n];
+            v[u] = jmax(keep, __shfl_xor_sync(0xffffffffu, send, o));
+        }
+    }
+    double r = v[0];
+    r = jmax(r, __shfl_xor_sync(0xffffffffu, r, 2));
+    r = jmax(r, __shfl_xor_sync(0xffffffffu, r, 1));
+    return r;
+}
+
+// One update item of the cooperative kernel over the panel: row i = q COOP_ROWS + tid of chunk q
+// (when i >= ilo), columns [jb, je) (at most COOP_COLS, all < w); for "G" only entries on or below
+// the diagonal (the others are the U^T part). KIND 0 only reads (the first maxima), 1 is an LDLT 1x1
+// step, 2 an LDLT 2x2 step, 3 an LU step. The arithmetic is the sequential update's:
+//   1x1  F[i, j] -= T(F[i, k] / dk) F[k, j]
+//   2x2  F[i, j] -= T(l1) F[k, j] + T(l2) F[k + 1, j],  (l1, l2) = (F[i, k], F[i, k + 1]) E
+//   LU   F[i, j] -= F[i, k] / T(dk) F[k, j]
+// Loads go out eight columns at a time. The maxima of the first nmax columns over the item's rows
+// >= w go to part[j nch + q] (all threads of the CTA call this with the same arguments).
+template <int KIND, typename T, bool GEN>
+__device__ void coop_panel_item(const CoopStore<T, GEN>& F, int k, int q, int ilo, int jb, int je, int nmax,
+                                const CoopStep& cs, T tdk, double (*pred)[COOP_COLS], int tid) {
+    const int warp = tid >> 5, lane = tid & 31;
+    const int i = q * COOP_ROWS + tid;
+    const bool live = i >= ilo && i < F.f;
+    const bool below = live && i >= F.w;
+    T l1 = T(0), l2 = T(0);
+    if (KIND != 0 && live) {
+        if (KIND == 1) {
+            l1 = T(F.get(i, k) / cs.dk);
+        } else if (KIND == 2) {
+            const double x1 = F.get(i, k), x2 = F.get(i, k + 1);
+            l1 = T(x1 * cs.e11 + x2 * cs.e21);
+            l2 = T(x1 * cs.e12 + x2 * cs.e22);
+        } else {
+            l1 = F.at(i, k) / tdk;
+        }
+    }
+    for (int u0 = 0; jb + u0 < je; u0 += 8) {
+        T a[8], b1[8], b2[8];
+        double mx[8];
+#pragma unroll
+        for (int u = 0; u < 8; ++u) {
+            const int j = jb + u0 + u;
+            const bool ok = live && j < je && (!GEN || i >= j);
+            if (KIND != 0) b1[u] = j < je ? F.at(k, j) : T(0);
+            if (KIND == 2) b2[u] = j < je ? F.at(k + 1, j) : T(0);
+            a[u] = ok ? F.at(i, j) : T(0);
+        }
+#pragma unroll
+        for (int u = 0; u < 8; ++u) {
+            const int j = jb + u0 + u;
+            const bool ok = live && j < je && (!GEN || i >= j);
+            T v = a[u];
+            if (KIND != 0 && ok) {
+                if (KIND == 2) v -= l1 * b1[u] + l2 * b2[u];
+                else v -= l1 * b1[u];
+                F.at(i, j) = v;
+            }
+            mx[u] = ok && below ? fabs((double)v) : 0.0;
+        }
+        if (u0 < nmax) {
+            const double r = transpose_jmax8(mx, lane);
+            if ((lane & 3) == 0) pred[warp][u0 + ((lane >> 2) & 7)] = r;
+        }
+    }
+    if (nmax > 0) {
+        __syncthreads();
+        if (tid < nmax) {
+            double m = pred[0][tid];
+            for (int x = 1; x < COOP_THREADS / 32; ++x) m = jmax(m, pred[x][tid]);
+            F.part[(int64_t)(jb + tid) * F.nch + q] = m;
+        }
+        __syncthreads();
+    }
+}
+
+// The U^T part of an LU step: rows [rb, re) (fully-summed, > k) against column j = cb + tid (one per
+// thread, i < j < f), F[i, j] -= F[i, k] / T(dk) F[k, j]; coalesced in the U^T panel (U[j + i f])
+template <typename T>
+__device__ void coop_u_item(const CoopStore<T, true>& F, int k, int rb, int re, int cb, T tdk, int tid) {
+    const int j = cb + tid;
+    if (j >= F.f || j <= rb) return;
+    const int64_t f = F.f;
+    const T fkj = F.U[j + k * f];
+    for (int i0 = rb; i0 < re; i0 += 8) {
+        T l[8], a[8];
+#pragma unroll
+        for (int u = 0; u < 8; ++u) {
+            const int i = i0 + u;
+            const bool ok = i < re && i < j;
+            l[u] = ok ? F.P[i + k * f] / tdk : T(0);
+            a[u] = ok ? F.U[j + i * f] : T(0);
+        }
+#pragma unroll
+        for (int u = 0; u < 8; ++u) {
+            const int i = i0 + u;
+            if (i < re && i < j) F.U[j + i * f] = a[u] - l[u] * fkj;
+        }
+    }
+}
+
+// Wide LDLT / LU fronts on a group of co-resident CTAs (one group per front of the launch, barriers
+// over the group). A step: CTA 0 takes the pivot decision while every CTA writes the previous step's
+// multipliers into its column (the update needs them unscaled until then); barrier; the interchange
+// (one phase) and a barrier when there is one; the update, which also leaves the maxima of the updated
+// fully-summed columns over each chunk of rows below the block, so that the next decision scans only
+// the w fully-summed rows; barrier. The decisions and the arithmetic are those of the sequential
+// kernel.
 template <typename T, int STRUCT>
 __global__ void __launch_bounds__(COOP_THREADS) large_pivot_coop_kernel(LargePivotArgs<T> A, CoopGroups G) {
     int lo = 0, hi = A.count - 1;
@@ -483,12 +610,14 @@ __global__ void __launch_bounds__(COOP_THREADS) large_pivot_coop_kernel(LargePiv
     sc.kd = reinterpret_cast<signed char*>(sc.ctl + 16);
     unsigned int* bar = G.bar + fi;
     unsigned int epoch = 0;
-    const int tid = threadIdx.x, nt = blockDim.x, lane = tid & 31;
-    const int gt = rank * nt + tid, GT = gs * nt, gw = gt >> 5, GW = GT >> 5;
+    const int tid = threadIdx.x, nt = blockDim.x;
+    const int gt = rank * nt + tid, GT = gs * nt;
     const bool lead = rank == 0 && tid == 0;
-    GlobalStore<T, GEN> F{P, U, f, w};
+    const int nch = (f + COOP_ROWS - 1) / COOP_ROWS;
+    const CoopStore<T, GEN> F{{P, U, f, w}, scr + pivot_scratch_base(f, w), nch, w / COOP_ROWS};
     __shared__ double team_red[COOP_THREADS / 32];
     __shared__ int team_redi[COOP_THREADS / 32];
+    __shared__ double pred[COOP_THREADS / 32][COOP_COLS];
     const CtaTeam team{tid, nt, team_red, team_redi};
     if (STRUCT == STRUCT_S) {
         for (int q = gt; q < w * w; q += GT) {
@@ -497,11 +626,40 @@ __global__ void __launch_bounds__(COOP_THREADS) large_pivot_coop_kernel(LargePiv
         }
     }
     for (int q = gt; q < w; q += GT) sc.lp[q] = q;
+    {   // maxima below the block of the columns the first decision may scan (all for "S", column 0 for "G")
+        const int nq = nch - F.q0, ncg = GEN ? 1 : (w + COOP_COLS - 1) / COOP_COLS;
+        for (int it = rank; it < nq * ncg; it += gs) {
+            const int q = F.q0 + it % nq, jb = (it / nq) * COOP_COLS;
+            const int je = GEN ? 1 : min(w, jb + COOP_COLS);
+            coop_panel_item<0>(F, 0, q, w, jb, je, je - jb, CoopStep{}, T(1), pred, tid);
+        }
+    }
     group_barrier(bar, epoch, gs, G.status);
     int64_t st[NSTAT] = {0, 0, 0, 0, 0, 0};
-    if (STRUCT == STRUCT_S) {
+    if constexpr (STRUCT == STRUCT_S) {
+        int pk = -1, pkind = 0;   // the step whose multipliers are still to be written (1: 1x1, 2: 2x2)
+        CoopStep pc{};
+        // write the multipliers of step pk into its column(s); the pivot block's own entries (which the
+        // final pass overwrites) only before the last step
+        auto flush = [&](bool last) {
+            if (pkind == 1) {
+                for (int i = pk + 1 + gt; i < f; i += GT) F.at(i, pk) = T(F.get(i, pk) / pc.dk);
+                if (lead && !last) F.at(pk, pk) = T(pc.dk);
+            } else if (pkind == 2) {
+                for (int i = pk + 2 + gt; i < f; i += GT) {
+                    const double x1 = F.get(i, pk), x2 = F.get(i, pk + 1);
+                    F.at(i, pk) = T(x1 * pc.e11 + x2 * pc.e21);
+                    F.at(i, pk + 1) = T(x1 * pc.e12 + x2 * pc.e22);
+                }
+                if (lead) {
+                    if (!last) F.at(pk, pk + 1) = T(pc.b);
+                    F.at(pk + 1, pk) = T(0);
+                }
+            }
+        };
         int k = 0;
         while (k < w) {
+            flush(false);
             if (rank == 0) {   // the whole first CTA takes the decision (row scans split over its threads)
                 int c, r;
                 choose_pivot(F, k, w, A.pivot, A.u, A.eps, team, c, r);
@@ -511,17 +669,25 @@ __global__ void __launch_bounds__(COOP_THREADS) large_pivot_coop_kernel(LargePiv
             const int c = sc.ctl[0], r = sc.ctl[1];
             const int p = r < 0 ? k : k + 1, qsw = r < 0 ? c : r;
             if (p != qsw) {
+                // the symmetric interchange of p and qsw: columns (rows other than p, qsw), rows (columns
+                // other than p, qsw) and the 2x2 block they share, in one phase
                 for (int i = gt; i < f; i += GT) {
+                    if (i == p || i == qsw) continue;
                     T t = F.at(i, p); F.at(i, p) = F.at(i, qsw); F.at(i, qsw) = t;
                 }
-                group_barrier(bar, epoch, gs, G.status);
                 for (int j = gt; j < w; j += GT) {
+                    if (j == p || j == qsw) continue;
                     T t = F.at(p, j); F.at(p, j) = F.at(qsw, j); F.at(qsw, j) = t;
                 }
-                if (lead) { int t = sc.lp[p]; sc.lp[p] = sc.lp[qsw]; sc.lp[qsw] = t; }
+                if (lead) {
+                    T t = F.at(p, p); F.at(p, p) = F.at(qsw, qsw); F.at(qsw, qsw) = t;
+                    t = F.at(p, qsw); F.at(p, qsw) = F.at(qsw, p); F.at(qsw, p) = t;
+                    int tl = sc.lp[p]; sc.lp[p] = sc.lp[qsw]; sc.lp[qsw] = tl;
+                }
                 group_barrier(bar, epoch, gs, G.status);
             }
-            const int nch = (f - k - 1 + COOP_ROWS - 1) / COOP_ROWS;
+            CoopStep cs{};
+            const int nb = r < 0 ? 1 : 2;
             if (r < 0) {
                 double dk = F.get(k, k);
                 signed char kk = KIND_1X1;
@@ -535,59 +701,50 @@ __global__ void __launch_bounds__(COOP_THREADS) large_pivot_coop_kernel(LargePiv
                 }
                 if (dk > 0) st[ST_NPOS]++;
                 else if (dk < 0) st[ST_NNEG]++;
-                for (int i = k + 1 + gt; i < f; i += GT) sc.lvec[i] = F.get(i, k) / dk;
-                group_barrier(bar, epoch, gs, G.status);
-                if (lead) { F.at(k, k) = T(dk); sc.dd[k] = dk; sc.ee[k] = 0.0; sc.kd[k] = kk; }
-                const int nj = w - k - 1;
-                for (int item = gw; item < nj * nch; item += GW) {
-                    const int j = k + 1 + item % nj, ch = item / nj;
-                    const T fkj = F.at(k, j);
-                    const int i1 = min(f, k + 1 + (ch + 1) * COOP_ROWS);
-                    for (int i = k + 1 + ch * COOP_ROWS + lane; i < i1; i += 32) F.at(i, j) -= T(sc.lvec[i]) * fkj;
-                }
-                for (int i = k + 1 + gt; i < f; i += GT) F.at(i, k) = T(sc.lvec[i]);
-                group_barrier(bar, epoch, gs, G.status);
-                k += 1;
+                if (lead) { sc.dd[k] = dk; sc.ee[k] = 0.0; sc.kd[k] = kk; }
+                cs.dk = dk;
             } else {
                 const double a = F.get(k, k), b = F.get(k + 1, k), c2 = F.get(k + 1, k + 1);
                 const double det = a * c2 - b * b;
-                const double e11 = c2 / det, e12 = -b / det, e21 = -b / det, e22 = a / det;
+                cs.e11 = c2 / det; cs.e12 = -b / det; cs.e21 = -b / det; cs.e22 = a / det;
+                cs.b = b;
                 st[ST_N2X2]++;
                 if (det < 0) { st[ST_NPOS]++; st[ST_NNEG]++; }
                 else if (a > 0) st[ST_NPOS] += 2;
                 else st[ST_NNEG] += 2;
-                for (int i = k + 2 + gt; i < f; i += GT) {
-                    const double x1 = F.get(i, k), x2 = F.get(i, k + 1);
-                    sc.lvec[i] = x1 * e11 + x2 * e21;
-                    sc.lvec[f + i] = x1 * e12 + x2 * e22;
-                }
-                group_barrier(bar, epoch, gs, G.status);
                 if (lead) {
-                    F.at(k, k + 1) = T(b);
                     sc.dd[k] = a; sc.dd[k + 1] = c2; sc.ee[k] = b; sc.ee[k + 1] = 0.0;
                     sc.kd[k] = KIND_2X2_FIRST; sc.kd[k + 1] = KIND_2X2_SECOND;
                 }
-                const int nj = w - k - 2;
-                const int nch2 = (f - k - 2 + COOP_ROWS - 1) / COOP_ROWS;
-                for (int item = gw; nj > 0 && item < nj * nch2; item += GW) {
-                    const int j = k + 2 + item % nj, ch = item / nj;
-                    const T fkj = F.at(k, j), fk1j = F.at(k + 1, j);
-                    const int i1 = min(f, k + 2 + (ch + 1) * COOP_ROWS);
-                    for (int i = k + 2 + ch * COOP_ROWS + lane; i < i1; i += 32)
-                        F.at(i, j) -= T(sc.lvec[i]) * fkj + T(sc.lvec[f + i]) * fk1j;
-                }
-                for (int i = k + 2 + gt; i < f; i += GT) {
-                    F.at(i, k) = T(sc.lvec[i]);
-                    F.at(i, k + 1) = T(sc.lvec[f + i]);
-                }
-                if (lead) F.at(k + 1, k) = T(0);
-                group_barrier(bar, epoch, gs, G.status);
-                k += 2;
             }
+            const int j0 = k + nb, qa = j0 / COOP_ROWS, nq = nch - qa;
+            const int ncg = (w - j0 + COOP_COLS - 1) / COOP_COLS;
+            for (int it = rank; it < nq * ncg; it += gs) {
+                const int q = qa + it % nq, jb = j0 + (it / nq) * COOP_COLS, je = min(w, jb + COOP_COLS);
+                const int nmax = q >= F.q0 ? je - jb : 0;
+                if (r < 0) coop_panel_item<1>(F, k, q, j0, jb, je, nmax, cs, T(1), pred, tid);
+                else coop_panel_item<2>(F, k, q, j0, jb, je, nmax, cs, T(1), pred, tid);
+            }
+            group_barrier(bar, epoch, gs, G.status);
+            pk = k; pkind = nb; pc = cs;
+            k += nb;
         }
+        flush(true);
     } else {
         const bool pivoting = A.lu_pivot != 0;
+        int pk = -1;
+        T ptdk = T(1);
+        double pdk = 0.0;
+        // scale column pk into L and row pk into U (the update reads them unscaled); D into the pivot
+        // entry before the last step (the final pass overwrites it)
+        auto flush = [&](bool last) {
+            if (pk < 0) return;
+            for (int i = pk + 1 + gt; i < f; i += GT) F.at(i, pk) /= ptdk;
+            for (int j = pk + 1 + gt; j < f; j += GT) F.at(pk, j) /= ptdk;
+            if (lead && !last) F.at(pk, pk) = T(pdk);
+        };
         for (int k = 0; k < w; ++k) {
+            flush(false);
             if (rank == 0) {
                 int r = pivoting ? lu_choose_row(F, k, w, A.u, team) : k;
                 if (tid == 0) sc.ctl[0] = r;
@@ -610,25 +767,28 @@ __global__ void __launch_bounds__(COOP_THREADS) large_pivot_coop_kernel(LargePiv
                 st[ST_NPERT]++;
                 if (dk == 0.0 && st[ST_INFO] == 0) st[ST_INFO] = k + 1;
             }
-            group_barrier(bar, epoch, gs, G.status);   // every CTA has read F[k, k]
-            if (lead) { F.at(k, k) = T(dk); sc.dd[k] = dk; sc.kd[k] = kk; }
+            if (lead) { sc.dd[k] = dk; sc.kd[k] = kk; }
             const T tdk = T(dk);
-            const int nj = f - k - 1;
-            const int nch = (f - k - 1 + COOP_ROWS - 1) / COOP_ROWS;
-            for (int item = gw; item < nj * nch; item += GW) {
-                const int j = k + 1 + item % nj, ch = item / nj;
-                const int iend = j < w ? f : w;
-                const int i0 = k + 1 + ch * COOP_ROWS;
-                if (i0 >= iend) continue;
-                const T fkj = F.at(k, j);
-                const int i1 = min(iend, i0 + COOP_ROWS);
-                for (int i = i0 + lane; i < i1; i += 32) F.at(i, j) -= F.at(i, k) / tdk * fkj;
+            const int qa = (k + 1) / COOP_ROWS, nq = nch - qa;
+            const int ncg = (w - k - 1 + COOP_COLS - 1) / COOP_COLS;       // column groups; also row groups of U^T
+            const int nct = (f - k - 1 + COOP_ROWS - 1) / COOP_ROWS;       // column tiles of U^T
+            const int nl = nq * ncg;
+            for (int it = rank; it < nl + ncg * nct; it += gs) {
+                if (it < nl) {
+                    const int q = qa + it % nq, g = it / nq;
+                    const int jb = k + 1 + g * COOP_COLS, je = min(w, jb + COOP_COLS);
+                    coop_panel_item<3>(F, k, q, k + 1, jb, je, (g == 0 && q >= F.q0) ? 1 : 0, CoopStep{}, tdk, pred,
+                                       tid);
+                } else {
+                    const int u = it - nl, rg = u % ncg, ct = u / ncg;
+                    const int rb = k + 1 + rg * COOP_COLS, re = min(w, rb + COOP_COLS);
+                    coop_u_item(F, k, rb, re, k + 1 + ct * COOP_ROWS, tdk, tid);
+                }
             }
             group_barrier(bar, epoch, gs, G.status);
-            for (int i = k + 1 + gt; i < f; i += GT) F.at(i, k) /= tdk;
-            for (int j = k + 1 + gt; j < f; j += GT) F.at(k, j) /= tdk;
-            group_barrier(bar, epoch, gs, G.status);
+            pk = k; ptdk = tdk; pdk = dk;
         }
+        flush(true);
     }
     for (int q = gt; q < w * w; q += GT) {
         const int i = q % w, j = q / w;

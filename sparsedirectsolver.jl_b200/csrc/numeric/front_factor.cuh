@@ -29,6 +29,8 @@ struct SmemStore {
     int ld, f, w;
     __device__ T& at(int i, int j) const { return a[i + j * ld]; }
     __device__ double get(int i, int j) const { return (double)a[i + j * ld]; }
+    __device__ int scan_rows() const { return f; }
+    __device__ double part_max(int, int, int) const { return 0.0; }
 };
 
 // Large-front storage: F[:, 0:w] in the panel P (ld f); for "G" the strict upper
@@ -43,6 +45,22 @@ struct GlobalStore {
         return U[j + (int64_t)i * f];
     }
     __device__ double get(int i, int j) const { return (double)at(i, j); }
+    __device__ int scan_rows() const { return f; }
+    __device__ double part_max(int, int, int) const { return 0.0; }
+};
+
+// Large-front storage of the cooperative kernel: column scans read the fully-summed rows and take
+// the rows below from per-chunk maxima that the update phase leaves behind.
+template <typename T, bool GEN>
+struct CoopStore : GlobalStore<T, GEN> {
+    double* part;   // part[c nch + q]: max |F[i, c]| over the rows i >= w of row chunk q (COOP_ROWS rows)
+    int nch, q0;    // row chunks of the front; q0: the first that holds a row >= w
+    __device__ int scan_rows() const { return this->w; }
+    __device__ double part_max(int c, int rank, int size) const {
+        double m = 0.0;
+        for (int q = q0 + rank; q < nch; q += size) m = jmax(m, part[(int64_t)c * nch + q]);
+        return m;
+    }
 };
 
 __device__ __forceinline__ double perturb_sign_of(double d, int requested) {

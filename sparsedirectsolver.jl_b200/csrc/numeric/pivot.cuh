@@ -80,16 +80,21 @@ struct CtaTeam {
 };
 
 // Front accessor interface: F(i, j) returns the current value (double) of entry (i, j).
-// Acc must provide: double get(int i, int j) const; int f; int w.
+// Acc must provide: double get(int i, int j) const; int f; int w; int scan_rows() const (the rows
+// 0..scan_rows()-1 a column scan reads); double part_max(int c, int rank, int size) const (this
+// team member's share of max |F[i, c]| over the rows from scan_rows() on, kept by the accessor;
+// 0.0 when scan_rows() == f).
 
-// max |F[i, c]| over rows k..f-1, skipping c and skip (Julia max semantics)
+// max |F[i, c]| over rows k..f-1, skipping c and skip (Julia max semantics); c and skip are
+// fully-summed rows, so they are never among the rows the accessor keeps maxima for
 template <class Acc, class Team>
 __device__ double colmax(const Acc& F, int c, int k, int skip, const Team& tm) {
     double m = 0.0;
-    for (int i = k + tm.rank; i < F.f; i += tm.size) {
+    for (int i = k + tm.rank; i < F.scan_rows(); i += tm.size) {
         if (i == c || i == skip) continue;
         m = jmax(m, fabs(F.get(i, c)));
     }
+    m = jmax(m, F.part_max(c, tm.rank, tm.size));
     return tm.reduce_jmax(m);
 }
 
@@ -192,7 +197,8 @@ __device__ void choose_pivot(const Acc& F, int k, int w, int pivot, double u, do
 template <class Acc, class Team>
 __device__ int lu_choose_row(const Acc& F, int k, int w, double u, const Team& tm) {
     double g = 0.0;
-    for (int i = k + tm.rank; i < F.f; i += tm.size) g = jmax(g, fabs(F.get(i, k)));
+    for (int i = k + tm.rank; i < F.scan_rows(); i += tm.size) g = jmax(g, fabs(F.get(i, k)));
+    g = jmax(g, F.part_max(k, tm.rank, tm.size));
     g = tm.reduce_jmax(g);
     double akk = fabs(F.get(k, k));
     if (akk >= u * g) return k;

@@ -479,7 +479,7 @@ Plan* build_plan(const sdsb200_symbolic* sym, const sdsb200_plan_options* popts,
                     const DFront& F = P->fronts[s];
                     lists.push_back(s);
                     scr_off.push_back(so);
-                    so += 2 * (int64_t)F.f + 2 * (int64_t)F.w + (F.w + 16 + 1) / 2 + (F.w + 7) / 8 + 8;
+                    so += pivot_scratch_len(F.f, F.w);
                 }
                 P->scr_len = std::max(P->scr_len, so);
                 P->prog.push_back(pl);
@@ -699,7 +699,8 @@ Plan* build_plan(const sdsb200_symbolic* sym, const sdsb200_plan_options* popts,
         P->maps.am_loc = upload(P, am_loc, st);
         P->maps.amcol = upload(P, amcol, st);
         // cooperative pivot launches (single-member plans): a group of co-resident CTAs per wide front,
-        // sized by the front's update work f w^2 (at least one CTA, at most f w / 2048)
+        // sized by the front's update work f w^2, at least one CTA and at most the update items of its
+        // first step (row chunks x column groups; twice that for the U^T part of "G")
         std::vector<int32_t> coop_first;
         if (P->nbatch == 1) {
             const int cap = P->elsize == 8 ? large_pivot_coop_capacity<double>(P->structure)
@@ -716,7 +717,9 @@ Plan* build_plan(const sdsb200_symbolic* sym, const sdsb200_plan_options* popts,
                 for (int i = 0; i < L.count; ++i) {
                     const DFront& F = P->fronts[lists[L.list + i]];
                     const double share = total > 0 ? (double)cap * ((double)F.f * F.w * F.w) / total : 1.0;
-                    const int64_t most = std::max<int64_t>(1, (int64_t)F.f * F.w / 2048);
+                    const int64_t items = (int64_t)((F.f + COOP_ROWS - 1) / COOP_ROWS) *
+                                          ((F.w + COOP_COLS - 1) / COOP_COLS) * (gen ? 2 : 1);
+                    const int64_t most = std::max<int64_t>(1, items);
                     const int g = (int)std::max<int64_t>(1, std::min<int64_t>((int64_t)share, most));
                     coop_first.push_back(first);
                     first += g;
