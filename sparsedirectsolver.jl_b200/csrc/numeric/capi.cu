@@ -444,6 +444,7 @@ int run_persistent(Plan* P, int nrhs, bool transpose, const double* in, int64_t 
     a.in = in; a.ldin = ldin; a.out = out; a.ldout = ldout; a.mode = mode;
     a.xtmp = P->d_xtmp;
     a.barrier = P->d_barrier;
+    a.blkflag = P->d_blkflag;
     a.status = P->d_solve_status;
     a.trace = P->profile ? P->d_trace : nullptr;
     a.trace_cap = Plan::TRACE_CAP;
@@ -457,6 +458,7 @@ int run_persistent(Plan* P, int nrhs, bool transpose, const double* in, int64_t 
     const int grid = persistent_solve_grid<T>(smem);
     if (grid <= 0) return fail(SDSB200_CUDA_ERROR, "no co-resident grid for the persistent solve");
     CK(cudaMemsetAsync(P->d_barrier, 0, sizeof(unsigned int), st), "barrier reset");
+    CK(cudaMemsetAsync(P->d_blkflag, 0, sizeof(unsigned int) * P->n_blkflag, st), "block flag reset");
     prof_begin(P, st);
     cudaError_t e = launch_persistent_solve<T>(a, grid, smem, st);
     // algorithmic work: every stored panel entry read once per sweep (2 flops per entry and rhs each

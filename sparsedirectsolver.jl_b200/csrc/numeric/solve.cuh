@@ -53,7 +53,10 @@ struct PersistArgs {
     int32_t mode;              // 0: X = solve(B); 2: X += solve(R)
     double* xtmp;              // n x nrhs scratch
     unsigned int* barrier;     // grid barrier counter (zeroed before the launch)
-    int32_t* status;           // nonzero: a barrier wait gave up
+    unsigned int* blkflag;     // per 64-column diagonal block of the wide fronts (front s: from dinv_off[s] /
+                               // 4096): 1 once its forward solution is published, 2 once its backward one is
+                               // (zeroed before the launch)
+    int32_t* status;           // nonzero: a barrier or flag wait gave up
     int64_t* trace;            // profiling: (tag, %globaltimer ns) pairs written by CTA 0, or NULL
     int32_t trace_cap;
     int32_t warp_smem;         // doubles of shared memory per warp for the small fronts (xs + Ld)

@@ -605,92 +605,155 @@ __device__ __forceinline__ void grid_barrier(unsigned int* bar, unsigned int& ep
     __syncthreads();
 }
 
-// Shared memory of a wide-front tile: the 64 x 64 inverse block, y_b, x_b and partial sums.
+// Shared memory of a wide-front item: the 64 x 64 inverse block, the item's rows (or columns) of y,
+// x of the block being applied, and partial sums.
 constexpr int WT_SMEM_DOUBLES_FIXED = SOLVE_BLK * (SOLVE_BLK + 1);
 
-// forward, wide front s, block step b, row tile t: x_b = inv(L_bb) y_b; rows below get -L x_b
+// Flags of the wide fronts' dataflow: a block's solution is published by its owner (stores, fence,
+// release of the flag) and read by the items that need it after an acquire of the flag. The wait is
+// bounded like the grid barrier, and gives up at once when any wait of the launch has given up.
+__device__ __forceinline__ void publish_flag(unsigned int* flag, unsigned int v) {
+    __threadfence();
+    __syncthreads();
+    if (threadIdx.x == 0) asm volatile("st.release.gpu.u32 [%0], %1;" ::"l"(flag), "r"(v) : "memory");
+}
+
+__device__ __forceinline__ void wait_flag(const unsigned int* flag, unsigned int target, int32_t* status) {
+    if (threadIdx.x == 0) {
+        unsigned int v;
+        long spins = 0;
+        while (true) {
+            asm volatile("ld.acquire.gpu.u32 %0, [%1];" : "=r"(v) : "l"(flag) : "memory");
+            if (v >= target) break;
+            if (++spins > (1L << 26) || ((spins & 255) == 0 && *(volatile int32_t*)status != 0)) {
+                atomicExch(status, 1);
+                break;
+            }
+            __nanosleep(32);
+        }
+        __threadfence();
+    }
+    __syncthreads();
+}
+
+// Forward sweep of a wide front, row tile t (rows 64 t .. 64 t + 63), owned by one CTA: the tile takes
+// x_b of every block b <= t in increasing order (rows below block b: y -= L x_b for rows of the block
+// column, u += L x_b for the rows below the front's columns); at b = t the tile holds block t's rows and
+// solves them, x_t = inv(L_tt) y_t, publishing x_t for the tiles below. The arithmetic and its order
+// are those of a block-step sweep with a grid barrier after every step.
 template <typename T>
-__device__ void wide_forward_tile(const PersistArgs<T>& P, int s, int b, int t, double* sm) {
+__device__ void wide_forward_owner(const PersistArgs<T>& P, int s, int t, double* sm) {
     const SweepArgs<T>& A = P.fw;
     const DFront fd = A.fronts[s];
     const int f = fd.f, w = fd.w, m = f - w, nrhs = A.nrhs;
     const int64_t n = A.n;
-    const int jb = b * SOLVE_BLK, bw = min(SOLVE_BLK, w - jb);
+    const int nb = (w + SOLVE_BLK - 1) / SOLVE_BLK;
+    const int r0 = t * SOLVE_BLK, rows = min(SOLVE_BLK, f - r0);
     const T* L = A.fac + fd.panel;
-    const T* inv = P.dinv_fw + P.dinv_off[s] + (int64_t)b * SOLVE_BLK * SOLVE_BLK;
     double* Y = A.Y;
     double* u = m > 0 ? A.U + A.uoff[s] : nullptr;
+    unsigned int* flag = P.blkflag + P.dinv_off[s] / (SOLVE_BLK * SOLVE_BLK);
     double* Iv = sm;                                  // SOLVE_BLK x (SOLVE_BLK + 1)
-    double* yb = sm + WT_SMEM_DOUBLES_FIXED;          // SOLVE_BLK x nrhs
-    double* xb = yb + SOLVE_BLK * nrhs;               // SOLVE_BLK x nrhs
+    double* yb = sm + WT_SMEM_DOUBLES_FIXED;          // the tile's rows, SOLVE_BLK x nrhs
+    double* xb = yb + SOLVE_BLK * nrhs;               // x of the block being applied
     double* part = xb + SOLVE_BLK * nrhs;             // 4 x SOLVE_BLK x nrhs partial sums
     const int tid = threadIdx.x, nt = blockDim.x;
-    batched_copy<8>(tid, nt, SOLVE_BLK * SOLVE_BLK,
-                    [&](int q) { return (q % SOLVE_BLK < bw && q / SOLVE_BLK < bw) ? (double)inv[q] : 0.0; },
-                    [&](int q, double v) { Iv[q % SOLVE_BLK + (q / SOLVE_BLK) * (SOLVE_BLK + 1)] = v; });
     batched_copy<4>(tid, nt, SOLVE_BLK * nrhs,
-                    [&](int q) { return q % SOLVE_BLK < bw ? Y[fd.c0 + jb + q % SOLVE_BLK + (int64_t)(q / SOLVE_BLK) * n] : 0.0; },
+                    [&](int q) {
+                        const int i = q % SOLVE_BLK, r = q / SOLVE_BLK, row = r0 + i;
+                        if (i >= rows) return 0.0;
+                        return row < w ? Y[fd.c0 + row + (int64_t)r * n] : u[row - w + (int64_t)r * m];
+                    },
                     [&](int q, double v) { yb[q] = v; });
-    __syncthreads();
-    for (int q = tid; q < SOLVE_BLK * nrhs; q += nt) {
-        int i = q % SOLVE_BLK, r = q / SOLVE_BLK;
-        double acc = 0.0;
-#pragma unroll 8
-        for (int j = 0; j < SOLVE_BLK; ++j) acc += Iv[i + j * (SOLVE_BLK + 1)] * yb[j + r * SOLVE_BLK];
-        xb[q] = acc;
+    if (t < nb) {
+        const int bwt = min(SOLVE_BLK, w - r0);
+        const T* inv = P.dinv_fw + P.dinv_off[s] + (int64_t)t * SOLVE_BLK * SOLVE_BLK;
+        batched_copy<8>(tid, nt, SOLVE_BLK * SOLVE_BLK,
+                        [&](int q) { return (q % SOLVE_BLK < bwt && q / SOLVE_BLK < bwt) ? (double)inv[q] : 0.0; },
+                        [&](int q, double v) { Iv[q % SOLVE_BLK + (q / SOLVE_BLK) * (SOLVE_BLK + 1)] = v; });
     }
     __syncthreads();
-    const int r0 = t * SOLVE_BLK;
-    // rows of the tile below the block: 4 threads per row, 16 block columns each
     const int row = r0 + (tid & (SOLVE_BLK - 1)), quarter = tid / SOLVE_BLK;
-    const bool upd = tid < 4 * SOLVE_BLK && row < f && row >= jb + bw;
-    for (int r0_ = 0; r0_ < nrhs; r0_ += 8) {
-        const int rc = min(8, nrhs - r0_);
-        double acc[8];
-#pragma unroll
-        for (int r = 0; r < 8; ++r) acc[r] = 0.0;
-        if (upd) {
-            const int c0 = quarter * (SOLVE_BLK / 4), cw = max(0, min(SOLVE_BLK / 4, bw - c0));
-            row_dot(L + row + (int64_t)(jb + c0) * f, f, cw, xb + c0 + r0_ * SOLVE_BLK, SOLVE_BLK, rc, acc);
-        }
-        if (tid < 4 * SOLVE_BLK)
-            for (int r = 0; r < rc; ++r) part[(tid & (SOLVE_BLK - 1)) + SOLVE_BLK * (quarter + 4 * r)] = acc[r];
-        __syncthreads();
-        if (tid < SOLVE_BLK && row < f && row >= jb + bw) {
-            for (int r = 0; r < rc; ++r) {
-                const double v = part[tid + SOLVE_BLK * (4 * r)] + part[tid + SOLVE_BLK * (1 + 4 * r)] +
-                                 part[tid + SOLVE_BLK * (2 + 4 * r)] + part[tid + SOLVE_BLK * (3 + 4 * r)];
-                if (row < w) Y[fd.c0 + row + (int64_t)(r0_ + r) * n] -= v;
-                else u[row - w + (r0_ + r) * m] += v;
+    for (int b = 0; b <= min(t, nb - 1); ++b) {
+        const int jb = b * SOLVE_BLK, bw = min(SOLVE_BLK, w - jb);
+        if (b == t) {
+            for (int q = tid; q < SOLVE_BLK * nrhs; q += nt) {
+                const int i = q % SOLVE_BLK, r = q / SOLVE_BLK;
+                double acc = 0.0;
+#pragma unroll 8
+                for (int j = 0; j < SOLVE_BLK; ++j)
+                    acc += Iv[i + j * (SOLVE_BLK + 1)] * (j < bw ? yb[j + r * SOLVE_BLK] : 0.0);
+                xb[q] = acc;
             }
+            __syncthreads();
+            for (int q = tid; q < bw * nrhs; q += nt) {
+                const int k = q % bw, r = q / bw;
+                const double v = xb[k + r * SOLVE_BLK];
+                P.xtmp[fd.c0 + jb + k + (int64_t)r * n] = v;
+                Y[fd.c0 + jb + k + (int64_t)r * n] = v;
+            }
+            publish_flag(flag + b, 1u);
+        } else {
+            wait_flag(flag + b, 1u, P.status);
+            for (int q = tid; q < SOLVE_BLK * nrhs; q += nt) {
+                const int k = q % SOLVE_BLK, r = q / SOLVE_BLK;
+                xb[q] = k < bw ? P.xtmp[fd.c0 + jb + k + (int64_t)r * n] : 0.0;
+            }
+            __syncthreads();
         }
-        __syncthreads();
+        // rows of the tile below block b: 4 threads per row, 16 block columns each
+        const bool upd = tid < 4 * SOLVE_BLK && row < f && row >= jb + bw;
+        for (int r0_ = 0; r0_ < nrhs; r0_ += 8) {
+            const int rc = min(8, nrhs - r0_);
+            double acc[8];
+#pragma unroll
+            for (int r = 0; r < 8; ++r) acc[r] = 0.0;
+            if (upd) {
+                const int c0 = quarter * (SOLVE_BLK / 4), cw = max(0, min(SOLVE_BLK / 4, bw - c0));
+                row_dot(L + row + (int64_t)(jb + c0) * f, f, cw, xb + c0 + r0_ * SOLVE_BLK, SOLVE_BLK, rc, acc);
+            }
+            if (tid < 4 * SOLVE_BLK)
+                for (int r = 0; r < rc; ++r) part[(tid & (SOLVE_BLK - 1)) + SOLVE_BLK * (quarter + 4 * r)] = acc[r];
+            __syncthreads();
+            if (tid < SOLVE_BLK && row < f && row >= jb + bw) {
+                for (int r = 0; r < rc; ++r) {
+                    const double v = part[tid + SOLVE_BLK * (4 * r)] + part[tid + SOLVE_BLK * (1 + 4 * r)] +
+                                     part[tid + SOLVE_BLK * (2 + 4 * r)] + part[tid + SOLVE_BLK * (3 + 4 * r)];
+                    if (row < w) yb[tid + (r0_ + r) * SOLVE_BLK] -= v;
+                    else yb[tid + (r0_ + r) * SOLVE_BLK] += v;
+                }
+            }
+            __syncthreads();
+        }
     }
-    // the block's own rows: to the scratch, copied to Y after the level
-    if (t == b)
-        for (int q = tid; q < bw * nrhs; q += nt) {
-            int k = q % bw, r = q / bw;
-            P.xtmp[fd.c0 + jb + k + (int64_t)r * n] = xb[k + r * SOLVE_BLK];
-        }
+    // the tile's rows below the front's columns go back to the update vector
+    for (int q = tid; q < SOLVE_BLK * nrhs; q += nt) {
+        const int i = q % SOLVE_BLK, r = q / SOLVE_BLK;
+        if (i < rows && r0 + i >= w) u[r0 + i - w + (int64_t)r * m] = yb[q];
+    }
     __syncthreads();
 }
 
-// backward, wide front s, block step b, column tile t: x_b = inv(L_bb)^T y_b; columns before the
-// block get -L_b.^T x_b
+// Backward sweep of a wide front, block b (columns 64 b .. 64 b + 63), owned by one CTA, after the
+// grid-wide y1 -= L21^T x2: y_b takes -L_tb^T x_t of every later block t in decreasing order as each
+// is published, and x_b = inv(L_bb)^T y_b is published into the scratch. The arithmetic and its
+// order are those of a block-step sweep with a grid barrier after every step.
 template <typename T>
-__device__ void wide_backward_tile(const PersistArgs<T>& P, int s, int b, int t, double* sm) {
+__device__ void wide_backward_owner(const PersistArgs<T>& P, int s, int b, double* sm) {
     const SweepArgs<T>& A = P.bw;
     const DFront fd = A.fronts[s];
     const int f = fd.f, w = fd.w, nrhs = A.nrhs;
     const int64_t n = A.n;
+    const int nb = (w + SOLVE_BLK - 1) / SOLVE_BLK;
     const int jb = b * SOLVE_BLK, bw = min(SOLVE_BLK, w - jb);
     const T* L = A.fac + fd.panel;
     const T* inv = P.dinv_bw + P.dinv_off[s] + (int64_t)b * SOLVE_BLK * SOLVE_BLK;
+    unsigned int* flag = P.blkflag + P.dinv_off[s] / (SOLVE_BLK * SOLVE_BLK);
     double* Y = A.Y;
     double* Iv = sm;
     double* yb = sm + WT_SMEM_DOUBLES_FIXED;
     double* xb = yb + SOLVE_BLK * nrhs;
-    const int tid = threadIdx.x, nt = blockDim.x, lane = tid & 31, warp = tid >> 5, nwarps = nt >> 5;
+    const int tid = threadIdx.x, nt = blockDim.x, lane = tid & 31, warp = tid >> 5;
     batched_copy<8>(tid, nt, SOLVE_BLK * SOLVE_BLK,
                     [&](int q) { return (q % SOLVE_BLK < bw && q / SOLVE_BLK < bw) ? (double)inv[q] : 0.0; },
                     [&](int q, double v) { Iv[q % SOLVE_BLK + (q / SOLVE_BLK) * (SOLVE_BLK + 1)] = v; });
@@ -698,43 +761,47 @@ __device__ void wide_backward_tile(const PersistArgs<T>& P, int s, int b, int t,
                     [&](int q) { return q % SOLVE_BLK < bw ? Y[fd.c0 + jb + q % SOLVE_BLK + (int64_t)(q / SOLVE_BLK) * n] : 0.0; },
                     [&](int q, double v) { yb[q] = v; });
     __syncthreads();
-    for (int q = tid; q < SOLVE_BLK * nrhs; q += nt) {
-        int i = q % SOLVE_BLK, r = q / SOLVE_BLK;
-        double acc = 0.0;
-#pragma unroll 8
-        for (int j = 0; j < SOLVE_BLK; ++j) acc += Iv[j + i * (SOLVE_BLK + 1)] * yb[j + r * SOLVE_BLK];
-        xb[q] = acc;
-    }
-    __syncthreads();
-    const int c0 = t * SOLVE_BLK;
-    if (t == b) {  // the block's solution: to the scratch, scattered into Y after the level
-        for (int q = tid; q < bw * nrhs; q += nt) {
-            int k = q % bw, r = q / bw;
-            P.xtmp[fd.c0 + jb + k + (int64_t)r * n] = xb[k + r * SOLVE_BLK];
-        }
-    } else {
-        // columns of the tile: 8 per warp, all their loads issued before the reductions
-        const int a0 = c0 + warp * (SOLVE_BLK / 8);
+    const int a0 = jb + warp * (SOLVE_BLK / 8);
+    for (int t = nb - 1; t > b; --t) {
+        const int jt = t * SOLVE_BLK, bwt = min(SOLVE_BLK, w - jt);
+        // this warp's 8 columns of block b against the rows of block t, loaded before the wait
         double l1[SOLVE_BLK / 8], l2[SOLVE_BLK / 8];
 #pragma unroll
         for (int c = 0; c < SOLVE_BLK / 8; ++c) {
             const int a = a0 + c;
-            const bool ok = a < jb;
-            l1[c] = ok && lane < bw ? (double)L[(jb + lane) + (int64_t)a * f] : 0.0;
-            l2[c] = ok && lane + 32 < bw ? (double)L[(jb + lane + 32) + (int64_t)a * f] : 0.0;
+            l1[c] = lane < bwt ? (double)L[(jt + lane) + (int64_t)a * f] : 0.0;
+            l2[c] = lane + 32 < bwt ? (double)L[(jt + lane + 32) + (int64_t)a * f] : 0.0;
         }
+        wait_flag(flag + t, 2u, P.status);
+        for (int q = tid; q < SOLVE_BLK * nrhs; q += nt) {
+            const int k = q % SOLVE_BLK, r = q / SOLVE_BLK;
+            xb[q] = k < bwt ? P.xtmp[fd.c0 + jt + k + (int64_t)r * n] : 0.0;
+        }
+        __syncthreads();
         for (int r = 0; r < nrhs; ++r) {
             const double x1 = xb[lane + r * SOLVE_BLK], x2 = xb[lane + 32 + r * SOLVE_BLK];
 #pragma unroll
             for (int c = 0; c < SOLVE_BLK / 8; ++c) {
                 double v = l1[c] * x1 + l2[c] * x2;
                 for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
-                if (lane == 0 && a0 + c < jb) Y[fd.c0 + a0 + c + (int64_t)r * n] -= v;
+                if (lane == 0) yb[a0 + c - jb + r * SOLVE_BLK] -= v;
             }
         }
+        __syncthreads();
     }
-    (void)f; (void)nwarps;
+    for (int q = tid; q < SOLVE_BLK * nrhs; q += nt) {
+        const int i = q % SOLVE_BLK, r = q / SOLVE_BLK;
+        double acc = 0.0;
+#pragma unroll 8
+        for (int j = 0; j < SOLVE_BLK; ++j) acc += Iv[j + i * (SOLVE_BLK + 1)] * yb[j + r * SOLVE_BLK];
+        xb[q] = acc;
+    }
     __syncthreads();
+    for (int q = tid; q < bw * nrhs; q += nt) {
+        const int k = q % bw, r = q / bw;
+        P.xtmp[fd.c0 + jb + k + (int64_t)r * n] = xb[k + r * SOLVE_BLK];
+    }
+    publish_flag(flag + b, 2u);
 }
 
 __device__ __forceinline__ void trace_mark(int64_t* trace, int cap, int& n, int64_t tag) {
@@ -815,38 +882,25 @@ __global__ void __launch_bounds__(SOLVE_THREADS) persistent_solve_kernel(Persist
         }
         grid_barrier(P.barrier, epoch, P.status);
         TRACE(2, L, 0);
-        const int nb = P.lev_maxblk[L];
-        for (int b = 0; b < nb; ++b) {
-            // (front, row tile) pairs of this step, spread over the grid: task k -> front by running counts
+        if (lc) {
+            // wide fronts: one CTA per (front, row tile); a CTA takes its tiles of a front in increasing
+            // order, so every tile waits only on tiles taken earlier
             int total = 0;
-            for (int i = 0; i < lc; ++i) {
-                const DFront fd = P.fw.fronts[P.list[lo + i]];
-                if (b < (fd.w + SOLVE_BLK - 1) / SOLVE_BLK) total += (fd.f + SOLVE_BLK - 1) / SOLVE_BLK - b;
-            }
+            for (int i = 0; i < lc; ++i) total += (P.fw.fronts[P.list[lo + i]].f + SOLVE_BLK - 1) / SOLVE_BLK;
             for (int k = blockIdx.x; k < total; k += G) {
                 int kk = k;
                 for (int i = 0; i < lc; ++i) {
                     const int s = P.list[lo + i];
-                    const DFront fd = P.fw.fronts[s];
-                    if (b >= (fd.w + SOLVE_BLK - 1) / SOLVE_BLK) continue;
-                    const int cnt = (fd.f + SOLVE_BLK - 1) / SOLVE_BLK - b;
+                    const int cnt = (P.fw.fronts[s].f + SOLVE_BLK - 1) / SOLVE_BLK;
                     if (kk < cnt) {
-                        wide_forward_tile(P, s, b, b + kk, psm);
+                        wide_forward_owner(P, s, kk, psm);
                         break;
                     }
                     kk -= cnt;
                 }
             }
             grid_barrier(P.barrier, epoch, P.status);
-            TRACE(3, L, b);
-        }
-        // the wide fronts' solutions into Y (read again only after later barriers)
-        for (int i = 0; i < lc; ++i) {
-            const DFront fd = P.fw.fronts[P.list[lo + i]];
-            for (int64_t q = gtid; q < (int64_t)fd.w * nrhs; q += gstride) {
-                const int64_t k = q % fd.w, r = q / fd.w;
-                P.fw.Y[fd.c0 + k + r * n] = P.xtmp[fd.c0 + k + r * n];
-            }
+            TRACE(3, L, 0);
         }
     }
     // the copies of the last level's wide fronts must land before Y is read again
@@ -924,29 +978,23 @@ __global__ void __launch_bounds__(SOLVE_THREADS) persistent_solve_kernel(Persist
             }
             grid_barrier(P.barrier, epoch, P.status);
             TRACE(5, L, 0);
-            const int nb = P.lev_maxblk[L];
-            for (int b = nb - 1; b >= 0; --b) {
-                int total = 0;
+            // one CTA per (front, block); a CTA takes its blocks of a front in decreasing order
+            int total = 0;
+            for (int i = 0; i < lc; ++i) total += (P.bw.fronts[P.list[lo + i]].w + SOLVE_BLK - 1) / SOLVE_BLK;
+            for (int k = blockIdx.x; k < total; k += G) {
+                int kk = k;
                 for (int i = 0; i < lc; ++i) {
-                    const DFront fd = P.bw.fronts[P.list[lo + i]];
-                    if (b < (fd.w + SOLVE_BLK - 1) / SOLVE_BLK) total += b + 1;
-                }
-                for (int k = blockIdx.x; k < total; k += G) {
-                    int kk = k;
-                    for (int i = 0; i < lc; ++i) {
-                        const int s = P.list[lo + i];
-                        const DFront fd = P.bw.fronts[s];
-                        if (b >= (fd.w + SOLVE_BLK - 1) / SOLVE_BLK) continue;
-                        if (kk <= b) {
-                            wide_backward_tile(P, s, b, kk, psm);
-                            break;
-                        }
-                        kk -= b + 1;
+                    const int s = P.list[lo + i];
+                    const int nbs = (P.bw.fronts[s].w + SOLVE_BLK - 1) / SOLVE_BLK;
+                    if (kk < nbs) {
+                        wide_backward_owner(P, s, nbs - 1 - kk, psm);
+                        break;
                     }
+                    kk -= nbs;
                 }
-                grid_barrier(P.barrier, epoch, P.status);
-                TRACE(6, L, b);
             }
+            grid_barrier(P.barrier, epoch, P.status);
+            TRACE(6, L, 0);
             // the wide fronts' solutions into Y, undoing their local pivot order
             for (int i = 0; i < lc; ++i) {
                 const DFront fd = P.bw.fronts[P.list[lo + i]];
