@@ -59,7 +59,10 @@ def parse():
     ap.add_argument("--tuning", default=None,
                     help="fsmall,wide,area: fixed front tile shapes instead of the autotuner's search (for profilers)")
     ap.add_argument("--once", choices=["fp64", "mixed"], default=None,
-                    help="one analysis + factorization + solve of the workload in one form, untimed (for profilers)")
+                    help="one analysis + factorization + solve of the workload in one form, untimed (for profilers); "
+                         "with --config c3 or c5 that workload")
+    ap.add_argument("--kkt-grid", type=int, default=200,
+                    help="c3: the KKT's grid (200: n = 55 000; smaller grids scale the constraint count with the area)")
     return ap.parse_args()
 
 
@@ -70,20 +73,42 @@ def run_once(args):
     from sdsb200 import matrices as M
     from sdsb200.solver import DirectSolver
 
-    A, b = workload(args.grid)
     kw = dict(factor_precision="fp32", ir_n_steps=20, ir_tol=BERR_TARGET) if args.once == "mixed" else {}
     if args.tuning:
         from sdsb200.capi import tuning as make_tuning
 
         kw["tuning"] = make_tuning(*[int(v) for v in args.tuning.split(",")])
-    ds = DirectSolver(A, "SPD", reordering_alg="nd", max_nrhs=NRHS, **kw)
+    if args.config in ("c3", "c5"):
+        A, structure, ckw, nrhs = config_matrix(args)
+        kw = {**ckw, **kw}
+        b = M.rhs(A.shape[0], nrhs, seed=0)
+        size = {"kkt_grid": args.kkt_grid} if args.config == "c3" else {"grid": 40}
+    else:
+        A, b = workload(args.grid)
+        structure, nrhs = "SPD", NRHS
+        kw["reordering_alg"] = "nd"
+        size = {"grid": args.grid}
+    ds = DirectSolver(A, structure, max_nrhs=nrhs, **kw)
     ds.execute("analysis")
     ds.execute("factorization")
-    x = ds.execute("solve", None, b)
+    x = ds.execute("solve", None, torch.from_numpy(np.ascontiguousarray(b)).cuda())
     torch.cuda.synchronize()
-    berr = M.scaled_backward_error(A, x.cpu().numpy(), b)
-    print(json.dumps({"once": args.once, "grid": args.grid, "bwd_err": berr}), flush=True)
+    berr = M.scaled_backward_error(A, x.cpu().numpy().reshape(A.shape[0], -1), b.reshape(A.shape[0], -1))
+    print(json.dumps({"once": args.once, "config": args.config, **size, "bwd_err": berr}), flush=True)
     assert berr <= BERR_TARGET
+
+
+def config_matrix(args):
+    """The matrix, structure, solver options and right-hand-side count of --config c1, c3 or c5."""
+    from sdsb200 import matrices as M
+
+    if args.config == "c1":
+        return M.lap2d_shifted(64, 64, seed=0), "SPD", dict(reordering_alg="amd"), 1
+    if args.config == "c3":
+        # statically perturbed pivots make the plain solve inexact: both forms refine to 1e-12
+        g = args.kkt_grid
+        return M.kkt(g, g, int(round(15000 * (g / 200) ** 2)), seed=0), "S", dict(ir_n_steps=20, ir_tol=BERR_TARGET), 1
+    return M.convection_diffusion3d(40, 40, 40, seed=0), "G", dict(pivot_threshold=0.1, reordering_alg="nd"), 8
 
 
 def _time(torch, fn, steps, warmup):
@@ -122,23 +147,19 @@ def run_config(args):
     line = {"config": cfg, "steps": args.steps, "warmup": args.warmup, "data": "synthetic", "forms": {}}
     mixed_kw = dict(factor_precision="fp32", ir_n_steps=20, ir_tol=BERR_TARGET)
     if cfg in ("c1", "c3", "c5"):
+        A, structure, kw, nrhs = config_matrix(args)
         if cfg == "c1":
-            A, structure, kw, nrhs = M.lap2d_shifted(64, 64, seed=0), "SPD", dict(reordering_alg="amd"), 1
             name = "lap2d_64 SPD Cholesky, AMD, 1 RHS"
         elif cfg == "c3":
-            # statically perturbed pivots make the plain solve inexact: both forms refine to 1e-12
-            A, structure, kw, nrhs = M.kkt(200, 200, 15000, seed=0), "S", dict(ir_n_steps=20, ir_tol=BERR_TARGET), 1
-            name = "KKT [H J^T; J 0] n = 55 000 LDL^T (Bunch-Kaufman, pivot pairs), 1 RHS, FP64 refinement"
+            name = "KKT [H J^T; J 0] n = %d LDL^T (Bunch-Kaufman, pivot pairs), 1 RHS, FP64 refinement" % A.shape[0]
         else:
-            A, structure, kw, nrhs = M.convection_diffusion3d(40, 40, 40, seed=0), "G", \
-                dict(pivot_threshold=0.1, reordering_alg="nd"), 8
             name = "convection-diffusion 40^3 LU (threshold 0.1), 8 RHS, solves with A and A^T"
         n = A.shape[0]
         b = M.rhs(n, nrhs, seed=0)
         bt = torch.from_numpy(np.ascontiguousarray(b)).cuda()
         line["workload"] = name
         line["n"], line["nnz"] = int(n), int(A.nnz)
-        if cfg == "c3":
+        if cfg == "c3" and args.kkt_grid == 200:
             line["inertia_expected"] = [40000, 15000]
         base = None
         for form, fkw in (("fp64", {}), ("mixed", mixed_kw)):
