@@ -445,6 +445,8 @@ int run_persistent(Plan* P, int nrhs, bool transpose, const double* in, int64_t 
     a.xtmp = P->d_xtmp;
     a.barrier = P->d_barrier;
     a.blkflag = P->d_blkflag;
+    a.pullflag = P->d_blkflag + P->n_blkflag;
+    a.l21cnt = P->d_blkflag + 2 * P->n_blkflag;
     a.status = P->d_solve_status;
     a.trace = P->profile ? P->d_trace : nullptr;
     a.trace_cap = Plan::TRACE_CAP;
@@ -458,7 +460,7 @@ int run_persistent(Plan* P, int nrhs, bool transpose, const double* in, int64_t 
     const int grid = persistent_solve_grid<T>(smem);
     if (grid <= 0) return fail(SDSB200_CUDA_ERROR, "no co-resident grid for the persistent solve");
     CK(cudaMemsetAsync(P->d_barrier, 0, sizeof(unsigned int), st), "barrier reset");
-    CK(cudaMemsetAsync(P->d_blkflag, 0, sizeof(unsigned int) * P->n_blkflag, st), "block flag reset");
+    CK(cudaMemsetAsync(P->d_blkflag, 0, sizeof(unsigned int) * 3 * P->n_blkflag, st), "block flag reset");
     prof_begin(P, st);
     cudaError_t e = launch_persistent_solve<T>(a, grid, smem, st);
     // algorithmic work: every stored panel entry read once per sweep (2 flops per entry and rhs each

@@ -776,7 +776,7 @@ Plan* build_plan(const sdsb200_symbolic* sym, const sdsb200_plan_options* popts,
         P->d_xtmp = dalloc<double>(P, n * P->max_nrhs);
         P->d_barrier = dalloc<unsigned int>(P, 1);
         P->n_blkflag = std::max<int64_t>(1, P->dinv_len / ((int64_t)SOLVE_BLK * SOLVE_BLK));
-        P->d_blkflag = dalloc<unsigned int>(P, P->n_blkflag);
+        P->d_blkflag = dalloc<unsigned int>(P, 3 * P->n_blkflag);   // block flags, pull flags, L21 counts
         P->d_solve_status = dalloc<int32_t>(P, 1);
         P->d_trace = dalloc<int64_t>(P, 2 * Plan::TRACE_CAP);
         cudaMemsetAsync(P->d_solve_status, 0, sizeof(int32_t), st);

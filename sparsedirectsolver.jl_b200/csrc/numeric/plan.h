@@ -102,8 +102,8 @@ struct Plan {
     int n_binv_tasks = 0;
     double* d_xtmp = nullptr;
     unsigned int* d_barrier = nullptr;
-    unsigned int* d_blkflag = nullptr;   // persistent solve: one flag per 64-column block of the wide fronts
-    int64_t n_blkflag = 0;
+    unsigned int* d_blkflag = nullptr;   // persistent solve: 3 x n_blkflag words (block flags, pull flags,
+    int64_t n_blkflag = 0;               // L21 counts), one per 64-column block of the wide fronts
     int32_t* d_solve_status = nullptr;
     int64_t* d_trace = nullptr;   // persistent-solve phase stamps (profiling)
     static constexpr int TRACE_CAP = 16384;

@@ -55,7 +55,9 @@ struct PersistArgs {
     unsigned int* barrier;     // grid barrier counter (zeroed before the launch)
     unsigned int* blkflag;     // per 64-column diagonal block of the wide fronts (front s: from dinv_off[s] /
                                // 4096): 1 once its forward solution is published, 2 once its backward one is
-                               // (zeroed before the launch)
+    unsigned int* pullflag;    // per wide front (at its first block's index): 1 once its forward pull is done
+    unsigned int* l21cnt;      // per block: columns whose backward -L21^T x2 is applied
+                               // (all three zeroed before the launch)
     int32_t* status;           // nonzero: a barrier or flag wait gave up
     int64_t* trace;            // profiling: (tag, %globaltimer ns) pairs written by CTA 0, or NULL
     int32_t trace_cap;

@@ -636,7 +636,8 @@ __device__ __forceinline__ void wait_flag(const unsigned int* flag, unsigned int
     __syncthreads();
 }
 
-// Forward sweep of a wide front, row tile t (rows 64 t .. 64 t + 63), owned by one CTA: the tile takes
+// Forward sweep of a wide front, row tile t (rows 64 t .. 64 t + 63), owned by one CTA once the front's
+// pull is flagged: the tile takes
 // x_b of every block b <= t in increasing order (rows below block b: y -= L x_b for rows of the block
 // column, u += L x_b for the rows below the front's columns); at b = t the tile holds block t's rows and
 // solves them, x_t = inv(L_tt) y_t, publishing x_t for the tiles below. The arithmetic and its order
@@ -652,12 +653,14 @@ __device__ void wide_forward_owner(const PersistArgs<T>& P, int s, int t, double
     const T* L = A.fac + fd.panel;
     double* Y = A.Y;
     double* u = m > 0 ? A.U + A.uoff[s] : nullptr;
-    unsigned int* flag = P.blkflag + P.dinv_off[s] / (SOLVE_BLK * SOLVE_BLK);
+    const int64_t base = P.dinv_off[s] / (SOLVE_BLK * SOLVE_BLK);
+    unsigned int* flag = P.blkflag + base;
     double* Iv = sm;                                  // SOLVE_BLK x (SOLVE_BLK + 1)
     double* yb = sm + WT_SMEM_DOUBLES_FIXED;          // the tile's rows, SOLVE_BLK x nrhs
     double* xb = yb + SOLVE_BLK * nrhs;               // x of the block being applied
     double* part = xb + SOLVE_BLK * nrhs;             // 4 x SOLVE_BLK x nrhs partial sums
     const int tid = threadIdx.x, nt = blockDim.x;
+    wait_flag(P.pullflag + base, 1u, P.status);       // the front's children are pulled into Y and u
     batched_copy<4>(tid, nt, SOLVE_BLK * nrhs,
                     [&](int q) {
                         const int i = q % SOLVE_BLK, r = q / SOLVE_BLK, row = r0 + i;
@@ -734,8 +737,8 @@ __device__ void wide_forward_owner(const PersistArgs<T>& P, int s, int t, double
     __syncthreads();
 }
 
-// Backward sweep of a wide front, block b (columns 64 b .. 64 b + 63), owned by one CTA, after the
-// grid-wide y1 -= L21^T x2: y_b takes -L_tb^T x_t of every later block t in decreasing order as each
+// Backward sweep of a wide front, block b (columns 64 b .. 64 b + 63), owned by one CTA, once the
+// warps of the y1 -= L21^T x2 phase have counted all of the block's columns: y_b takes -L_tb^T x_t of every later block t in decreasing order as each
 // is published, and x_b = inv(L_bb)^T y_b is published into the scratch. The arithmetic and its
 // order are those of a block-step sweep with a grid barrier after every step.
 template <typename T>
@@ -748,12 +751,14 @@ __device__ void wide_backward_owner(const PersistArgs<T>& P, int s, int b, doubl
     const int jb = b * SOLVE_BLK, bw = min(SOLVE_BLK, w - jb);
     const T* L = A.fac + fd.panel;
     const T* inv = P.dinv_bw + P.dinv_off[s] + (int64_t)b * SOLVE_BLK * SOLVE_BLK;
-    unsigned int* flag = P.blkflag + P.dinv_off[s] / (SOLVE_BLK * SOLVE_BLK);
+    const int64_t base = P.dinv_off[s] / (SOLVE_BLK * SOLVE_BLK);
+    unsigned int* flag = P.blkflag + base;
     double* Y = A.Y;
     double* Iv = sm;
     double* yb = sm + WT_SMEM_DOUBLES_FIXED;
     double* xb = yb + SOLVE_BLK * nrhs;
     const int tid = threadIdx.x, nt = blockDim.x, lane = tid & 31, warp = tid >> 5;
+    wait_flag(P.l21cnt + base + b, f > w ? (unsigned int)bw : 0u, P.status);   // y_b has taken -L21^T x2
     batched_copy<8>(tid, nt, SOLVE_BLK * SOLVE_BLK,
                     [&](int q) { return (q % SOLVE_BLK < bw && q / SOLVE_BLK < bw) ? (double)inv[q] : 0.0; },
                     [&](int q, double v) { Iv[q % SOLVE_BLK + (q / SOLVE_BLK) * (SOLVE_BLK + 1)] = v; });
@@ -802,6 +807,16 @@ __device__ void wide_backward_owner(const PersistArgs<T>& P, int s, int b, doubl
         P.xtmp[fd.c0 + jb + k + (int64_t)r * n] = xb[k + r * SOLVE_BLK];
     }
     publish_flag(flag + b, 2u);
+    if (b == 0) {
+        // the last block of the front's chain: every other block's solution was acquired above, and
+        // every owner of this front has read its y; the solution goes into Y in the original order
+        for (int q = tid; q < w * nrhs; q += nt) {
+            const int k = q % w, r = q / w;
+            const int64_t dst = A.reorder ? A.piv[fd.c0 + k] - 1 : fd.c0 + k;
+            Y[dst + (int64_t)r * n] = P.xtmp[fd.c0 + k + (int64_t)r * n];
+        }
+        __syncthreads();
+    }
 }
 
 __device__ __forceinline__ void trace_mark(int64_t* trace, int cap, int& n, int64_t tag) {
@@ -878,9 +893,8 @@ __global__ void __launch_bounds__(SOLVE_THREADS) persistent_solve_kernel(Persist
                                 return xt[src + (int64_t)(q / w) * n];
                             },
                             [&](int q, double v) { Y[fd.c0 + q % w + (int64_t)(q / w) * n] = v; });
-            __syncthreads();
+            publish_flag(P.pullflag + P.dinv_off[s] / (SOLVE_BLK * SOLVE_BLK), 1u);
         }
-        grid_barrier(P.barrier, epoch, P.status);
         TRACE(2, L, 0);
         if (lc) {
             // wide fronts: one CTA per (front, row tile); a CTA takes its tiles of a front in increasing
@@ -899,9 +913,9 @@ __global__ void __launch_bounds__(SOLVE_THREADS) persistent_solve_kernel(Persist
                     kk -= cnt;
                 }
             }
-            grid_barrier(P.barrier, epoch, P.status);
-            TRACE(3, L, 0);
         }
+        grid_barrier(P.barrier, epoch, P.status);
+        TRACE(3, L, 0);
     }
     // the copies of the last level's wide fronts must land before Y is read again
     grid_barrier(P.barrier, epoch, P.status);
@@ -975,10 +989,26 @@ __global__ void __launch_bounds__(SOLVE_THREADS) persistent_solve_kernel(Persist
                         if (lane == 0 && r < rc) P.bw.Y[fd.c0 + j + (int64_t)(r0 + r) * n] -= v;
                     }
                 }
+                if (lane == 0) {   // release the column to its block's owner
+                    __threadfence();
+                    atomicAdd(P.l21cnt + P.dinv_off[s] / (SOLVE_BLK * SOLVE_BLK) + j / SOLVE_BLK, 1u);
+                }
+                __syncwarp();
             }
-            grid_barrier(P.barrier, epoch, P.status);
             TRACE(5, L, 0);
-            // one CTA per (front, block); a CTA takes its blocks of a front in decreasing order
+        }
+        // the level's small fronts (independent of its wide fronts; nothing here waits)
+        if (sc >= G * (blockDim.x >> 5) / 2) {
+            const int wpc = blockDim.x >> 5, warp = threadIdx.x >> 5;
+            double* xs = psm + warp * P.warp_smem;
+            for (int i = blockIdx.x * wpc + warp; i < sc; i += G * wpc)
+                warp_backward_front(P.bw, P.list[so + i], xs, xs + P.warp_xs);
+        } else {
+            for (int i = blockIdx.x; i < sc; i += G) backward_front(P.bw, P.list[so + i], 0, psm);
+        }
+        if (lc) {
+            // one CTA per (front, block); a CTA takes its blocks of a front in decreasing order, and the
+            // owner of block 0 puts the front's solution into Y
             int total = 0;
             for (int i = 0; i < lc; ++i) total += (P.bw.fronts[P.list[lo + i]].w + SOLVE_BLK - 1) / SOLVE_BLK;
             for (int k = blockIdx.x; k < total; k += G) {
@@ -993,25 +1023,6 @@ __global__ void __launch_bounds__(SOLVE_THREADS) persistent_solve_kernel(Persist
                     kk -= nbs;
                 }
             }
-            grid_barrier(P.barrier, epoch, P.status);
-            TRACE(6, L, 0);
-            // the wide fronts' solutions into Y, undoing their local pivot order
-            for (int i = 0; i < lc; ++i) {
-                const DFront fd = P.bw.fronts[P.list[lo + i]];
-                for (int64_t q = gtid; q < (int64_t)fd.w * nrhs; q += gstride) {
-                    const int64_t k = q % fd.w, r = q / fd.w;
-                    const int64_t dst = P.bw.reorder ? P.bw.piv[fd.c0 + k] - 1 : fd.c0 + k;
-                    P.bw.Y[dst + r * n] = P.xtmp[fd.c0 + k + r * n];
-                }
-            }
-        }
-        if (sc >= G * (blockDim.x >> 5) / 2) {
-            const int wpc = blockDim.x >> 5, warp = threadIdx.x >> 5;
-            double* xs = psm + warp * P.warp_smem;
-            for (int i = blockIdx.x * wpc + warp; i < sc; i += G * wpc)
-                warp_backward_front(P.bw, P.list[so + i], xs, xs + P.warp_xs);
-        } else {
-            for (int i = blockIdx.x; i < sc; i += G) backward_front(P.bw, P.list[so + i], 0, psm);
         }
         grid_barrier(P.barrier, epoch, P.status);
         TRACE(7, L, 0);
