@@ -24,6 +24,7 @@ NUMERIC_SOURCES = [
     "numeric/plan.cu",
     "numeric/factor_kernels.cu",
     "numeric/dense_kernels.cu",
+    "numeric/pivot_kernels.cu",
     "numeric/solve_kernels.cu",
     "numeric/adjoint_kernels.cu",
     "numeric/tc_kernels.cu",
@@ -52,6 +53,11 @@ def build_analysis(force: bool = False) -> str:
     return out
 
 
+# Units that restate the reference's scalar in-front arithmetic: no fused multiply-add, so that their
+# values, and the pivots and inertia that depend on exact cancellation, match the reference's
+NO_CONTRACTION = {"factor_kernels.cu", "pivot_kernels.cu"}
+
+
 def build_numeric(force: bool = False) -> str:
     out = os.path.join(HERE, "libsdsb200.so")
     srcs = [os.path.join(CSRC, s) for s in NUMERIC_SOURCES]
@@ -64,8 +70,9 @@ def build_numeric(force: bool = False) -> str:
     objs = []
     for s in srcs:
         o = os.path.join(objdir, os.path.basename(s).replace(".cu", ".o"))
+        fmad = ["--fmad=false"] if os.path.basename(s) in NO_CONTRACTION else []
         _run([NVCC, *ARCH, "-lineinfo", "-O3", "-std=c++17", "-Xcompiler", "-fPIC", "-I", INCLUDE,
-              "--expt-relaxed-constexpr", "-c", s, "-o", o])
+              "--expt-relaxed-constexpr", *fmad, "-c", s, "-o", o])
         objs.append(o)
     _run([NVCC, *ARCH, "-shared", "-o", out, *objs, "-lcudart"])
     return out

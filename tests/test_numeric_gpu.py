@@ -172,6 +172,57 @@ def test_lu_convection_diffusion(torch_cuda, g):
     assert _check_solve(ds, A, 2, transpose=True) <= BERR
 
 
+@pytest.mark.parametrize("case", ["kkt_ldlt", "cd_lu", "kkt_lu"])
+def test_wide_fronts_many_chunks(torch_cuda, case):
+    # fronts of more than two 256-row chunks, and (kkt_ldlt, cd_lu) of more than one 32-column group:
+    # the chunked large-front assembly, and the cooperative kernel's per-chunk column maxima, update
+    # items and deferred multiplier writes; kkt_lu also interchanges hundreds of rows
+    if case == "kkt_ldlt":
+        A, st, kw = small_kkt(40, 40, 600, seed=3), "S", {}
+    elif case == "cd_lu":
+        A, st, kw = M.convection_diffusion3d(28, 28, 28, seed=1), "G", dict(pivot_threshold=0.1, reordering_alg="nd")
+    else:
+        A, st, kw = small_kkt(40, 40, 600, seed=3), "G", dict(pivot_threshold=0.1)
+    okw = {"pivot_threshold": kw["pivot_threshold"]} if st == "G" else {}
+    if case == "kkt_lu":
+        # LU of the KKT perturbs 189 zero pivots to +-eps, which grows entries to ~1e13. The large
+        # fronts' contribution-block GEMMs (blocked sums on the tensor cores, as the reference's
+        # cuBLAS path) then differ from the oracle's sequential sums by more than the 1e-10 bound.
+        # Pivots, kinds, statistics and perm_row stay exact.
+        S, O, info = oracle_for(A, st, **okw)
+        ds = _solver(A, st, **kw)
+        ds.execute("analysis")
+        assert np.array_equal(ds.symbolic.perm, S.perm)
+        assert ds.execute("factorization") == info
+        piv, kind, d = ds.pivots_host()
+        assert np.array_equal(piv[: S.n], O.piv[: S.n])
+        assert np.array_equal(kind[: S.n], O.kind[: S.n])
+        assert np.array_equal(ds.stats_host(), O.stats_matrix())
+        fac, ufac = ds.factor_host()
+        assert rel_max_diff(dense_panels(S, fac), dense_panels(S, O.factor)) <= 1e-6
+        assert rel_max_diff(dense_panels(S, ufac), dense_panels(S, O.ufactor)) <= 1e-6
+    else:
+        ds, S, O = _check_factor(A, st, torch_cuda, okw=okw, **kw)
+    f, w = S.front_nrows.astype(int), S.front_ncols.astype(int)
+    assert f.max() > 512
+    if case != "kkt_lu":
+        assert ((f > 512) & (w > 32)).any()
+    else:
+        assert (O.piv[: S.n] != np.arange(1, S.n + 1)).sum() > 100
+    # a plain FP64 solve reaches the bound only without statically perturbed pivots (the KKT cases
+    # perturb some: their parity is the factor's)
+    exact = O.stats_matrix()[:, 3].sum() == 0
+    if st == "G":
+        assert np.array_equal(ds.getparam("perm_row"), S.perm[O.piv[: S.n] - 1])
+        if exact:
+            assert _check_solve(ds, A, 2) <= BERR
+            assert _check_solve(ds, A, 2, transpose=True) <= BERR
+    else:
+        assert ds.getparam("inertia") == (1600, 600)
+        if exact:
+            assert _check_solve(ds, A, 2) <= BERR
+
+
 def test_lu_row_swaps(torch_cuda):
     # weak diagonal: threshold pivoting must swap rows inside the fully-summed block
     rng = np.random.default_rng(7)
