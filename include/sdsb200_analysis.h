@@ -78,6 +78,22 @@ int sdsa_get(const sdsa_result* r, const char* name, int64_t* out);
 double sdsa_stat(const sdsa_result* r, const char* name);
 
 void sdsa_free(sdsa_result* r);
+
+/* Matching and scaling of the n x n CSR matrix (rowptr, colval, nzval; index_base 0 or 1) from its
+ * values: MC64 (Duff & Koster 2001) as the reference's compute_matching runs it at analysis
+ * (src/matching/mc64.jl:302-398). `job` is the reference's matching_alg: 1 maximum cardinality,
+ * 2 and 3 bottleneck (largest smallest matched |a_ij|), 4 maximum sum, 5 maximum product with the
+ * scalings, 6 the automatic choice (= 5).
+ * structure SDSA_STRUCTURE_G matches the stored rows; the symmetric structures match the full matrix
+ * rebuilt from the triangle `view` selects, and return the symmetric scaling d = sqrt(r c)
+ * (rscale = cscale = d, |d_i a_ij d_j| <= 1).
+ * Outputs, n entries each: perm (1-based column matched to each row, the reference's
+ * "perm_matching"; unmatched rows of a structurally singular matrix take the unmatched columns in
+ * increasing order), matched (1 or 0), rscale and cscale ("scale_row", "scale_col"; ones for jobs 1-4).
+ * Returns 0, or -1 with the message in sdsa_last_error(). */
+int sdsa_matching(int64_t n, const int64_t* rowptr, const int64_t* colval, const double* nzval, int structure,
+                  int view, int index_base, int job, int64_t* perm, int8_t* matched, double* rscale,
+                  double* cscale);
 const char* sdsa_last_error(void);
 
 #ifdef __cplusplus

@@ -13,6 +13,7 @@
 #include <cmath>
 #include <cstdint>
 #include <cstring>
+#include <limits>
 #include <memory>
 #include <tuple>
 #include <numeric>
@@ -1126,6 +1127,289 @@ void build_maps(sdsa_result& R, const Csr& A, int structure, int view) {
     for (int r = 1; r <= A.n; ++r) R.full_rowptr[r] = R.full_rowptr[r - 1] + nrow[r];
 }
 
+// ---------------------------------------------------------------------------
+// Matching and scaling: MC64 (Duff & Koster 2001) as the reference restates it
+// (src/matching/mc64.jl). Rows of the square matrix are matched to columns from
+// |a_ij|, on the host, from the values. 0-based in this section.
+
+// Row-wise |a| of the matrix the matching reads (`_abs_csr`, mc64.jl:216-239): "G" the stored rows;
+// the symmetric structures the full matrix rebuilt from the view's triangle. Duplicates are summed
+// (in input order) before the absolute value; explicit zeros stay (job 1 counts them). Columns of a
+// row ascending.
+struct AbsCsr {
+    vector<i64> ptr;
+    vector<int> adj;
+    vector<double> w;
+};
+
+AbsCsr abs_csr(const Csr& A, const double* nz, int structure, int view) {
+    const int n = A.n;
+    struct Entry {
+        int r, c;
+        double x;
+    };
+    vector<Entry> e;
+    for (int r = 1; r <= n; ++r)
+        for (i64 p = A.rp[r]; p < A.rp[r + 1]; ++p) {
+            const int c = (int)A.cv[p];
+            if (!keep_entry(structure, view, r, c)) continue;
+            const double x = nz[p - 1];
+            e.push_back({r - 1, c - 1, x});
+            if (structure != SDSA_STRUCTURE_G && r != c) e.push_back({c - 1, r - 1, x});
+        }
+    std::stable_sort(e.begin(), e.end(), [](const Entry& a, const Entry& b) { return a.r != b.r ? a.r < b.r : a.c < b.c; });
+    AbsCsr M;
+    M.ptr.assign(n + 1, 0);
+    for (size_t k = 0; k < e.size();) {
+        size_t q = k;
+        double sum = 0.0;
+        for (; q < e.size() && e[q].r == e[k].r && e[q].c == e[k].c; ++q) sum += e[q].x;
+        M.adj.push_back(e[k].c);
+        M.w.push_back(std::fabs(sum));
+        M.ptr[e[k].r + 1]++;
+        k = q;
+    }
+    for (int i = 0; i < n; ++i) M.ptr[i + 1] += M.ptr[i];
+    return M;
+}
+
+// Binary min-heap of (key, vertex) with lazy deletion. Equal keys keep the order of the sift rules
+// below (parent wins ties going up, the left child wins ties going down), so the matching's choices
+// among equal distances are reproducible.
+struct MinHeap {
+    vector<double> key;
+    vector<int> val;
+    void clear() { key.clear(); val.clear(); }
+    bool empty() const { return key.empty(); }
+    void push(double k, int v) {
+        key.push_back(k);
+        val.push_back(v);
+        size_t i = key.size() - 1;
+        while (i > 0) {
+            const size_t p = (i - 1) / 2;
+            if (key[p] <= key[i]) break;
+            std::swap(key[p], key[i]);
+            std::swap(val[p], val[i]);
+            i = p;
+        }
+    }
+    void pop(double& k, int& v) {
+        k = key[0];
+        v = val[0];
+        const double lk = key.back();
+        const int lv = val.back();
+        key.pop_back();
+        val.pop_back();
+        const size_t m = key.size();
+        if (m == 0) return;
+        key[0] = lk;
+        val[0] = lv;
+        size_t i = 0;
+        while (true) {
+            const size_t l = 2 * i + 1;
+            if (l >= m) break;
+            const size_t c = (l + 1 < m && key[l + 1] < key[l]) ? l + 1 : l;
+            if (key[i] <= key[c]) break;
+            std::swap(key[i], key[c]);
+            std::swap(val[i], val[c]);
+            i = c;
+        }
+    }
+};
+
+// Minimum-cost matching of maximum cardinality between rows 0..n-1 and columns 0..n-1 (costs >= 0 on
+// the edges adj[ptr[i]..ptr[i+1]), by successive shortest augmenting paths: Dijkstra on the reduced
+// costs cost - u[i] - v[j] >= 0 (min_cost_matching, mc64.jl:109-189). lmate[i] = the column matched to
+// row i or -1; u + v <= cost on every edge, with equality on the matched ones.
+void min_cost_matching(const vector<i64>& ptr, const vector<int>& adj, const vector<double>& cost, int n,
+                       vector<int>& lmate, vector<double>& u, vector<double>& v) {
+    const double inf = std::numeric_limits<double>::infinity();
+    lmate.assign(n, -1);
+    vector<int> rmate(n, -1);
+    u.assign(n, 0.0);
+    v.assign(n, 0.0);
+    // feasible start (u = min(0, row minimum) = 0 for nonnegative costs, v = 0), then a cheap
+    // matching of the tight edges
+    for (int i = 0; i < n; ++i) {
+        double mn = 0.0;
+        for (i64 p = ptr[i]; p < ptr[i + 1]; ++p) mn = std::min(mn, cost[p]);
+        u[i] = mn;
+        for (i64 p = ptr[i]; p < ptr[i + 1]; ++p) {
+            const int j = adj[p];
+            if (rmate[j] < 0 && cost[p] - u[i] <= 0.0) {
+                lmate[i] = j;
+                rmate[j] = i;
+                break;
+            }
+        }
+    }
+    vector<double> dist(n, inf);
+    vector<int> pred(n, -1);
+    vector<char> done(n, 0);
+    vector<int> touched, finals;
+    MinHeap heap;
+    for (int i0 = 0; i0 < n; ++i0) {
+        if (lmate[i0] >= 0) continue;
+        touched.clear();
+        finals.clear();
+        heap.clear();
+        int cur = i0, jfree = -1;
+        double dcur = 0.0, len = inf;
+        while (true) {
+            for (i64 p = ptr[cur]; p < ptr[cur + 1]; ++p) {
+                const int j = adj[p];
+                if (done[j]) continue;
+                const double nd = dcur + std::max(cost[p] - u[cur] - v[j], 0.0);
+                if (nd < dist[j]) {
+                    if (std::isinf(dist[j])) touched.push_back(j);
+                    dist[j] = nd;
+                    pred[j] = cur;
+                    heap.push(nd, j);
+                }
+            }
+            int j = -1;
+            while (!heap.empty()) {
+                double d;
+                int jj;
+                heap.pop(d, jj);
+                if (done[jj] || d > dist[jj]) continue;
+                j = jj;
+                break;
+            }
+            if (j < 0) break;   // no augmenting path: row i0 stays unmatched
+            done[j] = 1;
+            finals.push_back(j);
+            if (rmate[j] < 0) {
+                jfree = j;
+                len = dist[j];
+                break;
+            }
+            cur = rmate[j];     // the matched edge has reduced cost 0
+            dcur = dist[j];
+        }
+        if (jfree >= 0) {
+            u[i0] += len;
+            for (int j : finals) {
+                if (j == jfree) continue;
+                u[rmate[j]] += len - dist[j];
+                v[j] -= len - dist[j];
+            }
+            int j = jfree;
+            while (true) {      // flip the alternating path
+                const int i = pred[j];
+                const int nj = lmate[i];
+                lmate[i] = j;
+                rmate[j] = i;
+                if (i == i0) break;
+                j = nj;
+            }
+        }
+        for (int j : touched) {
+            dist[j] = inf;
+            done[j] = 0;
+        }
+    }
+}
+
+int matched_count(const vector<int>& lmate) {
+    int c = 0;
+    for (int j : lmate) c += j >= 0;
+    return c;
+}
+
+// maximum cardinality matching on the edges with keep[p] (zero costs)
+vector<int> cardinality_matching(const AbsCsr& M, int n, const vector<char>& keep) {
+    vector<i64> sp(n + 1, 0);
+    vector<int> sa;
+    for (int i = 0; i < n; ++i) {
+        for (i64 p = M.ptr[i]; p < M.ptr[i + 1]; ++p)
+            if (keep[p]) sa.push_back(M.adj[p]);
+        sp[i + 1] = (i64)sa.size();
+    }
+    vector<int> lmate;
+    vector<double> u, v;
+    min_cost_matching(sp, sa, vector<double>(sa.size(), 0.0), n, lmate, u, v);
+    return lmate;
+}
+
+// jobs 2 and 3: maximize the smallest matched |a_ij| (bottleneck), by bisection over the distinct
+// nonzero values (`_bottleneck_matching`, mc64.jl:258-279)
+vector<int> bottleneck_matching(const AbsCsr& M, int n) {
+    const size_t ne = M.w.size();
+    vector<int> full = cardinality_matching(M, n, vector<char>(ne, 1));
+    const int target = matched_count(full);
+    vector<double> vals;
+    for (double x : M.w)
+        if (x > 0) vals.push_back(x);
+    std::sort(vals.begin(), vals.end());
+    vals.erase(std::unique(vals.begin(), vals.end()), vals.end());
+    if (vals.empty()) return full;
+    auto at_least = [&](double t) {
+        vector<char> keep(ne);
+        for (size_t p = 0; p < ne; ++p) keep[p] = M.w[p] >= t;
+        return cardinality_matching(M, n, keep);
+    };
+    vector<int> best = at_least(vals[0]);
+    if (matched_count(best) != target) return full;
+    size_t lo = 0, hi = vals.size() - 1;   // the largest threshold index that keeps `target` matches
+    while (lo < hi) {
+        const size_t mid = (lo + hi + 1) >> 1;
+        vector<int> m = at_least(vals[mid]);
+        if (matched_count(m) == target) {
+            lo = mid;
+            best = std::move(m);
+        } else {
+            hi = mid - 1;
+        }
+    }
+    return best;
+}
+
+void finite_scaling(vector<double>& s) {
+    for (double& x : s)
+        if (!(std::isfinite(x) && x > 0)) x = 1.0;
+}
+
+// MC64 jobs 1-5 (`mc64`, mc64.jl:302-333): lmate and the row / column scalings (ones except job 5,
+// r_i = exp(u_i) / max_k |a_ik|, c_j = exp(v_j) from the assignment on log max_k |a_ik| - log |a_ij|,
+// so that |r_i a_ij c_j| <= 1 with equality on the matched entries)
+void mc64(const AbsCsr& M, int n, int job, vector<int>& lmate, vector<double>& rs, vector<double>& cs) {
+    rs.assign(n, 1.0);
+    cs.assign(n, 1.0);
+    if (job == 1) {
+        lmate = cardinality_matching(M, n, vector<char>(M.w.size(), 1));
+        return;
+    }
+    if (job == 2 || job == 3) {
+        lmate = bottleneck_matching(M, n);
+        return;
+    }
+    vector<double> rowmax(n, 0.0);
+    for (int i = 0; i < n; ++i)
+        for (i64 p = M.ptr[i]; p < M.ptr[i + 1]; ++p) rowmax[i] = std::max(rowmax[i], M.w[p]);
+    vector<i64> sp(n + 1, 0);
+    vector<int> sa;
+    vector<double> cost;
+    for (int i = 0; i < n; ++i) {
+        for (i64 p = M.ptr[i]; p < M.ptr[i + 1]; ++p) {
+            if (!(M.w[p] > 0)) continue;
+            sa.push_back(M.adj[p]);
+            cost.push_back(job == 5 ? std::log(rowmax[i]) - std::log(M.w[p]) : rowmax[i] - M.w[p]);
+        }
+        sp[i + 1] = (i64)sa.size();
+    }
+    vector<double> u, v;
+    min_cost_matching(sp, sa, cost, n, lmate, u, v);
+    if (job == 5) {
+        for (int i = 0; i < n; ++i) {
+            rs[i] = rowmax[i] > 0 ? std::exp(u[i]) / rowmax[i] : 1.0;
+            cs[i] = std::exp(v[i]);
+        }
+        finite_scaling(rs);
+        finite_scaling(cs);
+    }
+}
+
 }  // namespace
 
 extern "C" {
@@ -1336,5 +1620,65 @@ double sdsa_stat(const sdsa_result* r, const char* name) {
 }
 
 void sdsa_free(sdsa_result* r) { delete r; }
+
+int sdsa_matching(int64_t n, const int64_t* rowptr, const int64_t* colval, const double* nzval, int structure,
+                  int view, int index_base, int job, int64_t* perm, int8_t* matched, double* rscale,
+                  double* cscale) {
+    try {
+        if (n < 0) throw AnalysisError("n must be nonnegative");
+        if (structure != SDSA_STRUCTURE_G && structure != SDSA_STRUCTURE_S && structure != SDSA_STRUCTURE_SPD)
+            throw AnalysisError("structure must be G, S or SPD");
+        if (view != 'L' && view != 'U' && view != 'F') throw AnalysisError("view must be 'L', 'U' or 'F'");
+        if (job == 6) job = 5;   // "algo6" (automatic) runs job 5
+        if (job < 1 || job > 5) throw AnalysisError("unknown matching job; expected 1 to 6");
+        if (n > 0 && (!rowptr || !colval || !nzval || !perm || !matched || !rscale || !cscale))
+            throw AnalysisError("NULL array");
+        Csr A = host_pattern(n, rowptr, colval, index_base);
+        const int nn = (int)n;
+        AbsCsr M = abs_csr(A, nzval, structure, view);
+        vector<int> lmate;
+        vector<double> rs, cs;
+        mc64(M, nn, job, lmate, rs, cs);
+        // the matching permutation (`_complete_matching`, mc64.jl:344-357): unmatched rows take the
+        // unmatched columns in increasing order
+        vector<char> used(nn, 0);
+        for (int j : lmate)
+            if (j >= 0) used[j] = 1;
+        int next_free = 0;
+        for (int i = 0; i < nn; ++i) {
+            matched[i] = lmate[i] >= 0 ? 1 : 0;
+            int j = lmate[i];
+            if (j < 0) {
+                while (used[next_free]) ++next_free;
+                j = next_free++;
+            }
+            perm[i] = j + 1;
+        }
+        if (structure == SDSA_STRUCTURE_G) {
+            for (int i = 0; i < nn; ++i) {
+                rscale[i] = rs[i];
+                cscale[i] = cs[i];
+            }
+            return 0;
+        }
+        // symmetric scaling d = sqrt(r c) (Duff & Pralet 2005); an unmatched index takes
+        // 1 / max_j |a_ij| d_j over its matched neighbours (compute_matching, mc64.jl:378-398)
+        vector<double> d(nn);
+        for (int i = 0; i < nn; ++i) d[i] = std::sqrt(rs[i] * cs[i]);
+        for (int i = 0; i < nn; ++i) {
+            if (matched[i]) continue;
+            double m = 0.0;
+            for (i64 p = M.ptr[i]; p < M.ptr[i + 1]; ++p)
+                if (matched[M.adj[p]]) m = std::max(m, M.w[p] * d[M.adj[p]]);
+            d[i] = m > 0 ? 1.0 / m : 1.0;
+        }
+        finite_scaling(d);
+        for (int i = 0; i < nn; ++i) rscale[i] = cscale[i] = d[i];
+        return 0;
+    } catch (const std::exception& e) {
+        g_err = e.what();
+        return -1;
+    }
+}
 
 }  // extern "C"

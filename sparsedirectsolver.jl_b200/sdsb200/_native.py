@@ -42,6 +42,9 @@ def analysis_lib():
         lib.sdsa_free.restype = None
         lib.sdsa_last_error.argtypes = []
         lib.sdsa_last_error.restype = C.c_char_p
+        lib.sdsa_matching.argtypes = [C.c_int64, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_int,
+                                      C.c_int, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
+        lib.sdsa_matching.restype = C.c_int
         _analysis = lib
     return _analysis
 

@@ -111,3 +111,51 @@ def analyze(rowptr, colval, n, structure="SPD", nzval=None, view="F", index_base
 def analyze_csr(A, structure="SPD", **kw) -> Symbolic:
     """``analyze`` for a scipy CSR matrix (0-based arrays)."""
     return analyze(A.indptr, A.indices, A.shape[0], structure, nzval=A.data, index_base=0, **kw)
+
+
+MATCHING_JOBS = {"algo1": 1, "algo2": 2, "algo3": 3, "algo4": 4, "algo5": 5, "algo6": 6}
+
+
+@dataclass
+class Matching:
+    """Result of :func:`compute_matching`, the reference's ``Matching`` (src/matching/mc64.jl:18-45).
+
+    ``perm[i]`` is the 1-based column matched to row ``i`` (``"perm_matching"``), ``matched[i]`` whether
+    row ``i`` has a matched entry, ``rscale``/``cscale`` the row and column scalings (``"scale_row"``,
+    ``"scale_col"``; ones for jobs 1-4, equal for the symmetric structures, whose factored matrix
+    would be ``D A D``)."""
+
+    job: int
+    perm: np.ndarray
+    matched: np.ndarray
+    rscale: np.ndarray
+    cscale: np.ndarray
+    symmetric: bool
+
+
+def compute_matching(rowptr, colval, nzval, n, structure="G", matching_alg="algo5", view="F",
+                     index_base=0) -> Matching:
+    """MC64 matching and scaling of an ``n x n`` CSR matrix from its values (``compute_matching``,
+    src/matching/mc64.jl:378-398): ``matching_alg`` ``"algo1"``-``"algo6"`` (or 1-6) is the MC64 job.
+    ``"G"`` matches the stored rows; ``"S"``/``"SPD"`` the full matrix read from ``view``'s triangle,
+    with the symmetric scaling ``d = sqrt(r c)``."""
+    lib = analysis_lib()
+    job = MATCHING_JOBS[matching_alg] if isinstance(matching_alg, str) else int(matching_alg)
+    rp = np.ascontiguousarray(rowptr, dtype=np.int64)
+    cv = np.ascontiguousarray(colval, dtype=np.int64)
+    if rp.size != n + 1:
+        raise ValueError(f"rowptr has {rp.size} entries, expected n + 1 = {n + 1}")
+    nz = np.ascontiguousarray(np.asarray(nzval, dtype=np.float64).reshape(-1)[: cv.size])
+    perm = np.zeros(max(n, 1), np.int64)
+    matched = np.zeros(max(n, 1), np.int8)
+    rs = np.ones(max(n, 1))
+    cs = np.ones(max(n, 1))
+    rc = lib.sdsa_matching(C.c_int64(n), rp.ctypes.data_as(C.c_void_p), cv.ctypes.data_as(C.c_void_p),
+                           nz.ctypes.data_as(C.c_void_p), STRUCTURES[structure], ord(view), int(index_base), job,
+                           perm.ctypes.data_as(C.c_void_p), matched.ctypes.data_as(C.c_void_p),
+                           rs.ctypes.data_as(C.c_void_p), cs.ctypes.data_as(C.c_void_p))
+    if rc != 0:
+        raise ValueError("matching failed: " + lib.sdsa_last_error().decode())
+    return Matching(job=5 if job == 6 else job, perm=perm[:n], matched=matched[:n].astype(bool), rscale=rs[:n],
+                    cscale=cs[:n], symmetric=structure != "G")
+

@@ -1,0 +1,136 @@
+"""MC64 matching and scaling of the analysis library (CPU).
+
+The reference's matching (src/matching/mc64.jl) has no golden outputs, and Julia cannot run here, so
+the checks are the properties its docstrings state and the reference's own matching tests assert
+(optimality of the assignment, the scaling bounds, the completion rule), against scipy's
+independent assignment and bipartite-matching solvers.
+"""
+import numpy as np
+import pytest
+import scipy.sparse as sp
+from scipy.optimize import linear_sum_assignment
+from scipy.sparse.csgraph import maximum_bipartite_matching
+
+from sdsb200.analysis import compute_matching
+
+
+def _random_nonsingular(n, density, seed):
+    """Sparse n x n with a full structural matching hidden behind a random column permutation."""
+    rng = np.random.default_rng(seed)
+    A = sp.random(n, n, density=density, random_state=seed, format="coo")
+    P = sp.coo_matrix((rng.uniform(0.1, 10.0, n) * rng.choice([-1, 1], n), (np.arange(n), rng.permutation(n))),
+                      shape=(n, n))
+    A = (A + P).tocsr()
+    A.data *= np.exp(rng.normal(0, 3, A.nnz))          # values spread over many orders of magnitude
+    return A
+
+
+def _matched_values(A, perm):
+    D = np.abs(A.toarray())
+    return D[np.arange(A.shape[0]), perm - 1]
+
+
+def _optimum(A, objective):
+    D = np.abs(A.toarray())
+    if objective == "product":
+        cost = np.where(D > 0, -np.log(np.where(D > 0, D, 1.0)), 1e6)
+    else:
+        cost = np.where(D > 0, -D, 1e12)
+    r, c = linear_sum_assignment(cost)
+    return D[r, c]
+
+
+@pytest.mark.parametrize("seed", [0, 1, 2])
+def test_job5_maximizes_product_and_scales(seed):
+    A = _random_nonsingular(60, 0.08, seed)
+    m = compute_matching(A.indptr, A.indices, A.data, 60, "G", "algo5")
+    assert m.matched.all()
+    assert sorted(m.perm) == list(range(1, 61))
+    got = np.log(_matched_values(A, m.perm)).sum()
+    best = np.log(_optimum(A, "product")).sum()
+    assert got == pytest.approx(best, rel=0, abs=1e-9 * max(1.0, abs(best)))
+    # |r_i a_ij c_j| <= 1 on every stored entry, = 1 on the matched ones
+    S = sp.diags(m.rscale) @ abs(A) @ sp.diags(m.cscale)
+    assert S.max() <= 1 + 1e-12
+    assert np.allclose(S.toarray()[np.arange(60), m.perm - 1], 1.0, rtol=1e-12)
+
+
+def test_job4_maximizes_sum():
+    A = _random_nonsingular(50, 0.1, 7)
+    m = compute_matching(A.indptr, A.indices, A.data, 50, "G", 4)
+    assert _matched_values(A, m.perm).sum() == pytest.approx(_optimum(A, "sum").sum(), rel=1e-12)
+    assert np.all(m.rscale == 1.0) and np.all(m.cscale == 1.0)
+
+
+@pytest.mark.parametrize("job", [2, 3])
+def test_bottleneck_jobs(job):
+    A = _random_nonsingular(40, 0.1, 11)
+    m = compute_matching(A.indptr, A.indices, A.data, 40, "G", job)
+    assert m.matched.all()
+    got = _matched_values(A, m.perm).min()
+    # the largest threshold that still admits a perfect matching
+    vals = np.unique(np.abs(A.data[A.data != 0]))
+    best = 0.0
+    for t in vals:
+        B = A.copy()
+        B.data = (np.abs(B.data) >= t).astype(float)
+        B.eliminate_zeros()
+        if (maximum_bipartite_matching(B, perm_type="column") >= 0).sum() == 40:
+            best = t
+    assert got == best
+
+
+def test_job1_structurally_singular_completion():
+    # rows 2 and 5 share their only columns with others: structural rank n - 1
+    rows = [0, 0, 1, 2, 3, 3, 4, 5, 6]
+    cols = [0, 1, 1, 2, 3, 4, 4, 2, 6]
+    A = sp.csr_matrix((np.ones(len(rows)), (rows, cols)), shape=(7, 7))
+    m = compute_matching(A.indptr, A.indices, A.data, 7, "G", "algo1")
+    rank = (maximum_bipartite_matching(A, perm_type="column") >= 0).sum()
+    assert m.matched.sum() == rank == 6
+    assert sorted(m.perm) == list(range(1, 8))
+    for i in np.nonzero(m.matched)[0]:
+        assert A[i, m.perm[i] - 1] != 0
+    # the unmatched row takes the unmatched column (here column 6, 1-based)
+    (u,) = np.nonzero(~m.matched)
+    assert m.perm[u[0]] == 6
+
+
+def test_explicit_zero_counts_for_job1_only():
+    A = sp.csr_matrix((np.array([1.0, 0.0, 1.0]), (np.array([0, 1, 1]), np.array([1, 0, 1]))), shape=(2, 2))
+    assert compute_matching(A.indptr, A.indices, A.data, 2, "G", 1).matched.all()
+    assert not compute_matching(A.indptr, A.indices, A.data, 2, "G", 5).matched.all()
+
+
+@pytest.mark.parametrize("structure", ["S", "SPD"])
+def test_symmetric_scaling_from_either_triangle(structure):
+    rng = np.random.default_rng(3)
+    B = sp.random(80, 80, density=0.05, random_state=3, format="csr")
+    A = (B + B.T).tocsr()
+    A.setdiag(rng.uniform(0.01, 100.0, 80) * (1 if structure == "SPD" else rng.choice([-1, 1], 80)))
+    A = A.tocsr()
+    A.sort_indices()
+    full = compute_matching(A.indptr, A.indices, A.data, 80, structure, "algo5", view="F")
+    L = sp.tril(A).tocsr()
+    low = compute_matching(L.indptr, L.indices, L.data, 80, structure, "algo5", view="L")
+    U = sp.triu(A).tocsr()
+    up = compute_matching(U.indptr, U.indices, U.data, 80, structure, "algo5", view="U")
+    assert full.symmetric
+    assert np.array_equal(full.rscale, full.cscale)
+    assert np.array_equal(full.rscale, low.rscale) and np.array_equal(full.rscale, up.rscale)
+    assert np.array_equal(full.perm, low.perm)
+    d = full.rscale
+    S = sp.diags(d) @ abs(A) @ sp.diags(d)
+    assert S.max() <= 1 + 1e-12
+
+
+def test_index_base_one_and_errors():
+    A = _random_nonsingular(20, 0.2, 5)
+    m0 = compute_matching(A.indptr, A.indices, A.data, 20, "G", 5)
+    m1 = compute_matching(A.indptr + 1, A.indices + 1, A.data, 20, "G", 5, index_base=1)
+    assert np.array_equal(m0.perm, m1.perm) and np.array_equal(m0.rscale, m1.rscale)
+    assert compute_matching(A.indptr, A.indices, A.data, 20, "G", "algo6").job == 5
+    with pytest.raises(ValueError, match="unknown matching job"):
+        compute_matching(A.indptr, A.indices, A.data, 20, "G", 7)
+    with pytest.raises(ValueError, match="column index out of range"):
+        compute_matching(A.indptr, A.indices + 30, A.data, 20, "G", 5)
