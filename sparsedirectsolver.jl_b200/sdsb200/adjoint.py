@@ -137,4 +137,8 @@ def solve(solver: DirectSolver, nzval, b, refactorize: bool = False):
     """x = A(nzval)^{-1} b, differentiable in ``nzval`` (one value per stored entry of the solver's
     pattern, times nbatch) and in ``b``. ``solver`` is a DirectSolver on that pattern; it is analysed
     on first use and factored with ``nzval`` in the forward."""
+    if solver.params["matching_alg"] not in ("default", "none", 0):
+        from .solver import NotSupportedError
+
+        raise NotSupportedError("the adjoint of a solve with matching_alg is not supported")
     return _Solve.get().apply(nzval, b, solver, refactorize)

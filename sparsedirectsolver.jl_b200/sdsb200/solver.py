@@ -17,7 +17,7 @@ import numpy as np
 
 from . import capi
 from ._native import numeric_lib
-from .analysis import analyze
+from .analysis import analyze, compute_matching
 
 
 class SparseDirectSolverError(Exception):
@@ -105,6 +105,8 @@ class DirectSolver:
         self._info = np.zeros(self.nbatch, dtype=np.int64)
         self._ir_steps = -1
         self._keep = []
+        self._matching = None     # host Matching of matching_alg (None: no matching)
+        self._mdev = None         # its device tensors: entry weights, row / column scalings, permutation
 
     # -- values ------------------------------------------------------------------------------------------------
     def _set_values(self, nzval):
@@ -160,6 +162,60 @@ class DirectSolver:
         self._create_plan()
         self._stage = 1
 
+    def _prepare_matching(self):
+        """Matching and scaling of ``matching_alg`` (the reference's ``_reorder!`` and ``_matching_state``,
+        src/solver.jl:545-592), from the first batch member's values: the analysis, factorization and
+        solve then work on ``M = (Dr A Dc)[:, q]`` ("G": the matched entry of row i moves to column i;
+        its pattern is the stored one with relabeled columns, no value moves) or on ``D A D`` (the
+        symmetric structures, whose inertia it keeps). Returns the column indices the analysis reads."""
+        torch = self._torch
+        alg = self.params["matching_alg"]
+        self._matching = self._mdev = None
+        if alg in ("default", "none", 0):
+            return self.colval
+        if self.params["ir_mode"] == "fgmres":
+            raise NotSupportedError("matching_alg with ir_mode \"fgmres\" is not supported")
+        m = compute_matching(self.rowptr, self.colval, self.nzval[: self.nnz].cpu().numpy(), self.n, self.structure,
+                             alg, view=self.view, index_base=self.index_base)
+        rp = np.asarray(self.rowptr, np.int64) - self.index_base
+        cols = np.asarray(self.colval, np.int64) - self.index_base
+        rows = np.repeat(np.arange(self.n), np.diff(rp))
+        w = m.rscale[rows] * m.cscale[cols]
+        dev = lambda a: torch.from_numpy(np.ascontiguousarray(a)).to(self.device)  # noqa: E731
+        perm0 = m.perm - 1
+        self._matching = m
+        self._mdev = {"w": dev(w), "w_host": w, "r": dev(m.rscale), "c": dev(m.cscale), "perm0": dev(perm0),
+                      "c_perm": dev(m.cscale[perm0])}
+        if self.structure != "G":
+            return self.colval
+        inv = np.empty(self.n, np.int64)
+        inv[perm0] = np.arange(self.n)
+        return inv[cols] + self.index_base
+
+    def _factor_values(self):
+        """The values the numeric phase factors: the user's, or scaled by the matching's entry weights."""
+        if self._matching is None:
+            return self.nzval
+        w = self._mdev["w"]
+        return (self.nzval.reshape(self.nbatch, -1) * w).reshape(-1).contiguous()
+
+    def _scaled_rhs(self, Bcm, mode):
+        """The right-hand sides of the matched system (last axis: the n rows). "G": M y = Dr b, or for
+        A^T: M^T z = Q^T Dc b; the symmetric structures: (D A D) y = D b."""
+        d = self._mdev
+        if self._matching.symmetric or mode == 0:
+            return (Bcm * d["r"]).contiguous()
+        return (Bcm * d["c"])[..., d["perm0"]].contiguous()
+
+    def _unscaled_solution(self, Ycm, mode):
+        """x from the matched system's solution: "G" x = Dc Q y (A), x = Dr z (A^T); symmetric x = D y."""
+        d = self._mdev
+        if self._matching.symmetric or mode != 0:
+            return Ycm * d["r"]
+        X = self._torch.empty_like(Ycm)
+        X[..., d["perm0"]] = Ycm * d["c_perm"]
+        return X
+
     def _plan_exists(self):
         return getattr(self, "_plan", None) is not None
 
@@ -169,8 +225,16 @@ class DirectSolver:
             return int(self._info[0]) if self.nbatch == 1 else self._info.copy()
         if name == "ir_n_steps" and self._ir_steps >= 0:
             return self._ir_steps
+        if name in ("perm_matching", "scale_row", "scale_col"):
+            self._need(1, name)
+            if self._matching is None:
+                raise InvalidValueError(f"{name!r} needs matching_alg other than \"default\"")
+            m = self._matching
+            return {"perm_matching": m.perm, "scale_row": m.rscale, "scale_col": m.cscale}[name].copy()
         if name in ("perm_reorder_row", "perm_reorder_col", "perm_col"):
             self._need(1, name)
+            if name == "perm_col" and self._matching is not None and self.structure == "G":
+                return self._matching.perm[self.symbolic.perm - 1]
             return self.symbolic.perm.copy()
         if name == "perm_row":
             self._need(1, name)
@@ -241,7 +305,10 @@ class DirectSolver:
     def _analysis(self):
         p = self.params
         nz_host = self.nzval[: self.nnz].cpu().numpy() if self.structure == "S" else None
-        self.symbolic = analyze(self.rowptr, self.colval, self.n, self.structure, nzval=nz_host, view=self.view,
+        colval = self._prepare_matching()
+        if self._matching is not None and nz_host is not None:
+            nz_host = nz_host * self._mdev["w_host"]
+        self.symbolic = analyze(self.rowptr, colval, self.n, self.structure, nzval=nz_host, view=self.view,
                                 index_base=self.index_base, reordering=p["reordering_alg"],
                                 user_perm=p["user_perm"], pivot_pairs=p["pivot_pairs"],
                                 pivot_pair_tolerance=p["pivot_pair_tolerance"],
@@ -302,7 +369,8 @@ class DirectSolver:
         info = np.zeros(self.nbatch, np.int64)
         stream = self._torch.cuda.current_stream(self.device).cuda_stream
         o = self._opts()
-        rc = lib.sdsb200_factor(self._plan, C.c_void_p(self.nzval.data_ptr()),
+        self._fvals = self._factor_values()
+        rc = lib.sdsb200_factor(self._plan, C.c_void_p(self._fvals.data_ptr()),
                                 ps_arr.ctypes.data if ps_arr is not None else None, C.byref(o), info.ctypes.data,
                                 C.c_void_p(stream))
         if rc == capi.INTERRUPTED:
@@ -329,9 +397,13 @@ class DirectSolver:
         else:
             Bcm = Bm.transpose(1, 2).contiguous()
             nrhs = Bm.shape[2]
-        Xcm = torch.empty_like(Bcm)
         o = self._opts()
+        if self._matching is not None:
+            Bcm = self._scaled_rhs(Bcm, int(o.solve_mode))
+        Xcm = torch.empty_like(Bcm)
         fgmres = self.params["ir_mode"] == "fgmres" and o.ir_n_steps > 0
+        if fgmres and self._matching is not None:
+            raise NotSupportedError("matching_alg with ir_mode \"fgmres\" is not supported")
         if fgmres:
             # FGMRES-IR (fgmres_refine!, src/solve/refinement.jl:577-614): a plain solve, then the
             # Krylov refinement on the host above the C ABI
@@ -341,9 +413,12 @@ class DirectSolver:
             o.ir_n_steps = 0
         steps = C.c_int32(0)
         stream = torch.cuda.current_stream(self.device).cuda_stream
+        vals = self.nzval if self._matching is None else self._factor_values()
         _check(lib.sdsb200_solve(self._plan, C.c_void_p(Xcm.data_ptr()), n, C.c_void_p(Bcm.data_ptr()), n, nrhs,
-                                 C.c_void_p(self.nzval.data_ptr()), C.byref(o), C.byref(steps),
+                                 C.c_void_p(vals.data_ptr()), C.byref(o), C.byref(steps),
                                  C.c_void_p(stream)), lib)
+        if self._matching is not None:
+            Xcm = self._unscaled_solution(Xcm, int(o.solve_mode))
         self._ir_steps = int(steps.value) if o.ir_n_steps > 0 else -1
         if fgmres:
             from .refinement import fgmres_refine

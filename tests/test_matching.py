@@ -134,3 +134,62 @@ def test_index_base_one_and_errors():
         compute_matching(A.indptr, A.indices, A.data, 20, "G", 7)
     with pytest.raises(ValueError, match="column index out of range"):
         compute_matching(A.indptr, A.indices + 30, A.data, 20, "G", 5)
+
+
+def _host_solver(A, structure, alg="algo5"):
+    """A DirectSolver's host side only (CPU tensors, no plan): enough for the matching algebra."""
+    import torch
+
+    from sdsb200.solver import _DEFAULTS, DirectSolver
+
+    ds = DirectSolver.__new__(DirectSolver)
+    ds._torch = torch
+    ds.device = torch.device("cpu")
+    ds.rowptr, ds.colval, ds.n, ds.nnz = A.indptr.astype(np.int64), A.indices.astype(np.int64), A.shape[0], A.nnz
+    ds.structure, ds.view, ds.index_base, ds.nbatch = structure, "F", 0, 1
+    ds.params = dict(_DEFAULTS)
+    ds.params["matching_alg"] = alg
+    ds.nzval = torch.from_numpy(A.data.astype(np.float64))
+    ds._matching = ds._mdev = None
+    return ds
+
+
+@pytest.mark.parametrize("structure", ["G", "S", "SPD"])
+@pytest.mark.parametrize("mode", [0, 1])
+def test_matched_system_algebra(structure, mode):
+    """The matched system the numeric phase would factor, solved here by scipy, maps back to A x = b
+    (or A^T x = b): the relabeled analysis columns, the entry weights, the right-hand-side scaling and
+    the solution's unscaling of DirectSolver."""
+    import torch
+    from scipy.sparse.linalg import spsolve
+
+    rng = np.random.default_rng(5)
+    n = 50
+    if structure == "G":
+        A = _random_nonsingular(n, 0.1, 9)
+    else:
+        B = sp.random(n, n, density=0.08, random_state=9, format="csr")
+        A = (B + B.T).tocsr()
+        A.setdiag(rng.uniform(1.0, 5.0, n) * (1 if structure == "SPD" else rng.choice([-1, 1], n)) + 0.0)
+        if structure == "SPD":
+            A = A + sp.eye(n) * (abs(A).sum(1).max() + 1.0)
+        D = sp.diags(np.exp(rng.normal(0, 4, n)))
+        A = (D @ A @ D).tocsr()
+    A.sort_indices()
+    ds = _host_solver(A, structure)
+    colval = ds._prepare_matching()
+    w = ds._mdev["w_host"]
+    # M: the stored entries with the analysis' column indices and the factored values
+    rows = np.repeat(np.arange(n), np.diff(A.indptr))
+    M = sp.csr_matrix((A.data * w, (rows, np.asarray(colval) - 0)), shape=(n, n))
+    if structure == "G":
+        # the matched entries are on M's diagonal, of modulus 1 (job 5)
+        assert np.allclose(np.abs(M.diagonal()), 1.0, rtol=1e-12)
+    b = rng.uniform(-1, 1, (n, 2))
+    Bcm = torch.from_numpy(np.ascontiguousarray(b.T))
+    rhs = ds._scaled_rhs(Bcm, mode).numpy().T
+    Y = spsolve((M if mode == 0 else M.T).tocsc(), rhs)
+    X = ds._unscaled_solution(torch.from_numpy(np.ascontiguousarray(Y.T)), mode).numpy().T
+    AA = A if mode == 0 else A.T
+    res = np.abs(AA @ X - b).max() / (np.abs(AA).max() * np.abs(X).max() + np.abs(b).max())
+    assert res <= 1e-12
