@@ -27,6 +27,7 @@ import os
 import statistics
 import subprocess
 import sys
+import tempfile
 import time
 
 ROOT = os.path.dirname(os.path.abspath(__file__))
@@ -316,7 +317,9 @@ class ClockSampler:
     def __init__(self, index):
         self.index = index
         self.proc = None
-        self.path = os.path.join(ROOT, "gpurun_out", f"clocks_{os.getpid()}.csv")
+        # the raw samples: SDSB200_CLOCKS_DIR when set, else the temporary directory
+        base = os.environ.get("SDSB200_CLOCKS_DIR") or tempfile.gettempdir()
+        self.path = os.path.join(base, f"sdsb200_clocks_{os.getpid()}.csv")
 
     def __enter__(self):
         os.makedirs(os.path.dirname(self.path), exist_ok=True)
