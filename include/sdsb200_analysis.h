@@ -52,6 +52,9 @@ typedef struct sdsa_options {
     int amalg_max_width;    /* 32 */
     double amalg_zero_fraction; /* 0.25 */
     int amalg_min_width;    /* 8 */
+    const int64_t* user_pairs; /* structure "S": 2 x n_user_pairs 1-based (partner, candidate) pairs the
+                                  ordering keeps adjacent instead of searching the values, or NULL */
+    int64_t n_user_pairs;
 } sdsa_options;
 
 typedef struct sdsa_result sdsa_result;
@@ -94,6 +97,17 @@ void sdsa_free(sdsa_result* r);
 int sdsa_matching(int64_t n, const int64_t* rowptr, const int64_t* colval, const double* nzval, int structure,
                   int view, int index_base, int job, int64_t* perm, int8_t* matched, double* rscale,
                   double* cscale);
+
+/* The 2x2 pivot pairs of structure "S" from the cycles of a symmetric matching (the reference's
+ * matching_pairs, src/matching/mc64.jl:380-441): perm, matched and d (= rscale) from sdsa_matching of
+ * the same matrix. pivot_pairs SDSA_PAIRS_NONE gives none, SDSA_PAIRS_ALL keeps every pair of the
+ * cycles, SDSA_PAIRS_DEFAULT only pairs with a 2x2 candidate (scaled |a_ii| <= pivot_pair_tolerance *
+ * max_{j != i} scaled |a_ij|). Writes *npairs (partner, candidate) 1-based pairs, sorted by candidate,
+ * into pairs (room for n entries: at most n / 2 pairs); pass them as sdsa_options.user_pairs.
+ * Returns 0, or -1 with the message in sdsa_last_error(). */
+int sdsa_matching_pairs(int64_t n, const int64_t* rowptr, const int64_t* colval, const double* nzval, int view,
+                        int index_base, const int64_t* perm, const int8_t* matched, const double* d, int pivot_pairs,
+                        double pivot_pair_tolerance, int64_t* pairs, int64_t* npairs);
 const char* sdsa_last_error(void);
 
 #ifdef __cplusplus

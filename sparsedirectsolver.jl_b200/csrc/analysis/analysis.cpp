@@ -1370,6 +1370,74 @@ void finite_scaling(vector<double>& s) {
         if (!(std::isfinite(x) && x > 0)) x = 1.0;
 }
 
+// 2x2 pivot pairs of "S" from the cycles of a symmetric matching (`matching_pairs`, mc64.jl:380-441;
+// Duff & Pralet 2005). perm is the 1-based matching permutation, d the symmetric scaling. Cycles of
+// matched indices of length >= 2 are split into pairs of consecutive indices (a_{i, perm(i)} != 0):
+// an even cycle takes the alternative with the larger product of scaled |a|, an odd one leaves out
+// the index with the largest scaled diagonal. A pair is kept when one of its indices is a 2x2
+// candidate (scaled |a_ii| <= tol * max_{j != i} scaled |a_ij|), or always with keep_all; its
+// candidate is the index with the smaller scaled-diagonal ratio. Pairs (partner, candidate), 1-based,
+// sorted by candidate.
+vector<std::pair<i64, i64>> matching_pairs(const AbsCsr& M, int n, const i64* perm, const int8_t* matched,
+                                           const double* d, double tol, bool keep_all) {
+    vector<double> dg(n, 0.0), offmax(n, 0.0);
+    for (int i = 0; i < n; ++i)
+        for (i64 p = M.ptr[i]; p < M.ptr[i + 1]; ++p) {
+            const int j = M.adj[p];
+            const double x = d[i] * M.w[p] * d[j];
+            if (j == i) dg[i] = x;
+            else offmax[i] = std::max(offmax[i], x);
+        }
+    auto entry = [&](int i, int j) {
+        for (i64 p = M.ptr[i]; p < M.ptr[i + 1]; ++p)
+            if (M.adj[p] == j) return d[i] * M.w[p] * d[j];
+        return 0.0;
+    };
+    auto ratio = [&](int i) { return offmax[i] > 0 ? dg[i] / offmax[i] : std::numeric_limits<double>::infinity(); };
+    auto candidate = [&](int i) { return dg[i] <= tol * offmax[i]; };
+    vector<char> seen(n, 0);
+    vector<std::pair<i64, i64>> pairs;
+    vector<int> cyc;
+    for (int i0 = 0; i0 < n; ++i0) {
+        if (seen[i0] || !matched[i0]) continue;
+        cyc.clear();
+        int i = i0;
+        bool ok = true;
+        while (!seen[i]) {
+            seen[i] = 1;
+            cyc.push_back(i);
+            if (!matched[i]) ok = false;
+            i = (int)perm[i] - 1;
+        }
+        const int L = (int)cyc.size();
+        if (!(ok && i == i0 && L >= 2)) continue;
+        int start;   // 0-based position of the first pair's first index
+        if (L % 2 == 0) {
+            double p0 = 1.0, p1 = 1.0;
+            for (int k = 0; k < L; k += 2) {
+                p0 *= entry(cyc[k], cyc[k + 1]);
+                p1 *= entry(cyc[k + 1], cyc[(k + 2) % L]);
+            }
+            start = p1 > p0 ? 1 : 0;
+        } else {
+            int big = 0;   // the first largest scaled diagonal stays a singleton
+            for (int k = 1; k < L; ++k)
+                if (dg[cyc[k]] > dg[cyc[big]]) big = k;
+            start = (big + 1) % L;
+        }
+        for (int t = 0; t + 1 < L; t += 2) {
+            const int a = cyc[(start + t) % L], b = cyc[(start + t + 1) % L];
+            if (!(keep_all || candidate(a) || candidate(b))) continue;
+            if (ratio(a) < ratio(b)) pairs.push_back({b + 1, a + 1});
+            else pairs.push_back({a + 1, b + 1});
+        }
+    }
+    std::stable_sort(pairs.begin(), pairs.end(), [](const std::pair<i64, i64>& x, const std::pair<i64, i64>& y) {
+        return x.second < y.second;
+    });
+    return pairs;
+}
+
 // MC64 jobs 1-5 (`mc64`, mc64.jl:302-333): lmate and the row / column scalings (ones except job 5,
 // r_i = exp(u_i) / max_k |a_ik|, c_j = exp(v_j) from the assignment on log max_k |a_ik| - log |a_ij|,
 // so that |r_i a_ij c_j| <= 1 with equality on the matched entries)
@@ -1474,6 +1542,16 @@ int sdsa_analyze(int64_t n, const int64_t* rowptr, const int64_t* colval, const 
                           requested != SDSA_REORDER_NATURAL && nzval != nullptr;
             PairCandidates cands;
             vector<IPair> fixed;
+            if (structure == SDSA_STRUCTURE_S && opts->user_pairs && opts->n_user_pairs > 0) {
+                // pairs chosen by the caller (the cycles of a matching): the ordering keeps each pair
+                // adjacent, with no value-based search
+                for (i64 k = 0; k < opts->n_user_pairs; ++k) {
+                    const i64 a = opts->user_pairs[2 * k], b = opts->user_pairs[2 * k + 1];
+                    if (a < 1 || a > n || b < 1 || b > n || a == b) throw AnalysisError("user_pairs out of range");
+                    fixed.push_back({(int)a, (int)b});
+                }
+                search = false;
+            }
             if (search) {
                 cands = pivot_candidates(P, A, nzval, structure, view, opts->pivot_pair_tolerance);
                 if (opts->pivot_pairs == SDSA_PAIRS_ALL) {
@@ -1620,6 +1698,32 @@ double sdsa_stat(const sdsa_result* r, const char* name) {
 }
 
 void sdsa_free(sdsa_result* r) { delete r; }
+
+int sdsa_matching_pairs(int64_t n, const int64_t* rowptr, const int64_t* colval, const double* nzval, int view,
+                        int index_base, const int64_t* perm, const int8_t* matched, const double* d, int pivot_pairs,
+                        double pivot_pair_tolerance, int64_t* pairs, int64_t* npairs) {
+    try {
+        *npairs = 0;
+        if (n < 0) throw AnalysisError("n must be nonnegative");
+        if (view != 'L' && view != 'U' && view != 'F') throw AnalysisError("view must be 'L', 'U' or 'F'");
+        if (pivot_pairs == SDSA_PAIRS_NONE || n == 0) return 0;
+        Csr A = host_pattern(n, rowptr, colval, index_base);
+        const int nn = (int)n;
+        for (int i = 0; i < nn; ++i)
+            if (perm[i] < 1 || perm[i] > n) throw AnalysisError("perm out of range");
+        AbsCsr M = abs_csr(A, nzval, SDSA_STRUCTURE_S, view);
+        auto pr = matching_pairs(M, nn, perm, matched, d, pivot_pair_tolerance, pivot_pairs == SDSA_PAIRS_ALL);
+        for (size_t k = 0; k < pr.size(); ++k) {
+            pairs[2 * k] = pr[k].first;
+            pairs[2 * k + 1] = pr[k].second;
+        }
+        *npairs = (int64_t)pr.size();
+        return 0;
+    } catch (const std::exception& e) {
+        g_err = e.what();
+        return -1;
+    }
+}
 
 int sdsa_matching(int64_t n, const int64_t* rowptr, const int64_t* colval, const double* nzval, int structure,
                   int view, int index_base, int job, int64_t* perm, int8_t* matched, double* rscale,

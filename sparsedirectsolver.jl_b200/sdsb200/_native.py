@@ -45,6 +45,10 @@ def analysis_lib():
         lib.sdsa_matching.argtypes = [C.c_int64, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_int,
                                       C.c_int, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
         lib.sdsa_matching.restype = C.c_int
+        lib.sdsa_matching_pairs.argtypes = [C.c_int64, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_int,
+                                            C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_double, C.c_void_p,
+                                            C.c_void_p]
+        lib.sdsa_matching_pairs.restype = C.c_int
         _analysis = lib
     return _analysis
 

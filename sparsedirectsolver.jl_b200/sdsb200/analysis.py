@@ -29,7 +29,7 @@ class _Opts(C.Structure):
                 ("user_perm", C.POINTER(C.c_int64)), ("pivot_pairs", C.c_int),
                 ("pivot_pair_tolerance", C.c_double), ("pivot_threshold", C.c_double),
                 ("use_superpanels", C.c_int), ("amalg_max_width", C.c_int), ("amalg_zero_fraction", C.c_double),
-                ("amalg_min_width", C.c_int)]
+                ("amalg_min_width", C.c_int), ("user_pairs", C.c_void_p), ("n_user_pairs", C.c_int64)]
 
 
 @dataclass
@@ -66,7 +66,7 @@ class Symbolic:
 
 def analyze(rowptr, colval, n, structure="SPD", nzval=None, view="F", index_base=0, reordering="default",
             user_perm=None, pivot_pairs="default", pivot_pair_tolerance=1e-6, pivot_threshold=0.01,
-            use_superpanels=1, amalgamation=(32, 0.25, 8)) -> Symbolic:
+            use_superpanels=1, amalgamation=(32, 0.25, 8), user_pairs=None) -> Symbolic:
     """Analyse the pattern of an ``n x n`` CSR matrix (``index_base`` of its arrays)."""
     lib = analysis_lib()
     rp = np.ascontiguousarray(rowptr, dtype=np.int64)
@@ -86,6 +86,11 @@ def analyze(rowptr, colval, n, structure="SPD", nzval=None, view="F", index_base
     o.pivot_threshold = pivot_threshold
     o.use_superpanels = int(use_superpanels)
     o.amalg_max_width, o.amalg_zero_fraction, o.amalg_min_width = amalgamation
+    up = None
+    if user_pairs is not None and len(user_pairs) > 0:
+        up = np.ascontiguousarray(np.asarray(user_pairs, dtype=np.int64).reshape(-1, 2))
+        o.user_pairs = up.ctypes.data
+        o.n_user_pairs = up.shape[0]
     res = C.c_void_p()
     rc = lib.sdsa_analyze(C.c_int64(n), rp.ctypes.data_as(C.c_void_p), cv.ctypes.data_as(C.c_void_p),
                           nz.ctypes.data_as(C.c_void_p) if nz is not None else None, C.byref(o), C.byref(res))
@@ -158,4 +163,28 @@ def compute_matching(rowptr, colval, nzval, n, structure="G", matching_alg="algo
         raise ValueError("matching failed: " + lib.sdsa_last_error().decode())
     return Matching(job=5 if job == 6 else job, perm=perm[:n], matched=matched[:n].astype(bool), rscale=rs[:n],
                     cscale=cs[:n], symmetric=structure != "G")
+
+
+def matching_pairs(rowptr, colval, nzval, n, m: Matching, pivot_pairs="default", pivot_pair_tolerance=1e-6,
+                   view="F", index_base=0) -> np.ndarray:
+    """The 2x2 pivot pairs of ``"S"`` from the cycles of the symmetric matching ``m`` (the reference's
+    ``matching_pairs``, src/matching/mc64.jl:380-441): an array of 1-based (partner, candidate) rows,
+    sorted by candidate, for ``analyze(..., user_pairs=...)``."""
+    lib = analysis_lib()
+    rp = np.ascontiguousarray(rowptr, dtype=np.int64)
+    cv = np.ascontiguousarray(colval, dtype=np.int64)
+    nz = np.ascontiguousarray(np.asarray(nzval, dtype=np.float64).reshape(-1)[: cv.size])
+    perm = np.ascontiguousarray(m.perm, dtype=np.int64)
+    matched = np.ascontiguousarray(m.matched, dtype=np.int8)
+    d = np.ascontiguousarray(m.rscale, dtype=np.float64)
+    out = np.zeros(max(n, 2), np.int64)
+    cnt = C.c_int64(0)
+    rc = lib.sdsa_matching_pairs(C.c_int64(n), rp.ctypes.data_as(C.c_void_p), cv.ctypes.data_as(C.c_void_p),
+                                 nz.ctypes.data_as(C.c_void_p), ord(view), int(index_base),
+                                 perm.ctypes.data_as(C.c_void_p), matched.ctypes.data_as(C.c_void_p),
+                                 d.ctypes.data_as(C.c_void_p), PAIRS[pivot_pairs], float(pivot_pair_tolerance),
+                                 out.ctypes.data_as(C.c_void_p), C.byref(cnt))
+    if rc != 0:
+        raise ValueError("matching pairs failed: " + lib.sdsa_last_error().decode())
+    return out[: 2 * cnt.value].reshape(-1, 2).copy()
 

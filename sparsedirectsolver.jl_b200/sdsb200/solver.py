@@ -17,7 +17,7 @@ import numpy as np
 
 from . import capi
 from ._native import numeric_lib
-from .analysis import analyze, compute_matching
+from .analysis import analyze, compute_matching, matching_pairs
 
 
 class SparseDirectSolverError(Exception):
@@ -306,14 +306,21 @@ class DirectSolver:
         p = self.params
         nz_host = self.nzval[: self.nnz].cpu().numpy() if self.structure == "S" else None
         colval = self._prepare_matching()
+        user_pairs = None
         if self._matching is not None and nz_host is not None:
+            if self._matching.job == 5 and p["pivot_pairs"] != "none":
+                # "S" with a job-5 matching: the 2x2 pairs come from the matching's cycles (src/solver.jl:560-566)
+                user_pairs = matching_pairs(self.rowptr, self.colval, nz_host, self.n, self._matching,
+                                            pivot_pairs=p["pivot_pairs"],
+                                            pivot_pair_tolerance=p["pivot_pair_tolerance"], view=self.view,
+                                            index_base=self.index_base)
             nz_host = nz_host * self._mdev["w_host"]
         self.symbolic = analyze(self.rowptr, colval, self.n, self.structure, nzval=nz_host, view=self.view,
                                 index_base=self.index_base, reordering=p["reordering_alg"],
                                 user_perm=p["user_perm"], pivot_pairs=p["pivot_pairs"],
                                 pivot_pair_tolerance=p["pivot_pair_tolerance"],
                                 pivot_threshold=p["pivot_threshold"], use_superpanels=p["use_superpanels"],
-                                amalgamation=tuple(p["amalgamation"]))
+                                amalgamation=tuple(p["amalgamation"]), user_pairs=user_pairs)
         self._create_plan()
         self._stage = 1
 

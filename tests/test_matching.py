@@ -193,3 +193,33 @@ def test_matched_system_algebra(structure, mode):
     AA = A if mode == 0 else A.T
     res = np.abs(AA @ X - b).max() / (np.abs(AA).max() * np.abs(X).max() + np.abs(b).max())
     assert res <= 1e-12
+
+
+def test_matching_pairs_from_cycles():
+    """The 2x2 pairs of "S" from a job-5 matching's cycles (matching_pairs, src/matching/mc64.jl:380-441),
+    and the analysis keeping each pair adjacent when they are passed as user_pairs."""
+    from helpers import small_kkt
+    from sdsb200.analysis import analyze, matching_pairs
+
+    A = small_kkt(8, 8, 20, seed=1).tocsr()
+    A.sort_indices()
+    n = A.shape[0]
+    m = compute_matching(A.indptr, A.indices, A.data, n, "S", "algo5")
+    pr = matching_pairs(A.indptr, A.indices, A.data, n, m)
+    assert len(pr) == 20                                    # one per constraint row of [H J^T; J 0]
+    flat = pr.ravel()
+    assert len(set(flat.tolist())) == flat.size             # disjoint
+    assert np.all(np.diff(pr[:, 1]) > 0)                    # sorted by candidate
+    D = A.toarray()
+    for partner, cand in pr:
+        assert D[partner - 1, cand - 1] != 0                # consecutive in a cycle: adjacent in A
+        assert D[cand - 1, cand - 1] == 0                   # the candidate is the zero-diagonal row
+    assert len(matching_pairs(A.indptr, A.indices, A.data, n, m, pivot_pairs="none")) == 0
+    assert len(matching_pairs(A.indptr, A.indices, A.data, n, m, pivot_pairs="all")) >= len(pr)
+    S = analyze(A.indptr, A.indices, n, "S", nzval=A.data, user_pairs=pr)
+    assert np.array_equal(S.maps["pairs"], pr.ravel())
+    pos = np.empty(n, int)
+    pos[S.perm - 1] = np.arange(n)
+    assert all(abs(pos[a - 1] - pos[b - 1]) == 1 for a, b in pr)
+    with pytest.raises(ValueError, match="user_pairs out of range"):
+        analyze(A.indptr, A.indices, n, "S", nzval=A.data, user_pairs=[[1, n + 5]])
