@@ -136,9 +136,6 @@ class _Solve:
 def solve(solver: DirectSolver, nzval, b, refactorize: bool = False):
     """x = A(nzval)^{-1} b, differentiable in ``nzval`` (one value per stored entry of the solver's
     pattern, times nbatch) and in ``b``. ``solver`` is a DirectSolver on that pattern; it is analysed
-    on first use and factored with ``nzval`` in the forward."""
-    if solver.params["matching_alg"] not in ("default", "none", 0):
-        from .solver import NotSupportedError
-
-        raise NotSupportedError("the adjoint of a solve with matching_alg is not supported")
+    on first use and factored with ``nzval`` in the forward. With ``matching_alg`` the solves run on the
+    matched system and map back (the matching is the analysis'), so x, b-bar and A-bar are those of A."""
     return _Solve.get().apply(nzval, b, solver, refactorize)

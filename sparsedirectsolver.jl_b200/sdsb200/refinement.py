@@ -23,8 +23,9 @@ import math
 import numpy as np
 
 
-def fgmres_refine(solver, Xcm, Bcm, nrhs, solve_mode, nsteps, tol):
-    """Refine Xcm (device, column-major per member: (nbatch, nrhs, n) or (nrhs, n)) in place.
+def fgmres_refine(solver, Xcm, Bcm, nrhs, solve_mode, nsteps, tol, nzval=None):
+    """Refine Xcm (device, column-major per member: (nbatch, nrhs, n) or (nrhs, n)) in place, for the
+    matrix with values ``nzval`` (default: the solver's; with a matching, the matched system's).
 
     Returns the FGMRES iterations performed."""
     import torch
@@ -37,7 +38,8 @@ def fgmres_refine(solver, Xcm, Bcm, nrhs, solve_mode, nsteps, tol):
     if nsteps <= 0 or n == 0:
         return 0
     stream = C.c_void_p(torch.cuda.current_stream(solver.device).cuda_stream)
-    nz = C.c_void_p(solver.nzval.data_ptr())
+    vals = solver.nzval if nzval is None else nzval
+    nz = C.c_void_p(vals.data_ptr())
     shape = Xcm.shape
     zeros = torch.zeros_like(Bcm)
 

@@ -173,8 +173,6 @@ class DirectSolver:
         self._matching = self._mdev = None
         if alg in ("default", "none", 0):
             return self.colval
-        if self.params["ir_mode"] == "fgmres":
-            raise NotSupportedError("matching_alg with ir_mode \"fgmres\" is not supported")
         m = compute_matching(self.rowptr, self.colval, self.nzval[: self.nnz].cpu().numpy(), self.n, self.structure,
                              alg, view=self.view, index_base=self.index_base)
         rp = np.asarray(self.rowptr, np.int64) - self.index_base
@@ -409,8 +407,6 @@ class DirectSolver:
             Bcm = self._scaled_rhs(Bcm, int(o.solve_mode))
         Xcm = torch.empty_like(Bcm)
         fgmres = self.params["ir_mode"] == "fgmres" and o.ir_n_steps > 0
-        if fgmres and self._matching is not None:
-            raise NotSupportedError("matching_alg with ir_mode \"fgmres\" is not supported")
         if fgmres:
             # FGMRES-IR (fgmres_refine!, src/solve/refinement.jl:577-614): a plain solve, then the
             # Krylov refinement on the host above the C ABI
@@ -424,13 +420,13 @@ class DirectSolver:
         _check(lib.sdsb200_solve(self._plan, C.c_void_p(Xcm.data_ptr()), n, C.c_void_p(Bcm.data_ptr()), n, nrhs,
                                  C.c_void_p(vals.data_ptr()), C.byref(o), C.byref(steps),
                                  C.c_void_p(stream)), lib)
-        if self._matching is not None:
-            Xcm = self._unscaled_solution(Xcm, int(o.solve_mode))
         self._ir_steps = int(steps.value) if o.ir_n_steps > 0 else -1
         if fgmres:
             from .refinement import fgmres_refine
 
-            self._ir_steps = fgmres_refine(self, Xcm, Bcm, nrhs, int(o.solve_mode), fg_steps, fg_tol)
+            self._ir_steps = fgmres_refine(self, Xcm, Bcm, nrhs, int(o.solve_mode), fg_steps, fg_tol, nzval=vals)
+        if self._matching is not None:   # refinement ran on the matched system; back to A's unknowns
+            Xcm = self._unscaled_solution(Xcm, int(o.solve_mode))
         out = Xcm.t() if Xcm.dim() == 2 else Xcm.transpose(1, 2)
         out = out.reshape(Bt.shape)
         if X is not None:

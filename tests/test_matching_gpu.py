@@ -87,3 +87,40 @@ def test_matching_outputs_need_matching(torch_cuda):
     ds.execute("analysis")
     with pytest.raises(InvalidValueError):
         ds.getparam("perm_matching")
+
+
+def test_matching_fgmres_and_adjoint(torch_cuda):
+    """FGMRES-IR on the matched system, and the solve's adjoint with matching against the host's
+    (the matching changes how A is factored, not x, b-bar or A-bar): b-bar = A^-T x-bar and
+    A-bar_ij = -b-bar_i x_j on the stored entries."""
+    from scipy.sparse.linalg import spsolve
+
+    from sdsb200 import adjoint
+    from sdsb200.solver import DirectSolver
+
+    torch = torch_cuda
+    rng = np.random.default_rng(6)
+    A0 = M.convection_diffusion3d(8, 8, 8, seed=6)
+    n = A0.shape[0]
+    P = sp.csr_matrix((np.ones(n), (np.arange(n), rng.permutation(n))), shape=(n, n))
+    A = (sp.diags(np.exp(rng.normal(0, 2, n))) @ P @ A0).tocsr()
+    A.sort_indices()
+    ds = DirectSolver(A, "G", matching_alg="algo5", pivot_threshold=0.1, ir_mode="fgmres", ir_n_steps=10,
+                      ir_tol=1e-14)
+    ds.execute("analysis")
+    ds.execute("factorization")
+    b = M.rhs(n, 2, seed=7)
+    x = ds.execute("solve", None, b).cpu().numpy()
+    assert M.scaled_backward_error(A, x, b) <= BERR
+    s = DirectSolver(A, "G", matching_alg="algo5", pivot_threshold=0.1)
+    nz = torch.from_numpy(A.data.copy()).cuda().requires_grad_(True)
+    bt = torch.from_numpy(b[:, 0].copy()).cuda().requires_grad_(True)
+    xbar = np.linspace(-1.0, 1.0, n)
+    xt = adjoint.solve(s, nz, bt)
+    (xt * torch.from_numpy(xbar).cuda()).sum().backward()
+    xh = spsolve(A.tocsc(), b[:, 0])
+    bbar = spsolve(A.T.tocsc(), xbar)
+    rows = np.repeat(np.arange(n), np.diff(A.indptr))
+    abar = -bbar[rows] * xh[A.indices]
+    assert np.abs(bt.grad.cpu().numpy() - bbar).max() <= 1e-8 * np.abs(bbar).max()
+    assert np.abs(nz.grad.cpu().numpy() - abar).max() <= 1e-8 * np.abs(abar).max()
