@@ -12,9 +12,11 @@
 #include "oracle.h"
 
 #include <algorithm>
+#include <atomic>
 #include <cmath>
 #include <cstdint>
 #include <cstring>
+#include <thread>
 #include <vector>
 
 using std::vector;
@@ -40,6 +42,75 @@ struct Ctx {
     i64 w(i64 s) const { return S->super_ptr[s] - S->super_ptr[s - 1]; }
     i64 base(i64 s) const { return S->front_ptr[s - 1]; }
 };
+
+// Host threads for the fronts (oracle_set_threads); 1 = the serial postorder of the reference.
+int g_threads = 1;
+thread_local bool t_worker = false;   // inside a level-parallel worker: the dense loops stay serial
+
+// fn(i) for i in [lo, hi) on the host threads, when the loop is worth it (work in multiply-adds) and
+// the caller is not itself a worker; each i is one thread's, so every entry sees the serial arithmetic
+template <class Fn>
+void parallel_for(i64 lo, i64 hi, double work, Fn fn) {
+    const i64 nt = std::min<i64>(g_threads, hi - lo);
+    if (nt <= 1 || t_worker || work < 5.0e5) {
+        for (i64 i = lo; i < hi; ++i) fn(i);
+        return;
+    }
+    std::atomic<i64> next(lo);
+    vector<std::thread> pool;
+    for (i64 k = 0; k < nt; ++k)
+        pool.emplace_back([&]() {
+            t_worker = true;
+            for (i64 i = next++; i < hi; i = next++) fn(i);
+        });
+    for (std::thread& th : pool) th.join();
+}
+
+// Runs body(s) for every supernode, children before parents. Serially it follows the postorder and
+// stops at the first nonzero return (a failed Cholesky pivot). With several threads, the fronts of
+// one elimination-tree level run concurrently: a front reads only its children's contribution
+// blocks and writes its own panel, statistics and block, so the results are those of the serial
+// order. Every front is processed, and the first nonzero return in postorder is returned, which is
+// the serial return value.
+template <class Body>
+i64 run_fronts(const Ctx& C, Body body) {
+    const oracle_symbolic* S = C.S;
+    if (g_threads <= 1 || C.ns < 2) {
+        for (i64 t = 0; t < C.ns; ++t) {
+            i64 r = body(S->snpost[t]);
+            if (r) return r;
+        }
+        return 0;
+    }
+    vector<i64> level(C.ns + 1, 0);
+    i64 nlev = 0;
+    for (i64 t = 0; t < C.ns; ++t) {          // postorder: children first
+        i64 s = S->snpost[t], p = S->snparent[s - 1];
+        if (p != 0) level[p] = std::max(level[p], level[s] + 1);
+        nlev = std::max(nlev, level[s] + 1);
+    }
+    vector<vector<i64>> bylevel(nlev);
+    for (i64 t = 0; t < C.ns; ++t) bylevel[level[S->snpost[t]]].push_back(S->snpost[t]);
+    vector<i64> ret(C.ns + 1, 0);
+    for (const vector<i64>& fronts : bylevel) {
+        const int nt = (int)std::min<i64>(g_threads, (i64)fronts.size());
+        if (nt <= 1) {
+            for (i64 s : fronts) ret[s] = body(s);
+            continue;
+        }
+        std::atomic<i64> next(0);
+        vector<std::thread> pool;
+        for (int k = 0; k < nt; ++k)
+            pool.emplace_back([&]() {
+                t_worker = true;
+                for (i64 q = next++; q < (i64)fronts.size(); q = next++) ret[fronts[q]] = body(fronts[q]);
+            });
+        for (std::thread& th : pool) th.join();
+    }
+    for (i64 t = 0; t < C.ns; ++t)
+        if (ret[S->snpost[t]]) return ret[S->snpost[t]];
+    return 0;
+}
 
 // assembly of A and extend-add of the children (cholesky.jl:67-84; lu.jl:115-131)
 void assemble(const Ctx& C, i64 s, const double* nz, Front& F, vector<vector<double>>& cbs, vector<i64>& cbm,
@@ -74,44 +145,58 @@ i64 factor_cholesky(const Ctx& C, const double* nz, double eps, double* factor, 
     const oracle_symbolic* S = C.S;
     vector<vector<double>> cbs(C.ns + 1);
     vector<i64> cbm(C.ns + 1, -1);
-    for (i64 t = 0; t < C.ns; ++t) {
-        i64 s = S->snpost[t];
+    return run_fronts(C, [&](i64 s) -> i64 {
         i64 f = C.f(s), w = C.w(s), m = f - w, base = C.base(s);
         Front F{f, w, vector<double>(f * f, 0.0)};
         assemble(C, s, nz, F, cbs, cbm, false);
-        // potrf on F11 (right-looking, lower)
-        for (i64 j = 0; j < w; ++j) {
-            double ajj = F(j, j);
-            bool ok = ajj > eps || (eps > 0 && ajj >= 0);
-            if (!ok) {
-                stats[(s - 1) * NF + ST_NPOS] = j;
-                stats[(s - 1) * NF + ST_INFO] = j + 1;
-                return S->perm[S->super_ptr[s - 1] + j - 1];
-            }
-            double djj = std::sqrt(std::max(ajj, eps));
-            F(j, j) = djj;
-            for (i64 i = j + 1; i < w; ++i) F(i, j) /= djj;
-            for (i64 k = j + 1; k < w; ++k) {
-                double l = F(k, j);
-                for (i64 i = k; i < w; ++i) F(i, k) -= F(i, j) * l;
-            }
-        }
-        if (m > 0) {
-            // trsm R,L,T: F21 <- F21 L11^-T (column by column)
-            for (i64 j = 0; j < w; ++j) {
-                double djj = F(j, j);
-                for (i64 i = w; i < f; ++i) F(i, j) /= djj;
-                for (i64 k = j + 1; k < w; ++k) {
+        // potrf on F11 (right-looking, lower), in panels of 64 columns: a panel's columns are factored
+        // in order with the updates among them, then every later column takes the panel's updates in
+        // increasing j. Each entry receives the updates of j = 0, 1, ... in order, as in the unblocked
+        // loop; the later columns of a panel run on the host threads.
+        constexpr i64 PB = 64;
+        for (i64 j0 = 0; j0 < w; j0 += PB) {
+            const i64 j1 = std::min(w, j0 + PB);
+            for (i64 j = j0; j < j1; ++j) {
+                double ajj = F(j, j);
+                bool ok = ajj > eps || (eps > 0 && ajj >= 0);
+                if (!ok) {
+                    stats[(s - 1) * NF + ST_NPOS] = j;
+                    stats[(s - 1) * NF + ST_INFO] = j + 1;
+                    return S->perm[S->super_ptr[s - 1] + j - 1];
+                }
+                double djj = std::sqrt(std::max(ajj, eps));
+                F(j, j) = djj;
+                for (i64 i = j + 1; i < w; ++i) F(i, j) /= djj;
+                for (i64 k = j + 1; k < j1; ++k) {
                     double l = F(k, j);
-                    for (i64 i = w; i < f; ++i) F(i, k) -= F(i, j) * l;
+                    for (i64 i = k; i < w; ++i) F(i, k) -= F(i, j) * l;
                 }
             }
-            // syrk: F22 -= F21 F21^T (lower)
-            for (i64 k = 0; k < w; ++k)
-                for (i64 jj = w; jj < f; ++jj) {
+            const double rest = (double)(w - j1);
+            parallel_for(j1, w, 0.5 * rest * rest * (double)(j1 - j0), [&](i64 k) {
+                for (i64 j = j0; j < j1; ++j) {
+                    double l = F(k, j);
+                    for (i64 i = k; i < w; ++i) F(i, k) -= F(i, j) * l;
+                }
+            });
+        }
+        if (m > 0) {
+            // trsm R,L,T: F21 <- F21 L11^-T, row by row (each entry takes the updates of columns j < k, in
+            // order, then its division, as in the column-by-column form)
+            parallel_for(w, f, 0.5 * (double)m * w * w, [&](i64 i) {
+                for (i64 j = 0; j < w; ++j) {
+                    F(i, j) /= F(j, j);
+                    const double x = F(i, j);
+                    for (i64 k = j + 1; k < w; ++k) F(i, k) -= x * F(k, j);
+                }
+            });
+            // syrk: F22 -= F21 F21^T (lower), column by column (each entry takes k = 0..w-1 in order)
+            parallel_for(w, f, 0.5 * (double)m * m * w, [&](i64 jj) {
+                for (i64 k = 0; k < w; ++k) {
                     double l = F(jj, k);
                     for (i64 ii = jj; ii < f; ++ii) F(ii, jj) -= F(ii, k) * l;
                 }
+            });
             if (S->snparent[s - 1] != 0) {
                 cbs[s].assign(m * m, 0.0);
                 for (i64 jj = 0; jj < m; ++jj)
@@ -122,8 +207,8 @@ i64 factor_cholesky(const Ctx& C, const double* nz, double eps, double* factor, 
         for (i64 j = 0; j < w; ++j)
             for (i64 i = j; i < f; ++i) factor[base - 1 + j * f + i] = F(i, j);
         stats[(s - 1) * NF + ST_NPOS] = w;
-    }
-    return 0;
+        return 0;
+    });
 }
 
 // ---------------------------------------------------------------------------
@@ -241,8 +326,7 @@ i64 factor_ldlt(const Ctx& C, const double* nz, const LdltParams& prm, const int
     i64 n = S->n;
     vector<vector<double>> cbs(C.ns + 1);
     vector<i64> cbm(C.ns + 1, -1);
-    for (i64 t = 0; t < C.ns; ++t) {
-        i64 s = S->snpost[t];
+    return run_fronts(C, [&](i64 s) -> i64 {
         i64 f = C.f(s), w = C.w(s), m = f - w, base = C.base(s);
         i64 c0 = S->super_ptr[s - 1];
         Front F{f, w, vector<double>(f * f, 0.0)};
@@ -348,8 +432,8 @@ i64 factor_ldlt(const Ctx& C, const double* nz, const LdltParams& prm, const int
             factor[base - 1 + j * f + j] = 1.0;
             for (i64 i = j + 1; i < f; ++i) factor[base - 1 + j * f + i] = F(i, j);
         }
-    }
-    return 0;
+        return 0;
+    });
 }
 
 // ---------------------------------------------------------------------------
@@ -373,8 +457,7 @@ i64 factor_lu(const Ctx& C, const double* nz, bool pivot, double u, double eps, 
     const oracle_symbolic* S = C.S;
     vector<vector<double>> cbs(C.ns + 1);
     vector<i64> cbm(C.ns + 1, -1);
-    for (i64 t = 0; t < C.ns; ++t) {
-        i64 s = S->snpost[t];
+    return run_fronts(C, [&](i64 s) -> i64 {
         i64 f = C.f(s), w = C.w(s), m = f - w, base = C.base(s);
         i64 c0 = S->super_ptr[s - 1];
         Front F{f, w, vector<double>(f * f, 0.0)};
@@ -436,8 +519,8 @@ i64 factor_lu(const Ctx& C, const double* nz, bool pivot, double u, double eps, 
                 ufactor[base - 1 + j * f + i] = F(j, i);
             }
         }
-    }
-    return 0;
+        return 0;
+    });
 }
 
 i64 host_info(const Ctx& C, const int64_t* stats) {  // ldlt.jl:206-214
@@ -584,6 +667,9 @@ int64_t oracle_factor(const oracle_symbolic* S, const double* nzval, int structu
     }
     return -1;
 }
+
+// Host threads for the factorizations (1, the default: the reference's serial postorder).
+void oracle_set_threads(int n) { g_threads = n < 1 ? 1 : n; }
 
 int oracle_solve(const oracle_symbolic* S, int structure, const double* factor, const double* ufactor,
                  const double* d, const int32_t* piv, const int8_t* kind, double* X, const double* B, int64_t nrhs,

@@ -51,6 +51,10 @@ int64_t oracle_factor(const oracle_symbolic* S, const double* nzval, int structu
                       double eps, int eps_scaled, const int8_t* psign, double* factor, double* ufactor, double* d,
                       int32_t* piv, int8_t* kind, int64_t* stats);
 
+/* Host threads of oracle_factor: 1 (the default) follows the reference's serial postorder; more run
+ * the fronts of one elimination-tree level concurrently, with the same results. */
+void oracle_set_threads(int n);
+
 /* X = A^{-1} B (transpose != 0: A^T), B and X n x nrhs column-major (X == B allowed). */
 int oracle_solve(const oracle_symbolic* S, int structure, const double* factor, const double* ufactor,
                  const double* d, const int32_t* piv, const int8_t* kind, double* X, const double* B, int64_t nrhs,

@@ -24,6 +24,9 @@ def build(force: bool = False) -> str:
     if force or not os.path.exists(LIB) or os.path.getmtime(src) > os.path.getmtime(LIB) or \
             os.path.getmtime(os.path.join(HERE, "oracle.h")) > os.path.getmtime(LIB):
         subprocess.check_call(["make", "-C", HERE, "-B" if force else "liboracle.so"])
+    from .blas_port import build as build_blas_port   # the benchmark's CPU-baseline port
+
+    build_blas_port(force)
     return LIB
 
 
@@ -43,6 +46,8 @@ def _load():
         lib.oracle_factor.argtypes = [C.POINTER(_Sym), C.c_void_p, C.c_int, C.c_int, C.c_double, C.c_double,
                                       C.c_int, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
                                       C.c_void_p, C.c_void_p]
+        lib.oracle_set_threads.restype = None
+        lib.oracle_set_threads.argtypes = [C.c_int]
         lib.oracle_solve.restype = C.c_int
         lib.oracle_solve.argtypes = [C.POINTER(_Sym), C.c_int, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
                                      C.c_void_p, C.c_void_p, C.c_void_p, C.c_int64, C.c_int]
@@ -118,3 +123,10 @@ class Oracle:
 
     def stats_matrix(self):
         return self.stats[: 6 * self.sym.ns].reshape(self.sym.ns, 6)
+
+
+def set_threads(n: int) -> None:
+    """Host threads of the factorizations (1: the reference's serial postorder; more: the fronts of one
+    elimination-tree level concurrently, with the same results)."""
+    _load().oracle_set_threads(int(n))
+
