@@ -12,6 +12,9 @@
  *                         factorize_ldlt! src/numeric/ldlt.jl:1447-1475,
  *                         factorize_lu! src/numeric/lu.jl:543-555, with the info
  *                         read of _numeric_info! factorize.jl:383-415
+ *   sdsb200_solve_phase   the solve sub-phases and Schur phases of _solve_phase!
+ *                         src/solver.jl:847-900
+ *   sdsb200_schur_matrix  schur_matrix! src/numeric/schur.jl:134-174 (Schur complement mode)
  *   sdsb200_solve         _solve_phase! src/solver.jl:810-871 (permute_rhs!,
  *                         forward_sweep!, diagonal_sweep!, backward_sweep!,
  *                         unpermute_solution!) and _refine_phase! :902-926 (refine!
@@ -84,6 +87,10 @@ typedef struct sdsb200_symbolic {
     const void* full_src;
     int64_t full_nnz;         /* entries of M */
     int64_t full_nsrc;        /* length of full_src */
+    /* Schur complement mode (schedule.schur, src/symbolic/schedule.jl:194-227,351-360): the root
+     * supernode (1-based) that the factorization assembles and does not factor; 0 = none. It must be
+     * a root with no rows below its columns; its columns are the Schur indices. */
+    int64_t schur;
 } sdsb200_symbolic;
 
 typedef struct sdsb200_plan_options {
@@ -138,6 +145,34 @@ int sdsb200_factor(sdsb200_plan* plan, const double* nzval, const int8_t* h_psig
 int sdsb200_solve(sdsb200_plan* plan, double* X, int64_t ldx, const double* B, int64_t ldb, int32_t nrhs,
                   const double* nzval, const sdsb200_opts* opts, int32_t* h_ir_steps, void* stream);
 
+/* Solve sub-phases (execute! "solve_fwd_perm", "solve_fwd", "solve_diag", "solve_bwd", "solve_bwd_perm"
+ * of _solve_phase! src/solver.jl:847-867, and the steps of the Schur phases :876-900): one step of the
+ * solve on the plan's working vectors Y (n x nrhs per active member, factor order, kept in the plan
+ * between calls; between the forward and backward sweeps each supernode's slice is in its local pivot
+ * order, as the reference's ws.Y). No refinement. op(A) as opts->solve_mode; the diagonal step is the
+ * identity for "SPD". X and B (device, column-major, ld >= n, members at stride ld * nrhs) are read
+ * or written only by the phases that name them. A Schur plan's forward sweep leaves the condensed
+ * right-hand side b2 - A21 A11^{-1} b1 in the Schur rows of Y, and its backward sweep takes the Schur
+ * solution from there. */
+#define SDSB200_PHASE_FWD_PERM 1  /* Y = B[perm]                permute_rhs!        src/solve/permute.jl:117-131 */
+#define SDSB200_PHASE_FWD 2       /* Y <- L^{-1} Y              forward_sweep!      src/solve/sweeps.jl:908-942 */
+#define SDSB200_PHASE_DIAG 3      /* Y <- D^{-1} Y              diagonal_sweep!     src/solve/sweeps.jl:955-969 */
+#define SDSB200_PHASE_BWD 4       /* Y <- L^{-T} Y (LU: U^{-1}) backward_sweep!     src/solve/sweeps.jl:984-1004 */
+#define SDSB200_PHASE_BWD_PERM 5  /* X[perm] = Y                unpermute_solution! src/solve/permute.jl:138-149 */
+#define SDSB200_PHASE_LOAD 6      /* Y = B, no permutation (the Schur phases' identity permute_rhs!) */
+#define SDSB200_PHASE_STORE 7     /* X = Y, no permutation (the Schur phases' identity unpermute_solution!) */
+int sdsb200_solve_phase(sdsb200_plan* plan, int32_t phase, double* X, int64_t ldx, const double* B, int64_t ldb,
+                        int32_t nrhs, const sdsb200_opts* opts, void* stream);
+
+/* Schur complement mode: S = A22 - A21 A11^{-1} A12 as assembled by the last factorization
+ * (schur_matrix!, src/numeric/schur.jl:134-174), written to the dense column-major DEVICE matrix D
+ * (ns x ns, ld ldd >= ns; ns = sdsb200_plan_stat "schur_n") in the increasing original order of the
+ * Schur indices; transposed != 0 writes S^T (the reference's transposed = true for a CSC input).
+ * "G": the lower triangle from L's panel, the strict upper one from the U^T panel; "S" and "SPD": the
+ * lower triangle mirrored. */
+int sdsb200_schur_matrix(sdsb200_plan* plan, int32_t member, double* D, int64_t ldd, int32_t transposed,
+                         void* stream);
+
 /* residual! (src/solve/refinement.jl:229-248): R = B - op(A) X over the full pattern with the values
  * nzval, for the active members (R: n x nrhs per member, ld n, members at stride n * nrhs; X, B as in
  * sdsb200_solve). solve_mode 1 or 2 with "G": op(A) = A^T. Used by FGMRES-IR for its residual and
@@ -178,6 +213,7 @@ int64_t sdsb200_get_trace(sdsb200_plan* plan, int64_t* h_out, int64_t cap);
 
 /* Plan facts: "ns", "nlevels", "factor_len", "cb_len", "launches_factor", "launches_solve",
  * "launches_done" (kernel launches of the last factor or solve call), "device_bytes", "flops",
+ * "schur_n" (order of the Schur complement, 0 without one), "schur_level",
  * "solve_status" (synchronizes; nonzero when a bounded wait of the persistent solve gave up);
  * with profiling, "prof_ms:<kind>", "prof_flops:<kind>", "prof_bytes:<kind>", "prof_launches:<kind>"
  * for kinds small assemble panel gemm pivot scale stats fwd bwd diag permute residual.

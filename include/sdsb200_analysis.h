@@ -55,6 +55,10 @@ typedef struct sdsa_options {
     const int64_t* user_pairs; /* structure "S": 2 x n_user_pairs 1-based (partner, candidate) pairs the
                                   ordering keeps adjacent instead of searching the values, or NULL */
     int64_t n_user_pairs;
+    const int8_t* user_schur_indices; /* Schur complement mode (schur_mode = 1): n flags 0/1, 1 = the row and
+                                  column belong to the Schur complement; NULL = off. The flagged indices are
+                                  ordered last, in increasing order, as one dense root supernode that the
+                                  factorization assembles and does not factor; no 2x2 pivot pairs. */
 } sdsa_options;
 
 typedef struct sdsa_result sdsa_result;
@@ -72,12 +76,15 @@ int sdsa_analyze(int64_t n, const int64_t* rowptr, const int64_t* colval, const 
  * perm iperm super_ptr snparent snpost rowptr rowval front_ptr front_nrows front_ncols
  * child_ptr child_list relind_ptr relind amap amap_ptr amap_src counts
  * pairs (2*npairs: partner, candidate)
- * full_rowptr full_colval full_srcptr full_src full_conj  (residual map of the full matrix) */
+ * full_rowptr full_colval full_srcptr full_src full_conj  (residual map of the full matrix)
+ * schur_rowptr schur_colval  (Schur complement mode: 1-based CSR pattern of S over the Schur indices in
+ *                            increasing order, both triangles and the whole diagonal) */
 int64_t sdsa_len(const sdsa_result* r, const char* name);
 int sdsa_get(const sdsa_result* r, const char* name, int64_t* out);
 
 /* Scalars by name: n nnz ns nnz_stored nnz_L flops factor_len sdepth alg_used
- * (1 amd, 2 nd, 3 natural, 4 user) npairs pair_rounds */
+ * (1 amd, 2 nd, 3 natural, 4 user) npairs pair_rounds schur (the Schur root supernode, 1-based; 0 none)
+ * schur_n (order of the Schur complement) */
 double sdsa_stat(const sdsa_result* r, const char* name);
 
 void sdsa_free(sdsa_result* r);

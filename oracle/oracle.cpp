@@ -138,6 +138,28 @@ void assemble(const Ctx& C, i64 s, const double* nz, Front& F, vector<vector<dou
     }
 }
 
+// Schur complement mode (assemble_schur!, src/numeric/schur.jl:15-98): the root supernode S->schur is
+// assembled and not factored. Its panel keeps the assembled front: the lower triangle in `factor`, and
+// for LU the strict upper triangle transposed in `ufactor`; its columns get the identity local order,
+// unit 1x1 pivots (d = 1, no 2x2 part) and zero statistics.
+void store_schur(const Ctx& C, i64 s, Front& F, bool general, double* factor, double* ufactor, double* d,
+                 int32_t* piv, int8_t* kind) {
+    const oracle_symbolic* S = C.S;
+    const i64 f = F.f, base = C.base(s), c0 = S->super_ptr[s - 1];
+    for (i64 j = 0; j < f; ++j)
+        for (i64 i = j; i < f; ++i) {
+            factor[base - 1 + j * f + i] = F(i, j);
+            if (general && i > j) ufactor[base - 1 + j * f + i] = F(j, i);
+        }
+    if (!piv) return;
+    for (i64 k = 0; k < f; ++k) {
+        piv[c0 - 1 + k] = (int32_t)(c0 + k);
+        kind[c0 - 1 + k] = KIND_1X1;
+        d[c0 - 1 + k] = 1.0;
+        d[S->n + c0 - 1 + k] = 0.0;
+    }
+}
+
 // ---------------------------------------------------------------------------
 // Cholesky (cholesky.jl:44-111). eps > 0 adds the device path's static clamp
 // (src/numeric/front.jl:38-53): a pivot in [0, eps] is raised to eps.
@@ -149,6 +171,10 @@ i64 factor_cholesky(const Ctx& C, const double* nz, double eps, double* factor, 
         i64 f = C.f(s), w = C.w(s), m = f - w, base = C.base(s);
         Front F{f, w, vector<double>(f * f, 0.0)};
         assemble(C, s, nz, F, cbs, cbm, false);
+        if (s == S->schur) {
+            store_schur(C, s, F, false, factor, nullptr, nullptr, nullptr, nullptr);
+            return 0;
+        }
         // potrf on F11 (right-looking, lower), in panels of 64 columns: a panel's columns are factored
         // in order with the updates among them, then every later column takes the panel's updates in
         // increasing j. Each entry receives the updates of j = 0, 1, ... in order, as in the unblocked
@@ -331,6 +357,10 @@ i64 factor_ldlt(const Ctx& C, const double* nz, const LdltParams& prm, const int
         i64 c0 = S->super_ptr[s - 1];
         Front F{f, w, vector<double>(f * f, 0.0)};
         assemble(C, s, nz, F, cbs, cbm, false);
+        if (s == S->schur) {
+            store_schur(C, s, F, false, factor, nullptr, d, piv, kind);
+            return 0;
+        }
         for (i64 j = 0; j < w; ++j)
             for (i64 i = j + 1; i < w; ++i) F(j, i) = F(i, j);
         vector<i64> lp(w);
@@ -462,6 +492,10 @@ i64 factor_lu(const Ctx& C, const double* nz, bool pivot, double u, double eps, 
         i64 c0 = S->super_ptr[s - 1];
         Front F{f, w, vector<double>(f * f, 0.0)};
         assemble(C, s, nz, F, cbs, cbm, true);
+        if (s == S->schur) {
+            store_schur(C, s, F, true, factor, ufactor, d, piv, kind);
+            return 0;
+        }
         vector<i64> lp(w);
         for (i64 k = 0; k < w; ++k) lp[k] = k;
         vector<int8_t> kd(w, KIND_1X1);

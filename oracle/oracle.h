@@ -39,6 +39,8 @@ typedef struct oracle_symbolic {
     const int64_t* amap;       /* nnz, signed offsets */
     const int64_t* amap_ptr;   /* ns + 1 */
     const int64_t* amap_src;
+    int64_t schur;             /* Schur complement mode: the root supernode (1-based) that is assembled and
+                                  not factored (src/numeric/schur.jl:15-98); 0 = none */
 } oracle_symbolic;
 
 /* structure: 0 "G" (LU), 1 "S" (LDL^T), 3 "SPD" (Cholesky)

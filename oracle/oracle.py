@@ -34,7 +34,7 @@ class _Sym(C.Structure):
     _fields_ = [("n", C.c_int64), ("ns", C.c_int64), ("nnz", C.c_int64)] + [
         (nm, C.POINTER(C.c_int64)) for nm in (
             "perm", "super_ptr", "snparent", "snpost", "rowptr", "rowval", "front_ptr", "child_ptr", "child_list",
-            "relind_ptr", "relind", "amap", "amap_ptr", "amap_src")]
+            "relind_ptr", "relind", "amap", "amap_ptr", "amap_src")] + [("schur", C.c_int64)]
 
 
 def _load():
@@ -79,7 +79,7 @@ class Oracle:
                 a = np.zeros(1, np.int64)
             self._keep[nm] = a
             fields[nm] = a.ctypes.data_as(C.POINTER(C.c_int64))
-        self._s = _Sym(n=sym.n, ns=sym.ns, nnz=sym.nnz, **fields)
+        self._s = _Sym(n=sym.n, ns=sym.ns, nnz=sym.nnz, schur=int(getattr(sym, "schur", 0)), **fields)
         self.factor = self.ufactor = self.d = self.piv = self.kind = self.stats = None
         self.structure = None
 

@@ -978,6 +978,123 @@ Ordered pair_ordering(const Pattern& P, int alg, const PairCandidates& cands, do
     return o;
 }
 
+// ---------------------------------------------------------------------------
+// Schur complement mode (src/symbolic/ordering.jl:330-470, src/symbolic/supernodes.jl:380-425)
+
+// the pattern of P restricted to `vertices` (increasing), renumbered 1..|vertices| in their order
+// (induced_pattern, src/symbolic/ordering.jl:355-371)
+Pattern induced_pattern(const Pattern& P, const vector<int>& vertices) {
+    vector<int> loc(P.n + 1, 0);
+    for (size_t k = 0; k < vertices.size(); ++k) loc[vertices[k]] = (int)k + 1;
+    Pattern Q;
+    Q.n = (int)vertices.size();
+    Q.colptr.assign(Q.n + 2, 0);
+    Q.colptr[1] = 1;
+    Q.rowval.assign(1, 0);
+    for (int k = 1; k <= Q.n; ++k) {
+        const int v = vertices[k - 1];
+        for (const int* q = P.nb_begin(v); q != P.nb_end(v); ++q)
+            if (loc[*q] > 0) Q.rowval.push_back(loc[*q]);
+        Q.colptr[k + 1] = (int)Q.rowval.size();
+    }
+    return Q;
+}
+
+// The column partition of Schur complement mode (schur_supernode_partition,
+// src/symbolic/supernodes.jl:391-425): the last ns columns of perm form one dense root supernode, the
+// last, whose etree is the chain of its columns with the dense column counts ns, ns - 1, ..., 1; the
+// other columns are partitioned as usual on their own elimination forest (fundamental supernodes,
+// then amalgamation), so nothing merges into the root; a supernode whose last column has its etree
+// parent among the Schur columns becomes a child of the root.
+SupernodePartition schur_supernode_partition(const Pattern& P, const vector<int>& perm, int ns, bool amalg, int mw,
+                                             double zf, int minw, int& sdepth) {
+    const int n = P.n, m = n - ns;
+    if (ns < 1 || ns > n) throw AnalysisError("the Schur complement must have between 1 and n rows");
+    vector<int> parent = etree(P, perm), post = postorder(parent), counts = colcounts(P, perm, parent, post);
+    vector<int> subparent(m + 1, 0);
+    for (int j = 1; j <= m; ++j) subparent[j] = parent[j] > m ? 0 : parent[j];
+    for (int j = m + 1; j <= n; ++j) {
+        parent[j] = j < n ? j + 1 : 0;
+        counts[j] = n - j + 1;
+    }
+    vector<int> subcounts(counts.begin(), counts.begin() + m + 1);
+    ColumnPartition cp;
+    if (m > 0) {
+        cp = fundamental_supernodes(subparent, postorder(subparent), subcounts);
+        if (amalg) cp = amalgamate(cp, subparent, subcounts, mw, zf, minw);
+    } else {
+        cp.order.assign(1, 0);
+        cp.super_ptr = {0, 1};
+        cp.snparent.assign(1, 0);
+    }
+    const int nsub = cp.ns();
+    ColumnPartition full = cp;
+    for (int j = m + 1; j <= n; ++j) full.order.push_back(j);
+    full.super_ptr.push_back(n + 1);
+    for (int s = 1; s <= nsub; ++s)
+        if (full.snparent[s] == 0 && parent[cp.order[cp.super_ptr[s + 1] - 1]] > m) full.snparent[s] = nsub + 1;
+    full.snparent.push_back(0);
+    sdepth = tree_height(full.snparent);
+    return supernode_partition(P, perm, parent, counts, full);
+}
+
+// The pattern of S = A22 - A21 A11^{-1} A12 over the flagged vertices in increasing order (schur_pattern,
+// src/symbolic/ordering.jl:424-470): (i, j) when i == j, when (i, j) is in P, or when both are adjacent
+// to one connected component of the graph of the other vertices. 1-based CSR, sorted columns.
+void schur_pattern(const Pattern& P, const vector<char>& flag, vector<i64>& rowptr, vector<i64>& colval) {
+    const int n = P.n;
+    vector<int> loc(n + 1, 0);
+    int ns = 0;
+    for (int v = 1; v <= n; ++v)
+        if (flag[v]) loc[v] = ++ns;
+    vector<vector<int>> adj(ns + 1);
+    for (int k = 1; k <= ns; ++k) adj[k].push_back(k);
+    for (int v = 1; v <= n; ++v) {
+        if (!loc[v]) continue;
+        for (const int* q = P.nb_begin(v); q != P.nb_end(v); ++q)
+            if (loc[*q]) adj[loc[v]].push_back(loc[*q]);
+    }
+    vector<char> seen(n + 1, 0);
+    vector<int> mark(ns + 1, 0), stack, nbrs;
+    int ncomp = 0;
+    for (int v0 = 1; v0 <= n; ++v0) {
+        if (loc[v0] || seen[v0]) continue;
+        ++ncomp;
+        nbrs.clear();
+        seen[v0] = 1;
+        stack.push_back(v0);
+        while (!stack.empty()) {
+            const int v = stack.back();
+            stack.pop_back();
+            for (const int* q = P.nb_begin(v); q != P.nb_end(v); ++q) {
+                const int i = *q;
+                if (loc[i]) {
+                    if (mark[loc[i]] != ncomp) {
+                        mark[loc[i]] = ncomp;
+                        nbrs.push_back(loc[i]);
+                    }
+                } else if (!seen[i]) {
+                    seen[i] = 1;
+                    stack.push_back(i);
+                }
+            }
+        }
+        for (int a : nbrs)
+            for (int b : nbrs)
+                if (a != b) adj[a].push_back(b);
+    }
+    rowptr.assign(ns + 1, 0);
+    rowptr[0] = 1;
+    colval.clear();
+    for (int k = 1; k <= ns; ++k) {
+        vector<int>& c = adj[k];
+        std::sort(c.begin(), c.end());
+        c.erase(std::unique(c.begin(), c.end()), c.end());
+        colval.insert(colval.end(), c.begin(), c.end());
+        rowptr[k] = (i64)colval.size() + 1;
+    }
+}
+
 }  // namespace
 
 // ---------------------------------------------------------------------------
@@ -993,6 +1110,8 @@ struct sdsa_result {
     vector<i64> panel_ptr, front_nrows, front_ncols, child_ptr, child_list, relind_ptr, relind, amap, amap_ptr,
         amap_src;
     vector<i64> full_rowptr, full_colval, full_srcptr, full_src, full_conj;
+    int schur = 0;       // Schur complement mode: the root supernode (1-based), 0 = off
+    vector<i64> schur_rowptr, schur_colval;
 };
 
 namespace {
@@ -1521,9 +1640,7 @@ int sdsa_analyze(int64_t n, const int64_t* rowptr, const int64_t* colval, const 
         R->n = (int)n;
         R->nnz = (i64)A.cv.size() - 1;
         R->structure = structure;
-        // ordering (with 2x2 pairs for "S")
-        Ordered chosen;
-        if (opts->user_perm) {
+        auto user_perm = [&]() {
             vector<int> perm(n + 1, 0);
             vector<char> seen(n + 2, 0);
             bool zero_based = false;
@@ -1534,8 +1651,58 @@ int sdsa_analyze(int64_t n, const int64_t* rowptr, const int64_t* colval, const 
                 seen[v] = 1;
                 perm[k + 1] = (int)v;
             }
-            chosen.alg = 4;
+            return perm;
+        };
+        // Schur complement mode: the flagged rows and columns (schur_flags, src/symbolic/ordering.jl:339-346)
+        vector<char> sflag;
+        int nschur = 0;
+        if (opts->user_schur_indices) {
+            sflag.assign(n + 1, 0);
+            for (i64 k = 0; k < n; ++k)
+                if (opts->user_schur_indices[k] != 0) {
+                    sflag[k + 1] = 1;
+                    ++nschur;
+                }
+            if (nschur == 0) throw AnalysisError("user_schur_indices selects no row: the Schur complement would be empty");
+        }
+        // ordering (with 2x2 pairs for "S")
+        Ordered chosen;
+        if (nschur > 0) {
+            // compute_schur_ordering (src/symbolic/ordering.jl:386-415): the flagged vertices last in
+            // increasing order; the others in the user permutation's relative order, or by the fill-reducing
+            // ordering of the pattern they induce; no 2x2 pivot pairs
+            vector<int> inner, perm(1, 0);
+            for (int v = 1; v <= (int)n; ++v)
+                if (!sflag[v]) inner.push_back(v);
+            if (opts->user_perm) {
+                const vector<int> up = user_perm();
+                for (int k = 1; k <= (int)n; ++k)
+                    if (!sflag[up[k]]) perm.push_back(up[k]);
+                chosen.alg = 4;
+            } else {
+                Pattern Q = induced_pattern(P, inner);
+                const int requested = opts->reordering;
+                vector<int> algs = requested == SDSA_REORDER_DEFAULT ? vector<int>{SDSA_REORDER_AMD, SDSA_REORDER_ND}
+                                                                      : vector<int>{requested};
+                vector<int> best;
+                double best_cost = 0;
+                for (int a : algs) {
+                    vector<int> q = ordering_perm(Q, a);
+                    const double c = evaluate_ordering(Q, q, amalg, mw, zf, minw).cost;
+                    if (best.empty() || c < best_cost) {
+                        best = q;
+                        best_cost = c;
+                        chosen.alg = a;
+                    }
+                }
+                for (int k = 1; k <= Q.n; ++k) perm.push_back(inner[best[k] - 1]);
+            }
+            for (int v = 1; v <= (int)n; ++v)
+                if (sflag[v]) perm.push_back(v);
             chosen.perm = perm;
+        } else if (opts->user_perm) {
+            chosen.alg = 4;
+            chosen.perm = user_perm();
         } else {
             int requested = opts->reordering;
             bool search = structure == SDSA_STRUCTURE_S && opts->pivot_pairs != SDSA_PAIRS_NONE &&
@@ -1602,12 +1769,18 @@ int sdsa_analyze(int64_t n, const int64_t* rowptr, const int64_t* colval, const 
         R->pairs = chosen.pairs;
         R->pair_rounds = chosen.rounds;
         Pattern F = pair_pattern(P, chosen.pairs);
-        vector<int> parent = etree(F, chosen.perm), post = postorder(parent),
-                    counts = colcounts(F, chosen.perm, parent, post);
-        ColumnPartition cp = fundamental_supernodes(parent, post, counts);
-        if (amalg) cp = amalgamate(cp, parent, counts, mw, zf, minw);
-        R->sdepth = tree_height(cp.snparent);
-        R->sp = supernode_partition(F, chosen.perm, parent, counts, cp);
+        if (nschur > 0) {
+            R->sp = schur_supernode_partition(F, chosen.perm, nschur, amalg, mw, zf, minw, R->sdepth);
+            R->schur = R->sp.ns();
+            schur_pattern(P, sflag, R->schur_rowptr, R->schur_colval);
+        } else {
+            vector<int> parent = etree(F, chosen.perm), post = postorder(parent),
+                        counts = colcounts(F, chosen.perm, parent, post);
+            ColumnPartition cp = fundamental_supernodes(parent, post, counts);
+            if (amalg) cp = amalgamate(cp, parent, counts, mw, zf, minw);
+            R->sdepth = tree_height(cp.snparent);
+            R->sp = supernode_partition(F, chosen.perm, parent, counts, cp);
+        }
         build_maps(*R, A, structure, view);
         *out = R.release();
         return 0;
@@ -1647,6 +1820,8 @@ static const vector<i64>* i64_field(const sdsa_result* r, const std::string& nm)
     if (nm == "full_srcptr") return &r->full_srcptr;
     if (nm == "full_src") return &r->full_src;
     if (nm == "full_conj") return &r->full_conj;
+    if (nm == "schur_rowptr") return &r->schur_rowptr;
+    if (nm == "schur_colval") return &r->schur_colval;
     return nullptr;
 }
 
@@ -1694,6 +1869,8 @@ double sdsa_stat(const sdsa_result* r, const char* name) {
     if (nm == "alg_used") return r->alg_used;
     if (nm == "npairs") return (double)r->pairs.size();
     if (nm == "pair_rounds") return r->pair_rounds;
+    if (nm == "schur") return r->schur;
+    if (nm == "schur_n") return r->schur ? r->sp.width(r->schur) : 0;
     return NAN;
 }
 

@@ -313,7 +313,9 @@ int run_factor(Plan* P, const double* nzval, double eps, double u, int pivot, in
 }
 
 template <typename T>
-int run_sweeps(Plan* P, int nrhs, bool transpose, cudaStream_t st) {
+// which: 1 forward sweep, 2 diagonal, 4 backward sweep (or-ed). The unfactored Schur root (its own
+// last level) is only pulled into by the forward sweep and skipped by the backward one.
+int run_sweeps(Plan* P, int nrhs, bool transpose, cudaStream_t st, int which) {
     const int nm = P->nact;
     const int32_t* members = P->all_members ? nullptr : P->d_members;
     const bool gen = P->structure == STRUCT_G, ldl = P->structure == STRUCT_S;
@@ -342,6 +344,8 @@ int run_sweeps(Plan* P, int nrhs, bool transpose, cudaStream_t st) {
         const int ns_ = P->level_nsmall[L], nl_ = P->level_nlarge[L];
         double ent = P->level_panel_entries[L];   // booked on the first launch of the level
         const int pk = fwd ? PK_FWD : PK_BWD;
+        const bool schur = L == P->schur_level;
+        if (schur && !fwd) return SDSB200_OK;   // the Schur block of Y holds its solution already
         if (!fwd && P->level_nbtile[L]) {
             SweepArgs<T> t = a;
             t.tiles = P->d_rect_tiles + 2 * P->level_btile_off[L];
@@ -358,6 +362,7 @@ int run_sweeps(Plan* P, int nrhs, bool transpose, cudaStream_t st) {
             t.list = P->d_level_lists + off + (part == 0 ? 0 : ns_);
             t.count = cnt;
             t.rect = part == 0;
+            t.pull_only = schur;
             prof_begin(P, st);
             cudaError_t e = launch_sweep<T>(fwd, t, nm, part == 0 ? P->level_maxw_small[L] : P->level_maxw_large[L], st);
             prof_end(P, st, pk, 2.0 * ent * nrhs * nm, (double)sizeof(T) * ent * nm);
@@ -374,11 +379,11 @@ int run_sweeps(Plan* P, int nrhs, bool transpose, cudaStream_t st) {
         }
         return SDSB200_OK;
     };
-    for (int L = 0; L < P->nlevels; ++L) {
+    for (int L = 0; (which & 1) && L < P->nlevels; ++L) {
         int rc = level_sweep(true, L);
         if (rc) return rc;
     }
-    if (P->structure != STRUCT_SPD) {
+    if ((which & 2) && P->structure != STRUCT_SPD) {
         DiagArgs d{};
         d.members = members; d.d = P->d_d; d.kind = P->d_kind; d.Y = P->d_Y; d.n = P->n; d.nrhs = nrhs; d.two = ldl;
         prof_begin(P, st);
@@ -388,7 +393,7 @@ int run_sweeps(Plan* P, int nrhs, bool transpose, cudaStream_t st) {
     }
     a.fac = (gen && !transpose) ? ufactor : factor;
     a.reorder = ldl || (gen && transpose);
-    for (int L = P->nlevels - 1; L >= 0; --L) {
+    for (int L = P->nlevels - 1; (which & 4) && L >= 0; --L) {
         int rc = level_sweep(false, L);
         if (rc) return rc;
     }
@@ -473,14 +478,17 @@ int run_persistent(Plan* P, int nrhs, bool transpose, const double* in, int64_t 
 
 bool use_persistent(const Plan* P) { return P->nact == 1 && P->all_members && P->persistent; }
 
-int sweeps(Plan* P, int nrhs, bool transpose, cudaStream_t st) {
-    return P->elsize == 8 ? run_sweeps<double>(P, nrhs, transpose, st) : run_sweeps<float>(P, nrhs, transpose, st);
+int sweeps(Plan* P, int nrhs, bool transpose, cudaStream_t st, int which = 7) {
+    return P->elsize == 8 ? run_sweeps<double>(P, nrhs, transpose, st, which)
+                          : run_sweeps<float>(P, nrhs, transpose, st, which);
 }
 
-int permute(Plan* P, int mode, const double* in, int64_t ldin, double* out, int64_t ldout, int nrhs, cudaStream_t st) {
+// mode 0: Y = in[perm], 1: out[perm] = Y, 2: out[perm] += Y; identity: factor order, no permutation
+int permute(Plan* P, int mode, const double* in, int64_t ldin, double* out, int64_t ldout, int nrhs, cudaStream_t st,
+            bool identity = false) {
     PermArgs a{};
     a.members = P->all_members ? nullptr : P->d_members;
-    a.perm = P->d_perm0;
+    a.perm = identity ? nullptr : P->d_perm0;
     a.Y = P->d_Y;
     a.in = in; a.out = out; a.ldin = ldin; a.ldout = ldout;
     a.n = P->n; a.nrhs = nrhs; a.mode = mode;
@@ -600,6 +608,9 @@ int sdsb200_solve(sdsb200_plan* plan, double* X, int64_t ldx, const double* B, i
     Plan* P = reinterpret_cast<Plan*>(plan);
     if (!P) return fail(SDSB200_INVALID_VALUE, "plan is NULL");
     if (!P->factored) return fail(SDSB200_PHASE_ORDER, "solve before a successful factorization");
+    if (P->schur_front >= 0)
+        return fail(SDSB200_NOT_SUPPORTED, "Schur complement mode: the factorization is partial; use the solve "
+                                           "phases (sdsb200_solve_phase)");
     if (nrhs < 1 || nrhs > P->max_nrhs) return fail(SDSB200_INVALID_VALUE, "nrhs outside 1:max_nrhs of the plan");
     if (ldx < P->n || ldb < P->n) return fail(SDSB200_INVALID_VALUE, "leading dimension smaller than n");
     if (!X || !B) return fail(SDSB200_INVALID_VALUE, "X or B is NULL");
@@ -705,6 +716,73 @@ int sdsb200_solve(sdsb200_plan* plan, double* X, int64_t ldx, const double* B, i
         CK(cudaStreamSynchronize(st), "solve");
         prof_resolve(P);
     }
+    return SDSB200_OK;
+}
+
+int sdsb200_solve_phase(sdsb200_plan* plan, int32_t phase, double* X, int64_t ldx, const double* B, int64_t ldb,
+                        int32_t nrhs, const sdsb200_opts* opts, void* stream) {
+    Plan* P = reinterpret_cast<Plan*>(plan);
+    if (!P) return fail(SDSB200_INVALID_VALUE, "plan is NULL");
+    if (phase < SDSB200_PHASE_FWD_PERM || phase > SDSB200_PHASE_STORE)
+        return fail(SDSB200_INVALID_VALUE, "unknown solve phase");
+    if (!P->factored) return fail(SDSB200_PHASE_ORDER, "solve phase before a successful factorization");
+    if (nrhs < 1 || nrhs > P->max_nrhs) return fail(SDSB200_INVALID_VALUE, "nrhs outside 1:max_nrhs of the plan");
+    const bool reads_b = phase == SDSB200_PHASE_FWD_PERM || phase == SDSB200_PHASE_LOAD;
+    const bool writes_x = phase == SDSB200_PHASE_BWD_PERM || phase == SDSB200_PHASE_STORE;
+    if (reads_b && (!B || ldb < P->n)) return fail(SDSB200_INVALID_VALUE, "B is NULL or its leading dimension < n");
+    if (writes_x && (!X || ldx < P->n)) return fail(SDSB200_INVALID_VALUE, "X is NULL or its leading dimension < n");
+    sdsb200_opts o;
+    if (opts) o = *opts;
+    else sdsb200_default_opts(&o);
+    if (o.solve_mode < 0 || o.solve_mode > 2) return fail(SDSB200_INVALID_VALUE, "solve_mode must be 0, 1 or 2");
+    const bool transpose = P->structure == STRUCT_G && o.solve_mode != 0;
+    int maxw = 1;
+    for (int w : P->level_maxw) maxw = std::max(maxw, w);
+    if ((size_t)maxw * nrhs * sizeof(double) > 200 * 1024)
+        return fail(SDSB200_NOT_SUPPORTED, "front too wide for this many right-hand sides in one solve");
+    cudaStream_t st = (cudaStream_t)stream;
+    P->launches_done = 0;
+    int rc = SDSB200_OK;
+    switch (phase) {
+        case SDSB200_PHASE_FWD_PERM: rc = permute(P, 0, B, ldb, nullptr, 0, nrhs, st); break;
+        case SDSB200_PHASE_FWD: rc = sweeps(P, nrhs, transpose, st, 1); break;
+        case SDSB200_PHASE_DIAG: rc = sweeps(P, nrhs, transpose, st, 2); break;
+        case SDSB200_PHASE_BWD: rc = sweeps(P, nrhs, transpose, st, 4); break;
+        case SDSB200_PHASE_BWD_PERM: rc = permute(P, 1, nullptr, 0, X, ldx, nrhs, st); break;
+        case SDSB200_PHASE_LOAD: rc = permute(P, 0, B, ldb, nullptr, 0, nrhs, st, true); break;
+        default: rc = permute(P, 1, nullptr, 0, X, ldx, nrhs, st, true); break;
+    }
+    if (rc) return rc;
+    CK(cudaGetLastError(), "solve phase");
+    if (P->profile) {
+        CK(cudaStreamSynchronize(st), "solve phase");
+        prof_resolve(P);
+    }
+    return SDSB200_OK;
+}
+
+int sdsb200_schur_matrix(sdsb200_plan* plan, int32_t member, double* D, int64_t ldd, int32_t transposed,
+                         void* stream) {
+    Plan* P = reinterpret_cast<Plan*>(plan);
+    if (!P) return fail(SDSB200_INVALID_VALUE, "plan is NULL");
+    if (P->schur_front < 0) return fail(SDSB200_INVALID_VALUE, "the analysis has no Schur complement (schur_mode = 0)");
+    if (!P->factored) return fail(SDSB200_PHASE_ORDER, "Schur complement before a successful factorization");
+    if (member < 0 || member >= P->nbatch) return fail(SDSB200_INVALID_VALUE, "member out of range");
+    const DFront& R = P->fronts[P->schur_front];
+    if (!D || ldd < R.w) return fail(SDSB200_INVALID_VALUE, "D is NULL or its leading dimension is below the Schur order");
+    cudaStream_t st = (cudaStream_t)stream;
+    const bool gen = P->structure == STRUCT_G;
+    cudaError_t e;
+    if (P->elsize == 8) {
+        const double* fac = static_cast<const double*>(P->d_factor) + (int64_t)member * P->factor_len;
+        const double* ufac = gen ? static_cast<const double*>(P->d_ufactor) + (int64_t)member * P->factor_len : nullptr;
+        e = launch_schur_dense<double>(fac, ufac, R.panel, R.w, D, ldd, transposed != 0, st);
+    } else {
+        const float* fac = static_cast<const float*>(P->d_factor) + (int64_t)member * P->factor_len;
+        const float* ufac = gen ? static_cast<const float*>(P->d_ufactor) + (int64_t)member * P->factor_len : nullptr;
+        e = launch_schur_dense<float>(fac, ufac, R.panel, R.w, D, ldd, transposed != 0, st);
+    }
+    CK(e, "Schur complement export");
     return SDSB200_OK;
 }
 
@@ -839,6 +917,8 @@ double sdsb200_plan_stat(const sdsb200_plan* plan, const char* name) {
     if (nm == "flops") return P->flops;
     if (nm == "elsize") return P->elsize;
     if (nm == "launches_done") return (double)P->launches_done;
+    if (nm == "schur_n") return P->schur_front >= 0 ? (double)P->fronts[P->schur_front].w : 0.0;
+    if (nm == "schur_level") return (double)P->schur_level;
     if (nm == "solve_status") {
         int32_t v = 0;
         cudaDeviceSynchronize();
@@ -974,6 +1054,9 @@ int sdsb200_solve_noalloc(sdsb200_plan* plan, double* X, int64_t ldx, const doub
     Plan* P = reinterpret_cast<Plan*>(plan);
     if (!P) return fail(SDSB200_INVALID_VALUE, "plan is NULL");
     if (!P->factored) return fail(SDSB200_PHASE_ORDER, "solve before a successful factorization");
+    if (P->schur_front >= 0)
+        return fail(SDSB200_NOT_SUPPORTED, "Schur complement mode: the factorization is partial; use the solve "
+                                           "phases (sdsb200_solve_phase)");
     if (nrhs < 1 || nrhs > P->max_nrhs) return fail(SDSB200_INVALID_VALUE, "nrhs outside 1:max_nrhs of the plan");
     if (ldx < P->n || ldb < P->n) return fail(SDSB200_INVALID_VALUE, "leading dimension smaller than n");
     if (!X || !B) return fail(SDSB200_INVALID_VALUE, "X or B is NULL");

@@ -154,6 +154,10 @@ size_t small_front_smem(int fmax, int elsize);
 template <typename T>
 cudaError_t launch_assemble_large(int structure, const LargeAsmArgs<T>& a, int nmembers, cudaStream_t st);
 cudaError_t launch_stats(const StatsArgs& a, int nmembers, cudaStream_t st);
+// the Schur complement of the unfactored root panel at p0 as a dense matrix (schur_kernels.cu)
+template <typename T>
+cudaError_t launch_schur_dense(const T* factor, const T* ufactor, int64_t p0, int ns, double* D, int64_t ldd,
+                               int transposed, cudaStream_t st);
 template <typename T>
 cudaError_t launch_gemm(const GemmArgs<T>& a, int nmembers, cudaStream_t st);
 // Inverses of the 64 x 64 diagonal blocks of the L11 panels of the wide fronts (for the solve)

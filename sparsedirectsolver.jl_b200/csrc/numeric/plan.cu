@@ -208,10 +208,30 @@ Plan* build_plan(const sdsb200_symbolic* sym, const sdsb200_plan_options* popts,
             F.level = 0;
             F.rc_begin = -1;
         }
+        // Schur complement mode (schedule.schur, src/symbolic/schedule.jl:351-360): a dense root
+        // supernode that the factorization assembles and does not factor
+        if (sym->schur != 0) {
+            const int64_t r = sym->schur - 1;
+            if (r < 0 || r >= ns) throw BuildError(SDSB200_INVALID_VALUE, "schur is not a supernode");
+            if (P->nbatch > 1)
+                throw BuildError(SDSB200_NOT_SUPPORTED, "Schur complement mode does not support uniform batches");
+            const DFront& R = P->fronts[r];
+            if (R.parent >= 0 || R.f != R.w)
+                throw BuildError(SDSB200_INVALID_VALUE, "the Schur front must be a root with no rows below its columns");
+            P->schur_front = (int)r;
+        }
         // levels: height above the leaves (children are numbered first)
         for (int64_t s = 0; s < ns; ++s) {
             int p = P->fronts[s].parent;
             if (p >= 0) P->fronts[p].level = std::max(P->fronts[p].level, P->fronts[s].level + 1);
+        }
+        if (P->schur_front >= 0) {
+            // the Schur root gets the last level to itself (src/symbolic/schedule.jl:457-458)
+            int top = 0;
+            for (int64_t s = 0; s < ns; ++s)
+                if (s != P->schur_front) top = std::max(top, P->fronts[s].level + 1);
+            P->fronts[P->schur_front].level = top;
+            P->schur_level = top;
         }
         P->nlevels = 0;
         for (auto& F : P->fronts) P->nlevels = std::max(P->nlevels, F.level + 1);
@@ -284,7 +304,7 @@ Plan* build_plan(const sdsb200_symbolic* sym, const sdsb200_plan_options* popts,
         for (int64_t s = 0; s < ns; ++s) {
             DFront& F = P->fronts[s];
             F.eacol_begin = (int32_t)eacol.size();
-            if (class_of(F.f) != 0) continue;
+            if (class_of(F.f) != 0 && s != P->schur_front) continue;
             std::vector<std::vector<std::pair<int, int>>> per(F.f);
             const int nchunk = (F.f + ASM_ROWS - 1) / ASM_ROWS;
             for (int q = F.ch_begin; q < F.ch_end; ++q) {
@@ -349,7 +369,7 @@ Plan* build_plan(const sdsb200_symbolic* sym, const sdsb200_plan_options* popts,
             std::map<int, std::vector<int>> small;
             std::vector<int> large;
             for (int s : P->level_fronts[L]) {
-                int c = class_of(P->fronts[s].f);
+                int c = s == P->schur_front ? 0 : class_of(P->fronts[s].f);
                 if (c) small[c].push_back(s);
                 else large.push_back(s);
             }
@@ -385,6 +405,7 @@ Plan* build_plan(const sdsb200_symbolic* sym, const sdsb200_plan_options* popts,
                 pl.count = (int)(coltasks.size() - pl.list);
                 P->prog.push_back(pl);
             }
+            if (L == P->schur_level) continue;   // the Schur root is assembled, not factored
             if (P->structure == STRUCT_SPD) {
                 const int NB = CHOL_NB;
                 int maxw = 0;
@@ -522,7 +543,7 @@ Plan* build_plan(const sdsb200_symbolic* sym, const sdsb200_plan_options* popts,
         auto solve_wide = [&](const DFront& F) { return F.w >= wide_w || (int64_t)(F.f - F.w) * F.w >= wide_area; };
         for (int64_t s = 0; s < ns; ++s) {
             const DFront& F = P->fronts[s];
-            if (!solve_wide(F)) continue;
+            if (!solve_wide(F) || s == P->schur_front) continue;
             dinv_off[s] = P->dinv_len;
             int nblk = (F.w + SOLVE_BLK - 1) / SOLVE_BLK;
             for (int b = 0; b < nblk; ++b) {
@@ -550,14 +571,14 @@ Plan* build_plan(const sdsb200_symbolic* sym, const sdsb200_plan_options* popts,
             for (int L = 0; L < P->nlevels; ++L) {
                 psmall[2 * L] = (int32_t)plist.size();
                 for (int s : P->level_fronts[L])
-                    if (!solve_wide(P->fronts[s])) {
+                    if (!solve_wide(P->fronts[s]) && s != P->schur_front) {
                         plist.push_back(s);
                         P->p_maxw_small = std::max(P->p_maxw_small, P->fronts[s].w);
                     }
                 psmall[2 * L + 1] = (int32_t)plist.size() - psmall[2 * L];
                 plarge[2 * L] = (int32_t)plist.size();
                 for (int s : P->level_fronts[L])
-                    if (solve_wide(P->fronts[s])) {
+                    if (solve_wide(P->fronts[s]) && s != P->schur_front) {
                         plist.push_back(s);
                         pmaxblk[L] = std::max(pmaxblk[L], (P->fronts[s].w + SOLVE_BLK - 1) / SOLVE_BLK);
                     }
@@ -809,6 +830,22 @@ Plan* build_plan(const sdsb200_symbolic* sym, const sdsb200_plan_options* popts,
         cudaMemsetAsync(P->d_kind, 0, n * nb, st);
         cudaMemsetAsync(P->d_d, 0, sizeof(double) * 2 * n * nb, st);
         cudaMemsetAsync(P->d_piv, 0, sizeof(int32_t) * n * nb, st);
+        std::vector<int32_t> spiv;
+        std::vector<int8_t> skind;
+        std::vector<double> sd;
+        if (P->schur_front >= 0) {
+            // the Schur root's columns: identity local order, unit 1x1 pivots, d = 1 and no 2x2 part
+            // (src/numeric/schur.jl:15-29); no kernel writes them, so they are set once here
+            const DFront& R = P->fronts[P->schur_front];
+            for (int k = 0; k < R.w; ++k) spiv.push_back(R.c0 + k + 1);
+            skind.assign(R.w, (int8_t)KIND_1X1);
+            sd.assign(R.w, 1.0);
+            for (int64_t mb = 0; mb < nb; ++mb) {
+                cudaMemcpyAsync(P->d_piv + mb * n + R.c0, spiv.data(), sizeof(int32_t) * R.w, cudaMemcpyHostToDevice, st);
+                cudaMemcpyAsync(P->d_kind + mb * n + R.c0, skind.data(), R.w, cudaMemcpyHostToDevice, st);
+                cudaMemcpyAsync(P->d_d + mb * 2 * n + R.c0, sd.data(), sizeof(double) * R.w, cudaMemcpyHostToDevice, st);
+            }
+        }
         cudaError_t e = cudaStreamSynchronize(st);
         if (e != cudaSuccess) throw BuildError(SDSB200_CUDA_ERROR, cudaGetErrorString(e));
         return P;

@@ -45,6 +45,9 @@ struct Plan {
     int64_t factor_len = 0, cb_len = 0, ulen = 0, scr_len = 0, work_len = 0, inv_len = 0;
     int nlevels = 0;
     int fsmall_max = 0;
+    // Schur complement mode: the root front that is assembled but not factored (-1: none), alone on
+    // the last level
+    int schur_front = -1, schur_level = -1;
     std::vector<DFront> fronts;
     std::vector<std::vector<int>> level_fronts;
     std::vector<int> level_maxw;

@@ -26,6 +26,7 @@ struct SweepArgs {
     int32_t unit;              // unit diagonal (LDLT, LU)
     int32_t reorder;           // apply (forward) / undo (backward) the local pivot order
     int32_t rect;              // 1: this CTA also does the rectangular part (L21 x / L21^T x)
+    int32_t pull_only;         // forward: only pull the children's updates into Y (the unfactored Schur root)
     const int32_t* tiles;      // split rectangular part of large fronts: (front, first row / column) pairs
 };
 
@@ -77,7 +78,7 @@ struct DiagArgs {
 
 struct PermArgs {
     const int32_t* members;
-    const int32_t* perm;       // 0-based original index of each factor position
+    const int32_t* perm;       // 0-based original index of each factor position; NULL: the identity
     double* Y;
     const double* in;          // mode 0
     double* out;               // modes 1, 2

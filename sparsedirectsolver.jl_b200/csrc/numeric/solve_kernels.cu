@@ -148,6 +148,12 @@ __device__ void forward_front(const SweepArgs<T>& A, int s, int member, double* 
         pull_child(tid, nt, mc * nrhs, mc, ri, uc, w, m, xs, w, u);
         __syncthreads();
     }
+    if (A.pull_only) {
+        // the Schur root: its rows keep Y2 - L21 Y1, the condensed right-hand side
+        for (int q = tid; q < w * nrhs; q += nt) Y[fd.c0 + q % w + (int64_t)(q / w) * n] = xs[q];
+        __syncthreads();
+        return;
+    }
     if (A.reorder) {
         // apply the local pivot order (the rows of this front's own columns only)
         for (int q = tid; q < w * nrhs; q += nt) {
@@ -1107,7 +1113,7 @@ __global__ void permute_kernel(PermArgs A) {
     double* Y = A.Y + (int64_t)member * n * A.nrhs;
     for (int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; q < n * A.nrhs; q += (int64_t)gridDim.x * blockDim.x) {
         const int64_t k = q % n, r = q / n;
-        const int64_t g = A.perm[k];
+        const int64_t g = A.perm ? A.perm[k] : k;
         if (A.mode == 0) {
             Y[q] = A.in[member * A.ldin * A.nrhs + g + r * A.ldin];
         } else if (A.mode == 1) {

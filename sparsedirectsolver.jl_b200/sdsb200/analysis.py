@@ -21,7 +21,8 @@ PAIRS = {"none": 0, "default": 1, "all": 2}
 
 MAP_NAMES = ("perm", "iperm", "super_ptr", "snparent", "snpost", "rowptr", "rowval", "front_ptr", "front_nrows",
              "front_ncols", "child_ptr", "child_list", "relind_ptr", "relind", "amap", "amap_ptr", "amap_src",
-             "counts", "pairs", "full_rowptr", "full_colval", "full_srcptr", "full_src", "full_conj")
+             "counts", "pairs", "full_rowptr", "full_colval", "full_srcptr", "full_src", "full_conj",
+             "schur_rowptr", "schur_colval")
 
 
 class _Opts(C.Structure):
@@ -29,7 +30,8 @@ class _Opts(C.Structure):
                 ("user_perm", C.POINTER(C.c_int64)), ("pivot_pairs", C.c_int),
                 ("pivot_pair_tolerance", C.c_double), ("pivot_threshold", C.c_double),
                 ("use_superpanels", C.c_int), ("amalg_max_width", C.c_int), ("amalg_zero_fraction", C.c_double),
-                ("amalg_min_width", C.c_int), ("user_pairs", C.c_void_p), ("n_user_pairs", C.c_int64)]
+                ("amalg_min_width", C.c_int), ("user_pairs", C.c_void_p), ("n_user_pairs", C.c_int64),
+                ("user_schur_indices", C.c_void_p)]
 
 
 @dataclass
@@ -37,7 +39,11 @@ class Symbolic:
     """The reference's ``Symbolic`` (src/symbolic/maps.jl:62-95): 1-based int64 maps.
 
     Field names follow ``DEVICE_MAPS`` (maps.jl:16-18); ``snpost``, ``counts``,
-    ``pairs`` and the ``full_*`` residual map are the host-side extras.
+    ``pairs`` and the ``full_*`` residual map are the host-side extras. Schur
+    complement mode: ``schur`` is the root supernode that is assembled and not
+    factored (``schedule.schur``, 1-based; 0 = none), ``schur_n`` its order, and
+    ``schur_rowptr``/``schur_colval`` the 1-based CSR pattern of S
+    (``schur_pattern``, src/symbolic/ordering.jl:424-470).
     """
 
     n: int
@@ -52,6 +58,8 @@ class Symbolic:
     sdepth: int
     alg_used: int
     maps: dict = field(default_factory=dict)
+    schur: int = 0
+    schur_n: int = 0
 
     def __getattr__(self, name):
         maps = self.__dict__.get("maps")
@@ -66,8 +74,12 @@ class Symbolic:
 
 def analyze(rowptr, colval, n, structure="SPD", nzval=None, view="F", index_base=0, reordering="default",
             user_perm=None, pivot_pairs="default", pivot_pair_tolerance=1e-6, pivot_threshold=0.01,
-            use_superpanels=1, amalgamation=(32, 0.25, 8), user_pairs=None) -> Symbolic:
-    """Analyse the pattern of an ``n x n`` CSR matrix (``index_base`` of its arrays)."""
+            use_superpanels=1, amalgamation=(32, 0.25, 8), user_pairs=None, user_schur_indices=None) -> Symbolic:
+    """Analyse the pattern of an ``n x n`` CSR matrix (``index_base`` of its arrays).
+
+    ``user_schur_indices`` (n flags 0/1, or None): Schur complement mode, the flagged rows and columns
+    ordered last as one unfactored root supernode (compute_schur_ordering and
+    schur_supernode_partition, src/symbolic/ordering.jl:386-415, src/symbolic/supernodes.jl:391-425)."""
     lib = analysis_lib()
     rp = np.ascontiguousarray(rowptr, dtype=np.int64)
     cv = np.ascontiguousarray(colval, dtype=np.int64)
@@ -86,11 +98,17 @@ def analyze(rowptr, colval, n, structure="SPD", nzval=None, view="F", index_base
     o.pivot_threshold = pivot_threshold
     o.use_superpanels = int(use_superpanels)
     o.amalg_max_width, o.amalg_zero_fraction, o.amalg_min_width = amalgamation
-    up = None
+    upairs = None
     if user_pairs is not None and len(user_pairs) > 0:
-        up = np.ascontiguousarray(np.asarray(user_pairs, dtype=np.int64).reshape(-1, 2))
-        o.user_pairs = up.ctypes.data
-        o.n_user_pairs = up.shape[0]
+        upairs = np.ascontiguousarray(np.asarray(user_pairs, dtype=np.int64).reshape(-1, 2))
+        o.user_pairs = upairs.ctypes.data
+        o.n_user_pairs = upairs.shape[0]
+    flags = None
+    if user_schur_indices is not None:
+        flags = np.ascontiguousarray(np.asarray(user_schur_indices).reshape(-1) != 0, dtype=np.int8)
+        if flags.size != n:
+            raise ValueError(f"user_schur_indices has {flags.size} entries, the matrix has {n} rows")
+        o.user_schur_indices = flags.ctypes.data
     res = C.c_void_p()
     rc = lib.sdsa_analyze(C.c_int64(n), rp.ctypes.data_as(C.c_void_p), cv.ctypes.data_as(C.c_void_p),
                           nz.ctypes.data_as(C.c_void_p) if nz is not None else None, C.byref(o), C.byref(res))
@@ -108,7 +126,7 @@ def analyze(rowptr, colval, n, structure="SPD", nzval=None, view="F", index_base
         return Symbolic(n=int(n), nnz=int(cv.size), ns=int(st("ns")), structure=structure, view=view,
                         index_base=int(index_base), nnz_stored=int(st("nnz_stored")), nnz_L=int(st("nnz_L")),
                         flops=float(st("flops")), sdepth=int(st("sdepth")), alg_used=int(st("alg_used")),
-                        maps=maps)
+                        maps=maps, schur=int(st("schur")), schur_n=int(st("schur_n")))
     finally:
         lib.sdsa_free(res)
 

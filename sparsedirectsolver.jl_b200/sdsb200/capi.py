@@ -19,7 +19,11 @@ PIVOT_TYPE = {"A": 0, "N": 1, "C": 2, "R": 3, "D": 4, "L": 5, "B": 6}
 EXPORTS = ("sdsb200_default_opts", "sdsb200_plan_create", "sdsb200_plan_destroy", "sdsb200_factor", "sdsb200_solve",
            "sdsb200_get_stats", "sdsb200_get_pivots", "sdsb200_get_factor", "sdsb200_set_members",
            "sdsb200_set_interrupt", "sdsb200_set_graphs", "sdsb200_set_persistent", "sdsb200_set_profiling", "sdsb200_get_trace", "sdsb200_plan_stat", "sdsb200_last_error",
-           "sdsb200_solve_noalloc", "sdsb200_sampled_outer", "sdsb200_residual")
+           "sdsb200_solve_noalloc", "sdsb200_sampled_outer", "sdsb200_residual", "sdsb200_solve_phase",
+           "sdsb200_schur_matrix")
+
+# solve sub-phases of sdsb200_solve_phase
+PHASE = {"fwd_perm": 1, "fwd": 2, "diag": 3, "bwd": 4, "bwd_perm": 5, "load": 6, "store": 7}
 
 
 class Symbolic(C.Structure):
@@ -28,7 +32,7 @@ class Symbolic(C.Structure):
         (nm, C.c_void_p) for nm in ("perm", "super_ptr", "snparent", "rowptr", "rowval", "front_ptr", "child_ptr",
                                     "child_list", "relind_ptr", "relind", "amap", "amap_ptr", "amap_src",
                                     "full_rowptr", "full_colval", "full_srcptr", "full_src")] + [
-        ("full_nnz", C.c_int64), ("full_nsrc", C.c_int64)]
+        ("full_nnz", C.c_int64), ("full_nsrc", C.c_int64), ("schur", C.c_int64)]
 
 
 class PlanOptions(C.Structure):
@@ -67,6 +71,8 @@ def bind(lib):
         "sdsb200_last_error": (C.c_char_p, []),
         "sdsb200_solve_noalloc": (C.c_int, [P, P, C.c_int64, P, C.c_int64, C.c_int32, C.c_int32, P, P]),
         "sdsb200_residual": (C.c_int, [P, P, P, C.c_int64, P, C.c_int64, C.c_int32, P, C.c_int32, P]),
+        "sdsb200_solve_phase": (C.c_int, [P, C.c_int32, P, C.c_int64, P, C.c_int64, C.c_int32, C.POINTER(Opts), P]),
+        "sdsb200_schur_matrix": (C.c_int, [P, C.c_int32, P, C.c_int64, C.c_int32, P]),
         "sdsb200_sampled_outer": (C.c_int, [C.c_int64, C.c_int64, P, P, C.c_int32, C.c_int32, C.c_int32, C.c_int32,
                                             P, C.c_int64, P, C.c_int64, C.c_int32, C.c_int32, C.c_double, P, P]),
     }

@@ -50,6 +50,7 @@ _DEFAULTS = {
     "ubatch_index": -1, "use_superpanels": 1, "ir_mode": "plain", "factor_precision": None,
     "amalgamation": (32, 0.25, 8), "pivot_pairs": "default", "pivot_pair_tolerance": 1e-6, "user_perm": None,
     "pivot_sign": None, "user_host_interrupt": None, "max_nrhs": 8, "tuning": 0,
+    "schur_mode": 0, "user_schur_indices": None,
 }
 
 
@@ -130,6 +131,8 @@ class DirectSolver:
 
     # -- parameters -------------------------------------------------------------------------------------------
     def setparam(self, name, value):
+        if name == "schur_matrix":
+            return self._set_schur_dest(value)
         if name not in _DEFAULTS:
             raise InvalidValueError(f"unknown parameter {name!r}")
         if name == "pivot_type" and value not in capi.PIVOT_TYPE:
@@ -150,6 +153,14 @@ class DirectSolver:
             value = np.asarray(value, dtype=np.int8)
             if value.size != self.n if hasattr(self, "n") else False:
                 raise InvalidValueError(f"pivot_sign has {value.size} entries, the matrix has {self.n} rows")
+        if name == "schur_mode" and int(value) not in (0, 1):
+            raise InvalidValueError("schur_mode must be 0 or 1")
+        if name == "user_schur_indices" and value is not None:
+            value = np.asarray(value).reshape(-1)
+            if hasattr(self, "n") and value.size != self.n:
+                raise InvalidValueError(f"user_schur_indices has {value.size} entries, the matrix has {self.n} rows")
+            if not np.all((value == 0) | (value == 1)):
+                raise InvalidValueError("user_schur_indices must hold flags 0 or 1")
         if name == "ubatch_index" and self._plan_exists():
             self._apply_members(int(value))
         self.params[name] = value
@@ -258,6 +269,11 @@ class DirectSolver:
         if name == "diag":
             self._need(2, name)
             return self.factor_diag()
+        if name in ("schur_shape", "schur_matrix"):
+            self._need(1 if name == "schur_shape" else 2, name)
+            if self.symbolic.schur == 0:
+                raise InvalidValueError(f"the data parameter {name!r} needs an analysis with schur_mode = 1")
+            return self._schur_shape() if name == "schur_shape" else self._schur_matrix()
         if name in self.params:
             return self.params[name]
         raise InvalidValueError(f"unknown parameter {name!r}")
@@ -275,9 +291,15 @@ class DirectSolver:
         if phase in ("factorization", "refactorization"):
             return self._factorize(refactor=phase == "refactorization")
         if phase in ("solve", "solve_refinement", "solve_fwd_perm", "solve_fwd", "solve_diag", "solve_bwd",
-                     "solve_bwd_perm"):
+                     "solve_bwd_perm", "solve_fwd_schur", "solve_bwd_schur"):
+            if self._stage < 2:
+                raise FactorizationError(f"phase {phase!r} before the factorization")
+            if self.symbolic.schur > 0:
+                return self._schur_phase(phase, X, B)
+            if phase in ("solve_fwd_schur", "solve_bwd_schur"):
+                raise FactorizationError(f"phase {phase!r} needs an analysis with schur_mode = 1")
             if phase not in ("solve", "solve_refinement"):
-                raise NotSupportedError(f"phase {phase!r}: only the complete solve is exposed")
+                return self._sub_phase(phase, X, B)
             return self._solve(X, B)
         raise InvalidValueError(f"unknown phase {phase!r}")
 
@@ -302,6 +324,22 @@ class DirectSolver:
 
     def _analysis(self):
         p = self.params
+        flags = None
+        if int(p["schur_mode"]) == 1:
+            # Schur complement mode (src/solver.jl:471-475, 554-559): the flagged rows and columns last, as
+            # one root front that the factorization assembles and does not factor
+            if p["matching_alg"] != "default":
+                raise NotSupportedError("matching_alg is not supported with schur_mode = 1")
+            if self.nbatch > 1:
+                raise NotSupportedError("schur_mode = 1 is not supported for uniform batches")
+            if p["user_schur_indices"] is None:
+                raise InvalidValueError("schur_mode = 1 needs \"user_schur_indices\" (n flags 0/1)")
+            flags = np.asarray(p["user_schur_indices"]).reshape(-1)
+            if flags.size != self.n:
+                raise InvalidValueError(f"user_schur_indices has {flags.size} entries, the matrix has {self.n} rows")
+            if not np.any(flags != 0):
+                raise InvalidValueError("user_schur_indices selects no row: the Schur complement would be empty")
+        self._schur_dest = None
         nz_host = self.nzval[: self.nnz].cpu().numpy() if self.structure == "S" else None
         colval = self._prepare_matching()
         user_pairs = None
@@ -318,7 +356,8 @@ class DirectSolver:
                                 user_perm=p["user_perm"], pivot_pairs=p["pivot_pairs"],
                                 pivot_pair_tolerance=p["pivot_pair_tolerance"],
                                 pivot_threshold=p["pivot_threshold"], use_superpanels=p["use_superpanels"],
-                                amalgamation=tuple(p["amalgamation"]), user_pairs=user_pairs)
+                                amalgamation=tuple(p["amalgamation"]), user_pairs=user_pairs,
+                                user_schur_indices=flags)
         self._create_plan()
         self._stage = 1
 
@@ -343,6 +382,7 @@ class DirectSolver:
             setattr(sym, nm, a.ctypes.data)
         sym.full_nnz = int(S.full_colval.size)
         sym.full_nsrc = int(S.full_src.size)
+        sym.schur = int(getattr(S, "schur", 0))
         po = capi.PlanOptions(nbatch=self.nbatch, precision=self._precision(), max_nrhs=int(self.params["max_nrhs"]),
                               tuning=int(self.params["tuning"]))
         plan = C.c_void_p()
@@ -436,6 +476,178 @@ class DirectSolver:
             np.copyto(X, out.cpu().numpy())
             return X
         return out
+
+    # -- solve sub-phases and Schur complement mode -------------------------------------------------------------
+    def _colmajor(self, B):
+        """B (n, n x nrhs, or nbatch x n x nrhs; host or device) as a device column-major tensor
+        (members, nrhs, n), with its nrhs and a function that maps a result back to B's shape."""
+        torch = self._torch
+        Bt = B if isinstance(B, torch.Tensor) else torch.from_numpy(np.asarray(B, dtype=np.float64))
+        Bt = Bt.to(self.device, torch.float64)
+        n = self.n
+        vec = Bt.dim() == 1
+        Bm = Bt.reshape(n, -1) if vec or self.nbatch == 1 else Bt.reshape(self.nbatch, n, -1)
+        if Bm.dim() == 2:
+            cm, nrhs = Bm.t().contiguous(), Bm.shape[1]
+        else:
+            cm, nrhs = Bm.transpose(1, 2).contiguous(), Bm.shape[2]
+        shape = Bt.shape
+
+        def back(Xcm):
+            out = Xcm.t() if Xcm.dim() == 2 else Xcm.transpose(1, 2)
+            return out.reshape(shape)
+
+        return cm, int(nrhs), back
+
+    def _deliver(self, X, out):
+        if X is None:
+            return out
+        if isinstance(X, self._torch.Tensor):
+            X.copy_(out)
+            return X
+        np.copyto(X, out.cpu().numpy())
+        return X
+
+    def _run_phase(self, code, Xcm, Bcm, nrhs, o=None):
+        lib = numeric_lib()
+        stream = self._torch.cuda.current_stream(self.device).cuda_stream
+        o = self._opts() if o is None else o
+        n = self.n
+        _check(lib.sdsb200_solve_phase(self._plan, capi.PHASE[code],
+                                       C.c_void_p(Xcm.data_ptr()) if Xcm is not None else None, n,
+                                       C.c_void_p(Bcm.data_ptr()) if Bcm is not None else None, n, nrhs,
+                                       C.byref(o), C.c_void_p(stream)), lib)
+
+    def _phase_nrhs(self, X, B):
+        src = B if B is not None else X
+        if src is not None:
+            return self._colmajor(src)[1]
+        if getattr(self, "_last_phase_nrhs", None) is None:
+            raise FactorizationError("no right-hand side: run \"solve_fwd_perm\" first")
+        return self._last_phase_nrhs
+
+    def _sub_phase(self, phase, X, B):
+        """``execute!(phase)`` for the solve sub-phases (src/solver.jl:856-867): "solve_fwd_perm" reads B into
+        the plan's working vectors Y (factor order; with matching, scaled as the complete solve scales it),
+        "solve_fwd", "solve_diag" and "solve_bwd" work on Y, and "solve_bwd_perm" writes X from Y (and
+        returns it). No refinement."""
+        o = self._opts()
+        if phase == "solve_fwd_perm":
+            if B is None:
+                raise InvalidValueError("\"solve_fwd_perm\" needs B")
+            Bcm, nrhs, _ = self._colmajor(B)
+            if self._matching is not None:
+                Bcm = self._scaled_rhs(Bcm, int(o.solve_mode))
+            self._run_phase("fwd_perm", None, Bcm, nrhs, o)
+            self._last_phase_nrhs = nrhs
+            return None
+        if phase in ("solve_fwd", "solve_diag", "solve_bwd"):
+            self._run_phase(phase[6:], None, None, self._phase_nrhs(X, B), o)
+            return None
+        # solve_bwd_perm
+        src = X if X is not None else B
+        if src is None:
+            raise InvalidValueError("\"solve_bwd_perm\" needs X (or B for its shape)")
+        Xcm, nrhs, back = self._colmajor(src)
+        Xcm = self._torch.empty_like(Xcm)
+        self._run_phase("bwd_perm", Xcm, None, nrhs, o)
+        if self._matching is not None:
+            Xcm = self._unscaled_solution(Xcm, int(o.solve_mode))
+        return self._deliver(X, back(Xcm))
+
+    def _schur_phase(self, phase, X, B):
+        """The solve phases of Schur complement mode (_schur_solve_phase!, src/solver.jl:876-900). Each reads B
+        and writes X (returned; X is B allowed); the vectors are in factor order, the last ns entries being the
+        Schur block in increasing original order:
+        "solve_fwd_schur": permutation and forward sweep; the Schur block of X is b2 - A21 A11^{-1} b1;
+        "solve_diag": D^{-1} of LDLT on the factored part (the identity for Cholesky and LU, and on the Schur
+        block);
+        "solve_bwd_schur": with the Schur solution x2 in the Schur block of B, the diagonal of LU, the
+        backward sweep and the inverse permutation: X solves op(A) x = b."""
+        if phase not in ("solve_fwd_schur", "solve_diag", "solve_bwd_schur"):
+            raise NotSupportedError(f"phase {phase!r} with schur_mode = 1: the factorization is partial; use "
+                                    "\"solve_fwd_schur\", \"solve_diag\" and \"solve_bwd_schur\"")
+        if B is None:
+            raise InvalidValueError(f"phase {phase!r} needs B")
+        o = self._opts()
+        Bcm, nrhs, back = self._colmajor(B)
+        Xcm = self._torch.empty_like(Bcm)
+        lu = self.structure == "G"
+        if phase == "solve_fwd_schur":
+            steps = [("fwd_perm", None, Bcm), ("fwd", None, None), ("store", Xcm, None)]
+        elif phase == "solve_diag":
+            steps = [("load", None, Bcm)] + ([] if lu else [("diag", None, None)]) + [("store", Xcm, None)]
+        else:
+            steps = ([("load", None, Bcm)] + ([("diag", None, None)] if lu else []) +
+                     [("bwd", None, None), ("bwd_perm", Xcm, None)])
+        for code, x, b in steps:
+            self._run_phase(code, x, b, nrhs, o)
+        return self._deliver(X, back(Xcm))
+
+    def _schur_pattern_nnz(self, lower):
+        S = self.symbolic
+        rp, cv = S.schur_rowptr, S.schur_colval
+        if not lower:
+            return int(cv.size)
+        rows = np.repeat(np.arange(1, S.schur_n + 1), np.diff(rp))
+        return int(np.count_nonzero(cv <= rows))
+
+    def _schur_shape(self):
+        """``getparam("schur_shape")`` (src/solver.jl:1267-1271): (ns, ns, nnz of the pattern of S; one triangle
+        with the diagonal for the symmetric structures)."""
+        ns = self.symbolic.schur_n
+        return (ns, ns, self._schur_pattern_nnz(self.structure != "G"))
+
+    def _set_schur_dest(self, value):
+        """``setparam!("schur_matrix", dest)`` (src/solver.jl:1303-1316): the destination that
+        ``getparam("schur_matrix")`` fills: None (a new dense matrix each time), a dense (ns, ns) float64 CUDA
+        tensor, or a sparse ``(rowptr, colval, nzval)`` triple of CUDA tensors (CSR with the pattern of
+        ``schur_shape`` over the full matrix or, as a 4th item 'L' or 'U', one triangle; 0- or 1-based)."""
+        torch = self._torch
+        sym = getattr(self, "symbolic", None)
+        if sym is None or sym.schur == 0:
+            raise InvalidValueError("the data parameter \"schur_matrix\" needs an analysis with schur_mode = 1")
+        ns = self.symbolic.schur_n
+        if value is None:
+            self._schur_dest = None
+            return
+        if isinstance(value, torch.Tensor):
+            if tuple(value.shape) != (ns, ns) or value.dtype != torch.float64 or value.device.type != "cuda":
+                raise InvalidValueError(f"schur_matrix: expected a ({ns}, {ns}) float64 CUDA tensor")
+            self._schur_dest = value
+            return
+        if isinstance(value, tuple) and len(value) in (3, 4):
+            view = value[3] if len(value) == 4 else "F"
+            if view not in ("F", "L", "U"):
+                raise InvalidValueError("schur_matrix: the view must be 'F', 'L' or 'U'")
+            rowptr, colval, nzval = value[:3]
+            nz = self._schur_pattern_nnz(view != "F")
+            if rowptr.numel() != ns + 1 or colval.numel() != nz or nzval.numel() != nz:
+                raise InvalidValueError(f"schur_matrix: the sparse Schur complement with view {view!r} has {nz} "
+                                        f"entries; see \"schur_shape\"")
+            self._schur_dest = (rowptr, colval, nzval, view)
+            return
+        raise InvalidValueError("schur_matrix: expected None, a dense CUDA tensor or (rowptr, colval, nzval[, view])")
+
+    def _schur_matrix(self):
+        """``getparam("schur_matrix")`` (src/solver.jl:1114-1121): S = A22 - A21 A11^{-1} A12 of the last
+        factorization, written into the registered destination (or a new dense CUDA matrix) and returned."""
+        torch = self._torch
+        lib = numeric_lib()
+        ns = self.symbolic.schur_n
+        stream = torch.cuda.current_stream(self.device).cuda_stream
+        dest = getattr(self, "_schur_dest", None)
+        D = dest if isinstance(dest, torch.Tensor) else torch.empty((ns, ns), dtype=torch.float64, device=self.device)
+        # D is row-major (ns, ns) for torch: the column-major export of S^T lands as S
+        _check(lib.sdsb200_schur_matrix(self._plan, 0, C.c_void_p(D.data_ptr()), ns, 1, C.c_void_p(stream)), lib)
+        if not isinstance(dest, tuple):
+            return D
+        rowptr, colval, nzval, _ = dest
+        base = int(rowptr[0].item())
+        rows = torch.repeat_interleave(torch.arange(ns, device=D.device),
+                                       (rowptr[1:] - rowptr[:-1]).to(torch.int64))
+        nzval.copy_(D[rows, colval.to(torch.int64) - base])
+        return nzval
 
     # -- outputs for tests -------------------------------------------------------------------------------------
     def factor_host(self, member=0):
