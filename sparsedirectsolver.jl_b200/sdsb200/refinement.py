@@ -1,4 +1,14 @@
-"""FGMRES-IR: the reference's ``fgmres_refine!`` (src/solve/refinement.jl:577-614).
+"""Refinement of a given X on the host above the C ABI: plain iterative refinement (the reference's
+``refine!``, src/solve/refinement.jl:359-397) for the "solve_refinement" phase, and FGMRES-IR
+(``fgmres_refine!``, src/solve/refinement.jl:577-614).
+
+Plain refinement, at most nsteps steps of
+
+    R = B - op(A) X                        sdsb200_residual
+    stop if tol > 0 and max_k ||R_k|| / ||B_k|| <= tol
+    X += op(A)^{-1} R                      sdsb200_solve without refinement
+
+FGMRES-IR:
 
 On the stacked compact columns (all right-hand sides of all members as one vector of length
 n * ncols):
@@ -21,6 +31,74 @@ import ctypes as C
 import math
 
 import numpy as np
+
+
+def _max_relative(R, B, n):
+    """max over the columns of ||R_k|| / ||B_k|| (||R_k|| where B_k = 0), as the reference's
+    _max_relative_residual."""
+    import torch
+
+    rn = R.reshape(-1, n).norm(dim=1)
+    bn = B.reshape(-1, n).norm(dim=1)
+    rel = torch.where(bn > 0, rn / torch.where(bn > 0, bn, torch.ones_like(bn)), rn)
+    return float(rel.max()) if rel.numel() else 0.0
+
+
+def ir_iterate(residual, solve, Xcm, Bcm, n, nsteps, tol, interrupted=None):
+    """Plain iterative refinement of Xcm in place (refine!, src/solve/refinement.jl:359-397) with the
+    callables residual(X, B) -> B - op(A) X and solve(R) -> op(A)^{-1} R. tol = 0 never stops early.
+    interrupted() is polled before every step; when it returns True the refinement stops and
+    (steps done, True) is returned, X holding the last completed iterate. Returns (steps, False)
+    otherwise."""
+    steps = 0
+    for _ in range(int(nsteps)):
+        if interrupted is not None and interrupted():
+            return steps, True
+        R = residual(Xcm, Bcm)
+        if tol > 0 and _max_relative(R, Bcm, n) <= tol:
+            break
+        Xcm += solve(R)
+        steps += 1
+    return steps, False
+
+
+def _capi_ops(solver, nrhs, solve_mode, nzval):
+    """residual(X, B) and solve(R) through the C ABI on the solver's plan and current stream."""
+    import torch
+
+    from ._native import numeric_lib
+    from .solver import _check
+
+    lib = numeric_lib()
+    n = solver.n
+    stream = C.c_void_p(torch.cuda.current_stream(solver.device).cuda_stream)
+    nz = C.c_void_p((solver.nzval if nzval is None else nzval).data_ptr())
+    opts = solver._opts()
+    opts.ir_n_steps = 0
+    opts.solve_mode = solve_mode
+    steps = C.c_int32(0)
+
+    def residual(X, B):
+        X = X.contiguous()
+        R = torch.empty_like(B)
+        _check(lib.sdsb200_residual(solver._plan, C.c_void_p(R.data_ptr()), C.c_void_p(X.data_ptr()), n,
+                                    C.c_void_p(B.data_ptr()), n, nrhs, nz, solve_mode, stream), lib)
+        return R
+
+    def solve(R):
+        out = torch.empty_like(R)
+        _check(lib.sdsb200_solve(solver._plan, C.c_void_p(out.data_ptr()), n, C.c_void_p(R.data_ptr()), n, nrhs,
+                                 nz, C.byref(opts), C.byref(steps), stream), lib)
+        return out
+
+    return residual, solve
+
+
+def ir_refine(solver, Xcm, Bcm, nrhs, solve_mode, nsteps, tol, nzval=None, interrupted=None):
+    """Plain refinement of Xcm (device, column-major per member) in place through the C ABI; returns
+    (steps, interrupted) as ir_iterate."""
+    residual, solve = _capi_ops(solver, nrhs, solve_mode, nzval)
+    return ir_iterate(residual, solve, Xcm, Bcm, solver.n, nsteps, tol, interrupted)
 
 
 def fgmres_refine(solver, Xcm, Bcm, nrhs, solve_mode, nsteps, tol, nzval=None):

@@ -216,6 +216,13 @@ class DirectSolver:
             return (Bcm * d["r"]).contiguous()
         return (Bcm * d["c"])[..., d["perm0"]].contiguous()
 
+    def _scaled_solution(self, Xcm, mode):
+        """The matched system's unknowns from x (the inverse of _unscaled_solution)."""
+        d = self._mdev
+        if self._matching.symmetric or mode != 0:
+            return (Xcm / d["r"]).contiguous()
+        return (Xcm[..., d["perm0"]] / d["c_perm"]).contiguous()
+
     def _unscaled_solution(self, Ycm, mode):
         """x from the matched system's solution: "G" x = Dc Q y (A), x = Dr z (A^T); symmetric x = D y."""
         d = self._mdev
@@ -298,7 +305,9 @@ class DirectSolver:
                 return self._schur_phase(phase, X, B)
             if phase in ("solve_fwd_schur", "solve_bwd_schur"):
                 raise FactorizationError(f"phase {phase!r} needs an analysis with schur_mode = 1")
-            if phase not in ("solve", "solve_refinement"):
+            if phase == "solve_refinement":
+                return self._refine(X, B)
+            if phase != "solve":
                 return self._sub_phase(phase, X, B)
             return self._solve(X, B)
         raise InvalidValueError(f"unknown phase {phase!r}")
@@ -554,6 +563,52 @@ class DirectSolver:
         if self._matching is not None:
             Xcm = self._unscaled_solution(Xcm, int(o.solve_mode))
         return self._deliver(X, back(Xcm))
+
+    def _refine(self, X, B):
+        """``execute!("solve_refinement", X, B)`` (_refine_phase!, src/solver.jl:902-926): refine the given
+        solution X of op(A) X = B in place, ``ir_n_steps`` steps of plain refinement (stopping once
+        max_k ||R_k|| / ||B_k|| <= ``ir_tol`` when ir_tol > 0) or of FGMRES-IR (``ir_mode = "fgmres"``).
+        With ir_n_steps = 0, X is left as it is. X and B must not alias. With a matching, the
+        refinement runs on the matched system, as the complete solve's does."""
+        torch = self._torch
+        if X is None or B is None:
+            raise InvalidValueError("\"solve_refinement\" needs X (the solution to refine) and B")
+        if isinstance(X, torch.Tensor) and isinstance(B, torch.Tensor) and X.data_ptr() == B.data_ptr():
+            raise InvalidValueError("\"solve_refinement\" needs the original right-hand side: X and B must not alias")
+        if isinstance(X, np.ndarray) and isinstance(B, np.ndarray) and np.shares_memory(X, B):
+            raise InvalidValueError("\"solve_refinement\" needs the original right-hand side: X and B must not alias")
+        o = self._opts()
+        nsteps, tol, mode = int(o.ir_n_steps), float(o.ir_tol), int(o.solve_mode)
+        if nsteps <= 0:
+            self._ir_steps = 0
+            return X
+        if int(self.params["ubatch_index"]) >= 0:
+            raise NotSupportedError("\"solve_refinement\" refines all batch members together")
+        Xcm, nrhs, back = self._colmajor(X)
+        Bcm, nrhs_b, _ = self._colmajor(B)
+        if nrhs_b != nrhs:
+            raise InvalidValueError(f"X has {nrhs} right-hand sides, B {nrhs_b}")
+        vals = self.nzval if self._matching is None else self._factor_values()
+        if self._matching is not None:
+            Xcm = self._scaled_solution(Xcm, mode)
+            Bcm = self._scaled_rhs(Bcm, mode)
+        Xcm = Xcm.clone()
+        from .refinement import fgmres_refine, ir_refine
+
+        if self.params["ir_mode"] == "fgmres":
+            self._ir_steps = fgmres_refine(self, Xcm, Bcm, nrhs, mode, nsteps, tol, nzval=vals)
+            stopped = False
+        else:
+            flag = self.params["user_host_interrupt"]
+            poll = (lambda: flag.value != 0) if flag is not None else None
+            self._ir_steps, stopped = ir_refine(self, Xcm, Bcm, nrhs, mode, nsteps, tol, nzval=vals,
+                                                interrupted=poll)
+        if self._matching is not None:
+            Xcm = self._unscaled_solution(Xcm, mode)
+        out = self._deliver(X, back(Xcm))
+        if stopped:
+            raise InterruptedError_("interrupted by user_host_interrupt")
+        return out
 
     def _schur_phase(self, phase, X, B):
         """The solve phases of Schur complement mode (_schur_solve_phase!, src/solver.jl:876-900). Each reads B
