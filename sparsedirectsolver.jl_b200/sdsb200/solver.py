@@ -50,7 +50,7 @@ _DEFAULTS = {
     "ubatch_index": -1, "use_superpanels": 1, "ir_mode": "plain", "factor_precision": None,
     "amalgamation": (32, 0.25, 8), "pivot_pairs": "default", "pivot_pair_tolerance": 1e-6, "user_perm": None,
     "pivot_sign": None, "user_host_interrupt": None, "max_nrhs": 8, "tuning": 0,
-    "schur_mode": 0, "user_schur_indices": None,
+    "schur_mode": 0, "user_schur_indices": None, "ubatch_mask": None,
 }
 
 
@@ -62,6 +62,17 @@ def _check(rc, lib):
 
 def _i32(a):
     return np.ascontiguousarray(a, dtype=np.int32)
+
+
+def active_members(nb, index, mask):
+    """The members (0-based) the next numeric or solve phase processes (active_members,
+    src/numeric/batch.jl:115-129): ``ubatch_index`` (-1 = all) and the 0/1 flags of ``ubatch_mask``
+    (None = all) together."""
+    if not (index == -1 or 0 <= index < nb):
+        raise InvalidValueError(f"ubatch_index = {index} is outside the batch (0:{nb - 1}, or -1 for all members)")
+    if mask is not None and len(mask) != nb:
+        raise InvalidValueError(f"ubatch_mask has {len(mask)} entries, the batch has {nb} members")
+    return [k for k in range(nb) if (index == -1 or k == index) and (mask is None or mask[k] != 0)]
 
 
 class DirectSolver:
@@ -161,8 +172,20 @@ class DirectSolver:
                 raise InvalidValueError(f"user_schur_indices has {value.size} entries, the matrix has {self.n} rows")
             if not np.all((value == 0) | (value == 1)):
                 raise InvalidValueError("user_schur_indices must hold flags 0 or 1")
-        if name == "ubatch_index" and self._plan_exists():
-            self._apply_members(int(value))
+        if name == "ubatch_mask" and value is not None:
+            value = np.asarray(value).reshape(-1)
+            if not np.all((value == 0) | (value == 1)):
+                raise InvalidValueError("ubatch_mask must hold flags 0 or 1")
+        if name in ("ubatch_index", "ubatch_mask"):
+            old = self.params[name]
+            self.params[name] = int(value) if name == "ubatch_index" else value
+            if self._plan_exists():
+                try:
+                    self._apply_members()
+                except Exception:
+                    self.params[name] = old
+                    raise
+            return
         self.params[name] = value
 
     def replan(self):
@@ -398,21 +421,29 @@ class DirectSolver:
         stream = self._torch.cuda.current_stream(self.device).cuda_stream
         _check(lib.sdsb200_plan_create(C.byref(plan), C.byref(sym), C.byref(po), C.c_void_p(stream)), lib)
         self._plan = plan
-        if int(self.params["ubatch_index"]) >= 0:
-            self._apply_members(int(self.params["ubatch_index"]))
+        if self._subset():
+            self._apply_members()
         if self.params["user_host_interrupt"] is not None:
             flag = self.params["user_host_interrupt"]
             lib.sdsb200_set_interrupt(self._plan, C.addressof(flag))
 
-    def _apply_members(self, index):
+    def _subset(self):
+        return int(self.params["ubatch_index"]) != -1 or self.params["ubatch_mask"] is not None
+
+    def _members(self):
+        return active_members(self.nbatch, int(self.params["ubatch_index"]), self.params["ubatch_mask"])
+
+    def _apply_members(self):
+        """set_members! (src/numeric/storage.jl:290-306) for ``ubatch_index`` and ``ubatch_mask``."""
         lib = numeric_lib()
-        if index < 0:
+        if not self._subset():
             _check(lib.sdsb200_set_members(self._plan, None, -1), lib)
-        else:
-            if index >= self.nbatch:
-                raise InvalidValueError(f"ubatch_index {index} outside 0:{self.nbatch - 1}")
-            m = np.array([index], np.int32)
-            _check(lib.sdsb200_set_members(self._plan, m.ctypes.data, 1), lib)
+            return
+        members = self._members()
+        if not members:
+            raise InvalidValueError("ubatch_index and ubatch_mask select no batch member")
+        m = np.asarray(members, np.int32)
+        _check(lib.sdsb200_set_members(self._plan, m.ctypes.data, len(members)), lib)
 
     def _factorize(self, refactor=False):
         if self._stage < 1:
@@ -440,10 +471,10 @@ class DirectSolver:
             raise FactorizationError("solve before factorization")
         lib = numeric_lib()
         n = self.n
-        vec = B.dim() == 1 if isinstance(B, torch.Tensor) else np.asarray(B).ndim == 1
         Bt = B if isinstance(B, torch.Tensor) else torch.from_numpy(np.asarray(B, dtype=np.float64))
         Bt = Bt.to(self.device, torch.float64)
-        Bm = Bt.reshape(n, -1) if vec or self.nbatch == 1 else Bt.reshape(self.nbatch, n, -1)
+        # a batch's right-hand sides are member after member, whatever the shape (a vector too)
+        Bm = Bt.reshape(n, -1) if self.nbatch == 1 else Bt.reshape(self.nbatch, n, -1)
         # column-major storage: (members, nrhs, n) contiguous
         if Bm.dim() == 2:
             Bcm = Bm.t().contiguous()
@@ -454,12 +485,13 @@ class DirectSolver:
         o = self._opts()
         if self._matching is not None:
             Bcm = self._scaled_rhs(Bcm, int(o.solve_mode))
-        Xcm = torch.empty_like(Bcm)
+        subset = self._subset() and self.nbatch > 1
+        Xcm = torch.zeros_like(Bcm) if subset else torch.empty_like(Bcm)
         fgmres = self.params["ir_mode"] == "fgmres" and o.ir_n_steps > 0
         if fgmres:
             # FGMRES-IR (fgmres_refine!, src/solve/refinement.jl:577-614): a plain solve, then the
             # Krylov refinement on the host above the C ABI
-            if int(self.params["ubatch_index"]) >= 0:
+            if self._subset():
                 raise NotSupportedError("ir_mode \"fgmres\" refines all batch members together")
             fg_steps, fg_tol = int(o.ir_n_steps), float(o.ir_tol)
             o.ir_n_steps = 0
@@ -478,6 +510,13 @@ class DirectSolver:
             Xcm = self._unscaled_solution(Xcm, int(o.solve_mode))
         out = Xcm.t() if Xcm.dim() == 2 else Xcm.transpose(1, 2)
         out = out.reshape(Bt.shape)
+        if X is not None and subset:
+            # ubatch_index / ubatch_mask: the other members' solutions in X are left as they are
+            Xt = X if isinstance(X, torch.Tensor) else torch.from_numpy(np.asarray(X, dtype=np.float64))
+            cur = Xt.to(self.device, torch.float64).reshape(self.nbatch, n, -1).clone()
+            sel = torch.as_tensor(self._members(), device=self.device, dtype=torch.int64)
+            cur[sel] = out.reshape(self.nbatch, n, -1)[sel]
+            out = cur.reshape(Bt.shape)
         if X is not None:
             if isinstance(X, torch.Tensor):
                 X.copy_(out)
@@ -494,8 +533,8 @@ class DirectSolver:
         Bt = B if isinstance(B, torch.Tensor) else torch.from_numpy(np.asarray(B, dtype=np.float64))
         Bt = Bt.to(self.device, torch.float64)
         n = self.n
-        vec = Bt.dim() == 1
-        Bm = Bt.reshape(n, -1) if vec or self.nbatch == 1 else Bt.reshape(self.nbatch, n, -1)
+        # a batch's right-hand sides are member after member, whatever the shape (a vector too)
+        Bm = Bt.reshape(n, -1) if self.nbatch == 1 else Bt.reshape(self.nbatch, n, -1)
         if Bm.dim() == 2:
             cm, nrhs = Bm.t().contiguous(), Bm.shape[1]
         else:
@@ -582,7 +621,7 @@ class DirectSolver:
         if nsteps <= 0:
             self._ir_steps = 0
             return X
-        if int(self.params["ubatch_index"]) >= 0:
+        if self._subset():
             raise NotSupportedError("\"solve_refinement\" refines all batch members together")
         Xcm, nrhs, back = self._colmajor(X)
         Bcm, nrhs_b, _ = self._colmajor(B)

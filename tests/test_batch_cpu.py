@@ -1,5 +1,7 @@
-"""Host logic of uneven batches (CPU): block-diagonal assembly, stacking and per-system errors."""
+"""Host logic of batches (CPU): block-diagonal assembly, stacking and per-system errors of uneven
+batches, and the active-member selection of uniform batches."""
 import numpy as np
+import pytest
 import scipy.sparse as sp
 import scipy.sparse.linalg as spla
 
@@ -26,3 +28,20 @@ def test_block_diagonal_and_per_system_errors():
     assert errs2[2] > 1e-3 and np.delete(errs2, 2).max() < 1e-14
     parts = ub.split(x)
     assert len(parts) == 6 and all(p.shape[0] == A.shape[0] for p, A in zip(parts, systems))
+
+
+def test_active_members_restates_the_reference():
+    """active_members (src/numeric/batch.jl:115-129): ubatch_index and ubatch_mask together."""
+    from sdsb200.solver import InvalidValueError, active_members
+
+    assert active_members(4, -1, None) == [0, 1, 2, 3]
+    assert active_members(4, 2, None) == [2]
+    assert active_members(4, -1, [1, 0, 1, 1]) == [0, 2, 3]
+    assert active_members(4, 2, [1, 0, 1, 1]) == [2]
+    assert active_members(4, 1, [1, 0, 1, 1]) == []
+    with pytest.raises(InvalidValueError):
+        active_members(4, 4, None)
+    with pytest.raises(InvalidValueError):
+        active_members(4, -2, None)
+    with pytest.raises(InvalidValueError):
+        active_members(4, -1, [1, 0, 1])
