@@ -692,7 +692,15 @@ SupernodePartition supernode_partition(const Pattern& P, const vector<int>& perm
                 int i = sp.rowval[p];
                 if (i > last && mark[i] != s) { mark[i] = s; below.push_back(i); }
             }
-        std::sort(below.begin(), below.end());
+        if ((i64)below.size() * 16 > (i64)(n - last)) {
+            // dense: the marked rows in increasing order (the rows of the top fronts, where a sort
+            // would cost |below| log |below| per front)
+            below.clear();
+            for (int i = last + 1; i <= n; ++i)
+                if (mark[i] == s) below.push_back(i);
+        } else {
+            std::sort(below.begin(), below.end());
+        }
         for (int j = first; j <= last; ++j) sp.rowval.push_back(j);
         sp.rowval.insert(sp.rowval.end(), below.begin(), below.end());
         sp.rowptr[s + 1] = (int)sp.rowval.size();
@@ -1132,6 +1140,7 @@ void build_maps(sdsa_result& R, const Csr& A, int structure, int view) {
     }
     i64 nnz = (i64)A.cv.size() - 1;
     R.amap.assign(nnz, 0);
+    vector<int> owner(nnz, 0);                 // the front of each kept entry (1-based), 0 = dropped
     bool neg = structure == SDSA_STRUCTURE_G;  // real element types: only "G" mirrors into Uᵀ
     for (int r = 1; r <= A.n; ++r)
         for (i64 p = A.rp[r]; p < A.rp[r + 1]; ++p) {
@@ -1148,32 +1157,35 @@ void build_maps(sdsa_result& R, const Csr& A, int structure, int view) {
             i64 f = re - rb;
             i64 off = R.panel_ptr[s - 1] + (i64)(j - sp.super_ptr[s]) * f + (q - rb);
             R.amap[p - 1] = (flip && neg) ? -off : off;
+            owner[p - 1] = s;
         }
-    // grouping: sorted by (|off|, off < 0 [G only], p)
-    vector<i64> order;
-    for (i64 p = 0; p < nnz; ++p)
-        if (R.amap[p] != 0) order.push_back(p);
-    bool signed_ = structure == SDSA_STRUCTURE_G;
-    std::stable_sort(order.begin(), order.end(), [&](i64 a, i64 b) {
-        i64 oa = std::llabs(R.amap[a]), ob = std::llabs(R.amap[b]);
-        if (oa != ob) return oa < ob;
-        if (signed_) {
-            bool na = R.amap[a] < 0, nb = R.amap[b] < 0;
-            if (na != nb) return !na;
-        }
-        return a < b;
-    });
+    // grouping: the kept entries ordered by (|off|, off < 0 [G only], p). The fronts own disjoint,
+    // increasing ranges of offsets, so the entries are bucketed by front (a counting sort, in p order)
+    // and each front's bucket is sorted by that key: the same strict order as one sort of all entries.
+    vector<i64> cnt(ns + 1, 0);
+    for (i64 p = 0; p < nnz; ++p) cnt[owner[p]]++;
     R.amap_ptr.assign(ns + 1, 0);
     R.amap_ptr[0] = 1;
-    vector<i64> cnt(ns + 1, 0);
-    for (i64 p : order) {
-        i64 off = std::llabs(R.amap[p]);
-        int s = (int)(std::upper_bound(R.panel_ptr.begin(), R.panel_ptr.end(), off) - R.panel_ptr.begin());
-        cnt[s]++;
-    }
     for (int s = 1; s <= ns; ++s) R.amap_ptr[s] = R.amap_ptr[s - 1] + cnt[s];
-    R.amap_src.resize(order.size());
-    for (size_t k = 0; k < order.size(); ++k) R.amap_src[k] = order[k] + 1;
+    R.amap_src.assign(R.amap_ptr[ns] - 1, 0);
+    {
+        vector<i64> next(R.amap_ptr.begin(), R.amap_ptr.end() - 1);
+        for (i64 p = 0; p < nnz; ++p)
+            if (owner[p]) R.amap_src[next[owner[p] - 1]++ - 1] = p;
+    }
+    bool signed_ = structure == SDSA_STRUCTURE_G;
+    for (int s = 1; s <= ns; ++s)
+        std::sort(R.amap_src.begin() + (R.amap_ptr[s - 1] - 1), R.amap_src.begin() + (R.amap_ptr[s] - 1),
+                  [&](i64 a, i64 b) {
+                      i64 oa = std::llabs(R.amap[a]), ob = std::llabs(R.amap[b]);
+                      if (oa != ob) return oa < ob;
+                      if (signed_) {
+                          bool na = R.amap[a] < 0, nb = R.amap[b] < 0;
+                          if (na != nb) return !na;
+                      }
+                      return a < b;
+                  });
+    for (i64& q : R.amap_src) q += 1;
     // children in increasing id (maps.jl:209-223)
     R.child_ptr.assign(ns + 1, 0);
     R.child_ptr[0] = 1;
@@ -1190,39 +1202,60 @@ void build_maps(sdsa_result& R, const Csr& A, int structure, int view) {
         next[p - 1]++;
     }
     // relative indices (maps.jl:110-132)
+    // (each parent's row positions are tabulated once and read by all of its children)
     R.relind_ptr.assign(ns + 1, 0);
     R.relind_ptr[0] = 1;
-    R.relind.clear();
-    for (int c = 1; c <= ns; ++c) {
-        int p = sp.snparent[c];
-        if (p != 0) {
-            const int* prow = sp.rowval.data() + sp.rowptr[p];
-            int plen = sp.nrows(p);
-            int k = 0;
-            for (int q = sp.rowptr[c] + sp.width(c); q < sp.rowptr[c + 1]; ++q) {
-                int i = sp.rowval[q];
-                while (k < plen && prow[k] < i) ++k;
-                if (!(k < plen && prow[k] == i)) throw AnalysisError("row missing from the parent");
-                R.relind.push_back(k + 1);
+    for (int c = 1; c <= ns; ++c)
+        R.relind_ptr[c] = R.relind_ptr[c - 1] + (sp.snparent[c] != 0 ? sp.nrows(c) - sp.width(c) : 0);
+    R.relind.assign(R.relind_ptr[ns] - 1, 0);
+    {
+        vector<int> at(sp.n + 1, 0), stamp(sp.n + 1, 0);
+        for (int p = 1; p <= ns; ++p) {
+            if (R.child_ptr[p] == R.child_ptr[p - 1]) continue;
+            for (int k = 0, q = sp.rowptr[p]; q < sp.rowptr[p + 1]; ++q, ++k) {
+                at[sp.rowval[q]] = k;
+                stamp[sp.rowval[q]] = p;
+            }
+            for (i64 t = R.child_ptr[p - 1]; t < R.child_ptr[p]; ++t) {
+                const int c = (int)R.child_list[t - 1];
+                i64 o = R.relind_ptr[c - 1] - 1;
+                for (int q = sp.rowptr[c] + sp.width(c); q < sp.rowptr[c + 1]; ++q) {
+                    const int i = sp.rowval[q];
+                    if (stamp[i] != p) throw AnalysisError("row missing from the parent");
+                    R.relind[o++] = at[i] + 1;
+                }
             }
         }
-        R.relind_ptr[c] = (i64)R.relind.size() + 1;
     }
     // full-pattern map of the residual (src/symbolic/pattern.jl:249-290)
+    // the contributions (r, c, p) ordered by (r, c, p): bucketed by row (a counting sort), then each
+    // row's few entries sorted by (c, p), the same strict order as one sort of all of them
     struct Contrib { i64 r, c, p; char cj; };
-    vector<Contrib> con;
+    vector<i64> rstart(A.n + 2, 0);
     for (int r = 1; r <= A.n; ++r)
         for (i64 p = A.rp[r]; p < A.rp[r + 1]; ++p) {
             int c = (int)A.cv[p];
             if (!keep_entry(structure, view, r, c)) continue;
-            con.push_back({r, c, p, 0});
-            if (structure != SDSA_STRUCTURE_G && r != c) con.push_back({c, r, p, 0});
+            rstart[r + 1]++;
+            if (structure != SDSA_STRUCTURE_G && r != c) rstart[c + 1]++;
         }
-    std::sort(con.begin(), con.end(), [](const Contrib& a, const Contrib& b) {
-        if (a.r != b.r) return a.r < b.r;
-        if (a.c != b.c) return a.c < b.c;
-        return a.p < b.p;
-    });
+    for (int r = 1; r <= A.n; ++r) rstart[r + 1] += rstart[r];
+    vector<Contrib> con(rstart[A.n + 1]);
+    {
+        vector<i64> next(rstart.begin(), rstart.end());
+        for (int r = 1; r <= A.n; ++r)
+            for (i64 p = A.rp[r]; p < A.rp[r + 1]; ++p) {
+                int c = (int)A.cv[p];
+                if (!keep_entry(structure, view, r, c)) continue;
+                con[next[r]++] = {r, c, p, 0};
+                if (structure != SDSA_STRUCTURE_G && r != c) con[next[c]++] = {c, r, p, 0};
+            }
+    }
+    for (int r = 1; r <= A.n; ++r)
+        std::sort(con.begin() + rstart[r], con.begin() + rstart[r + 1], [](const Contrib& a, const Contrib& b) {
+            if (a.c != b.c) return a.c < b.c;
+            return a.p < b.p;
+        });
     R.full_rowptr.assign(A.n + 1, 0);
     R.full_colval.clear();
     R.full_srcptr.assign(1, 1);
