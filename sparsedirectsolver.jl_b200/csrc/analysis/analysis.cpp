@@ -17,7 +17,6 @@
 #include <memory>
 #include <tuple>
 #include <numeric>
-#include <set>
 #include <stdexcept>
 #include <string>
 #include <unordered_map>
@@ -131,19 +130,41 @@ vector<int> amd_order0(int n, const vector<vector<int>>& adj) {
     vector<i64> esize(n, 0), w(n, 0);
     vector<int> wflag(n, 0), mark(n, 0);
     int stamp = 0, wstamp = 0;
-    std::set<std::pair<int, int>> heap;
+    // the variables by (degree, index): a binary min-heap whose entries carry the variable's version;
+    // an erase bumps the version, so stale entries are skipped when they surface, and the entry taken
+    // is always the least (degree, index) among the variables present, as an ordered set would give
+    struct Entry { int d, i, ver; };
+    auto later = [](const Entry& a, const Entry& b) { return a.d != b.d ? a.d > b.d : a.i > b.i; };
+    vector<Entry> heap;
+    heap.reserve(4 * (size_t)n + 16);
+    vector<int> ver(n, 0);
+    vector<char> present(n, 0);
+    auto push = [&](int i) {
+        present[i] = 1;
+        heap.push_back({deg[i], i, ++ver[i]});
+        std::push_heap(heap.begin(), heap.end(), later);
+    };
+    auto erase = [&](int i) { present[i] = 0; ++ver[i]; };
     for (int i = 0; i < n; ++i) {
         members[i].push_back(i);
         deg[i] = (int)A[i].size();
-        heap.insert({deg[i], i});
+        push(i);
     }
     vector<int> order;
     order.reserve(n);
     int nelim = 0;
-    vector<int> Lp;
-    while (!heap.empty()) {
-        int p = heap.begin()->second;
-        heap.erase(heap.begin());
+    vector<int> Lp, g;
+    vector<std::pair<i64, int>> hashed;
+    while (true) {
+        while (!heap.empty() && !(present[heap.front().i] && heap.front().ver == ver[heap.front().i])) {
+            std::pop_heap(heap.begin(), heap.end(), later);
+            heap.pop_back();
+        }
+        if (heap.empty()) break;
+        int p = heap.front().i;
+        std::pop_heap(heap.begin(), heap.end(), later);
+        heap.pop_back();
+        erase(p);
         ++stamp;
         mark[p] = stamp;
         Lp.clear();
@@ -163,7 +184,7 @@ vector<int> amd_order0(int n, const vector<vector<int>>& adj) {
         vector<int>().swap(A[p]);
         vector<int>().swap(E[p]);
         i64 lpw = 0;
-        for (int v : Lp) { lpw += nv[v]; heap.erase({deg[v], v}); }
+        for (int v : Lp) { lpw += nv[v]; erase(v); }
         L[p] = Lp;
         esize[p] = lpw;
         // |L_e \ L_p| for the elements adjacent to L_p
@@ -205,15 +226,22 @@ vector<int> amd_order0(int n, const vector<vector<int>>& adj) {
         }
         // supervariables: identical element and variable lists
         if (Lp.size() > 1) {
-            std::unordered_map<i64, vector<int>> buckets;
+            // hash groups (each in Lp order; the groups are disjoint, so their order is immaterial)
+            hashed.clear();
             for (int i : Lp) {
                 i64 h = 0;
                 for (int e : E[i]) h += e;
                 for (int v : A[i]) h += v;
-                buckets[h].push_back(i);
+                hashed.push_back({h, i});
             }
-            for (auto& kv : buckets) {
-                vector<int>& g = kv.second;
+            std::stable_sort(hashed.begin(), hashed.end(),
+                             [](const std::pair<i64, int>& a, const std::pair<i64, int>& b) { return a.first < b.first; });
+            for (size_t g0 = 0; g0 < hashed.size();) {
+                size_t g1 = g0 + 1;
+                while (g1 < hashed.size() && hashed[g1].first == hashed[g0].first) ++g1;
+                g.clear();
+                for (size_t t = g0; t < g1; ++t) g.push_back(hashed[t].second);
+                g0 = g1;
                 if (g.size() < 2) continue;
                 for (size_t a = 0; a < g.size(); ++a) {
                     int i = g[a];
@@ -241,7 +269,7 @@ vector<int> amd_order0(int n, const vector<vector<int>>& adj) {
             }
         }
         for (int i : Lp)
-            if (status[i] == 0) heap.insert({deg[i], i});
+            if (status[i] == 0) push(i);
     }
     return order;
 }
