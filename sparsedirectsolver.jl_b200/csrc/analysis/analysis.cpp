@@ -819,39 +819,46 @@ vector<IPair> all_pivot_pairs(const Pattern& P, const PairCandidates& cands) {
 
 vector<int> structural_zero_pivots(const PairCandidates& cands, const Pattern& P, const vector<int>& perm,
                                    const vector<IPair>& pairs) {
-    int n = P.n;
-    vector<int> pos = invperm(perm), mate(n + 1, 0), colm(n + 1, 0), seen(n + 1, 0);
+    // The search runs in elimination positions. Each row's edges with a nonzero value come in the
+    // row's own order, with the diagonal of a non-candidate last, every column replaced by its
+    // position. The depth-first order is the reference's, and so is every augmenting path and every
+    // failure; a column's test is then one comparison with k and one seen mark.
+    const int n = P.n;
+    vector<int> pos = invperm(perm), mate(n + 1, 0);
     for (auto& ab : pairs) { mate[ab.first] = ab.second; mate[ab.second] = ab.first; }
-    vector<int> srow, sptr, scol, out;
+    vector<int> aptr(n + 2, 0), adj;
+    adj.reserve(P.rowval.size());
     for (int k = 1; k <= n; ++k) {
-        int v = perm[k], m = mate[v];
-        if (m != 0 && pos[m] == k - 1) { colm[v] = m; colm[m] = v; continue; }
-        if (!cands.candidate[v] || m != 0) { colm[v] = v; continue; }
-        srow.assign(1, v); sptr.assign(1, P.colptr[v]); scol.assign(1, 0);
+        const int r = perm[k];
+        aptr[k] = (int)adj.size();
+        for (int p = P.colptr[r]; p < P.colptr[r + 1]; ++p)
+            if (cands.w[p] > 0) adj.push_back(pos[P.rowval[p]]);
+        if (!cands.candidate[r]) adj.push_back(k);
+    }
+    aptr[n + 1] = (int)adj.size();
+    vector<int> colm(n + 1, 0), seen(n + 1, 0), srow, sptr, scol, out;
+    for (int k = 1; k <= n; ++k) {
+        const int v = perm[k], m = mate[v];
+        if (m != 0 && pos[m] == k - 1) { colm[k] = k - 1; colm[k - 1] = k; continue; }
+        if (!cands.candidate[v] || m != 0) { colm[k] = k; continue; }
+        srow.assign(1, k); sptr.assign(1, aptr[k]); scol.assign(1, 0);
         bool found = false;
         while (!srow.empty()) {
-            int r = srow.back(), p = sptr.back();
-            if (p > P.colptr[r + 1]) { srow.pop_back(); sptr.pop_back(); scol.pop_back(); continue; }
-            sptr.back() = p + 1;
-            int j;
-            if (p == P.colptr[r + 1]) {
-                if (cands.candidate[r]) continue;
-                j = r;
-            } else {
-                j = P.rowval[p];
-                if (!(cands.w[p] > 0)) continue;
-            }
-            if (!(pos[j] <= k && seen[j] != k)) continue;
+            const int r = srow.back(), q = sptr.back();
+            if (q >= aptr[r + 1]) { srow.pop_back(); sptr.pop_back(); scol.pop_back(); continue; }
+            sptr.back() = q + 1;
+            const int j = adj[q];
+            if (!(j <= k && seen[j] != k)) continue;
             seen[j] = k;
             scol.back() = j;
-            if (j == v) {
+            if (j == k) {
                 for (size_t t = 0; t < srow.size(); ++t) colm[scol[t]] = srow[t];
                 found = true;
                 break;
             }
-            srow.push_back(colm[j]); sptr.push_back(P.colptr[colm[j]]); scol.push_back(0);
+            srow.push_back(colm[j]); sptr.push_back(aptr[colm[j]]); scol.push_back(0);
         }
-        if (!found) { out.push_back(v); colm[v] = v; }
+        if (!found) { out.push_back(v); colm[k] = k; }
     }
     return out;
 }
