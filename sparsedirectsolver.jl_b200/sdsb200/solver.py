@@ -64,6 +64,30 @@ def _i32(a):
     return np.ascontiguousarray(a, dtype=np.int32)
 
 
+def memory_slots(structure, n, ns, nbatch, elsize, factor_len, cb_len, device_bytes, host_bytes, extra_device=0):
+    """``getparam("memory_estimates")`` (memory_estimates, src/symbolic/maps.jl:307-356): 16 byte counts in
+    cuDSS's slot layout, from a plan that allocates every buffer when it is built:
+      1 permanent device memory (every buffer but the update stack; plus ``extra_device``, the matching's
+        buffers), 2 peak device memory (slot 1 + the update stack), 3 and 4 host memory (the Symbolic
+        maps), 5 = slot 2, 6 = 0 (no hybrid memory mode);
+      7 factor panels (L and U^T for "G"), 8 D (2n doubles), 9 the update stack (the contribution-block
+        arena), 11 per-front statistics, status, pivot order, kinds and sign requests, 10 the rest of the
+        plan's buffers (device maps, launch lists, solve and refinement workspaces);
+      12-16 = 0."""
+    nb = int(nbatch)
+    est = [0] * 16
+    est[6] = (2 if structure == "G" else 1) * int(factor_len) * int(elsize) * nb
+    est[7] = 2 * int(n) * 8 * nb
+    est[8] = int(cb_len) * int(elsize) * nb
+    est[10] = (6 * int(ns) * 8 + int(ns) * 4 + 6 * 8 + 8 + int(n) * 4 + int(n)) * nb + int(n) + 8
+    est[9] = max(int(device_bytes) - est[6] - est[7] - est[8] - est[10], 0)
+    est[1] = int(device_bytes) + int(extra_device)
+    est[0] = est[1] - est[8]
+    est[2] = est[3] = int(host_bytes)
+    est[4] = est[1]
+    return est
+
+
 def active_members(nb, index, mask):
     """The members (0-based) the next numeric or solve phase processes (active_members,
     src/numeric/batch.jl:115-129): ``ubatch_index`` (-1 = all) and the 0/1 flags of ``ubatch_mask``
@@ -299,6 +323,18 @@ class DirectSolver:
         if name == "diag":
             self._need(2, name)
             return self.factor_diag()
+        if name == "memory_estimates":
+            self._need(1, name)
+            st = lambda k: int(lib.sdsb200_plan_stat(self._plan, k.encode()))  # noqa: E731
+            host = sum(int(a.nbytes) for a in self.symbolic.maps.values())
+            extra = 0
+            if self._mdev is not None:
+                extra = sum(int(t.numel() * t.element_size()) for t in self._mdev.values()
+                            if isinstance(t, self._torch.Tensor) and t.is_cuda)
+                extra += self.nnz * self.nbatch * 8          # the scaled values
+            es = 4 if self._precision() == 1 else 8
+            return memory_slots(self.structure, self.n, self.symbolic.ns, self.nbatch, es, st("factor_len"),
+                                st("cb_len"), st("device_bytes"), host, extra)
         if name in ("schur_shape", "schur_matrix"):
             self._need(1 if name == "schur_shape" else 2, name)
             if self.symbolic.schur == 0:

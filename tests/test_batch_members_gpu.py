@@ -57,6 +57,9 @@ def test_ubatch_mask_refactor_and_solve(torch_cuda):
     with pytest.raises(InvalidValueError):
         ds.setparam("ubatch_mask", [0] * nb)
     assert ds.getparam("ubatch_mask") is None
+    # memory_estimates: the plan's buffers in the reference's slots (every member's panels in slot 7)
+    est = ds.getparam("memory_estimates")
+    assert len(est) == 16 and est[1] >= est[0] > 0 and est[6] >= nb * 8 * A.nnz // 2
     # a vector right-hand side of a batch is member after member
     xv = ds.execute("solve", None, b.reshape(-1)).cpu().numpy()
     assert np.array_equal(xv.reshape(nb, n), x)
