@@ -160,3 +160,23 @@ def test_golden_fixtures():
         else:
             assert list(O.kind[:n]) == c["kind"]
             assert np.allclose(O.d[: 2 * n], np.array(c["d"]), rtol=1e-13, atol=1e-14)
+
+
+@pytest.mark.parametrize("structure", ["SPD", "S", "G"])
+def test_edge_cases_small_and_empty(structure):
+    """The smallest inputs the reference's tests use: n = 0, n = 1, a diagonal matrix (every front a
+    single column), and a structurally empty row. The empty row meets the static pivot of the SPD clamp
+    (0 <= a_jj accepted as eps = 1e-13, src/numeric/front.jl:38-53) and the LDLT/LU perturbation to
+    eps, so its unknown is b / eps."""
+    from sdsb200 import analyze_csr
+
+    S = analyze_csr(sp.csr_matrix((0, 0)), structure)
+    assert S.n == 0 and S.ns == 0
+    for A, x_expected in ((sp.csr_matrix(np.array([[4.0]])), [0.25]),
+                          (sp.diags(np.arange(1.0, 6.0)).tocsr(), 1.0 / np.arange(1.0, 6.0)),
+                          (sp.csr_matrix(np.array([[2.0, 0.0], [0.0, 0.0]])), [0.5, 1e13])):
+        S, O, info = oracle_for(A, structure)
+        assert info == 0
+        assert S.ns == A.shape[0]
+        x = O.solve(np.ones(A.shape[0]))
+        assert np.allclose(x, x_expected, rtol=1e-12)
