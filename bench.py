@@ -484,7 +484,9 @@ def main():
             ds._stage = 1
             ds.replan()
         else:
+            t_an = time.perf_counter()
             ds.execute("analysis")
+            analysis_s = time.perf_counter() - t_an
         # front tile shapes picked by the autotuner (outside the timed region, like the analysis)
         if args.tuning:
             from sdsb200.capi import tuning as make_tuning
@@ -671,6 +673,7 @@ def main():
                  "bwd_err": results["fp64"]["berr"], "unit": "GFLOP/s",
                  "speedup_mixed_vs_fp64": round(results["fp64"]["ms"] / r["ms"], 3)},
         "tuning": tuned,
+        "analysis_s": round(analysis_s, 3),
         "gpu_launches": int(r["launches"]),
         "clocks": r["clocks"],
         "roofline": roofline,
