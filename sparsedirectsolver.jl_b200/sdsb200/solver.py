@@ -547,12 +547,7 @@ class DirectSolver:
         out = Xcm.t() if Xcm.dim() == 2 else Xcm.transpose(1, 2)
         out = out.reshape(Bt.shape)
         if X is not None and subset:
-            # ubatch_index / ubatch_mask: the other members' solutions in X are left as they are
-            Xt = X if isinstance(X, torch.Tensor) else torch.from_numpy(np.asarray(X, dtype=np.float64))
-            cur = Xt.to(self.device, torch.float64).reshape(self.nbatch, n, -1).clone()
-            sel = torch.as_tensor(self._members(), device=self.device, dtype=torch.int64)
-            cur[sel] = out.reshape(self.nbatch, n, -1)[sel]
-            out = cur.reshape(Bt.shape)
+            out = self._keep_inactive(X, out)
         if X is not None:
             if isinstance(X, torch.Tensor):
                 X.copy_(out)
@@ -582,6 +577,16 @@ class DirectSolver:
             return out.reshape(shape)
 
         return cm, int(nrhs), back
+
+    def _keep_inactive(self, X, out):
+        """``out`` with the inactive batch members' entries taken from X (ubatch_index / ubatch_mask: the other
+        members' solutions are left as they are)."""
+        torch = self._torch
+        Xt = X if isinstance(X, torch.Tensor) else torch.from_numpy(np.asarray(X, dtype=np.float64))
+        cur = Xt.to(self.device, torch.float64).reshape(self.nbatch, self.n, -1).clone()
+        sel = torch.as_tensor(self._members(), device=self.device, dtype=torch.int64)
+        cur[sel] = out.reshape(self.nbatch, self.n, -1)[sel]
+        return cur.reshape(out.shape)
 
     def _deliver(self, X, out):
         if X is None:
@@ -637,7 +642,10 @@ class DirectSolver:
         self._run_phase("bwd_perm", Xcm, None, nrhs, o)
         if self._matching is not None:
             Xcm = self._unscaled_solution(Xcm, int(o.solve_mode))
-        return self._deliver(X, back(Xcm))
+        out = back(Xcm)
+        if X is not None and self._subset() and self.nbatch > 1:
+            out = self._keep_inactive(X, out)
+        return self._deliver(X, out)
 
     def _refine(self, X, B):
         """``execute!("solve_refinement", X, B)`` (_refine_phase!, src/solver.jl:902-926): refine the given
