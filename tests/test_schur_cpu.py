@@ -144,3 +144,59 @@ def test_oracle_schur_complement(structure, k):
         ev = np.linalg.eigvalsh(A.toarray()[np.ix_(rest, rest)])
         tot = st.sum(0)
         assert (tot[0], tot[1]) == (int((ev > 0).sum()), int((ev < 0).sum()))
+
+
+@pytest.mark.parametrize("variant", ["amd", "nd", "natural", "user_perm", "no_amalgamation"])
+def test_schur_forest_of_two_blocks(variant):
+    """As the reference's Schur edge-case test (test/test_schur.jl:186-210): two disconnected blocks with the
+    Schur indices in the second one only, so the first block is a tree of its own."""
+    A = sp.block_diag([M.laplacian2d(6, 6), M.laplacian2d(7, 5)]).tocsr()
+    A.sort_indices()
+    n = A.shape[0]
+    fl = np.zeros(n, np.int8)
+    fl[np.array([40, 45, 50, 55, 60, 70]) - 1] = 1
+    kw = {"amd": dict(reordering="amd"), "nd": dict(reordering="nd"), "natural": dict(reordering="natural"),
+          "user_perm": dict(user_perm=np.random.default_rng(1).permutation(n) + 1),
+          "no_amalgamation": dict(use_superpanels=0)}[variant]
+    S, O, info = oracle_for(A, "SPD", user_schur_indices=fl, **kw)
+    assert info == 0
+    assert np.array_equal(S.perm[n - 6:], np.flatnonzero(fl) + 1)
+    assert (S.snparent == 0).sum() >= 2                       # the first block's root besides the Schur root
+    Sd = dense_schur(A, fl)
+    assert np.abs(oracle_schur(S, O, "SPD") - Sd).max() <= 1e-12 * np.abs(Sd).max()
+    rows = np.repeat(np.arange(6), np.diff(S.schur_rowptr))
+    lower = int(np.count_nonzero(S.schur_colval - 1 <= rows))
+    assert lower == int(np.count_nonzero(np.tril(np.abs(Sd) > 1e-13)))
+
+
+def test_schur_shape_of_a_corner():
+    """The first four indices of a 6 x 6 Laplacian: S is dense, 4 x 4 with 10 lower entries
+    (test/test_schur.jl:238)."""
+    A = sp.tril(M.laplacian2d(6, 6)).tocsr()
+    fl = np.zeros(36, np.int8)
+    fl[:4] = 1
+    S = analyze_csr(A, "SPD", view="L", user_schur_indices=fl)
+    rows = np.repeat(np.arange(4), np.diff(S.schur_rowptr))
+    assert S.schur_n == 4 and int(np.count_nonzero(S.schur_colval - 1 <= rows)) == 10
+
+
+def test_schur_directsolver_errors():
+    """DirectSolver refuses Schur mode without indices, with an empty set, and for a uniform batch, before
+    any device work (device="cpu": these checks precede the analysis)."""
+    torch = pytest.importorskip("torch")  # noqa: F841
+    from sdsb200.solver import DirectSolver, InvalidValueError, NotSupportedError
+
+    A = M.lap2d_shifted(6, 6)
+    for ind in (None, np.zeros(36)):
+        ds = DirectSolver(A, "SPD", device="cpu", schur_mode=1)
+        if ind is not None:
+            ds.setparam("user_schur_indices", ind)
+        with pytest.raises(InvalidValueError):
+            ds.execute("analysis")
+    with pytest.raises(InvalidValueError):
+        DirectSolver(A, "SPD", device="cpu", user_schur_indices=np.ones(35))
+    vals = np.concatenate([A.data, 2 * A.data])
+    batch = DirectSolver((A.indptr, A.indices, vals, 36), "SPD", device="cpu", schur_mode=1,
+                         user_schur_indices=np.eye(1, 36, 0).ravel())
+    with pytest.raises(NotSupportedError):
+        batch.execute("analysis")
