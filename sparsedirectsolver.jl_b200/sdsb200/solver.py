@@ -201,14 +201,9 @@ class DirectSolver:
             if not np.all((value == 0) | (value == 1)):
                 raise InvalidValueError("ubatch_mask must hold flags 0 or 1")
         if name in ("ubatch_index", "ubatch_mask"):
-            old = self.params[name]
+            # checked against the batch by the next factorization or solve, as the reference's _set_members!
             self.params[name] = int(value) if name == "ubatch_index" else value
-            if self._plan_exists():
-                try:
-                    self._apply_members()
-                except Exception:
-                    self.params[name] = old
-                    raise
+            self._members_dirty = True
             return
         self.params[name] = value
 
@@ -360,6 +355,7 @@ class DirectSolver:
                      "solve_bwd_perm", "solve_fwd_schur", "solve_bwd_schur"):
             if self._stage < 2:
                 raise FactorizationError(f"phase {phase!r} before the factorization")
+            self._sync_members()
             if self.symbolic.schur > 0:
                 return self._schur_phase(phase, X, B)
             if phase in ("solve_fwd_schur", "solve_bwd_schur"):
@@ -457,8 +453,7 @@ class DirectSolver:
         stream = self._torch.cuda.current_stream(self.device).cuda_stream
         _check(lib.sdsb200_plan_create(C.byref(plan), C.byref(sym), C.byref(po), C.c_void_p(stream)), lib)
         self._plan = plan
-        if self._subset():
-            self._apply_members()
+        self._members_dirty = self._subset()     # a new plan processes every member
         if self.params["user_host_interrupt"] is not None:
             flag = self.params["user_host_interrupt"]
             lib.sdsb200_set_interrupt(self._plan, C.addressof(flag))
@@ -468,6 +463,14 @@ class DirectSolver:
 
     def _members(self):
         return active_members(self.nbatch, int(self.params["ubatch_index"]), self.params["ubatch_mask"])
+
+    def _sync_members(self):
+        """The members of the next numeric or solve phase (_set_members!, src/solver.jl:694-705), sent to the
+        plan when ubatch_index or ubatch_mask changed; InvalidValueError for a selection outside the batch
+        or an empty one."""
+        if self._plan_exists() and getattr(self, "_members_dirty", False):
+            self._apply_members()
+            self._members_dirty = False
 
     def _apply_members(self):
         """set_members! (src/numeric/storage.jl:290-306) for ``ubatch_index`` and ``ubatch_mask``."""
@@ -484,6 +487,7 @@ class DirectSolver:
     def _factorize(self, refactor=False):
         if self._stage < 1:
             raise FactorizationError("factorization before analysis")
+        self._sync_members()
         lib = numeric_lib()
         ps = self.params["pivot_sign"]
         ps_arr = None if ps is None else np.ascontiguousarray(ps, dtype=np.int8)

@@ -47,15 +47,29 @@ def test_ubatch_mask_refactor_and_solve(torch_cuda):
             assert M.scaled_backward_error(Ak, X[k].reshape(n, 1), b[k].reshape(n, 1)) <= BERR
         else:
             assert np.all(X[k] == 7.0)                     # an inactive member's solution: untouched
+    # ubatch_index and ubatch_mask together: their intersection (member 4)
+    ds.setparam("ubatch_index", 4)
+    X = np.full((nb, n), 7.0)
+    ds.execute("solve", X, b)
+    assert np.all(X[:4] == 7.0) and not np.any(X[4] == 7.0)
+    ds.setparam("ubatch_index", -1)
     # all members again: the inactive ones kept their old factors
     ds.setparam("ubatch_mask", None)
     x = ds.execute("solve", None, b).cpu().numpy()
     for k in (1, 3):
         assert np.array_equal(x[k], x_all[k])
+    # a mask or an index outside the batch, or an empty selection: an error at the next phase
+    ds.setparam("ubatch_mask", [1, 0, 1])
     with pytest.raises(InvalidValueError):
-        ds.setparam("ubatch_mask", [1, 0, 1])
+        ds.execute("refactorization")
+    ds.setparam("ubatch_mask", [0] * nb)
     with pytest.raises(InvalidValueError):
-        ds.setparam("ubatch_mask", [0] * nb)
+        ds.execute("solve", None, b)
+    ds.setparam("ubatch_mask", None)
+    ds.setparam("ubatch_index", nb)
+    with pytest.raises(InvalidValueError):
+        ds.execute("refactorization")
+    ds.setparam("ubatch_index", -1)
     assert ds.getparam("ubatch_mask") is None
     # memory_estimates: the plan's buffers in the reference's slots (every member's panels in slot 7)
     est = ds.getparam("memory_estimates")

@@ -65,3 +65,27 @@ def test_schur_parameter_checks():
     assert ds.getparam("schur_mode") == 1
     with pytest.raises(InvalidValueError):
         ds.setparam("schur_matrix", None)                       # no analysis with schur_mode = 1 yet
+
+
+def test_member_selection_checked_at_the_next_phase():
+    """As the reference's _set_members!: setparam stores ubatch_index / ubatch_mask as given, and the next
+    factorization or solve raises InvalidValueError for a selection outside the batch or an empty one.
+    A stand-in plan handle is enough here: the selection is checked before any call into the library."""
+    import ctypes
+
+    ds, n = _batch(4)
+    ds.setparam("ubatch_index", 4)                              # outside 0:3, stored
+    assert ds.getparam("ubatch_index") == 4
+    ds._plan = ctypes.c_void_p(1)
+    try:
+        with pytest.raises(InvalidValueError):
+            ds._sync_members()
+        ds.setparam("ubatch_index", -1)
+        ds.setparam("ubatch_mask", [0, 0, 0, 0])
+        with pytest.raises(InvalidValueError):
+            ds._sync_members()
+        ds.setparam("ubatch_mask", [1, 0])
+        with pytest.raises(InvalidValueError):
+            ds._sync_members()
+    finally:
+        ds._plan = None
