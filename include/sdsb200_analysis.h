@@ -78,7 +78,9 @@ int sdsa_analyze(int64_t n, const int64_t* rowptr, const int64_t* colval, const 
  * pairs (2*npairs: partner, candidate)
  * full_rowptr full_colval full_srcptr full_src full_conj  (residual map of the full matrix)
  * schur_rowptr schur_colval  (Schur complement mode: 1-based CSR pattern of S over the Schur indices in
- *                            increasing order, both triangles and the whole diagonal) */
+ *                            increasing order, both triangles and the whole diagonal)
+ * ordering  (n: the ordering algorithm's permutation before the supernodal renumbering; `perm` is the
+ *           factor's, the two composed, src/solver.jl:1082-1085) */
 int64_t sdsa_len(const sdsa_result* r, const char* name);
 int sdsa_get(const sdsa_result* r, const char* name, int64_t* out);
 

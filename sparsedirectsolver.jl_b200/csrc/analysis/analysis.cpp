@@ -1155,6 +1155,8 @@ struct sdsa_result {
     vector<i64> full_rowptr, full_colval, full_srcptr, full_src, full_conj;
     int schur = 0;       // Schur complement mode: the root supernode (1-based), 0 = off
     vector<i64> schur_rowptr, schur_colval;
+    vector<int> ordering;  // the ordering algorithm's permutation (1-based, slot 0 unused), before the
+                           // supernodal renumbering that `perm` composes with it
 };
 
 namespace {
@@ -1834,6 +1836,7 @@ int sdsa_analyze(int64_t n, const int64_t* rowptr, const int64_t* colval, const 
             chosen = cands_o[best];
         }
         R->alg_used = chosen.alg;
+        R->ordering = chosen.perm;
         R->pairs = chosen.pairs;
         R->pair_rounds = chosen.rounds;
         Pattern F = pair_pattern(P, chosen.pairs);
@@ -1869,6 +1872,7 @@ static const vector<int>* int_field(const sdsa_result* r, const std::string& nm,
     if (nm == "snpost") return &sp.snpost;
     if (nm == "rowptr") return &sp.rowptr;
     if (nm == "rowval") return &sp.rowval;
+    if (nm == "ordering") return &r->ordering;
     return nullptr;
 }
 

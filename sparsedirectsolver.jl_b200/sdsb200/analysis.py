@@ -22,7 +22,7 @@ PAIRS = {"none": 0, "default": 1, "all": 2}
 MAP_NAMES = ("perm", "iperm", "super_ptr", "snparent", "snpost", "rowptr", "rowval", "front_ptr", "front_nrows",
              "front_ncols", "child_ptr", "child_list", "relind_ptr", "relind", "amap", "amap_ptr", "amap_src",
              "counts", "pairs", "full_rowptr", "full_colval", "full_srcptr", "full_src", "full_conj",
-             "schur_rowptr", "schur_colval")
+             "schur_rowptr", "schur_colval", "ordering")
 
 
 class _Opts(C.Structure):

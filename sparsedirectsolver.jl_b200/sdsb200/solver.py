@@ -289,6 +289,9 @@ class DirectSolver:
                 raise InvalidValueError(f"{name!r} needs matching_alg other than \"default\"")
             m = self._matching
             return {"perm_matching": m.perm, "scale_row": m.rscale, "scale_col": m.cscale}[name].copy()
+        if name in ("perm_reorder_row", "perm_reorder_col") and self._stage < 1 and getattr(self, "_reordered", False):
+            # after "reordering" alone: the ordering algorithm's permutation (src/solver.jl:1082-1085)
+            return self.symbolic.ordering.copy()
         if name in ("perm_reorder_row", "perm_reorder_col", "perm_col"):
             self._need(1, name)
             if name == "perm_col" and self._matching is not None and self.structure == "G":
@@ -347,8 +350,12 @@ class DirectSolver:
     # -- phases -----------------------------------------------------------------------------------------------
     def execute(self, phase, X=None, B=None):
         """``execute!(phase, solver, X, B)``."""
-        if phase in ("reordering", "symbolic_factorization", "analysis"):
+        if phase == "analysis":
             return self._analysis()
+        if phase == "reordering":
+            return self._analysis(plan=False)
+        if phase == "symbolic_factorization":
+            return self._symbolic_factorization()
         if phase in ("factorization", "refactorization"):
             return self._factorize(refactor=phase == "refactorization")
         if phase in ("solve", "solve_refinement", "solve_fwd_perm", "solve_fwd", "solve_diag", "solve_bwd",
@@ -386,8 +393,16 @@ class DirectSolver:
         fp = self.params["factor_precision"]
         return 1 if fp in ("fp32", "float32") else 0
 
-    def _analysis(self):
+    def _analysis(self, plan=True):
+        """``"analysis"`` = ``"reordering"`` then ``"symbolic_factorization"`` (src/solver.jl:444-452). The
+        host analysis (ordering, supernodes, maps) runs here; ``plan=False`` ("reordering") stops before
+        the device plan, which ``"symbolic_factorization"`` then builds."""
         p = self.params
+        if self._plan_exists():                 # a new analysis drops the previous one's plan
+            numeric_lib().sdsb200_plan_destroy(self._plan)
+            self._plan = None
+        self._stage = 0
+        self._reordered = False
         flags = None
         if int(p["schur_mode"]) == 1:
             # Schur complement mode (src/solver.jl:471-475, 554-559): the flagged rows and columns last, as
@@ -422,6 +437,15 @@ class DirectSolver:
                                 pivot_threshold=p["pivot_threshold"], use_superpanels=p["use_superpanels"],
                                 amalgamation=tuple(p["amalgamation"]), user_pairs=user_pairs,
                                 user_schur_indices=flags)
+        self._reordered = True
+        if plan:
+            self._symbolic_factorization()
+
+    def _symbolic_factorization(self):
+        """``"symbolic_factorization"`` (_symbolic!, src/solver.jl:609-660): the device plan of the analysis
+        "reordering" computed (the maps and every buffer of the numeric and solve phases)."""
+        if not getattr(self, "_reordered", False):
+            raise FactorizationError("phase \"symbolic_factorization\" needs \"reordering\" (or run \"analysis\")")
         self._create_plan()
         self._stage = 1
 

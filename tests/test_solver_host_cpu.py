@@ -89,3 +89,21 @@ def test_member_selection_checked_at_the_next_phase():
             ds._sync_members()
     finally:
         ds._plan = None
+
+
+def test_reordering_then_symbolic_factorization():
+    """The analysis phases as the reference splits them (src/solver.jl:444-452, 609-612, 1082-1085):
+    "reordering" alone gives the ordering algorithm's permutation as perm_reorder_row, and
+    "symbolic_factorization" without it is a FactorizationError. ("reordering" is host work only: no
+    device is needed.)"""
+    from sdsb200.analysis import analyze_csr
+    from sdsb200.solver import FactorizationError
+
+    A = M.lap2d_shifted(8, 8)
+    ds = DirectSolver(A, "SPD", device="cpu", reordering_alg="nd")
+    with pytest.raises(FactorizationError):
+        ds.execute("symbolic_factorization")
+    assert ds.execute("reordering") is None
+    S = analyze_csr(A, "SPD", reordering="nd")
+    assert np.array_equal(ds.getparam("perm_reorder_row"), S.ordering)
+    assert sorted(ds.getparam("perm_reorder_col")) == list(range(1, 65))
