@@ -222,6 +222,7 @@ int run_factor(Plan* P, const double* nzval, double eps, double u, int pivot, in
                 a.status = P->d_solve_status;
                 a.copy_src = static_cast<const T*>(P->d_inv);
                 a.copy_stride = P->inv_len;
+                a.exact = sizeof(T) == 8 ? L.exact : 0;
                 e = launch_gemm<T>(a, nm, st);
                 break;
             }

@@ -9,6 +9,7 @@
 // * chol_step_kernel: one 32-column step of a large Cholesky front (diagonal block + trsm).
 // * block_inv_kernel: inverses of the 64 x 64 diagonal blocks of the solve's wide fronts.
 // * scale_ld_kernel: W = L21 D for the contribution-block update of those fronts.
+// * gemm_nt_exact_kernel: that update in FP64 in the oracle's summation order (SIMT).
 #include <cuda_runtime.h>
 #include <math.h>
 #include <stdint.h>
@@ -126,12 +127,95 @@ __global__ void __launch_bounds__(128) gemm_nt_dmma_kernel(GemmArgs<double> A) {
             }
 }
 
+// The FP64 contribution-block update of an LDLT / LU front in the oracle's order (ref_ldlt!
+// src/reference/ldlt.jl:184-191: F22 -= W L21^T one rank-1 term after another; ref_lu!
+// src/reference/lu.jl:142-150: F22 -= sum_k (L21 d)_k U12_k, the sum accumulated from zero first).
+// Every product and sum is rounded on its own (__dmul_rn / __dadd_rn / __dsub_rn are never fused),
+// so the contribution blocks, and the pivot decisions of the parents that assemble them, are those
+// of the oracle bit for bit. SIMT FP64, 64 x 64 tile, 256 threads of 4 x 4 entries, K staged 16 at a
+// time in two shared-memory buffers; mode-0 tiles only.
+__global__ void __launch_bounds__(256) gemm_nt_exact_kernel(GemmArgs<double> A) {
+    constexpr int BM = 64, BK = 16, LDS = 72;
+    __shared__ __align__(16) double As[2][BK][LDS];
+    __shared__ __align__(16) double Bs[2][BK][LDS];
+    const GemmTile t = A.tiles[blockIdx.x];
+    const int member = A.members ? A.members[blockIdx.y] : blockIdx.y;
+    if (A.finfo && t.front >= 0 && A.finfo[(int64_t)member * A.ns + t.front] != 0) return;
+    const double* Ab = A.abuf + (int64_t)member * A.astride + t.a;
+    const double* Bb = A.bbuf + (int64_t)member * A.bstride + t.b;
+    double* Cb = A.cbuf + (int64_t)member * A.cstride + t.c;
+    const int tid = threadIdx.x, tx = tid & 15, ty = tid >> 4;
+    const int M = t.m, N = t.n, K = t.k;
+    const bool running = A.exact == 1;
+    double c[4][4], acc[4][4];
+#pragma unroll
+    for (int i = 0; i < 4; ++i)
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+            const int r = tx + 16 * i, col = ty + 16 * j;
+            c[i][j] = (r < M && col < N && r + t.diag >= col) ? Cb[r + (int64_t)col * t.ldc] : 0.0;
+            acc[i][j] = 0.0;
+        }
+    auto load = [&](int buf, int k0) {
+#pragma unroll
+        for (int q = 0; q < (BM * BK) / 256; ++q) {
+            int e = tid + 256 * q, r = e % BM, kk = e / BM;
+            bool va = r < M && k0 + kk < K;
+            cp_async8(&As[buf][kk][r], va ? Ab + r + (int64_t)(k0 + kk) * t.lda : Ab, va);
+            bool vb = r < N && k0 + kk < K;
+            cp_async8(&Bs[buf][kk][r], vb ? Bb + r + (int64_t)(k0 + kk) * t.ldb : Bb, vb);
+        }
+        cp_async_commit();
+    };
+    const int nk = (K + BK - 1) / BK;
+    load(0, 0);
+    for (int it = 0; it < nk; ++it) {
+        const int buf = it & 1;
+        if (it + 1 < nk) {
+            load(buf ^ 1, (it + 1) * BK);
+            cp_async_wait<1>();
+        } else {
+            cp_async_wait<0>();
+        }
+        __syncthreads();
+        const int kc = min(BK, K - it * BK);
+        for (int kk = 0; kk < kc; ++kk) {
+            double a[4], b[4];
+#pragma unroll
+            for (int i = 0; i < 4; ++i) a[i] = As[buf][kk][tx + 16 * i];
+#pragma unroll
+            for (int j = 0; j < 4; ++j) b[j] = Bs[buf][kk][ty + 16 * j];
+            if (running) {
+#pragma unroll
+                for (int i = 0; i < 4; ++i)
+#pragma unroll
+                    for (int j = 0; j < 4; ++j) c[i][j] = __dsub_rn(c[i][j], __dmul_rn(a[i], b[j]));
+            } else {
+#pragma unroll
+                for (int i = 0; i < 4; ++i)
+#pragma unroll
+                    for (int j = 0; j < 4; ++j) acc[i][j] = __dadd_rn(acc[i][j], __dmul_rn(a[i], b[j]));
+            }
+        }
+        __syncthreads();
+    }
+#pragma unroll
+    for (int i = 0; i < 4; ++i)
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+            const int r = tx + 16 * i, col = ty + 16 * j;
+            if (r < M && col < N && r + t.diag >= col)
+                Cb[r + (int64_t)col * t.ldc] = running ? c[i][j] : __dsub_rn(c[i][j], acc[i][j]);
+        }
+}
+
 template <typename T>
 cudaError_t launch_gemm(const GemmArgs<T>& a, int nmembers, cudaStream_t st) {
     if (a.count == 0) return cudaSuccess;
     dim3 grid(a.count, nmembers);
     if constexpr (sizeof(T) == 8) {
-        gemm_nt_dmma_kernel<<<grid, 128, 0, st>>>(a);
+        if (a.exact) gemm_nt_exact_kernel<<<grid, 256, 0, st>>>(a);
+        else gemm_nt_dmma_kernel<<<grid, 128, 0, st>>>(a);
     } else {
         return launch_gemm_tc32(a, nmembers, st);   // 3xTF32 on tcgen05
     }
@@ -372,14 +456,15 @@ __global__ void scale_ld_kernel(ScaleArgs<T> A) {
     for (int i = threadIdx.x; i < m; i += blockDim.x) {
         double v;
         double x = (double)P[w + i + (int64_t)q * f];
+        // each product and the sum rounded on its own, as the oracle's W (ldlt.jl:184-189)
         if (STRUCT == STRUCT_S && kq == KIND_2X2_FIRST) {
             double x2 = (double)P[w + i + (int64_t)(q + 1) * f];
-            v = x * d[g] + x2 * d[A.n + g];
+            v = __dadd_rn(__dmul_rn(x, d[g]), __dmul_rn(x2, d[A.n + g]));
         } else if (STRUCT == STRUCT_S && kq == KIND_2X2_SECOND) {
             double x1 = (double)P[w + i + (int64_t)(q - 1) * f];
-            v = x1 * d[A.n + g - 1] + x * d[g];
+            v = __dadd_rn(__dmul_rn(x1, d[A.n + g - 1]), __dmul_rn(x, d[g]));
         } else {
-            v = x * d[g];
+            v = __dmul_rn(x, d[g]);
         }
         W[i + (int64_t)q * m] = T(v);
     }

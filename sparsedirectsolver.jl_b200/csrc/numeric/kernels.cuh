@@ -102,6 +102,8 @@ struct GemmArgs {
     int32_t* status;   // tensor-core GEMM: nonzero when a bounded wait for the MMAs gave up
     const T* copy_src; // mode-2 tiles: C = copy_src[a ...] (ld lda), m x n
     int64_t copy_stride;   // per-member stride of copy_src
+    int32_t exact;     // FP64 mode-0 tiles summed in the oracle's order, every product and sum rounded:
+                       // 1 (LDLT) c = c - a_k b_k for k = 0, 1, ...; 2 (LU) c = c - (a_0 b_0 + a_1 b_1 + ...)
 };
 
 // FP32 grouped GEMM on the tensor cores (tcgen05, 3xTF32); tc_kernels.cu

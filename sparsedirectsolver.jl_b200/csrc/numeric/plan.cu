@@ -517,6 +517,7 @@ Plan* build_plan(const sdsb200_symbolic* sym, const sdsb200_plan_options* popts,
                     ProgLaunch gl{};
                     gl.kind = L_GEMM; gl.level = L;
                     gl.abuf = BUF_WORK; gl.bbuf = gen ? BUF_UFACTOR : BUF_FACTOR; gl.cbuf = BUF_CB;
+                    gl.exact = gen ? 2 : 1;
                     gl.list = (int64_t)tiles.size();
                     for (int s : withcb) {
                         const DFront& F = P->fronts[s];

@@ -28,6 +28,8 @@ struct ProgLaunch {
     double bytes;      // algorithmic device-memory bytes of the launch
     int32_t coop = -1;      // pivot: offset of the group prefix in coop_first (-1: one CTA per front)
     int32_t coop_grid = 0;  // pivot: CTAs of the cooperative launch
+    int32_t exact = 0;      // gemm: the contribution-block update of an LDLT / LU front, which the FP64
+                            // form sums in the oracle's order (1: LDLT, 2: LU)
 };
 
 // per-kind accounting of the profiling mode (CUDA events around every launch)
