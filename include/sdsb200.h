@@ -199,16 +199,22 @@ int sdsb200_set_interrupt(sdsb200_plan* plan, const volatile int32_t* h_flag);
  * then polled before a factorization and before each refinement step, not between launch groups. */
 int sdsb200_set_graphs(sdsb200_plan* plan, int32_t on);
 
-/* Solve engine (on by default): one cooperative persistent launch per solve when a single batch member
- * is active (off: one launch per level and sweep, the engine of uniform batches). */
+/* Solve engine when a single batch member is active. 1 (default): the dataflow solve, one cooperative
+ * persistent launch per group of 8 right-hand sides with no grid barrier (tasks in a topological order
+ * of the elimination tree, synchronised by per-front counters and per-block flags); 2: one cooperative
+ * launch with a grid barrier per tree level; 0: one launch per level and sweep (the engine of uniform
+ * batches and of the solve sub-phases). */
 int sdsb200_set_persistent(sdsb200_plan* plan, int32_t on);
 
 /* Profiling mode (on != 0): CUDA events around every launch of the following factor and solve
  * calls, accumulated per kernel kind (resets the totals). Costs one event record per launch. */
 int sdsb200_set_profiling(sdsb200_plan* plan, int32_t on);
 
-/* Profiling: copy up to cap (tag, nanoseconds) pairs of the persistent solve's phase stamps (written
- * when profiling is on; tag = kind << 40 | level << 16 | step). Returns the pairs copied or -1. */
+/* Profiling: copy up to cap (tag, nanoseconds) pairs of the level-kernel solve's phase stamps (written
+ * when profiling is on; tag = kind << 40 | level << 16 | step). Returns the pairs copied or -1. With
+ * cap < 0: the dataflow solve's task trace of its last launch, 6 int64 per task (task start, end of its
+ * dependency wait, task end in ns of %globaltimer; CTA; task kind; a | b << 32), up to -cap tasks;
+ * returns the tasks copied. */
 int64_t sdsb200_get_trace(sdsb200_plan* plan, int64_t* h_out, int64_t cap);
 
 /* Plan facts: "ns", "nlevels", "factor_len", "cb_len", "launches_factor", "launches_solve",
@@ -237,7 +243,11 @@ int sdsb200_sampled_outer(int64_t n, int64_t nnz, const void* rowptr, const void
                           void* stream);
 
 /* Solve without allocating (no counterpart in the reference): op(A) X = B for one active batch member,
- * no refinement, as one cooperative kernel launch plus two small memsets. sdsb200_solve keeps its
+ * no refinement, as two small memsets (the status word; the plan's flag and counter buffer, which is
+ * plan memory allocated at plan creation and shared by every solve on the plan) and one cooperative
+ * kernel launch per group of 8 right-hand sides. On a plan with an FP32 factor it returns the
+ * unrefined solution through that factor (FP32 accuracy); refine it with sdsb200_residual and further
+ * calls when FP64 accuracy is needed. sdsb200_solve keeps its
  * working vectors in the plan and records its launches into a CUDA graph per set of buffers, and
  * building that graph makes the driver allocate device memory on the first call with new buffers.
  * Callers that may not allocate once set-up is over (a framework whose pool allocator owns all device
@@ -248,11 +258,14 @@ int sdsb200_sampled_outer(int64_t n, int64_t nnz, const void* rowptr, const void
  * SDSB200_INVALID_VALUE: 512 + 8 * (2 * n * nrhs + ulen) bytes must fit, ulen being the plan's
  * update-vector length (the sum over fronts of the rows below the pivot block, times max_nrhs); the
  * error message gives the bytes needed. The first call on a device looks up the array's device address (which may also load the
- * library's device code), so make one call during set-up, before any stream capture. The array is
+ * library's device code) and keeps it for the life of the process, so make one call during set-up,
+ * before any stream capture; a device reset (cudaDeviceReset) after that first call is not supported. The array is
  * shared by every call on that device and keeps the last call's contents; calls that overlap on the
  * GPU (other streams, other plans, other threads) race on it and must be serialised by the caller.
  * solve_mode as sdsb200_opts (1, 2: A^T for "G"). status (device int32, may be NULL): set to 0, then
- * nonzero if a bounded grid-barrier wait of the launch gave up. */
+ * nonzero if a bounded wait of the launch gave up (X is then not the solution). With status NULL the
+ * call reads a status word of its own back at the end, which waits for the stream, and returns
+ * SDSB200_TIMEOUT if a wait gave up. */
 #define SDSB200_NOALLOC_SCRATCH_BYTES (32ull << 20)
 int sdsb200_solve_noalloc(sdsb200_plan* plan, double* X, int64_t ldx, const double* B, int64_t ldb, int32_t nrhs,
                           int32_t solve_mode, int32_t* status, void* stream);

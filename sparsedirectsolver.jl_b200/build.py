@@ -26,6 +26,7 @@ NUMERIC_SOURCES = [
     "numeric/dense_kernels.cu",
     "numeric/pivot_kernels.cu",
     "numeric/solve_kernels.cu",
+    "numeric/solve_dataflow.cu",
     "numeric/schur_kernels.cu",
     "numeric/adjoint_kernels.cu",
     "numeric/tc_kernels.cu",

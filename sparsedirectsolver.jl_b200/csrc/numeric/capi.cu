@@ -82,7 +82,7 @@ void prof_resolve(Plan* P) {
 }
 
 const char* const PROF_NAMES[PK_COUNT] = {"small", "assemble", "panel", "gemm", "pivot", "scale",
-                                          "stats", "fwd", "bwd", "diag", "permute", "residual"};
+                                          "stats", "fwd", "bwd", "diag", "permute", "residual", "inv"};
 
 int prof_kind_of(LaunchKind k) {
     switch (k) {
@@ -92,7 +92,8 @@ int prof_kind_of(LaunchKind k) {
         case L_GEMM: return PK_GEMM;
         case L_PIVOT_FRONT: return PK_PIVOT;
         case L_SCALE: return PK_SCALE;
-        case L_BLOCKINV: return PK_PANEL;
+        case L_BLOCKINV: return PK_INV;
+        case L_DFINV: return PK_INV;
         default: return PK_STATS;
     }
 }
@@ -294,6 +295,42 @@ int run_factor(Plan* P, const double* nzval, double eps, double u, int pivot, in
                 }
                 break;
             }
+            case L_DFINV: {
+                // the dataflow solve's inverses: L11^-1 of the warp fronts, 64 x 64 diagonal blocks of
+                // the tiled fronts (of the L panels, and of the U^T panels for LU)
+                for (int side = 0; side < (P->structure == STRUCT_G ? 2 : 1) && e == cudaSuccess; ++side) {
+                    const T* panels = side ? ufactor : factor;
+                    T* inv = static_cast<T*>(side ? P->d_dfinv_U : P->d_dfinv_L);
+                    SmallInvArgs<T> a{};
+                    a.fronts = P->d_fronts;
+                    a.list = P->d_df_small;
+                    a.count = P->n_df_small;
+                    a.inv_off = P->d_df_inv_off;
+                    a.members = members;
+                    a.panels = panels;
+                    a.inv = inv;
+                    a.factor_len = P->factor_len;
+                    a.inv_len = P->df_inv_len;
+                    a.finfo = P->d_finfo;
+                    a.ns = (int32_t)P->ns;
+                    e = launch_small_inv<T>(a, nm, st);
+                    if (e != cudaSuccess) break;
+                    BlockInvArgs<T> b{};
+                    b.fronts = P->d_fronts;
+                    b.tasks = P->d_df_blkinv;
+                    b.count = P->n_df_blkinv;
+                    b.dinv_off = P->d_df_inv_off;
+                    b.members = members;
+                    b.panels = panels;
+                    b.dinv = inv;
+                    b.factor_len = P->factor_len;
+                    b.dinv_len = P->df_inv_len;
+                    b.finfo = P->d_finfo;
+                    b.ns = (int32_t)P->ns;
+                    e = launch_block_inv<T>(b, nm, st);
+                }
+                break;
+            }
             case L_STATS: {
                 StatsArgs a{};
                 a.stats = P->d_stats;
@@ -477,6 +514,87 @@ int run_persistent(Plan* P, int nrhs, bool transpose, const double* in, int64_t 
     return e == cudaSuccess ? SDSB200_OK : cuda_fail(e, "persistent solve");
 }
 
+// the whole solve as dataflow tasks in one persistent launch per group of up to DF_MAX_NRHS
+// right-hand sides (solve_dataflow.cu)
+template <typename T>
+int run_dataflow(Plan* P, int nrhs, bool transpose, const double* in, int64_t ldin, double* out, int64_t ldout,
+                 int mode, cudaStream_t st) {
+    const bool gen = P->structure == STRUCT_G, ldl = P->structure == STRUCT_S;
+    const T* factor = static_cast<const T*>(P->d_factor);
+    const T* ufactor = static_cast<const T*>(P->d_ufactor);
+    const T* iL = static_cast<const T*>(P->d_dfinv_L);
+    const T* iU = static_cast<const T*>(P->d_dfinv_U);
+    DataflowArgs<T> a{};
+    a.tasks = P->d_df_tasks;
+    a.ntasks = P->n_df_tasks;
+    a.fronts = P->d_fronts;
+    a.df = P->d_df;
+    a.bundles = P->d_df_bundles;
+    a.rptr = P->d_df_rptr;
+    a.csrc = P->d_df_csrc;
+    a.facf = (gen && transpose) ? ufactor : factor;
+    a.facb = (gen && !transpose) ? ufactor : factor;
+    a.invf = (gen && transpose) ? iU : iL;
+    a.invb = (gen && !transpose) ? iU : iL;
+    a.rowval = P->maps.rowval;
+    a.piv = P->d_piv;
+    a.perm = P->d_perm0;
+    a.d = P->d_d;
+    a.kind = P->d_kind;
+    a.n = P->n;
+    a.Y = P->d_Y;
+    a.U = P->d_U;
+    a.xtmp = P->d_xtmp;
+    a.part = P->d_df_part;
+    unsigned int* fl = P->d_df_flags;
+    const int64_t ns = P->ns;
+    a.fcnt = fl;
+    a.bdone = fl + ns;
+    a.xflag = fl + 2 * ns;
+    a.pcnt = fl + 2 * ns + P->df_nblk;
+    a.head = fl + 2 * ns + 2 * (int64_t)P->df_nblk;
+    a.status = P->d_solve_status;
+    a.reorder_fw = ldl || (gen && !transpose);
+    a.reorder_bw = ldl || (gen && transpose);
+    a.diag_mode = P->structure == STRUCT_SPD ? 0 : (ldl ? 2 : 1);
+    a.mode = mode;
+    a.ldin = ldin;
+    a.ldout = ldout;
+    a.trace = P->profile ? P->d_df_trace : nullptr;
+    double ent = 0.0;
+    for (double v : P->level_panel_entries) ent += v;
+    for (int r0 = 0; r0 < nrhs; r0 += DF_MAX_NRHS) {
+        a.nrhs = std::min(DF_MAX_NRHS, nrhs - r0);
+        // shared memory: per warp of a bundle f x nrhs doubles; a tiled task 2 x 64 + DF_CHUNK rows of
+        // nrhs doubles
+        a.warp_smem = (int32_t)(((int64_t)P->df_fwarp_max * a.nrhs + 1) & ~int64_t(1));
+        const size_t smem = sizeof(double) * std::max<size_t>((size_t)a.warp_smem * (DF_THREADS / 32),
+                                                              (2 * DF_BLK + DF_CHUNK) * (size_t)DF_MAX_NRHS);
+        const int grid = dataflow_solve_grid<T>(a.nrhs, smem);
+        if (grid <= 0) return fail(SDSB200_CUDA_ERROR, "no co-resident grid for the dataflow solve");
+        a.in = in + (int64_t)r0 * ldin;
+        a.out = out + (int64_t)r0 * ldout;
+        CK(cudaMemsetAsync(P->d_df_flags, 0, sizeof(unsigned int) * P->df_flags_len, st), "dataflow flag reset");
+        prof_begin(P, st);
+        cudaError_t e = launch_dataflow_solve<T>(a, grid, smem, st);
+        // algorithmic work: every stored panel entry read once per sweep (2 flops per entry and rhs
+        // each way), the right-hand side read and the solution written
+        prof_end(P, st, PK_FWD, 4.0 * ent * a.nrhs, 2.0 * sizeof(T) * ent + 24.0 * P->n * a.nrhs);
+        if (e != cudaSuccess) return cuda_fail(e, "dataflow solve");
+    }
+    return SDSB200_OK;
+}
+
+// the one-launch solve of a single active member: the dataflow kernel (default) or the level kernel
+int run_one_launch(Plan* P, int nrhs, bool transpose, const double* in, int64_t ldin, double* out, int64_t ldout,
+                   int mode, cudaStream_t st) {
+    if (P->dataflow)
+        return P->elsize == 8 ? run_dataflow<double>(P, nrhs, transpose, in, ldin, out, ldout, mode, st)
+                              : run_dataflow<float>(P, nrhs, transpose, in, ldin, out, ldout, mode, st);
+    return P->elsize == 8 ? run_persistent<double>(P, nrhs, transpose, in, ldin, out, ldout, mode, st)
+                          : run_persistent<float>(P, nrhs, transpose, in, ldin, out, ldout, mode, st);
+}
+
 bool use_persistent(const Plan* P) { return P->nact == 1 && P->all_members && P->persistent; }
 
 int sweeps(Plan* P, int nrhs, bool transpose, cudaStream_t st, int which = 7) {
@@ -637,9 +755,7 @@ int sdsb200_solve(sdsb200_plan* plan, double* X, int64_t ldx, const double* B, i
     std::vector<uint64_t> key = {(uint64_t)(uintptr_t)X, (uint64_t)ldx, (uint64_t)(uintptr_t)B, (uint64_t)ldb, common,
                                  (uint64_t)P->nact};
     int rc = run_graph(P, P->g_solve, key, st, [&](cudaStream_t s) -> int {
-        if (use_persistent(P))
-            return P->elsize == 8 ? run_persistent<double>(P, nrhs, transpose, B, ldb, X, ldx, 0, s)
-                                  : run_persistent<float>(P, nrhs, transpose, B, ldb, X, ldx, 0, s);
+        if (use_persistent(P)) return run_one_launch(P, nrhs, transpose, B, ldb, X, ldx, 0, s);
         int r = permute(P, 0, B, ldb, nullptr, 0, nrhs, s);
         if (r) return r;
         r = sweeps(P, nrhs, transpose, s);
@@ -699,9 +815,7 @@ int sdsb200_solve(sdsb200_plan* plan, double* X, int64_t ldx, const double* B, i
         }
         std::vector<uint64_t> ckey = key;
         rc = run_graph(P, P->g_corr, ckey, st, [&](cudaStream_t s) -> int {
-            if (use_persistent(P))
-                return P->elsize == 8 ? run_persistent<double>(P, nrhs, transpose, P->d_R, P->n, X, ldx, 2, s)
-                                      : run_persistent<float>(P, nrhs, transpose, P->d_R, P->n, X, ldx, 2, s);
+            if (use_persistent(P)) return run_one_launch(P, nrhs, transpose, P->d_R, P->n, X, ldx, 2, s);
             int r = permute(P, 0, P->d_R, P->n, nullptr, 0, nrhs, s);
             if (r) return r;
             r = sweeps(P, nrhs, transpose, s);
@@ -864,6 +978,13 @@ int sdsb200_set_members(sdsb200_plan* plan, const int32_t* h_members, int32_t na
 int64_t sdsb200_get_trace(sdsb200_plan* plan, int64_t* h_out, int64_t cap) {
     Plan* P = reinterpret_cast<Plan*>(plan);
     if (!P || !h_out) return -1;
+    if (cap < 0) {
+        // the dataflow solve's task trace of its last launch: 6 int64 per task (start and end of the task
+        // and the end of its dependency wait in %globaltimer ns, CTA, kind, a | b << 32), up to -cap tasks
+        int64_t nt = std::min<int64_t>(-cap, P->n_df_tasks);
+        if (cudaMemcpy(h_out, P->d_df_trace, sizeof(int64_t) * 6 * nt, cudaMemcpyDeviceToHost) != cudaSuccess) return -1;
+        return nt;
+    }
     int64_t n = std::min<int64_t>(cap, Plan::TRACE_CAP);
     if (cudaMemcpy(h_out, P->d_trace, sizeof(int64_t) * 2 * n, cudaMemcpyDeviceToHost) != cudaSuccess) return -1;
     return n;
@@ -873,6 +994,7 @@ int sdsb200_set_persistent(sdsb200_plan* plan, int32_t on) {
     Plan* P = reinterpret_cast<Plan*>(plan);
     if (!P) return fail(SDSB200_INVALID_VALUE, "plan is NULL");
     P->persistent = on != 0;
+    P->dataflow = on != 2;
     for (Plan::CachedGraph* g : {&P->g_solve, &P->g_corr})
         g->key.clear();
     return SDSB200_OK;
@@ -1085,14 +1207,23 @@ int sdsb200_solve_noalloc(sdsb200_plan* plan, double* X, int64_t ldx, const doub
     double* xt = Y + vec;
     double* U = xt + vec;
     cudaStream_t st = (cudaStream_t)stream;
-    // only the status word and the barrier counter must start at zero (the launch zeroes the barrier);
-    // Y, xtmp and the update vectors are written before they are read in every solve
+    // only the status word must start at zero here (the launch sequence zeroes the plan's flags and
+    // counters); Y, xtmp and the update vectors are written before they are read in every solve
     CK(cudaMemsetAsync(st_word, 0, sizeof(int32_t), st), "sdsb200_solve_noalloc: status reset");
     const bool transpose = P->structure == STRUCT_G && solve_mode != 0;
-    ScratchSwap swap(P, Y, U, xt, bar, st_word);
     P->launches_done = 0;
-    return P->elsize == 8 ? run_persistent<double>(P, nrhs, transpose, B, ldb, X, ldx, 0, st)
-                          : run_persistent<float>(P, nrhs, transpose, B, ldb, X, ldx, 0, st);
+    {
+        ScratchSwap swap(P, Y, U, xt, bar, st_word);
+        rc = run_one_launch(P, nrhs, transpose, B, ldb, X, ldx, 0, st);
+    }
+    if (rc || status) return rc;
+    // no status word of the caller's: read the fallback word back (a plain copy into a host variable,
+    // which allocates nothing) so that a wait that gave up is not lost
+    int32_t word = 0;
+    CK(cudaMemcpyAsync(&word, st_word, sizeof(word), cudaMemcpyDeviceToHost, st), "sdsb200_solve_noalloc: status read");
+    CK(cudaStreamSynchronize(st), "sdsb200_solve_noalloc: status read");
+    if (word != 0) return fail(SDSB200_TIMEOUT, "sdsb200_solve_noalloc: a bounded wait of the solve gave up");
+    return SDSB200_OK;
 }
 
 }  // extern "C"

@@ -78,6 +78,7 @@ enum LaunchKind : int32_t {
     L_SCALE,           // W = L21 D of large LDLT / LU fronts
     L_BLOCKINV,        // inverses of the diagonal blocks of the wide fronts (solve)
     L_CHOL_STEP,       // large Cholesky: one 32-column step (diagonal block + trsm of the rows below)
+    L_DFINV,           // diagonal-block inverses of every front for the dataflow solve
 };
 
 struct Launch {

@@ -418,6 +418,49 @@ __global__ void __launch_bounds__(256) block_inv_kernel(BlockInvArgs<T> A) {
         if (ri[k] >= 0 && ri[k] < nbb && ci[k] < nbb) inv[ri[k] + (int64_t)ci[k] * NB] = T(x[k]);
 }
 
+// L11^-1 of a warp front of the dataflow solve (w <= 32; unit or not, as stored), one warp per front:
+// lane c computes column c by forward substitution, X[k, c] = (delta_kc - sum_{j<k} L[k, j] X[j, c]) / L[k, k],
+// with row k of L11 read once per step (the same address for the whole warp)
+template <typename T>
+__global__ void __launch_bounds__(256) small_inv_kernel(SmallInvArgs<T> A) {
+    const int wi = (int)((blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5), lane = threadIdx.x & 31;
+    if (wi >= A.count) return;
+    const int s = A.list[wi];
+    const int member = A.members ? A.members[blockIdx.y] : blockIdx.y;
+    if (A.finfo && A.finfo[(int64_t)member * A.ns + s] != 0) return;
+    const DFront fd = A.fronts[s];
+    const int f = fd.f, w = fd.w;
+    const T* P = A.panels + (int64_t)member * A.factor_len + fd.panel;
+    T* inv = A.inv + (int64_t)member * A.inv_len + A.inv_off[s];
+    double x[32];
+#pragma unroll
+    for (int k = 0; k < 32; ++k) {
+        double acc = (k == lane) ? 1.0 : 0.0;
+        if (k < w) {
+#pragma unroll
+            for (int j = 0; j < k; ++j) acc -= (double)P[k + (int64_t)j * f] * x[j];
+            acc /= (double)P[k + (int64_t)k * f];
+        }
+        x[k] = (k < w && lane < w) ? acc : 0.0;
+    }
+    if (lane < w) {
+#pragma unroll
+        for (int k = 0; k < 32; ++k)
+            if (k < w) inv[k + (int64_t)w * lane] = T(k >= lane ? x[k] : 0.0);
+    }
+}
+
+template <typename T>
+cudaError_t launch_small_inv(const SmallInvArgs<T>& a, int nmembers, cudaStream_t st) {
+    if (a.count == 0) return cudaSuccess;
+    dim3 grid((a.count + 7) / 8, nmembers);
+    small_inv_kernel<T><<<grid, 256, 0, st>>>(a);
+    return cudaGetLastError();
+}
+
+template cudaError_t launch_small_inv<double>(const SmallInvArgs<double>&, int, cudaStream_t);
+template cudaError_t launch_small_inv<float>(const SmallInvArgs<float>&, int, cudaStream_t);
+
 template <typename T>
 cudaError_t launch_block_inv(const BlockInvArgs<T>& a, int nmembers, cudaStream_t st) {
     if (a.count == 0) return cudaSuccess;

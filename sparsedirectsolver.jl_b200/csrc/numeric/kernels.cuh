@@ -179,6 +179,24 @@ struct BlockInvArgs {
 template <typename T>
 cudaError_t launch_block_inv(const BlockInvArgs<T>& a, int nmembers, cudaStream_t st);
 
+// Inverses of L11 (w <= 32) of the dataflow solve's warp fronts, w x w (ld w, zero above the diagonal)
+template <typename T>
+struct SmallInvArgs {
+    const DFront* fronts;
+    const int32_t* list;       // the fronts
+    int32_t count;
+    const int64_t* inv_off;    // per front
+    const int32_t* members;
+    const T* panels;           // factor or U^T panels
+    T* inv;
+    int64_t factor_len, inv_len;
+    const int32_t* finfo;
+    int32_t ns;
+};
+template <typename T>
+cudaError_t launch_small_inv(const SmallInvArgs<T>& a, int nmembers, cudaStream_t st);
+cudaError_t prepare_dataflow_kernels(int max_smem);
+
 constexpr int CHOL_NB = 32;   // column block of the large-front Cholesky (one warp per diagonal block)
 cudaError_t prepare_factor_kernels(int max_smem);
 cudaError_t prepare_dense_kernels(int max_smem);

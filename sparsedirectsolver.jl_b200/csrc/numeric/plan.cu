@@ -561,6 +561,133 @@ Plan* build_plan(const sdsb200_symbolic* sym, const sdsb200_plan_options* popts,
             bl.count = P->n_binv_tasks;
             P->prog.push_back(bl);
         }
+        // dataflow solve: front classes, task list, inverse layout, contribution lists (solve.cuh)
+        {
+            std::vector<DfFront> df(ns);
+            std::vector<int64_t> inv_off(ns, -1);
+            std::vector<int32_t> small_list, blkinv;
+            int64_t il = 0;
+            int32_t nblk = 0, npart = 0;
+            for (int64_t s = 0; s < ns; ++s) {
+                const DFront& F = P->fronts[s];
+                DfFront& d = df[s];
+                d = DfFront{};
+                if (s == P->schur_front) continue;
+                const int m = F.f - F.w;
+                d.tiled = !(F.w <= DF_WARP_W && F.f <= DF_WARP_F);
+                d.inv = inv_off[s] = il;
+                if (!d.tiled) {
+                    il += ((int64_t)F.w * F.w + 1) & ~int64_t(1);
+                    d.fsig = 1;
+                    small_list.push_back((int32_t)s);
+                    P->df_fwarp_max = std::max(P->df_fwarp_max, F.f);
+                } else {
+                    d.nblk = (F.w + DF_BLK - 1) / DF_BLK;
+                    d.ntile = (F.f + DF_BLK - 1) / DF_BLK;
+                    d.nchunk = m > DF_CHUNK ? (m + DF_CHUNK - 1) / DF_CHUNK : 0;
+                    d.blk = nblk;
+                    d.part = npart;
+                    d.fsig = d.ntile;
+                    nblk += d.nblk;
+                    npart += d.nblk * d.nchunk;
+                    il += (int64_t)d.nblk * DF_BLK * DF_BLK;
+                    for (int b = 0; b < d.nblk; ++b) {
+                        blkinv.push_back((int32_t)s);
+                        blkinv.push_back(b);
+                    }
+                }
+            }
+            for (int64_t s = 0; s < ns; ++s)
+                if (s != P->schur_front && P->fronts[s].parent >= 0) df[P->fronts[s].parent].fneed += df[s].fsig;
+            // global update rows (U of the dataflow solve is (update row) x nrhs, row-major) and the
+            // per-row contribution lists: for every front row, the children's update rows that land on
+            // it, in child order (the order of the level kernels' pulls)
+            std::vector<int32_t> rptr, csrc;
+            {
+                int64_t ur = 0, rb = 0;
+                for (int64_t s = 0; s < ns; ++s) {
+                    df[s].urow = to_i32(ur, "update rows");
+                    df[s].rbase = to_i32(rb, "front rows");
+                    ur += P->fronts[s].f - P->fronts[s].w;
+                    rb += P->fronts[s].f + 1;
+                }
+                rptr.assign(rb, 0);
+                std::vector<std::pair<int32_t, int32_t>> hits;   // (front row, global update row)
+                for (int64_t s = 0; s < ns; ++s) {
+                    const DFront& F = P->fronts[s];
+                    hits.clear();
+                    for (int cq = F.ch_begin; cq < F.ch_end; ++cq) {
+                        const int c = (int)(child_list[cq] - 1);
+                        const DFront& Cf = P->fronts[c];
+                        const int mc = Cf.f - Cf.w;
+                        for (int i2 = 0; i2 < mc; ++i2)
+                            hits.push_back({(int32_t)(relind[Cf.ri_begin + i2] - 1), df[c].urow + i2});
+                    }
+                    std::stable_sort(hits.begin(), hits.end(),
+                                     [](const std::pair<int32_t, int32_t>& x, const std::pair<int32_t, int32_t>& y) {
+                                         return x.first < y.first;
+                                     });
+                    const int64_t base = df[s].rbase;
+                    size_t h = 0;
+                    for (int p2 = 0; p2 <= F.f; ++p2) {
+                        rptr[base + p2] = to_i32((int64_t)csrc.size(), "contributions");
+                        if (p2 == F.f) break;
+                        while (h < hits.size() && hits[h].first == p2) csrc.push_back(hits[h++].second);
+                    }
+                    if (h != hits.size()) throw BuildError(SDSB200_INVALID_VALUE, "relind outside the parent's rows");
+                }
+            }
+            std::vector<DfTask> tasks;
+            std::vector<int32_t> bundles;
+            auto push_bundles = [&](int L, int kind) {
+                std::vector<int32_t> wl;
+                for (int s : P->level_fronts[L])
+                    if (s != P->schur_front && !df[s].tiled) wl.push_back(s);
+                for (size_t o = 0; o < wl.size(); o += DF_BUNDLE) {
+                    const int cnt = (int)std::min<size_t>(DF_BUNDLE, wl.size() - o);
+                    tasks.push_back(DfTask{kind, (int32_t)bundles.size(), cnt, 0});
+                    bundles.insert(bundles.end(), wl.begin() + o, wl.begin() + o + cnt);
+                }
+            };
+            for (int L = 0; L < P->nlevels; ++L) {
+                for (int s : P->level_fronts[L]) {
+                    if (s == P->schur_front || !df[s].tiled) continue;
+                    for (int t = 0; t < df[s].ntile; ++t) tasks.push_back(DfTask{DF_FW_TILE, s, t, 0});
+                }
+                push_bundles(L, DF_FW_BUNDLE);
+            }
+            for (int L = P->nlevels - 1; L >= 0; --L) {
+                for (int s : P->level_fronts[L]) {
+                    if (s == P->schur_front || !df[s].tiled) continue;
+                    for (int b = 0; b < df[s].nblk; ++b)
+                        for (int c = 0; c < df[s].nchunk; ++c) tasks.push_back(DfTask{DF_BW_PART, s, b, c});
+                    for (int b = df[s].nblk - 1; b >= 0; --b) tasks.push_back(DfTask{DF_BW_OWNER, s, b, 0});
+                }
+                push_bundles(L, DF_BW_BUNDLE);
+            }
+            P->df_inv_len = std::max<int64_t>(il, 2);
+            P->df_nblk = nblk;
+            P->df_flags_len = 2 * ns + 2 * (int64_t)nblk + 8;
+            P->n_df_tasks = (int32_t)tasks.size();
+            P->n_df_small = (int32_t)small_list.size();
+            P->n_df_blkinv = (int32_t)(blkinv.size() / 2);
+            P->d_df = upload(P, df, st);
+            P->d_df_tasks = upload(P, tasks, st);
+            P->d_df_bundles = upload(P, bundles, st);
+            P->d_df_inv_off = upload(P, inv_off, st);
+            P->d_df_small = upload(P, small_list, st);
+            P->d_df_blkinv = upload(P, blkinv, st);
+            P->d_df_rptr = upload(P, rptr, st);
+            P->d_df_csrc = upload(P, csrc, st);
+            P->d_df_part = dalloc<double>(P, std::max<int64_t>(1, (int64_t)npart * DF_BLK * DF_MAX_NRHS));
+            P->d_df_flags = dalloc<unsigned int>(P, P->df_flags_len);
+            P->d_df_trace = dalloc<int64_t>(P, 6 * (int64_t)std::max<int32_t>(1, P->n_df_tasks));
+            ProgLaunch il_{};
+            il_.kind = L_DFINV;
+            il_.level = P->nlevels;
+            il_.count = P->n_df_small + P->n_df_blkinv;
+            P->prog.push_back(il_);
+        }
         {
             ProgLaunch pl{};
             pl.kind = L_STATS;
@@ -795,6 +922,8 @@ Plan* build_plan(const sdsb200_symbolic* sym, const sdsb200_plan_options* popts,
             P->d_dinv_L = alloc_bytes(es * P->dinv_len * nb);
             if (gen) P->d_dinv_U = alloc_bytes(es * P->dinv_len * nb);
         }
+        P->d_dfinv_L = alloc_bytes(es * P->df_inv_len * nb);
+        if (gen) P->d_dfinv_U = alloc_bytes(es * P->df_inv_len * nb);
         P->d_xtmp = dalloc<double>(P, n * P->max_nrhs);
         P->d_barrier = dalloc<unsigned int>(P, 1);
         P->n_blkflag = std::max<int64_t>(1, P->dinv_len / ((int64_t)SOLVE_BLK * SOLVE_BLK));
@@ -817,6 +946,7 @@ Plan* build_plan(const sdsb200_symbolic* sym, const sdsb200_plan_options* popts,
             cudaError_t ke = prepare_factor_kernels(optin);
             if (ke == cudaSuccess) ke = prepare_dense_kernels(optin);
             if (ke == cudaSuccess) ke = prepare_solve_kernels(optin);
+            if (ke == cudaSuccess) ke = prepare_dataflow_kernels(optin);
             if (ke == cudaSuccess) ke = prepare_tc_kernels();
             if (ke != cudaSuccess)
                 throw BuildError(SDSB200_CUDA_ERROR, std::string("kernel attribute setup failed: ") + cudaGetErrorString(ke));

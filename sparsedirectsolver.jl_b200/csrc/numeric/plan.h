@@ -10,6 +10,7 @@
 
 #include "common.cuh"
 #include "kernels.cuh"
+#include "solve.cuh"
 
 namespace sds {
 
@@ -34,7 +35,7 @@ struct ProgLaunch {
 
 // per-kind accounting of the profiling mode (CUDA events around every launch)
 enum ProfKind { PK_SMALL = 0, PK_ASSEMBLE, PK_PANEL, PK_GEMM, PK_PIVOT, PK_SCALE, PK_STATS, PK_FWD, PK_BWD, PK_DIAG,
-                PK_PERMUTE, PK_RESIDUAL, PK_COUNT };
+                PK_PERMUTE, PK_RESIDUAL, PK_INV, PK_COUNT };
 
 struct ProfAcc {
     double ms = 0, flops = 0, bytes = 0;
@@ -105,6 +106,29 @@ struct Plan {
     void* d_dinv_U = nullptr;
     int32_t* d_binv_tasks = nullptr;
     int n_binv_tasks = 0;
+    // dataflow solve (solve.cuh): per-front classes, the task list, the inverses of every front's diagonal
+    // blocks (warp fronts: w x w; tiled fronts: 64 x 64 blocks), flags and counters zeroed per launch
+    DfFront* d_df = nullptr;
+    DfTask* d_df_tasks = nullptr;
+    int32_t n_df_tasks = 0;
+    int32_t* d_df_bundles = nullptr;
+    int64_t* d_df_inv_off = nullptr;    // per front: offset of its inverses
+    int64_t df_inv_len = 0;
+    void* d_dfinv_L = nullptr;          // inverses of the factor's (L) diagonal blocks
+    void* d_dfinv_U = nullptr;          // ... of the U^T panels (LU)
+    int32_t* d_df_small = nullptr;      // warp fronts (the small-inverse launch)
+    int32_t n_df_small = 0;
+    int32_t* d_df_blkinv = nullptr;     // (front, block) pairs of the tiled fronts' 64 x 64 inverses
+    int32_t n_df_blkinv = 0;
+    int32_t* d_df_rptr = nullptr;       // per front row: start of its contributions (f + 1 per front)
+    int32_t* d_df_csrc = nullptr;       // contributions: the children's global update rows, in child order
+    unsigned int* d_df_flags = nullptr; // fcnt (ns), bdone (ns), xflag (nblk), pcnt (nblk), head
+    int64_t df_flags_len = 0;
+    int32_t df_nblk = 0;
+    double* d_df_part = nullptr;        // backward partial sums: slots of 64 x DF_MAX_NRHS doubles
+    int64_t* d_df_trace = nullptr;      // profiling: 6 int64 per task (start, wait done, end, CTA, kind, a | b << 32)
+    int32_t df_fwarp_max = 1;           // tallest warp front
+    bool dataflow = true;               // the dataflow kernel for the one-launch solve (else the level kernel)
     double* d_xtmp = nullptr;
     unsigned int* d_barrier = nullptr;
     unsigned int* d_blkflag = nullptr;   // persistent solve: 3 x n_blkflag words (block flags, pull flags,

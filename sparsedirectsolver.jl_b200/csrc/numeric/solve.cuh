@@ -66,6 +66,98 @@ struct PersistArgs {
     int32_t warp_xs;           // doubles of xs within it
 };
 
+// ---------------------------------------------------------------------------------------------------
+// Dataflow solve: the whole solve (forward, diagonal, backward, both permutations) in one persistent
+// cooperative launch with no grid barrier. Work is a list of tasks in a topological order of the
+// elimination tree (forward leaves to roots, then backward roots to leaves). CTAs take tasks in list
+// order from one atomic counter; a task waits only on tasks earlier in the list (counters and flags
+// with bounded waits), so the launch cannot deadlock while all CTAs are resident.
+//
+// Front classes:
+//  * warp fronts (w <= DF_WARP_W and f <= DF_WARP_F): one warp each; DF_BUNDLE fronts of one level per
+//    task, taken by the CTA's warps in turn. L11^-1 (w x w, ld w) is precomputed after the factorization.
+//  * tiled fronts (the rest): forward = one task per 64-row tile, which gathers its own rows (the right-
+//    hand side and the children's updates) and takes the 64-column blocks k <= t in order (block t's
+//    own tile solves it with the precomputed 64 x 64 inverse and publishes x_t); backward = partial-sum
+//    tasks over DF_CHUNK-row chunks of the update rows (-L21^T x2 per block) and one owner task per
+//    64-column block, from the last block to the first.
+// The children's updates reach a front through per-row contribution lists (the child update rows that
+// land on each front row, in child order), so every row is gathered by one thread with independent
+// loads and a fixed summation order.
+constexpr int DF_WARP_W = 32;     // widest warp front
+constexpr int DF_WARP_F = 128;    // tallest warp front
+constexpr int DF_BUNDLE = 16;     // warp fronts per task
+constexpr int DF_BLK = 64;        // tile rows and block columns of the tiled fronts
+constexpr int DF_CHUNK = 128;     // update rows per backward partial task
+constexpr int DF_MAX_NRHS = 8;    // right-hand sides per launch (more are solved in groups of 8)
+constexpr int DF_THREADS = 256;
+
+enum DfTaskKind : int32_t { DF_FW_BUNDLE = 1, DF_FW_TILE = 3, DF_BW_BUNDLE = 4, DF_BW_PART = 5, DF_BW_OWNER = 6 };
+
+struct DfTask {
+    int32_t kind, a, b, c;   // bundle: a = offset in the bundle list, b = count; tile: a = front, b = tile;
+                             // part: a = front, b = block, c = chunk; owner: a = front, b = block
+};
+
+struct DfFront {
+    int64_t inv;       // offset of the front's diagonal-block inverses (warp: w x w; tiled: nblk x 64 x 64)
+    int32_t tiled;     // 0: warp front; 1: tiled
+    int32_t ntile;     // tiled: 64-row tiles of the forward
+    int32_t nblk;      // tiled: 64-column blocks
+    int32_t nchunk;    // tiled: backward partial tasks per block (0: the owners sum the update rows themselves)
+    int32_t fneed;     // forward signals this front waits for (one per forward task of each child)
+    int32_t fsig;      // forward tasks of this front (each signals its parent, or the front itself at a root)
+    int32_t blk;       // tiled: first index of its blocks in the per-block flags
+    int32_t part;      // tiled: first partial slot (nblk x nchunk slots of 64 x DF_MAX_NRHS doubles)
+    int32_t urow;      // first of its update rows in the global numbering of update rows (U is
+                       // U[(urow + i) * nrhs + r] for update row i and right-hand side r)
+    int32_t rbase;     // its f + 1 row pointers into the contribution lists start at rptr[rbase]
+};
+
+template <typename T>
+struct DataflowArgs {
+    const DfTask* tasks;
+    int32_t ntasks;
+    const DFront* fronts;
+    const DfFront* df;
+    const int32_t* bundles;    // fronts of the warp bundles
+    const int32_t* rptr;       // per front row: start of its contributions in csrc
+    const int32_t* csrc;       // contributions: global update rows of the children, in child order
+    const T* facf;             // panels of the forward sweep (L; U^T panels for LU with A^T)
+    const T* facb;             // panels of the backward sweep
+    const T* invf;             // diagonal-block inverses of facf's panels
+    const T* invb;             // ... of facb's panels
+    const int32_t* rowval;
+    const int32_t* piv;        // 1-based local pivot order (LDLT, LU)
+    const int32_t* perm;       // 0-based original index of each factor position
+    const double* d;
+    const int8_t* kind;
+    const double* in;          // B (mode 0) or R (mode 2), column-major, ld ldin
+    double* out;               // X, ld ldout
+    int64_t ldin, ldout, n;
+    double* Y;                 // n x nrhs: forward result (pre-D) then solution, factor order
+    double* U;                 // update vectors, (global update row) x nrhs, row-major
+    double* xtmp;              // n x nrhs: a tiled front's published block solutions
+    double* part;              // backward partial sums
+    unsigned int* fcnt;        // ns: forward signals received (from children; at a root from itself)
+    unsigned int* bdone;       // ns: 1 once the front's backward solution is in Y
+    unsigned int* xflag;       // per block: 1 forward x_k published, 2 backward x_k published
+    unsigned int* pcnt;        // per block: backward partials written
+    unsigned int* head;        // the task counter
+    int32_t* status;           // nonzero: a bounded wait gave up
+    int32_t nrhs;              // <= DF_MAX_NRHS
+    int32_t reorder_fw, reorder_bw;
+    int32_t diag_mode;         // 0 none (Cholesky), 1 D (LU), 2 D with 2x2 blocks (LDLT)
+    int32_t mode;              // 0: X = solve(B); 2: X += solve(R)
+    int32_t warp_smem;         // doubles of shared memory per warp of a bundle task
+    int64_t* trace;            // profiling, or NULL: per task (start, wait done, end) %globaltimer ns, CTA, kind, a | b << 32
+};
+
+template <typename T>
+cudaError_t launch_dataflow_solve(const DataflowArgs<T>& a, int grid, size_t smem, cudaStream_t st);
+template <typename T>
+int dataflow_solve_grid(int nrhs, size_t smem);
+
 struct DiagArgs {
     const int32_t* members;
     const double* d;
