@@ -86,7 +86,7 @@ struct PersistArgs {
 // loads and a fixed summation order.
 constexpr int DF_WARP_W = 32;     // widest warp front
 constexpr int DF_WARP_F = 128;    // tallest warp front
-constexpr int DF_BUNDLE = 16;     // warp fronts per task
+constexpr int DF_BUNDLE = 8;      // warp fronts per task (one per warp)
 constexpr int DF_BLK = 64;        // tile rows and block columns of the tiled fronts
 constexpr int DF_CHUNK = 128;     // update rows per backward partial task
 constexpr int DF_MAX_NRHS = 8;    // right-hand sides per launch (more are solved in groups of 8)
