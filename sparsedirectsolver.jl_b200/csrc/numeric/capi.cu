@@ -224,6 +224,9 @@ int run_factor(Plan* P, const double* nzval, double eps, double u, int pivot, in
                 a.copy_src = static_cast<const T*>(P->d_inv);
                 a.copy_stride = P->inv_len;
                 a.exact = sizeof(T) == 8 ? L.exact : 0;
+                // FP32: the panel steps' rank-32 updates (C in the factor) on the SIMT pipes; the
+                // contribution-block (Schur complement) updates on the tensor cores
+                a.simt = (sizeof(T) == 4 && L.cbuf == BUF_FACTOR) ? 1 : 0;
                 e = launch_gemm<T>(a, nm, st);
                 break;
             }

@@ -209,6 +209,92 @@ __global__ void __launch_bounds__(256) gemm_nt_exact_kernel(GemmArgs<double> A) 
         }
 }
 
+// FP32 grouped GEMM on the SIMT pipes for the thin (K = 32) updates of the panel steps: 64 x 64 tile,
+// 256 threads of 4 x 4 entries, K staged 16 at a time in two shared-memory buffers; mode 0 (C -= A B^T,
+// masked to the tile's lower part) and mode 2 (copy) tiles
+__device__ __forceinline__ void cp_async4(void* smem, const void* gmem, bool valid) {
+    unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+    int sz = valid ? 4 : 0;
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4, %2;\n" ::"r"(s), "l"(gmem), "r"(sz));
+}
+
+__global__ void __launch_bounds__(256) gemm_nt_f32_kernel(GemmArgs<float> A) {
+    constexpr int BM = 64, BK = 16, LDS = 68;
+    __shared__ __align__(16) float As[2][BK][LDS];
+    __shared__ __align__(16) float Bs[2][BK][LDS];
+    const GemmTile t = A.tiles[blockIdx.x];
+    const int member = A.members ? A.members[blockIdx.y] : blockIdx.y;
+    if (A.finfo && t.front >= 0 && A.finfo[(int64_t)member * A.ns + t.front] != 0) return;
+    if (t.mode == 2) {   // deferred diagonal-block write
+        const float* src = A.copy_src + (int64_t)member * A.copy_stride + t.a;
+        float* dst = A.cbuf + (int64_t)member * A.cstride + t.c;
+        for (int q = threadIdx.x; q < t.m * t.n; q += blockDim.x) dst[q % t.m + (int64_t)(q / t.m) * t.ldc] = src[q % t.m + (int64_t)(q / t.m) * t.lda];
+        return;
+    }
+    const float* Ab = A.abuf + (int64_t)member * A.astride + t.a;
+    const float* Bb = A.bbuf + (int64_t)member * A.bstride + t.b;
+    float* Cb = A.cbuf + (int64_t)member * A.cstride + t.c;
+    const int tid = threadIdx.x, tx = tid & 15, ty = tid >> 4;
+    const int M = t.m, N = t.n, K = t.k;
+    float acc[4][4];
+#pragma unroll
+    for (int i = 0; i < 4; ++i)
+#pragma unroll
+        for (int j = 0; j < 4; ++j) acc[i][j] = 0.f;
+    auto load = [&](int buf, int k0) {
+#pragma unroll
+        for (int q = 0; q < (BM * BK) / 256; ++q) {
+            int e = tid + 256 * q, r = e % BM, kk = e / BM;
+            bool va = r < M && k0 + kk < K;
+            cp_async4(&As[buf][kk][r], va ? Ab + r + (int64_t)(k0 + kk) * t.lda : Ab, va);
+            bool vb = r < N && k0 + kk < K;
+            cp_async4(&Bs[buf][kk][r], vb ? Bb + r + (int64_t)(k0 + kk) * t.ldb : Bb, vb);
+        }
+        cp_async_commit();
+    };
+    const int nk = (K + BK - 1) / BK;
+    load(0, 0);
+    for (int it = 0; it < nk; ++it) {
+        const int buf = it & 1;
+        if (it + 1 < nk) {
+            load(buf ^ 1, (it + 1) * BK);
+            cp_async_wait<1>();
+        } else {
+            cp_async_wait<0>();
+        }
+        __syncthreads();
+#pragma unroll
+        for (int kk = 0; kk < BK; ++kk) {
+            float a[4], b[4];
+#pragma unroll
+            for (int i = 0; i < 4; ++i) a[i] = As[buf][kk][tx + 16 * i];
+#pragma unroll
+            for (int j = 0; j < 4; ++j) b[j] = Bs[buf][kk][ty + 16 * j];
+#pragma unroll
+            for (int i = 0; i < 4; ++i)
+#pragma unroll
+                for (int j = 0; j < 4; ++j) acc[i][j] += a[i] * b[j];
+        }
+        __syncthreads();
+    }
+    // every C load before the first store (see the DMMA kernel's epilogue)
+    float cv[4][4];
+#pragma unroll
+    for (int i = 0; i < 4; ++i)
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+            const int r = tx + 16 * i, c = ty + 16 * j;
+            cv[i][j] = (r < M && c < N && r + t.diag >= c) ? Cb[r + (int64_t)c * t.ldc] : 0.f;
+        }
+#pragma unroll
+    for (int i = 0; i < 4; ++i)
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+            const int r = tx + 16 * i, c = ty + 16 * j;
+            if (r < M && c < N && r + t.diag >= c) Cb[r + (int64_t)c * t.ldc] = cv[i][j] - acc[i][j];
+        }
+}
+
 template <typename T>
 cudaError_t launch_gemm(const GemmArgs<T>& a, int nmembers, cudaStream_t st) {
     if (a.count == 0) return cudaSuccess;
@@ -217,7 +303,8 @@ cudaError_t launch_gemm(const GemmArgs<T>& a, int nmembers, cudaStream_t st) {
         if (a.exact) gemm_nt_exact_kernel<<<grid, 256, 0, st>>>(a);
         else gemm_nt_dmma_kernel<<<grid, 128, 0, st>>>(a);
     } else {
-        return launch_gemm_tc32(a, nmembers, st);   // 3xTF32 on tcgen05
+        if (a.simt) gemm_nt_f32_kernel<<<grid, 256, 0, st>>>(a);
+        else return launch_gemm_tc32(a, nmembers, st);   // 3xTF32 on tcgen05
     }
     return cudaGetLastError();
 }
@@ -230,10 +317,13 @@ cudaError_t launch_gemm(const GemmArgs<T>& a, int nmembers, cudaStream_t st) {
 // into the panel (a diagonal block with no rows below is written directly by its only task).
 template <typename T>
 __global__ void __launch_bounds__(128) chol_step_kernel(CholStepArgs<T> A) {
+    // the arithmetic type is the factor's: FP32 steps compute in float (one 32-bit shuffle per value,
+    // single-precision reciprocal square root) instead of rounding double results to float
+    using CT = T;
     constexpr int NB = CHOL_NB, LD = NB + 1, TR = 64;
-    __shared__ double L[NB * LD];
-    __shared__ double rdiag[NB];          // reciprocal diagonal of L11 (zero past the block)
-    __shared__ double Bt[TR * LD];
+    __shared__ CT L[NB * LD];
+    __shared__ CT rdiag[NB];          // reciprocal diagonal of L11 (zero past the block)
+    __shared__ CT Bt[TR * LD];
     __shared__ int s_status;
     const CholStepTask task = A.tasks[blockIdx.x];
     const int member = A.members ? A.members[blockIdx.y] : blockIdx.y;
@@ -249,42 +339,43 @@ __global__ void __launch_bounds__(128) chol_step_kernel(CholStepArgs<T> A) {
         // lane i holds row i of the block in registers; L[j][l] comes from lane j by shuffle, so the
         // dependent path of a column is one shuffle, a short reduction and one reciprocal square root
         const int i = lane;
-        double x[NB];
+        CT x[NB];
 #pragma unroll
         for (int j = 0; j < NB; ++j)
-            x[j] = (i < nbb && j < nbb && j <= i) ? (double)P[(kb + i) + (int64_t)(kb + j) * f] : 0.0;
-        const double eps = A.eps;
+            x[j] = (i < nbb && j < nbb && j <= i) ? P[(kb + i) + (int64_t)(kb + j) * f] : CT(0);
+        const CT eps = (CT)A.eps;
         int status = 0;
 #pragma unroll
         for (int j = 0; j < NB; ++j) {
             if (j < nbb && status == 0) {
-                double a0 = 0.0, a1 = 0.0, a2 = 0.0, a3 = 0.0;
+                CT a0 = 0, a1 = 0, a2 = 0, a3 = 0;
 #pragma unroll
                 for (int l = 0; l < j; ++l) {
-                    const double t = x[l] * __shfl_sync(0xffffffffu, x[l], j);
+                    const CT t = x[l] * __shfl_sync(0xffffffffu, x[l], j);
                     if ((l & 3) == 0) a0 += t;
                     else if ((l & 3) == 1) a1 += t;
                     else if ((l & 3) == 2) a2 += t;
                     else a3 += t;
                 }
-                const double sv = x[j] - ((a0 + a1) + (a2 + a3));
-                const double ajj = __shfl_sync(0xffffffffu, sv, j);
+                const CT sv = x[j] - ((a0 + a1) + (a2 + a3));
+                const CT ajj = __shfl_sync(0xffffffffu, sv, j);
                 if (!(ajj > eps || (eps > 0 && ajj >= 0))) {
                     status = j + 1;
                 } else {
-                    const double r = rsqrt(fmax(ajj, eps));
+                    const CT d = ajj > eps ? ajj : eps;
+                    const CT r = rsqrt(d);
                     if (i == j) {
-                        x[j] = (double)T(fmax(ajj, eps) * r);
+                        x[j] = d * r;
                         rdiag[j] = r;
                     } else if (i > j && i < nbb) {
-                        x[j] = (double)T(sv * r);
+                        x[j] = sv * r;
                     }
                 }
             }
         }
 #pragma unroll
         for (int j = 0; j < NB; ++j) L[i * LD + j] = x[j];
-        if (i >= nbb) rdiag[i] = 0.0;   // reciprocal diagonal beyond the block: zero
+        if (i >= nbb) rdiag[i] = CT(0);   // reciprocal diagonal beyond the block: zero
         if (lane == 0) s_status = status;
     } else {
         batched_copy<8>(tid - 32, 96, TR * NB,
@@ -292,7 +383,7 @@ __global__ void __launch_bounds__(128) chol_step_kernel(CholStepArgs<T> A) {
                             const int r = q % TR, c = q / TR;
                             return (r < rows && c < nbb) ? (double)P[(row0 + r) + (int64_t)(kb + c) * f] : 0.0;
                         },
-                        [&](int q, double v) { Bt[(q % TR) * LD + q / TR] = v; });
+                        [&](int q, double v) { Bt[(q % TR) * LD + q / TR] = (CT)v; });
     }
     __syncthreads();
     if (finfo[s] != 0) return;   // an earlier step of this front failed
@@ -325,13 +416,13 @@ __global__ void __launch_bounds__(128) chol_step_kernel(CholStepArgs<T> A) {
     // the block have a zero reciprocal diagonal and come out zero
     const int r = tid;
     if (r < rows) {
-        double x[NB];
+        CT x[NB];
 #pragma unroll
         for (int j = 0; j < NB; ++j) {
-            double a0 = Bt[r * LD + j], a1 = 0.0, a2 = 0.0, a3 = 0.0;
+            CT a0 = Bt[r * LD + j], a1 = 0, a2 = 0, a3 = 0;
 #pragma unroll
             for (int l = 0; l < j; ++l) {
-                const double t = x[l] * L[j * LD + l];
+                const CT t = x[l] * L[j * LD + l];
                 if ((l & 3) == 0) a0 -= t;
                 else if ((l & 3) == 1) a1 -= t;
                 else if ((l & 3) == 2) a2 -= t;

@@ -104,6 +104,7 @@ struct GemmArgs {
     int64_t copy_stride;   // per-member stride of copy_src
     int32_t exact;     // FP64 mode-0 tiles summed in the oracle's order, every product and sum rounded:
                        // 1 (LDLT) c = c - a_k b_k for k = 0, 1, ...; 2 (LU) c = c - (a_0 b_0 + a_1 b_1 + ...)
+    int32_t simt;      // FP32: the SIMT kernel (the panel steps' rank-32 updates) instead of tcgen05
 };
 
 // FP32 grouped GEMM on the tensor cores (tcgen05, 3xTF32); tc_kernels.cu
