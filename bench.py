@@ -292,8 +292,8 @@ def run_config(args):
 
 
 def profiled_traffic(form):
-    """DRAM bytes per launch of the persistent solve from the committed ncu summary, or None."""
-    path = os.path.join(ROOT, "profiles", f"persistent_solve_{form}_lap3d48.md")
+    """DRAM bytes per launch of the dataflow solve from the committed ncu summary, or None."""
+    path = os.path.join(ROOT, "profiles", f"dataflow_solve_{form}_lap3d48.md")
     try:
         for line in open(path):
             if line.startswith("traffic_bytes_per_launch:"):
@@ -365,13 +365,14 @@ class ClockSampler:
                 "samples": len(sm)}
 
 
-def measured_gemm_peak(torch, dtype):
-    """Dense GEMM throughput of cuBLAS on this GPU (TFLOP/s), best of a few 8192^3 products."""
+def measured_gemm_peak(torch, dtype, tf32=False):
+    """Dense GEMM throughput of cuBLAS on this GPU (TFLOP/s), best of a few 8192^3 products. tf32: FP32
+    operands on the tensor cores (TF32), the unit the 3xTF32 contribution-block updates run on."""
     n = 8192
     a = torch.randn(n, n, device="cuda", dtype=dtype)
     bm = torch.randn(n, n, device="cuda", dtype=dtype)
     prev = torch.backends.cuda.matmul.allow_tf32
-    torch.backends.cuda.matmul.allow_tf32 = False
+    torch.backends.cuda.matmul.allow_tf32 = bool(tf32)
     for _ in range(2):
         torch.matmul(a, bm)
     best = 0.0
@@ -572,7 +573,7 @@ def main():
         torch.cuda.synchronize()
         kinds = {}
         for k in ("small", "assemble", "panel", "gemm", "pivot", "scale", "stats", "fwd", "bwd", "diag", "permute",
-                  "residual"):
+                  "residual", "inv"):
             ms_k = lib.sdsb200_plan_stat(ds._plan, f"prof_ms:{k}".encode())
             if ms_k > 0:
                 kinds[k] = dict(ms=ms_k, flops=lib.sdsb200_plan_stat(ds._plan, f"prof_flops:{k}".encode()),
@@ -584,6 +585,7 @@ def main():
     peaks, peak_kind = measured_peaks()
     fp64_peak = measured_gemm_peak(torch, torch.float64)
     fp32_peak = measured_gemm_peak(torch, torch.float32)
+    tf32_peak = measured_gemm_peak(torch, torch.float32, tf32=True)
     head = "mixed"
     kinds = prof[head]
     dom = max(kinds, key=lambda k: kinds[k]["ms"]) if kinds else None
@@ -592,11 +594,18 @@ def main():
         d = kinds[dom]
         per_launch_ms = d["ms"] / max(d["launches"], 1)
         if dom in ("gemm", "panel", "pivot"):
-            peak = fp32_peak if head == "mixed" else fp64_peak
+            if head != "mixed":
+                peak, bound, src = fp64_peak, "fp64", "cuBLAS FP64 GEMM measured in this run (DMMA tensor path)"
+            elif dom == "gemm":
+                # the FP32 form's updates: 3xTF32 on tcgen05 (three tensor products per product) and the
+                # steps' thin updates on the SIMT pipes; the tensor bound is a third of TF32
+                peak, bound, src = tf32_peak / 3.0, "tf32x3", "cuBLAS TF32 GEMM measured in this run, / 3 (3xTF32)"
+            else:
+                peak, bound, src = fp32_peak, "fp32", "cuBLAS FP32 GEMM measured in this run (SIMT)"
             ach = d["flops"] / (d["ms"] / 1e3) / 1e12
-            roofline = {"kernel": dom, "bound": "fp32" if head == "mixed" else "fp64", "achieved": round(ach, 3),
+            roofline = {"kernel": dom, "bound": bound, "achieved": round(ach, 3),
                         "peak": round(peak, 3), "unit": "TFLOP/s", "frac": round(ach / peak, 4),
-                        "peak_source": "cuBLAS GEMM of the same precision measured in this run (no tensor cores)",
+                        "peak_source": src,
                         "traffic": None, "launches": d["launches"], "ms_per_launch": round(per_launch_ms, 4)}
         else:
             peak = float(peaks.get("hbm_gbs", 6650.0))
@@ -605,7 +614,7 @@ def main():
             roofline = {"kernel": dom, "bound": "hbm", "achieved": round(ach, 2), "peak": peak, "unit": "GB/s",
                         "frac": round(ach / peak, 4), "peak_source": f"MEASURED_PEAKS.json hbm_gbs ({peak_kind})",
                         "traffic": traffic, "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum, "
-                        f"profiles/persistent_solve_{head}_lap3d48.md" if traffic else None,
+                        f"profiles/dataflow_solve_{head}_lap3d48.md" if traffic else None,
                         "algorithmic_bytes_per_launch": round(d["bytes"] / max(d["launches"], 1)),
                         "launches": d["launches"], "ms_per_launch": round(per_launch_ms, 4)}
 
@@ -680,6 +689,7 @@ def main():
         "kernel_profile": {k: {kk: {"ms": round(v["ms"], 4), "launches": v["launches"]} for kk, v in prof[k].items()}
                            for k in prof},
         "peaks": {"fp64_gemm_tflops_measured": round(fp64_peak, 2), "fp32_gemm_tflops_measured": round(fp32_peak, 2),
+                  "tf32_gemm_tflops_measured": round(tf32_peak, 2),
                   "hbm_gbs": peaks.get("hbm_gbs"), "source": peak_kind},
         "cpu_baseline": cpu,
         "e2e": e2e,

@@ -102,9 +102,9 @@ typedef struct sdsb200_plan_options {
 
 /* Plan tuning (the shapes an autotuner chooses; no counterpart in the reference):
  * fsmall = the largest front order handled by the shared-memory small-front kernel (one of 32, 64,
- * 96, 128, 160, and 224 for FP32; 0 = the largest class); wide, area = a front is "wide" in the
- * solve, its columns split into 64-column block steps over the whole grid, when its width is at
- * least `wide` (16..2047, 0 = 96) or (f - w) * w is at least 1024 * area (area 1..2047, 0 = 8). */
+ * 96, 128, 160, and 224 for FP32; 0 = the largest class); wide = the tallest front (at most 32
+ * columns) that the dataflow solve gives to one warp, larger fronts going to 64-row tile tasks
+ * (16..128, 0 = 128); area: reserved (ignored). */
 #define SDSB200_TUNING(fsmall, wide, area) \
     ((int32_t)(fsmall) | ((int32_t)(wide) << 9) | ((int32_t)(area) << 20))
 
@@ -199,22 +199,19 @@ int sdsb200_set_interrupt(sdsb200_plan* plan, const volatile int32_t* h_flag);
  * then polled before a factorization and before each refinement step, not between launch groups. */
 int sdsb200_set_graphs(sdsb200_plan* plan, int32_t on);
 
-/* Solve engine when a single batch member is active. 1 (default): the dataflow solve, one cooperative
- * persistent launch per group of 8 right-hand sides with no grid barrier (tasks in a topological order
- * of the elimination tree, synchronised by per-front counters and per-block flags); 2: one cooperative
- * launch with a grid barrier per tree level; 0: one launch per level and sweep (the engine of uniform
- * batches and of the solve sub-phases). */
+/* Solve engine when a single batch member is active. Nonzero (default): the dataflow solve, one
+ * cooperative persistent launch per group of 8 right-hand sides with no grid barrier (tasks in a
+ * topological order of the elimination tree, synchronised by per-front counters and per-block flags);
+ * 0: one launch per level and sweep (the engine of uniform batches and of the solve sub-phases). */
 int sdsb200_set_persistent(sdsb200_plan* plan, int32_t on);
 
 /* Profiling mode (on != 0): CUDA events around every launch of the following factor and solve
  * calls, accumulated per kernel kind (resets the totals). Costs one event record per launch. */
 int sdsb200_set_profiling(sdsb200_plan* plan, int32_t on);
 
-/* Profiling: copy up to cap (tag, nanoseconds) pairs of the level-kernel solve's phase stamps (written
- * when profiling is on; tag = kind << 40 | level << 16 | step). Returns the pairs copied or -1. With
- * cap < 0: the dataflow solve's task trace of its last launch, 6 int64 per task (task start, end of its
- * dependency wait, task end in ns of %globaltimer; CTA; task kind; a | b << 32), up to -cap tasks;
- * returns the tasks copied. */
+/* Profiling: the dataflow solve's task trace of its last launch made while profiling was on, 6 int64
+ * per task for up to cap tasks (task start, end of its dependency wait and task end in ns of
+ * %globaltimer; CTA; task kind; a | b << 32 of the task record). Returns the tasks copied or -1. */
 int64_t sdsb200_get_trace(sdsb200_plan* plan, int64_t* h_out, int64_t cap);
 
 /* Plan facts: "ns", "nlevels", "factor_len", "cb_len", "launches_factor", "launches_solve",

@@ -92,7 +92,6 @@ int prof_kind_of(LaunchKind k) {
         case L_GEMM: return PK_GEMM;
         case L_PIVOT_FRONT: return PK_PIVOT;
         case L_SCALE: return PK_SCALE;
-        case L_BLOCKINV: return PK_INV;
         case L_DFINV: return PK_INV;
         default: return PK_STATS;
     }
@@ -277,27 +276,6 @@ int run_factor(Plan* P, const double* nzval, double eps, double u, int pivot, in
                 e = launch_scale_ld_front<T>(P->structure, a, L.maxw, nm, st);
                 break;
             }
-            case L_BLOCKINV: {
-                BlockInvArgs<T> a{};
-                a.fronts = P->d_fronts;
-                a.tasks = P->d_binv_tasks;
-                a.count = P->n_binv_tasks;
-                a.dinv_off = P->d_dinv_off;
-                a.members = members;
-                a.panels = factor;
-                a.dinv = static_cast<T*>(P->d_dinv_L);
-                a.factor_len = P->factor_len;
-                a.dinv_len = P->dinv_len;
-                a.finfo = P->d_finfo;
-                a.ns = (int32_t)P->ns;
-                e = launch_block_inv<T>(a, nm, st);
-                if (e == cudaSuccess && P->structure == STRUCT_G) {
-                    a.panels = ufactor;
-                    a.dinv = static_cast<T*>(P->d_dinv_U);
-                    e = launch_block_inv<T>(a, nm, st);
-                }
-                break;
-            }
             case L_DFINV: {
                 // the dataflow solve's inverses: L11^-1 of the warp fronts, 64 x 64 diagonal blocks of
                 // the tiled fronts (of the L panels, and of the U^T panels for LU)
@@ -441,82 +419,6 @@ int run_sweeps(Plan* P, int nrhs, bool transpose, cudaStream_t st, int which) {
     return SDSB200_OK;
 }
 
-constexpr int SOLVE_THREADS_HOST = 256;   // threads of the persistent solve kernel
-
-// the whole solve in one cooperative launch (one active batch member)
-template <typename T>
-int run_persistent(Plan* P, int nrhs, bool transpose, const double* in, int64_t ldin, double* out, int64_t ldout,
-                   int mode, cudaStream_t st) {
-    const bool gen = P->structure == STRUCT_G, ldl = P->structure == STRUCT_S;
-    const int32_t member = 0;
-    (void)member;
-    PersistArgs<T> a{};
-    SweepArgs<T> base{};
-    base.fronts = P->d_fronts;
-    base.members = nullptr;
-    base.Y = P->d_Y;
-    base.U = P->d_U;
-    base.uoff = P->d_uoff;
-    base.child_list = P->maps.child_list;
-    base.relind = P->maps.relind;
-    base.rowval = P->maps.rowval;
-    base.piv = P->d_piv;
-    base.n = P->n; base.factor_len = P->factor_len; base.ulen = P->ulen;
-    base.nrhs = nrhs;
-    base.unit = P->structure != STRUCT_SPD;
-    base.rect = 1;
-    const T* factor = static_cast<const T*>(P->d_factor);
-    const T* ufactor = static_cast<const T*>(P->d_ufactor);
-    const T* dL = static_cast<const T*>(P->d_dinv_L);
-    const T* dU = static_cast<const T*>(P->d_dinv_U);
-    a.fw = base;
-    a.fw.fac = (gen && transpose) ? ufactor : factor;
-    a.fw.reorder = ldl || (gen && !transpose);
-    a.bw = base;
-    a.bw.fac = (gen && !transpose) ? ufactor : factor;
-    a.bw.reorder = ldl || (gen && transpose);
-    a.dinv_fw = (gen && transpose) ? dU : dL;
-    a.dinv_bw = (gen && !transpose) ? dU : dL;
-    a.dinv_off = P->d_dinv_off;
-    a.lev_small = P->d_p_lev_small;
-    a.lev_large = P->d_p_lev_large;
-    a.lev_maxblk = P->d_p_lev_maxblk;
-    a.list = P->d_p_list;
-    a.nlevels = P->nlevels;
-    a.d = P->d_d;
-    a.kind = P->d_kind;
-    a.diag_mode = P->structure == STRUCT_SPD ? 0 : (ldl ? 2 : 1);
-    a.perm = P->d_perm0;
-    a.in = in; a.ldin = ldin; a.out = out; a.ldout = ldout; a.mode = mode;
-    a.xtmp = P->d_xtmp;
-    a.barrier = P->d_barrier;
-    a.blkflag = P->d_blkflag;
-    a.pullflag = P->d_blkflag + P->n_blkflag;
-    a.l21cnt = P->d_blkflag + 2 * P->n_blkflag;
-    a.status = P->d_solve_status;
-    a.trace = P->profile ? P->d_trace : nullptr;
-    a.trace_cap = Plan::TRACE_CAP;
-    // wide tiles: the inverse block, y_b, x_b and 4 partial sums per rhs (at most 8 per pass)
-    const size_t wide = (size_t)SOLVE_BLK * (SOLVE_BLK + 1) + 2 * SOLVE_BLK * (size_t)nrhs +
-                        4 * SOLVE_BLK * (size_t)std::min(nrhs, 8);
-    // small fronts: one warp each, xs (w x nrhs) and the staged diagonal block (32 x 33) per warp
-    a.warp_xs = (int32_t)(((size_t)P->p_maxw_small * nrhs + 1) & ~size_t(1));
-    a.warp_smem = a.warp_xs + 32 * 33;
-    const size_t smem = sizeof(double) * std::max<size_t>((size_t)a.warp_smem * (SOLVE_THREADS_HOST / 32), wide);
-    const int grid = persistent_solve_grid<T>(smem);
-    if (grid <= 0) return fail(SDSB200_CUDA_ERROR, "no co-resident grid for the persistent solve");
-    CK(cudaMemsetAsync(P->d_barrier, 0, sizeof(unsigned int), st), "barrier reset");
-    CK(cudaMemsetAsync(P->d_blkflag, 0, sizeof(unsigned int) * 3 * P->n_blkflag, st), "block flag reset");
-    prof_begin(P, st);
-    cudaError_t e = launch_persistent_solve<T>(a, grid, smem, st);
-    // algorithmic work: every stored panel entry read once per sweep (2 flops per entry and rhs each
-    // way), Y and the right-hand side read, the solution written
-    double ent = 0.0;
-    for (double v : P->level_panel_entries) ent += v;
-    prof_end(P, st, PK_FWD, 4.0 * ent * nrhs, 2.0 * sizeof(T) * ent + 24.0 * P->n * nrhs);
-    return e == cudaSuccess ? SDSB200_OK : cuda_fail(e, "persistent solve");
-}
-
 // the whole solve as dataflow tasks in one persistent launch per group of up to DF_MAX_NRHS
 // right-hand sides (solve_dataflow.cu)
 template <typename T>
@@ -588,14 +490,11 @@ int run_dataflow(Plan* P, int nrhs, bool transpose, const double* in, int64_t ld
     return SDSB200_OK;
 }
 
-// the one-launch solve of a single active member: the dataflow kernel (default) or the level kernel
+// the one-launch solve of a single active member
 int run_one_launch(Plan* P, int nrhs, bool transpose, const double* in, int64_t ldin, double* out, int64_t ldout,
                    int mode, cudaStream_t st) {
-    if (P->dataflow)
-        return P->elsize == 8 ? run_dataflow<double>(P, nrhs, transpose, in, ldin, out, ldout, mode, st)
-                              : run_dataflow<float>(P, nrhs, transpose, in, ldin, out, ldout, mode, st);
-    return P->elsize == 8 ? run_persistent<double>(P, nrhs, transpose, in, ldin, out, ldout, mode, st)
-                          : run_persistent<float>(P, nrhs, transpose, in, ldin, out, ldout, mode, st);
+    return P->elsize == 8 ? run_dataflow<double>(P, nrhs, transpose, in, ldin, out, ldout, mode, st)
+                          : run_dataflow<float>(P, nrhs, transpose, in, ldin, out, ldout, mode, st);
 }
 
 bool use_persistent(const Plan* P) { return P->nact == 1 && P->all_members && P->persistent; }
@@ -980,24 +879,18 @@ int sdsb200_set_members(sdsb200_plan* plan, const int32_t* h_members, int32_t na
 
 int64_t sdsb200_get_trace(sdsb200_plan* plan, int64_t* h_out, int64_t cap) {
     Plan* P = reinterpret_cast<Plan*>(plan);
-    if (!P || !h_out) return -1;
-    if (cap < 0) {
-        // the dataflow solve's task trace of its last launch: 6 int64 per task (start and end of the task
-        // and the end of its dependency wait in %globaltimer ns, CTA, kind, a | b << 32), up to -cap tasks
-        int64_t nt = std::min<int64_t>(-cap, P->n_df_tasks);
-        if (cudaMemcpy(h_out, P->d_df_trace, sizeof(int64_t) * 6 * nt, cudaMemcpyDeviceToHost) != cudaSuccess) return -1;
-        return nt;
-    }
-    int64_t n = std::min<int64_t>(cap, Plan::TRACE_CAP);
-    if (cudaMemcpy(h_out, P->d_trace, sizeof(int64_t) * 2 * n, cudaMemcpyDeviceToHost) != cudaSuccess) return -1;
-    return n;
+    if (!P || !h_out || cap < 0) return -1;
+    // the dataflow solve's task trace of its last profiled launch: 6 int64 per task (start and end of the
+    // task and the end of its dependency wait in %globaltimer ns, CTA, kind, a | b << 32)
+    const int64_t nt = std::min<int64_t>(cap, P->n_df_tasks);
+    if (cudaMemcpy(h_out, P->d_df_trace, sizeof(int64_t) * 6 * nt, cudaMemcpyDeviceToHost) != cudaSuccess) return -1;
+    return nt;
 }
 
 int sdsb200_set_persistent(sdsb200_plan* plan, int32_t on) {
     Plan* P = reinterpret_cast<Plan*>(plan);
     if (!P) return fail(SDSB200_INVALID_VALUE, "plan is NULL");
     P->persistent = on != 0;
-    P->dataflow = on != 2;
     for (Plan::CachedGraph* g : {&P->g_solve, &P->g_corr})
         g->key.clear();
     return SDSB200_OK;
@@ -1015,7 +908,7 @@ int sdsb200_set_profiling(sdsb200_plan* plan, int32_t on) {
     if (!P) return fail(SDSB200_INVALID_VALUE, "plan is NULL");
     P->profile = on != 0;
     P->records.clear();
-    cudaMemset(P->d_trace, 0, sizeof(int64_t) * 2 * Plan::TRACE_CAP);
+    cudaMemset(P->d_df_trace, 0, sizeof(int64_t) * 6 * std::max<int64_t>(1, P->n_df_tasks));
     for (int k = 0; k < PK_COUNT; ++k) P->prof[k] = ProfAcc();
     P->pending.clear();
     P->prof_next = 0;
@@ -1127,7 +1020,7 @@ extern "C" int sdsb200_sampled_outer(int64_t n, int64_t nnz, const void* rowptr,
 }
 
 // ---------------------------------------------------------------------------
-// sdsb200_solve_noalloc: the persistent solve with its working vectors in a static device array, for
+// sdsb200_solve_noalloc: the dataflow solve with its working vectors in a static device array, for
 // callers that may not allocate device memory after set-up. In host code the array's name is only a
 // host-side stand-in: its device address comes from cudaGetSymbolAddress, once per device.
 static __device__ __align__(256) unsigned char g_noalloc_scratch[SDSB200_NOALLOC_SCRATCH_BYTES];
@@ -1137,7 +1030,7 @@ static __device__ __align__(256) unsigned char g_noalloc_scratch[SDSB200_NOALLOC
 namespace {
 
 constexpr int NOALLOC_MAX_DEVICES = 64;
-constexpr size_t NOALLOC_HEADER = 512;   // barrier counter at 0, fallback status word at 256
+constexpr size_t NOALLOC_HEADER = 512;   // the fallback status word at 256 (the first bytes unused)
 std::mutex g_noalloc_mu;
 void* g_noalloc_base[NOALLOC_MAX_DEVICES] = {};
 
@@ -1163,12 +1056,12 @@ int noalloc_base(void** out) {
 // arguments, on the host, before this returns).
 struct ScratchSwap {
     Plan* P;
-    double* Y; double* U; double* xtmp; unsigned int* barrier; int32_t* status;
-    ScratchSwap(Plan* p, double* y, double* u, double* xt, unsigned int* bar, int32_t* st)
-        : P(p), Y(p->d_Y), U(p->d_U), xtmp(p->d_xtmp), barrier(p->d_barrier), status(p->d_solve_status) {
-        P->d_Y = y; P->d_U = u; P->d_xtmp = xt; P->d_barrier = bar; P->d_solve_status = st;
+    double* Y; double* U; double* xtmp; int32_t* status;
+    ScratchSwap(Plan* p, double* y, double* u, double* xt, int32_t* st)
+        : P(p), Y(p->d_Y), U(p->d_U), xtmp(p->d_xtmp), status(p->d_solve_status) {
+        P->d_Y = y; P->d_U = u; P->d_xtmp = xt; P->d_solve_status = st;
     }
-    ~ScratchSwap() { P->d_Y = Y; P->d_U = U; P->d_xtmp = xtmp; P->d_barrier = barrier; P->d_solve_status = status; }
+    ~ScratchSwap() { P->d_Y = Y; P->d_U = U; P->d_xtmp = xtmp; P->d_solve_status = status; }
 };
 
 }  // namespace
@@ -1204,7 +1097,6 @@ int sdsb200_solve_noalloc(sdsb200_plan* plan, double* X, int64_t ldx, const doub
     int rc = noalloc_base(&base);
     if (rc) return rc;
     unsigned char* b = static_cast<unsigned char*>(base);
-    unsigned int* bar = reinterpret_cast<unsigned int*>(b);
     int32_t* st_word = status ? status : reinterpret_cast<int32_t*>(b + 256);
     double* Y = reinterpret_cast<double*>(b + NOALLOC_HEADER);
     double* xt = Y + vec;
@@ -1216,7 +1108,7 @@ int sdsb200_solve_noalloc(sdsb200_plan* plan, double* X, int64_t ldx, const doub
     const bool transpose = P->structure == STRUCT_G && solve_mode != 0;
     P->launches_done = 0;
     {
-        ScratchSwap swap(P, Y, U, xt, bar, st_word);
+        ScratchSwap swap(P, Y, U, xt, st_word);
         rc = run_one_launch(P, nrhs, transpose, B, ldb, X, ldx, 0, st);
     }
     if (rc || status) return rc;

@@ -76,7 +76,6 @@ enum LaunchKind : int32_t {
     L_PIVOT_FRONT,     // large LDLT / LU: cooperative pivoting over the panel
     L_STATS,           // statistics reduction
     L_SCALE,           // W = L21 D of large LDLT / LU fronts
-    L_BLOCKINV,        // inverses of the diagonal blocks of the wide fronts (solve)
     L_CHOL_STEP,       // large Cholesky: one 32-column step (diagonal block + trsm of the rows below)
     L_DFINV,           // diagonal-block inverses of every front for the dataflow solve
 };

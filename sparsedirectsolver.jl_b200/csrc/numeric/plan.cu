@@ -268,13 +268,16 @@ Plan* build_plan(const sdsb200_symbolic* sym, const sdsb200_plan_options* popts,
                                                   : std::vector<int>{32, 64, 96, 128, 160, 224};
         const int tune_fsmall = popts ? (popts->tuning & 0x1FF) : 0;
         const int tune_wide = popts ? ((popts->tuning >> 9) & 0x7FF) : 0;
-        const int tune_area = popts ? ((popts->tuning >> 20) & 0x7FF) : 0;
+        const int tune_rsv = popts ? ((popts->tuning >> 20) & 0x7FF) : 0;
         if (tune_fsmall) {
             if (std::find(classes.begin(), classes.end(), tune_fsmall) == classes.end())
                 throw BuildError(SDSB200_INVALID_VALUE, "tuning: fsmall must be one of the front classes");
             while (classes.back() > tune_fsmall) classes.pop_back();
         }
-        if (tune_wide && tune_wide < 16) throw BuildError(SDSB200_INVALID_VALUE, "tuning: wide must lie in 16..2047");
+        if (tune_wide && (tune_wide < 16 || tune_wide > DF_WARP_F))
+            throw BuildError(SDSB200_INVALID_VALUE, "tuning: wide (the tallest warp front of the solve) must lie in 16..128");
+        (void)tune_rsv;   // bits 20..30: reserved, ignored
+        const int warp_f = tune_wide ? tune_wide : DF_WARP_F;
         P->fsmall_max = classes.back();
         auto class_of = [&](int f) {
             for (int c : classes)
@@ -536,31 +539,6 @@ Plan* build_plan(const sdsb200_symbolic* sym, const sdsb200_plan_options* popts,
                 }
             }
         }
-        // solve-wide fronts: inverses of their 64 x 64 diagonal blocks, computed after the factorization
-        std::vector<int64_t> dinv_off(ns, -1);
-        std::vector<int32_t> binv_tasks;
-        const int wide_w = tune_wide ? tune_wide : 96;
-        const int64_t wide_area = 1024 * (int64_t)(tune_area ? tune_area : 8);
-        auto solve_wide = [&](const DFront& F) { return F.w >= wide_w || (int64_t)(F.f - F.w) * F.w >= wide_area; };
-        for (int64_t s = 0; s < ns; ++s) {
-            const DFront& F = P->fronts[s];
-            if (!solve_wide(F) || s == P->schur_front) continue;
-            dinv_off[s] = P->dinv_len;
-            int nblk = (F.w + SOLVE_BLK - 1) / SOLVE_BLK;
-            for (int b = 0; b < nblk; ++b) {
-                binv_tasks.push_back((int32_t)s);
-                binv_tasks.push_back(b);
-            }
-            P->dinv_len += (int64_t)nblk * SOLVE_BLK * SOLVE_BLK;
-        }
-        P->n_binv_tasks = (int)(binv_tasks.size() / 2);
-        if (P->n_binv_tasks) {
-            ProgLaunch bl{};
-            bl.kind = L_BLOCKINV;
-            bl.level = P->nlevels;
-            bl.count = P->n_binv_tasks;
-            P->prog.push_back(bl);
-        }
         // dataflow solve: front classes, task list, inverse layout, contribution lists (solve.cuh)
         {
             std::vector<DfFront> df(ns);
@@ -574,7 +552,7 @@ Plan* build_plan(const sdsb200_symbolic* sym, const sdsb200_plan_options* popts,
                 d = DfFront{};
                 if (s == P->schur_front) continue;
                 const int m = F.f - F.w;
-                d.tiled = !(F.w <= DF_WARP_W && F.f <= DF_WARP_F);
+                d.tiled = !(F.w <= DF_WARP_W && F.f <= warp_f);
                 d.inv = inv_off[s] = il;
                 if (!d.tiled) {
                     il += ((int64_t)F.w * F.w + 1) & ~int64_t(1);
@@ -693,32 +671,6 @@ Plan* build_plan(const sdsb200_symbolic* sym, const sdsb200_plan_options* popts,
             pl.kind = L_STATS;
             P->prog.push_back(pl);
         }
-        // persistent solve lists
-        {
-            std::vector<int32_t> plist, psmall(2 * P->nlevels), plarge(2 * P->nlevels), pmaxblk(P->nlevels, 0);
-            for (int L = 0; L < P->nlevels; ++L) {
-                psmall[2 * L] = (int32_t)plist.size();
-                for (int s : P->level_fronts[L])
-                    if (!solve_wide(P->fronts[s]) && s != P->schur_front) {
-                        plist.push_back(s);
-                        P->p_maxw_small = std::max(P->p_maxw_small, P->fronts[s].w);
-                    }
-                psmall[2 * L + 1] = (int32_t)plist.size() - psmall[2 * L];
-                plarge[2 * L] = (int32_t)plist.size();
-                for (int s : P->level_fronts[L])
-                    if (solve_wide(P->fronts[s]) && s != P->schur_front) {
-                        plist.push_back(s);
-                        pmaxblk[L] = std::max(pmaxblk[L], (P->fronts[s].w + SOLVE_BLK - 1) / SOLVE_BLK);
-                    }
-                plarge[2 * L + 1] = (int32_t)plist.size() - plarge[2 * L];
-            }
-            P->d_p_list = upload(P, plist, st);
-            P->d_p_lev_small = upload(P, psmall, st);
-            P->d_p_lev_large = upload(P, plarge, st);
-            P->d_p_lev_maxblk = upload(P, pmaxblk, st);
-        }
-        P->d_dinv_off = upload(P, dinv_off, st);
-        P->d_binv_tasks = upload(P, binv_tasks, st);
         P->launches_factor = (int)P->prog.size();
 
         // solve: update vectors, per-level lists
@@ -918,18 +870,10 @@ Plan* build_plan(const sdsb200_symbolic* sym, const sdsb200_plan_options* popts,
         if (P->scr_len) P->d_scratch = dalloc<double>(P, P->scr_len * nb);
         if (P->work_len) P->d_work = alloc_bytes(es * P->work_len * nb);
         if (P->inv_len) P->d_inv = alloc_bytes(es * P->inv_len * nb);
-        if (P->dinv_len) {
-            P->d_dinv_L = alloc_bytes(es * P->dinv_len * nb);
-            if (gen) P->d_dinv_U = alloc_bytes(es * P->dinv_len * nb);
-        }
         P->d_dfinv_L = alloc_bytes(es * P->df_inv_len * nb);
         if (gen) P->d_dfinv_U = alloc_bytes(es * P->df_inv_len * nb);
         P->d_xtmp = dalloc<double>(P, n * P->max_nrhs);
-        P->d_barrier = dalloc<unsigned int>(P, 1);
-        P->n_blkflag = std::max<int64_t>(1, P->dinv_len / ((int64_t)SOLVE_BLK * SOLVE_BLK));
-        P->d_blkflag = dalloc<unsigned int>(P, 3 * P->n_blkflag);   // block flags, pull flags, L21 counts
         P->d_solve_status = dalloc<int32_t>(P, 1);
-        P->d_trace = dalloc<int64_t>(P, 2 * Plan::TRACE_CAP);
         cudaMemsetAsync(P->d_solve_status, 0, sizeof(int32_t), st);
         P->d_Y = dalloc<double>(P, n * P->max_nrhs * nb);
         P->d_U = dalloc<double>(P, P->ulen * nb);

@@ -94,18 +94,6 @@ struct Plan {
     int32_t* d_level_lists = nullptr;   // fronts of each level for the solve sweeps: small first, then large
     std::vector<int64_t> level_list_off;
     std::vector<int> level_nsmall, level_nlarge, level_maxw_small, level_maxw_large;
-    // persistent solve: fronts by level (small, then wide), the diagonal-block inverses of the wide fronts
-    int32_t* d_p_list = nullptr;
-    int32_t* d_p_lev_small = nullptr;
-    int32_t* d_p_lev_large = nullptr;
-    int32_t* d_p_lev_maxblk = nullptr;
-    int p_maxw_small = 1;
-    int64_t dinv_len = 0;
-    int64_t* d_dinv_off = nullptr;
-    void* d_dinv_L = nullptr;
-    void* d_dinv_U = nullptr;
-    int32_t* d_binv_tasks = nullptr;
-    int n_binv_tasks = 0;
     // dataflow solve (solve.cuh): per-front classes, the task list, the inverses of every front's diagonal
     // blocks (warp fronts: w x w; tiled fronts: 64 x 64 blocks), flags and counters zeroed per launch
     DfFront* d_df = nullptr;
@@ -128,14 +116,8 @@ struct Plan {
     double* d_df_part = nullptr;        // backward partial sums: slots of 64 x DF_MAX_NRHS doubles
     int64_t* d_df_trace = nullptr;      // profiling: 6 int64 per task (start, wait done, end, CTA, kind, a | b << 32)
     int32_t df_fwarp_max = 1;           // tallest warp front
-    bool dataflow = true;               // the dataflow kernel for the one-launch solve (else the level kernel)
     double* d_xtmp = nullptr;
-    unsigned int* d_barrier = nullptr;
-    unsigned int* d_blkflag = nullptr;   // persistent solve: 3 x n_blkflag words (block flags, pull flags,
-    int64_t n_blkflag = 0;               // L21 counts), one per 64-column block of the wide fronts
     int32_t* d_solve_status = nullptr;
-    int64_t* d_trace = nullptr;   // persistent-solve phase stamps (profiling)
-    static constexpr int TRACE_CAP = 16384;
     int32_t* d_rect_tiles = nullptr;    // (front, start) pairs: forward row tiles, backward column tiles
     std::vector<int64_t> level_ftile_off, level_btile_off;
     std::vector<int> level_nftile, level_nbtile;
@@ -168,7 +150,7 @@ struct Plan {
         int64_t launches = 0;
     };
     bool use_graphs = true;
-    bool persistent = true;        // the one-launch cooperative solve for a single active member
+    bool persistent = true;        // the one-launch dataflow solve for a single active member
     cudaStream_t own = nullptr;          // capture / replay stream, joined to the caller's by events
     cudaEvent_t join_in = nullptr, join_out = nullptr;
     CachedGraph g_factor, g_solve, g_resid, g_corr;

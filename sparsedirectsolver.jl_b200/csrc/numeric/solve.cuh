@@ -30,42 +30,6 @@ struct SweepArgs {
     const int32_t* tiles;      // split rectangular part of large fronts: (front, first row / column) pairs
 };
 
-// One cooperative launch for a whole solve (nact == 1): permutation, forward levels, diagonal,
-// backward levels, inverse permutation, separated by bounded grid barriers.
-template <typename T>
-struct PersistArgs {
-    SweepArgs<T> fw;           // forward sweep configuration (fac, unit, reorder, piv, Y, U, ...)
-    SweepArgs<T> bw;           // backward sweep configuration
-    const T* dinv_fw;          // inverses of the 64 x 64 diagonal blocks of the forward panels
-    const T* dinv_bw;          // ... of the backward panels
-    const int64_t* dinv_off;   // per front (-1: not a wide front)
-    const int32_t* lev_small;  // per level: offset and count of small fronts in `list`
-    const int32_t* lev_large;  // per level: offset and count of wide fronts in `list`
-    const int32_t* lev_maxblk; // per level: largest number of 64-column blocks among its wide fronts
-    const int32_t* list;       // fronts of all levels
-    int32_t nlevels;
-    const double* d;
-    const int8_t* kind;
-    int32_t diag_mode;         // 0 none (Cholesky), 1 D (LU), 2 D with 2x2 blocks (LDLT)
-    const int32_t* perm;
-    const double* in;          // B (mode 0) or R (mode 2)
-    double* out;               // X
-    int64_t ldin, ldout;
-    int32_t mode;              // 0: X = solve(B); 2: X += solve(R)
-    double* xtmp;              // n x nrhs scratch
-    unsigned int* barrier;     // grid barrier counter (zeroed before the launch)
-    unsigned int* blkflag;     // per 64-column diagonal block of the wide fronts (front s: from dinv_off[s] /
-                               // 4096): 1 once its forward solution is published, 2 once its backward one is
-    unsigned int* pullflag;    // per wide front (at its first block's index): 1 once its forward pull is done
-    unsigned int* l21cnt;      // per block: columns whose backward -L21^T x2 is applied
-                               // (all three zeroed before the launch)
-    int32_t* status;           // nonzero: a barrier or flag wait gave up
-    int64_t* trace;            // profiling: (tag, %globaltimer ns) pairs written by CTA 0, or NULL
-    int32_t trace_cap;
-    int32_t warp_smem;         // doubles of shared memory per warp for the small fronts (xs + Ld)
-    int32_t warp_xs;           // doubles of xs within it
-};
-
 // ---------------------------------------------------------------------------------------------------
 // Dataflow solve: the whole solve (forward, diagonal, backward, both permutations) in one persistent
 // cooperative launch with no grid barrier. Work is a list of tasks in a topological order of the
@@ -85,7 +49,7 @@ struct PersistArgs {
 // land on each front row, in child order), so every row is gathered by one thread with independent
 // loads and a fixed summation order.
 constexpr int DF_WARP_W = 32;     // widest warp front
-constexpr int DF_WARP_F = 128;    // tallest warp front
+constexpr int DF_WARP_F = 128;    // tallest warp front (the plan's tuning may lower it)
 constexpr int DF_BUNDLE = 8;      // warp fronts per task (one per warp)
 constexpr int DF_BLK = 64;        // tile rows and block columns of the tiled fronts
 constexpr int DF_CHUNK = 128;     // update rows per backward partial task
@@ -210,11 +174,6 @@ cudaError_t launch_sweep_rect(bool forward, const SweepArgs<T>& a, int ntiles, i
 constexpr int RECT_ROWS = 256;   // rows of a forward tile
 constexpr int RECT_COLS = 16;    // columns of a backward tile (one warp each, 16 warps)
 cudaError_t launch_diag(const DiagArgs& a, int nmembers, cudaStream_t st);
-template <typename T>
-cudaError_t launch_persistent_solve(const PersistArgs<T>& a, int grid, size_t smem, cudaStream_t st);
-template <typename T>
-int persistent_solve_grid(size_t smem);
-constexpr int SOLVE_BLK = 64;    // column block of the wide-front sweeps (the diagonal-block inverses)
 cudaError_t launch_permute(const PermArgs& a, int nmembers, cudaStream_t st);
 cudaError_t launch_residual(const ResidualArgs& a, int nmembers, cudaStream_t st);
 cudaError_t launch_norms(const NormArgs& a, int ncols, cudaStream_t st);

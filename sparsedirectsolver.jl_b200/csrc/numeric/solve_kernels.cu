@@ -404,677 +404,6 @@ template cudaError_t launch_sweep<double>(bool, const SweepArgs<double>&, int, i
 template cudaError_t launch_sweep<float>(bool, const SweepArgs<float>&, int, int, cudaStream_t);
 
 
-// ---------------------------------------------------------------------------
-// Warp-per-front sweeps of the small fronts in the persistent solve (w < 96): eight fronts in flight per
-// CTA. xs: w x nrhs, Ld: 32 x 33 (both per warp, shared memory).
-template <typename T>
-__device__ void warp_forward_front(const SweepArgs<T>& A, int s, double* xs, double* Ld) {
-    const DFront fd = A.fronts[s];
-    const int f = fd.f, w = fd.w, m = f - w, nrhs = A.nrhs, lane = threadIdx.x & 31;
-    const int64_t n = A.n;
-    const T* L = A.fac + fd.panel;
-    double* Y = A.Y;
-    double* U = A.U;
-    double* u = m > 0 ? U + A.uoff[s] : nullptr;
-    batched_copy<8>(lane, 32, w * nrhs, [&](int q) { return Y[fd.c0 + q % w + (int64_t)(q / w) * n]; },
-                    [&](int q, double v) { xs[q] = v; });
-    for (int q = lane; q < m * nrhs; q += 32) u[q] = 0.0;
-    __syncwarp();
-    for (int cq = fd.ch_begin; cq < fd.ch_end; ++cq) {
-        const int c = A.child_list[cq];
-        const DFront cd = A.fronts[c];
-        const int mc = cd.f - cd.w;
-        if (mc <= 0) continue;
-        const double* uc = U + A.uoff[c];
-        const int32_t* ri = A.relind + cd.ri_begin;
-        pull_child(lane, 32, mc * nrhs, mc, ri, uc, w, m, xs, w, u);
-        __syncwarp();
-    }
-    if (A.reorder) {
-        for (int q = lane; q < w * nrhs; q += 32) Y[fd.c0 + q % w + (int64_t)(q / w) * n] = xs[q];
-        __syncwarp();
-        batched_copy<8>(lane, 32, w * nrhs, [&](int q) { return Y[A.piv[fd.c0 + q % w] - 1 + (int64_t)(q / w) * n]; },
-                        [&](int q, double v) { xs[q] = v; });
-        __syncwarp();
-    }
-    for (int jb = 0; jb < w; jb += 32) {
-        const int bw = min(32, w - jb);
-        batched_copy<8>(0, 1, bw,
-                        [&](int j) { return (lane < bw && lane >= j) ? (double)L[(jb + lane) + (int64_t)(jb + j) * f] : 0.0; },
-                        [&](int j, double v) { Ld[lane * 33 + j] = v; });
-        __syncwarp();
-        // all right-hand sides (chunks of 8) in one shuffle chain; reciprocal diagonal per lane
-        const double rdl = (!A.unit && lane < bw) ? 1.0 / Ld[lane * 33 + lane] : 1.0;
-        for (int r0 = 0; r0 < nrhs; r0 += 8) {
-            const int rc = min(8, nrhs - r0);
-            double val[8];
-#pragma unroll
-            for (int r = 0; r < 8; ++r) val[r] = (lane < bw && r < rc) ? xs[jb + lane + (r0 + r) * w] : 0.0;
-            for (int j = 0; j < bw; ++j) {
-                const double lj = Ld[lane * 33 + j];
-#pragma unroll
-                for (int r = 0; r < 8; ++r) {
-                    if (lane == j) val[r] *= rdl;
-                    const double xj = __shfl_sync(0xffffffffu, val[r], j);
-                    if (lane > j) val[r] -= lj * xj;
-                }
-            }
-#pragma unroll
-            for (int r = 0; r < 8; ++r)
-                if (lane < bw && r < rc) xs[jb + lane + (r0 + r) * w] = val[r];
-        }
-        __syncwarp();
-        for (int q = jb + bw + lane; q < w; q += 32) {
-            for (int r0 = 0; r0 < nrhs; r0 += 8) {
-                const int rc = min(8, nrhs - r0);
-                double acc[8];
-#pragma unroll
-                for (int r = 0; r < 8; ++r) acc[r] = 0.0;
-                row_dot(L + q + (int64_t)jb * f, f, bw, xs + jb + r0 * w, w, rc, acc);
-                for (int r = 0; r < rc; ++r) xs[q + (r0 + r) * w] -= acc[r];
-            }
-        }
-        __syncwarp();
-    }
-    for (int i = lane; i < m; i += 32) {
-        for (int r0 = 0; r0 < nrhs; r0 += 8) {
-            const int rc = min(8, nrhs - r0);
-            double acc[8];
-#pragma unroll
-            for (int r = 0; r < 8; ++r) acc[r] = 0.0;
-            row_dot(L + w + i, f, w, xs + r0 * w, w, rc, acc);
-            for (int r = 0; r < rc; ++r) u[i + (r0 + r) * m] += acc[r];
-        }
-    }
-    for (int q = lane; q < w * nrhs; q += 32) Y[fd.c0 + q % w + (int64_t)(q / w) * n] = xs[q];
-    __syncwarp();
-}
-
-template <typename T>
-__device__ void warp_backward_front(const SweepArgs<T>& A, int s, double* xs, double* Ld) {
-    const DFront fd = A.fronts[s];
-    const int f = fd.f, w = fd.w, m = f - w, nrhs = A.nrhs, lane = threadIdx.x & 31;
-    const int64_t n = A.n;
-    const T* L = A.fac + fd.panel;
-    double* Y = A.Y;
-    const int32_t* rows = A.rowval + fd.row_begin + w;
-    batched_copy<8>(lane, 32, w * nrhs, [&](int q) { return Y[fd.c0 + q % w + (int64_t)(q / w) * n]; },
-                    [&](int q, double v) { xs[q] = v; });
-    __syncwarp();
-    // x1 -= L21^T x2: x2 = Y[rows below] gathered in chunks into Ld, lanes over the columns
-    const int CH = max(1, (32 * 33) / nrhs);
-    for (int i0 = 0; i0 < m; i0 += CH) {
-        const int ch = min(CH, m - i0);
-        batched_copy<8>(lane, 32, ch * nrhs, [&](int q) { return Y[rows[i0 + q % ch] + (int64_t)(q / ch) * n]; },
-                        [&](int q, double v) { Ld[q] = v; });
-        __syncwarp();
-        for (int j = lane; j < w; j += 32) {
-            const T* Lc = L + w + i0 + (int64_t)j * f;
-            for (int r0 = 0; r0 < nrhs; r0 += 8) {
-                const int rc = min(8, nrhs - r0);
-                double acc[8];
-#pragma unroll
-                for (int r = 0; r < 8; ++r) acc[r] = 0.0;
-                int i = 0;
-                for (; i + 8 <= ch; i += 8) {
-                    double lv[8];
-#pragma unroll
-                    for (int u = 0; u < 8; ++u) lv[u] = (double)Lc[i + u];
-#pragma unroll
-                    for (int u = 0; u < 8; ++u)
-#pragma unroll
-                        for (int r = 0; r < 8; ++r)
-                            if (r < rc) acc[r] += lv[u] * Ld[i + u + (r0 + r) * ch];
-                }
-                for (; i < ch; ++i) {
-                    const double l = (double)Lc[i];
-#pragma unroll
-                    for (int r = 0; r < 8; ++r)
-                        if (r < rc) acc[r] += l * Ld[i + (r0 + r) * ch];
-                }
-                for (int r = 0; r < rc; ++r) xs[j + (r0 + r) * w] -= acc[r];
-            }
-        }
-        __syncwarp();
-    }
-    const int nblk = (w + 31) / 32;
-    for (int bq = nblk - 1; bq >= 0; --bq) {
-        const int jb = bq * 32, bw = min(32, w - jb);
-        batched_copy<8>(0, 1, bw,
-                        [&](int j) { return (lane < bw && lane >= j) ? (double)L[(jb + lane) + (int64_t)(jb + j) * f] : 0.0; },
-                        [&](int j, double v) { Ld[lane * 33 + j] = v; });
-        __syncwarp();
-        const double rdl = (!A.unit && lane < bw) ? 1.0 / Ld[lane * 33 + lane] : 1.0;
-        for (int r0 = 0; r0 < nrhs; r0 += 8) {
-            const int rc = min(8, nrhs - r0);
-            double val[8];
-#pragma unroll
-            for (int r = 0; r < 8; ++r) val[r] = (lane < bw && r < rc) ? xs[jb + lane + (r0 + r) * w] : 0.0;
-            for (int j = bw - 1; j >= 0; --j) {
-                const double lj = Ld[j * 33 + lane];
-#pragma unroll
-                for (int r = 0; r < 8; ++r) {
-                    if (lane == j) val[r] *= rdl;
-                    const double xj = __shfl_sync(0xffffffffu, val[r], j);
-                    if (lane < j) val[r] -= lj * xj;
-                }
-            }
-#pragma unroll
-            for (int r = 0; r < 8; ++r)
-                if (lane < bw && r < rc) xs[jb + lane + (r0 + r) * w] = val[r];
-        }
-        __syncwarp();
-        for (int i = lane; i < jb; i += 32) {
-            const T* Lr = L + jb + (int64_t)i * f;   // L[jb + k, i], contiguous in k
-            for (int r0 = 0; r0 < nrhs; r0 += 8) {
-                const int rc = min(8, nrhs - r0);
-                double acc[8];
-#pragma unroll
-                for (int r = 0; r < 8; ++r) acc[r] = 0.0;
-                row_dot(Lr, 1, bw, xs + jb + r0 * w, w, rc, acc);
-                for (int r = 0; r < rc; ++r) xs[i + (r0 + r) * w] -= acc[r];
-            }
-        }
-        __syncwarp();
-    }
-    for (int q = lane; q < w * nrhs; q += 32) {
-        const int k = q % w;
-        const int dst = A.reorder ? A.piv[fd.c0 + k] - 1 : fd.c0 + k;
-        Y[dst + (int64_t)(q / w) * n] = xs[q];
-    }
-    __syncwarp();
-}
-
-// ---------------------------------------------------------------------------
-// Persistent solve. Grid barrier: one arrival per CTA on a monotonic counter; the wait is bounded
-// (about two seconds of spinning), after which the CTA records the failure and goes on, so a lost
-// CTA never hangs the device (the results are then garbage and the status word says so).
-__device__ __forceinline__ void grid_barrier(unsigned int* bar, unsigned int& epoch, int32_t* status) {
-    __syncthreads();
-    epoch += gridDim.x;
-    if (threadIdx.x == 0) {
-        __threadfence();
-        atomicAdd(bar, 1u);
-        unsigned int v;
-        long spins = 0;
-        while (true) {
-            asm volatile("ld.acquire.gpu.u32 %0, [%1];" : "=r"(v) : "l"(bar));
-            if ((int)(v - epoch) >= 0) break;
-            if (++spins > (1L << 26)) {
-                atomicExch(status, 1);
-                break;
-            }
-            __nanosleep(32);
-        }
-        __threadfence();
-    }
-    __syncthreads();
-}
-
-// Shared memory of a wide-front item: the 64 x 64 inverse block, the item's rows (or columns) of y,
-// x of the block being applied, and partial sums.
-constexpr int WT_SMEM_DOUBLES_FIXED = SOLVE_BLK * (SOLVE_BLK + 1);
-
-// Flags of the wide fronts' dataflow: a block's solution is published by its owner (stores, fence,
-// release of the flag) and read by the items that need it after an acquire of the flag. The wait is
-// bounded like the grid barrier, and gives up at once when any wait of the launch has given up.
-__device__ __forceinline__ void publish_flag(unsigned int* flag, unsigned int v) {
-    __threadfence();
-    __syncthreads();
-    if (threadIdx.x == 0) asm volatile("st.release.gpu.u32 [%0], %1;" ::"l"(flag), "r"(v) : "memory");
-}
-
-__device__ __forceinline__ void wait_flag(const unsigned int* flag, unsigned int target, int32_t* status) {
-    if (threadIdx.x == 0) {
-        unsigned int v;
-        long spins = 0;
-        while (true) {
-            asm volatile("ld.acquire.gpu.u32 %0, [%1];" : "=r"(v) : "l"(flag) : "memory");
-            if (v >= target) break;
-            if (++spins > (1L << 26) || ((spins & 255) == 0 && *(volatile int32_t*)status != 0)) {
-                atomicExch(status, 1);
-                break;
-            }
-            __nanosleep(32);
-        }
-        __threadfence();
-    }
-    __syncthreads();
-}
-
-// Forward sweep of a wide front, row tile t (rows 64 t .. 64 t + 63), owned by one CTA once the front's
-// pull is flagged: the tile takes
-// x_b of every block b <= t in increasing order (rows below block b: y -= L x_b for rows of the block
-// column, u += L x_b for the rows below the front's columns); at b = t the tile holds block t's rows and
-// solves them, x_t = inv(L_tt) y_t, publishing x_t for the tiles below. The arithmetic and its order
-// are those of a block-step sweep with a grid barrier after every step.
-template <typename T>
-__device__ void wide_forward_owner(const PersistArgs<T>& P, int s, int t, double* sm) {
-    const SweepArgs<T>& A = P.fw;
-    const DFront fd = A.fronts[s];
-    const int f = fd.f, w = fd.w, m = f - w, nrhs = A.nrhs;
-    const int64_t n = A.n;
-    const int nb = (w + SOLVE_BLK - 1) / SOLVE_BLK;
-    const int r0 = t * SOLVE_BLK, rows = min(SOLVE_BLK, f - r0);
-    const T* L = A.fac + fd.panel;
-    double* Y = A.Y;
-    double* u = m > 0 ? A.U + A.uoff[s] : nullptr;
-    const int64_t base = P.dinv_off[s] / (SOLVE_BLK * SOLVE_BLK);
-    unsigned int* flag = P.blkflag + base;
-    double* Iv = sm;                                  // SOLVE_BLK x (SOLVE_BLK + 1)
-    double* yb = sm + WT_SMEM_DOUBLES_FIXED;          // the tile's rows, SOLVE_BLK x nrhs
-    double* xb = yb + SOLVE_BLK * nrhs;               // x of the block being applied
-    double* part = xb + SOLVE_BLK * nrhs;             // 4 x SOLVE_BLK x nrhs partial sums
-    const int tid = threadIdx.x, nt = blockDim.x;
-    wait_flag(P.pullflag + base, 1u, P.status);       // the front's children are pulled into Y and u
-    batched_copy<4>(tid, nt, SOLVE_BLK * nrhs,
-                    [&](int q) {
-                        const int i = q % SOLVE_BLK, r = q / SOLVE_BLK, row = r0 + i;
-                        if (i >= rows) return 0.0;
-                        return row < w ? Y[fd.c0 + row + (int64_t)r * n] : u[row - w + (int64_t)r * m];
-                    },
-                    [&](int q, double v) { yb[q] = v; });
-    if (t < nb) {
-        const int bwt = min(SOLVE_BLK, w - r0);
-        const T* inv = P.dinv_fw + P.dinv_off[s] + (int64_t)t * SOLVE_BLK * SOLVE_BLK;
-        batched_copy<8>(tid, nt, SOLVE_BLK * SOLVE_BLK,
-                        [&](int q) { return (q % SOLVE_BLK < bwt && q / SOLVE_BLK < bwt) ? (double)inv[q] : 0.0; },
-                        [&](int q, double v) { Iv[q % SOLVE_BLK + (q / SOLVE_BLK) * (SOLVE_BLK + 1)] = v; });
-    }
-    __syncthreads();
-    const int row = r0 + (tid & (SOLVE_BLK - 1)), quarter = tid / SOLVE_BLK;
-    for (int b = 0; b <= min(t, nb - 1); ++b) {
-        const int jb = b * SOLVE_BLK, bw = min(SOLVE_BLK, w - jb);
-        if (b == t) {
-            for (int q = tid; q < SOLVE_BLK * nrhs; q += nt) {
-                const int i = q % SOLVE_BLK, r = q / SOLVE_BLK;
-                double acc = 0.0;
-#pragma unroll 8
-                for (int j = 0; j < SOLVE_BLK; ++j)
-                    acc += Iv[i + j * (SOLVE_BLK + 1)] * (j < bw ? yb[j + r * SOLVE_BLK] : 0.0);
-                xb[q] = acc;
-            }
-            __syncthreads();
-            for (int q = tid; q < bw * nrhs; q += nt) {
-                const int k = q % bw, r = q / bw;
-                const double v = xb[k + r * SOLVE_BLK];
-                P.xtmp[fd.c0 + jb + k + (int64_t)r * n] = v;
-                Y[fd.c0 + jb + k + (int64_t)r * n] = v;
-            }
-            publish_flag(flag + b, 1u);
-        } else {
-            wait_flag(flag + b, 1u, P.status);
-            for (int q = tid; q < SOLVE_BLK * nrhs; q += nt) {
-                const int k = q % SOLVE_BLK, r = q / SOLVE_BLK;
-                xb[q] = k < bw ? P.xtmp[fd.c0 + jb + k + (int64_t)r * n] : 0.0;
-            }
-            __syncthreads();
-        }
-        // rows of the tile below block b: 4 threads per row, 16 block columns each
-        const bool upd = tid < 4 * SOLVE_BLK && row < f && row >= jb + bw;
-        for (int r0_ = 0; r0_ < nrhs; r0_ += 8) {
-            const int rc = min(8, nrhs - r0_);
-            double acc[8];
-#pragma unroll
-            for (int r = 0; r < 8; ++r) acc[r] = 0.0;
-            if (upd) {
-                const int c0 = quarter * (SOLVE_BLK / 4), cw = max(0, min(SOLVE_BLK / 4, bw - c0));
-                row_dot(L + row + (int64_t)(jb + c0) * f, f, cw, xb + c0 + r0_ * SOLVE_BLK, SOLVE_BLK, rc, acc);
-            }
-            if (tid < 4 * SOLVE_BLK)
-                for (int r = 0; r < rc; ++r) part[(tid & (SOLVE_BLK - 1)) + SOLVE_BLK * (quarter + 4 * r)] = acc[r];
-            __syncthreads();
-            if (tid < SOLVE_BLK && row < f && row >= jb + bw) {
-                for (int r = 0; r < rc; ++r) {
-                    const double v = part[tid + SOLVE_BLK * (4 * r)] + part[tid + SOLVE_BLK * (1 + 4 * r)] +
-                                     part[tid + SOLVE_BLK * (2 + 4 * r)] + part[tid + SOLVE_BLK * (3 + 4 * r)];
-                    if (row < w) yb[tid + (r0_ + r) * SOLVE_BLK] -= v;
-                    else yb[tid + (r0_ + r) * SOLVE_BLK] += v;
-                }
-            }
-            __syncthreads();
-        }
-    }
-    // the tile's rows below the front's columns go back to the update vector
-    for (int q = tid; q < SOLVE_BLK * nrhs; q += nt) {
-        const int i = q % SOLVE_BLK, r = q / SOLVE_BLK;
-        if (i < rows && r0 + i >= w) u[r0 + i - w + (int64_t)r * m] = yb[q];
-    }
-    __syncthreads();
-}
-
-// Backward sweep of a wide front, block b (columns 64 b .. 64 b + 63), owned by one CTA, once the
-// warps of the y1 -= L21^T x2 phase have counted all of the block's columns: y_b takes -L_tb^T x_t of every later block t in decreasing order as each
-// is published, and x_b = inv(L_bb)^T y_b is published into the scratch. The arithmetic and its
-// order are those of a block-step sweep with a grid barrier after every step.
-template <typename T>
-__device__ void wide_backward_owner(const PersistArgs<T>& P, int s, int b, double* sm) {
-    const SweepArgs<T>& A = P.bw;
-    const DFront fd = A.fronts[s];
-    const int f = fd.f, w = fd.w, nrhs = A.nrhs;
-    const int64_t n = A.n;
-    const int nb = (w + SOLVE_BLK - 1) / SOLVE_BLK;
-    const int jb = b * SOLVE_BLK, bw = min(SOLVE_BLK, w - jb);
-    const T* L = A.fac + fd.panel;
-    const T* inv = P.dinv_bw + P.dinv_off[s] + (int64_t)b * SOLVE_BLK * SOLVE_BLK;
-    const int64_t base = P.dinv_off[s] / (SOLVE_BLK * SOLVE_BLK);
-    unsigned int* flag = P.blkflag + base;
-    double* Y = A.Y;
-    double* Iv = sm;
-    double* yb = sm + WT_SMEM_DOUBLES_FIXED;
-    double* xb = yb + SOLVE_BLK * nrhs;
-    const int tid = threadIdx.x, nt = blockDim.x, lane = tid & 31, warp = tid >> 5;
-    wait_flag(P.l21cnt + base + b, f > w ? (unsigned int)bw : 0u, P.status);   // y_b has taken -L21^T x2
-    batched_copy<8>(tid, nt, SOLVE_BLK * SOLVE_BLK,
-                    [&](int q) { return (q % SOLVE_BLK < bw && q / SOLVE_BLK < bw) ? (double)inv[q] : 0.0; },
-                    [&](int q, double v) { Iv[q % SOLVE_BLK + (q / SOLVE_BLK) * (SOLVE_BLK + 1)] = v; });
-    batched_copy<4>(tid, nt, SOLVE_BLK * nrhs,
-                    [&](int q) { return q % SOLVE_BLK < bw ? Y[fd.c0 + jb + q % SOLVE_BLK + (int64_t)(q / SOLVE_BLK) * n] : 0.0; },
-                    [&](int q, double v) { yb[q] = v; });
-    __syncthreads();
-    const int a0 = jb + warp * (SOLVE_BLK / 8);
-    for (int t = nb - 1; t > b; --t) {
-        const int jt = t * SOLVE_BLK, bwt = min(SOLVE_BLK, w - jt);
-        // this warp's 8 columns of block b against the rows of block t, loaded before the wait
-        double l1[SOLVE_BLK / 8], l2[SOLVE_BLK / 8];
-#pragma unroll
-        for (int c = 0; c < SOLVE_BLK / 8; ++c) {
-            const int a = a0 + c;
-            l1[c] = lane < bwt ? (double)L[(jt + lane) + (int64_t)a * f] : 0.0;
-            l2[c] = lane + 32 < bwt ? (double)L[(jt + lane + 32) + (int64_t)a * f] : 0.0;
-        }
-        wait_flag(flag + t, 2u, P.status);
-        for (int q = tid; q < SOLVE_BLK * nrhs; q += nt) {
-            const int k = q % SOLVE_BLK, r = q / SOLVE_BLK;
-            xb[q] = k < bwt ? P.xtmp[fd.c0 + jt + k + (int64_t)r * n] : 0.0;
-        }
-        __syncthreads();
-        for (int r = 0; r < nrhs; ++r) {
-            const double x1 = xb[lane + r * SOLVE_BLK], x2 = xb[lane + 32 + r * SOLVE_BLK];
-#pragma unroll
-            for (int c = 0; c < SOLVE_BLK / 8; ++c) {
-                double v = l1[c] * x1 + l2[c] * x2;
-                for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
-                if (lane == 0) yb[a0 + c - jb + r * SOLVE_BLK] -= v;
-            }
-        }
-        __syncthreads();
-    }
-    for (int q = tid; q < SOLVE_BLK * nrhs; q += nt) {
-        const int i = q % SOLVE_BLK, r = q / SOLVE_BLK;
-        double acc = 0.0;
-#pragma unroll 8
-        for (int j = 0; j < SOLVE_BLK; ++j) acc += Iv[j + i * (SOLVE_BLK + 1)] * yb[j + r * SOLVE_BLK];
-        xb[q] = acc;
-    }
-    __syncthreads();
-    for (int q = tid; q < bw * nrhs; q += nt) {
-        const int k = q % bw, r = q / bw;
-        P.xtmp[fd.c0 + jb + k + (int64_t)r * n] = xb[k + r * SOLVE_BLK];
-    }
-    publish_flag(flag + b, 2u);
-    if (b == 0) {
-        // the last block of the front's chain: every other block's solution was acquired above, and
-        // every owner of this front has read its y; the solution goes into Y in the original order
-        for (int q = tid; q < w * nrhs; q += nt) {
-            const int k = q % w, r = q / w;
-            const int64_t dst = A.reorder ? A.piv[fd.c0 + k] - 1 : fd.c0 + k;
-            Y[dst + (int64_t)r * n] = P.xtmp[fd.c0 + k + (int64_t)r * n];
-        }
-        __syncthreads();
-    }
-}
-
-__device__ __forceinline__ void trace_mark(int64_t* trace, int cap, int& n, int64_t tag) {
-    if (trace && blockIdx.x == 0 && threadIdx.x == 0 && n < cap) {
-        uint64_t t;
-        asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
-        trace[2 * n] = tag;
-        trace[2 * n + 1] = (int64_t)t;
-        ++n;
-    }
-}
-
-template <typename T>
-__global__ void __launch_bounds__(SOLVE_THREADS) persistent_solve_kernel(PersistArgs<T> P) {
-    extern __shared__ double psm[];
-    unsigned int epoch = 0;
-    int ntr = 0;
-    // phase tags: 1 perm, 2 fwd level A, 3 fwd block step, 4 diag, 5 bwd L21^T, 6 bwd block step,
-    // 7 bwd level end (small fronts), 8 final; tag = kind << 40 | level << 16 | step
-#define TRACE(kind, lev, stp) trace_mark(P.trace, P.trace_cap, ntr, ((int64_t)(kind) << 40) | ((int64_t)(lev) << 16) | (stp))
-    TRACE(0, 0, 0);
-    const int G = gridDim.x;
-    const int64_t n = P.fw.n;
-    const int nrhs = P.fw.nrhs;
-    const int64_t gtid = blockIdx.x * (int64_t)blockDim.x + threadIdx.x, gstride = (int64_t)G * blockDim.x;
-    // Y = in[perm]
-    for (int64_t q = gtid; q < n * nrhs; q += gstride) {
-        int64_t k = q % n, r = q / n;
-        P.fw.Y[q] = P.in[P.perm[k] + r * P.ldin];
-    }
-    grid_barrier(P.barrier, epoch, P.status);
-    TRACE(1, 0, 0);
-    // forward levels
-    for (int L = 0; L < P.nlevels; ++L) {
-        const int so = P.lev_small[2 * L], sc = P.lev_small[2 * L + 1];
-        const int lo = P.lev_large[2 * L], lc = P.lev_large[2 * L + 1];
-        if (sc >= G * (blockDim.x >> 5) / 2) {
-            // many small fronts: one warp each
-            const int wpc = blockDim.x >> 5, warp = threadIdx.x >> 5;
-            double* xs = psm + warp * P.warp_smem;
-            for (int i = blockIdx.x * wpc + warp; i < sc; i += G * wpc)
-                warp_forward_front(P.fw, P.list[so + i], xs, xs + P.warp_xs);
-        } else {
-            // few: one CTA each
-            for (int i = blockIdx.x; i < sc; i += G) forward_front(P.fw, P.list[so + i], 0, psm);
-        }
-        // wide fronts: pull the children and apply the local pivot order (one CTA each, from the end)
-        for (int i = G - 1 - blockIdx.x; i < lc; i += G) {
-            const int s = P.list[lo + i];
-            const DFront fd = P.fw.fronts[s];
-            const int w = fd.w, m = fd.f - fd.w;
-            double* Y = P.fw.Y;
-            double* xt = P.xtmp;
-            double* u = m > 0 ? P.fw.U + P.fw.uoff[s] : nullptr;
-            batched_copy<8>(threadIdx.x, blockDim.x, w * nrhs,
-                            [&](int q) { return Y[fd.c0 + q % w + (int64_t)(q / w) * n]; },
-                            [&](int q, double v) { xt[fd.c0 + q % w + (int64_t)(q / w) * n] = v; });
-            for (int q = threadIdx.x; q < m * nrhs; q += blockDim.x) u[q] = 0.0;
-            __syncthreads();
-            for (int cq = fd.ch_begin; cq < fd.ch_end; ++cq) {
-                const int c = P.fw.child_list[cq];
-                const DFront cd = P.fw.fronts[c];
-                const int mc = cd.f - cd.w;
-                if (mc <= 0) continue;
-                const double* uc = P.fw.U + P.fw.uoff[c];
-                const int32_t* ri = P.fw.relind + cd.ri_begin;
-                pull_child(threadIdx.x, blockDim.x, mc * nrhs, mc, ri, uc, w, m, xt + fd.c0, n, u);
-                __syncthreads();
-            }
-            batched_copy<8>(threadIdx.x, blockDim.x, w * nrhs,
-                            [&](int q) {
-                                const int k = q % w;
-                                const int src = P.fw.reorder ? P.fw.piv[fd.c0 + k] - 1 : fd.c0 + k;
-                                return xt[src + (int64_t)(q / w) * n];
-                            },
-                            [&](int q, double v) { Y[fd.c0 + q % w + (int64_t)(q / w) * n] = v; });
-            publish_flag(P.pullflag + P.dinv_off[s] / (SOLVE_BLK * SOLVE_BLK), 1u);
-        }
-        TRACE(2, L, 0);
-        if (lc) {
-            // wide fronts: one CTA per (front, row tile); a CTA takes its tiles of a front in increasing
-            // order, so every tile waits only on tiles taken earlier
-            int total = 0;
-            for (int i = 0; i < lc; ++i) total += (P.fw.fronts[P.list[lo + i]].f + SOLVE_BLK - 1) / SOLVE_BLK;
-            for (int k = blockIdx.x; k < total; k += G) {
-                int kk = k;
-                for (int i = 0; i < lc; ++i) {
-                    const int s = P.list[lo + i];
-                    const int cnt = (P.fw.fronts[s].f + SOLVE_BLK - 1) / SOLVE_BLK;
-                    if (kk < cnt) {
-                        wide_forward_owner(P, s, kk, psm);
-                        break;
-                    }
-                    kk -= cnt;
-                }
-            }
-        }
-        grid_barrier(P.barrier, epoch, P.status);
-        TRACE(3, L, 0);
-    }
-    // the copies of the last level's wide fronts must land before Y is read again
-    grid_barrier(P.barrier, epoch, P.status);
-    // diagonal: D^{-1} with 1x1 and 2x2 blocks
-    if (P.diag_mode) {
-        for (int64_t q = gtid; q < n * nrhs; q += gstride) {
-            const int64_t k = q % n, r = q / n;
-            const int kk = P.kind[k];
-            double* Y = P.fw.Y;
-            if (P.diag_mode == 2 && kk == KIND_2X2_SECOND) continue;
-            if (P.diag_mode == 2 && kk == KIND_2X2_FIRST) {
-                double a = P.d[k], b = P.d[n + k], c = P.d[k + 1];
-                double det = a * c - b * b;
-                double y1 = Y[k + r * n], y2 = Y[k + 1 + r * n];
-                Y[k + r * n] = (c * y1 - b * y2) / det;
-                Y[k + 1 + r * n] = (a * y2 - b * y1) / det;
-            } else {
-                Y[k + r * n] /= P.d[k];
-            }
-        }
-        grid_barrier(P.barrier, epoch, P.status);
-        TRACE(4, 0, 0);
-    }
-    // backward levels
-    for (int L = P.nlevels - 1; L >= 0; --L) {
-        const int so = P.lev_small[2 * L], sc = P.lev_small[2 * L + 1];
-        const int lo = P.lev_large[2 * L], lc = P.lev_large[2 * L + 1];
-        if (lc) {
-            // stage x2 = Y[rows below] of the wide fronts in their update vectors (free in this sweep)
-            for (int i = 0; i < lc; ++i) {
-                const int s = P.list[lo + i];
-                const DFront fd = P.bw.fronts[s];
-                const int w = fd.w, m = fd.f - fd.w;
-                if (m == 0) continue;
-                double* xb = P.bw.U + P.bw.uoff[s];
-                const int32_t* rows = P.bw.rowval + fd.row_begin + w;
-                for (int64_t q = gtid; q < (int64_t)m * nrhs; q += gstride) {
-                    const int i2 = (int)(q % m), r = (int)(q / m);
-                    xb[q] = P.bw.Y[rows[i2] + (int64_t)r * n];
-                }
-            }
-            grid_barrier(P.barrier, epoch, P.status);
-            // x1 -= L21^T x2 for the wide fronts: one warp per column, columns spread over the grid
-            const int warps = blockDim.x >> 5, lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-            int totc = 0;
-            for (int i = 0; i < lc; ++i) totc += P.bw.fronts[P.list[lo + i]].w;
-            for (int col = blockIdx.x * warps + warp; col < totc; col += G * warps) {
-                int j = col, i = 0, s = 0;
-                for (; i < lc; ++i) {
-                    s = P.list[lo + i];
-                    const int wi = P.bw.fronts[s].w;
-                    if (j < wi) break;
-                    j -= wi;
-                }
-                const DFront fd = P.bw.fronts[s];
-                const int f = fd.f, w = fd.w, m = f - w;
-                if (m == 0) continue;
-                const T* Lp = P.bw.fac + fd.panel;
-                const double* xb = P.bw.U + P.bw.uoff[s];
-                for (int r0 = 0; r0 < nrhs; r0 += 8) {
-                    const int rc = min(8, nrhs - r0);
-                    double acc[8];
-#pragma unroll
-                    for (int r = 0; r < 8; ++r) acc[r] = 0.0;
-                    col_dot(Lp + w + (int64_t)j * f, m, lane, rc,
-                            [&](int i2, int r) { return xb[i2 + (r0 + r) * m]; }, acc);
-#pragma unroll
-                    for (int r = 0; r < 8; ++r) {
-                        double v = acc[r];
-                        for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
-                        if (lane == 0 && r < rc) P.bw.Y[fd.c0 + j + (int64_t)(r0 + r) * n] -= v;
-                    }
-                }
-                if (lane == 0) {   // release the column to its block's owner
-                    __threadfence();
-                    atomicAdd(P.l21cnt + P.dinv_off[s] / (SOLVE_BLK * SOLVE_BLK) + j / SOLVE_BLK, 1u);
-                }
-                __syncwarp();
-            }
-            TRACE(5, L, 0);
-        }
-        // the level's small fronts (independent of its wide fronts; nothing here waits)
-        if (sc >= G * (blockDim.x >> 5) / 2) {
-            const int wpc = blockDim.x >> 5, warp = threadIdx.x >> 5;
-            double* xs = psm + warp * P.warp_smem;
-            for (int i = blockIdx.x * wpc + warp; i < sc; i += G * wpc)
-                warp_backward_front(P.bw, P.list[so + i], xs, xs + P.warp_xs);
-        } else {
-            for (int i = blockIdx.x; i < sc; i += G) backward_front(P.bw, P.list[so + i], 0, psm);
-        }
-        if (lc) {
-            // one CTA per (front, block); a CTA takes its blocks of a front in decreasing order, and the
-            // owner of block 0 puts the front's solution into Y
-            int total = 0;
-            for (int i = 0; i < lc; ++i) total += (P.bw.fronts[P.list[lo + i]].w + SOLVE_BLK - 1) / SOLVE_BLK;
-            for (int k = blockIdx.x; k < total; k += G) {
-                int kk = k;
-                for (int i = 0; i < lc; ++i) {
-                    const int s = P.list[lo + i];
-                    const int nbs = (P.bw.fronts[s].w + SOLVE_BLK - 1) / SOLVE_BLK;
-                    if (kk < nbs) {
-                        wide_backward_owner(P, s, nbs - 1 - kk, psm);
-                        break;
-                    }
-                    kk -= nbs;
-                }
-            }
-        }
-        grid_barrier(P.barrier, epoch, P.status);
-        TRACE(7, L, 0);
-    }
-    // out[perm] = Y (or +=)
-    for (int64_t q = gtid; q < n * nrhs; q += gstride) {
-        int64_t k = q % n, r = q / n;
-        double* o = P.out + P.perm[k] + r * P.ldout;
-        if (P.mode == 2) *o += P.fw.Y[q];
-        else *o = P.fw.Y[q];
-    }
-    TRACE(8, 0, 0);
-#undef TRACE
-}
-
-template <typename T>
-int persistent_solve_grid(size_t smem) {
-    int dev = 0, sms = 0, per = 0;
-    cudaGetDevice(&dev);
-    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, persistent_solve_kernel<T>, SOLVE_THREADS, smem) !=
-        cudaSuccess)
-        return 0;
-    return sms * std::min(per, 2);
-}
-
-template <typename T>
-cudaError_t launch_persistent_solve(const PersistArgs<T>& a, int grid, size_t smem, cudaStream_t st) {
-    cudaLaunchConfig_t cfg = {};
-    cfg.gridDim = dim3(grid);
-    cfg.blockDim = dim3(SOLVE_THREADS);
-    cfg.dynamicSmemBytes = smem;
-    cfg.stream = st;
-    cudaLaunchAttribute attr[1];
-    attr[0].id = cudaLaunchAttributeCooperative;
-    attr[0].val.cooperative = 1;
-    cfg.attrs = attr;
-    cfg.numAttrs = 1;
-    return cudaLaunchKernelEx(&cfg, persistent_solve_kernel<T>, a);
-}
-
-template cudaError_t launch_persistent_solve<double>(const PersistArgs<double>&, int, size_t, cudaStream_t);
-template cudaError_t launch_persistent_solve<float>(const PersistArgs<float>&, int, size_t, cudaStream_t);
-template int persistent_solve_grid<double>(size_t);
-template int persistent_solve_grid<float>(size_t);
-
 // D^{-1} (1x1 and 2x2 blocks, d[k], d[n + k], d[k + 1]) -- _sv_diag_kernel! sweeps.jl:549-569
 __global__ void diag_kernel(DiagArgs A) {
     const int member = A.members ? A.members[blockIdx.y] : blockIdx.y;
@@ -1225,8 +554,6 @@ cudaError_t prepare_solve_kernels(int max_smem) {
     set((const void*)backward_kernel<float>);
     set((const void*)forward_rect_kernel<double>);
     set((const void*)forward_rect_kernel<float>);
-    set((const void*)persistent_solve_kernel<double>);
-    set((const void*)persistent_solve_kernel<float>);
     return e;
 }
 

@@ -183,7 +183,22 @@ __global__ void __launch_bounds__(128) gemm_nt_tc32_kernel(GemmArgs<float> A) {
             }
             // one verdict for the whole CTA: tcgen05.ld below is warp-collective
             ok = __syncthreads_and(done != 0) != 0;
-            if (!ok && tid == 0 && A.status) atomicExch(A.status, 2);
+            if (!ok && tid == 0) {
+                if (A.status) atomicExch(A.status, 2);
+                // The stage's MMAs may still be running: they read this CTA's shared memory and write the
+                // tensor memory that the exit path frees. Give their commit a second bounded wait before
+                // the dealloc below. The status word already fails the factorization, so the C tile that
+                // this CTA leaves unwritten is never used.
+                uint32_t drained = 0;
+                for (long s = 0; !drained && s < (1L << 24); ++s)
+                    asm volatile(
+                        "{\n\t.reg .pred p;\n\t"
+                        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+                        "selp.b32 %0, 1, 0, p;\n\t}\n"
+                        : "=r"(drained)
+                        : "r"(smem_u32(mbar)), "r"(phase)
+                        : "memory");
+            }
         }
         phase ^= 1u;
     }

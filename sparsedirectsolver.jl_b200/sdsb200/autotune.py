@@ -3,9 +3,8 @@
 Two shapes decide how the fronts of a plan map onto the kernels:
 * ``fsmall``: the largest front order factored in shared memory by the small-front kernel. Larger
   fronts take the column-owner assembly, diagonal-block and DMMA GEMM path.
-* ``wide``, ``area``: a front whose width reaches ``wide`` or whose rectangular part (f - w) w
-  reaches 1024 ``area`` is "wide" in the solve: its columns go in 64-column block steps over the
-  whole grid instead of one CTA or warp.
+* ``wide``: the tallest front (of at most 32 columns) that the dataflow solve gives to one warp;
+  taller or wider fronts go to 64-row tile tasks spread over the grid. (``area`` is reserved.)
 
 The autotuner times factorization + solve for each candidate on the solver's own matrix and
 right-hand side (CUDA events, after a warm-up), keeps the fastest, and leaves the solver planned
@@ -15,7 +14,7 @@ from __future__ import annotations
 
 from .capi import tuning as make_tuning
 
-CANDIDATES = tuple((fs, wd, ar) for fs in (0, 128, 96) for wd in (0, 64) for ar in (0, 16))
+CANDIDATES = tuple((fs, wd, 0) for fs in (0, 128, 96) for wd in (0, 64))
 
 _cache: dict = {}
 

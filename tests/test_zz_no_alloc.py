@@ -7,11 +7,12 @@ working vectors in the plan and builds a CUDA graph on the first call with new
 buffers, and building that graph allocates. sdsb200_solve_noalloc takes its
 working vectors from one fixed static device array of the library instead
 (SDSB200_NOALLOC_SCRATCH_BYTES, 32 MiB) and launches the same persistent solve
-kernel directly.
+kernel (the dataflow solve) directly.
 
 These tests call it through the C ABI and compare it with sdsb200_solve (no
 refinement) on two calls in a row, within the FP64 tolerance of the other parity
-tests, and check that sizes beyond the array are refused. The file is named so
+tests (the FP32 tolerance for an FP32 factor, whose solve neither entry point
+refines here), and check that sizes beyond the array are refused. The file is named so
 that pytest collects it last: a run that stops at the first failure has then
 already run every other test.
 """
@@ -27,6 +28,8 @@ pytestmark = pytest.mark.gpu
 
 FP64_TOL = 1e-10   # solutions relative to max(1, max|x|), as the other FP64 parity tests
 BERR = 1e-12       # scaled backward error of every FP64 solve
+FP32_TOL = 1e-5    # the same for an FP32 factor, unrefined
+FP32_BERR = 1e-5   # scaled backward error of an unrefined solve with an FP32 factor
 SCRATCH_BYTES = 32 << 20
 
 
@@ -63,7 +66,7 @@ def _noalloc(torch, ds, b, solve_mode=0):
     if rc != 0:
         return rc, lib.sdsb200_last_error().decode()
     torch.cuda.synchronize()
-    assert int(status.item()) == 0, "a grid-barrier wait of the persistent solve gave up"
+    assert int(status.item()) == 0, "a dependency wait of the dataflow solve gave up"
     return rc, xcm.T.cpu().numpy()
 
 
@@ -75,8 +78,11 @@ def _existing(ds, b, solve_mode=0):
 
 
 CASES = {
-    # wide separators (the block-step phases) and many small fronts
+    # wide separators (the tiled fronts) and many small fronts
     "SPD": (lambda: M.lap3d(20, 20, 20, seed=6), "SPD", dict(reordering_alg="nd", max_nrhs=3), (0,)),
+    # the same with an FP32 factor: the float instance of the solve kernel, unrefined
+    "SPD_fp32": (lambda: M.lap3d(20, 20, 20, seed=6), "SPD",
+                 dict(reordering_alg="nd", max_nrhs=3, factor_precision="fp32"), (0,)),
     # Bunch-Kaufman LDL^T with 2x2 pivots: the local pivot order and the 2x2 diagonal blocks
     "S": (lambda: small_kkt(22, 22, 200, seed=6), "S", dict(max_nrhs=3), (0,)),
     # threshold-pivoting LU, solves with A and with A^T
@@ -88,6 +94,8 @@ CASES = {
 @pytest.mark.parametrize("case", sorted(CASES))
 def test_noalloc_matches_solve_twice(torch_cuda, case):
     make, structure, params, modes = CASES[case]
+    fp32 = params.get("factor_precision") == "fp32"
+    tol, berr = (FP32_TOL, FP32_BERR) if fp32 else (FP64_TOL, BERR)
     A = make()
     ds = _factored(A, structure, **params)
     for mode in modes:
@@ -99,8 +107,8 @@ def test_noalloc_matches_solve_twice(torch_cuda, case):
             assert rc == 0, x
             ref = _existing(ds, b, mode)
             assert np.all(np.isfinite(x))
-            assert rel_max_diff(x, ref) <= FP64_TOL
-            assert M.scaled_backward_error(AA, x, b) <= BERR
+            assert rel_max_diff(x, ref) <= tol
+            assert M.scaled_backward_error(AA, x, b) <= berr
 
 
 def test_noalloc_rejects_sizes_beyond_the_array(torch_cuda):
