@@ -58,7 +58,7 @@ def parse():
                          "other workloads: c1 lap2d_64 SPD AMD, c3 KKT LDL^T (n = 55 000), c4 1024 uneven "
                          "systems, c4u uniform batch 96x96 x 256, c5 LU convection-diffusion 40^3 with A and A^T")
     ap.add_argument("--tuning", default=None,
-                    help="fsmall,wide,area: fixed front tile shapes instead of the autotuner's search (for profilers)")
+                    help="fsmall,wide,chains: fixed front tile shapes instead of the autotuner's search (for profilers)")
     ap.add_argument("--once", choices=["fp64", "mixed"], default=None,
                     help="one analysis + factorization + solve of the workload in one form, untimed (for profilers); "
                          "with --config c3 or c5 that workload")

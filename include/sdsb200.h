@@ -103,10 +103,12 @@ typedef struct sdsb200_plan_options {
 /* Plan tuning (the shapes an autotuner chooses; no counterpart in the reference):
  * fsmall = the largest front order handled by the shared-memory small-front kernel (one of 32, 64,
  * 96, 128, 160, and 224 for FP32; 0 = the largest class); wide = the tallest front (at most 32
- * columns) that the dataflow solve gives to one warp, larger fronts going to 64-row tile tasks
- * (16..128, 0 = 128); area: reserved (ignored). */
-#define SDSB200_TUNING(fsmall, wide, area) \
-    ((int32_t)(fsmall) | ((int32_t)(wide) << 9) | ((int32_t)(area) << 20))
+ * columns) that the dataflow solve gives to one warp, larger fronts going to tile tasks (16..128,
+ * 0 = 128); chains = how the dataflow solve treats those tiled fronts: 0, through their inverse
+ * panels [L11^-1; L21 L11^-1] (f x w each, built after every factorization of a single-system plan),
+ * 1: through chains of 64-column blocks. */
+#define SDSB200_TUNING(fsmall, wide, chains) \
+    ((int32_t)(fsmall) | ((int32_t)(wide) << 9) | ((int32_t)(chains) << 20))
 
 /* The Options fields the numeric and solve phases read (src/options.jl:155-223). */
 typedef struct sdsb200_opts {

@@ -27,6 +27,7 @@ NUMERIC_SOURCES = [
     "numeric/pivot_kernels.cu",
     "numeric/solve_kernels.cu",
     "numeric/solve_dataflow.cu",
+    "numeric/pinv_kernels.cu",
     "numeric/schur_kernels.cu",
     "numeric/adjoint_kernels.cu",
     "numeric/tc_kernels.cu",

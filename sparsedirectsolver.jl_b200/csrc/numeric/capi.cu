@@ -93,6 +93,7 @@ int prof_kind_of(LaunchKind k) {
         case L_PIVOT_FRONT: return PK_PIVOT;
         case L_SCALE: return PK_SCALE;
         case L_DFINV: return PK_INV;
+        case L_PINV: return PK_INV;
         default: return PK_STATS;
     }
 }
@@ -121,7 +122,9 @@ int run_graph(Plan* P, Plan::CachedGraph& g, const std::vector<uint64_t>& key, c
         CK(e, "end capture");
         g.launches = P->launches_done - before;
         P->launches_done = before;
-        e = cudaGraphInstantiate(&g.exec, graph, 0);
+        // kernel nodes keep the priority of the stream they were captured from (the side launches' is
+        // the lowest)
+        e = cudaGraphInstantiateWithFlags(&g.exec, graph, cudaGraphInstantiateFlagUseNodePriority);
         cudaGraphDestroy(graph);
         CK(e, "graph instantiate");
         g.key = key;
@@ -165,11 +168,28 @@ int run_factor(Plan* P, const double* nzval, double eps, double u, int pivot, in
     T* cb = static_cast<T*>(P->d_cb);
     T* work = static_cast<T*>(P->d_work);
     int last_level = -1;
+    const cudaStream_t main_st = st;
+    bool on_side = false, any_side = false;
     for (const ProgLaunch& L : P->prog) {
-        if (L.kind != L_STATS && L.level != last_level) {
-            if (interrupted(P)) return fail(SDSB200_INTERRUPTED, "interrupted by user_host_interrupt");
+        if (L.kind != L_STATS && !L.side && L.level != last_level) {
+            if (interrupted(P)) {
+                if (any_side) {   // rejoin the side stream (a capture must end joined)
+                    cudaEventRecord(P->side_join, P->side);
+                    cudaStreamWaitEvent(main_st, P->side_join, 0);
+                }
+                return fail(SDSB200_INTERRUPTED, "interrupted by user_host_interrupt");
+            }
             last_level = L.level;
         }
+        // side launches: the side stream waits for the main stream's launches so far, then runs them
+        // beside the following levels of the factorization
+        if (L.side && !on_side) {
+            CK(cudaEventRecord(P->side_fork, main_st), "side fork");
+            CK(cudaStreamWaitEvent(P->side, P->side_fork, 0), "side fork");
+        }
+        on_side = L.side != 0;
+        any_side = any_side || on_side;
+        st = on_side ? P->side : main_st;
         cudaError_t e = cudaSuccess;
         P->cur_level = L.level;
         prof_begin(P, st);
@@ -284,8 +304,8 @@ int run_factor(Plan* P, const double* nzval, double eps, double u, int pivot, in
                     T* inv = static_cast<T*>(side ? P->d_dfinv_U : P->d_dfinv_L);
                     SmallInvArgs<T> a{};
                     a.fronts = P->d_fronts;
-                    a.list = P->d_df_small;
-                    a.count = P->n_df_small;
+                    a.list = P->d_df_small + L.list;
+                    a.count = L.count;
                     a.inv_off = P->d_df_inv_off;
                     a.members = members;
                     a.panels = panels;
@@ -298,8 +318,8 @@ int run_factor(Plan* P, const double* nzval, double eps, double u, int pivot, in
                     if (e != cudaSuccess) break;
                     BlockInvArgs<T> b{};
                     b.fronts = P->d_fronts;
-                    b.tasks = P->d_df_blkinv;
-                    b.count = P->n_df_blkinv;
+                    b.tasks = P->d_df_blkinv + 2 * L.list2;
+                    b.count = L.count2;
                     b.dinv_off = P->d_df_inv_off;
                     b.members = members;
                     b.panels = panels;
@@ -308,7 +328,39 @@ int run_factor(Plan* P, const double* nzval, double eps, double u, int pivot, in
                     b.dinv_len = P->df_inv_len;
                     b.finfo = P->d_finfo;
                     b.ns = (int32_t)P->ns;
+                    b.panel_layout = P->df_pinv ? 1 : 0;
                     e = launch_block_inv<T>(b, nm, st);
+                }
+                break;
+            }
+            case L_PINV: {
+                // one launch of the inverse-panel GEMMs (cls 1: T = L[C, A] X[A, A] into the scratch;
+                // 2: X[C, A] = -X[C, C] T; 3: L21 X), for each panel set
+                const int sides = P->structure == STRUCT_G ? 2 : 1;
+                for (int side = 0; side < sides && e == cudaSuccess; ++side) {
+                    const T* panels = side ? ufactor : factor;
+                    T* pinv = static_cast<T*>(side ? P->d_dfinv_U : P->d_dfinv_L);
+                    T* work = static_cast<T*>(P->d_pwork) + (int64_t)side * P->pwork_len * P->nbatch;
+                    PinvGemmArgs<T> a{};
+                    a.tiles = P->d_pinv_tiles + L.list;
+                    a.count = L.count;
+                    a.members = members;
+                    a.finfo = P->d_finfo;
+                    a.ns = (int32_t)P->ns;
+                    if (L.cls == 1) {
+                        a.abuf = panels; a.astride = P->factor_len;
+                        a.bbuf = pinv; a.bstride = P->df_inv_len;
+                        a.cbuf = work; a.cstride = P->pwork_len;
+                    } else if (L.cls == 2) {
+                        a.abuf = pinv; a.astride = P->df_inv_len;
+                        a.bbuf = work; a.bstride = P->pwork_len;
+                        a.cbuf = pinv; a.cstride = P->df_inv_len;
+                    } else {
+                        a.abuf = panels; a.astride = P->factor_len;
+                        a.bbuf = pinv; a.bstride = P->df_inv_len;
+                        a.cbuf = pinv; a.cstride = P->df_inv_len;
+                    }
+                    e = launch_pinv_gemm<T>(a, nm, st);
                 }
                 break;
             }
@@ -327,6 +379,11 @@ int run_factor(Plan* P, const double* nzval, double eps, double u, int pivot, in
         }
         prof_end(P, st, prof_kind_of(L.kind), L.flops * nm, L.bytes * nm);
         if (e != cudaSuccess) return cuda_fail(e, "factorization launch");
+    }
+    st = main_st;
+    if (any_side) {   // the factorization ends when the side launches are done too
+        CK(cudaEventRecord(P->side_join, P->side), "side join");
+        CK(cudaStreamWaitEvent(st, P->side_join, 0), "side join");
     }
     return SDSB200_OK;
 }
@@ -457,7 +514,9 @@ int run_dataflow(Plan* P, int nrhs, bool transpose, const double* in, int64_t ld
     a.bdone = fl + ns;
     a.xflag = fl + 2 * ns;
     a.pcnt = fl + 2 * ns + P->df_nblk;
-    a.head = fl + 2 * ns + 2 * (int64_t)P->df_nblk;
+    a.tcnt = fl + 2 * ns + 2 * (int64_t)P->df_nblk;
+    a.ccnt = a.tcnt + P->df_ntcnt;
+    a.head = a.ccnt + P->df_nccnt;
     a.status = P->d_solve_status;
     a.reorder_fw = ldl || (gen && !transpose);
     a.reorder_bw = ldl || (gen && transpose);
@@ -471,10 +530,11 @@ int run_dataflow(Plan* P, int nrhs, bool transpose, const double* in, int64_t ld
     for (int r0 = 0; r0 < nrhs; r0 += DF_MAX_NRHS) {
         a.nrhs = std::min(DF_MAX_NRHS, nrhs - r0);
         // shared memory: per warp of a bundle f x nrhs doubles; a tiled task 2 x 64 + DF_CHUNK rows of
-        // nrhs doubles
+        // nrhs doubles; an inverse-panel forward task DF_PCOLS + 5 x 64 rows
         a.warp_smem = (int32_t)(((int64_t)P->df_fwarp_max * a.nrhs + 1) & ~int64_t(1));
-        const size_t smem = sizeof(double) * std::max<size_t>((size_t)a.warp_smem * (DF_THREADS / 32),
-                                                              (2 * DF_BLK + DF_CHUNK) * (size_t)DF_MAX_NRHS);
+        const size_t smem = sizeof(double) * std::max<size_t>({(size_t)a.warp_smem * (DF_THREADS / 32),
+                                                               (2 * DF_BLK + DF_CHUNK) * (size_t)DF_MAX_NRHS,
+                                                               (DF_PCOLS + 5 * DF_BLK) * (size_t)DF_MAX_NRHS});
         const int grid = dataflow_solve_grid<T>(a.nrhs, smem);
         if (grid <= 0) return fail(SDSB200_CUDA_ERROR, "no co-resident grid for the dataflow solve");
         a.in = in + (int64_t)r0 * ldin;

@@ -78,6 +78,16 @@ enum LaunchKind : int32_t {
     L_SCALE,           // W = L21 D of large LDLT / LU fronts
     L_CHOL_STEP,       // large Cholesky: one 32-column step (diagonal block + trsm of the rows below)
     L_DFINV,           // diagonal-block inverses of every front for the dataflow solve
+    L_PINV,            // GEMM tiles that build the inverse panels of the dataflow solve's tiled fronts
+};
+
+// One 64 x 64 output tile of the inverse-panel GEMMs: C = A B, or C = -A B (column-major operands)
+struct PinvTile {
+    int64_t a, b, c;     // element offsets of A (m x k), B (k x n) and C (m x n)
+    int32_t lda, ldb, ldc;
+    int32_t m, n, k;
+    int32_t front;       // skipped when this front failed
+    int32_t neg;
 };
 
 struct Launch {

@@ -447,71 +447,100 @@ cudaError_t launch_chol_step(const CholStepArgs<T>& a, int nmembers, cudaStream_
 template cudaError_t launch_chol_step<double>(const CholStepArgs<double>&, int, cudaStream_t);
 template cudaError_t launch_chol_step<float>(const CholStepArgs<float>&, int, cudaStream_t);
 
-// inverse of one 64 x 64 diagonal block of a panel (lower triangle as stored; unit or not), with the
-// register-owned right-looking substitution
+// Inverse of a lower-triangular 32 x 32 matrix held by the warp: lane c computes column c by forward
+// substitution, x_k = (delta_kc - sum_{j<k} L[k, j] x_j) r_k, with the reciprocals r_k = 1 / L[k, k]
+// taken up front (off the substitution's dependency chain). L(k, j) reads entry (k, j) (k, j < 32).
+template <class Get>
+__device__ __forceinline__ void warp_tri_inv32(Get L, int lane, double (&x)[32]) {
+    double rd[32];
+#pragma unroll
+    for (int k = 0; k < 32; ++k) rd[k] = 1.0 / L(k, k);
+#pragma unroll
+    for (int k = 0; k < 32; ++k) {
+        double acc = (k == lane) ? 1.0 : 0.0;
+#pragma unroll
+        for (int j = 0; j < k; ++j) acc -= L(k, j) * x[j];
+        x[k] = acc * rd[k];
+    }
+}
+
+// Inverse of one 64 x 64 diagonal block of a panel (lower triangle as stored; unit or not). Warps 0 and
+// 1 invert the two 32 x 32 diagonal sub-blocks X11 and X22 (a partial block is padded with the
+// identity), then X21 = -X22 (L21 X11) in two 32 x 32 products over the four warps. One shared array:
+// L, then X in place (X11 and X22 over L11 and L22, X21 over L21 once T = L21 X11 is formed in the
+// unused upper right quarter).
 template <typename T>
-__global__ void __launch_bounds__(256) block_inv_kernel(BlockInvArgs<T> A) {
-    constexpr int NB = 64, NE = NB * (NB + 1) / 2, SLOTS = (NE + 255) / 256;
-    __shared__ double colv[2][NB];
-    __shared__ double rowv[2][NB];
+__global__ void __launch_bounds__(128) block_inv_kernel(BlockInvArgs<T> A) {
+    constexpr int NB = 64, LD = NB + 1;
+    __shared__ double S[NB * LD];        // (i, j) at i + j LD
     const int s = A.tasks[2 * blockIdx.x], b = A.tasks[2 * blockIdx.x + 1];
     const int member = A.members ? A.members[blockIdx.y] : blockIdx.y;
     if (A.finfo && A.finfo[(int64_t)member * A.ns + s] != 0) return;
     const DFront fd = A.fronts[s];
     const int f = fd.f, jb = b * NB, nbb = min(NB, fd.w - jb);
     const T* P = A.panels + (int64_t)member * A.factor_len + fd.panel;
-    T* inv = A.dinv + (int64_t)member * A.dinv_len + A.dinv_off[s] + (int64_t)b * NB * NB;
-    const int tid = threadIdx.x;
-    int ri[SLOTS], ci[SLOTS];
-    double a[SLOTS], x[SLOTS];
-#pragma unroll
-    for (int k = 0; k < SLOTS; ++k) {
-        int e = tid + 256 * k, col = 0;
-        if (e < NE) {
-            int rem = e;
-            while (rem >= NB - col) { rem -= NB - col; ++col; }
-            ri[k] = col + rem;
-            ci[k] = col;
-        } else {
-            ri[k] = -1;
-            ci[k] = NB;
+    const int ldo = A.panel_layout ? f : NB;
+    T* inv = A.dinv + (int64_t)member * A.dinv_len + A.dinv_off[s] +
+             (A.panel_layout ? (int64_t)jb * (1 + f) : (int64_t)b * NB * NB);
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    for (int q = tid; q < NB * NB; q += blockDim.x) {
+        const int i = q % NB, j = q / NB;
+        double v = 0.0;
+        if (i < nbb && j < nbb) {
+            if (i >= j) v = (double)P[(jb + i) + (int64_t)(jb + j) * f];
+        } else if (i == j) {
+            v = 1.0;
         }
-        const bool in = ri[k] >= 0 && ri[k] < nbb && ci[k] < nbb;
-        a[k] = in ? (double)P[(jb + ri[k]) + (int64_t)(jb + ci[k]) * f] : 0.0;
-        x[k] = (in && ri[k] == ci[k]) ? 1.0 : 0.0;
+        S[i + j * LD] = v;
     }
-    for (int l = 0; l < nbb; ++l) {
-        double* cv = colv[l & 1];
-        double* rv = rowv[l & 1];
+    __syncthreads();
+    if (warp < 2) {
+        const int o = 32 * warp;
+        double x[32];
+        warp_tri_inv32([&](int k, int j) { return S[(o + k) + (o + j) * LD]; }, lane, x);
+        __syncwarp();
 #pragma unroll
-        for (int k = 0; k < SLOTS; ++k)
-            if (ci[k] == l) cv[ri[k]] = a[k];
-        __syncthreads();
-        const double rl = 1.0 / cv[l];
-#pragma unroll
-        for (int k = 0; k < SLOTS; ++k)
-            if (ri[k] == l) {
-                x[k] *= rl;
-                rv[ci[k]] = x[k];
-            }
-        __syncthreads();
-#pragma unroll
-        for (int k = 0; k < SLOTS; ++k)
-            if (ri[k] > l && ri[k] < nbb && ci[k] <= l) x[k] -= cv[ri[k]] * rv[ci[k]];
+        for (int k = 0; k < 32; ++k) S[(o + k) + (o + lane) * LD] = k >= lane ? x[k] : 0.0;
     }
-    for (int q = tid; q < NB * NB; q += 256) {
-        int i = q % NB, j = q / NB;
-        if (i < j || i >= nbb) inv[i + (int64_t)j * NB] = T(0);
+    __syncthreads();
+    const int c = tid & 31, r0 = 8 * (tid >> 5);
+    // T = L21 X11 into the upper right quarter: thread (c, rows r0 ..); X11 is lower triangular (j >= c)
+#pragma unroll
+    for (int rr = 0; rr < 8; ++rr) {
+        const int r = r0 + rr;
+        double acc = 0.0;
+        for (int j = c; j < 32; ++j) acc += S[(32 + r) + j * LD] * S[j + c * LD];
+        S[r + (32 + c) * LD] = acc;
+    }
+    __syncthreads();
+    // X21 = -X22 T over L21; X22 is lower triangular (j <= r)
+    double x21[8];
+#pragma unroll
+    for (int rr = 0; rr < 8; ++rr) {
+        const int r = r0 + rr;
+        double acc = 0.0;
+        for (int j = 0; j <= r; ++j) acc += S[(32 + r) + (32 + j) * LD] * S[j + (32 + c) * LD];
+        x21[rr] = -acc;
     }
     __syncthreads();
 #pragma unroll
-    for (int k = 0; k < SLOTS; ++k)
-        if (ri[k] >= 0 && ri[k] < nbb && ci[k] < nbb) inv[ri[k] + (int64_t)ci[k] * NB] = T(x[k]);
+    for (int rr = 0; rr < 8; ++rr) {
+        S[(32 + r0 + rr) + c * LD] = x21[rr];
+        S[(r0 + rr) + (32 + c) * LD] = 0.0;
+    }
+    __syncthreads();
+    for (int q = tid; q < NB * NB; q += blockDim.x) {
+        const int i = q % NB, j = q / NB;
+        if (A.panel_layout) {
+            if (i < nbb && j < nbb) inv[i + (int64_t)j * ldo] = T(i >= j ? S[i + j * LD] : 0.0);
+        } else {
+            inv[i + (int64_t)j * ldo] = T((i >= j && i < nbb && j < nbb) ? S[i + j * LD] : 0.0);
+        }
+    }
 }
 
-// L11^-1 of a warp front of the dataflow solve (w <= 32; unit or not, as stored), one warp per front:
-// lane c computes column c by forward substitution, X[k, c] = (delta_kc - sum_{j<k} L[k, j] X[j, c]) / L[k, k],
-// with row k of L11 read once per step (the same address for the whole warp)
+// L11^-1 of a warp front of the dataflow solve (w <= 32; unit or not, as stored), one warp per front,
+// padded with the identity past w
 template <typename T>
 __global__ void __launch_bounds__(256) small_inv_kernel(SmallInvArgs<T> A) {
     const int wi = (int)((blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5), lane = threadIdx.x & 31;
@@ -524,16 +553,7 @@ __global__ void __launch_bounds__(256) small_inv_kernel(SmallInvArgs<T> A) {
     const T* P = A.panels + (int64_t)member * A.factor_len + fd.panel;
     T* inv = A.inv + (int64_t)member * A.inv_len + A.inv_off[s];
     double x[32];
-#pragma unroll
-    for (int k = 0; k < 32; ++k) {
-        double acc = (k == lane) ? 1.0 : 0.0;
-        if (k < w) {
-#pragma unroll
-            for (int j = 0; j < k; ++j) acc -= (double)P[k + (int64_t)j * f] * x[j];
-            acc /= (double)P[k + (int64_t)k * f];
-        }
-        x[k] = (k < w && lane < w) ? acc : 0.0;
-    }
+    warp_tri_inv32([&](int k, int j) { return k < w ? (double)P[k + (int64_t)j * f] : (k == j ? 1.0 : 0.0); }, lane, x);
     if (lane < w) {
 #pragma unroll
         for (int k = 0; k < 32; ++k)
@@ -556,7 +576,7 @@ template <typename T>
 cudaError_t launch_block_inv(const BlockInvArgs<T>& a, int nmembers, cudaStream_t st) {
     if (a.count == 0) return cudaSuccess;
     dim3 grid(a.count, nmembers);
-    block_inv_kernel<T><<<grid, 256, 0, st>>>(a);
+    block_inv_kernel<T><<<grid, 128, 0, st>>>(a);
     return cudaGetLastError();
 }
 

@@ -176,7 +176,25 @@ struct BlockInvArgs {
     int64_t factor_len, dinv_len;
     const int32_t* finfo;
     int32_t ns;
+    int32_t panel_layout;      // 1: block b goes to rows and columns 64 b of the front's f x w inverse panel
+                               // (ld f, only the block's own entries written); 0: 64 x 64 blocks in turn
 };
+
+// The inverse-panel GEMMs (pinv_kernels.cu): C = +-A B over a list of 64 x 64 tiles
+template <typename T>
+struct PinvGemmArgs {
+    const PinvTile* tiles;
+    int32_t count;
+    const int32_t* members;
+    const T* abuf;
+    const T* bbuf;
+    T* cbuf;
+    int64_t astride, bstride, cstride;   // per-member strides
+    const int32_t* finfo;
+    int32_t ns;
+};
+template <typename T>
+cudaError_t launch_pinv_gemm(const PinvGemmArgs<T>& a, int nmembers, cudaStream_t st);
 template <typename T>
 cudaError_t launch_block_inv(const BlockInvArgs<T>& a, int nmembers, cudaStream_t st);
 

@@ -276,8 +276,10 @@ Plan* build_plan(const sdsb200_symbolic* sym, const sdsb200_plan_options* popts,
         }
         if (tune_wide && (tune_wide < 16 || tune_wide > DF_WARP_F))
             throw BuildError(SDSB200_INVALID_VALUE, "tuning: wide (the tallest warp front of the solve) must lie in 16..128");
-        (void)tune_rsv;   // bits 20..30: reserved, ignored
+        if (tune_rsv > 1)
+            throw BuildError(SDSB200_INVALID_VALUE, "tuning: chains must be 0 (inverse panels) or 1 (block chains)");
         const int warp_f = tune_wide ? tune_wide : DF_WARP_F;
+        const bool pinv_mode = tune_rsv == 0;   // tiled fronts solved through inverse panels
         P->fsmall_max = classes.back();
         auto class_of = [&](int f) {
             for (int c : classes)
@@ -545,7 +547,7 @@ Plan* build_plan(const sdsb200_symbolic* sym, const sdsb200_plan_options* popts,
             std::vector<int64_t> inv_off(ns, -1);
             std::vector<int32_t> small_list, blkinv;
             int64_t il = 0;
-            int32_t nblk = 0, npart = 0;
+            int32_t nblk = 0, npart = 0, ntcnt = 0, nccnt = 0;
             for (int64_t s = 0; s < ns; ++s) {
                 const DFront& F = P->fronts[s];
                 DfFront& d = df[s];
@@ -554,11 +556,29 @@ Plan* build_plan(const sdsb200_symbolic* sym, const sdsb200_plan_options* popts,
                 const int m = F.f - F.w;
                 d.tiled = !(F.w <= DF_WARP_W && F.f <= warp_f);
                 d.inv = inv_off[s] = il;
+                d.bsig = 1;
                 if (!d.tiled) {
                     il += ((int64_t)F.w * F.w + 1) & ~int64_t(1);
                     d.fsig = 1;
                     small_list.push_back((int32_t)s);
                     P->df_fwarp_max = std::max(P->df_fwarp_max, F.f);
+                } else if (pinv_mode) {
+                    // the f x w inverse panel; its diagonal blocks come from the block-inverse launch
+                    d.pinv = 1;
+                    d.nblk = (F.w + DF_BLK - 1) / DF_BLK;
+                    d.ntile = (F.f + DF_BLK - 1) / DF_BLK;
+                    d.pbblk = (F.w + DF_PBCOLS - 1) / DF_PBCOLS;
+                    d.fsig = d.ntile;
+                    d.bsig = d.pbblk;
+                    d.tcnt = ntcnt;
+                    d.ccnt = nccnt;
+                    ntcnt += d.ntile;
+                    nccnt += d.pbblk;
+                    il += ((int64_t)F.f * F.w + 1) & ~int64_t(1);
+                    for (int b = 0; b < d.nblk; ++b) {
+                        blkinv.push_back((int32_t)s);
+                        blkinv.push_back(b);
+                    }
                 } else {
                     d.nblk = (F.w + DF_BLK - 1) / DF_BLK;
                     d.ntile = (F.f + DF_BLK - 1) / DF_BLK;
@@ -627,25 +647,60 @@ Plan* build_plan(const sdsb200_symbolic* sym, const sdsb200_plan_options* popts,
                     bundles.insert(bundles.end(), wl.begin() + o, wl.begin() + o + cnt);
                 }
             };
+            // partial-product slots of the inverse-panel tasks: one per task of a tile (block) that has
+            // more than one; the task record carries the tile's (block's) first slot
+            int64_t npslot = 0;
+            auto slot_field = [&](int chunk, int nchunks) {
+                if (nchunks > 1 && npslot + nchunks > (int64_t(1) << 22))
+                    throw BuildError(SDSB200_INVALID_VALUE, "dataflow solve: too many partial slots");
+                return (int32_t)(chunk | ((nchunks > 1 ? npslot : 0) << 8));
+            };
             for (int L = 0; L < P->nlevels; ++L) {
                 for (int s : P->level_fronts[L]) {
                     if (s == P->schur_front || !df[s].tiled) continue;
-                    for (int t = 0; t < df[s].ntile; ++t) tasks.push_back(DfTask{DF_FW_TILE, s, t, 0});
+                    if (df[s].pinv) {
+                        const int w = P->fronts[s].w;
+                        if ((w + DF_PCOLS - 1) / DF_PCOLS > 255)
+                            throw BuildError(SDSB200_INVALID_VALUE, "dataflow solve: front too wide for the inverse panels");
+                        for (int t = 0; t < df[s].ntile; ++t) {
+                            const int nk = df_pf_chunks(w, t);
+                            for (int k = 0; k < nk; ++k) tasks.push_back(DfTask{DF_FW_PINV, s, t, slot_field(k, nk)});
+                            if (nk > 1) npslot += nk;
+                        }
+                    } else {
+                        for (int t = 0; t < df[s].ntile; ++t) tasks.push_back(DfTask{DF_FW_TILE, s, t, 0});
+                    }
                 }
                 push_bundles(L, DF_FW_BUNDLE);
             }
             for (int L = P->nlevels - 1; L >= 0; --L) {
                 for (int s : P->level_fronts[L]) {
                     if (s == P->schur_front || !df[s].tiled) continue;
-                    for (int b = 0; b < df[s].nblk; ++b)
-                        for (int c = 0; c < df[s].nchunk; ++c) tasks.push_back(DfTask{DF_BW_PART, s, b, c});
-                    for (int b = df[s].nblk - 1; b >= 0; --b) tasks.push_back(DfTask{DF_BW_OWNER, s, b, 0});
+                    if (df[s].pinv) {
+                        const int f = P->fronts[s].f;
+                        if ((f + DF_PROWS - 1) / DF_PROWS > 255)
+                            throw BuildError(SDSB200_INVALID_VALUE, "dataflow solve: front too tall for the inverse panels");
+                        for (int b = df[s].pbblk - 1; b >= 0; --b) {
+                            const int nr = df_pb_chunks(f, b), r0 = df_pb_first(b);
+                            for (int k = 0; k < nr; ++k)
+                                tasks.push_back(DfTask{DF_BW_PINV, s, b, slot_field(r0 + k, nr)});
+                            if (nr > 1) npslot += nr;
+                        }
+                    } else {
+                        for (int b = 0; b < df[s].nblk; ++b)
+                            for (int c = 0; c < df[s].nchunk; ++c) tasks.push_back(DfTask{DF_BW_PART, s, b, c});
+                        for (int b = df[s].nblk - 1; b >= 0; --b) tasks.push_back(DfTask{DF_BW_OWNER, s, b, 0});
+                    }
                 }
                 push_bundles(L, DF_BW_BUNDLE);
             }
             P->df_inv_len = std::max<int64_t>(il, 2);
             P->df_nblk = nblk;
-            P->df_flags_len = 2 * ns + 2 * (int64_t)nblk + 8;
+            P->df_ntcnt = ntcnt;
+            P->df_nccnt = nccnt;
+            P->df_pinv = pinv_mode;
+            // fcnt, bdone (ns each), xflag, pcnt (nblk each), tcnt, ccnt, the task counter
+            P->df_flags_len = 2 * ns + 2 * (int64_t)nblk + ntcnt + nccnt + 8;
             P->n_df_tasks = (int32_t)tasks.size();
             P->n_df_small = (int32_t)small_list.size();
             P->n_df_blkinv = (int32_t)(blkinv.size() / 2);
@@ -653,18 +708,150 @@ Plan* build_plan(const sdsb200_symbolic* sym, const sdsb200_plan_options* popts,
             P->d_df_tasks = upload(P, tasks, st);
             P->d_df_bundles = upload(P, bundles, st);
             P->d_df_inv_off = upload(P, inv_off, st);
-            P->d_df_small = upload(P, small_list, st);
-            P->d_df_blkinv = upload(P, blkinv, st);
+
             P->d_df_rptr = upload(P, rptr, st);
             P->d_df_csrc = upload(P, csrc, st);
-            P->d_df_part = dalloc<double>(P, std::max<int64_t>(1, (int64_t)npart * DF_BLK * DF_MAX_NRHS));
+            P->d_df_part = dalloc<double>(P, std::max<int64_t>(1, std::max<int64_t>(npart, npslot) * DF_BLK * DF_MAX_NRHS));
             P->d_df_flags = dalloc<unsigned int>(P, P->df_flags_len);
             P->d_df_trace = dalloc<int64_t>(P, 6 * (int64_t)std::max<int32_t>(1, P->n_df_tasks));
-            ProgLaunch il_{};
-            il_.kind = L_DFINV;
-            il_.level = P->nlevels;
-            il_.count = P->n_df_small + P->n_df_blkinv;
-            P->prog.push_back(il_);
+            // The inverses are built level by level on the side stream, each level's right after its
+            // factorization launches (single-system plans only: a batch is solved by the per-level
+            // sweeps). Per level: the warp fronts' L11^-1 and the tiled fronts' 64 x 64 diagonal-block
+            // inverses; then for the inverse-panel fronts L11^-1 by recursive doubling over those blocks
+            // (at each doubling level, for every pair of adjacent aligned block ranges A (full, h blocks)
+            // and C (up to h blocks): T = L[C, A] X[A, A] into the scratch, X[C, A] = -X[C, C] T) and
+            // the update rows L21 X. X lives in the inverse panel (ld f).
+            if (P->nbatch == 1) {
+                std::vector<std::vector<ProgLaunch>> side(P->nlevels);
+                std::vector<int32_t> small_sorted, blk_sorted;
+                std::vector<PinvTile> pt;
+                auto bw_of = [](int w, int b) { return std::min(DF_BLK, w - DF_BLK * b); };
+                int64_t pwork = 0;
+                for (int L = 0; L < P->nlevels; ++L) {
+                    std::vector<int> pf;   // the level's inverse-panel fronts
+                    ProgLaunch il_{};
+                    il_.kind = L_DFINV;
+                    il_.level = L;
+                    il_.side = 1;
+                    il_.list = (int64_t)small_sorted.size();
+                    il_.list2 = (int64_t)blk_sorted.size() / 2;
+                    for (int s : P->level_fronts[L]) {
+                        if (s == P->schur_front) continue;
+                        if (!df[s].tiled) {
+                            small_sorted.push_back(s);
+                            continue;
+                        }
+                        for (int b = 0; b < df[s].nblk; ++b) {
+                            blk_sorted.push_back(s);
+                            blk_sorted.push_back(b);
+                        }
+                        if (df[s].pinv) pf.push_back(s);
+                    }
+                    il_.count = to_i32((int64_t)small_sorted.size() - il_.list, "inverse launch");
+                    il_.count2 = to_i32((int64_t)blk_sorted.size() / 2 - il_.list2, "inverse launch");
+                    if (il_.count + il_.count2 > 0) side[L].push_back(il_);
+                    auto push_launch = [&](size_t first, int cls) {
+                        ProgLaunch pl{};
+                        pl.kind = L_PINV;
+                        pl.level = L;
+                        pl.side = 1;
+                        pl.cls = cls;
+                        pl.list = (int64_t)first;
+                        pl.count = to_i32((int64_t)(pt.size() - first), "inverse-panel tiles");
+                        for (size_t q = first; q < pt.size(); ++q) pl.flops += 2.0 * pt[q].m * pt[q].n * pt[q].k;
+                        if (pl.count > 0) side[L].push_back(pl);
+                    };
+                    int maxK = 0;
+                    for (int s : pf) maxK = std::max(maxK, df[s].nblk);
+                    for (int h = 1; h < maxK; h *= 2) {
+                        std::vector<PinvTile> g2;
+                        const size_t first = pt.size();
+                        int64_t toff = 0;
+                        for (int s : pf) {
+                            const DFront& F = P->fronts[s];
+                            const int K = df[s].nblk, f = F.f, w = F.w;
+                            const int64_t po = inv_off[s], pa = F.panel;
+                            for (int a0 = 0; a0 + h < K; a0 += 2 * h) {
+                                const int c0 = a0 + h, c1 = std::min(a0 + 2 * h, K);
+                                const int rowsC = std::min(w, DF_BLK * c1) - DF_BLK * c0;
+                                for (int ci = c0; ci < c1; ++ci)
+                                    for (int aj = a0; aj < c0; ++aj) {
+                                        PinvTile t1{};
+                                        t1.a = pa + DF_BLK * ci + (int64_t)DF_BLK * aj * f;
+                                        t1.lda = f;
+                                        t1.b = po + DF_BLK * aj + (int64_t)DF_BLK * aj * f;
+                                        t1.ldb = f;
+                                        t1.c = toff + DF_BLK * (ci - c0) + (int64_t)DF_BLK * (aj - a0) * rowsC;
+                                        t1.ldc = rowsC;
+                                        t1.m = bw_of(w, ci);
+                                        t1.n = DF_BLK;
+                                        t1.k = DF_BLK * (c0 - aj);
+                                        t1.front = (int32_t)s;
+                                        pt.push_back(t1);
+                                        PinvTile t2{};
+                                        t2.a = po + DF_BLK * ci + (int64_t)DF_BLK * c0 * f;
+                                        t2.lda = f;
+                                        t2.b = toff + (int64_t)DF_BLK * (aj - a0) * rowsC;
+                                        t2.ldb = rowsC;
+                                        t2.c = po + DF_BLK * ci + (int64_t)DF_BLK * aj * f;
+                                        t2.ldc = f;
+                                        t2.m = bw_of(w, ci);
+                                        t2.n = DF_BLK;
+                                        t2.k = DF_BLK * (ci - c0) + bw_of(w, ci);
+                                        t2.front = (int32_t)s;
+                                        t2.neg = 1;
+                                        g2.push_back(t2);
+                                    }
+                                toff += (int64_t)rowsC * DF_BLK * h;
+                            }
+                        }
+                        pwork = std::max(pwork, toff);
+                        push_launch(first, 1);
+                        const size_t first2 = pt.size();
+                        pt.insert(pt.end(), g2.begin(), g2.end());
+                        push_launch(first2, 2);
+                    }
+                    const size_t firstw = pt.size();
+                    for (int s : pf) {
+                        const DFront& F = P->fronts[s];
+                        const int K = df[s].nblk, f = F.f, w = F.w, m = f - w;
+                        const int64_t po = inv_off[s], pa = F.panel;
+                        for (int r0 = 0; r0 < m; r0 += DF_BLK)
+                            for (int aj = 0; aj < K; ++aj) {
+                                PinvTile t{};
+                                t.a = pa + w + r0 + (int64_t)DF_BLK * aj * f;
+                                t.lda = f;
+                                t.b = po + DF_BLK * aj + (int64_t)DF_BLK * aj * f;
+                                t.ldb = f;
+                                t.c = po + w + r0 + (int64_t)DF_BLK * aj * f;
+                                t.ldc = f;
+                                t.m = std::min(DF_BLK, m - r0);
+                                t.n = bw_of(w, aj);
+                                t.k = w - DF_BLK * aj;
+                                t.front = (int32_t)s;
+                                pt.push_back(t);
+                            }
+                    }
+                    push_launch(firstw, 3);
+                }
+                P->d_df_small = upload(P, small_sorted, st);
+                P->d_df_blkinv = upload(P, blk_sorted, st);
+                P->pwork_len = pinv_mode ? std::max<int64_t>(pwork, 2) : 0;
+                P->d_pinv_tiles = upload(P, pt, st);
+                // every level's side launches right after the level's last launch of the factorization
+                std::vector<ProgLaunch> merged;
+                for (size_t q = 0; q < P->prog.size(); ++q) {
+                    merged.push_back(P->prog[q]);
+                    const int L = P->prog[q].level;
+                    const bool last_of_level = q + 1 == P->prog.size() || P->prog[q + 1].level != L;
+                    if (last_of_level && L >= 0 && L < P->nlevels) {
+                        merged.insert(merged.end(), side[L].begin(), side[L].end());
+                        side[L].clear();
+                    }
+                }
+                for (int L = 0; L < P->nlevels; ++L) merged.insert(merged.end(), side[L].begin(), side[L].end());
+                P->prog.swap(merged);
+            }
         }
         {
             ProgLaunch pl{};
@@ -872,6 +1059,7 @@ Plan* build_plan(const sdsb200_symbolic* sym, const sdsb200_plan_options* popts,
         if (P->inv_len) P->d_inv = alloc_bytes(es * P->inv_len * nb);
         P->d_dfinv_L = alloc_bytes(es * P->df_inv_len * nb);
         if (gen) P->d_dfinv_U = alloc_bytes(es * P->df_inv_len * nb);
+        if (P->pwork_len) P->d_pwork = alloc_bytes(es * P->pwork_len * nb * (gen ? 2 : 1));
         P->d_xtmp = dalloc<double>(P, n * P->max_nrhs);
         P->d_solve_status = dalloc<int32_t>(P, 1);
         cudaMemsetAsync(P->d_solve_status, 0, sizeof(int32_t), st);
@@ -897,9 +1085,16 @@ Plan* build_plan(const sdsb200_symbolic* sym, const sdsb200_plan_options* popts,
             if ((int64_t)small_front_smem(P->fsmall_max, P->elsize) > optin)
                 throw BuildError(SDSB200_NOT_SUPPORTED, "shared memory per block too small for the front classes");
         }
-        if (cudaStreamCreateWithFlags(&P->own, cudaStreamNonBlocking) != cudaSuccess ||
+        // the capture stream at the highest priority, the side stream (the solve's inverses, beside the
+        // factorization) at the lowest
+        int prio_low = 0, prio_high = 0;
+        cudaDeviceGetStreamPriorityRange(&prio_low, &prio_high);
+        if (cudaStreamCreateWithPriority(&P->own, cudaStreamNonBlocking, prio_high) != cudaSuccess ||
+            cudaStreamCreateWithPriority(&P->side, cudaStreamNonBlocking, prio_low) != cudaSuccess ||
             cudaEventCreateWithFlags(&P->join_in, cudaEventDisableTiming) != cudaSuccess ||
-            cudaEventCreateWithFlags(&P->join_out, cudaEventDisableTiming) != cudaSuccess)
+            cudaEventCreateWithFlags(&P->join_out, cudaEventDisableTiming) != cudaSuccess ||
+            cudaEventCreateWithFlags(&P->side_fork, cudaEventDisableTiming) != cudaSuccess ||
+            cudaEventCreateWithFlags(&P->side_join, cudaEventDisableTiming) != cudaSuccess)
             throw BuildError(SDSB200_CUDA_ERROR, "stream or event creation failed");
         cudaMemsetAsync(P->d_psign, 0, n, st);
         cudaMemsetAsync(P->d_kind, 0, n * nb, st);
@@ -938,7 +1133,10 @@ void free_plan(Plan* P) {
         if (g->exec) cudaGraphExecDestroy(g->exec);
     if (P->join_in) cudaEventDestroy(P->join_in);
     if (P->join_out) cudaEventDestroy(P->join_out);
+    if (P->side_fork) cudaEventDestroy(P->side_fork);
+    if (P->side_join) cudaEventDestroy(P->side_join);
     if (P->own) cudaStreamDestroy(P->own);
+    if (P->side) cudaStreamDestroy(P->side);
     if (P->h_norms) cudaFreeHost(P->h_norms);
     if (P->h_info_pinned) cudaFreeHost(P->h_info_pinned);
     delete P;

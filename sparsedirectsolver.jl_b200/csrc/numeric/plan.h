@@ -31,6 +31,10 @@ struct ProgLaunch {
     int32_t coop_grid = 0;  // pivot: CTAs of the cooperative launch
     int32_t exact = 0;      // gemm: the contribution-block update of an LDLT / LU front, which the FP64
                             // form sums in the oracle's order (1: LDLT, 2: LU)
+    int32_t side = 0;       // runs on the plan's side stream (the solve's inverses, off the factorization's
+                            // critical path), after the main stream's launches that precede it
+    int64_t list2 = 0;      // inverses: first (front, block) pair of the block inverses; count2 pairs
+    int32_t count2 = 0;
 };
 
 // per-kind accounting of the profiling mode (CUDA events around every launch)
@@ -113,6 +117,11 @@ struct Plan {
     unsigned int* d_df_flags = nullptr; // fcnt (ns), bdone (ns), xflag (nblk), pcnt (nblk), head
     int64_t df_flags_len = 0;
     int32_t df_nblk = 0;
+    int32_t df_ntcnt = 0, df_nccnt = 0;  // inverse panels: forward row-tile and backward column-block counters
+    bool df_pinv = false;               // tiled fronts solved through their inverse panels
+    PinvTile* d_pinv_tiles = nullptr;   // the GEMM tiles that build the inverse panels (kind L_PINV)
+    int64_t pwork_len = 0;              // their scratch (T = L[C, A] X[A, A] of one doubling level), per member and side
+    void* d_pwork = nullptr;
     double* d_df_part = nullptr;        // backward partial sums: slots of 64 x DF_MAX_NRHS doubles
     int64_t* d_df_trace = nullptr;      // profiling: 6 int64 per task (start, wait done, end, CTA, kind, a | b << 32)
     int32_t df_fwarp_max = 1;           // tallest warp front
@@ -153,6 +162,8 @@ struct Plan {
     bool persistent = true;        // the one-launch dataflow solve for a single active member
     cudaStream_t own = nullptr;          // capture / replay stream, joined to the caller's by events
     cudaEvent_t join_in = nullptr, join_out = nullptr;
+    cudaStream_t side = nullptr;         // low-priority stream of the side launches of the factorization
+    cudaEvent_t side_fork = nullptr, side_join = nullptr;
     CachedGraph g_factor, g_solve, g_resid, g_corr;
 
     bool profile = false;

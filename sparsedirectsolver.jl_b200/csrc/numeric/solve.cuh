@@ -40,11 +40,18 @@ struct SweepArgs {
 // Front classes:
 //  * warp fronts (w <= DF_WARP_W and f <= DF_WARP_F): one warp each; DF_BUNDLE fronts of one level per
 //    task, taken by the CTA's warps in turn. L11^-1 (w x w, ld w) is precomputed after the factorization.
-//  * tiled fronts (the rest): forward = one task per 64-row tile, which gathers its own rows (the right-
-//    hand side and the children's updates) and takes the 64-column blocks k <= t in order (block t's
-//    own tile solves it with the precomputed 64 x 64 inverse and publishes x_t); backward = partial-sum
-//    tasks over DF_CHUNK-row chunks of the update rows (-L21^T x2 per block) and one owner task per
-//    64-column block, from the last block to the first.
+//  * tiled fronts (the rest), in one of two forms chosen per plan:
+//    - inverse panels (default): the front's f x w inverse panel P = [L11^-1; L21 L11^-1] (ld f) is
+//      precomputed after the factorization, so that the forward is [x1; u - u_children] = P z1 and the
+//      backward x1 = P^T [y1; -x2]: one matrix-vector product per sweep, split into tasks over
+//      (64-row tile, DF_PCOLS-column chunk) in the forward and (DF_PBCOLS-column block, DF_PROWS-row
+//      chunk) in the backward; the last task of a tile or block to finish (a counter) sums the
+//      partial products in chunk order;
+//    - block chains: forward = one task per 64-row tile, which gathers its own rows (the right-hand
+//      side and the children's updates) and takes the 64-column blocks k <= t in order (block t's own
+//      tile solves it with the precomputed 64 x 64 inverse and publishes x_t); backward = partial-sum
+//      tasks over DF_CHUNK-row chunks of the update rows (-L21^T x2 per block) and one owner task per
+//      64-column block, from the last block to the first.
 // The children's updates reach a front through per-row contribution lists (the child update rows that
 // land on each front row, in child order), so every row is gathered by one thread with independent
 // loads and a fixed summation order.
@@ -55,17 +62,39 @@ constexpr int DF_BLK = 64;        // tile rows and block columns of the tiled fr
 constexpr int DF_CHUNK = 128;     // update rows per backward partial task
 constexpr int DF_MAX_NRHS = 8;    // right-hand sides per launch (more are solved in groups of 8)
 constexpr int DF_THREADS = 256;
+constexpr int DF_PCOLS = 128;     // inverse panels, forward: columns per task (a 64 x 128 part of P)
+constexpr int DF_PBCOLS = 32;     // inverse panels, backward: columns per task ...
+constexpr int DF_PROWS = 128;     // ... and rows (a 128 x 32 part of P)
 
-enum DfTaskKind : int32_t { DF_FW_BUNDLE = 1, DF_FW_TILE = 3, DF_BW_BUNDLE = 4, DF_BW_PART = 5, DF_BW_OWNER = 6 };
+enum DfTaskKind : int32_t {
+    DF_FW_BUNDLE = 1, DF_FW_TILE = 3, DF_BW_BUNDLE = 4, DF_BW_PART = 5, DF_BW_OWNER = 6, DF_FW_PINV = 7, DF_BW_PINV = 8
+};
 
 struct DfTask {
     int32_t kind, a, b, c;   // bundle: a = offset in the bundle list, b = count; tile: a = front, b = tile;
-                             // part: a = front, b = block, c = chunk; owner: a = front, b = block
+                             // part: a = front, b = block, c = chunk; owner: a = front, b = block;
+                             // inverse panel: a = front, b = row tile (forward) or column block (backward),
+                             // c = chunk | first partial slot of the tile or block << 8
 };
 
+// inverse-panel fronts: column chunks of forward row tile t, and row chunks of backward column block b
+// (the first one, b DF_PBCOLS / DF_PROWS, is the first that reaches the block's diagonal)
+__host__ __device__ inline int df_pf_chunks(int w, int t) {
+    const int cols = w < DF_BLK * (t + 1) ? w : DF_BLK * (t + 1);
+    return (cols + DF_PCOLS - 1) / DF_PCOLS;
+}
+__host__ __device__ inline int df_pb_first(int b) { return (DF_PBCOLS * b) / DF_PROWS; }
+__host__ __device__ inline int df_pb_chunks(int f, int b) { return (f + DF_PROWS - 1) / DF_PROWS - df_pb_first(b); }
+
 struct DfFront {
-    int64_t inv;       // offset of the front's diagonal-block inverses (warp: w x w; tiled: nblk x 64 x 64)
+    int64_t inv;       // offset of the front's inverses (warp: L11^-1, w x w; tiled: the inverse panel,
+                       // f x w, or the nblk 64 x 64 diagonal-block inverses)
     int32_t tiled;     // 0: warp front; 1: tiled
+    int32_t pinv;      // tiled: solved through its inverse panel
+    int32_t bsig;      // backward signals of this front (its children wait for bdone >= bsig)
+    int32_t tcnt;      // inverse panel: first of its forward row-tile counters
+    int32_t ccnt;      // inverse panel: first of its backward column-block counters
+    int32_t pbblk;     // inverse panel: backward column blocks (DF_PBCOLS wide)
     int32_t ntile;     // tiled: 64-row tiles of the forward
     int32_t nblk;      // tiled: 64-column blocks
     int32_t nchunk;    // tiled: backward partial tasks per block (0: the owners sum the update rows themselves)
@@ -101,12 +130,15 @@ struct DataflowArgs {
     int64_t ldin, ldout, n;
     double* Y;                 // n x nrhs: forward result (pre-D) then solution, factor order
     double* U;                 // update vectors, (global update row) x nrhs, row-major
-    double* xtmp;              // n x nrhs: a tiled front's published block solutions
+    double* xtmp;              // n x nrhs: a tiled front's published block solutions; an inverse-panel
+                               // front's forward result (its backward then writes the solution into Y)
     double* part;              // backward partial sums
     unsigned int* fcnt;        // ns: forward signals received (from children; at a root from itself)
     unsigned int* bdone;       // ns: 1 once the front's backward solution is in Y
     unsigned int* xflag;       // per block: 1 forward x_k published, 2 backward x_k published
     unsigned int* pcnt;        // per block: backward partials written
+    unsigned int* tcnt;        // inverse panels: per forward row tile, partial products written
+    unsigned int* ccnt;        // inverse panels: per backward column block, partial products written
     unsigned int* head;        // the task counter
     int32_t* status;           // nonzero: a bounded wait gave up
     int32_t nrhs;              // <= DF_MAX_NRHS

@@ -69,13 +69,17 @@ __device__ __forceinline__ void df_release(unsigned int* p, unsigned int v) {
     asm volatile("st.release.gpu.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
 }
 
-// publish: the CTA's writes, then one thread's fence and release of the flag (or increment of the
-// counter); the barrier orders the other threads' writes before that thread's fence
+// counter increment with release semantics (no fence of its own)
+__device__ __forceinline__ void df_release_add(unsigned int* p) {
+    asm volatile("red.release.gpu.global.add.u32 [%0], 1;" ::"l"(p) : "memory");
+}
+
+// publish: the CTA's writes, then one thread's release of the flag (or release increment of the
+// counter); the barrier orders the other threads' writes before that thread's release
 __device__ __forceinline__ void df_publish_cta(unsigned int* p, unsigned int v, bool add) {
     __syncthreads();
     if (threadIdx.x == 0) {
-        __threadfence();
-        if (add) atomicAdd(p, 1u);
+        if (add) df_release_add(p);
         else df_release(p, v);
     }
 }
@@ -88,23 +92,24 @@ __device__ __forceinline__ double quad_sum(double v) {
 }
 
 // y = D^{-1} z at factor position g (1x1 pivots, and the 2x2 blocks of LDLT: a = d[k], b = d[n + k],
-// c = d[k + 1] of the block's first position k) for right-hand side r, z read from Y
+// c = d[k + 1] of the block's first position k) for right-hand side r, z read from Z (n x nrhs: Y, or
+// xtmp for an inverse-panel front)
 template <typename T>
-__device__ __forceinline__ double df_dinv(const DataflowArgs<T>& A, int64_t g, int r) {
+__device__ __forceinline__ double df_dinv(const DataflowArgs<T>& A, const double* Z, int64_t g, int r) {
     const int64_t n = A.n;
-    const double y = A.Y[g + r * n];
+    const double y = Z[g + r * n];
     if (A.diag_mode == 0) return y;
     if (A.diag_mode == 1) return y / A.d[g];
     const int kk = A.kind[g];
     if (kk == KIND_2X2_FIRST) {
         const double a = A.d[g], b = A.d[n + g], c = A.d[g + 1];
         const double det = a * c - b * b;
-        return (c * y - b * A.Y[g + 1 + r * n]) / det;
+        return (c * y - b * Z[g + 1 + r * n]) / det;
     }
     if (kk == KIND_2X2_SECOND) {
         const double a = A.d[g - 1], b = A.d[n + g - 1], c = A.d[g];
         const double det = a * c - b * b;
-        return (a * y - b * A.Y[g - 1 + r * n]) / det;
+        return (a * y - b * Z[g - 1 + r * n]) / det;
     }
     return y / A.d[g];
 }
@@ -276,10 +281,7 @@ __device__ __noinline__ void df_warp_forward(const DataflowArgs<T>& A, int s, do
             }
     }
     __syncwarp();
-    if (lane == 0) {
-        __threadfence();
-        atomicAdd(A.fcnt + (fd.parent >= 0 ? fd.parent : s), 1u);
-    }
+    if (lane == 0) df_release_add(A.fcnt + (fd.parent >= 0 ? fd.parent : s));
     __syncwarp();
 }
 
@@ -306,15 +308,16 @@ __device__ __noinline__ void df_warp_backward(const DataflowArgs<T>& A, int s, d
     double lv0[16];
 #pragma unroll
     for (int e = 0; e < 16; ++e) lv0[e] = (lane < w && e < m) ? (double)Lc[e] : 0.0;
+    const unsigned pbsig = fd.parent >= 0 ? (unsigned)A.df[fd.parent].bsig : 0u;
     if (lane == 0) {
-        if (fd.parent >= 0) df_wait(A.bdone + fd.parent, 1u, A.status);
+        if (fd.parent >= 0) df_wait(A.bdone + fd.parent, pbsig, A.status);
         else df_wait(A.fcnt + s, (unsigned)(q.fneed + q.fsig), A.status);
         if (stamp) *stamp = (int64_t)df_clock();
     }
     __syncwarp();
     double y[NR];
 #pragma unroll
-    for (int r = 0; r < NR; ++r) y[r] = (lane < w && r < nrhs) ? df_dinv(A, fd.c0 + lane, r) : 0.0;
+    for (int r = 0; r < NR; ++r) y[r] = (lane < w && r < nrhs) ? df_dinv(A, A.Y, fd.c0 + lane, r) : 0.0;
     // x2: the solution at the rows below the front's columns (final: every ancestor is done)
     double* x2 = z;                 // m x nrhs
     double* ys = z + m * nrhs;      // w x nrhs
@@ -376,10 +379,7 @@ __device__ __noinline__ void df_warp_backward(const DataflowArgs<T>& A, int s, d
             }
     }
     __syncwarp();
-    if (lane == 0) {
-        __threadfence();
-        df_release(A.bdone + s, 1u);
-    }
+    if (lane == 0) df_release(A.bdone + s, 1u);
     __syncwarp();
 }
 
@@ -590,8 +590,9 @@ __device__ __noinline__ void df_tiled_part(const DataflowArgs<T>& A, int s, int 
 #pragma unroll
     for (int e = 0; e < DF_CHUNK / 4; ++e) lv[e] = (j < bw && qq + 4 * e < cnt) ? (double)Lc[qq + 4 * e] : 0.0;
     const int32_t ridx = tid < cnt ? A.rowval[fd.row_begin + w + r0 + tid] : 0;
+    const unsigned pbsig = (unsigned)A.df[fd.parent].bsig;
     if (tid == 0) {
-        df_wait(A.bdone + fd.parent, 1u, A.status);
+        df_wait(A.bdone + fd.parent, pbsig, A.status);
         if (stamp) *stamp = (int64_t)df_clock();
     }
     __syncthreads();
@@ -648,9 +649,10 @@ __device__ __noinline__ void df_tiled_owner(const DataflowArgs<T>& A, int s, int
     const bool inline_part = C == 0 && m > 0;
     const int32_t ridx = (inline_part && tid < m) ? A.rowval[fd.row_begin + w + tid] : 0;
     if (inline_part) df_prefetch_block_rows(L, f, w, b, bw, 0, m);
+    const unsigned pbsig = fd.parent >= 0 ? (unsigned)A.df[fd.parent].bsig : 0u;
     if (tid == 0) {
         if (C > 0) df_wait(A.pcnt + q.blk + b, (unsigned)C, A.status);
-        else if (fd.parent >= 0) df_wait(A.bdone + fd.parent, 1u, A.status);
+        else if (fd.parent >= 0) df_wait(A.bdone + fd.parent, pbsig, A.status);
         else df_wait(A.fcnt + s, (unsigned)(q.fneed + q.fsig), A.status);
         if (stamp) *stamp = (int64_t)df_clock();
     }
@@ -660,7 +662,7 @@ __device__ __noinline__ void df_tiled_owner(const DataflowArgs<T>& A, int s, int
         const int jr = idx % DF_BLK, r = idx / DF_BLK;
         double v = 0.0;
         if (jr < bw && r < nrhs) {
-            v = df_dinv(A, fd.c0 + DF_BLK * b + jr, r);
+            v = df_dinv(A, A.Y, fd.c0 + DF_BLK * b + jr, r);
             for (int c = 0; c < C; ++c)
                 v -= A.part[((int64_t)q.part + (int64_t)b * C + c) * (DF_BLK * NR) + jr + DF_BLK * r];
         }
@@ -738,6 +740,296 @@ __device__ __noinline__ void df_tiled_owner(const DataflowArgs<T>& A, int s, int
     df_publish_cta(A.bdone + s, 1u, false);
 }
 
+// ---------------------------------------------------------------------------------------------------
+// inverse-panel fronts: P = [L11^-1; L21 L11^-1] (f x w, ld f) of the front's panel; the part of L11^-1
+// above its diagonal is never read (masked by index)
+
+// Called by every thread after the CTA wrote its partial product: the counter of the tile (or block)
+// counts the tasks done (one acquire-release increment per task); true in the CTA that arrived last,
+// after the other tasks' partials are visible
+__device__ __forceinline__ bool df_last_arrival(unsigned int* cnt, unsigned count, int* flag) {
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        unsigned old;
+        asm volatile("atom.acq_rel.gpu.global.add.u32 %0, [%1], 1;" : "=r"(old) : "l"(cnt) : "memory");
+        *flag = old + 1 == count;
+    }
+    __syncthreads();
+    return *flag != 0;
+}
+
+// one halving step of a cross-lane reduction of NV values: lanes with bit O set keep the upper half
+template <int NV, int O>
+__device__ __forceinline__ void df_fold(double* v, int lane) {
+    const bool upper = (lane & O) != 0;
+#pragma unroll
+    for (int i = 0; i < NV / 2; ++i) {
+        const double send = upper ? v[i] : v[i + NV / 2];
+        const double keep = upper ? v[i + NV / 2] : v[i];
+        v[i] = keep + __shfl_xor_sync(0xffffffffu, send, O);
+    }
+}
+
+// the warp sums of NV (a power of two, <= 32) values per lane: lane l returns the sum over the warp of
+// value l / (32 / NV), in a fixed order
+template <int NV>
+__device__ __forceinline__ double df_lane_reduce(double* v, int lane) {
+    if constexpr (NV >= 2) df_fold<NV, 16>(v, lane); else v[0] += __shfl_xor_sync(0xffffffffu, v[0], 16);
+    if constexpr (NV >= 4) df_fold<NV / 2, 8>(v, lane); else v[0] += __shfl_xor_sync(0xffffffffu, v[0], 8);
+    if constexpr (NV >= 8) df_fold<NV / 4, 4>(v, lane); else v[0] += __shfl_xor_sync(0xffffffffu, v[0], 4);
+    if constexpr (NV >= 16) df_fold<NV / 8, 2>(v, lane); else v[0] += __shfl_xor_sync(0xffffffffu, v[0], 2);
+    if constexpr (NV >= 32) df_fold<NV / 16, 1>(v, lane); else v[0] += __shfl_xor_sync(0xffffffffu, v[0], 1);
+    return v[0];
+}
+
+// Forward of an inverse-panel front, row tile t (64 rows) times column chunk kc of P:
+// [x1; u] = P z1 + [0; children's updates], z1 = the own rows' right-hand side minus the children's
+// updates (local pivot order). 256 threads: thread (i = tid % 64, g = tid / 64) takes row i of the tile
+// over 32 columns of the chunk; the four groups' sums add in order. With several chunks the tasks write
+// partial products and the last one sums them in chunk order. x1 goes to xtmp (the backward reads it
+// there), u to the update vectors.
+template <typename T, int NR>
+__device__ __noinline__ void df_pinv_forward(const DataflowArgs<T>& A, int s, int t, int cc, double* sm, int64_t* stamp) {
+    __shared__ int last;
+    const DFront fd = A.fronts[s];
+    const DfFront q = A.df[s];
+    const int f = fd.f, w = fd.w, nrhs = A.nrhs, tid = threadIdx.x;
+    const int64_t n = A.n;
+    const int kc = cc & 255, slot0 = cc >> 8;
+    const int nkc = df_pf_chunks(w, t);
+    const int i = tid & (DF_BLK - 1), g = tid >> 6;
+    const int row = DF_BLK * t + i;
+    const int col0 = DF_PCOLS * kc;
+    const int ncol = min(DF_PCOLS, w - col0);
+    const T* Pm = A.invf + q.inv;
+    double* zs = sm;                          // DF_PCOLS x NR: z1 over the chunk's columns
+    double* red = zs + DF_PCOLS * NR;         // NR x 4 x 64: the column groups' sums
+    double* pass = red + 4 * DF_BLK * NR;     // 64 x NR: the tile's update rows, minus the children's updates
+    // before the children are done: the thread's 32 entries of P, the chunk's own rows' right-hand side
+    // and contribution lists (threads < ncol), with the first chunk the contribution lists of the tile's
+    // update rows (threads DF_PCOLS + i)
+    T pv[32];
+#pragma unroll
+    for (int e = 0; e < 32; ++e) {
+        const int col = col0 + 32 * g + e;
+        pv[e] = (row < f && col < w && (row >= w || col <= row)) ? Pm[row + (int64_t)col * f] : T(0);
+    }
+    const int prow = tid < DF_PCOLS ? col0 + tid : DF_BLK * t + (tid - DF_PCOLS);
+    const bool own = tid < ncol;
+    const bool thru = kc == 0 && tid >= DF_PCOLS && tid < DF_PCOLS + DF_BLK && prow >= w && prow < f;
+    RowPull rp{0, 0, {-1, -1, -1, -1}};
+    double val[NR];
+#pragma unroll
+    for (int r = 0; r < NR; ++r) val[r] = 0.0;
+    if (own) {
+        const int srow = A.reorder_fw ? A.piv[fd.c0 + prow] - 1 - fd.c0 : prow;
+        rp = df_row_pull_prep(A.rptr, A.csrc, (int64_t)q.rbase + srow);
+        const int64_t src = A.perm[fd.c0 + srow];
+#pragma unroll
+        for (int r = 0; r < NR; ++r)
+            if (r < nrhs) val[r] = A.in[src + r * A.ldin];
+    } else if (thru) {
+        rp = df_row_pull_prep(A.rptr, A.csrc, (int64_t)q.rbase + prow);
+    }
+    if (tid == 0 && q.fneed > 0) df_wait(A.fcnt + s, (unsigned)q.fneed, A.status);
+    __syncthreads();
+    if (stamp && tid == 0) *stamp = (int64_t)df_clock();
+    if (own || thru) df_row_pull<NR>(rp, A.csrc, A.U, nrhs, val);
+    if (tid < DF_PCOLS) {
+#pragma unroll
+        for (int r = 0; r < NR; ++r) zs[tid + DF_PCOLS * r] = own ? val[r] : 0.0;
+    } else if (tid < DF_PCOLS + DF_BLK) {
+#pragma unroll
+        for (int r = 0; r < NR; ++r) pass[(tid - DF_PCOLS) + DF_BLK * r] = thru ? val[r] : 0.0;
+    }
+    __syncthreads();
+#pragma unroll
+    for (int r = 0; r < NR; ++r) {
+        double acc = 0.0;
+        if (r < nrhs) {
+#pragma unroll
+            for (int e = 0; e < 32; ++e) acc += (double)pv[e] * zs[32 * g + e + DF_PCOLS * r];
+        }
+        red[(r * 4 + g) * DF_BLK + i] = acc;
+    }
+    __syncthreads();
+    double v[NR];
+#pragma unroll
+    for (int r = 0; r < NR; ++r)
+        v[r] = tid < DF_BLK ? red[(r * 4) * DF_BLK + tid] + red[(r * 4 + 1) * DF_BLK + tid] +
+                                  red[(r * 4 + 2) * DF_BLK + tid] + red[(r * 4 + 3) * DF_BLK + tid] -
+                                  pass[tid + DF_BLK * r]
+                            : 0.0;
+    if (nkc > 1) {
+        double* p = A.part + (int64_t)(slot0 + kc) * (DF_BLK * DF_MAX_NRHS);
+        if (tid < DF_BLK) {
+#pragma unroll
+            for (int r = 0; r < NR; ++r)
+                if (r < nrhs) p[tid + DF_BLK * r] = v[r];
+        }
+        if (!df_last_arrival(A.tcnt + q.tcnt + t, (unsigned)nkc, &last)) return;
+        // the partials in parallel: thread (i, kq) sums chunks kq, kq + 4, ... of row i; then the four
+        // groups add in order
+        {
+            const int kq = tid >> 6;
+            double acc[NR];
+#pragma unroll
+            for (int r = 0; r < NR; ++r) acc[r] = 0.0;
+            for (int k = kq; k < nkc; k += 4) {
+                const double* pk = A.part + (int64_t)(slot0 + k) * (DF_BLK * DF_MAX_NRHS);
+#pragma unroll
+                for (int r = 0; r < NR; ++r)
+                    if (r < nrhs) acc[r] += __ldcg(pk + i + DF_BLK * r);
+            }
+#pragma unroll
+            for (int r = 0; r < NR; ++r) red[(r * 4 + kq) * DF_BLK + i] = acc[r];
+        }
+        __syncthreads();
+#pragma unroll
+        for (int r = 0; r < NR; ++r)
+            v[r] = tid < DF_BLK ? red[(r * 4) * DF_BLK + tid] + red[(r * 4 + 1) * DF_BLK + tid] +
+                                      red[(r * 4 + 2) * DF_BLK + tid] + red[(r * 4 + 3) * DF_BLK + tid]
+                                : 0.0;
+    }
+    if (tid < DF_BLK && row < f) {
+        if (row < w) {
+#pragma unroll
+            for (int r = 0; r < NR; ++r)
+                if (r < nrhs) A.xtmp[fd.c0 + row + r * n] = v[r];
+        } else {
+            double* u = A.U + ((int64_t)q.urow + row - w) * nrhs;
+#pragma unroll
+            for (int r = 0; r < NR; ++r)
+                if (r < nrhs) u[r] = v[r];
+        }
+    }
+    df_publish_cta(A.fcnt + (fd.parent >= 0 ? fd.parent : s), 0u, true);
+}
+
+// Backward of an inverse-panel front, column block b (DF_PBCOLS columns) times row chunk rc of P:
+// x1 = P^T [y1; -x2], y1 = D^-1 (the forward result), x2 = the solution at the front's update rows.
+// Warp wp takes columns 4 wp .. 4 wp + 3 of the block, lane l the chunk's rows l + 32 e; the lanes' sums
+// reduce across the warp. With several chunks the last task sums the partials in chunk order and
+// writes the block's solution (local pivot order undone) into Y and X; every block signals bdone.
+template <typename T, int NR>
+__device__ __noinline__ void df_pinv_backward(const DataflowArgs<T>& A, int s, int b, int cc, double* sm, int64_t* stamp) {
+    __shared__ int last;
+    const DFront fd = A.fronts[s];
+    const DfFront q = A.df[s];
+    const int f = fd.f, w = fd.w, nrhs = A.nrhs, tid = threadIdx.x;
+    const int64_t n = A.n;
+    const int rc = cc & 255, slot0 = cc >> 8;
+    const int first = df_pb_first(b), nrc = df_pb_chunks(f, b);
+    const int j0 = DF_PBCOLS * b, i0 = DF_PROWS * rc;
+    const int wp = tid >> 5, lane = tid & 31;
+    const T* Pm = A.invb + q.inv;
+    double* zs = sm;                          // DF_PROWS x NR: [y1; -x2] over the chunk's rows
+    double* xs = zs + DF_PROWS * NR;          // DF_PBCOLS x NR: the block's sums (then 8 x that: the
+                                              // finisher's partial sums)
+    static_assert(DF_PBCOLS == 4 * (DF_THREADS / 32) && DF_PROWS == 4 * 32 && DF_THREADS / DF_PBCOLS == 8,
+                  "backward task shape");
+    // before the parent is done: the thread's 16 entries of P and the chunk's update-row indices
+    T pv[4][4];
+#pragma unroll
+    for (int c4 = 0; c4 < 4; ++c4)
+#pragma unroll
+        for (int e = 0; e < 4; ++e) {
+            const int row = i0 + lane + 32 * e, col = j0 + 4 * wp + c4;
+            pv[c4][e] = (row < f && col < w && (row >= w || row >= col)) ? Pm[row + (int64_t)col * f] : T(0);
+        }
+    const int zrow = i0 + tid;
+    const bool zin = tid < DF_PROWS && zrow < f;
+    const int32_t ridx = (zin && zrow >= w) ? A.rowval[fd.row_begin + zrow] : 0;
+    const unsigned pbsig = fd.parent >= 0 ? (unsigned)A.df[fd.parent].bsig : 0u;
+    if (tid == 0) {
+        if (fd.parent >= 0) df_wait(A.bdone + fd.parent, pbsig, A.status);
+        else df_wait(A.fcnt + s, (unsigned)(q.fneed + q.fsig), A.status);
+        if (stamp) *stamp = (int64_t)df_clock();
+    }
+    __syncthreads();
+    if (tid < DF_PROWS) {
+#pragma unroll
+        for (int r = 0; r < NR; ++r) {
+            double z = 0.0;
+            if (zin && r < nrhs) z = zrow < w ? df_dinv(A, A.xtmp, fd.c0 + zrow, r) : -A.Y[ridx + r * n];
+            zs[tid + DF_PROWS * r] = z;
+        }
+    }
+    __syncthreads();
+    constexpr int NV = 4 * NR, G = 32 / NV;
+    double v[NV];
+#pragma unroll
+    for (int c4 = 0; c4 < 4; ++c4)
+#pragma unroll
+        for (int r = 0; r < NR; ++r) {
+            double acc = 0.0;
+            if (r < nrhs) {
+#pragma unroll
+                for (int e = 0; e < 4; ++e) acc += (double)pv[c4][e] * zs[lane + 32 * e + DF_PROWS * r];
+            }
+            v[c4 * NR + r] = acc;
+        }
+    const double red = df_lane_reduce<NV>(v, lane);
+    if (lane % G == 0) {
+        const int idx = lane / G;
+        xs[4 * wp + idx / NR + DF_PBCOLS * (idx % NR)] = red;
+    }
+    __syncthreads();
+    double x[NR];
+#pragma unroll
+    for (int r = 0; r < NR; ++r) x[r] = tid < DF_PBCOLS ? xs[tid + DF_PBCOLS * r] : 0.0;
+    if (nrc > 1) {
+        double* p = A.part + (int64_t)(slot0 + rc - first) * (DF_BLK * DF_MAX_NRHS);
+        if (tid < DF_PBCOLS) {
+#pragma unroll
+            for (int r = 0; r < NR; ++r)
+                if (r < nrhs) p[tid + DF_PBCOLS * r] = x[r];
+        }
+        if (!df_last_arrival(A.ccnt + q.ccnt + b, (unsigned)nrc, &last)) return;
+        // the partials in parallel: thread (jj, kq) sums chunks kq, kq + 8, ... of column jj; then the
+        // eight groups add in order
+        double* grp = xs + DF_PBCOLS * NR;    // 8 x DF_PBCOLS x NR
+        {
+            const int jj = tid & (DF_PBCOLS - 1), kq = tid / DF_PBCOLS;
+            double acc[NR];
+#pragma unroll
+            for (int r = 0; r < NR; ++r) acc[r] = 0.0;
+            for (int k = kq; k < nrc; k += DF_THREADS / DF_PBCOLS) {
+                const double* pk = A.part + (int64_t)(slot0 + k) * (DF_BLK * DF_MAX_NRHS);
+#pragma unroll
+                for (int r = 0; r < NR; ++r)
+                    if (r < nrhs) acc[r] += __ldcg(pk + jj + DF_PBCOLS * r);
+            }
+#pragma unroll
+            for (int r = 0; r < NR; ++r) grp[(r * 8 + kq) * DF_PBCOLS + jj] = acc[r];
+        }
+        __syncthreads();
+        if (tid < DF_PBCOLS) {
+#pragma unroll
+            for (int r = 0; r < NR; ++r) {
+                double sum = 0.0;
+#pragma unroll
+                for (int kq = 0; kq < 8; ++kq) sum += grp[(r * 8 + kq) * DF_PBCOLS + tid];
+                x[r] = sum;
+            }
+        }
+    }
+    const int k = j0 + tid;
+    if (tid < DF_PBCOLS && k < w) {
+        const int64_t dst = A.reorder_bw ? A.piv[fd.c0 + k] - 1 : fd.c0 + k;
+        const int64_t o = A.perm[dst];
+#pragma unroll
+        for (int r = 0; r < NR; ++r)
+            if (r < nrhs) {
+                A.Y[dst + r * n] = x[r];
+                double* op = A.out + o + r * A.ldout;
+                if (A.mode == 2) *op += x[r];
+                else *op = x[r];
+            }
+    }
+    df_publish_cta(A.bdone + s, 0u, true);
+}
+
 }  // namespace
 
 template <typename T, int NR>
@@ -782,6 +1074,8 @@ __global__ void __launch_bounds__(DF_THREADS, 2) dataflow_solve_kernel(DataflowA
             case DF_FW_TILE: df_tile_forward<T, NR>(A, tk.a, tk.b, dsm, stamp); break;
             case DF_BW_PART: df_tiled_part<T, NR>(A, tk.a, tk.b, tk.c, dsm, stamp); break;
             case DF_BW_OWNER: df_tiled_owner<T, NR>(A, tk.a, tk.b, dsm, stamp); break;
+            case DF_FW_PINV: df_pinv_forward<T, NR>(A, tk.a, tk.b, tk.c, dsm, stamp); break;
+            case DF_BW_PINV: df_pinv_backward<T, NR>(A, tk.a, tk.b, tk.c, dsm, stamp); break;
             default: break;
         }
         __syncthreads();

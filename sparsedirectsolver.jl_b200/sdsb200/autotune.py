@@ -4,7 +4,10 @@ Two shapes decide how the fronts of a plan map onto the kernels:
 * ``fsmall``: the largest front order factored in shared memory by the small-front kernel. Larger
   fronts take the column-owner assembly, diagonal-block and DMMA GEMM path.
 * ``wide``: the tallest front (of at most 32 columns) that the dataflow solve gives to one warp;
-  taller or wider fronts go to 64-row tile tasks spread over the grid. (``area`` is reserved.)
+  taller or wider fronts go to tile tasks spread over the grid.
+* ``chains``: 0 solves those tiled fronts through inverse panels [L11^-1; L21 L11^-1], built after the
+  factorization (one matrix-vector product per front and sweep); 1 through chains of 64-column
+  blocks (no extra factorization work, one dependency link per block).
 
 The autotuner times factorization + solve for each candidate on the solver's own matrix and
 right-hand side (CUDA events, after a warm-up), keeps the fastest, and leaves the solver planned
@@ -14,7 +17,7 @@ from __future__ import annotations
 
 from .capi import tuning as make_tuning
 
-CANDIDATES = tuple((fs, wd, 0) for fs in (0, 128, 96) for wd in (0, 64))
+CANDIDATES = tuple((fs, wd, ch) for fs in (0, 128, 96) for wd in (0, 64) for ch in (0, 1))
 
 _cache: dict = {}
 
@@ -64,7 +67,7 @@ def autotune(solver, B, candidates=CANDIDATES, reps=3, use_cache=True):
 
 
 def describe(t):
-    return {"fsmall": int(t) & 0x1FF, "wide": (int(t) >> 9) & 0x7FF, "area": (int(t) >> 20) & 0x7FF}
+    return {"fsmall": int(t) & 0x1FF, "wide": (int(t) >> 9) & 0x7FF, "chains": (int(t) >> 20) & 0x7FF}
 
 
 __all__ = ["autotune", "describe", "CANDIDATES"]

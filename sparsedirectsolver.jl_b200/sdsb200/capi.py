@@ -39,9 +39,10 @@ class PlanOptions(C.Structure):
     _fields_ = [("nbatch", C.c_int32), ("precision", C.c_int32), ("max_nrhs", C.c_int32), ("tuning", C.c_int32)]
 
 
-def tuning(fsmall=0, wide=0, area=0):
-    """SDSB200_TUNING(fsmall, wide, area): the plan's front tile shapes (0 = defaults)."""
-    return int(fsmall) | (int(wide) << 9) | (int(area) << 20)
+def tuning(fsmall=0, wide=0, chains=0):
+    """SDSB200_TUNING(fsmall, wide, chains): the plan's front shapes (0 = defaults); chains = 1 solves the
+    tiled fronts by 64-column block chains instead of inverse panels."""
+    return int(fsmall) | (int(wide) << 9) | (int(chains) << 20)
 
 
 class Opts(C.Structure):

@@ -328,6 +328,38 @@ def test_persistent_solve_matches_level_launches(torch_cuda, structure):
         assert np.abs(x1 - x0).max() <= 1e-10 * np.abs(x0).max()
 
 
+@pytest.mark.parametrize("structure,precision", [("SPD", "fp64"), ("S", "fp64"), ("G", "fp64"), ("SPD", "fp32")])
+def test_inverse_panels_match_block_chains(torch_cuda, structure, precision):
+    # the dataflow solve's two forms for tiled fronts: inverse panels [L11^-1; L21 L11^-1] built after the
+    # factorization (the default) and 64-column block chains; fronts wider than 64 and taller than 128
+    # (several doubling levels, partial last blocks, partial-product chunks in both sweeps)
+    from sdsb200.capi import tuning
+
+    A = {"SPD": lambda: M.lap3d(20, 20, 20, seed=6),
+         "S": lambda: small_kkt(30, 30, 400, seed=2),   # the well-conditioned KKT of test_ldlt_kkt
+         "G": lambda: M.convection_diffusion3d(16, 16, 16, seed=6)}[structure]()
+    b = M.rhs(A.shape[0], 3, seed=7)
+    xs = {}
+    for chains in (0, 1):
+        ds = _solver(A, structure, reordering_alg="nd", max_nrhs=4, factor_precision=precision,
+                     tuning=tuning(0, 0, chains))
+        ds.execute("analysis")
+        assert ds.execute("factorization") == 0
+        if chains == 0:
+            assert ds.symbolic.front_ncols.max() > 128 and ds.symbolic.front_nrows.max() > 256
+        for tr in ((False, True) if structure == "G" else (False,)):
+            ds.setparam("solve_mode", int(tr))
+            x = ds.execute("solve", None, b).cpu().numpy()
+            AA = A.T.tocsr() if tr else A
+            berr = M.scaled_backward_error(AA, x, b)
+            assert berr <= (BERR if precision == "fp64" else 1e-5), (chains, tr, berr)
+            xs[chains, tr] = x
+        assert ds.plan_stat("solve_status") == 0
+    tol = 1e-10 if precision == "fp64" else 1e-4
+    for tr in ((False, True) if structure == "G" else (False,)):
+        assert rel_max_diff(xs[0, tr], xs[1, tr]) <= tol
+
+
 @pytest.mark.parametrize("case", ["SPD", "G", "G_T", "S"])
 def test_fgmres_refinement(torch_cuda, case):
     # FGMRES-IR with the FP32 factor as right preconditioner reaches the FP64 accuracy target, and
