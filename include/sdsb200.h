@@ -106,9 +106,12 @@ typedef struct sdsb200_plan_options {
  * columns) that the dataflow solve gives to one warp, larger fronts going to tile tasks (16..128,
  * 0 = 128); chains = how the dataflow solve treats those tiled fronts: 0, through their inverse
  * panels [L11^-1; L21 L11^-1] (f x w each, built after every factorization of a single-system plan),
- * 1: through chains of 64-column blocks. */
+ * 1: through chains of 64-column blocks; streams = the factorization streams of a single-system
+ * Cholesky plan (independent subtrees factored concurrently; 0 = 4, 1 = level by level, up to 15). */
 #define SDSB200_TUNING(fsmall, wide, chains) \
     ((int32_t)(fsmall) | ((int32_t)(wide) << 9) | ((int32_t)(chains) << 20))
+#define SDSB200_TUNING_STREAMS(fsmall, wide, chains, streams) \
+    (SDSB200_TUNING(fsmall, wide, chains) | ((int32_t)(streams) << 21))
 
 /* The Options fields the numeric and solve phases read (src/options.jl:155-223). */
 typedef struct sdsb200_opts {
@@ -221,7 +224,9 @@ int64_t sdsb200_get_trace(sdsb200_plan* plan, int64_t* h_out, int64_t cap);
  * "schur_n" (order of the Schur complement, 0 without one), "schur_level",
  * "solve_status" (synchronizes; nonzero when a bounded wait of the persistent solve gave up);
  * with profiling, "prof_ms:<kind>", "prof_flops:<kind>", "prof_bytes:<kind>", "prof_launches:<kind>"
- * for kinds small assemble panel gemm pivot scale stats fwd bwd diag permute residual.
+ * for kinds small assemble panel gemm pivot scale stats fwd bwd diag permute residual inv, and per
+ * launch of the last calls "prof_records" (their count), "prof_record:<i>:kind|level|ms|start" (start:
+ * ms after the call's first launch began; kind: the index of the kind in that list).
  * Returns -1 for an unknown name. */
 double sdsb200_plan_stat(const sdsb200_plan* plan, const char* name);
 

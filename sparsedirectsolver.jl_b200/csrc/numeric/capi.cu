@@ -66,11 +66,12 @@ void prof_end(Plan* P, cudaStream_t st, int kind, double flops, double bytes) {
 void prof_resolve(Plan* P) {
     if (!P->profile) return;
     for (size_t q = 0; q < P->pending.size(); ++q) {
-        float ms = 0;
+        float ms = 0, at = 0;
         cudaEventSynchronize(P->events[2 * q + 1]);
         cudaEventElapsedTime(&ms, P->events[2 * q], P->events[2 * q + 1]);
+        cudaEventElapsedTime(&at, P->events[0], P->events[2 * q]);
         ProfAcc& a = P->prof[P->pending[q].first];
-        P->records.push_back({P->pending[q].first, P->pending_level[q], (double)ms});
+        P->records.push_back({P->pending[q].first, P->pending_level[q], (double)ms, (double)at});
         a.ms += ms;
         a.flops += P->pending[q].second.first;
         a.bytes += P->pending[q].second.second;
@@ -170,26 +171,43 @@ int run_factor(Plan* P, const double* nzval, double eps, double u, int pivot, in
     int last_level = -1;
     const cudaStream_t main_st = st;
     bool on_side = false, any_side = false;
+    cudaStream_t last_main = main_st;
+    // the extra factorization streams start after the caller's prior work on `st`
+    for (int g = 1; g < P->nfstreams; ++g) {
+        if (g == 1) CK(cudaEventRecord(P->fstream_fork, main_st), "stream fork");
+        CK(cudaStreamWaitEvent(P->fstreams[g - 1], P->fstream_fork, 0), "stream fork");
+    }
+    // every stream rejoins the caller's (a capture must end joined)
+    auto join_all = [&]() {
+        for (int g = 1; g < P->nfstreams; ++g) {
+            cudaEventRecord(P->fevents[P->nfevents + g - 1], P->fstreams[g - 1]);
+            cudaStreamWaitEvent(main_st, P->fevents[P->nfevents + g - 1], 0);
+        }
+        if (any_side) {
+            cudaEventRecord(P->side_join, P->side);
+            cudaStreamWaitEvent(main_st, P->side_join, 0);
+        }
+    };
     for (const ProgLaunch& L : P->prog) {
         if (L.kind != L_STATS && !L.side && L.level != last_level) {
             if (interrupted(P)) {
-                if (any_side) {   // rejoin the side stream (a capture must end joined)
-                    cudaEventRecord(P->side_join, P->side);
-                    cudaStreamWaitEvent(main_st, P->side_join, 0);
-                }
+                join_all();
                 return fail(SDSB200_INTERRUPTED, "interrupted by user_host_interrupt");
             }
             last_level = L.level;
         }
-        // side launches: the side stream waits for the main stream's launches so far, then runs them
-        // beside the following levels of the factorization
+        // side launches: the side stream waits for the launches so far of the stream of the batch
+        // they follow, then runs them beside the following levels of the factorization
         if (L.side && !on_side) {
-            CK(cudaEventRecord(P->side_fork, main_st), "side fork");
+            CK(cudaEventRecord(P->side_fork, last_main), "side fork");
             CK(cudaStreamWaitEvent(P->side, P->side_fork, 0), "side fork");
         }
         on_side = L.side != 0;
         any_side = any_side || on_side;
-        st = on_side ? P->side : main_st;
+        if (!on_side) last_main = L.fstream > 0 ? P->fstreams[L.fstream - 1] : main_st;
+        st = on_side ? P->side : last_main;
+        for (int q = 0; q < L.wait_count; ++q)
+            CK(cudaStreamWaitEvent(st, P->fevents[P->fwaits[L.wait_begin + q]], 0), "stream wait");
         cudaError_t e = cudaSuccess;
         P->cur_level = L.level;
         prof_begin(P, st);
@@ -347,6 +365,8 @@ int run_factor(Plan* P, const double* nzval, double eps, double u, int pivot, in
                     a.members = members;
                     a.finfo = P->d_finfo;
                     a.ns = (int32_t)P->ns;
+                    a.part = static_cast<T*>(P->d_psplit);
+                    a.cnt = P->d_pcnt;
                     if (L.cls == 1) {
                         a.abuf = panels; a.astride = P->factor_len;
                         a.bbuf = pinv; a.bstride = P->df_inv_len;
@@ -378,13 +398,14 @@ int run_factor(Plan* P, const double* nzval, double eps, double u, int pivot, in
             }
         }
         prof_end(P, st, prof_kind_of(L.kind), L.flops * nm, L.bytes * nm);
-        if (e != cudaSuccess) return cuda_fail(e, "factorization launch");
+        if (e != cudaSuccess) {
+            join_all();
+            return cuda_fail(e, "factorization launch");
+        }
+        if (L.record >= 0) CK(cudaEventRecord(P->fevents[L.record], st), "stream record");
     }
     st = main_st;
-    if (any_side) {   // the factorization ends when the side launches are done too
-        CK(cudaEventRecord(P->side_join, P->side), "side join");
-        CK(cudaStreamWaitEvent(st, P->side_join, 0), "side join");
-    }
+    join_all();   // the factorization ends when every stream's launches are done
     return SDSB200_OK;
 }
 
@@ -1006,7 +1027,7 @@ double sdsb200_plan_stat(const sdsb200_plan* plan, const char* name) {
     }
     if (nm == "prof_records") return (double)P->records.size();
     if (nm.rfind("prof_record:", 0) == 0) {
-        // "prof_record:<i>:kind|level|ms"
+        // "prof_record:<i>:kind|level|ms|start" (start: ms after the phase's first launch began)
         size_t a = nm.find(':', 12);
         if (a == std::string::npos) return -1;
         size_t i = (size_t)atol(nm.substr(12, a - 12).c_str());
@@ -1015,6 +1036,7 @@ double sdsb200_plan_stat(const sdsb200_plan* plan, const char* name) {
         if (f == "kind") return P->records[i].kind;
         if (f == "level") return P->records[i].level;
         if (f == "ms") return P->records[i].ms;
+        if (f == "start") return P->records[i].start;
         return -1;
     }
     for (int k = 0; k < PK_COUNT; ++k) {

@@ -81,14 +81,22 @@ enum LaunchKind : int32_t {
     L_PINV,            // GEMM tiles that build the inverse panels of the dataflow solve's tiled fronts
 };
 
-// One 64 x 64 output tile of the inverse-panel GEMMs: C = A B, or C = -A B (column-major operands)
+// One 64 x 64 output tile of the inverse-panel GEMMs: C = A B, or C = -A B (column-major operands).
+// A long inner dimension is split over nsplit CTAs (split = this CTA's part, its A and B offsets and k
+// already advanced): each writes its partial product to slot `slot + split` of the launch's partial
+// buffer and the last of them to finish (counter `cnt`, which it resets) sums the parts in order.
 struct PinvTile {
     int64_t a, b, c;     // element offsets of A (m x k), B (k x n) and C (m x n)
     int32_t lda, ldb, ldc;
     int32_t m, n, k;
     int32_t front;       // skipped when this front failed
     int32_t neg;
+    int32_t nsplit, split, slot, cnt;
 };
+constexpr int PINV_KSPLIT = 256;   // longest inner dimension of one CTA's part
+
+constexpr int FSTREAM_DEFAULT = 4;   // factorization streams of a single-system Cholesky plan
+constexpr int FSTREAM_MIN_CP = 16;   // the critical path (32-column steps) of a subtree given its own stream
 
 struct Launch {
     LaunchKind kind;

@@ -192,6 +192,8 @@ struct PinvGemmArgs {
     int64_t astride, bstride, cstride;   // per-member strides
     const int32_t* finfo;
     int32_t ns;
+    T* part;                   // split tiles: 64 x 64 partial products (single-member plans)
+    unsigned int* cnt;         // split tiles: arrival counters, zero between launches
 };
 template <typename T>
 cudaError_t launch_pinv_gemm(const PinvGemmArgs<T>& a, int nmembers, cudaStream_t st);

@@ -2,7 +2,8 @@
 // fronts. L11^-1 is formed by recursive doubling over the 64 x 64 diagonal-block inverses:
 // inv([A 0; B C]) = [A^-1 0; -C^-1 (B A^-1) C^-1], two GEMM launches per doubling level over every front;
 // then L21 L11^-1 in one more launch. Each output tile is 64 x 64, C = A B or C = -A B with column-major
-// operands and any leading dimensions; every entry is summed by one thread in a fixed order.
+// operands and any leading dimensions; every entry is summed by one thread in a fixed order (a tile with
+// a long inner dimension by several CTAs, whose parts the last one adds in order).
 // * FP64: mma.sync m8n8k4 (DMMA), 4 warps of 32 x 32, K staged 16 at a time by cp.async in two buffers;
 // * FP32: SIMT, 256 threads of 4 x 4 entries, the same staging.
 #include <cuda_runtime.h>
@@ -28,6 +29,38 @@ template <int N>
 __device__ __forceinline__ void pinv_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N)); }
 
 constexpr int PBK = 16;   // K per stage
+
+// The epilogue of a tile: value v (this CTA's sum) of entry (r, c). Unsplit tiles write C = +-v; split
+// tiles write their part, and the last part to arrive sums all parts in split order and writes C.
+// `put` visits the CTA's entries: put(r, c, v&) for each one it owns.
+template <typename T, class Visit>
+__device__ __forceinline__ void pinv_epilogue(const PinvGemmArgs<T>& A, const PinvTile& t, T* Cb, Visit visit) {
+    __shared__ int last;
+    if (t.nsplit <= 1) {
+        visit([&](int r, int c, double v) {
+            if (r < t.m && c < t.n) Cb[r + (int64_t)c * t.ldc] = T(t.neg ? -v : v);
+        });
+        return;
+    }
+    T* mine = A.part + (int64_t)(t.slot + t.split) * 64 * 64;
+    visit([&](int r, int c, double v) { mine[r + 64 * c] = T(v); });
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        unsigned old;
+        asm volatile("atom.acq_rel.gpu.global.add.u32 %0, [%1], 1;" : "=r"(old) : "l"(A.cnt + t.cnt) : "memory");
+        last = old + 1 == (unsigned)t.nsplit;
+        if (last) A.cnt[t.cnt] = 0u;   // every part has arrived: reset for the next launch
+    }
+    __syncthreads();
+    if (!last) return;
+    for (int q = threadIdx.x; q < 64 * 64; q += blockDim.x) {
+        const int r = q & 63, c = q >> 6;
+        if (r >= t.m || c >= t.n) continue;
+        double v = 0.0;
+        for (int sp = 0; sp < t.nsplit; ++sp) v += (double)__ldcg(A.part + (int64_t)(t.slot + sp) * 64 * 64 + q);
+        Cb[r + (int64_t)c * t.ldc] = T(t.neg ? -v : v);
+    }
+}
 
 // stage the K-slice [k0, k0 + PBK) of A (64 rows) and B (64 columns) into As[kk][r] and Bs[kk][c]
 template <typename T, int NT, int LDS>
@@ -92,16 +125,15 @@ __global__ void __launch_bounds__(128) pinv_gemm_dmma_kernel(PinvGemmArgs<double
         }
         __syncthreads();
     }
+    pinv_epilogue<double>(A, t, Cb, [&](auto put) {
 #pragma unroll
-    for (int i = 0; i < 4; ++i)
+        for (int i = 0; i < 4; ++i)
 #pragma unroll
-        for (int j = 0; j < 4; ++j)
+            for (int j = 0; j < 4; ++j)
 #pragma unroll
-            for (int e = 0; e < 2; ++e) {
-                const int r = wm * 32 + i * 8 + (lane >> 2);
-                const int c = wn * 32 + j * 8 + (lane & 3) * 2 + e;
-                if (r < t.m && c < t.n) Cb[r + (int64_t)c * t.ldc] = t.neg ? -acc[i][j][e] : acc[i][j][e];
-            }
+                for (int e = 0; e < 2; ++e)
+                    put(wm * 32 + i * 8 + (lane >> 2), wn * 32 + j * 8 + (lane & 3) * 2 + e, acc[i][j][e]);
+    });
 }
 
 __global__ void __launch_bounds__(256) pinv_gemm_f32_kernel(PinvGemmArgs<float> A) {
@@ -145,13 +177,12 @@ __global__ void __launch_bounds__(256) pinv_gemm_f32_kernel(PinvGemmArgs<float> 
         }
         __syncthreads();
     }
+    pinv_epilogue<float>(A, t, Cb, [&](auto put) {
 #pragma unroll
-    for (int i = 0; i < 4; ++i)
+        for (int i = 0; i < 4; ++i)
 #pragma unroll
-        for (int j = 0; j < 4; ++j) {
-            const int r = tx + 16 * i, c = ty + 16 * j;
-            if (r < t.m && c < t.n) Cb[r + (int64_t)c * t.ldc] = t.neg ? -acc[i][j] : acc[i][j];
-        }
+            for (int j = 0; j < 4; ++j) put(tx + 16 * i, ty + 16 * j, (double)acc[i][j]);
+    });
 }
 
 }  // namespace

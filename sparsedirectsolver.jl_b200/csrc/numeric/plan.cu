@@ -276,10 +276,11 @@ Plan* build_plan(const sdsb200_symbolic* sym, const sdsb200_plan_options* popts,
         }
         if (tune_wide && (tune_wide < 16 || tune_wide > DF_WARP_F))
             throw BuildError(SDSB200_INVALID_VALUE, "tuning: wide (the tallest warp front of the solve) must lie in 16..128");
-        if (tune_rsv > 1)
-            throw BuildError(SDSB200_INVALID_VALUE, "tuning: chains must be 0 (inverse panels) or 1 (block chains)");
+        const int tune_chains = tune_rsv & 1, tune_streams = (tune_rsv >> 1) & 15;
+        if (tune_rsv > 31)
+            throw BuildError(SDSB200_INVALID_VALUE, "tuning: the third field is chains (bit 0) | streams << 1 (streams < 16)");
         const int warp_f = tune_wide ? tune_wide : DF_WARP_F;
-        const bool pinv_mode = tune_rsv == 0;   // tiled fronts solved through inverse panels
+        const bool pinv_mode = tune_chains == 0;   // tiled fronts solved through inverse panels
         P->fsmall_max = classes.back();
         auto class_of = [&](int f) {
             for (int c : classes)
@@ -287,19 +288,57 @@ Plan* build_plan(const sdsb200_symbolic* sym, const sdsb200_plan_options* popts,
             return 0;
         };
 
-        // contribution blocks on one arena, by lifetime [level, parent level]
+        // Factorization streams (single-system Cholesky plans): the level-batched launches run per
+        // (level, stream). Walking down from the roots, a front's heaviest child subtree (by its
+        // critical path of 32-column steps) stays on the front's stream and every other child subtree
+        // with a critical path of at least FSTREAM_MIN_CP steps starts a new stream while fewer than
+        // `streams` are in use, so that independent subtrees factor concurrently instead of level by
+        // level. A front waits for its children on other streams through events.
+        std::vector<int> fstream(ns, 0);
+        P->nfstreams = 1;
         {
-            Arena arena;
-            std::vector<int> order;
-            for (int L = 0; L < P->nlevels; ++L)
-                for (int s : P->level_fronts[L]) order.push_back(s);
-            for (int s : order) {
-                DFront& F = P->fronts[s];
-                int64_t m = F.f - F.w;
-                if (F.parent < 0 || m == 0) continue;
-                F.cb = arena.place(m * m, F.level, P->fronts[F.parent].level);
+            const int want = tune_streams ? tune_streams : FSTREAM_DEFAULT;
+            if (P->structure == STRUCT_SPD && P->nbatch == 1 && P->schur_front < 0 && want > 1) {
+                std::vector<int64_t> cp(ns, 0);
+                for (int64_t s = 0; s < ns; ++s) {   // children precede parents
+                    const DFront& F = P->fronts[s];
+                    cp[s] += 1 + (class_of(F.f) ? 0 : (F.w + CHOL_NB - 1) / CHOL_NB);
+                    if (F.parent >= 0) cp[F.parent] = std::max(cp[F.parent], cp[s]);
+                }
+                for (int64_t s = ns - 1; s >= 0; --s) {
+                    const DFront& F = P->fronts[s];
+                    std::vector<int> kids;
+                    for (int q = F.ch_begin; q < F.ch_end; ++q) kids.push_back((int)(child_list[q] - 1));
+                    std::stable_sort(kids.begin(), kids.end(), [&](int a, int b) { return cp[a] > cp[b]; });
+                    for (size_t q = 0; q < kids.size(); ++q) {
+                        const int c = kids[q];
+                        if (q > 0 && cp[c] >= FSTREAM_MIN_CP && P->nfstreams < want) fstream[c] = P->nfstreams++;
+                        else fstream[c] = fstream[s];
+                    }
+                }
             }
-            P->cb_len = ((arena.top + 31) & ~int64_t(31));
+        }
+
+        // contribution blocks on one arena per stream, by lifetime [level, parent level]: a stream's
+        // launches run level by level, and the only fronts whose parent is on another stream are the
+        // tops of their streams' subtrees (nothing on their stream comes after them)
+        {
+            std::vector<Arena> arenas(P->nfstreams);
+            for (int L = 0; L < P->nlevels; ++L)
+                for (int s : P->level_fronts[L]) {
+                    DFront& F = P->fronts[s];
+                    int64_t m = F.f - F.w;
+                    if (F.parent < 0 || m == 0) continue;
+                    F.cb = arenas[fstream[s]].place(m * m, F.level, P->fronts[F.parent].level);
+                }
+            int64_t base = 0;
+            for (int g = 0; g < P->nfstreams; ++g) {
+                const int64_t len = (arenas[g].top + 31) & ~int64_t(31);
+                for (int64_t s = 0; s < ns; ++s)
+                    if (fstream[s] == g && P->fronts[s].cb >= 0) P->fronts[s].cb += base;
+                base += len;
+            }
+            P->cb_len = base;
         }
 
         // column-owner extend-add lists of the large fronts
@@ -370,14 +409,36 @@ Plan* build_plan(const sdsb200_symbolic* sym, const sdsb200_plan_options* popts,
                 }
             return 2.0 * K * entries;
         };
-        for (int L = 0; L < P->nlevels; ++L) {
+        // per batch (level, stream): its first and last launch, and the step scratch of each stream
+        struct Batch { int level, stream; size_t first, last; };
+        std::vector<Batch> batches;
+        std::vector<int> batch_of(ns, -1);
+        std::vector<int64_t> scr_stream(P->nfstreams, 0);   // each stream's step scratch size
+        // step tasks and copy tiles whose scratch slots move to their stream's part of the scratch
+        std::vector<std::vector<size_t>> step_rebase(P->nfstreams), tile_rebase(P->nfstreams);
+        for (int L = 0; L < P->nlevels; ++L)
+          for (int sg = 0; sg < P->nfstreams; ++sg) {
             std::map<int, std::vector<int>> small;
             std::vector<int> large;
             for (int s : P->level_fronts[L]) {
+                if (fstream[s] != sg) continue;
                 int c = s == P->schur_front ? 0 : class_of(P->fronts[s].f);
                 if (c) small[c].push_back(s);
                 else large.push_back(s);
             }
+            if (small.empty() && large.empty()) continue;
+            const size_t prog_first = P->prog.size();
+            struct BatchEnd {   // closes the batch whatever path the body leaves by
+                std::vector<Batch>& b; std::vector<int>& of; Plan* P; int L, sg; size_t first;
+                const std::map<int, std::vector<int>>& sm; const std::vector<int>& lg;
+                ~BatchEnd() {
+                    if (P->prog.size() == first) return;
+                    for (auto& kv : sm) for (int s : kv.second) of[s] = (int)b.size();
+                    for (int s : lg) of[s] = (int)b.size();
+                    for (size_t q = first; q < P->prog.size(); ++q) P->prog[q].fstream = sg;
+                    b.push_back({L, sg, first, P->prog.size() - 1});
+                }
+            } batch_end{batches, batch_of, P, L, sg, prog_first, small, large};
             for (auto& kv : small) {
                 ProgLaunch pl{};
                 pl.kind = L_SMALL; pl.level = L; pl.count = (int)kv.second.size(); pl.cls = kv.first;
@@ -431,6 +492,7 @@ Plan* build_plan(const sdsb200_symbolic* sym, const sdsb200_plan_options* popts,
                     t.diag = 1 << 29;
                     t.front = -1;
                     t.mode = 2;
+                    tile_rebase[sg].push_back(tiles.size());
                     tiles.push_back(t);
                 };
                 for (int kb = 0; kb < maxw; kb += NB) {
@@ -447,7 +509,10 @@ Plan* build_plan(const sdsb200_symbolic* sym, const sdsb200_plan_options* popts,
                         } else {
                             const int64_t slot = scr;
                             scr += (int64_t)NB * NB;
-                            for (int t = 0; t * 64 < rows; ++t) steptasks.push_back({s, t, slot, F.panel, F.f, F.w});
+                            for (int t = 0; t * 64 < rows; ++t) {
+                                step_rebase[sg].push_back(steptasks.size());
+                                steptasks.push_back({s, t, slot, F.panel, F.f, F.w});
+                            }
                             if (F.w > kb + NB) step_copy.push_back({s, slot});
                             else last_copy.push_back({s, slot});
                         }
@@ -472,7 +537,7 @@ Plan* build_plan(const sdsb200_symbolic* sym, const sdsb200_plan_options* popts,
                     gl.count = (int)(tiles.size() - gl.list);
                     if (gl.count) P->prog.push_back(gl);
                 }
-                P->inv_len = std::max(P->inv_len, scr);
+                scr_stream[sg] = std::max(scr_stream[sg], scr);
                 ProgLaunch cl{};
                 cl.kind = L_GEMM; cl.level = L; cl.list = (int64_t)tiles.size();
                 cl.abuf = cl.bbuf = BUF_FACTOR; cl.cbuf = BUF_CB;
@@ -540,6 +605,39 @@ Plan* build_plan(const sdsb200_symbolic* sym, const sdsb200_plan_options* popts,
                     P->prog.push_back(gl);
                 }
             }
+        }
+        // the streams' step scratch side by side; events between the streams' batches: a batch waits for
+        // the batches of its fronts' children on other streams (each the top of its stream's subtree)
+        {
+            int64_t base = 0;
+            for (int g = 0; g < P->nfstreams; ++g) {
+                for (size_t i : step_rebase[g]) steptasks[i].scr += base;
+                for (size_t i : tile_rebase[g]) tiles[i].a += base;
+                base += scr_stream[g];
+            }
+            P->inv_len = std::max(P->inv_len, base);
+            std::vector<int> ev_of_batch(batches.size(), -1);
+            std::vector<std::vector<int>> waits(batches.size());
+            int nev = 0;
+            for (int64_t s = 0; s < ns; ++s) {
+                const int p = P->fronts[s].parent;
+                if (p < 0 || batch_of[s] < 0 || batch_of[p] < 0 || fstream[s] == fstream[p]) continue;
+                const int cb_ = batch_of[s], pb = batch_of[p];
+                if (ev_of_batch[cb_] < 0) {
+                    ev_of_batch[cb_] = nev++;
+                    P->prog[batches[cb_].last].record = ev_of_batch[cb_];
+                }
+                if (std::find(waits[pb].begin(), waits[pb].end(), ev_of_batch[cb_]) == waits[pb].end())
+                    waits[pb].push_back(ev_of_batch[cb_]);
+            }
+            for (size_t bi = 0; bi < batches.size(); ++bi) {
+                if (waits[bi].empty()) continue;
+                ProgLaunch& first = P->prog[batches[bi].first];
+                first.wait_begin = (int32_t)P->fwaits.size();
+                first.wait_count = (int32_t)waits[bi].size();
+                P->fwaits.insert(P->fwaits.end(), waits[bi].begin(), waits[bi].end());
+            }
+            P->nfevents = nev;
         }
         // dataflow solve: front classes, task list, inverse layout, contribution lists (solve.cuh)
         {
@@ -722,13 +820,15 @@ Plan* build_plan(const sdsb200_symbolic* sym, const sdsb200_plan_options* popts,
             // and C (up to h blocks): T = L[C, A] X[A, A] into the scratch, X[C, A] = -X[C, C] T) and
             // the update rows L21 X. X lives in the inverse panel (ld f).
             if (P->nbatch == 1) {
-                std::vector<std::vector<ProgLaunch>> side(P->nlevels);
+                std::map<std::pair<int, int>, std::vector<ProgLaunch>> side;   // per batch (level, stream)
                 std::vector<int32_t> small_sorted, blk_sorted;
                 std::vector<PinvTile> pt;
                 auto bw_of = [](int w, int b) { return std::min(DF_BLK, w - DF_BLK * b); };
                 int64_t pwork = 0;
-                for (int L = 0; L < P->nlevels; ++L) {
-                    std::vector<int> pf;   // the level's inverse-panel fronts
+                for (int L = 0; L < P->nlevels; ++L)
+                  for (int sg = 0; sg < P->nfstreams; ++sg) {
+                    std::vector<ProgLaunch>& side_b = side[{L, sg}];
+                    std::vector<int> pf;   // the batch's inverse-panel fronts
                     ProgLaunch il_{};
                     il_.kind = L_DFINV;
                     il_.level = L;
@@ -736,7 +836,7 @@ Plan* build_plan(const sdsb200_symbolic* sym, const sdsb200_plan_options* popts,
                     il_.list = (int64_t)small_sorted.size();
                     il_.list2 = (int64_t)blk_sorted.size() / 2;
                     for (int s : P->level_fronts[L]) {
-                        if (s == P->schur_front) continue;
+                        if (s == P->schur_front || fstream[s] != sg) continue;
                         if (!df[s].tiled) {
                             small_sorted.push_back(s);
                             continue;
@@ -749,23 +849,50 @@ Plan* build_plan(const sdsb200_symbolic* sym, const sdsb200_plan_options* popts,
                     }
                     il_.count = to_i32((int64_t)small_sorted.size() - il_.list, "inverse launch");
                     il_.count2 = to_i32((int64_t)blk_sorted.size() / 2 - il_.list2, "inverse launch");
-                    if (il_.count + il_.count2 > 0) side[L].push_back(il_);
-                    auto push_launch = [&](size_t first, int cls) {
+                    if (il_.count + il_.count2 > 0) side_b.push_back(il_);
+                    // one launch of tiles; a tile with a long inner dimension becomes nsplit CTAs
+                    auto push_launch = [&](std::vector<PinvTile>& v, int cls) {
                         ProgLaunch pl{};
                         pl.kind = L_PINV;
                         pl.level = L;
                         pl.side = 1;
                         pl.cls = cls;
-                        pl.list = (int64_t)first;
-                        pl.count = to_i32((int64_t)(pt.size() - first), "inverse-panel tiles");
-                        for (size_t q = first; q < pt.size(); ++q) pl.flops += 2.0 * pt[q].m * pt[q].n * pt[q].k;
-                        if (pl.count > 0) side[L].push_back(pl);
+                        pl.list = (int64_t)pt.size();
+                        int32_t slots = 0, cnts = 0;
+                        for (const PinvTile& t0 : v) {
+                            pl.flops += 2.0 * t0.m * t0.n * t0.k;
+                            const int ns_ = (t0.k + PINV_KSPLIT - 1) / PINV_KSPLIT;
+                            if (ns_ <= 1) {
+                                PinvTile t = t0;
+                                t.nsplit = 1;
+                                pt.push_back(t);
+                                continue;
+                            }
+                            for (int sp = 0; sp < ns_; ++sp) {
+                                PinvTile t = t0;
+                                const int k0 = sp * PINV_KSPLIT;
+                                t.a += (int64_t)k0 * t0.lda;
+                                t.b += k0;
+                                t.k = std::min(PINV_KSPLIT, t0.k - k0);
+                                t.nsplit = ns_;
+                                t.split = sp;
+                                t.slot = slots;
+                                t.cnt = cnts;
+                                pt.push_back(t);
+                            }
+                            slots += ns_;
+                            cnts += 1;
+                        }
+                        P->psplit_slots = std::max(P->psplit_slots, (int64_t)slots);
+                        P->psplit_cnts = std::max(P->psplit_cnts, (int64_t)cnts);
+                        pl.count = to_i32((int64_t)(pt.size() - pl.list), "inverse-panel tiles");
+                        if (pl.count > 0) side_b.push_back(pl);
+                        v.clear();
                     };
                     int maxK = 0;
                     for (int s : pf) maxK = std::max(maxK, df[s].nblk);
                     for (int h = 1; h < maxK; h *= 2) {
-                        std::vector<PinvTile> g2;
-                        const size_t first = pt.size();
+                        std::vector<PinvTile> g1, g2;
                         int64_t toff = 0;
                         for (int s : pf) {
                             const DFront& F = P->fronts[s];
@@ -787,7 +914,7 @@ Plan* build_plan(const sdsb200_symbolic* sym, const sdsb200_plan_options* popts,
                                         t1.n = DF_BLK;
                                         t1.k = DF_BLK * (c0 - aj);
                                         t1.front = (int32_t)s;
-                                        pt.push_back(t1);
+                                        g1.push_back(t1);
                                         PinvTile t2{};
                                         t2.a = po + DF_BLK * ci + (int64_t)DF_BLK * c0 * f;
                                         t2.lda = f;
@@ -806,12 +933,10 @@ Plan* build_plan(const sdsb200_symbolic* sym, const sdsb200_plan_options* popts,
                             }
                         }
                         pwork = std::max(pwork, toff);
-                        push_launch(first, 1);
-                        const size_t first2 = pt.size();
-                        pt.insert(pt.end(), g2.begin(), g2.end());
-                        push_launch(first2, 2);
+                        push_launch(g1, 1);
+                        push_launch(g2, 2);
                     }
-                    const size_t firstw = pt.size();
+                    std::vector<PinvTile> gw;
                     for (int s : pf) {
                         const DFront& F = P->fronts[s];
                         const int K = df[s].nblk, f = F.f, w = F.w, m = f - w;
@@ -829,27 +954,29 @@ Plan* build_plan(const sdsb200_symbolic* sym, const sdsb200_plan_options* popts,
                                 t.n = bw_of(w, aj);
                                 t.k = w - DF_BLK * aj;
                                 t.front = (int32_t)s;
-                                pt.push_back(t);
+                                gw.push_back(t);
                             }
                     }
-                    push_launch(firstw, 3);
+                    push_launch(gw, 3);
                 }
                 P->d_df_small = upload(P, small_sorted, st);
                 P->d_df_blkinv = upload(P, blk_sorted, st);
                 P->pwork_len = pinv_mode ? std::max<int64_t>(pwork, 2) : 0;
                 P->d_pinv_tiles = upload(P, pt, st);
-                // every level's side launches right after the level's last launch of the factorization
+                // every batch's side launches right after the batch's last launch of the factorization
                 std::vector<ProgLaunch> merged;
                 for (size_t q = 0; q < P->prog.size(); ++q) {
                     merged.push_back(P->prog[q]);
-                    const int L = P->prog[q].level;
-                    const bool last_of_level = q + 1 == P->prog.size() || P->prog[q + 1].level != L;
-                    if (last_of_level && L >= 0 && L < P->nlevels) {
-                        merged.insert(merged.end(), side[L].begin(), side[L].end());
-                        side[L].clear();
+                    const std::pair<int, int> key{P->prog[q].level, P->prog[q].fstream};
+                    const bool last_of_batch = q + 1 == P->prog.size() || P->prog[q + 1].level != key.first ||
+                                               P->prog[q + 1].fstream != key.second;
+                    auto it = side.find(key);
+                    if (last_of_batch && it != side.end()) {
+                        merged.insert(merged.end(), it->second.begin(), it->second.end());
+                        side.erase(it);
                     }
                 }
-                for (int L = 0; L < P->nlevels; ++L) merged.insert(merged.end(), side[L].begin(), side[L].end());
+                for (auto& kv : side) merged.insert(merged.end(), kv.second.begin(), kv.second.end());
                 P->prog.swap(merged);
             }
         }
@@ -1060,6 +1187,11 @@ Plan* build_plan(const sdsb200_symbolic* sym, const sdsb200_plan_options* popts,
         P->d_dfinv_L = alloc_bytes(es * P->df_inv_len * nb);
         if (gen) P->d_dfinv_U = alloc_bytes(es * P->df_inv_len * nb);
         if (P->pwork_len) P->d_pwork = alloc_bytes(es * P->pwork_len * nb * (gen ? 2 : 1));
+        if (P->psplit_slots) {
+            P->d_psplit = alloc_bytes(es * P->psplit_slots * 64 * 64);
+            P->d_pcnt = dalloc<unsigned int>(P, P->psplit_cnts);
+            cudaMemsetAsync(P->d_pcnt, 0, sizeof(unsigned int) * P->psplit_cnts, st);
+        }
         P->d_xtmp = dalloc<double>(P, n * P->max_nrhs);
         P->d_solve_status = dalloc<int32_t>(P, 1);
         cudaMemsetAsync(P->d_solve_status, 0, sizeof(int32_t), st);
@@ -1094,8 +1226,23 @@ Plan* build_plan(const sdsb200_symbolic* sym, const sdsb200_plan_options* popts,
             cudaEventCreateWithFlags(&P->join_in, cudaEventDisableTiming) != cudaSuccess ||
             cudaEventCreateWithFlags(&P->join_out, cudaEventDisableTiming) != cudaSuccess ||
             cudaEventCreateWithFlags(&P->side_fork, cudaEventDisableTiming) != cudaSuccess ||
-            cudaEventCreateWithFlags(&P->side_join, cudaEventDisableTiming) != cudaSuccess)
+            cudaEventCreateWithFlags(&P->side_join, cudaEventDisableTiming) != cudaSuccess ||
+            cudaEventCreateWithFlags(&P->fstream_fork, cudaEventDisableTiming) != cudaSuccess)
             throw BuildError(SDSB200_CUDA_ERROR, "stream or event creation failed");
+        // the factorization's extra streams and their events (the cross-stream ones, then one join per
+        // extra stream)
+        for (int g = 1; g < P->nfstreams; ++g) {
+            cudaStream_t fs = nullptr;
+            if (cudaStreamCreateWithPriority(&fs, cudaStreamNonBlocking, prio_high) != cudaSuccess)
+                throw BuildError(SDSB200_CUDA_ERROR, "stream creation failed");
+            P->fstreams.push_back(fs);
+        }
+        for (int q = 0; q < P->nfevents + P->nfstreams - 1; ++q) {
+            cudaEvent_t ev = nullptr;
+            if (cudaEventCreateWithFlags(&ev, cudaEventDisableTiming) != cudaSuccess)
+                throw BuildError(SDSB200_CUDA_ERROR, "event creation failed");
+            P->fevents.push_back(ev);
+        }
         cudaMemsetAsync(P->d_psign, 0, n, st);
         cudaMemsetAsync(P->d_kind, 0, n * nb, st);
         cudaMemsetAsync(P->d_d, 0, sizeof(double) * 2 * n * nb, st);
@@ -1137,6 +1284,9 @@ void free_plan(Plan* P) {
     if (P->side_join) cudaEventDestroy(P->side_join);
     if (P->own) cudaStreamDestroy(P->own);
     if (P->side) cudaStreamDestroy(P->side);
+    if (P->fstream_fork) cudaEventDestroy(P->fstream_fork);
+    for (cudaStream_t fs : P->fstreams) cudaStreamDestroy(fs);
+    for (cudaEvent_t ev : P->fevents) cudaEventDestroy(ev);
     if (P->h_norms) cudaFreeHost(P->h_norms);
     if (P->h_info_pinned) cudaFreeHost(P->h_info_pinned);
     delete P;

@@ -35,6 +35,9 @@ struct ProgLaunch {
                             // critical path), after the main stream's launches that precede it
     int64_t list2 = 0;      // inverses: first (front, block) pair of the block inverses; count2 pairs
     int32_t count2 = 0;
+    int32_t fstream = 0;    // factorization stream (0: the caller's)
+    int32_t wait_begin = 0, wait_count = 0;   // events (in fwaits) this launch's stream waits for first
+    int32_t record = -1;    // event recorded on the launch's stream after it (-1: none)
 };
 
 // per-kind accounting of the profiling mode (CUDA events around every launch)
@@ -122,6 +125,9 @@ struct Plan {
     PinvTile* d_pinv_tiles = nullptr;   // the GEMM tiles that build the inverse panels (kind L_PINV)
     int64_t pwork_len = 0;              // their scratch (T = L[C, A] X[A, A] of one doubling level), per member and side
     void* d_pwork = nullptr;
+    int64_t psplit_slots = 0, psplit_cnts = 0;   // split tiles: most partial slots and counters of a launch
+    void* d_psplit = nullptr;           // their 64 x 64 partial products
+    unsigned int* d_pcnt = nullptr;     // their arrival counters (reset by the last arrival)
     double* d_df_part = nullptr;        // backward partial sums: slots of 64 x DF_MAX_NRHS doubles
     int64_t* d_df_trace = nullptr;      // profiling: 6 int64 per task (start, wait done, end, CTA, kind, a | b << 32)
     int32_t df_fwarp_max = 1;           // tallest warp front
@@ -164,6 +170,12 @@ struct Plan {
     cudaEvent_t join_in = nullptr, join_out = nullptr;
     cudaStream_t side = nullptr;         // low-priority stream of the side launches of the factorization
     cudaEvent_t side_fork = nullptr, side_join = nullptr;
+    int nfstreams = 1;                   // factorization streams (stream 0 is the caller's / capture stream)
+    std::vector<cudaStream_t> fstreams;  // streams 1 .. nfstreams - 1
+    std::vector<cudaEvent_t> fevents;    // the cross-stream events of the factorization
+    int nfevents = 0;
+    std::vector<int32_t> fwaits;         // per launch wait lists (ProgLaunch::wait_begin / wait_count)
+    cudaEvent_t fstream_fork = nullptr;  // the extra streams start after the caller's prior work
     CachedGraph g_factor, g_solve, g_resid, g_corr;
 
     bool profile = false;
@@ -172,7 +184,7 @@ struct Plan {
     size_t prof_next = 0;
     std::vector<std::pair<int, std::pair<double, double>>> pending;  // kind, (flops, bytes) per event pair
     std::vector<int> pending_level;
-    struct LaunchRecord { int kind, level; double ms; };
+    struct LaunchRecord { int kind, level; double ms, start; };
     std::vector<LaunchRecord> records;   // every profiled launch of the last calls
     int cur_level = -1;
 };

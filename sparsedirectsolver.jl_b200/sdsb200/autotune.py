@@ -8,6 +8,8 @@ Two shapes decide how the fronts of a plan map onto the kernels:
 * ``chains``: 0 solves those tiled fronts through inverse panels [L11^-1; L21 L11^-1], built after the
   factorization (one matrix-vector product per front and sweep); 1 through chains of 64-column
   blocks (no extra factorization work, one dependency link per block).
+* ``streams`` (not searched, default 4): independent subtrees of a Cholesky front tree factored on
+  separate streams.
 
 The autotuner times factorization + solve for each candidate on the solver's own matrix and
 right-hand side (CUDA events, after a warm-up), keeps the fastest, and leaves the solver planned
@@ -67,7 +69,8 @@ def autotune(solver, B, candidates=CANDIDATES, reps=3, use_cache=True):
 
 
 def describe(t):
-    return {"fsmall": int(t) & 0x1FF, "wide": (int(t) >> 9) & 0x7FF, "chains": (int(t) >> 20) & 0x7FF}
+    return {"fsmall": int(t) & 0x1FF, "wide": (int(t) >> 9) & 0x7FF, "chains": (int(t) >> 20) & 1,
+            "streams": (int(t) >> 21) & 15}
 
 
 __all__ = ["autotune", "describe", "CANDIDATES"]
