@@ -107,11 +107,15 @@ typedef struct sdsb200_plan_options {
  * 0 = 128); chains = how the dataflow solve treats those tiled fronts: 0, through their inverse
  * panels [L11^-1; L21 L11^-1] (f x w each, built after every factorization of a single-system plan),
  * 1: through chains of 64-column blocks; streams = the factorization streams of a single-system
- * Cholesky plan (independent subtrees factored concurrently; 0 = 4, 1 = level by level, up to 15). */
+ * Cholesky plan (independent subtrees factored concurrently; 0 = 4, 1 = level by level, up to 15);
+ * steps (bit 5 of the third field, SDSB200_TUNING_STEPS): 1 = a single-system Cholesky plan runs each
+ * batch of its large fronts' 32-column steps as dataflow tasks in one persistent launch, 0 (default) =
+ * one launch per step and kernel. */
 #define SDSB200_TUNING(fsmall, wide, chains) \
     ((int32_t)(fsmall) | ((int32_t)(wide) << 9) | ((int32_t)(chains) << 20))
 #define SDSB200_TUNING_STREAMS(fsmall, wide, chains, streams) \
     (SDSB200_TUNING(fsmall, wide, chains) | ((int32_t)(streams) << 21))
+#define SDSB200_TUNING_STEPS ((int32_t)1 << 25)
 
 /* The Options fields the numeric and solve phases read (src/options.jl:155-223). */
 typedef struct sdsb200_opts {
@@ -216,7 +220,10 @@ int sdsb200_set_profiling(sdsb200_plan* plan, int32_t on);
 
 /* Profiling: the dataflow solve's task trace of its last launch made while profiling was on, 6 int64
  * per task for up to cap tasks (task start, end of its dependency wait and task end in ns of
- * %globaltimer; CTA; task kind; a | b << 32 of the task record). Returns the tasks copied or -1. */
+ * %globaltimer; CTA; task kind; a | b << 32 of the task record). With cap < 0: the factorization's
+ * Cholesky step tasks of its last profiled call, 4 int64 per task (start, end of its first waits, end;
+ * CTA | kind << 12 | step << 16 | update block << 28 | front << 40) for up to -cap tasks in the plan's
+ * task order. Returns the tasks copied or -1. */
 int64_t sdsb200_get_trace(sdsb200_plan* plan, int64_t* h_out, int64_t cap);
 
 /* Plan facts: "ns", "nlevels", "factor_len", "cb_len", "launches_factor", "launches_solve",

@@ -90,6 +90,7 @@ int prof_kind_of(LaunchKind k) {
         case L_SMALL: return PK_SMALL;
         case L_ASSEMBLE: return PK_ASSEMBLE;
         case L_CHOL_STEP: return PK_PANEL;
+        case L_CHOL_FLOW: return PK_PANEL;
         case L_GEMM: return PK_GEMM;
         case L_PIVOT_FRONT: return PK_PIVOT;
         case L_SCALE: return PK_SCALE;
@@ -279,6 +280,26 @@ int run_factor(Plan* P, const double* nzval, double eps, double u, int pivot, in
                 a.finfo = P->d_finfo; a.stats = P->d_stats;
                 a.factor_len = P->factor_len; a.ns = (int32_t)P->ns; a.kb = L.cls; a.eps = eps;
                 e = launch_chol_step<T>(a, nm, st);
+                break;
+            }
+            case L_CHOL_FLOW: {
+                // single-system plans only (member 0)
+                unsigned int* cnt = P->d_flow_cnt + L.list2;
+                e = cudaMemsetAsync(cnt, 0, sizeof(unsigned int) * (size_t)(L.count2 + 1), st);
+                if (e != cudaSuccess) break;
+                CholFlowArgs<T> a{};
+                a.tasks = P->d_flow_tasks + L.list;
+                a.ntasks = L.count;
+                a.factor = factor;
+                a.scratch = static_cast<T*>(P->d_inv);
+                a.finfo = P->d_finfo;
+                a.stats = P->d_stats;
+                a.eps = eps;
+                a.cnt = cnt;
+                a.ncnt = L.count2;
+                a.status = P->d_flow_status;
+                a.trace = P->profile ? P->d_flow_trace + 4 * L.list : nullptr;
+                e = launch_chol_flow<T>(a, st);
                 break;
             }
             case L_PIVOT_FRONT: {
@@ -690,8 +711,14 @@ int sdsb200_factor(sdsb200_plan* plan, const double* nzval, const int8_t* h_psig
     if (rc != SDSB200_OK) return rc;
     // the phase's one host synchronization: the reduced info of the active members
     CK(cudaMemcpyAsync(P->h_info_pinned, P->d_info, sizeof(int64_t) * P->nact, cudaMemcpyDeviceToHost, st), "info");
+    int32_t* h_flow_status = reinterpret_cast<int32_t*>(P->h_info_pinned + P->nbatch);
+    CK(cudaMemcpyAsync(h_flow_status, P->d_flow_status, sizeof(int32_t), cudaMemcpyDeviceToHost, st), "status");
     CK(cudaStreamSynchronize(st), "factorization");
     prof_resolve(P);
+    if (*h_flow_status != 0) {
+        cudaMemsetAsync(P->d_flow_status, 0, sizeof(int32_t), st);
+        return fail(SDSB200_TIMEOUT, "a bounded wait of the factorization's step tasks gave up");
+    }
     if (h_info) {
         if (P->all_members) {
             for (int k = 0; k < P->nact; ++k) h_info[k] = P->h_info_pinned[k];
@@ -960,7 +987,14 @@ int sdsb200_set_members(sdsb200_plan* plan, const int32_t* h_members, int32_t na
 
 int64_t sdsb200_get_trace(sdsb200_plan* plan, int64_t* h_out, int64_t cap) {
     Plan* P = reinterpret_cast<Plan*>(plan);
-    if (!P || !h_out || cap < 0) return -1;
+    if (!P || !h_out) return -1;
+    if (cap < 0) {
+        // the factorization's Cholesky step tasks of its last profiled call, in the plan's task order
+        const int64_t nt = std::min<int64_t>(-cap, P->n_flow_tasks);
+        if (nt > 0 && cudaMemcpy(h_out, P->d_flow_trace, sizeof(int64_t) * 4 * nt, cudaMemcpyDeviceToHost) != cudaSuccess)
+            return -1;
+        return nt;
+    }
     // the dataflow solve's task trace of its last profiled launch: 6 int64 per task (start and end of the
     // task and the end of its dependency wait in %globaltimer ns, CTA, kind, a | b << 32)
     const int64_t nt = std::min<int64_t>(cap, P->n_df_tasks);

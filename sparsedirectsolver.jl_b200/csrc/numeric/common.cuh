@@ -79,6 +79,7 @@ enum LaunchKind : int32_t {
     L_CHOL_STEP,       // large Cholesky: one 32-column step (diagonal block + trsm of the rows below)
     L_DFINV,           // diagonal-block inverses of every front for the dataflow solve
     L_PINV,            // GEMM tiles that build the inverse panels of the dataflow solve's tiled fronts
+    L_CHOL_FLOW,       // large Cholesky: every 32-column step of a batch as dataflow tasks in one launch
 };
 
 // One 64 x 64 output tile of the inverse-panel GEMMs: C = A B, or C = -A B (column-major operands).

@@ -12,6 +12,8 @@
 // * gemm_nt_exact_kernel: that update in FP64 in the oracle's summation order (SIMT).
 #include <cuda_runtime.h>
 #include <math.h>
+
+#include <algorithm>
 #include <stdint.h>
 
 #include "common.cuh"
@@ -436,6 +438,374 @@ __global__ void __launch_bounds__(128) chol_step_kernel(CholStepArgs<T> A) {
     }
 }
 
+// ---------------------------------------------------------------------------------------------------
+// The Cholesky steps of a batch as dataflow tasks in one persistent launch (kernels.cuh, FlowTask)
+
+__device__ __forceinline__ uint64_t flow_clock() {
+    uint64_t t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+
+// bounded wait of one thread until *p >= target (about two seconds, then the status word)
+__device__ __noinline__ void flow_wait(const unsigned int* p, unsigned int target, int32_t* status) {
+    unsigned int v;
+    uint64_t t0 = 0;
+    for (long spins = 0;; ++spins) {
+        asm volatile("ld.acquire.gpu.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+        if (v >= target) break;
+        if ((spins & 255) == 0) {
+            if (*(volatile int32_t*)status != 0) return;
+            const uint64_t now = flow_clock();
+            if (spins == 0) t0 = now;
+            else if (now - t0 > 2000000000ull) {
+                atomicExch(status, 1);
+                return;
+            }
+        }
+        if (spins > 4096) __nanosleep(64);
+    }
+}
+
+__device__ __forceinline__ void flow_add(unsigned int* p) {
+    asm volatile("red.release.gpu.global.add.u32 [%0], 1;" ::"l"(p) : "memory");
+}
+
+// acc = A B^T over 32 inner columns on DMMA (mma.sync m8n8k4 f64): warp wp's rows 16 wp .. 16 wp + 15 of
+// a 64-row A, all 32 rows of B; getA(i, l) and getB(c, l) read the staged operands. Entry (i2, j, e) of
+// acc is row 16 wp + 8 i2 + lane / 4, column 8 j + 2 (lane % 4) + e.
+template <class GA, class GB>
+__device__ __forceinline__ void flow_dmma_64x32(int wp, int lane, double (&acc)[2][4][2], GA getA, GB getB) {
+#pragma unroll
+    for (int i = 0; i < 2; ++i)
+#pragma unroll
+        for (int j = 0; j < 4; ++j) acc[i][j][0] = acc[i][j][1] = 0.0;
+#pragma unroll
+    for (int kk = 0; kk < CHOL_NB; kk += 4) {
+        double av[2], bv[4];
+#pragma unroll
+        for (int i = 0; i < 2; ++i) av[i] = getA(16 * wp + 8 * i + (lane >> 2), kk + (lane & 3));
+#pragma unroll
+        for (int j = 0; j < 4; ++j) bv[j] = getB(8 * j + (lane >> 2), kk + (lane & 3));
+#pragma unroll
+        for (int i = 0; i < 2; ++i)
+#pragma unroll
+            for (int j = 0; j < 4; ++j)
+                asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};\n"
+                             : "+d"(acc[i][j][0]), "+d"(acc[i][j][1])
+                             : "d"(av[i]), "d"(bv[j]));
+    }
+}
+
+// C[i, c] -= sum_l A(i, l) B(c, l) over a 64 x 32 tile of the panel at (r0, c0) (rows < nr, columns < nc,
+// row r0 + i >= column c0 + c only), A and B staged in shared memory (getA, getB). FP64 on DMMA; FP32 on
+// the SIMT pipes, thread (tx, ty) owning rows tx + 16 q and columns ty + 8 p. Every C load is issued
+// before the arithmetic.
+template <typename T, class GA, class GB>
+__device__ __forceinline__ void flow_tile_update(T* P, int f, int r0, int c0, int nr, int nc, GA getA, GB getB) {
+    const int tid = threadIdx.x;
+    if constexpr (sizeof(T) == 8) {
+        const int wp = tid >> 5, lane = tid & 31;
+        double cd[2][4][2], acc[2][4][2];
+#pragma unroll
+        for (int i2 = 0; i2 < 2; ++i2)
+#pragma unroll
+            for (int j = 0; j < 4; ++j)
+#pragma unroll
+                for (int e = 0; e < 2; ++e) {
+                    const int i = 16 * wp + 8 * i2 + (lane >> 2), c = 8 * j + 2 * (lane & 3) + e;
+                    cd[i2][j][e] = (i < nr && c < nc && r0 + i >= c0 + c) ? (double)P[(r0 + i) + (int64_t)(c0 + c) * f] : 0.0;
+                }
+        flow_dmma_64x32(wp, lane, acc, getA, getB);
+#pragma unroll
+        for (int i2 = 0; i2 < 2; ++i2)
+#pragma unroll
+            for (int j = 0; j < 4; ++j)
+#pragma unroll
+                for (int e = 0; e < 2; ++e) {
+                    const int i = 16 * wp + 8 * i2 + (lane >> 2), c = 8 * j + 2 * (lane & 3) + e;
+                    if (i < nr && c < nc && r0 + i >= c0 + c) P[(r0 + i) + (int64_t)(c0 + c) * f] = T(cd[i2][j][e] - acc[i2][j][e]);
+                }
+    } else {
+        const int tx = tid & 15, ty = tid >> 4;
+        T cv[4][4], acc[4][4];
+#pragma unroll
+        for (int q = 0; q < 4; ++q)
+#pragma unroll
+            for (int p = 0; p < 4; ++p) {
+                const int i = tx + 16 * q, c = ty + 8 * p;
+                acc[q][p] = T(0);
+                cv[q][p] = (i < nr && c < nc && r0 + i >= c0 + c) ? P[(r0 + i) + (int64_t)(c0 + c) * f] : T(0);
+            }
+#pragma unroll 8
+        for (int l = 0; l < CHOL_NB; ++l) {
+            T ra[4], rb[4];
+#pragma unroll
+            for (int q = 0; q < 4; ++q) ra[q] = getA(tx + 16 * q, l);
+#pragma unroll
+            for (int p = 0; p < 4; ++p) rb[p] = getB(ty + 8 * p, l);
+#pragma unroll
+            for (int q = 0; q < 4; ++q)
+#pragma unroll
+                for (int p = 0; p < 4; ++p) acc[q][p] += ra[q] * rb[p];
+        }
+#pragma unroll
+        for (int q = 0; q < 4; ++q)
+#pragma unroll
+            for (int p = 0; p < 4; ++p) {
+                const int i = tx + 16 * q, c = ty + 8 * p;
+                if (i < nr && c < nc && r0 + i >= c0 + c) P[(r0 + i) + (int64_t)(c0 + c) * f] = cv[q][p] - acc[q][p];
+            }
+    }
+}
+
+// One UPD task: C[rows b .., columns a ..] -= X[rows] X[block rows]^T over the step's 32 columns kb ..
+// (dynamic shared memory: X[rows] then X[block rows], ld 33). Every load of the operands is issued
+// before the first store to shared memory.
+template <typename T>
+__device__ __forceinline__ void flow_update(const CholFlowArgs<T>& A, const FlowTask& t) {
+    constexpr int NB = CHOL_NB, TR = 64, LD = NB + 1;
+    extern __shared__ __align__(16) unsigned char flow_dsm[];
+    T* As = reinterpret_cast<T*>(flow_dsm);   // X[rows]: As[i * LD + l]
+    T* Bs = As + TR * LD;                      // X[block rows]: Bs[c * LD + l]
+    T* P = A.factor + t.panel;
+    const int f = t.f, kb = t.kb, a = t.a, b = t.b;
+    const int nr = min(TR, f - b), nc = min(NB, t.w - a);
+    const int tid = threadIdx.x;
+    T av[(TR * NB) / 128], bv[(NB * NB) / 128];
+#pragma unroll
+    for (int e = 0; e < (TR * NB) / 128; ++e) {
+        const int q = tid + 128 * e, i = q % TR, l = q / TR;
+        av[e] = i < nr ? P[(b + i) + (int64_t)(kb + l) * f] : T(0);
+    }
+#pragma unroll
+    for (int e = 0; e < (NB * NB) / 128; ++e) {
+        const int q = tid + 128 * e, c = q % NB, l = q / NB;
+        bv[e] = c < nc ? P[(a + c) + (int64_t)(kb + l) * f] : T(0);
+    }
+#pragma unroll
+    for (int e = 0; e < (TR * NB) / 128; ++e) {
+        const int q = tid + 128 * e;
+        As[(q % TR) * LD + q / TR] = av[e];
+    }
+#pragma unroll
+    for (int e = 0; e < (NB * NB) / 128; ++e) {
+        const int q = tid + 128 * e;
+        Bs[(q % NB) * LD + q / NB] = bv[e];
+    }
+    __syncthreads();
+    flow_tile_update<T>(P, f, b, a, nr, nc, [&](int i, int l) { return As[i * LD + l]; },
+                        [&](int c, int l) { return Bs[c * LD + l]; });
+}
+
+// One STEP or STEPN task: step kb of front t.front (a block of nbb <= 32 columns) for its row tile t.a
+// (rows r1 + 64 t.a .., r1 = kb + nbb; t.a < 0: no rows below the block), as chol_step_kernel: warp 0
+// factors the diagonal block in registers while warps 1-3 stage the tile, whose rows are then
+// forward-substituted. STEPN then applies the step's update of the next column block (columns
+// kn = kb + 32 ..) to those rows: C[rows, kn ..] -= X[rows] X[kn .. kn + 31]^T (row >= column); the next
+// block's rows are tile 0's first rows.
+template <typename T>
+__device__ __forceinline__ void flow_step(const CholFlowArgs<T>& A, const FlowTask& t) {
+    using CT = T;
+    constexpr int NB = CHOL_NB, LD = NB + 1, TR = 64;
+    __shared__ CT L[NB * LD];
+    __shared__ CT rdiag[NB];          // reciprocal diagonal of L11 (zero past the block)
+    __shared__ CT Bt[TR * LD];        // the tile's rows: B, then X
+    __shared__ CT Ct[NB * LD];        // the next block's rows X (STEPN, tile > 0)
+    __shared__ int s_status, s_ok;
+    const bool next = t.kind == FLOW_STEPN;
+    const int s = t.front, f = t.f, w = t.w, kb = t.kb, tile = t.a;
+    const int nbb = min(NB, w - kb), r1 = kb + nbb, kn = kb + NB, nbn = next ? min(NB, w - kn) : 0;
+    const int row0 = r1 + max(tile, 0) * TR, rows = tile >= 0 ? min(TR, f - row0) : 0;
+    T* P = A.factor + t.panel;
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    if (warp == 0) {
+        const int i = lane;
+        CT x[NB];
+#pragma unroll
+        for (int j = 0; j < NB; ++j) x[j] = (i < nbb && j < nbb && j <= i) ? P[(kb + i) + (int64_t)(kb + j) * f] : CT(0);
+        const CT eps = (CT)A.eps;
+        int status = 0;
+#pragma unroll
+        for (int j = 0; j < NB; ++j) {
+            if (j < nbb && status == 0) {
+                CT a0 = 0, a1 = 0, a2 = 0, a3 = 0;
+#pragma unroll
+                for (int l = 0; l < j; ++l) {
+                    const CT v = x[l] * __shfl_sync(0xffffffffu, x[l], j);
+                    if ((l & 3) == 0) a0 += v;
+                    else if ((l & 3) == 1) a1 += v;
+                    else if ((l & 3) == 2) a2 += v;
+                    else a3 += v;
+                }
+                const CT sv = x[j] - ((a0 + a1) + (a2 + a3));
+                const CT ajj = __shfl_sync(0xffffffffu, sv, j);
+                if (!(ajj > eps || (eps > 0 && ajj >= 0))) {
+                    status = j + 1;
+                } else {
+                    const CT d = ajj > eps ? ajj : eps;
+                    const CT r = rsqrt(d);
+                    if (i == j) {
+                        x[j] = d * r;
+                        rdiag[j] = r;
+                    } else if (i > j && i < nbb) {
+                        x[j] = sv * r;
+                    }
+                }
+            }
+        }
+#pragma unroll
+        for (int j = 0; j < NB; ++j) L[i * LD + j] = x[j];
+        if (i >= nbb) rdiag[i] = CT(0);
+        if (lane == 0) s_status = status;
+    } else {
+        batched_copy<8>(tid - 32, 96, TR * NB,
+                        [&](int q) {
+                            const int r = q % TR, c = q / TR;
+                            return (r < rows && c < nbb) ? (double)P[(row0 + r) + (int64_t)(kb + c) * f] : 0.0;
+                        },
+                        [&](int q, double v) { Bt[(q % TR) * LD + q / TR] = (CT)v; });
+    }
+    __syncthreads();
+    const int status = s_status;
+    if (tid == 0) {
+        const bool alive = A.finfo[s] == 0;   // no earlier step of the front failed
+        s_ok = alive && status == 0;
+        if (alive && tile <= 0) {
+            int64_t* S = A.stats + (int64_t)s * NSTAT;
+            if (status) {
+                A.finfo[s] = kb + status;
+                S[ST_NPOS] = kb + status - 1;
+                S[ST_INFO] = kb + status;
+            } else if (kb + nbb == w) {
+                S[ST_NPOS] = w;
+                S[ST_INFO] = 0;
+            }
+        }
+    }
+    __syncthreads();
+    const bool ok = s_ok != 0;
+    if (ok && tile <= 0) {
+        // L11 with zeros above the diagonal: the scratch (the COPY task writes it into the panel), or the
+        // panel when no rows are below the block
+        T* dst = tile < 0 ? P + kb + (int64_t)kb * f : A.scratch + t.scr;
+        const int64_t ld = tile < 0 ? f : NB;
+        for (int q = tid; q < nbb * nbb; q += blockDim.x) {
+            const int i = q % nbb, j = q / nbb;
+            dst[i + j * ld] = j <= i ? T(L[i * LD + j]) : T(0);
+        }
+    }
+    // X = B L11^{-T}, threads < rows, into the panel and kept in Bt; columns past the block have a zero
+    // reciprocal diagonal
+    if (ok && tid < rows) {
+        const int r = tid;
+        CT x[NB];
+#pragma unroll
+        for (int j = 0; j < NB; ++j) {
+            CT a0 = Bt[r * LD + j], a1 = 0, a2 = 0, a3 = 0;
+#pragma unroll
+            for (int l = 0; l < j; ++l) {
+                const CT v = x[l] * L[j * LD + l];
+                if ((l & 3) == 0) a0 -= v;
+                else if ((l & 3) == 1) a1 -= v;
+                else if ((l & 3) == 2) a2 -= v;
+                else a3 -= v;
+            }
+            x[j] = ((a0 + a1) + (a2 + a3)) * rdiag[j];
+        }
+#pragma unroll
+        for (int j = 0; j < NB; ++j) {
+            Bt[r * LD + j] = x[j];
+            if (j < nbb) P[(row0 + r) + (int64_t)(kb + j) * f] = T(x[j]);
+        }
+    }
+    if (!next) return;
+    __syncthreads();
+    if (tid == 0) {
+        if (t.sig_mid >= 0) flow_add(A.cnt + t.sig_mid);
+        if (t.sig_head >= 0) flow_add(A.cnt + t.sig_head);
+        if (t.w_mid >= 0) flow_wait(A.cnt + t.w_mid, 1u, A.status);
+        if (t.w2 >= 0) flow_wait(A.cnt + t.w2, (unsigned)t.v2, A.status);
+    }
+    __syncthreads();
+    if (!ok) return;
+    if (tile > 0) {   // the next block's rows, solved by tile 0
+        for (int q = tid; q < NB * NB; q += blockDim.x) {
+            const int r = q % NB, c = q / NB;
+            Ct[r * LD + c] = r < nbn ? P[(kn + r) + (int64_t)(kb + c) * f] : CT(0);
+        }
+        __syncthreads();
+    }
+    const CT* Xn = tile > 0 ? Ct : Bt;
+    flow_tile_update<T>(P, f, row0, kn, rows, nbn, [&](int i, int l) { return Bt[i * LD + l]; },
+                        [&](int c, int l) { return Xn[c * LD + l]; });
+}
+
+template <typename T>
+__global__ void __launch_bounds__(128) chol_flow_kernel(CholFlowArgs<T> A) {
+    __shared__ int task_k;
+    const int tid = threadIdx.x;
+    while (true) {
+        if (tid == 0) {
+            task_k = (int)atomicAdd(A.cnt + A.ncnt, 1u);
+            if (*(volatile int32_t*)A.status != 0) task_k = A.ntasks;   // a wait gave up: stop
+        }
+        __syncthreads();
+        const int k = task_k;
+        if (k >= A.ntasks) break;
+        const FlowTask t = A.tasks[k];
+        if (tid == 0) {
+            if (A.trace) {
+                A.trace[4 * k] = (int64_t)flow_clock();
+                A.trace[4 * k + 3] = (int64_t)blockIdx.x | ((int64_t)t.kind << 12) | ((int64_t)(t.kb / CHOL_NB) << 16) |
+                                     ((int64_t)(t.kind == FLOW_UPD ? t.a / CHOL_NB : 0) << 28) | ((int64_t)t.front << 40);
+            }
+            if (t.w1 >= 0) flow_wait(A.cnt + t.w1, (unsigned)t.v1, A.status);
+            if (t.w2 >= 0 && t.kind != FLOW_STEPN) flow_wait(A.cnt + t.w2, (unsigned)t.v2, A.status);
+            if (A.trace) A.trace[4 * k + 1] = (int64_t)flow_clock();
+        }
+        __syncthreads();
+        if (t.kind == FLOW_STEP || t.kind == FLOW_STEPN) {
+            flow_step<T>(A, t);
+        } else if (t.kind == FLOW_COPY) {
+            const int nbb = min(CHOL_NB, t.w - t.kb);
+            const T* src = A.scratch + t.scr;
+            T* dst = A.factor + t.panel + t.kb + (int64_t)t.kb * t.f;
+            for (int q = tid; q < nbb * nbb; q += blockDim.x)
+                dst[q % nbb + (int64_t)(q / nbb) * t.f] = src[q % nbb + (q / nbb) * CHOL_NB];
+        } else if (t.kind == FLOW_UPD) {
+            if (A.finfo[t.front] == 0) flow_update<T>(A, t);
+        }
+        __syncthreads();
+        if (tid == 0) {
+            if (A.trace) A.trace[4 * k + 2] = (int64_t)flow_clock();
+            if (t.sig_add >= 0) flow_add(A.cnt + t.sig_add);
+            if (t.sig_store >= 0)
+                asm volatile("st.release.gpu.u32 [%0], %1;" ::"l"(A.cnt + t.sig_store), "r"((unsigned)t.sig_val) : "memory");
+        }
+    }
+}
+
+template <typename T>
+constexpr size_t chol_flow_smem() {
+    return sizeof(T) * (64 + CHOL_NB) * (CHOL_NB + 1);
+}
+
+template <typename T>
+cudaError_t launch_chol_flow(const CholFlowArgs<T>& a, cudaStream_t st) {
+    if (a.ntasks == 0) return cudaSuccess;
+    int dev = 0, sms = 0, per = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, chol_flow_kernel<T>, 128, chol_flow_smem<T>());
+    const int grid = std::max(1, std::min(a.ntasks, sms * std::max(per, 1)));
+    chol_flow_kernel<T><<<grid, 128, chol_flow_smem<T>(), st>>>(a);
+    return cudaGetLastError();
+}
+
+template cudaError_t launch_chol_flow<double>(const CholFlowArgs<double>&, cudaStream_t);
+template cudaError_t launch_chol_flow<float>(const CholFlowArgs<float>&, cudaStream_t);
+
 template <typename T>
 cudaError_t launch_chol_step(const CholStepArgs<T>& a, int nmembers, cudaStream_t st) {
     if (a.count == 0) return cudaSuccess;
@@ -584,8 +954,13 @@ template cudaError_t launch_block_inv<double>(const BlockInvArgs<double>&, int, 
 template cudaError_t launch_block_inv<float>(const BlockInvArgs<float>&, int, cudaStream_t);
 
 cudaError_t prepare_dense_kernels(int max_smem) {
-    (void)max_smem;   // the dense kernels use static shared memory only
-    return cudaSuccess;
+    (void)max_smem;   // static shared memory, but for the flow kernel's update stage
+    cudaError_t e = cudaFuncSetAttribute(chol_flow_kernel<double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)chol_flow_smem<double>());
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(chol_flow_kernel<float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)chol_flow_smem<float>());
+    return e;
 }
 
 template cudaError_t launch_gemm<double>(const GemmArgs<double>&, int, cudaStream_t);

@@ -69,6 +69,54 @@ struct CholStepTask {
     int32_t f, w;      // record before the block loads)
 };
 
+// The 32-column steps of a batch of large Cholesky fronts as dataflow in one persistent launch
+// (single-system plans). Tasks, in list order:
+//  * STEP: the step's diagonal block (factored by every task of the step, as chol_step_kernel does) and
+//    one 64-row tile of the rows below, forward-substituted; for the front's last step;
+//  * STEPN: the same, then the step's update of the next column block on the tile's rows, so that the
+//    chain of a front's steps is one task per step. After its substitution it signals sig_mid (its rows
+//    are in the panel; tile 0 also sig_head) and then waits for tile 0 (w_mid: the next block's rows
+//    are tile 0's first rows) and for the block's earlier updates (w2 >= v2);
+//  * COPY: the step's L11 from its scratch slot into the panel, once every task of the step is done;
+//  * UPD: the step's rank-32 update of one (64-row tile, 32-column block) of the front's trailing
+//    columns beyond the next block: C -= X_k[rows] X_k[block rows]^T, lower part only.
+// A task waits on counters (>= a target) and signals counters (increments, or a release store of a
+// value). Every wait is on tasks earlier in the list, so CTAs that take tasks in order from one counter
+// always progress; the updates of the following blocks come after the next step's tasks (lookahead).
+enum FlowKind : int32_t { FLOW_STEP = 1, FLOW_COPY = 2, FLOW_UPD = 3, FLOW_STEPN = 4 };
+struct FlowTask {
+    int32_t kind, front;
+    int32_t kb;              // the step's first column
+    int32_t a, b;            // STEP/STEPN: row tile (-1: no rows below the block); UPD: the block's first
+                             // column, the tile's first row
+    int32_t w1, v1, w2, v2;  // waits: counter w >= v (w < 0: none); STEPN waits for w2 after its substitution
+    int32_t sig_add;         // counter incremented when done (-1: none)
+    int32_t sig_store, sig_val;   // counter set to sig_val when done (-1: none)
+    int32_t sig_mid;         // STEPN: counter incremented once the tile's rows are in the panel (-1: none);
+    int32_t sig_head;        // tile 0 also increments this one (-1: none)
+    int32_t w_mid;           // STEPN tiles > 0 then wait for it (>= 1; -1: none)
+    int32_t f, w;
+    int64_t panel;           // the front's panel offset
+    int64_t scr;             // the step's L11 scratch slot
+};
+template <typename T>
+struct CholFlowArgs {
+    const FlowTask* tasks;
+    int32_t ntasks;
+    T* factor;
+    T* scratch;
+    int32_t* finfo;
+    int64_t* stats;
+    double eps;
+    unsigned int* cnt;       // the batch's counters, zero at launch; cnt[ncnt] is the task counter
+    int32_t ncnt;
+    int32_t* status;         // nonzero: a bounded wait gave up
+    int64_t* trace;          // profiling, or NULL: per task (start, wait done, end) %globaltimer ns, and
+                             // CTA | kind << 12 | step << 16 | update block << 28 | front << 40
+};
+template <typename T>
+cudaError_t launch_chol_flow(const CholFlowArgs<T>& a, cudaStream_t st);
+
 template <typename T>
 struct CholStepArgs {
     const DFront* fronts;

@@ -276,9 +276,10 @@ Plan* build_plan(const sdsb200_symbolic* sym, const sdsb200_plan_options* popts,
         }
         if (tune_wide && (tune_wide < 16 || tune_wide > DF_WARP_F))
             throw BuildError(SDSB200_INVALID_VALUE, "tuning: wide (the tallest warp front of the solve) must lie in 16..128");
-        const int tune_chains = tune_rsv & 1, tune_streams = (tune_rsv >> 1) & 15;
-        if (tune_rsv > 31)
-            throw BuildError(SDSB200_INVALID_VALUE, "tuning: the third field is chains (bit 0) | streams << 1 (streams < 16)");
+        const int tune_chains = tune_rsv & 1, tune_streams = (tune_rsv >> 1) & 15, tune_steps = (tune_rsv >> 5) & 1;
+        if (tune_rsv > 63)
+            throw BuildError(SDSB200_INVALID_VALUE,
+                             "tuning: the third field is chains (bit 0) | streams << 1 (streams < 16) | steps << 5");
         const int warp_f = tune_wide ? tune_wide : DF_WARP_F;
         const bool pinv_mode = tune_chains == 0;   // tiled fronts solved through inverse panels
         P->fsmall_max = classes.back();
@@ -416,6 +417,12 @@ Plan* build_plan(const sdsb200_symbolic* sym, const sdsb200_plan_options* popts,
         std::vector<int64_t> scr_stream(P->nfstreams, 0);   // each stream's step scratch size
         // step tasks and copy tiles whose scratch slots move to their stream's part of the scratch
         std::vector<std::vector<size_t>> step_rebase(P->nfstreams), tile_rebase(P->nfstreams);
+        std::vector<std::vector<size_t>> flow_rebase(P->nfstreams);
+        std::vector<FlowTask> flowtasks;
+        int64_t ncnt_total = 0;
+        // single-system Cholesky plans with tuning steps = 1: a batch's steps as one dataflow launch
+        // (default: one launch per step and kernel, measured faster on lap3d 48^3)
+        const bool flow_mode = P->nbatch == 1 && tune_steps == 1;
         for (int L = 0; L < P->nlevels; ++L)
           for (int sg = 0; sg < P->nfstreams; ++sg) {
             std::map<int, std::vector<int>> small;
@@ -472,7 +479,125 @@ Plan* build_plan(const sdsb200_symbolic* sym, const sdsb200_plan_options* popts,
                 P->prog.push_back(pl);
             }
             if (L == P->schur_level) continue;   // the Schur root is assembled, not factored
-            if (P->structure == STRUCT_SPD) {
+            if (P->structure == STRUCT_SPD && flow_mode) {
+                // the steps as dataflow tasks in one persistent launch (kernels.cuh, FlowTask), then the
+                // contribution-block update. Per front: counters of the steps' tasks done (sd), of the
+                // column blocks' tiles updated by their previous step (cr), of tile 0 substituted (hd),
+                // and per (block, row tile) the steps applied (tf).
+                const int NB = CHOL_NB;
+                ProgLaunch fl{};
+                fl.kind = L_CHOL_FLOW;
+                fl.level = L;
+                fl.list = (int64_t)flowtasks.size();
+                fl.list2 = ncnt_total;
+                int32_t nc = 0;
+                int64_t scr = 0;
+                struct FS { int s, K; int32_t sd, cr, hd, tf; std::vector<int32_t> tf_off; std::vector<int> nt; int64_t slot0; };
+                std::vector<FS> fs;
+                int Kmax = 0;
+                for (int s : large) {
+                    const DFront& F = P->fronts[s];
+                    FS x{};
+                    x.s = s;
+                    x.K = (F.w + NB - 1) / NB;
+                    Kmax = std::max(Kmax, x.K);
+                    x.sd = nc; nc += x.K;
+                    x.cr = nc; nc += x.K;
+                    x.hd = nc; nc += x.K;
+                    x.tf = nc;
+                    for (int j = 0; j < x.K; ++j) {
+                        x.tf_off.push_back(nc - x.tf);
+                        nc += (F.f - NB * j + 63) / 64;
+                    }
+                    for (int k = 0; k < x.K; ++k) {
+                        const int nbb = std::min(NB, F.w - NB * k), rows = F.f - (NB * k + nbb);
+                        x.nt.push_back(rows > 0 ? (rows + 63) / 64 : 1);
+                    }
+                    x.slot0 = scr;
+                    scr += (int64_t)NB * NB * x.K;
+                    fs.push_back(std::move(x));
+                }
+                // the update of step k on column block j (j >= k + 2; block k + 1 is updated by the
+                // step's own tasks), every row tile of the block
+                auto upd = [&](const FS& x, int k, int j) {
+                    const DFront& F = P->fronts[x.s];
+                    const int nr = (F.f - NB * j + 63) / 64;
+                    for (int r = 0; r < nr; ++r) {
+                        FlowTask t{};
+                        t.kind = FLOW_UPD; t.front = x.s; t.kb = NB * k; t.a = NB * j; t.b = NB * j + 64 * r;
+                        t.w1 = x.sd + k; t.v1 = x.nt[k];
+                        t.w2 = k > 0 ? x.tf + x.tf_off[j] + r : -1; t.v2 = k;
+                        t.sig_store = x.tf + x.tf_off[j] + r; t.sig_val = k + 1;
+                        t.sig_add = -1; t.sig_mid = -1; t.sig_head = -1; t.w_mid = -1;
+                        t.f = F.f; t.w = F.w; t.panel = F.panel; t.scr = 0;
+                        flowtasks.push_back(t);
+                        fl.flops += 2.0 * std::min(64, F.f - t.b) * std::min(NB, F.w - t.a) * NB;
+                    }
+                };
+                for (int k = 0; k < Kmax; ++k) {
+                    for (const FS& x : fs)   // the previous step's updates of this step's next block
+                        if (k >= 1 && k + 1 < x.K) upd(x, k - 1, k + 1);
+                    for (const FS& x : fs) {
+                        if (k >= x.K) continue;
+                        const DFront& F = P->fronts[x.s];
+                        const int nbb = std::min(NB, F.w - NB * k), rows = F.f - (NB * k + nbb);
+                        const bool next = k + 1 < x.K;   // STEPN: the step also updates block k + 1
+                        for (int t = 0; t < x.nt[k]; ++t) {
+                            FlowTask ft{};
+                            ft.kind = next ? FLOW_STEPN : FLOW_STEP; ft.front = x.s; ft.kb = NB * k;
+                            ft.a = rows > 0 ? t : -1; ft.b = 0;
+                            ft.w1 = k > 0 ? x.cr + k : -1;
+                            ft.v1 = k > 0 ? (F.f - NB * k + 63) / 64 : 0;
+                            ft.w2 = next && k > 0 ? x.tf + x.tf_off[k + 1] + t : -1;
+                            ft.v2 = k;
+                            if (next) {
+                                ft.sig_mid = x.sd + k;
+                                ft.sig_head = t == 0 ? x.hd + k : -1;
+                                ft.w_mid = t > 0 ? x.hd + k : -1;
+                                ft.sig_store = x.tf + x.tf_off[k + 1] + t; ft.sig_val = k + 1;
+                                ft.sig_add = x.cr + k + 1;
+                            } else {
+                                ft.sig_mid = -1; ft.sig_head = -1; ft.w_mid = -1; ft.sig_store = -1;
+                                ft.sig_add = x.sd + k;
+                            }
+                            ft.f = F.f; ft.w = F.w; ft.panel = F.panel;
+                            ft.scr = rows > 0 ? x.slot0 + (int64_t)NB * NB * k : 0;
+                            if (rows > 0) flow_rebase[sg].push_back(flowtasks.size());
+                            flowtasks.push_back(ft);
+                        }
+                        fl.flops += 2.0 * nbb * nbb * nbb / 3.0 + 2.0 * (double)std::max(rows, 0) * nbb * nbb;
+                        if (next) fl.flops += 2.0 * (F.f - NB * (k + 1)) * std::min(NB, F.w - NB * (k + 1)) * NB;
+                        if (rows > 0) {
+                            FlowTask ct{};
+                            ct.kind = FLOW_COPY; ct.front = x.s; ct.kb = NB * k;
+                            ct.w1 = x.sd + k; ct.v1 = x.nt[k]; ct.w2 = -1;
+                            ct.sig_add = -1; ct.sig_store = -1; ct.sig_mid = -1; ct.sig_head = -1; ct.w_mid = -1;
+                            ct.f = F.f; ct.w = F.w; ct.panel = F.panel;
+                            ct.scr = x.slot0 + (int64_t)NB * NB * k;
+                            flow_rebase[sg].push_back(flowtasks.size());
+                            flowtasks.push_back(ct);
+                        }
+                    }
+                    for (const FS& x : fs)   // the previous step's updates beyond
+                        for (int j = k + 2; k >= 1 && j < x.K; ++j) upd(x, k - 1, j);
+                }
+                fl.count = to_i32((int64_t)flowtasks.size() - fl.list, "flow tasks");
+                fl.count2 = nc;
+                ncnt_total += nc + 1;
+                scr_stream[sg] = std::max(scr_stream[sg], scr);
+                if (fl.count) P->prog.push_back(fl);
+                ProgLaunch cl{};
+                cl.kind = L_GEMM; cl.level = L; cl.list = (int64_t)tiles.size();
+                cl.abuf = cl.bbuf = BUF_FACTOR; cl.cbuf = BUF_CB;
+                for (int s : large) {
+                    const DFront& F = P->fronts[s];
+                    int m = F.f - F.w;
+                    if (F.cb < 0 || m == 0) continue;
+                    cl.flops += add_gemm_tiles(F.panel + F.w, F.f, F.panel + F.w, F.f, F.cb, m, m, m, F.w, true, s);
+                }
+                cl.count = (int)(tiles.size() - cl.list);
+                if (cl.count) P->prog.push_back(cl);
+            } else if (P->structure == STRUCT_SPD) {
                 const int NB = CHOL_NB;
                 int maxw = 0;
                 for (int s : large) maxw = std::max(maxw, P->fronts[s].w);
@@ -613,8 +738,13 @@ Plan* build_plan(const sdsb200_symbolic* sym, const sdsb200_plan_options* popts,
             for (int g = 0; g < P->nfstreams; ++g) {
                 for (size_t i : step_rebase[g]) steptasks[i].scr += base;
                 for (size_t i : tile_rebase[g]) tiles[i].a += base;
+                for (size_t i : flow_rebase[g]) flowtasks[i].scr += base;
                 base += scr_stream[g];
             }
+            P->d_flow_tasks = upload(P, flowtasks, st);
+            P->n_flow_tasks = (int64_t)flowtasks.size();
+            P->d_flow_trace = dalloc<int64_t>(P, 4 * std::max<int64_t>(1, P->n_flow_tasks));
+            P->flow_cnt_len = ncnt_total;
             P->inv_len = std::max(P->inv_len, base);
             std::vector<int> ev_of_batch(batches.size(), -1);
             std::vector<std::vector<int>> waits(batches.size());
@@ -1187,6 +1317,9 @@ Plan* build_plan(const sdsb200_symbolic* sym, const sdsb200_plan_options* popts,
         P->d_dfinv_L = alloc_bytes(es * P->df_inv_len * nb);
         if (gen) P->d_dfinv_U = alloc_bytes(es * P->df_inv_len * nb);
         if (P->pwork_len) P->d_pwork = alloc_bytes(es * P->pwork_len * nb * (gen ? 2 : 1));
+        if (P->flow_cnt_len) P->d_flow_cnt = dalloc<unsigned int>(P, P->flow_cnt_len);
+        P->d_flow_status = dalloc<int32_t>(P, 1);
+        cudaMemsetAsync(P->d_flow_status, 0, sizeof(int32_t), st);
         if (P->psplit_slots) {
             P->d_psplit = alloc_bytes(es * P->psplit_slots * 64 * 64);
             P->d_pcnt = dalloc<unsigned int>(P, P->psplit_cnts);
@@ -1201,7 +1334,8 @@ Plan* build_plan(const sdsb200_symbolic* sym, const sdsb200_plan_options* popts,
         P->d_norms = dalloc<double>(P, 2 * P->max_nrhs * nb);
         if (cudaMallocHost(&P->h_norms, sizeof(double) * 2 * P->max_nrhs * nb) != cudaSuccess)
             throw BuildError(SDSB200_ALLOC_FAILED, "cudaMallocHost");
-        if (cudaMallocHost(&P->h_info_pinned, sizeof(int64_t) * nb) != cudaSuccess)
+        // info of every member, then the step tasks' status word
+        if (cudaMallocHost(&P->h_info_pinned, sizeof(int64_t) * (nb + 1)) != cudaSuccess)
             throw BuildError(SDSB200_ALLOC_FAILED, "cudaMallocHost");
         {
             int dev = 0, optin = 0;

@@ -125,6 +125,12 @@ struct Plan {
     PinvTile* d_pinv_tiles = nullptr;   // the GEMM tiles that build the inverse panels (kind L_PINV)
     int64_t pwork_len = 0;              // their scratch (T = L[C, A] X[A, A] of one doubling level), per member and side
     void* d_pwork = nullptr;
+    FlowTask* d_flow_tasks = nullptr;   // the Cholesky steps' dataflow tasks (kind L_CHOL_FLOW)
+    int64_t n_flow_tasks = 0;
+    unsigned int* d_flow_cnt = nullptr; // their counters: per launch count2 + 1 at list2, zeroed per launch
+    int64_t flow_cnt_len = 0;
+    int32_t* d_flow_status = nullptr;   // nonzero: a bounded wait of the step tasks gave up
+    int64_t* d_flow_trace = nullptr;    // profiling: 4 int64 per step task
     int64_t psplit_slots = 0, psplit_cnts = 0;   // split tiles: most partial slots and counters of a launch
     void* d_psplit = nullptr;           // their 64 x 64 partial products
     unsigned int* d_pcnt = nullptr;     // their arrival counters (reset by the last arrival)

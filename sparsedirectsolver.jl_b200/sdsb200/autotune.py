@@ -70,7 +70,7 @@ def autotune(solver, B, candidates=CANDIDATES, reps=3, use_cache=True):
 
 def describe(t):
     return {"fsmall": int(t) & 0x1FF, "wide": (int(t) >> 9) & 0x7FF, "chains": (int(t) >> 20) & 1,
-            "streams": (int(t) >> 21) & 15}
+            "streams": (int(t) >> 21) & 15, "steps": (int(t) >> 25) & 1}
 
 
 __all__ = ["autotune", "describe", "CANDIDATES"]

@@ -328,6 +328,33 @@ def test_persistent_solve_matches_level_launches(torch_cuda, structure):
         assert np.abs(x1 - x0).max() <= 1e-10 * np.abs(x0).max()
 
 
+@pytest.mark.parametrize("precision", ["fp64", "fp32"])
+def test_dataflow_cholesky_steps_match_step_launches(torch_cuda, precision):
+    # the large fronts' 32-column steps as dataflow tasks in one persistent launch per batch (tuning
+    # steps = 1) against one launch per step and kernel: the same factor to rounding, the same statistics,
+    # on several streams; and against the oracle
+    from sdsb200.capi import tuning
+
+    A = M.lap3d(20, 20, 20, seed=6)
+    S, O, info = oracle_for(A, "SPD", reordering="nd")
+    out = {}
+    for steps in (0, 1):
+        ds = _solver(A, "SPD", reordering_alg="nd", max_nrhs=4, factor_precision=precision,
+                     tuning=tuning(0, 0, 0, 0, steps))
+        ds.execute("analysis")
+        assert ds.execute("factorization") == 0
+        fac, _ = ds.factor_host()
+        out[steps] = (dense_panels(S, fac), ds.stats_host())
+        b = M.rhs(A.shape[0], 3, seed=7)
+        x = ds.execute("solve", None, b).cpu().numpy()
+        assert M.scaled_backward_error(A, x, b) <= (BERR if precision == "fp64" else 1e-5)
+    tol = FP64_TOL if precision == "fp64" else 1e-5
+    assert rel_max_diff(out[1][0], out[0][0]) <= tol
+    assert np.array_equal(out[1][1], out[0][1])
+    assert rel_max_diff(out[1][0], dense_panels(S, O.factor)) <= tol
+    assert S.front_ncols.max() > 96   # several steps per front
+
+
 @pytest.mark.parametrize("structure,precision", [("SPD", "fp64"), ("S", "fp64"), ("G", "fp64"), ("SPD", "fp32")])
 def test_inverse_panels_match_block_chains(torch_cuda, structure, precision):
     # the dataflow solve's two forms for tiled fronts: inverse panels [L11^-1; L21 L11^-1] built after the
