@@ -59,6 +59,10 @@ def parse():
                          "systems, c4u uniform batch 96x96 x 256, c5 LU convection-diffusion 40^3 with A and A^T")
     ap.add_argument("--tuning", default=None,
                     help="fsmall,wide,chains: fixed front tile shapes instead of the autotuner's search (for profilers)")
+    ap.add_argument("--amalgamation", default="512,0.25,8",
+                    help="max_width,zero_fraction,min_width of the solver's supernode amalgamation (a solver option "
+                         "of the reference's; its default is 32,0.25,8). The metric's flops are always those of the "
+                         "default amalgamation, as the reference arm's")
     ap.add_argument("--once", choices=["fp64", "mixed"], default=None,
                     help="one analysis + factorization + solve of the workload in one form, untimed (for profilers); "
                          "with --config c3 or c5 that workload")
@@ -88,6 +92,7 @@ def run_once(args):
         A, b = workload(args.grid)
         structure, nrhs = "SPD", NRHS
         kw["reordering_alg"] = "nd"
+        kw["amalgamation"] = amalgamation_of(args)
         size = {"grid": args.grid}
     ds = DirectSolver(A, structure, max_nrhs=nrhs, **kw)
     ds.execute("analysis")
@@ -97,6 +102,11 @@ def run_once(args):
     berr = M.scaled_backward_error(A, x.cpu().numpy().reshape(A.shape[0], -1), b.reshape(A.shape[0], -1))
     print(json.dumps({"once": args.once, "config": args.config, **size, "bwd_err": berr}), flush=True)
     assert berr <= BERR_TARGET
+
+
+def amalgamation_of(args):
+    v = [x for x in args.amalgamation.split(",")]
+    return (int(v[0]), float(v[1]), int(v[2]))
 
 
 def config_matrix(args):
@@ -330,9 +340,19 @@ class ClockSampler:
                  "--query-gpu=clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
                  "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
                  "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap",
-                 "--format=csv,noheader,nounits", "-lms", "100"], stdout=self.fh, stderr=subprocess.DEVNULL)
+                 "--format=csv,noheader,nounits", "-lms", "50"], stdout=self.fh, stderr=subprocess.DEVNULL)
         except OSError:
             self.proc = None
+            return self
+        # the timed region is short (~0.1 s): start it only once nvidia-smi writes samples, and drop the
+        # samples taken before it
+        t0 = time.time()
+        while time.time() - t0 < 5.0 and self.proc.poll() is None:
+            self.fh.flush()
+            if os.path.getsize(self.path) > 0:
+                break
+            time.sleep(0.01)
+        self.skip = sum(1 for _ in open(self.path))
         return self
 
     def __exit__(self, *exc):
@@ -349,7 +369,9 @@ class ClockSampler:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
         sm, smax, reasons = [], None, set()
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for line in open(self.path):
+        lines = list(open(self.path))
+        # the samples from the timed region on (the last before it when none fell inside)
+        for line in lines[max(0, getattr(self, "skip", 0) - 1):]:
             parts = [x.strip() for x in line.split(",")]
             if len(parts) < 8:
                 continue
@@ -479,7 +501,7 @@ def main():
     tuned = {}
     Bt = torch.from_numpy(np.ascontiguousarray(b)).cuda()
     for name, kw in forms.items():
-        ds = DirectSolver(A, "SPD", reordering_alg="nd", max_nrhs=NRHS, **kw)
+        ds = DirectSolver(A, "SPD", reordering_alg="nd", max_nrhs=NRHS, amalgamation=amalgamation_of(args), **kw)
         if solvers:                      # one analysis for both forms
             ds.symbolic = next(iter(solvers.values())).symbolic
             ds._stage = 1
@@ -500,7 +522,12 @@ def main():
             tuned[name] = describe(min(times, key=times.get))
         solvers[name] = ds
     S = solvers["fp64"].symbolic
-    flops = S.flops + 4.0 * S.nnz_stored * NRHS
+    # the metric's flops: the reference's default amalgamation (as the reference arm's), whatever the
+    # solver's amalgamation (a wider one stores explicit zeros, whose flops are not counted)
+    from sdsb200 import analyze_csr
+
+    S0 = analyze_csr(A, "SPD", reordering="nd")
+    flops = S0.flops + 4.0 * S0.nnz_stored * NRHS
     stream = torch.cuda.current_stream()
     st = C.c_void_p(stream.cuda_stream)
     Bd = torch.from_numpy(np.ascontiguousarray(b.T)).cuda()        # column-major n x nrhs
@@ -657,7 +684,7 @@ def main():
     if rank == 0 and not args.no_cpu_baseline:
         from oracle.blas_port import CholeskyPort, blas_threads
 
-        P = CholeskyPort(S)
+        P = CholeskyPort(S0)                     # the reference's CPU path on its default Symbolic
         P.factorize(A.data)                      # once untimed: pages in the fronts and the BLAS threads
         t0 = time.perf_counter()
         P.factorize(A.data)
@@ -681,7 +708,8 @@ def main():
         "config": {"workload": f"lap3d_{args.grid} SPD Cholesky factor+solve to bwd err <= 1e-12, nested dissection, "
                                f"{NRHS} RHS (form: mixed FP32 factor + FP64 IR)",
                    "n": int(n), "nnz": int(A.nnz), "nnz_stored": int(S.nnz_stored), "flops_per_step": flops,
-                   "factor_flops": S.flops, "parallelism": f"replicas x{world}",
+                   "factor_flops": S0.flops, "amalgamation": list(amalgamation_of(args)),
+                   "factor_flops_stored": S.flops, "parallelism": f"replicas x{world}",
                    "l2": "inputs larger than L2 (factor %.0f MB)" % (S.nnz_stored * 4 / 1e6)},
         "bwd_err": r["berr"], "ir_steps": r["ir_steps"], "ir_probe_bwd_err": ir_probe,
         "err_vs_fp64_per_rhs": err_vs_fp64,

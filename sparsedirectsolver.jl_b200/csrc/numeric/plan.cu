@@ -865,12 +865,20 @@ Plan* build_plan(const sdsb200_symbolic* sym, const sdsb200_plan_options* popts,
             }
             std::vector<DfTask> tasks;
             std::vector<int32_t> bundles;
+            // a level's warp fronts in bundles of at least DF_BUNDLE, more when the level has more fronts
+            // than 8 per resident CTA: a bundle's warps take its fronts in turn, so a warp whose front
+            // waits long holds up fewer others, and the CTAs spend fewer task switches
+            int dev_ = 0, sms_ = 148;
+            cudaGetDevice(&dev_);
+            cudaDeviceGetAttribute(&sms_, cudaDevAttrMultiProcessorCount, dev_);
+            const size_t df_ctas = 2 * (size_t)std::max(sms_, 1);
             auto push_bundles = [&](int L, int kind) {
                 std::vector<int32_t> wl;
                 for (int s : P->level_fronts[L])
                     if (s != P->schur_front && !df[s].tiled) wl.push_back(s);
-                for (size_t o = 0; o < wl.size(); o += DF_BUNDLE) {
-                    const int cnt = (int)std::min<size_t>(DF_BUNDLE, wl.size() - o);
+                const size_t bsz = std::max<size_t>(DF_BUNDLE, (wl.size() + df_ctas - 1) / df_ctas);
+                for (size_t o = 0; o < wl.size(); o += bsz) {
+                    const int cnt = (int)std::min<size_t>(bsz, wl.size() - o);
                     tasks.push_back(DfTask{kind, (int32_t)bundles.size(), cnt, 0});
                     bundles.insert(bundles.end(), wl.begin() + o, wl.begin() + o + cnt);
                 }
