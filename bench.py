@@ -58,7 +58,8 @@ def parse():
                          "other workloads: c1 lap2d_64 SPD AMD, c3 KKT LDL^T (n = 55 000), c4 1024 uneven "
                          "systems, c4u uniform batch 96x96 x 256, c5 LU convection-diffusion 40^3 with A and A^T")
     ap.add_argument("--tuning", default=None,
-                    help="fsmall,wide,chains: fixed front tile shapes instead of the autotuner's search (for profilers)")
+                    help="fsmall,wide,chains[,streams,steps,subtree]: fixed front tile shapes instead of the "
+                         "autotuner's search (for profilers)")
     ap.add_argument("--amalgamation", default="512,0.25,8",
                     help="max_width,zero_fraction,min_width of the solver's supernode amalgamation (a solver option "
                          "of the reference's; its default is 32,0.25,8). The metric's flops are always those of the "

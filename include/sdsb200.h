@@ -110,12 +110,18 @@ typedef struct sdsb200_plan_options {
  * Cholesky plan (independent subtrees factored concurrently; 0 = 4, 1 = level by level, up to 15);
  * steps (bit 5 of the third field, SDSB200_TUNING_STEPS): 1 = a single-system Cholesky plan runs each
  * batch of its large fronts' 32-column steps as dataflow tasks in one persistent launch, 0 (default) =
- * one launch per step and kernel. */
+ * one launch per step and kernel; subtree (bits 26-29, SDSB200_TUNING_SUBTREE): the fused subtrees
+ * (the reference's regime A: maximal subtrees of shared-memory fronts, each factored by one CTA in
+ * one launch per size class) hold up to 2^subtree fronts of any shared-memory class (1..14), are off
+ * (15), or by default (0) hold up to 16 fronts of at most 64 rows and are used only when they take in
+ * at least 32 fronts per SM (many tiny fronts: batches of small systems).
+ * Bits 30 and 31 must be zero. */
 #define SDSB200_TUNING(fsmall, wide, chains) \
     ((int32_t)(fsmall) | ((int32_t)(wide) << 9) | ((int32_t)(chains) << 20))
 #define SDSB200_TUNING_STREAMS(fsmall, wide, chains, streams) \
     (SDSB200_TUNING(fsmall, wide, chains) | ((int32_t)(streams) << 21))
 #define SDSB200_TUNING_STEPS ((int32_t)1 << 25)
+#define SDSB200_TUNING_SUBTREE(subtree) ((int32_t)(subtree) << 26)
 
 /* The Options fields the numeric and solve phases read (src/options.jl:155-223). */
 typedef struct sdsb200_opts {
@@ -228,7 +234,8 @@ int64_t sdsb200_get_trace(sdsb200_plan* plan, int64_t* h_out, int64_t cap);
 
 /* Plan facts: "ns", "nlevels", "factor_len", "cb_len", "launches_factor", "launches_solve",
  * "launches_done" (kernel launches of the last factor or solve call), "device_bytes", "flops",
- * "schur_n" (order of the Schur complement, 0 without one), "schur_level",
+ * "schur_n" (order of the Schur complement, 0 without one), "schur_level", "subtrees" and
+ * "subtree_fronts" (the fused subtrees and the fronts in them),
  * "solve_status" (synchronizes; nonzero when a bounded wait of the persistent solve gave up);
  * with profiling, "prof_ms:<kind>", "prof_flops:<kind>", "prof_bytes:<kind>", "prof_launches:<kind>"
  * for kinds small assemble panel gemm pivot scale stats fwd bwd diag permute residual inv, and per

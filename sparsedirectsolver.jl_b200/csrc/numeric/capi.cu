@@ -88,6 +88,7 @@ const char* const PROF_NAMES[PK_COUNT] = {"small", "assemble", "panel", "gemm", 
 int prof_kind_of(LaunchKind k) {
     switch (k) {
         case L_SMALL: return PK_SMALL;
+        case L_SUBTREE: return PK_SMALL;
         case L_ASSEMBLE: return PK_ASSEMBLE;
         case L_CHOL_STEP: return PK_PANEL;
         case L_CHOL_FLOW: return PK_PANEL;
@@ -169,7 +170,7 @@ int run_factor(Plan* P, const double* nzval, double eps, double u, int pivot, in
     T* ufactor = static_cast<T*>(P->d_ufactor);
     T* cb = static_cast<T*>(P->d_cb);
     T* work = static_cast<T*>(P->d_work);
-    int last_level = -1;
+    int last_level = -2;   // the fused subtrees' launches are level -1
     const cudaStream_t main_st = st;
     bool on_side = false, any_side = false;
     cudaStream_t last_main = main_st;
@@ -213,10 +214,12 @@ int run_factor(Plan* P, const double* nzval, double eps, double u, int pivot, in
         P->cur_level = L.level;
         prof_begin(P, st);
         switch (L.kind) {
-            case L_SMALL: {
+            case L_SMALL:
+            case L_SUBTREE: {
                 SmallArgs<T> a{};
                 a.maps = P->maps;
-                a.list = P->d_lists + L.list;
+                a.list = P->d_lists + (L.kind == L_SUBTREE ? L.list2 : L.list);
+                a.sub_ptr = L.kind == L_SUBTREE ? P->d_lists + L.list : nullptr;
                 a.members = members;
                 a.nzval = nzval;
                 a.factor = factor; a.ufactor = ufactor; a.cb = cb;
@@ -1053,6 +1056,8 @@ double sdsb200_plan_stat(const sdsb200_plan* plan, const char* name) {
     if (nm == "launches_done") return (double)P->launches_done;
     if (nm == "schur_n") return P->schur_front >= 0 ? (double)P->fronts[P->schur_front].w : 0.0;
     if (nm == "schur_level") return (double)P->schur_level;
+    if (nm == "subtrees") return (double)P->nsubtrees;
+    if (nm == "subtree_fronts") return (double)P->nsubtree_fronts;
     if (nm == "solve_status") {
         int32_t v = 0;
         cudaDeviceSynchronize();

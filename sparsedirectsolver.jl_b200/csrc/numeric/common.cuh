@@ -80,6 +80,7 @@ enum LaunchKind : int32_t {
     L_DFINV,           // diagonal-block inverses of every front for the dataflow solve
     L_PINV,            // GEMM tiles that build the inverse panels of the dataflow solve's tiled fronts
     L_CHOL_FLOW,       // large Cholesky: every 32-column step of a batch as dataflow tasks in one launch
+    L_SUBTREE,         // fused subtrees of small fronts (one CTA per subtree, fronts in postorder)
 };
 
 // One 64 x 64 output tile of the inverse-panel GEMMs: C = A B, or C = -A B (column-major operands).
@@ -96,6 +97,9 @@ struct PinvTile {
 };
 constexpr int PINV_KSPLIT = 256;   // longest inner dimension of one CTA's part
 
+constexpr int SUBTREE_FRONTS_DEFAULT = 16;     // tuning subtree = 0: most fronts of one fused subtree,
+constexpr int SUBTREE_DEFAULT_MAX_ROWS = 64;    // the largest front order in one,
+constexpr int SUBTREE_MIN_FRONTS_PER_SM = 32;   // and the fewest fronts in subtrees per SM to use them
 constexpr int FSTREAM_DEFAULT = 4;   // factorization streams of a single-system Cholesky plan
 constexpr int FSTREAM_MIN_CP = 16;   // the critical path (32-column steps) of a subtree given its own stream
 

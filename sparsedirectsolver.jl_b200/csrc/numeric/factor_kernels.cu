@@ -7,12 +7,13 @@
 // fully-summed columns (Cholesky; Bunch-Kaufman LDLT; threshold-pivoting LU),
 // the Schur update of the contribution block, and the write-out of the panel,
 // D, pivots, statistics and contribution block. It replaces the reference's
-// regime A/B kernels (subtree_cholesky_kernel! src/numeric/subtree.jl:274-316,
-// front_cholesky_kernel! src/numeric/front.jl:154-206, front_ldlt_kernel!
-// src/numeric/ldlt.jl:992-1111, subtree_ldlt_kernel! :1133-1228,
-// front_lu_kernel! src/numeric/lu.jl:264-330, subtree_lu_kernel! :424-493) with
-// one level-batched design; the in-front arithmetic follows the CPU reference
+// regime B kernels (front_cholesky_kernel! src/numeric/front.jl:154-206,
+// front_ldlt_kernel! src/numeric/ldlt.jl:992-1111, front_lu_kernel!
+// src/numeric/lu.jl:264-330); the in-front arithmetic follows the CPU reference
 // (src/reference/*.jl) step by step.
+//
+// subtree_kernel: the same per-front body run by one CTA over a whole leaf
+// subtree of such fronts in postorder (the reference's regime A).
 //
 // assemble_large_kernel: column-owner assembly of the fronts too large for
 // shared memory: one warp per (front, parent index p) builds the column it
@@ -29,11 +30,11 @@
 
 namespace sds {
 
+// One front by the whole CTA, in shared memory (smem_raw holds at least small_front_smem(f)). The CTA's
+// threads all call it; it ends with the front's outputs written to global memory.
 template <typename T, int STRUCT>
-__global__ void __launch_bounds__(256) small_front_kernel(SmallArgs<T> A) {
-    extern __shared__ __align__(16) unsigned char smem_raw[];
-    const int s = A.list[blockIdx.x];
-    const int member = A.members ? A.members[blockIdx.y] : blockIdx.y;
+__device__ __forceinline__ void small_front(const SmallArgs<T>& A, const int s, const int member,
+                                            unsigned char* smem_raw) {
     const DFront fd = A.maps.fronts[s];
     const int f = fd.f, w = fd.w, m = f - w;
     const int ld = f | 1;
@@ -188,6 +189,33 @@ __global__ void __launch_bounds__(256) small_front_kernel(SmallArgs<T> A) {
     }
 }
 
+template <typename T, int STRUCT>
+__global__ void __launch_bounds__(256) small_front_kernel(SmallArgs<T> A) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const int member = A.members ? A.members[blockIdx.y] : blockIdx.y;
+    small_front<T, STRUCT>(A, A.list[blockIdx.x], member, smem_raw);
+}
+
+// Fused subtrees: one CTA factors a whole subtree of shared-memory fronts, front after front in the
+// subtree's postorder (A.list[A.sub_ptr[b] .. A.sub_ptr[b + 1]) for CTA b), in one launch for every
+// subtree of its size class instead of one launch per level. A child's contribution block goes to
+// global memory (the subtree's stack region of the arena, hot in L2) and its parent, later in the same
+// CTA, reads it back after the barrier between the two fronts, which makes the CTA's global writes
+// visible to all its threads. Each front's arithmetic is small_front's, so the factor is bit for bit
+// the level launches'. Replaces the reference's regime-A kernels (subtree_cholesky_kernel!
+// src/numeric/subtree.jl:274-316, subtree_ldlt_kernel! src/numeric/ldlt.jl:1133-1228,
+// subtree_lu_kernel! src/numeric/lu.jl:424-493).
+template <typename T, int STRUCT>
+__global__ void __launch_bounds__(256) subtree_kernel(SmallArgs<T> A) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const int member = A.members ? A.members[blockIdx.y] : blockIdx.y;
+    const int q0 = A.sub_ptr[blockIdx.x], q1 = A.sub_ptr[blockIdx.x + 1];
+    for (int q = q0; q < q1; ++q) {
+        small_front<T, STRUCT>(A, A.list[q], member, smem_raw);
+        __syncthreads();   // the front's shared memory is read out before the next front zeroes it
+    }
+}
+
 size_t small_front_smem(int fmax, int elsize) {
     size_t ld = fmax | 1;
     size_t b = (ld * fmax * elsize + 15) & ~size_t(15);
@@ -202,10 +230,19 @@ cudaError_t launch_small(int structure, const SmallArgs<T>& a, int count, int nm
     size_t smem = small_front_smem(fmax, sizeof(T));
     int threads = fmax <= 48 ? 128 : 256;
     dim3 grid(count, nmembers);
+    const bool sub = a.sub_ptr != nullptr;
     switch (structure) {
-        case STRUCT_SPD: small_front_kernel<T, STRUCT_SPD><<<grid, threads, smem, st>>>(a); break;
-        case STRUCT_S: small_front_kernel<T, STRUCT_S><<<grid, threads, smem, st>>>(a); break;
-        default: small_front_kernel<T, STRUCT_G><<<grid, threads, smem, st>>>(a);
+        case STRUCT_SPD:
+            if (sub) subtree_kernel<T, STRUCT_SPD><<<grid, threads, smem, st>>>(a);
+            else small_front_kernel<T, STRUCT_SPD><<<grid, threads, smem, st>>>(a);
+            break;
+        case STRUCT_S:
+            if (sub) subtree_kernel<T, STRUCT_S><<<grid, threads, smem, st>>>(a);
+            else small_front_kernel<T, STRUCT_S><<<grid, threads, smem, st>>>(a);
+            break;
+        default:
+            if (sub) subtree_kernel<T, STRUCT_G><<<grid, threads, smem, st>>>(a);
+            else small_front_kernel<T, STRUCT_G><<<grid, threads, smem, st>>>(a);
     }
     return cudaGetLastError();
 }
@@ -227,6 +264,12 @@ cudaError_t prepare_factor_kernels(int max_smem) {
     set((const void*)small_front_kernel<float, STRUCT_SPD>);
     set((const void*)small_front_kernel<float, STRUCT_S>);
     set((const void*)small_front_kernel<float, STRUCT_G>);
+    set((const void*)subtree_kernel<double, STRUCT_SPD>);
+    set((const void*)subtree_kernel<double, STRUCT_S>);
+    set((const void*)subtree_kernel<double, STRUCT_G>);
+    set((const void*)subtree_kernel<float, STRUCT_SPD>);
+    set((const void*)subtree_kernel<float, STRUCT_S>);
+    set((const void*)subtree_kernel<float, STRUCT_G>);
     return e;
 }
 

@@ -11,6 +11,8 @@ template <typename T>
 struct SmallArgs {
     DeviceMaps maps;
     const int32_t* list;     // fronts of this launch
+    const int32_t* sub_ptr;  // fused subtrees: subtree b is list[sub_ptr[b] .. sub_ptr[b + 1]) (NULL: one
+                             // front per CTA)
     const int32_t* members;  // active batch members (NULL: 0..nmembers-1)
     const double* nzval;
     T* factor;

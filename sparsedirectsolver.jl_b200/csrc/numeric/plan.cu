@@ -268,7 +268,10 @@ Plan* build_plan(const sdsb200_symbolic* sym, const sdsb200_plan_options* popts,
                                                   : std::vector<int>{32, 64, 96, 128, 160, 224};
         const int tune_fsmall = popts ? (popts->tuning & 0x1FF) : 0;
         const int tune_wide = popts ? ((popts->tuning >> 9) & 0x7FF) : 0;
-        const int tune_rsv = popts ? ((popts->tuning >> 20) & 0x7FF) : 0;
+        const int tune_rsv = popts ? ((popts->tuning >> 20) & 0x3F) : 0;
+        const int tune_sub = popts ? ((popts->tuning >> 26) & 0xF) : 0;
+        if (popts && (popts->tuning >> 30) != 0)
+            throw BuildError(SDSB200_INVALID_VALUE, "tuning: bits 30 and 31 must be zero");
         if (tune_fsmall) {
             if (std::find(classes.begin(), classes.end(), tune_fsmall) == classes.end())
                 throw BuildError(SDSB200_INVALID_VALUE, "tuning: fsmall must be one of the front classes");
@@ -277,9 +280,6 @@ Plan* build_plan(const sdsb200_symbolic* sym, const sdsb200_plan_options* popts,
         if (tune_wide && (tune_wide < 16 || tune_wide > DF_WARP_F))
             throw BuildError(SDSB200_INVALID_VALUE, "tuning: wide (the tallest warp front of the solve) must lie in 16..128");
         const int tune_chains = tune_rsv & 1, tune_streams = (tune_rsv >> 1) & 15, tune_steps = (tune_rsv >> 5) & 1;
-        if (tune_rsv > 63)
-            throw BuildError(SDSB200_INVALID_VALUE,
-                             "tuning: the third field is chains (bit 0) | streams << 1 (streams < 16) | steps << 5");
         const int warp_f = tune_wide ? tune_wide : DF_WARP_F;
         const bool pinv_mode = tune_chains == 0;   // tiled fronts solved through inverse panels
         P->fsmall_max = classes.back();
@@ -320,17 +320,131 @@ Plan* build_plan(const sdsb200_symbolic* sym, const sdsb200_plan_options* popts,
             }
         }
 
-        // contribution blocks on one arena per stream, by lifetime [level, parent level]: a stream's
-        // launches run level by level, and the only fronts whose parent is on another stream are the
-        // tops of their streams' subtrees (nothing on their stream comes after them)
+        // Fused subtrees (the reference's regime A, src/symbolic/schedule.jl:331-345): the maximal
+        // subtrees of shared-memory fronts, on one factorization stream, with at most `maxfronts` fronts
+        // and at most 1/SMs of the flops, so that a subtree's serial chain stays short and the subtrees
+        // fill the device. One CTA factors each, front after front in a postorder whose children come
+        // by decreasing (stack peak - contribution block) (Liu's order, as the reference's), so that the
+        // subtree's stack of contribution blocks stays small; they are launched before the stream's
+        // first level. tuning subtree: 15 = off; 1..14: subtrees of up to 2^subtree fronts of any
+        // shared-memory class; 0 (default): up to SUBTREE_FRONTS_DEFAULT fronts of at most 64 rows, and
+        // only when they hold at least SUBTREE_MIN_FRONTS_PER_SM fronts per SM. A subtree runs its
+        // fronts one after another, so it pays where the bottom levels are throughput-bound (far more
+        // tiny fronts than resident CTAs: batches of small systems), and costs where a level's launch
+        // is latency-bound (measured on lap3d 48^3 and lap2d 64^2).
+        std::vector<int> sub_of(ns, -1);
+        struct Sub { int root, stream, cls; int64_t stack; std::vector<int> order; std::vector<int64_t> off; };
+        std::vector<Sub> subs;
+        if (tune_sub != 15 && ns > 0) {
+            const int64_t maxfronts = tune_sub ? (int64_t(1) << tune_sub) : SUBTREE_FRONTS_DEFAULT;
+            const int fcap = tune_sub ? (1 << 30) : SUBTREE_DEFAULT_MAX_ROWS;
+            int dev0 = 0, sms0 = 148;
+            cudaGetDevice(&dev0);
+            cudaDeviceGetAttribute(&sms0, cudaDevAttrMultiProcessorCount, dev0);
+            std::vector<double> work(ns, 0.0);
+            double total = 0;
+            for (int64_t s = 0; s < ns; ++s) {
+                const double f = P->fronts[s].f;
+                for (int k = 0; k < P->fronts[s].w; ++k) work[s] += (f - k) * (f - k);
+                total += work[s];
+            }
+            std::vector<int64_t> nfr(ns, 1), peak(ns, 0), cbsz(ns, 0);
+            std::vector<char> elig(ns, 0);
+            std::vector<std::vector<int>> kids(ns);
+            for (int64_t s = 0; s < ns; ++s) {
+                const DFront& F = P->fronts[s];
+                const int64_t m = F.f - F.w;
+                cbsz[s] = (F.parent >= 0 && m > 0) ? ((m * m + 31) & ~int64_t(31)) : 0;
+                bool e = s != P->schur_front && class_of(F.f) != 0 && F.f <= fcap;
+                for (int q = F.ch_begin; q < F.ch_end; ++q) {
+                    const int c = (int)(child_list[q] - 1);
+                    kids[s].push_back(c);
+                    e = e && elig[c] && fstream[c] == fstream[s];
+                    nfr[s] += nfr[c];
+                    work[s] += work[c];
+                }
+                // stack peak of the subtree below s (its own contribution block not counted)
+                std::stable_sort(kids[s].begin(), kids[s].end(), [&](int a, int b) {
+                    return std::max(peak[a], cbsz[a]) - cbsz[a] > std::max(peak[b], cbsz[b]) - cbsz[b];
+                });
+                int64_t acc = 0, pk = 0;
+                for (int c : kids[s]) {
+                    pk = std::max(pk, acc + std::max(peak[c], cbsz[c]));
+                    acc += cbsz[c];
+                }
+                peak[s] = pk;
+                elig[s] = e && nfr[s] <= maxfronts && work[s] <= total / std::max(sms0, 1);
+            }
+            for (int64_t s = 0; s < ns; ++s) {
+                const DFront& F = P->fronts[s];
+                if (!elig[s] || (F.parent >= 0 && elig[F.parent])) continue;
+                Sub t;
+                t.root = (int)s;
+                t.stream = fstream[s];
+                t.cls = 0;
+                t.stack = 0;
+                // postorder, children in the sorted order; stack offsets of the contribution blocks:
+                // a front's children's blocks lie on top of the stack when it runs, and its own block
+                // (written after it has read theirs) replaces them from the first one's offset
+                int64_t top = 0;
+                std::vector<std::pair<int, size_t>> st2{{(int)s, 0}};
+                std::vector<int64_t> base{0};
+                while (!st2.empty()) {
+                    auto& fr = st2.back();
+                    const int x = fr.first;
+                    if (fr.second < kids[x].size()) {
+                        const int c = kids[x][fr.second++];
+                        st2.push_back({c, 0});
+                        base.push_back(top);
+                        continue;
+                    }
+                    top = base.back();
+                    st2.pop_back();
+                    base.pop_back();
+                    sub_of[x] = (int)subs.size();
+                    t.order.push_back(x);
+                    t.cls = std::max(t.cls, class_of(P->fronts[x].f));
+                    if (x != (int)s && cbsz[x] > 0) {
+                        t.off.push_back(top);
+                        top += cbsz[x];
+                        t.stack = std::max(t.stack, top);
+                    } else {
+                        t.off.push_back(-1);
+                    }
+                }
+                P->nsubtree_fronts += (int64_t)t.order.size();
+                subs.push_back(std::move(t));
+            }
+            if (!tune_sub && P->nsubtree_fronts < (int64_t)SUBTREE_MIN_FRONTS_PER_SM * sms0) {
+                subs.clear();
+                std::fill(sub_of.begin(), sub_of.end(), -1);
+                P->nsubtree_fronts = 0;
+            }
+            P->nsubtrees = (int64_t)subs.size();
+        }
+
+        // contribution blocks on one arena per stream, by lifetime [start, end] in the stream's launch
+        // order: 0 for its fused subtrees, L + 1 for its level L. A stream's launches run in that order,
+        // and the only fronts whose parent is on another stream are the tops of their streams' subtrees
+        // (nothing on their stream comes after them). A fused subtree's inner blocks live on its stack
+        // region (lifetime [0, 0]); its root's block lives until the root's parent's level.
         {
             std::vector<Arena> arenas(P->nfstreams);
+            auto t_of = [&](int s) { return sub_of[s] >= 0 ? 0 : P->fronts[s].level + 1; };
+            for (Sub& t : subs) {
+                const int64_t region = t.stack > 0 ? arenas[t.stream].place(t.stack, 0, 0) : 0;
+                for (size_t q = 0; q < t.order.size(); ++q)
+                    if (t.off[q] >= 0) P->fronts[t.order[q]].cb = region + t.off[q];
+                DFront& R = P->fronts[t.root];
+                const int64_t m = R.f - R.w;
+                if (R.parent >= 0 && m > 0) R.cb = arenas[t.stream].place(m * m, 0, t_of(R.parent));
+            }
             for (int L = 0; L < P->nlevels; ++L)
                 for (int s : P->level_fronts[L]) {
                     DFront& F = P->fronts[s];
                     int64_t m = F.f - F.w;
-                    if (F.parent < 0 || m == 0) continue;
-                    F.cb = arenas[fstream[s]].place(m * m, F.level, P->fronts[F.parent].level);
+                    if (F.parent < 0 || m == 0 || sub_of[s] >= 0) continue;
+                    F.cb = arenas[fstream[s]].place(m * m, L + 1, t_of(F.parent));
                 }
             int64_t base = 0;
             for (int g = 0; g < P->nfstreams; ++g) {
@@ -423,12 +537,54 @@ Plan* build_plan(const sdsb200_symbolic* sym, const sdsb200_plan_options* popts,
         // single-system Cholesky plans with tuning steps = 1: a batch's steps as one dataflow launch
         // (default: one launch per step and kernel, measured faster on lap3d 48^3)
         const bool flow_mode = P->nbatch == 1 && tune_steps == 1;
+        // each stream's fused subtrees first, one launch per size class (a batch of level -1): per
+        // launch the subtrees' starts (count + 1 entries, relative to the fronts) and then the fronts
+        for (int sg = 0; sg < P->nfstreams; ++sg) {
+            std::map<int, std::vector<int>> bycls;
+            for (size_t t = 0; t < subs.size(); ++t)
+                if (subs[t].stream == sg) bycls[subs[t].cls].push_back((int)t);
+            if (bycls.empty()) continue;
+            const size_t first = P->prog.size();
+            for (auto& kv : bycls) {
+                ProgLaunch pl{};
+                pl.kind = L_SUBTREE; pl.level = -1; pl.cls = kv.first; pl.fstream = sg;
+                pl.count = (int)kv.second.size();
+                pl.list = (int64_t)lists.size();
+                pl.list2 = pl.list + pl.count + 1;
+                int32_t at = 0;
+                for (int t : kv.second) {
+                    lists.push_back(at);
+                    at += (int32_t)subs[t].order.size();
+                }
+                lists.push_back(at);
+                double tri = (P->structure == STRUCT_G) ? 1.0 : 0.5;
+                for (int t : kv.second)
+                    for (int s : subs[t].order) {
+                        lists.push_back(s);
+                        const DFront& F = P->fronts[s];
+                        double f = F.f, w = F.w, m = F.f - F.w;
+                        for (int k = 0; k < F.w; ++k) pl.flops += (f - k) * (f - k);
+                        pl.bytes += P->elsize * (f * w * (gen ? 2 : 1) + (F.cb >= 0 ? tri * m * m : 0.0));
+                        pl.bytes += 12.0 * (F.am_end - F.am_begin);
+                        for (int q = F.ch_begin; q < F.ch_end; ++q) {
+                            const DFront& C = P->fronts[child_list[q] - 1];
+                            double mc = C.f - C.w;
+                            pl.bytes += P->elsize * tri * mc * mc + 4.0 * mc;
+                        }
+                    }
+                P->prog.push_back(pl);
+            }
+            for (size_t t = 0; t < subs.size(); ++t)
+                if (subs[t].stream == sg)
+                    for (int s : subs[t].order) batch_of[s] = (int)batches.size();
+            batches.push_back({-1, sg, first, P->prog.size() - 1});
+        }
         for (int L = 0; L < P->nlevels; ++L)
           for (int sg = 0; sg < P->nfstreams; ++sg) {
             std::map<int, std::vector<int>> small;
             std::vector<int> large;
             for (int s : P->level_fronts[L]) {
-                if (fstream[s] != sg) continue;
+                if (fstream[s] != sg || sub_of[s] >= 0) continue;
                 int c = s == P->schur_front ? 0 : class_of(P->fronts[s].f);
                 if (c) small[c].push_back(s);
                 else large.push_back(s);
@@ -963,8 +1119,19 @@ Plan* build_plan(const sdsb200_symbolic* sym, const sdsb200_plan_options* popts,
                 std::vector<PinvTile> pt;
                 auto bw_of = [](int w, int b) { return std::min(DF_BLK, w - DF_BLK * b); };
                 int64_t pwork = 0;
-                for (int L = 0; L < P->nlevels; ++L)
+                // batch "level" -1: the stream's fused subtrees
+                for (int L = -1; L < P->nlevels; ++L)
                   for (int sg = 0; sg < P->nfstreams; ++sg) {
+                    std::vector<int> lf;
+                    if (L < 0) {
+                        for (int L2 = 0; L2 < P->nlevels; ++L2)
+                            for (int s : P->level_fronts[L2])
+                                if (sub_of[s] >= 0) lf.push_back(s);
+                    } else {
+                        for (int s : P->level_fronts[L])
+                            if (sub_of[s] < 0) lf.push_back(s);
+                    }
+                    if (lf.empty()) continue;
                     std::vector<ProgLaunch>& side_b = side[{L, sg}];
                     std::vector<int> pf;   // the batch's inverse-panel fronts
                     ProgLaunch il_{};
@@ -973,7 +1140,7 @@ Plan* build_plan(const sdsb200_symbolic* sym, const sdsb200_plan_options* popts,
                     il_.side = 1;
                     il_.list = (int64_t)small_sorted.size();
                     il_.list2 = (int64_t)blk_sorted.size() / 2;
-                    for (int s : P->level_fronts[L]) {
+                    for (int s : lf) {
                         if (s == P->schur_front || fstream[s] != sg) continue;
                         if (!df[s].tiled) {
                             small_sorted.push_back(s);

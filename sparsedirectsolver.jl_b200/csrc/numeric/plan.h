@@ -177,6 +177,7 @@ struct Plan {
     cudaStream_t side = nullptr;         // low-priority stream of the side launches of the factorization
     cudaEvent_t side_fork = nullptr, side_join = nullptr;
     int nfstreams = 1;                   // factorization streams (stream 0 is the caller's / capture stream)
+    int64_t nsubtrees = 0, nsubtree_fronts = 0;   // fused subtrees and the fronts in them
     std::vector<cudaStream_t> fstreams;  // streams 1 .. nfstreams - 1
     std::vector<cudaEvent_t> fevents;    // the cross-stream events of the factorization
     int nfevents = 0;

@@ -436,3 +436,49 @@ def test_user_host_interrupt(torch_cuda):
     flag.value = 0
     x = ds.execute("solve", None, b).cpu().numpy()
     assert M.scaled_backward_error(A, x, b) <= BERR
+
+
+@pytest.mark.parametrize("structure,precision", [("SPD", "fp64"), ("SPD", "fp32"), ("S", "fp64"), ("S", "fp32"),
+                                                 ("G", "fp64")])
+def test_fused_subtrees_match_level_launches(torch_cuda, structure, precision):
+    # fused subtrees (one CTA factors a whole subtree of shared-memory fronts in postorder; at most 16
+    # fronts each, and at most 4) against one launch per level and size class (tuning subtree = 15): the
+    # same panels, pivots, kinds, D and statistics bit for bit; the oracle's pivots and statistics in
+    # FP64, and its inertia in FP32. The default (subtree = 0) leaves these small trees level by level.
+    from sdsb200.capi import tuning
+
+    A, reordering = {"SPD": lambda: (M.lap2d_shifted(40, 40, seed=3), "amd"),
+                     "S": lambda: (small_kkt(30, 30, 400, seed=2), "nd"),
+                     "G": lambda: (M.convection_diffusion3d(12, 12, 12, seed=6), "nd")}[structure]()
+    S, O, info = oracle_for(A, structure, reordering=reordering)
+    out = {}
+    for sub in (15, 4, 2, 0):
+        ir = {} if precision == "fp64" else dict(ir_n_steps=10, ir_tol=1e-14)
+        ds = _solver(A, structure, reordering_alg=reordering, max_nrhs=1, factor_precision=precision,
+                     tuning=tuning(subtree=sub), **ir)
+        ds.execute("analysis")
+        assert ds.execute("factorization") == info
+        fac, ufac = ds.factor_host()
+        piv, kind, d = ds.pivots_host()
+        out[sub] = dict(fac=fac, ufac=ufac, piv=piv, kind=kind, d=d, st=ds.stats_host(),
+                        nsub=ds.plan_stat("subtrees"), nfr=ds.plan_stat("subtree_fronts"))
+        b = M.rhs(A.shape[0], 1, seed=7)
+        x = ds.execute("solve", None, b[:, 0]).cpu().numpy()
+        assert M.scaled_backward_error(A, x.reshape(-1, 1), b) <= BERR
+    assert out[15]["nsub"] == 0 and out[0]["nsub"] == 0
+    assert out[4]["nsub"] > 0 and out[2]["nsub"] > out[4]["nsub"]
+    assert out[4]["nfr"] > out[4]["nsub"]   # subtrees of several fronts
+    for sub in (4, 2, 0):
+        for k in ("fac", "piv", "kind", "d", "st"):
+            assert np.array_equal(out[sub][k], out[15][k]), (sub, k)
+        if structure == "G":
+            assert np.array_equal(out[sub]["ufac"], out[15]["ufac"])
+    n = S.n
+    if precision == "fp64":
+        assert rel_max_diff(dense_panels(S, out[4]["fac"]), dense_panels(S, O.factor)) <= FP64_TOL
+        assert np.array_equal(out[4]["st"], O.stats_matrix())
+        if structure != "SPD":
+            assert np.array_equal(out[4]["piv"][:n], O.piv[:n])
+            assert np.array_equal(out[4]["kind"][:n], O.kind[:n])
+    else:
+        assert np.array_equal(out[4]["st"][:, :2].sum(0), O.stats_matrix()[:, :2].sum(0))
