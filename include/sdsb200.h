@@ -239,8 +239,9 @@ int64_t sdsb200_get_trace(sdsb200_plan* plan, int64_t* h_out, int64_t cap);
  * "solve_status" (synchronizes; nonzero when a bounded wait of the persistent solve gave up);
  * with profiling, "prof_ms:<kind>", "prof_flops:<kind>", "prof_bytes:<kind>", "prof_launches:<kind>"
  * for kinds small assemble panel gemm pivot scale stats fwd bwd diag permute residual inv, and per
- * launch of the last calls "prof_records" (their count), "prof_record:<i>:kind|level|ms|start" (start:
- * ms after the call's first launch began; kind: the index of the kind in that list).
+ * launch of the last calls "prof_records" (their count), "prof_record:<i>:kind|level|ms|start|flops"
+ * (start: ms after the call's first launch began; kind: the index of the kind in that list; flops: the
+ * launch's algorithmic flops).
  * Returns -1 for an unknown name. */
 double sdsb200_plan_stat(const sdsb200_plan* plan, const char* name);
 

@@ -71,7 +71,8 @@ void prof_resolve(Plan* P) {
         cudaEventElapsedTime(&ms, P->events[2 * q], P->events[2 * q + 1]);
         cudaEventElapsedTime(&at, P->events[0], P->events[2 * q]);
         ProfAcc& a = P->prof[P->pending[q].first];
-        P->records.push_back({P->pending[q].first, P->pending_level[q], (double)ms, (double)at});
+        P->records.push_back({P->pending[q].first, P->pending_level[q], (double)ms, (double)at,
+                              P->pending[q].second.first});
         a.ms += ms;
         a.flops += P->pending[q].second.first;
         a.bytes += P->pending[q].second.second;
@@ -1066,7 +1067,7 @@ double sdsb200_plan_stat(const sdsb200_plan* plan, const char* name) {
     }
     if (nm == "prof_records") return (double)P->records.size();
     if (nm.rfind("prof_record:", 0) == 0) {
-        // "prof_record:<i>:kind|level|ms|start" (start: ms after the phase's first launch began)
+        // "prof_record:<i>:kind|level|ms|start|flops" (start: ms after the phase's first launch began)
         size_t a = nm.find(':', 12);
         if (a == std::string::npos) return -1;
         size_t i = (size_t)atol(nm.substr(12, a - 12).c_str());
@@ -1076,6 +1077,7 @@ double sdsb200_plan_stat(const sdsb200_plan* plan, const char* name) {
         if (f == "level") return P->records[i].level;
         if (f == "ms") return P->records[i].ms;
         if (f == "start") return P->records[i].start;
+        if (f == "flops") return P->records[i].flops;
         return -1;
     }
     for (int k = 0; k < PK_COUNT; ++k) {

@@ -309,5 +309,6 @@ template <typename I>
 cudaError_t launch_sampled_outer(const OuterArgs<I>& a, int nmembers, cudaStream_t st);
 
 constexpr int GEMM_BM = 64, GEMM_BN = 64;
+constexpr int GEMM_BM_TC = 128;   // rows of a tcgen05 contribution-block tile (FP32 plans)
 
 }  // namespace sds

@@ -501,14 +501,17 @@ Plan* build_plan(const sdsb200_symbolic* sym, const sdsb200_plan_options* popts,
         std::vector<ColTask> coltasks;
         std::vector<GemmTile> tiles;
         std::vector<int64_t> scr_off, woff;
+        // tiles of the contribution-block updates: 128 rows in FP32 (the full M of a tcgen05 MMA), 64 in
+        // FP64 (the DMMA kernel's tile)
+        const int cb_bm = P->elsize == 4 ? GEMM_BM_TC : GEMM_BM;
         auto add_gemm_tiles = [&](int64_t a, int lda, int64_t b, int ldb, int64_t c, int ldc, int M, int N, int K,
-                                  bool lower, int front) -> double {
+                                  bool lower, int front, int bm = GEMM_BM) -> double {
             // algorithmic flops: 2 K per entry of C that is written (the lower trapezoid for SYRK-like updates)
             double entries = 0;
             for (int j = 0; j < N; ++j) entries += lower ? std::max(0, M - j) : M;
-            for (int ti = 0; ti < M; ti += GEMM_BM)
+            for (int ti = 0; ti < M; ti += bm)
                 for (int tj = 0; tj < N; tj += GEMM_BN) {
-                    int mm = std::min(GEMM_BM, M - ti), nn = std::min(GEMM_BN, N - tj);
+                    int mm = std::min(bm, M - ti), nn = std::min(GEMM_BN, N - tj);
                     if (lower && ti + mm - 1 < tj) continue;
                     GemmTile t;
                     t.a = a + ti;
@@ -749,7 +752,7 @@ Plan* build_plan(const sdsb200_symbolic* sym, const sdsb200_plan_options* popts,
                     const DFront& F = P->fronts[s];
                     int m = F.f - F.w;
                     if (F.cb < 0 || m == 0) continue;
-                    cl.flops += add_gemm_tiles(F.panel + F.w, F.f, F.panel + F.w, F.f, F.cb, m, m, m, F.w, true, s);
+                    cl.flops += add_gemm_tiles(F.panel + F.w, F.f, F.panel + F.w, F.f, F.cb, m, m, m, F.w, true, s, cb_bm);
                 }
                 cl.count = (int)(tiles.size() - cl.list);
                 if (cl.count) P->prog.push_back(cl);
@@ -826,7 +829,7 @@ Plan* build_plan(const sdsb200_symbolic* sym, const sdsb200_plan_options* popts,
                     const DFront& F = P->fronts[s];
                     int m = F.f - F.w;
                     if (F.cb < 0 || m == 0) continue;
-                    cl.flops += add_gemm_tiles(F.panel + F.w, F.f, F.panel + F.w, F.f, F.cb, m, m, m, F.w, true, s);
+                    cl.flops += add_gemm_tiles(F.panel + F.w, F.f, F.panel + F.w, F.f, F.cb, m, m, m, F.w, true, s, cb_bm);
                 }
                 cl.count = (int)(tiles.size() - cl.list);
                 if (cl.count) P->prog.push_back(cl);
@@ -875,7 +878,7 @@ Plan* build_plan(const sdsb200_symbolic* sym, const sdsb200_plan_options* popts,
                         int m = F.f - F.w;
                         lists.push_back(s);
                         woff.push_back(wo);
-                        gl.flops += add_gemm_tiles(wo, m, F.panel + F.w, F.f, F.cb, m, m, m, F.w, !gen, s);
+                        gl.flops += add_gemm_tiles(wo, m, F.panel + F.w, F.f, F.cb, m, m, m, F.w, !gen, s, cb_bm);
                         wo += ((int64_t)m * F.w + 31) & ~int64_t(31);
                         maxw = std::max(maxw, F.w);
                     }

@@ -191,7 +191,7 @@ struct Plan {
     size_t prof_next = 0;
     std::vector<std::pair<int, std::pair<double, double>>> pending;  // kind, (flops, bytes) per event pair
     std::vector<int> pending_level;
-    struct LaunchRecord { int kind, level; double ms, start; };
+    struct LaunchRecord { int kind, level; double ms, start, flops; };
     std::vector<LaunchRecord> records;   // every profiled launch of the last calls
     int cur_level = -1;
 };

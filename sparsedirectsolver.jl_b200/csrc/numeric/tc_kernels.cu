@@ -1,21 +1,25 @@
 // FP32 Schur updates on the fifth-generation tensor cores (tcgen05, accumulator in tensor memory).
 //
-// The FP32 form's grouped GEMM C -= A B^T (or C = A B^T in place, the trsm by an inverse) over the
-// plan's 64 x 64 tiles, as 3xTF32: each operand is split into a TF32 high part and a TF32 low part
-// (x = hi + lo, both rounded to nearest by cvt.rna.tf32.f32), and
+// The FP32 form's grouped GEMM C -= A B^T over the plan's tiles of the contribution-block updates
+// (128 x 64; tiles of 64 rows run with the other 64 operand rows zero), as 3xTF32: each operand is
+// split into a TF32 high part and a TF32 low part (x = hi + lo, both rounded to nearest by
+// cvt.rna.tf32.f32), and
 //     A B^T ~ A_lo B_hi^T + A_hi B_lo^T + A_hi B_hi^T,
 // accumulated in FP32 in tensor memory. The dropped A_lo B_lo^T term is below FP32 rounding, so the
 // result has FP32 accuracy at tensor-core rates.
 //
 // One CTA (4 warps) per tile:
-// * thread 0 issues tcgen05.mma (M = 128, N = 64, K = 8 per instruction; rows 64..127 of the A
-//   operand are zero, so the tile's 64 rows land in TMEM lanes 0..63);
-// * the operands are staged by all threads into shared memory in the K-major, no-swizzle
-//   canonical layout: 16-byte core-matrix rows, 8-row groups 128 bytes apart (SBO), K chunks of 4
-//   elements ROWS * 16 bytes apart (LBO);
-// * tcgen05.commit signals an mbarrier when the MMAs of a stage are done (the wait is bounded: on
-//   time-out the CTA records a status and returns after releasing its tensor memory);
-// * warps 0 and 1 read the accumulator back with tcgen05.ld (32 lanes x 32 bit, 16 columns per
+// * thread 0 issues tcgen05.mma (M = 128, N = 64, K = 8 per instruction) into 64 TMEM columns;
+// * all threads stage the operands, 32 columns of the inner dimension at a time, through registers
+//   into shared memory in the K-major, no-swizzle canonical layout (16-byte core-matrix rows, 8-row
+//   groups 128 bytes apart (SBO), K chunks of 4 elements ROWS * 16 bytes apart (LBO)), splitting
+//   them into hi and lo on the way. Two buffers: the next stage's global loads are in flight while
+//   the tensor cores run the current one. The operands are the reference's column-major panels and
+//   contribution blocks (leading dimension f or m, any value), whose columns need not start on the
+//   16-byte boundary that a TMA tensor map requires, and the split needs a register pass anyway;
+// * tcgen05.commit signals one mbarrier per buffer when the MMAs that read it are done (every wait is
+//   bounded: on time-out the CTA records a status and returns after releasing its tensor memory);
+// * the four warps read the accumulator back with tcgen05.ld (32 lanes x 32 bit, 16 columns per
 //   instruction) and apply the epilogue of the tile.
 #include <cuda_runtime.h>
 #include <stdint.h>
@@ -32,8 +36,10 @@ constexpr int TC_MROWS = 128, TC_NROWS = 64;    // MMA shape M x N
 constexpr int TC_CHUNKS = TC_BK / 4;            // 16-byte K chunks per row and stage
 constexpr int TC_A_BYTES = TC_CHUNKS * TC_MROWS * 16;   // 16 KB per A part
 constexpr int TC_B_BYTES = TC_CHUNKS * TC_NROWS * 16;   // 8 KB per B part
+constexpr int TC_STAGE = 2 * TC_A_BYTES + 2 * TC_B_BYTES;   // one buffer: A and B, hi and lo parts
+constexpr int TC_NBUF = 2;                      // operand buffers (the pipeline depth)
 constexpr int TC_TMEM_COLS = 64;
-constexpr int TC_HEADER = 64;                   // mbarrier (8 B) + TMEM address (4 B), padded
+constexpr int TC_HEADER = 64;                   // mbarriers (2 x 8 B) + TMEM address (4 B), padded
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
 
@@ -66,44 +72,16 @@ __device__ __forceinline__ void mma_tf32(uint32_t tmem, uint64_t adesc, uint64_t
         : "r"(tmem), "l"(adesc), "l"(bdesc), "r"(TC_IDESC), "r"(acc));
 }
 
-// stage one operand tile: rows r < rows_valid of X (column-major, ld ldx), columns k0 .. k0 + TC_BK
-// of the inner dimension (< K), split into TF32 hi and lo parts in the canonical layout
-template <int ROWS>
-__device__ __forceinline__ void stage(const float* X, int64_t ldx, int rows_valid, int k0, int K, uint8_t* hi,
-                                      uint8_t* lo) {
-    for (int q = threadIdx.x; q < 64 * TC_CHUNKS; q += blockDim.x) {
-        const int r = q % 64, c = q / 64;
-        float v[4];
-#pragma unroll
-        for (int j = 0; j < 4; ++j) {
-            const int k = k0 + 4 * c + j;
-            v[j] = (r < rows_valid && k < K) ? X[r + (int64_t)k * ldx] : 0.0f;
-        }
-        uint4 h, l;
-        uint32_t* hp = &h.x;
-        uint32_t* lp = &l.x;
-#pragma unroll
-        for (int j = 0; j < 4; ++j) {
-            const uint32_t hb = to_tf32(v[j]);
-            hp[j] = hb;
-            lp[j] = to_tf32(v[j] - __uint_as_float(hb));
-        }
-        const int off = (c * ROWS + r) * 16;
-        *reinterpret_cast<uint4*>(hi + off) = h;
-        *reinterpret_cast<uint4*>(lo + off) = l;
-    }
-}
-
 }  // namespace
 
+// Register-staged operand pipeline (two shared-memory buffers): stage s + 1's global loads are in
+// flight while the tensor cores run stage s, and a buffer is refilled only after the MMAs that read it
+// have committed (one mbarrier per buffer, phase = the buffer's use count). The tile is a full
+// 128 x 64 (M = 128 lanes of TMEM), so no half of an MMA is padding.
 __global__ void __launch_bounds__(128) gemm_nt_tc32_kernel(GemmArgs<float> A) {
     extern __shared__ __align__(1024) uint8_t tsm[];
-    uint8_t* a_hi = tsm;
-    uint8_t* a_lo = a_hi + TC_A_BYTES;
-    uint8_t* b_hi = a_lo + TC_A_BYTES;
-    uint8_t* b_lo = b_hi + TC_B_BYTES;
-    uint64_t* mbar = reinterpret_cast<uint64_t*>(b_lo + TC_B_BYTES);
-    uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(b_lo + TC_B_BYTES + 8);
+    uint64_t* mbar = reinterpret_cast<uint64_t*>(tsm + TC_NBUF * TC_STAGE);   // one per buffer
+    uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(tsm + TC_NBUF * TC_STAGE + 16);
 
     const GemmTile t = A.tiles[blockIdx.x];
     const int member = A.members ? A.members[blockIdx.y] : blockIdx.y;
@@ -120,12 +98,6 @@ __global__ void __launch_bounds__(128) gemm_nt_tc32_kernel(GemmArgs<float> A) {
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const int M = t.m, N = t.n, K = t.k;
 
-    // rows 64..127 of the A operand stay zero
-    for (int q = tid; q < TC_CHUNKS * 64; q += blockDim.x) {
-        const int r = 64 + q % 64, c = q / 64;
-        *reinterpret_cast<uint4*>(a_hi + (c * TC_MROWS + r) * 16) = make_uint4(0, 0, 0, 0);
-        *reinterpret_cast<uint4*>(a_lo + (c * TC_MROWS + r) * 16) = make_uint4(0, 0, 0, 0);
-    }
     if (warp == 0) {
         asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tmem_slot)),
                      "r"(TC_TMEM_COLS));
@@ -133,6 +105,7 @@ __global__ void __launch_bounds__(128) gemm_nt_tc32_kernel(GemmArgs<float> A) {
     }
     if (tid == 0) {
         asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(mbar)));
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(mbar + 1)));
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
     asm volatile("tcgen05.fence::before_thread_sync;");
@@ -140,19 +113,80 @@ __global__ void __launch_bounds__(128) gemm_nt_tc32_kernel(GemmArgs<float> A) {
     asm volatile("tcgen05.fence::after_thread_sync;");
     const uint32_t tmem = *tmem_slot;
 
+    // staging registers: A row `tid`, the stage's 32 columns of the inner dimension; B row tid % 64,
+    // 16 of them (the half tid / 64). Each load instruction of a warp reads 32 consecutive rows.
+    float ra[TC_BK], rb[TC_BK / 2];
+    const int rB = tid & (TC_NROWS - 1), kB = (tid / TC_NROWS) * (TC_BK / 2);
+    auto load = [&](int k0) {
+#pragma unroll
+        for (int j = 0; j < TC_BK; ++j) {
+            const int k = k0 + j;
+            ra[j] = (tid < M && k < K) ? Ab[tid + (int64_t)k * t.lda] : 0.0f;
+        }
+#pragma unroll
+        for (int j = 0; j < TC_BK / 2; ++j) {
+            const int k = k0 + kB + j;
+            rb[j] = (rB < N && k < K) ? Bb[rB + (int64_t)k * t.ldb] : 0.0f;
+        }
+    };
+    // split into TF32 hi and lo parts, in the K-major no-swizzle canonical layout (16-byte chunk c of
+    // row r at (c ROWS + r) 16)
+    auto put4 = [&](const float* v, uint8_t* hi, uint8_t* lo, int off) {
+        uint4 h, l;
+        uint32_t* hp = &h.x;
+        uint32_t* lp = &l.x;
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+            const uint32_t hb = to_tf32(v[j]);
+            hp[j] = hb;
+            lp[j] = to_tf32(v[j] - __uint_as_float(hb));
+        }
+        *reinterpret_cast<uint4*>(hi + off) = h;
+        *reinterpret_cast<uint4*>(lo + off) = l;
+    };
+    auto store = [&](int buf) {
+        uint8_t* a_hi = tsm + buf * TC_STAGE;
+        uint8_t* a_lo = a_hi + TC_A_BYTES;
+        uint8_t* b_hi = a_lo + TC_A_BYTES;
+        uint8_t* b_lo = b_hi + TC_B_BYTES;
+#pragma unroll
+        for (int c = 0; c < TC_CHUNKS; ++c) put4(ra + 4 * c, a_hi, a_lo, (c * TC_MROWS + tid) * 16);
+#pragma unroll
+        for (int c = 0; c < TC_CHUNKS / 2; ++c)
+            put4(rb + 4 * c, b_hi, b_lo, ((kB / 4 + c) * TC_NROWS + rB) * 16);
+    };
+    // bounded wait (about two seconds of polls) for the commit of a buffer's use `use`
+    auto wait_buf = [&](int buf, int use) -> bool {
+        uint32_t done = 0;
+        for (long spins = 0; !done && spins < (1L << 24); ++spins)
+            asm volatile(
+                "{\n\t.reg .pred p;\n\t"
+                "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+                "selp.b32 %0, 1, 0, p;\n\t}\n"
+                : "=r"(done)
+                : "r"(smem_u32(mbar + buf)), "r"((uint32_t)(use & 1))
+                : "memory");
+        return done != 0;
+    };
+
     bool ok = true;
-    uint32_t phase = 0;
+    int last = -1;   // the last stage whose MMAs were committed
     const int nst = (K + TC_BK - 1) / TC_BK;
-    for (int st = 0; st < nst && ok; ++st) {
-        const int k0 = st * TC_BK;
-        stage<TC_MROWS>(Ab, t.lda, M, k0, K, a_hi, a_lo);
-        stage<TC_NROWS>(Bb, t.ldb, N, k0, K, b_hi, b_lo);
+    load(0);
+    for (int st = 0; st < nst; ++st) {
+        const int buf = st & 1;
+        bool mine = true;
+        if (st >= TC_NBUF) mine = wait_buf(buf, (st - TC_NBUF) >> 1);   // the MMAs that read this buffer
+        if (mine) store(buf);
         // the generic-proxy stores must be visible to the tensor cores (async proxy)
         asm volatile("fence.proxy.async.shared::cta;");
-        __syncthreads();
+        ok = __syncthreads_and(mine) != 0;   // one verdict for the whole CTA
+        if (!ok) break;
         if (tid == 0) {
             asm volatile("tcgen05.fence::after_thread_sync;");
-            const uint32_t ah = smem_u32(a_hi), al = smem_u32(a_lo), bh = smem_u32(b_hi), bl = smem_u32(b_lo);
+            const uint32_t ah = smem_u32(tsm + buf * TC_STAGE), al = ah + TC_A_BYTES, bh = al + TC_A_BYTES,
+                           bl = bh + TC_B_BYTES;
+#pragma unroll
             for (int s = 0; s < TC_BK / 8; ++s) {
                 const uint32_t ao = 2 * s * TC_MROWS * 16, bo = 2 * s * TC_NROWS * 16;
                 const uint64_t dah = smem_desc(ah + ao, TC_MROWS * 16, 128);
@@ -164,46 +198,23 @@ __global__ void __launch_bounds__(128) gemm_nt_tc32_kernel(GemmArgs<float> A) {
                 mma_tf32(tmem, dah, dbh, 1u);
             }
             asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
-                             smem_u32(mbar))
+                             smem_u32(mbar + buf))
                          : "memory");
         }
-        // wait for the stage's MMAs (bounded: about two seconds)
-        {
-            uint32_t done = 0;
-            long spins = 0;
-            while (!done) {
-                asm volatile(
-                    "{\n\t.reg .pred p;\n\t"
-                    "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
-                    "selp.b32 %0, 1, 0, p;\n\t}\n"
-                    : "=r"(done)
-                    : "r"(smem_u32(mbar)), "r"(phase)
-                    : "memory");
-                if (!done && ++spins > (1L << 24)) break;
-            }
-            // one verdict for the whole CTA: tcgen05.ld below is warp-collective
-            ok = __syncthreads_and(done != 0) != 0;
-            if (!ok && tid == 0) {
-                if (A.status) atomicExch(A.status, 2);
-                // The stage's MMAs may still be running: they read this CTA's shared memory and write the
-                // tensor memory that the exit path frees. Give their commit a second bounded wait before
-                // the dealloc below. The status word already fails the factorization, so the C tile that
-                // this CTA leaves unwritten is never used.
-                uint32_t drained = 0;
-                for (long s = 0; !drained && s < (1L << 24); ++s)
-                    asm volatile(
-                        "{\n\t.reg .pred p;\n\t"
-                        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
-                        "selp.b32 %0, 1, 0, p;\n\t}\n"
-                        : "=r"(drained)
-                        : "r"(smem_u32(mbar)), "r"(phase)
-                        : "memory");
-            }
-        }
-        phase ^= 1u;
+        last = st;
+        if (st + 1 < nst) load((st + 1) * TC_BK);   // in flight while the tensor cores run this stage
+    }
+    // the last commit covers every MMA issued before it (K = 0: nothing to apply)
+    if (ok && last >= 0) ok = __syncthreads_and(wait_buf(last & 1, last >> 1)) != 0;
+    if (!ok && tid == 0) {
+        if (A.status) atomicExch(A.status, 2);
+        // MMAs may still be running: they read this CTA's shared memory and write the tensor memory that
+        // the exit path frees. Give the last commit a second bounded wait before the dealloc below. The
+        // status word already fails the factorization, so the C tile left unwritten is never used.
+        if (last >= 0) wait_buf(last & 1, last >> 1);
     }
     asm volatile("tcgen05.fence::after_thread_sync;");
-    if (ok && warp < 2) {
+    if (ok && last >= 0) {
         const int r = warp * 32 + lane;
         const uint32_t taddr = tmem + ((uint32_t)(warp * 32) << 16);
 #pragma unroll
@@ -238,7 +249,7 @@ __global__ void __launch_bounds__(128) gemm_nt_tc32_kernel(GemmArgs<float> A) {
         asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(TC_TMEM_COLS));
 }
 
-size_t gemm_tc32_smem() { return 2 * (size_t)TC_A_BYTES + 2 * (size_t)TC_B_BYTES + TC_HEADER; }
+size_t gemm_tc32_smem() { return (size_t)TC_NBUF * TC_STAGE + TC_HEADER; }
 
 cudaError_t launch_gemm_tc32(const GemmArgs<float>& a, int nmembers, cudaStream_t st) {
     if (a.count == 0) return cudaSuccess;
