@@ -35,7 +35,8 @@ constexpr int TC_BK = 32;                       // K per stage: 4 MMAs of K = 8
 constexpr int TC_MROWS = 128, TC_NROWS = 64;    // MMA shape M x N
 constexpr int TC_CHUNKS = TC_BK / 4;            // 16-byte K chunks per row and stage
 constexpr int TC_A_BYTES = TC_CHUNKS * TC_MROWS * 16;   // 16 KB per A part
-constexpr int TC_B_BYTES = TC_CHUNKS * TC_NROWS * 16;   // 8 KB per B part
+constexpr int TC_B_LBO = TC_NROWS * 16;                // B chunks 1 KB apart
+constexpr int TC_B_BYTES = TC_CHUNKS * TC_B_LBO;        // 8 KB per B part
 constexpr int TC_STAGE = 2 * TC_A_BYTES + 2 * TC_B_BYTES;   // one buffer: A and B, hi and lo parts
 constexpr int TC_NBUF = 2;                      // operand buffers (the pipeline depth)
 constexpr int TC_TMEM_COLS = 64;
@@ -74,63 +75,34 @@ __device__ __forceinline__ void mma_tf32(uint32_t tmem, uint64_t adesc, uint64_t
 
 }  // namespace
 
-// Register-staged operand pipeline (two shared-memory buffers): stage s + 1's global loads are in
-// flight while the tensor cores run stage s, and a buffer is refilled only after the MMAs that read it
-// have committed (one mbarrier per buffer, phase = the buffer's use count). The tile is a full
-// 128 x 64 (M = 128 lanes of TMEM), so no half of an MMA is padding.
-__global__ void __launch_bounds__(128) gemm_nt_tc32_kernel(GemmArgs<float> A) {
-    extern __shared__ __align__(1024) uint8_t tsm[];
-    uint64_t* mbar = reinterpret_cast<uint64_t*>(tsm + TC_NBUF * TC_STAGE);   // one per buffer
-    uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(tsm + TC_NBUF * TC_STAGE + 16);
-
-    const GemmTile t = A.tiles[blockIdx.x];
-    const int member = A.members ? A.members[blockIdx.y] : blockIdx.y;
-    if (A.finfo && t.front >= 0 && A.finfo[(int64_t)member * A.ns + t.front] != 0) return;
-    if (t.mode == 2) {   // deferred diagonal-block write
-        const float* src = A.copy_src + (int64_t)member * A.copy_stride + t.a;
-        float* dst = A.cbuf + (int64_t)member * A.cstride + t.c;
-        for (int q = threadIdx.x; q < t.m * t.n; q += blockDim.x) dst[q % t.m + (int64_t)(q / t.m) * t.ldc] = src[q % t.m + (int64_t)(q / t.m) * t.lda];
-        return;
-    }
-    const float* Ab = A.abuf + (int64_t)member * A.astride + t.a;
-    const float* Bb = A.bbuf + (int64_t)member * A.bstride + t.b;
-    float* Cb = A.cbuf + (int64_t)member * A.cstride + t.c;
-    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-    const int M = t.m, N = t.n, K = t.k;
-
-    if (warp == 0) {
-        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tmem_slot)),
-                     "r"(TC_TMEM_COLS));
-        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
-    }
-    if (tid == 0) {
-        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(mbar)));
-        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(mbar + 1)));
-        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
-    }
-    asm volatile("tcgen05.fence::before_thread_sync;");
-    __syncthreads();
-    asm volatile("tcgen05.fence::after_thread_sync;");
-    const uint32_t tmem = *tmem_slot;
-
-    // staging registers: A row `tid`, the stage's 32 columns of the inner dimension; B row tid % 64,
-    // 16 of them (the half tid / 64). Each load instruction of a warp reads 32 consecutive rows.
+// The MMA main loop: D (TMEM, 128 x 64 FP32) = A B^T over K, as 3xTF32. A is M x K column-major
+// (A[r + k lda], M <= 128); B is N x K column-major (B[c + k ldb]), N <= 64. Register-staged operand pipeline with two
+// shared-memory buffers: stage s + 1's global loads are in flight while the tensor cores run stage s,
+// and a buffer is refilled only after the MMAs that read it have committed (one mbarrier per buffer,
+// phase = the buffer's use count). Returns false (the same in every thread) when a bounded wait gave
+// up; `last` = the last stage whose MMAs were committed (-1: none).
+__device__ __forceinline__ bool tc32_mainloop(uint8_t* tsm, uint64_t* mbar, uint32_t tmem, const float* Ab,
+                                              int64_t lda, const float* Bb, int64_t ldb, int M, int N, int K,
+                                              int& last) {
+    const int tid = threadIdx.x;
+    // staging registers: A row `tid`, the stage's 32 columns of the inner dimension; B row tid % 64, 16
+    // of them (the half tid / 64). Each load instruction of a warp reads 32 consecutive rows.
     float ra[TC_BK], rb[TC_BK / 2];
     const int rB = tid & (TC_NROWS - 1), kB = (tid / TC_NROWS) * (TC_BK / 2);
     auto load = [&](int k0) {
 #pragma unroll
         for (int j = 0; j < TC_BK; ++j) {
             const int k = k0 + j;
-            ra[j] = (tid < M && k < K) ? Ab[tid + (int64_t)k * t.lda] : 0.0f;
+            ra[j] = (tid < M && k < K) ? Ab[tid + (int64_t)k * lda] : 0.0f;
         }
 #pragma unroll
         for (int j = 0; j < TC_BK / 2; ++j) {
             const int k = k0 + kB + j;
-            rb[j] = (rB < N && k < K) ? Bb[rB + (int64_t)k * t.ldb] : 0.0f;
+            rb[j] = (rB < N && k < K) ? Bb[rB + (int64_t)k * ldb] : 0.0f;
         }
     };
     // split into TF32 hi and lo parts, in the K-major no-swizzle canonical layout (16-byte chunk c of
-    // row r at (c ROWS + r) 16)
+    // row r at c LBO + 16 r)
     auto put4 = [&](const float* v, uint8_t* hi, uint8_t* lo, int off) {
         uint4 h, l;
         uint32_t* hp = &h.x;
@@ -152,8 +124,7 @@ __global__ void __launch_bounds__(128) gemm_nt_tc32_kernel(GemmArgs<float> A) {
 #pragma unroll
         for (int c = 0; c < TC_CHUNKS; ++c) put4(ra + 4 * c, a_hi, a_lo, (c * TC_MROWS + tid) * 16);
 #pragma unroll
-        for (int c = 0; c < TC_CHUNKS / 2; ++c)
-            put4(rb + 4 * c, b_hi, b_lo, ((kB / 4 + c) * TC_NROWS + rB) * 16);
+        for (int c = 0; c < TC_CHUNKS / 2; ++c) put4(rb + 4 * c, b_hi, b_lo, (kB / 4 + c) * TC_B_LBO + rB * 16);
     };
     // bounded wait (about two seconds of polls) for the commit of a buffer's use `use`
     auto wait_buf = [&](int buf, int use) -> bool {
@@ -170,9 +141,9 @@ __global__ void __launch_bounds__(128) gemm_nt_tc32_kernel(GemmArgs<float> A) {
     };
 
     bool ok = true;
-    int last = -1;   // the last stage whose MMAs were committed
+    last = -1;
     const int nst = (K + TC_BK - 1) / TC_BK;
-    load(0);
+    if (nst > 0) load(0);
     for (int st = 0; st < nst; ++st) {
         const int buf = st & 1;
         bool mine = true;
@@ -188,11 +159,11 @@ __global__ void __launch_bounds__(128) gemm_nt_tc32_kernel(GemmArgs<float> A) {
                            bl = bh + TC_B_BYTES;
 #pragma unroll
             for (int s = 0; s < TC_BK / 8; ++s) {
-                const uint32_t ao = 2 * s * TC_MROWS * 16, bo = 2 * s * TC_NROWS * 16;
+                const uint32_t ao = 2 * s * TC_MROWS * 16, bo = 2 * s * TC_B_LBO;
                 const uint64_t dah = smem_desc(ah + ao, TC_MROWS * 16, 128);
                 const uint64_t dal = smem_desc(al + ao, TC_MROWS * 16, 128);
-                const uint64_t dbh = smem_desc(bh + bo, TC_NROWS * 16, 128);
-                const uint64_t dbl = smem_desc(bl + bo, TC_NROWS * 16, 128);
+                const uint64_t dbh = smem_desc(bh + bo, TC_B_LBO, 128);
+                const uint64_t dbl = smem_desc(bl + bo, TC_B_LBO, 128);
                 mma_tf32(tmem, dal, dbh, (st > 0 || s > 0) ? 1u : 0u);
                 mma_tf32(tmem, dah, dbl, 1u);
                 mma_tf32(tmem, dah, dbh, 1u);
@@ -204,29 +175,86 @@ __global__ void __launch_bounds__(128) gemm_nt_tc32_kernel(GemmArgs<float> A) {
         last = st;
         if (st + 1 < nst) load((st + 1) * TC_BK);   // in flight while the tensor cores run this stage
     }
-    // the last commit covers every MMA issued before it (K = 0: nothing to apply)
+    // the last commit covers every MMA issued before it
     if (ok && last >= 0) ok = __syncthreads_and(wait_buf(last & 1, last >> 1)) != 0;
-    if (!ok && tid == 0) {
-        if (A.status) atomicExch(A.status, 2);
+    if (!ok && tid == 0 && last >= 0) {
         // MMAs may still be running: they read this CTA's shared memory and write the tensor memory that
-        // the exit path frees. Give the last commit a second bounded wait before the dealloc below. The
-        // status word already fails the factorization, so the C tile left unwritten is never used.
-        if (last >= 0) wait_buf(last & 1, last >> 1);
+        // the caller frees. Give the last commit a second bounded wait.
+        wait_buf(last & 1, last >> 1);
     }
+    return ok;
+}
+
+// TMEM allocation (64 columns) and the two mbarriers; every thread gets the TMEM address
+__device__ __forceinline__ uint32_t tc32_setup(uint64_t* mbar, uint32_t* tmem_slot) {
+    if ((threadIdx.x >> 5) == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tmem_slot)),
+                     "r"(TC_TMEM_COLS));
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+    }
+    if (threadIdx.x == 0) {
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(mbar)));
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(mbar + 1)));
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;");
+    __syncthreads();
     asm volatile("tcgen05.fence::after_thread_sync;");
-    if (ok && last >= 0) {
-        const int r = warp * 32 + lane;
-        const uint32_t taddr = tmem + ((uint32_t)(warp * 32) << 16);
+    return *tmem_slot;
+}
+
+__device__ __forceinline__ void tc32_teardown(uint32_t tmem) {
+    asm volatile("tcgen05.fence::before_thread_sync;");
+    __syncthreads();
+    if ((threadIdx.x >> 5) == 0)
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(TC_TMEM_COLS));
+}
+
+// 16 accumulator columns [cb, cb + 16) of this warp's 32 TMEM lanes (row warp * 32 + lane)
+__device__ __forceinline__ void tc32_ld16(uint32_t tmem, int cb, float* out) {
+    uint32_t v[16];
+    const uint32_t taddr = tmem + ((uint32_t)((threadIdx.x >> 5) * 32) << 16) + (uint32_t)cb;
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, "
+        "%14, %15}, [%16];"
+        : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7]),
+          "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]), "=r"(v[14]), "=r"(v[15])
+        : "r"(taddr));
+    asm volatile("tcgen05.wait::ld.sync.aligned;");
+#pragma unroll
+    for (int j = 0; j < 16; ++j) out[j] = __uint_as_float(v[j]);
+}
+
+// The contribution-block updates: C -= A B^T over the tile's lower part (r + diag >= c).
+__global__ void __launch_bounds__(128) gemm_nt_tc32_kernel(GemmArgs<float> A) {
+    extern __shared__ __align__(1024) uint8_t tsm[];
+    uint64_t* mbar = reinterpret_cast<uint64_t*>(tsm + TC_NBUF * TC_STAGE);   // one per buffer
+    uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(tsm + TC_NBUF * TC_STAGE + 16);
+
+    const GemmTile t = A.tiles[blockIdx.x];
+    const int member = A.members ? A.members[blockIdx.y] : blockIdx.y;
+    if (A.finfo && t.front >= 0 && A.finfo[(int64_t)member * A.ns + t.front] != 0) return;
+    if (t.mode == 2) {   // deferred diagonal-block write
+        const float* src = A.copy_src + (int64_t)member * A.copy_stride + t.a;
+        float* dst = A.cbuf + (int64_t)member * A.cstride + t.c;
+        for (int q = threadIdx.x; q < t.m * t.n; q += blockDim.x) dst[q % t.m + (int64_t)(q / t.m) * t.ldc] = src[q % t.m + (int64_t)(q / t.m) * t.lda];
+        return;
+    }
+    const float* Ab = A.abuf + (int64_t)member * A.astride + t.a;
+    const float* Bb = A.bbuf + (int64_t)member * A.bstride + t.b;
+    float* Cb = A.cbuf + (int64_t)member * A.cstride + t.c;
+    const int M = t.m, N = t.n;
+    const uint32_t tmem = tc32_setup(mbar, tmem_slot);
+    int last;
+    const bool ok = tc32_mainloop(tsm, mbar, tmem, Ab, t.lda, Bb, t.ldb, M, N, t.k, last);
+    if (!ok && threadIdx.x == 0 && A.status) atomicExch(A.status, 2);   // the factorization fails
+    asm volatile("tcgen05.fence::after_thread_sync;");
+    if (ok && last >= 0) {   // (K = 0: nothing to apply)
+        const int r = threadIdx.x;
 #pragma unroll
         for (int cb = 0; cb < TC_NROWS; cb += 16) {
-            uint32_t v[16];
-            asm volatile(
-                "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, "
-                "%14, %15}, [%16];"
-                : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7]),
-                  "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]), "=r"(v[14]), "=r"(v[15])
-                : "r"(taddr + (uint32_t)cb));
-            asm volatile("tcgen05.wait::ld.sync.aligned;");
+            float v[16];
+            tc32_ld16(tmem, cb, v);
             float cur[16];
 #pragma unroll
             for (int j = 0; j < 16; ++j) {
@@ -236,17 +264,11 @@ __global__ void __launch_bounds__(128) gemm_nt_tc32_kernel(GemmArgs<float> A) {
 #pragma unroll
             for (int j = 0; j < 16; ++j) {
                 const int c = cb + j;
-                if (r < M && c < N && r + t.diag >= c) {
-                    const float acc = __uint_as_float(v[j]);
-                    Cb[r + (int64_t)c * t.ldc] = t.mode ? acc : cur[j] - acc;
-                }
+                if (r < M && c < N && r + t.diag >= c) Cb[r + (int64_t)c * t.ldc] = t.mode ? v[j] : cur[j] - v[j];
             }
         }
     }
-    asm volatile("tcgen05.fence::before_thread_sync;");
-    __syncthreads();
-    if (warp == 0)
-        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(TC_TMEM_COLS));
+    tc32_teardown(tmem);
 }
 
 size_t gemm_tc32_smem() { return (size_t)TC_NBUF * TC_STAGE + TC_HEADER; }
