@@ -357,7 +357,7 @@ int run_factor(Plan* P, const double* nzval, double eps, double u, int pivot, in
                     a.inv_len = P->df_inv_len;
                     a.finfo = P->d_finfo;
                     a.ns = (int32_t)P->ns;
-                    e = launch_small_inv<T>(a, nm, st);
+                    e = launch_small_inv<T>(a, nm, L.cls, st);
                     if (e != cudaSuccess) break;
                     BlockInvArgs<T> b{};
                     b.fronts = P->d_fronts;
@@ -562,7 +562,7 @@ int run_dataflow(Plan* P, int nrhs, bool transpose, const double* in, int64_t ld
     a.pcnt = fl + 2 * ns + P->df_nblk;
     a.tcnt = fl + 2 * ns + 2 * (int64_t)P->df_nblk;
     a.ccnt = a.tcnt + P->df_ntcnt;
-    a.head = a.ccnt + P->df_nccnt;
+    a.head = fl + P->df_flags_len * P->nbatch;   // one task counter after every member's flags
     a.status = P->d_solve_status;
     a.reorder_fw = ldl || (gen && !transpose);
     a.reorder_bw = ldl || (gen && transpose);
@@ -570,7 +570,20 @@ int run_dataflow(Plan* P, int nrhs, bool transpose, const double* in, int64_t ld
     a.mode = mode;
     a.ldin = ldin;
     a.ldout = ldout;
-    a.trace = P->profile ? P->d_df_trace : nullptr;
+    // batch members: every task once per active member, member-dependent arrays by stride
+    a.nmembers = P->nact;
+    a.members = P->all_members ? nullptr : P->d_members;
+    a.s_fac = P->factor_len;
+    a.s_inv = P->df_inv_len;
+    a.s_piv = P->n;
+    a.s_d = 2 * P->n;
+    a.s_in = ldin * nrhs;
+    a.s_out = ldout * nrhs;
+    a.s_y = P->n * P->max_nrhs;
+    a.s_u = P->ulen;
+    a.s_part = P->df_part_len;
+    a.s_flags = P->df_flags_len;
+    a.trace = (P->profile && P->nact == 1) ? P->d_df_trace : nullptr;
     double ent = 0.0;
     for (double v : P->level_panel_entries) ent += v;
     for (int r0 = 0; r0 < nrhs; r0 += DF_MAX_NRHS) {
@@ -585,25 +598,27 @@ int run_dataflow(Plan* P, int nrhs, bool transpose, const double* in, int64_t ld
         if (grid <= 0) return fail(SDSB200_CUDA_ERROR, "no co-resident grid for the dataflow solve");
         a.in = in + (int64_t)r0 * ldin;
         a.out = out + (int64_t)r0 * ldout;
-        CK(cudaMemsetAsync(P->d_df_flags, 0, sizeof(unsigned int) * P->df_flags_len, st), "dataflow flag reset");
+        CK(cudaMemsetAsync(P->d_df_flags, 0, sizeof(unsigned int) * (P->df_flags_len * P->nbatch + 1), st),
+           "dataflow flag reset");
         prof_begin(P, st);
         cudaError_t e = launch_dataflow_solve<T>(a, grid, smem, st);
         // algorithmic work: every stored panel entry read once per sweep (2 flops per entry and rhs
-        // each way), the right-hand side read and the solution written
-        prof_end(P, st, PK_FWD, 4.0 * ent * a.nrhs, 2.0 * sizeof(T) * ent + 24.0 * P->n * a.nrhs);
+        // each way), the right-hand side read and the solution written, per member
+        prof_end(P, st, PK_FWD, 4.0 * ent * a.nrhs * P->nact,
+                 (2.0 * sizeof(T) * ent + 24.0 * P->n * a.nrhs) * P->nact);
         if (e != cudaSuccess) return cuda_fail(e, "dataflow solve");
     }
     return SDSB200_OK;
 }
 
-// the one-launch solve of a single active member
+// the one-launch solve of the active members
 int run_one_launch(Plan* P, int nrhs, bool transpose, const double* in, int64_t ldin, double* out, int64_t ldout,
                    int mode, cudaStream_t st) {
     return P->elsize == 8 ? run_dataflow<double>(P, nrhs, transpose, in, ldin, out, ldout, mode, st)
                           : run_dataflow<float>(P, nrhs, transpose, in, ldin, out, ldout, mode, st);
 }
 
-bool use_persistent(const Plan* P) { return P->nact == 1 && P->all_members && P->persistent; }
+bool use_persistent(const Plan* P) { return P->persistent; }
 
 int sweeps(Plan* P, int nrhs, bool transpose, cudaStream_t st, int which = 7) {
     return P->elsize == 8 ? run_sweeps<double>(P, nrhs, transpose, st, which)

@@ -817,16 +817,17 @@ cudaError_t launch_chol_step(const CholStepArgs<T>& a, int nmembers, cudaStream_
 template cudaError_t launch_chol_step<double>(const CholStepArgs<double>&, int, cudaStream_t);
 template cudaError_t launch_chol_step<float>(const CholStepArgs<float>&, int, cudaStream_t);
 
-// Inverse of a lower-triangular 32 x 32 matrix held by the warp: lane c computes column c by forward
-// substitution, x_k = (delta_kc - sum_{j<k} L[k, j] x_j) r_k, with the reciprocals r_k = 1 / L[k, k]
-// taken up front (off the substitution's dependency chain). L(k, j) reads entry (k, j) (k, j < 32).
-template <class Get>
-__device__ __forceinline__ void warp_tri_inv32(Get L, int lane, double (&x)[32]) {
-    double rd[32];
+// Inverse of a lower-triangular N x N matrix (N <= 32) held by the warp: lane c computes column c by
+// forward substitution, x_k = (delta_kc - sum_{j<k} L[k, j] x_j) r_k, with the reciprocals
+// r_k = 1 / L[k, k] taken up front (off the substitution's dependency chain). L(k, j) reads entry (k, j)
+// (k, j < N).
+template <int N, class Get>
+__device__ __forceinline__ void warp_tri_inv(Get L, int lane, double (&x)[N]) {
+    double rd[N];
 #pragma unroll
-    for (int k = 0; k < 32; ++k) rd[k] = 1.0 / L(k, k);
+    for (int k = 0; k < N; ++k) rd[k] = 1.0 / L(k, k);
 #pragma unroll
-    for (int k = 0; k < 32; ++k) {
+    for (int k = 0; k < N; ++k) {
         double acc = (k == lane) ? 1.0 : 0.0;
 #pragma unroll
         for (int j = 0; j < k; ++j) acc -= L(k, j) * x[j];
@@ -867,7 +868,7 @@ __global__ void __launch_bounds__(128) block_inv_kernel(BlockInvArgs<T> A) {
     if (warp < 2) {
         const int o = 32 * warp;
         double x[32];
-        warp_tri_inv32([&](int k, int j) { return S[(o + k) + (o + j) * LD]; }, lane, x);
+        warp_tri_inv<32>([&](int k, int j) { return S[(o + k) + (o + j) * LD]; }, lane, x);
         __syncwarp();
 #pragma unroll
         for (int k = 0; k < 32; ++k) S[(o + k) + (o + lane) * LD] = k >= lane ? x[k] : 0.0;
@@ -909,9 +910,11 @@ __global__ void __launch_bounds__(128) block_inv_kernel(BlockInvArgs<T> A) {
     }
 }
 
-// L11^-1 of a warp front of the dataflow solve (w <= 32; unit or not, as stored), one warp per front,
-// padded with the identity past w
-template <typename T>
+// L11^-1 of a warp front of the dataflow solve (w <= N <= 32; unit or not, as stored), one warp per
+// front, padded with the identity past w. Instances for N = 8, 16 and 32: the narrow ones hold a
+// fraction of the registers, so many more warps are resident (batches of small systems have hundreds
+// of thousands of such fronts).
+template <typename T, int N>
 __global__ void __launch_bounds__(256) small_inv_kernel(SmallInvArgs<T> A) {
     const int wi = (int)((blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5), lane = threadIdx.x & 31;
     if (wi >= A.count) return;
@@ -922,25 +925,27 @@ __global__ void __launch_bounds__(256) small_inv_kernel(SmallInvArgs<T> A) {
     const int f = fd.f, w = fd.w;
     const T* P = A.panels + (int64_t)member * A.factor_len + fd.panel;
     T* inv = A.inv + (int64_t)member * A.inv_len + A.inv_off[s];
-    double x[32];
-    warp_tri_inv32([&](int k, int j) { return k < w ? (double)P[k + (int64_t)j * f] : (k == j ? 1.0 : 0.0); }, lane, x);
+    double x[N];
+    warp_tri_inv<N>([&](int k, int j) { return k < w ? (double)P[k + (int64_t)j * f] : (k == j ? 1.0 : 0.0); }, lane, x);
     if (lane < w) {
 #pragma unroll
-        for (int k = 0; k < 32; ++k)
+        for (int k = 0; k < N; ++k)
             if (k < w) inv[k + (int64_t)w * lane] = T(k >= lane ? x[k] : 0.0);
     }
 }
 
 template <typename T>
-cudaError_t launch_small_inv(const SmallInvArgs<T>& a, int nmembers, cudaStream_t st) {
+cudaError_t launch_small_inv(const SmallInvArgs<T>& a, int nmembers, int wmax, cudaStream_t st) {
     if (a.count == 0) return cudaSuccess;
     dim3 grid((a.count + 7) / 8, nmembers);
-    small_inv_kernel<T><<<grid, 256, 0, st>>>(a);
+    if (wmax > 0 && wmax <= 8) small_inv_kernel<T, 8><<<grid, 256, 0, st>>>(a);
+    else if (wmax > 0 && wmax <= 16) small_inv_kernel<T, 16><<<grid, 256, 0, st>>>(a);
+    else small_inv_kernel<T, 32><<<grid, 256, 0, st>>>(a);
     return cudaGetLastError();
 }
 
-template cudaError_t launch_small_inv<double>(const SmallInvArgs<double>&, int, cudaStream_t);
-template cudaError_t launch_small_inv<float>(const SmallInvArgs<float>&, int, cudaStream_t);
+template cudaError_t launch_small_inv<double>(const SmallInvArgs<double>&, int, int, cudaStream_t);
+template cudaError_t launch_small_inv<float>(const SmallInvArgs<float>&, int, int, cudaStream_t);
 
 template <typename T>
 cudaError_t launch_block_inv(const BlockInvArgs<T>& a, int nmembers, cudaStream_t st) {

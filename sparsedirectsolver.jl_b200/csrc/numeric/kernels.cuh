@@ -265,7 +265,8 @@ struct SmallInvArgs {
     int32_t ns;
 };
 template <typename T>
-cudaError_t launch_small_inv(const SmallInvArgs<T>& a, int nmembers, cudaStream_t st);
+cudaError_t launch_small_inv(const SmallInvArgs<T>& a, int nmembers, int wmax, cudaStream_t st);   // wmax: widest
+                                                                                             // front (0: 32)
 cudaError_t prepare_dataflow_kernels(int max_smem);
 
 constexpr int CHOL_NB = 32;   // column block of the large-front Cholesky (one warp per diagonal block)

@@ -281,7 +281,8 @@ Plan* build_plan(const sdsb200_symbolic* sym, const sdsb200_plan_options* popts,
             throw BuildError(SDSB200_INVALID_VALUE, "tuning: wide (the tallest warp front of the solve) must lie in 16..128");
         const int tune_chains = tune_rsv & 1, tune_streams = (tune_rsv >> 1) & 15, tune_steps = (tune_rsv >> 5) & 1;
         const int warp_f = tune_wide ? tune_wide : DF_WARP_F;
-        const bool pinv_mode = tune_chains == 0;   // tiled fronts solved through inverse panels
+        // tiled fronts solved through inverse panels (single-system plans; batches use block chains)
+        const bool pinv_mode = tune_chains == 0 && P->nbatch == 1;
         P->fsmall_max = classes.back();
         auto class_of = [&](int f) {
             for (int c : classes)
@@ -1106,8 +1107,9 @@ Plan* build_plan(const sdsb200_symbolic* sym, const sdsb200_plan_options* popts,
 
             P->d_df_rptr = upload(P, rptr, st);
             P->d_df_csrc = upload(P, csrc, st);
-            P->d_df_part = dalloc<double>(P, std::max<int64_t>(1, std::max<int64_t>(npart, npslot) * DF_BLK * DF_MAX_NRHS));
-            P->d_df_flags = dalloc<unsigned int>(P, P->df_flags_len);
+            P->df_part_len = std::max<int64_t>(1, std::max<int64_t>(npart, npslot) * DF_BLK * DF_MAX_NRHS);
+            P->d_df_part = dalloc<double>(P, P->df_part_len * P->nbatch);
+            P->d_df_flags = dalloc<unsigned int>(P, P->df_flags_len * P->nbatch + 1);
             P->d_df_trace = dalloc<int64_t>(P, 6 * (int64_t)std::max<int32_t>(1, P->n_df_tasks));
             // The inverses are built level by level on the side stream, each level's right after its
             // factorization launches (single-system plans only: a batch is solved by the per-level
@@ -1286,6 +1288,48 @@ Plan* build_plan(const sdsb200_symbolic* sym, const sdsb200_plan_options* popts,
                 }
                 for (auto& kv : side) merged.insert(merged.end(), kv.second.begin(), kv.second.end());
                 P->prog.swap(merged);
+            } else {
+                // uniform batches: launches after the factorization build every member's warp-front
+                // L11^-1 (one launch per width class 8, 16, 32) and 64 x 64 diagonal-block inverses
+                // (the tiled fronts run as block chains)
+                std::vector<int32_t> small_all, blk_all;
+                std::vector<int32_t> by_w[3];
+                for (int L = 0; L < P->nlevels; ++L)
+                    for (int s : P->level_fronts[L]) {
+                        if (!df[s].tiled) {
+                            const int w = P->fronts[s].w;
+                            by_w[w <= 8 ? 0 : w <= 16 ? 1 : 2].push_back(s);
+                            continue;
+                        }
+                        for (int b = 0; b < df[s].nblk; ++b) {
+                            blk_all.push_back(s);
+                            blk_all.push_back(b);
+                        }
+                    }
+                const int wcls[3] = {8, 16, 32};
+                std::vector<ProgLaunch> inv_l;
+                for (int c = 0; c < 3; ++c) {
+                    ProgLaunch il_{};
+                    il_.kind = L_DFINV;
+                    il_.level = P->nlevels;
+                    il_.cls = wcls[c];
+                    il_.list = (int64_t)small_all.size();
+                    il_.list2 = 0;
+                    il_.count = to_i32((int64_t)by_w[c].size(), "inverse launch");
+                    il_.count2 = inv_l.empty() ? to_i32((int64_t)blk_all.size() / 2, "inverse launch") : 0;
+                    small_all.insert(small_all.end(), by_w[c].begin(), by_w[c].end());
+                    if (il_.count + il_.count2 > 0) inv_l.push_back(il_);
+                }
+                if (inv_l.empty() && !blk_all.empty()) {
+                    ProgLaunch il_{};
+                    il_.kind = L_DFINV;
+                    il_.level = P->nlevels;
+                    il_.count2 = to_i32((int64_t)blk_all.size() / 2, "inverse launch");
+                    inv_l.push_back(il_);
+                }
+                P->d_df_small = upload(P, small_all, st);
+                P->d_df_blkinv = upload(P, blk_all, st);
+                P->prog.insert(P->prog.end(), inv_l.begin(), inv_l.end());
             }
         }
         {
@@ -1503,7 +1547,7 @@ Plan* build_plan(const sdsb200_symbolic* sym, const sdsb200_plan_options* popts,
             P->d_pcnt = dalloc<unsigned int>(P, P->psplit_cnts);
             cudaMemsetAsync(P->d_pcnt, 0, sizeof(unsigned int) * P->psplit_cnts, st);
         }
-        P->d_xtmp = dalloc<double>(P, n * P->max_nrhs);
+        P->d_xtmp = dalloc<double>(P, n * P->max_nrhs * nb);
         P->d_solve_status = dalloc<int32_t>(P, 1);
         cudaMemsetAsync(P->d_solve_status, 0, sizeof(int32_t), st);
         P->d_Y = dalloc<double>(P, n * P->max_nrhs * nb);

@@ -118,7 +118,8 @@ struct Plan {
     int32_t* d_df_rptr = nullptr;       // per front row: start of its contributions (f + 1 per front)
     int32_t* d_df_csrc = nullptr;       // contributions: the children's global update rows, in child order
     unsigned int* d_df_flags = nullptr; // fcnt (ns), bdone (ns), xflag (nblk), pcnt (nblk), head
-    int64_t df_flags_len = 0;
+    int64_t df_flags_len = 0;            // per member (the task counter follows every member's flags)
+    int64_t df_part_len = 0;             // partial-product doubles per member
     int32_t df_nblk = 0;
     int32_t df_ntcnt = 0, df_nccnt = 0;  // inverse panels: forward row-tile and backward column-block counters
     bool df_pinv = false;               // tiled fronts solved through their inverse panels
@@ -171,7 +172,7 @@ struct Plan {
         int64_t launches = 0;
     };
     bool use_graphs = true;
-    bool persistent = true;        // the one-launch dataflow solve for a single active member
+    bool persistent = true;        // the one-launch dataflow solve (every active member in one launch)
     cudaStream_t own = nullptr;          // capture / replay stream, joined to the caller's by events
     cudaEvent_t join_in = nullptr, join_out = nullptr;
     cudaStream_t side = nullptr;         // low-priority stream of the side launches of the factorization

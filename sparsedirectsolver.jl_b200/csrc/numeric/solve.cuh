@@ -147,6 +147,12 @@ struct DataflowArgs {
     int32_t mode;              // 0: X = solve(B); 2: X += solve(R)
     int32_t warp_smem;         // doubles of shared memory per warp of a bundle task
     int64_t* trace;            // profiling, or NULL: per task (start, wait done, end) %globaltimer ns, CTA, kind, a | b << 32
+    // uniform batches: the launch runs every task for each of nmembers members (task-major, so a task
+    // still waits only on tasks earlier in the launch's order); the member-dependent arrays above are
+    // member 0's and advance by these strides (elements)
+    int32_t nmembers;
+    const int32_t* members;    // the members' indices (NULL: 0 .. nmembers - 1)
+    int64_t s_fac, s_inv, s_piv, s_d, s_in, s_out, s_y, s_u, s_part, s_flags;
 };
 
 template <typename T>

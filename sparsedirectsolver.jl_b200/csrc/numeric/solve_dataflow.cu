@@ -1032,20 +1032,50 @@ __device__ __noinline__ void df_pinv_backward(const DataflowArgs<T>& A, int s, i
 
 }  // namespace
 
+// the arguments of one batch member: the member-dependent arrays advanced by its strides
+template <typename T>
+__device__ __forceinline__ void df_member_args(const DataflowArgs<T>& A, int member, DataflowArgs<T>& B) {
+    B = A;
+    const int64_t q = member;
+    B.facf += q * A.s_fac;
+    B.facb += q * A.s_fac;
+    B.invf += q * A.s_inv;
+    B.invb += q * A.s_inv;
+    if (B.piv) B.piv += q * A.s_piv;
+    if (B.d) B.d += q * A.s_d;
+    if (B.kind) B.kind += q * A.s_piv;
+    B.in += q * A.s_in;
+    B.out += q * A.s_out;
+    B.Y += q * A.s_y;
+    B.xtmp += q * A.s_y;
+    B.U += q * A.s_u;
+    B.part += q * A.s_part;
+    B.fcnt += q * A.s_flags;
+    B.bdone += q * A.s_flags;
+    B.xflag += q * A.s_flags;
+    B.pcnt += q * A.s_flags;
+    B.tcnt += q * A.s_flags;
+    B.ccnt += q * A.s_flags;
+}
+
 template <typename T, int NR>
-__global__ void __launch_bounds__(DF_THREADS, 2) dataflow_solve_kernel(DataflowArgs<T> A) {
+__global__ void __launch_bounds__(DF_THREADS, 2) dataflow_solve_kernel(DataflowArgs<T> A0) {
     extern __shared__ double dsm[];
     __shared__ int task_k, bundle_next;
+    __shared__ DataflowArgs<T> A;   // this task's member's arguments
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int total = A0.ntasks * A0.nmembers;
     while (true) {
         if (threadIdx.x == 0) {
-            task_k = atomicAdd(A.head, 1u);
+            task_k = atomicAdd(A0.head, 1u);
             bundle_next = 0;
-            if (*(volatile int32_t*)A.status != 0) task_k = A.ntasks;   // a wait gave up: stop
+            if (*(volatile int32_t*)A0.status != 0) task_k = total;   // a wait gave up: stop
         }
         __syncthreads();
-        const int k = task_k;
-        if (k >= A.ntasks) break;
+        if (task_k >= total) break;
+        const int k = task_k / A0.nmembers, j = task_k - k * A0.nmembers;
+        if (threadIdx.x == 0) df_member_args(A0, A0.members ? A0.members[j] : j, A);
+        __syncthreads();
         const DfTask tk = A.tasks[k];
         if (A.trace && threadIdx.x == 0) {
             A.trace[6 * k] = (int64_t)df_clock();

@@ -482,3 +482,48 @@ def test_fused_subtrees_match_level_launches(torch_cuda, structure, precision):
             assert np.array_equal(out[4]["kind"][:n], O.kind[:n])
     else:
         assert np.array_equal(out[4]["st"][:, :2].sum(0), O.stats_matrix()[:, :2].sum(0))
+
+
+@pytest.mark.parametrize("structure,precision", [("SPD", "fp64"), ("S", "fp64"), ("G", "fp64"), ("SPD", "fp32")])
+def test_batch_dataflow_solve_matches_level_sweeps(torch_cuda, structure, precision):
+    # a uniform batch solved by the one-launch dataflow solve (every active member's tasks in one launch,
+    # block chains for the tiled fronts) against the per-level sweeps: all members, 10 right-hand sides
+    # (two groups of the launch), A^T for LU, and a subset of the members
+    from sdsb200._native import numeric_lib
+
+    lib = numeric_lib()
+    A = {"SPD": lambda: M.lap3d(12, 12, 12, seed=6), "S": lambda: small_kkt(16, 16, 100, seed=2),
+         "G": lambda: M.convection_diffusion3d(10, 10, 10, seed=6)}[structure]()
+    nb, n, nrhs = 5, A.shape[0], 10
+    vals = M.batch_members(A, nb, spread=0.1, seed=3)
+    ir = {} if precision == "fp64" else dict(ir_n_steps=10, ir_tol=1e-14)
+    ds = _solver((A.indptr, A.indices, vals.reshape(-1), n), structure, reordering_alg="nd", max_nrhs=nrhs,
+                 factor_precision=precision, **ir)
+    ds.execute("analysis")
+    assert list(ds.execute("factorization")) == [0] * nb
+    b = np.random.default_rng(4).uniform(-1, 1, (nb, n, nrhs))
+    out = {}
+    for mode in (1, 0):
+        lib.sdsb200_set_persistent(ds._plan, mode)
+        for tr in ((False, True) if structure == "G" else (False,)):
+            ds.setparam("solve_mode", int(tr))
+            x = ds.execute("solve", None, b).cpu().numpy().reshape(nb, n, nrhs)
+            for k in range(nb):
+                Ak = sp.csr_matrix((vals[k], A.indices, A.indptr), shape=A.shape)
+                assert M.scaled_backward_error(Ak.T.tocsr() if tr else Ak, x[k], b[k]) <= BERR
+            out[mode, tr] = x
+    ds.setparam("solve_mode", 0)
+    assert lib.sdsb200_plan_stat(ds._plan, b"solve_status") == 0
+    for key in out:
+        if key[0] == 1:
+            x1, x0 = out[key], out[0, key[1]]
+            assert np.abs(x1 - x0).max() <= (1e-10 if precision == "fp64" else 1e-9) * np.abs(x0).max()
+    # a subset of the members: the others' X is kept
+    lib.sdsb200_set_persistent(ds._plan, 1)
+    ds.setparam("ubatch_index", 2)
+    x0 = np.zeros((nb, n, nrhs))
+    xs = ds.execute("solve", x0, b)
+    xs = (xs.cpu().numpy() if hasattr(xs, "cpu") else np.asarray(xs)).reshape(nb, n, nrhs)
+    ds.setparam("ubatch_index", -1)
+    assert np.abs(xs[2] - out[1, False][2]).max() <= 1e-12 * np.abs(out[1, False][2]).max() + 1e-300
+    assert not np.any(xs[[0, 1, 3, 4]])
