@@ -1139,16 +1139,15 @@ Plan* build_plan(const sdsb200_symbolic* sym, const sdsb200_plan_options* popts,
                     if (lf.empty()) continue;
                     std::vector<ProgLaunch>& side_b = side[{L, sg}];
                     std::vector<int> pf;   // the batch's inverse-panel fronts
-                    ProgLaunch il_{};
-                    il_.kind = L_DFINV;
-                    il_.level = L;
-                    il_.side = 1;
-                    il_.list = (int64_t)small_sorted.size();
-                    il_.list2 = (int64_t)blk_sorted.size() / 2;
+                    // the warp fronts' L11^-1 in one launch per width class (8, 16, 32: the narrow
+                    // kernels hold far fewer registers); the first also takes the diagonal blocks
+                    std::vector<int32_t> by_w[3];
+                    const int64_t blk0 = (int64_t)blk_sorted.size() / 2;
                     for (int s : lf) {
                         if (s == P->schur_front || fstream[s] != sg) continue;
                         if (!df[s].tiled) {
-                            small_sorted.push_back(s);
+                            const int w = P->fronts[s].w;
+                            by_w[w <= 8 ? 0 : w <= 16 ? 1 : 2].push_back(s);
                             continue;
                         }
                         for (int b = 0; b < df[s].nblk; ++b) {
@@ -1157,9 +1156,23 @@ Plan* build_plan(const sdsb200_symbolic* sym, const sdsb200_plan_options* popts,
                         }
                         if (df[s].pinv) pf.push_back(s);
                     }
-                    il_.count = to_i32((int64_t)small_sorted.size() - il_.list, "inverse launch");
-                    il_.count2 = to_i32((int64_t)blk_sorted.size() / 2 - il_.list2, "inverse launch");
-                    if (il_.count + il_.count2 > 0) side_b.push_back(il_);
+                    bool blk_done = false;
+                    for (int c = 0; c < 3; ++c) {
+                        ProgLaunch il_{};
+                        il_.kind = L_DFINV;
+                        il_.level = L;
+                        il_.side = 1;
+                        il_.cls = 8 << c;
+                        il_.list = (int64_t)small_sorted.size();
+                        il_.list2 = blk0;
+                        il_.count = to_i32((int64_t)by_w[c].size(), "inverse launch");
+                        il_.count2 = blk_done ? 0 : to_i32((int64_t)blk_sorted.size() / 2 - blk0, "inverse launch");
+                        small_sorted.insert(small_sorted.end(), by_w[c].begin(), by_w[c].end());
+                        if (il_.count + il_.count2 > 0) {
+                            side_b.push_back(il_);
+                            blk_done = true;
+                        }
+                    }
                     // one launch of tiles; a tile with a long inner dimension becomes nsplit CTAs
                     auto push_launch = [&](std::vector<PinvTile>& v, int cls) {
                         ProgLaunch pl{};
