@@ -259,6 +259,13 @@ def run_config(args):
                 bt = torch.from_numpy(b).cuda()
                 times = autotune(ub.solver, bt, reps=2, use_cache=False)
                 best = min(times, key=times.get)
+                if form == "mixed":
+                    # the fewest refinement steps whose every system meets the bound (untimed probe)
+                    ub.execute("factorization")
+                    for k in range(0, 9):
+                        ub.solver.setparam("ir_n_steps", k)
+                        if ub.backward_errors(ub.execute("solve", None, bt).cpu().numpy(), b).max() <= BERR_TARGET:
+                            break
 
                 def step():
                     ub.execute("factorization")
@@ -269,6 +276,7 @@ def run_config(args):
                 errs = ub.backward_errors(x, b)
                 line["forms"][form] = {"ms_per_step": round(ms, 3), "systems_per_s": round(1024 / (ms / 1e3), 1),
                                        "max_bwd_err": float(errs.max()), "analysis_s": round(analysis_s, 2),
+                                       "ir_steps": ub.solver.getparam("ir_n_steps") if form == "mixed" else 0,
                                        "tuning": describe(best),
                                        "autotune_ms": {str(describe(k)): round(v, 3) for k, v in times.items()},
                                        "solve_launches": int(ub.solver.plan_stat("launches_done"))}
@@ -284,19 +292,32 @@ def run_config(args):
                 ds = DirectSolver((A.indptr, A.indices, vals.reshape(-1), n), "SPD", **fkw)
                 ds.execute("analysis")
 
+                def member_errs(x):
+                    out = []
+                    for k in range(256):
+                        Ak = A.copy()
+                        Ak.data = vals[k]
+                        out.append(M.scaled_backward_error(Ak, x[k], b[k]))
+                    return out
+
+                if form == "mixed":
+                    # the fewest refinement steps whose every member meets the bound (untimed probe)
+                    ds.execute("factorization")
+                    for k in range(0, 9):
+                        ds.setparam("ir_n_steps", k)
+                        if max(member_errs(ds.execute("solve", None, bt).cpu().numpy())) <= BERR_TARGET:
+                            break
+
                 def step():
                     ds.execute("factorization")
                     ds.execute("solve", None, bt)
 
                 ms = _time(torch, step, args.steps, args.warmup)
                 x = ds.execute("solve", None, bt).cpu().numpy()
-                errs = []
-                for k in range(256):
-                    Ak = A.copy()
-                    Ak.data = vals[k]
-                    errs.append(M.scaled_backward_error(Ak, x[k], b[k]))
+                errs = member_errs(x)
                 line["forms"][form] = {"ms_per_step": round(ms, 3), "systems_per_s": round(256 / (ms / 1e3), 1),
-                                       "max_bwd_err": float(max(errs))}
+                                       "max_bwd_err": float(max(errs)),
+                                       "ir_steps": ds.getparam("ir_n_steps") if form == "mixed" else 0}
         line["speedup_mixed_vs_fp64"] = round(line["forms"]["fp64"]["ms_per_step"] /
                                               line["forms"]["mixed"]["ms_per_step"], 3)
     print(json.dumps(line), flush=True)
