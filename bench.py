@@ -610,6 +610,27 @@ def main():
         berr = M.scaled_backward_error(A, x, b)
         results[name] = dict(ms=ms, gflops=world * flops / (ms / 1e3) / 1e9, berr=berr, ir_steps=irsteps[-1],
                              launches=launches, clocks=clk.summary(), x=x, info=int(info[0]))
+    # the API's default refinement loop, timed beside the headline (not the metric's value): the mixed
+    # form with a tolerance on max_k ||r_k|| / ||b_k|| (ir_tol = 1e-12, up to 20 steps), which reads the
+    # residual norms back to the host after every step and stops at the first step that meets it
+    tol_loop = None
+    if not dist:
+        mixed.setparam("ir_n_steps", 20)
+        mixed.setparam("ir_tol", BERR_TARGET)
+        for _ in range(args.warmup):
+            step(mixed)
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        tsteps = 0
+        for _ in range(args.steps):
+            tsteps = step(mixed)[0]
+        e1.record()
+        torch.cuda.synchronize()
+        tol_loop = {"ms_per_step": round(e0.elapsed_time(e1) / args.steps, 3), "ir_steps": tsteps,
+                    "ir_tol": BERR_TARGET, "bwd_err": float(M.scaled_backward_error(A, Xd.t().cpu().numpy(), b))}
+        mixed.setparam("ir_n_steps", results["mixed"]["ir_steps"])
+        mixed.setparam("ir_tol", 0.0)
     # error of the mixed solution against the FP64 one, per right-hand side
     xf, xm = results["fp64"]["x"], results["mixed"]["x"]
     err_vs_fp64 = [float(np.abs(xm[:, r] - xf[:, r]).max() / np.abs(xf[:, r]).max()) for r in range(NRHS)]
@@ -734,6 +755,7 @@ def main():
                    "factor_flops_stored": S.flops, "parallelism": f"replicas x{world}",
                    "l2": "inputs larger than L2 (factor %.0f MB)" % (S.nnz_stored * 4 / 1e6)},
         "bwd_err": r["berr"], "ir_steps": r["ir_steps"], "ir_probe_bwd_err": ir_probe,
+        "mixed_tolerance_loop": tol_loop,
         "err_vs_fp64_per_rhs": err_vs_fp64,
         "fp64": {"ms_per_step": round(results["fp64"]["ms"], 3), "value": round(results["fp64"]["gflops"], 3),
                  "bwd_err": results["fp64"]["berr"], "unit": "GFLOP/s",
