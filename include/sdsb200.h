@@ -214,10 +214,10 @@ int sdsb200_set_interrupt(sdsb200_plan* plan, const volatile int32_t* h_flag);
  * then polled before a factorization and before each refinement step, not between launch groups. */
 int sdsb200_set_graphs(sdsb200_plan* plan, int32_t on);
 
-/* Solve engine when a single batch member is active. Nonzero (default): the dataflow solve, one
- * cooperative persistent launch per group of 8 right-hand sides with no grid barrier (tasks in a
- * topological order of the elimination tree, synchronised by per-front counters and per-block flags);
- * 0: one launch per level and sweep (the engine of uniform batches and of the solve sub-phases). */
+/* Solve engine. Nonzero (default): the dataflow solve, one cooperative persistent launch per group of
+ * 8 right-hand sides with no grid barrier (tasks in a topological order of the elimination tree,
+ * synchronised by per-front counters and per-block flags; a uniform batch runs every active member's
+ * tasks in the same launch); 0: one launch per level and sweep (the engine of the solve sub-phases). */
 int sdsb200_set_persistent(sdsb200_plan* plan, int32_t on);
 
 /* Profiling mode (on != 0): CUDA events around every launch of the following factor and solve
