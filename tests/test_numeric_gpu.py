@@ -527,3 +527,4 @@ def test_batch_dataflow_solve_matches_level_sweeps(torch_cuda, structure, precis
     ds.setparam("ubatch_index", -1)
     assert np.abs(xs[2] - out[1, False][2]).max() <= 1e-12 * np.abs(out[1, False][2]).max() + 1e-300
     assert not np.any(xs[[0, 1, 3, 4]])
+
