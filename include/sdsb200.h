@@ -112,9 +112,7 @@ typedef struct sdsb200_plan_options {
  * batch of its large fronts' 32-column steps as dataflow tasks in one persistent launch, 0 (default) =
  * one launch per step and kernel; subtree (bits 26-29, SDSB200_TUNING_SUBTREE): the fused subtrees
  * (the reference's regime A: maximal subtrees of shared-memory fronts, each factored by one CTA in
- * one launch per size class) hold up to 2^subtree fronts of any shared-memory class (1..14), are off
- * (15), or by default (0) hold up to 16 fronts of at most 64 rows and are used only when they take in
- * at least 32 fronts per SM (many tiny fronts: batches of small systems).
+ * one launch per size class) hold up to 2^subtree fronts (1..14), or are off (0, the default, and 15).
  * Bits 30 and 31 must be zero. */
 #define SDSB200_TUNING(fsmall, wide, chains) \
     ((int32_t)(fsmall) | ((int32_t)(wide) << 9) | ((int32_t)(chains) << 20))

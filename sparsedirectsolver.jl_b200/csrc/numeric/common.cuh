@@ -97,9 +97,6 @@ struct PinvTile {
 };
 constexpr int PINV_KSPLIT = 256;   // longest inner dimension of one CTA's part
 
-constexpr int SUBTREE_FRONTS_DEFAULT = 16;     // tuning subtree = 0: most fronts of one fused subtree,
-constexpr int SUBTREE_DEFAULT_MAX_ROWS = 64;    // the largest front order in one,
-constexpr int SUBTREE_MIN_FRONTS_PER_SM = 32;   // and the fewest fronts in subtrees per SM to use them
 constexpr int FSTREAM_DEFAULT = 4;   // factorization streams of a single-system Cholesky plan
 constexpr int FSTREAM_MIN_CP = 16;   // the critical path (32-column steps) of a subtree given its own stream
 

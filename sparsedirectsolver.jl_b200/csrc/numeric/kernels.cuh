@@ -10,6 +10,7 @@ namespace sds {
 template <typename T>
 struct SmallArgs {
     DeviceMaps maps;
+    int32_t count;           // fronts of the launch (the warp-per-front kernel)
     const int32_t* list;     // fronts of this launch
     const int32_t* sub_ptr;  // fused subtrees: subtree b is list[sub_ptr[b] .. sub_ptr[b + 1]) (NULL: one
                              // front per CTA)

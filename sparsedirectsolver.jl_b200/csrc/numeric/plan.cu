@@ -327,18 +327,17 @@ Plan* build_plan(const sdsb200_symbolic* sym, const sdsb200_plan_options* popts,
         // fill the device. One CTA factors each, front after front in a postorder whose children come
         // by decreasing (stack peak - contribution block) (Liu's order, as the reference's), so that the
         // subtree's stack of contribution blocks stays small; they are launched before the stream's
-        // first level. tuning subtree: 15 = off; 1..14: subtrees of up to 2^subtree fronts of any
-        // shared-memory class; 0 (default): up to SUBTREE_FRONTS_DEFAULT fronts of at most 64 rows, and
-        // only when they hold at least SUBTREE_MIN_FRONTS_PER_SM fronts per SM. A subtree runs its
-        // fronts one after another, so it pays where the bottom levels are throughput-bound (far more
-        // tiny fronts than resident CTAs: batches of small systems), and costs where a level's launch
-        // is latency-bound (measured on lap3d 48^3 and lap2d 64^2).
+        // first level. tuning subtree: 1..14: subtrees of up to 2^subtree fronts; 0 and 15 (default):
+        // none. A subtree runs its fronts one after another, so it pays only where the bottom levels
+        // are throughput-bound (far more tiny fronts than resident CTAs: batches of small systems; the
+        // autotuner tries it) and costs where a level's launch is latency-bound (lap3d 48^3, lap2d 64^2);
+        // the warp-per-front launches of such batches are faster still where the fronts have at most
+        // 32 rows (1024 uneven 2-D systems: 6.40 against 6.79 ms with 16-front subtrees).
         std::vector<int> sub_of(ns, -1);
         struct Sub { int root, stream, cls; int64_t stack; std::vector<int> order; std::vector<int64_t> off; };
         std::vector<Sub> subs;
-        if (tune_sub != 15 && ns > 0) {
-            const int64_t maxfronts = tune_sub ? (int64_t(1) << tune_sub) : SUBTREE_FRONTS_DEFAULT;
-            const int fcap = tune_sub ? (1 << 30) : SUBTREE_DEFAULT_MAX_ROWS;
+        if (tune_sub != 15 && tune_sub != 0 && ns > 0) {
+            const int64_t maxfronts = int64_t(1) << tune_sub;
             int dev0 = 0, sms0 = 148;
             cudaGetDevice(&dev0);
             cudaDeviceGetAttribute(&sms0, cudaDevAttrMultiProcessorCount, dev0);
@@ -356,7 +355,7 @@ Plan* build_plan(const sdsb200_symbolic* sym, const sdsb200_plan_options* popts,
                 const DFront& F = P->fronts[s];
                 const int64_t m = F.f - F.w;
                 cbsz[s] = (F.parent >= 0 && m > 0) ? ((m * m + 31) & ~int64_t(31)) : 0;
-                bool e = s != P->schur_front && class_of(F.f) != 0 && F.f <= fcap;
+                bool e = s != P->schur_front && class_of(F.f) != 0;
                 for (int q = F.ch_begin; q < F.ch_end; ++q) {
                     const int c = (int)(child_list[q] - 1);
                     kids[s].push_back(c);
@@ -415,11 +414,6 @@ Plan* build_plan(const sdsb200_symbolic* sym, const sdsb200_plan_options* popts,
                 }
                 P->nsubtree_fronts += (int64_t)t.order.size();
                 subs.push_back(std::move(t));
-            }
-            if (!tune_sub && P->nsubtree_fronts < (int64_t)SUBTREE_MIN_FRONTS_PER_SM * sms0) {
-                subs.clear();
-                std::fill(sub_of.begin(), sub_of.end(), -1);
-                P->nsubtree_fronts = 0;
             }
             P->nsubtrees = (int64_t)subs.size();
         }

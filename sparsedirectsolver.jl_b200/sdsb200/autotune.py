@@ -10,9 +10,8 @@ Two shapes decide how the fronts of a plan map onto the kernels:
   blocks (no extra factorization work, one dependency link per block).
 * ``streams`` (not searched, default 4): independent subtrees of a Cholesky front tree factored on
   separate streams.
-* ``subtree``: fused subtrees of shared-memory fronts, one CTA each (0: the plan's default rule, up
-  to 16 fronts of at most 64 rows where there are many), or none (15: one launch per level and size
-  class).
+* ``subtree``: fused subtrees of shared-memory fronts, one CTA each (4: up to 16 fronts per
+  subtree), or none (0: one launch per level and size class).
 
 The autotuner times factorization + solve for each candidate on the solver's own matrix and
 right-hand side (CUDA events, after a warm-up), keeps the fastest, and leaves the solver planned
@@ -23,7 +22,7 @@ from __future__ import annotations
 from .capi import tuning as make_tuning
 
 CANDIDATES = tuple((fs, wd, ch, 0, 0, sub) for fs in (0, 128, 96) for wd in (0, 64) for ch in (0, 1)
-                   for sub in (0, 15))
+                   for sub in (0, 4))
 
 _cache: dict = {}
 

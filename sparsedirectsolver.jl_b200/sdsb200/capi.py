@@ -45,8 +45,7 @@ def tuning(fsmall=0, wide=0, chains=0, streams=0, steps=0, subtree=0):
     tiled fronts by 64-column block chains instead of inverse panels; streams = the factorization streams
     of a single-system Cholesky plan (0 = 4, 1 = level by level); steps = 1 runs its large fronts' steps
     as one dataflow launch per batch instead of one launch per step and kernel; subtree = the fused
-    subtrees (1..14: at most 2**subtree fronts each, 15: none, 0: at most 16 fronts of at most 64 rows,
-    used when they take in at least 32 fronts per SM)."""
+    subtrees (1..14: at most 2**subtree fronts each; 0, the default, and 15: none)."""
     return (int(fsmall) | (int(wide) << 9) | (int(chains) << 20) | (int(streams) << 21) | (int(steps) << 25)
             | (int(subtree) << 26))
 

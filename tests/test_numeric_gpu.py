@@ -444,7 +444,7 @@ def test_fused_subtrees_match_level_launches(torch_cuda, structure, precision):
     # fused subtrees (one CTA factors a whole subtree of shared-memory fronts in postorder; at most 16
     # fronts each, and at most 4) against one launch per level and size class (tuning subtree = 15): the
     # same panels, pivots, kinds, D and statistics bit for bit; the oracle's pivots and statistics in
-    # FP64, and its inertia in FP32. The default (subtree = 0) leaves these small trees level by level.
+    # FP64, and its inertia in FP32. The default (subtree = 0) fuses none.
     from sdsb200.capi import tuning
 
     A, reordering = {"SPD": lambda: (M.lap2d_shifted(40, 40, seed=3), "amd"),
