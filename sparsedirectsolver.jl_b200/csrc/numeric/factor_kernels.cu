@@ -219,28 +219,30 @@ __global__ void __launch_bounds__(256) subtree_kernel(SmallArgs<T> A) {
     }
 }
 
-// One Cholesky front of at most WARP_FRONT_F rows by one warp, in its own shared-memory slice F
-// (WARP_FRONT_F x (WARP_FRONT_F + 1) entries). The arithmetic of every entry is small_front's, in the
-// same order (assembly runs summed in entry order by the run's first lane; children's contributions
-// added in child order; per column the scaling by the reciprocal square root and the rank-1 update in
-// column order), so the results are bit for bit the CTA kernel's; only the mapping of entries to
-// threads differs. Batches of small systems have hundreds of thousands of such fronts, and a warp per
-// front keeps eight of them in flight per CTA instead of one; a launch of few fronts keeps the CTA
-// kernel, whose 128 threads shorten each front's chain (lap2d 64^2: 1.04 against 1.35 ms per
-// factorization). Fused subtrees keep the CTA kernel too: one warp per subtree was slower (1024
-// uneven systems: 6.79 against 5.93 ms).
+// One Cholesky front of at most WARP_FRONT_F rows by one warp, in its own shared-memory slice F: the
+// lower triangle packed by columns (column j holds rows j .. f - 1 from offset j f - j (j - 1) / 2),
+// since a Cholesky front reads and writes nothing above its diagonal. The arithmetic of every entry is
+// small_front's, in the same order (assembly runs summed in entry order by the run's first lane;
+// children's contributions added in child order; per column the scaling by the reciprocal square
+// root and the rank-1 update in column order), so the results are bit for bit the CTA kernel's; only
+// the mapping of entries to threads differs. Batches of small systems have hundreds of thousands of
+// such fronts, and a warp per front keeps eight of them in flight per CTA instead of one; a launch of
+// few fronts keeps the CTA kernel, whose 128 threads shorten each front's chain (lap2d 64^2: 1.04
+// against 1.35 ms per factorization). Fused subtrees keep the CTA kernel too: one warp per subtree was
+// slower (1024 uneven systems: 6.79 against 5.93 ms).
 constexpr int WARP_FRONT_F = 32;
 constexpr int WARP_FRONTS_PER_CTA = 8;
+constexpr int WARP_FRONT_LEN = WARP_FRONT_F * (WARP_FRONT_F + 1) / 2;   // packed entries per warp
 constexpr int64_t WARP_FRONT_MIN_LAUNCH = 4096;   // fronts x members of a launch for the warp kernel
 
 template <typename T>
 __device__ __forceinline__ void warp_front_spd(const SmallArgs<T>& A, const int s, const int member, T* F) {
     const DFront fd = A.maps.fronts[s];
     const int f = fd.f, w = fd.w, m = f - w;
-    const int ld = f | 1;
     const int lane = threadIdx.x & 31;
+    auto at = [&](int i, int j) -> T& { return F[j * f - ((j * (j - 1)) >> 1) + (i - j)]; };   // i >= j
     const double* nz = A.nzval + (int64_t)member * A.nnz;
-    for (int q = lane; q < ld * f; q += 32) F[q] = T(0);
+    for (int q = lane; q < (f * (f + 1)) / 2; q += 32) F[q] = T(0);
     __syncwarp();
     for (int k = fd.am_begin + lane; k < fd.am_end; k += 32) {
         const int code = A.maps.am_loc[k];
@@ -249,8 +251,10 @@ __device__ __forceinline__ void warp_front_spd(const SmallArgs<T>& A, const int 
         for (int q = k; q < fd.am_end && A.maps.am_loc[q] == code; ++q) acc += T(nz[A.maps.am_src[q]]);
         const int loc = (code > 0 ? code : -code) - 1;
         const int i = loc % f, j = loc / f;
-        if (code > 0) F[i + j * ld] += acc;
-        else F[j + i * ld] += acc;
+        // (an entry above the diagonal is never read by a Cholesky front: the CTA kernel's square
+        // slice holds it unused)
+        if (code > 0 && i >= j) at(i, j) += acc;
+        else if (code < 0 && j >= i) at(j, i) += acc;
     }
     __syncwarp();
     const T* cbar = A.cb + (int64_t)member * A.cb_len;
@@ -263,31 +267,31 @@ __device__ __forceinline__ void warp_front_spd(const SmallArgs<T>& A, const int 
         for (int jj = 0; jj < mc; ++jj) {
             const int pj = ri[jj];
             batched_add<4, T>(jj + lane, 32, mc, [&](int ii) { return (double)C[ii + (int64_t)jj * mc]; },
-                              [&](int ii) -> T* { return F + ri[ii] + pj * ld; });
+                              [&](int ii) -> T* { return &at(ri[ii], pj); });
         }
         __syncwarp();
     }
     int status = 0;
     const double eps = A.eps;
     for (int j = 0; j < w; ++j) {
-        const double ajj = (double)F[j + j * ld];
+        const double ajj = (double)at(j, j);
         const bool ok = ajj > eps || (eps > 0 && ajj >= 0);
         if (!ok) { status = j + 1; break; }
         const double djj = sqrt(fmax(ajj, eps));
         const T inv = T(1.0 / djj);
         __syncwarp();
-        for (int i = j + 1 + lane; i < f; i += 32) F[i + j * ld] *= inv;
-        if (lane == 0) F[j + j * ld] = T(djj);
+        for (int i = j + 1 + lane; i < f; i += 32) at(i, j) *= inv;
+        if (lane == 0) at(j, j) = T(djj);
         __syncwarp();
         for (int l = j + 1; l < f; ++l) {
-            const T flj = F[l + j * ld];
-            for (int i = l + lane; i < f; i += 32) F[i + l * ld] -= F[i + j * ld] * flj;
+            const T flj = at(l, j);
+            for (int i = l + lane; i < f; i += 32) at(i, l) -= at(i, j) * flj;
         }
         __syncwarp();
     }
     T* P = A.factor + (int64_t)member * A.factor_len + fd.panel;
     for (int j = 0; j < w; ++j)
-        for (int i = lane; i < f; i += 32) P[i + (int64_t)j * f] = i < j ? T(0) : F[i + j * ld];
+        for (int i = lane; i < f; i += 32) P[i + (int64_t)j * f] = i < j ? T(0) : at(i, j);
     if (lane == 0) {
         int64_t* S = A.stats + ((int64_t)member * A.ns + s) * NSTAT;
         S[ST_NPOS] = status ? status - 1 : w;
@@ -297,7 +301,7 @@ __device__ __forceinline__ void warp_front_spd(const SmallArgs<T>& A, const int 
     if (fd.cb >= 0 && m > 0 && status == 0) {
         T* C = A.cb + (int64_t)member * A.cb_len + fd.cb;
         for (int jj = 0; jj < m; ++jj)
-            for (int ii = jj + lane; ii < m; ii += 32) C[ii + (int64_t)jj * m] = F[w + ii + (w + jj) * ld];
+            for (int ii = jj + lane; ii < m; ii += 32) C[ii + (int64_t)jj * m] = at(w + ii, w + jj);
     }
     __syncwarp();
 }
@@ -309,7 +313,7 @@ __global__ void __launch_bounds__(256) warp_front_kernel(SmallArgs<T> A) {
     const int wi = blockIdx.x * WARP_FRONTS_PER_CTA + (threadIdx.x >> 5);
     const int member = A.members ? A.members[blockIdx.y] : blockIdx.y;
     if (wi >= A.count) return;
-    T* F = reinterpret_cast<T*>(smem_raw) + (threadIdx.x >> 5) * WARP_FRONT_F * (WARP_FRONT_F + 1);
+    T* F = reinterpret_cast<T*>(smem_raw) + (threadIdx.x >> 5) * WARP_FRONT_LEN;
     warp_front_spd<T>(A, A.list[wi], member, F);
 }
 
@@ -327,7 +331,7 @@ cudaError_t launch_small(int structure, const SmallArgs<T>& a, int count, int nm
     const bool sub = a.sub_ptr != nullptr;
     if (structure == STRUCT_SPD && fmax <= WARP_FRONT_F && !sub &&
         (int64_t)count * nmembers >= WARP_FRONT_MIN_LAUNCH) {   // a warp per front
-        const size_t wsmem = sizeof(T) * WARP_FRONTS_PER_CTA * WARP_FRONT_F * (WARP_FRONT_F + 1);
+        const size_t wsmem = sizeof(T) * WARP_FRONTS_PER_CTA * WARP_FRONT_LEN;
         dim3 wgrid((count + WARP_FRONTS_PER_CTA - 1) / WARP_FRONTS_PER_CTA, nmembers);
         SmallArgs<T> b = a;
         b.count = count;
