@@ -815,6 +815,7 @@ int sdsb200_solve(sdsb200_plan* plan, double* X, int64_t ldx, const double* B, i
             }
             r.nzval = nzval; r.X = X; r.B = B; r.R = P->d_R;
             r.n = P->n; r.nnz = P->nnz; r.ldx = ldx; r.ldb = ldb; r.nrhs = nrhs;
+            r.entries = P->full_nnz;
             prof_begin(P, s);
             cudaError_t re = launch_residual(r, P->nact, s);
             prof_end(P, s, PK_RESIDUAL, 2.0 * P->full_nnz * nrhs * P->nact,
@@ -1126,6 +1127,7 @@ extern "C" int sdsb200_residual(sdsb200_plan* plan, double* R, const double* X, 
     }
     r.nzval = nzval; r.X = X; r.B = B; r.R = R;
     r.n = P->n; r.nnz = P->nnz; r.ldx = ldx; r.ldb = ldb; r.nrhs = nrhs;
+    r.entries = P->full_nnz;
     cudaError_t e = launch_residual(r, P->nact, (cudaStream_t)stream);
     return e == cudaSuccess ? SDSB200_OK : cuda_fail(e, "residual");
 }

@@ -193,6 +193,7 @@ struct ResidualArgs {
     double* R;
     int64_t n, nnz, ldx, ldb;
     int32_t nrhs;
+    int64_t entries;           // entries of the map (rowptr[n]): short rows take one thread each
 };
 
 struct NormArgs {

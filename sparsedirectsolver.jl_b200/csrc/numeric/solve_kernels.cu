@@ -461,7 +461,8 @@ cudaError_t launch_permute(const PermArgs& a, int nmembers, cudaStream_t st) {
     return cudaGetLastError();
 }
 
-// R = B - op(A) X over the full-pattern map (duplicates summed in source order); one warp per row
+// R = B - op(A) X over the full-pattern map (duplicates summed in source order); one warp per row (long
+// rows; residual_rows_kernel below takes maps of short rows)
 __global__ void residual_kernel(ResidualArgs A) {
     const int member = A.members ? A.members[blockIdx.y] : blockIdx.y;
     const int64_t n = A.n;
@@ -496,7 +497,44 @@ __global__ void residual_kernel(ResidualArgs A) {
     }
 }
 
+// The same residual with one thread per row, for maps of short rows (a warp per row leaves most lanes
+// idle and holds one row's dependent loads in flight per warp): each row's entries summed in order.
+__global__ void residual_rows_kernel(ResidualArgs A) {
+    const int member = A.members ? A.members[blockIdx.y] : blockIdx.y;
+    const int64_t n = A.n;
+    const double* nz = A.nzval + (int64_t)member * A.nnz;
+    const double* X = A.X + (int64_t)member * A.ldx * A.nrhs;
+    const double* B = A.B + (int64_t)member * A.ldb * A.nrhs;
+    double* R = A.R + (int64_t)member * n * A.nrhs;
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t e0 = A.rowptr[i], e1 = A.rowptr[i + 1];
+        for (int r0 = 0; r0 < A.nrhs; r0 += 8) {
+            const int rc = min(8, A.nrhs - r0);
+            double acc[8];
+#pragma unroll
+            for (int r = 0; r < 8; ++r) acc[r] = 0.0;
+            for (int64_t e = e0; e < e1; ++e) {
+                double v = 0.0;
+                for (int64_t q = A.srcptr[e]; q < A.srcptr[e + 1]; ++q) v += nz[A.src[q]];
+                const int64_t c = A.colval[e];
+#pragma unroll
+                for (int r = 0; r < 8; ++r)
+                    if (r < rc) acc[r] += v * X[c + (int64_t)(r0 + r) * A.ldx];
+            }
+#pragma unroll
+            for (int r = 0; r < 8; ++r)
+                if (r < rc) R[i + (int64_t)(r0 + r) * n] = B[i + (int64_t)(r0 + r) * A.ldb] - acc[r];
+        }
+    }
+}
+
 cudaError_t launch_residual(const ResidualArgs& a, int nmembers, cudaStream_t st) {
+    if (a.n > 0 && a.entries <= 16 * a.n) {   // rows of at most 16 entries on average
+        int blocks = (int)std::min<int64_t>((a.n + 255) / 256, 8192);
+        dim3 grid(blocks > 0 ? blocks : 1, nmembers);
+        residual_rows_kernel<<<grid, 256, 0, st>>>(a);
+        return cudaGetLastError();
+    }
     int64_t warps = a.n;
     int blocks = (int)std::min<int64_t>((warps * 32 + 255) / 256, 8192);
     dim3 grid(blocks > 0 ? blocks : 1, nmembers);
