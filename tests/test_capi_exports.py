@@ -107,3 +107,34 @@ def test_ctypes_mirrors_match_the_headers(tmp_path):
         assert ctypes.sizeof(cls) == layout[(st, "size")], st
         for f in names:
             assert getattr(cls, f).offset == layout[(st, f)], (st, f)
+
+
+def test_tuning_encoder_matches_the_header_macros(tmp_path):
+    """capi.tuning (and autotune.describe) encode the plan tuning as the header's SDSB200_TUNING* macros."""
+    import shutil
+    import subprocess
+    import sys
+
+    if not shutil.which("gcc"):
+        pytest.skip("gcc is missing")
+    sys.path.insert(0, PKG)
+    from sdsb200.autotune import CANDIDATES, describe
+    from sdsb200.capi import tuning
+
+    cases = [(96, 64, 1, 3, 0, 0), (128, 0, 0, 0, 1, 4), (0, 32, 0, 15, 0, 14), (224, 128, 1, 1, 1, 15)]
+    lines = ['#include <stdio.h>', '#include "sdsb200.h"', "int main(void) {"]
+    for fs, wd, ch, st, steps, sub in cases:
+        expr = (f"SDSB200_TUNING_STREAMS({fs}, {wd}, {ch}, {st}) | SDSB200_TUNING_SUBTREE({sub})"
+                + (" | SDSB200_TUNING_STEPS" if steps else ""))
+        lines.append(f'printf("%d\\n", (int)({expr}));')
+    lines.append("return 0; }")
+    src = tmp_path / "tuning.c"
+    src.write_text("\n".join(lines))
+    exe = tmp_path / "tuning"
+    subprocess.run(["gcc", "-I", os.path.join(ROOT, "include"), str(src), "-o", str(exe)], check=True)
+    out = [int(v) for v in subprocess.run([str(exe)], check=True, capture_output=True, text=True).stdout.split()]
+    for case, c_value in zip(cases, out):
+        assert tuning(*case) == c_value, case
+        d = describe(c_value)
+        assert (d["fsmall"], d["wide"], d["chains"], d["streams"], d["steps"], d["subtree"]) == case
+    assert all(tuning(*c) >= 0 for c in CANDIDATES)
